@@ -1,0 +1,459 @@
+"""Python host mirror of the reference's sparse direct solver API over the C ABI of libampsolve.so.
+
+Names, argument meaning and error behaviour follow jwt625/applied-multiphysics packages/core/src/la/sparse.mjs
+(analyze, factorNumeric, solveNumeric, solveNumericMulti, SparseCholesky, amdOrder, ndOrder, patternFingerprint,
+checkSymbolic, matVec), ldlt.mjs (SupernodalLDLT) and order3d.mjs (nd3Order): misuse raises AmpError with the
+reference's message, a numerical failure returns ok = False. The symbolic phase runs on the host inside the library;
+the numeric factorization and the solves run on the GPU. There is no CPU fallback: without libampsolve.so (or without
+a GPU for the numeric calls) every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import time
+from typing import Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libampsolve.so")
+_lib = None
+
+AMP_OK, AMP_NOT_SPD, AMP_NONFINITE_PIVOT, AMP_PATTERN_MISMATCH, AMP_BAD_LENGTH, AMP_NO_FACTOR, AMP_NEED_COORDS, \
+    AMP_DEVICE_TIMEOUT, AMP_CUDA_ERROR, AMP_OOM, AMP_INVALID = range(11)
+ORDER_AMD, ORDER_ND, ORDER_ND3, ORDER_GIVEN = range(4)
+CHOLESKY, LDLT = 0, 1
+FP64, MIXED = 0, 1
+
+FIELDS = ["perm", "pinv", "parent", "colCount", "lowerP", "lowerI", "lowerSrc", "superStart", "colSuper",
+          "superParent", "childHead", "childNext", "Sp", "Si", "Lxp"]
+
+
+class AmpError(Exception):
+    """Raised where the reference throws an Error; ``code`` is the amp_status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(msg)
+        self.code = code
+
+
+class _AnalyzeOpts(C.Structure):
+    _fields_ = [("ordering", C.c_int), ("relax", C.c_int), ("perm", C.c_void_p), ("x", C.c_void_p),
+                ("y", C.c_void_p), ("z", C.c_void_p), ("leaf", C.c_int), ("device", C.c_int)]
+
+
+class _PlanInfo(C.Structure):
+    _fields_ = [("n", C.c_int32), ("nsuper", C.c_int32), ("max_front", C.c_int32), ("nlevels", C.c_int32),
+                ("nnz_l", C.c_int64), ("nnz_a", C.c_int64), ("nnz_l_stored", C.c_int64), ("pattern_nnz", C.c_int64),
+                ("fill", C.c_double), ("flops", C.c_double), ("ordering_ms", C.c_double),
+                ("symbolic_ms", C.c_double), ("device_bytes", C.c_int64)]
+
+
+class _FactorOpts(C.Structure):
+    _fields_ = [("kind", C.c_int), ("precision", C.c_int)]
+
+
+class _FactorResult(C.Structure):
+    _fields_ = [("ok", C.c_int32), ("n_neg", C.c_int32), ("n_perturbed", C.c_int32), ("fail_column", C.c_int32),
+                ("ms", C.c_double)]
+
+
+class _RefineOpts(C.Structure):
+    _fields_ = [("max_steps", C.c_int), ("tol", C.c_double)]
+
+
+class _RefineStats(C.Structure):
+    _fields_ = [("rel_residual", C.c_double), ("steps", C.c_int32)]
+
+
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+
+# every entry point of include/ampsolve.h with its argument types
+SIGNATURES = {
+    "amp_amd_order": (C.c_int, [C.c_int32, _i32p, _i32p, C.c_double, _i32p]),
+    "amp_nd_order": (C.c_int, [C.c_int32, _i32p, _i32p, C.c_void_p, C.c_void_p, C.c_int32, _i32p]),
+    "amp_nd3_order": (C.c_int, [C.c_int32, _i32p, _i32p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, _i32p]),
+    "amp_pattern_fingerprint": (C.c_int, [C.c_int32, _i32p, _i32p, C.c_char_p, C.c_int32]),
+    "amp_analyze": (C.c_int, [C.c_int32, _i32p, _i32p, C.POINTER(_AnalyzeOpts), C.POINTER(C.c_void_p)]),
+    "amp_plan_get_info": (C.c_int, [C.c_void_p, C.POINTER(_PlanInfo)]),
+    "amp_plan_array": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]),
+    "amp_plan_fingerprint": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32]),
+    "amp_plan_check_pattern": (C.c_int, [C.c_void_p, C.c_int32, _i32p, _i32p]),
+    "amp_plan_destroy": (None, [C.c_void_p]),
+    "amp_factor_create": (C.c_int, [C.c_void_p, C.POINTER(_FactorOpts), C.POINTER(C.c_void_p)]),
+    "amp_factor_numeric": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_double,
+                                     C.POINTER(_FactorResult)]),
+    "amp_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int]),
+    "amp_solve_refined": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int, C.POINTER(_RefineOpts),
+                                    C.POINTER(_RefineStats)]),
+    "amp_factor_download": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "amp_factor_destroy": (None, [C.c_void_p]),
+    "amp_matvec": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    "amp_last_error": (C.c_char_p, []),
+}
+
+
+def lib():
+    """The loaded libampsolve.so (raises when it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            raise RuntimeError(f"{_LIB_PATH} is missing: build it with __graft_entry__.build() (no CPU fallback)")
+        L = C.CDLL(_LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(code: int):
+    if code != AMP_OK:
+        raise AmpError(code, lib().amp_last_error().decode())
+
+
+def _pat(pat):
+    n = int(pat.n)
+    rp = np.ascontiguousarray(pat.rowptr, dtype=np.int32)
+    ci = np.ascontiguousarray(pat.colidx, dtype=np.int32)
+    if ci.size == 0:
+        ci = np.zeros(1, np.int32)
+    return n, rp, ci
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+# ---- orderings (sparse.mjs amdOrder / ndOrder, order3d.mjs nd3Order) ----------------------------------------------
+def amdOrder(pat, denseFactor: float = 10.0) -> np.ndarray:
+    n, rp, ci = _pat(pat)
+    out = np.zeros(max(n, 1), np.int32)
+    _check(lib().amp_amd_order(n, rp, ci, denseFactor, out))
+    return out[:n]
+
+
+def ndOrder(pat, x, y, leaf: int = 48) -> np.ndarray:
+    n, rp, ci = _pat(pat)
+    out = np.zeros(max(n, 1), np.int32)
+    xa, ya = _f64(x), _f64(y)
+    _check(lib().amp_nd_order(n, rp, ci, _ptr(xa), _ptr(ya), leaf, out))
+    return out[:n]
+
+
+def nd3Order(pat, x, y, z, leaf: int = 2000) -> np.ndarray:
+    n, rp, ci = _pat(pat)
+    out = np.zeros(max(n, 1), np.int32)
+    xa, ya, za = _f64(x), _f64(y), _f64(z)
+    _check(lib().amp_nd3_order(n, rp, ci, _ptr(xa), _ptr(ya), _ptr(za), leaf, out))
+    return out[:n]
+
+
+def patternFingerprint(pat) -> str:
+    n, rp, ci = _pat(pat)
+    buf = C.create_string_buffer(64)
+    _check(lib().amp_pattern_fingerprint(n, rp, ci, buf, 64))
+    return buf.value.decode()
+
+
+# ---- symbolic analysis --------------------------------------------------------------------------------------------
+class SymbolicAnalysis:
+    """Result of analyze (SymbolicAnalysis, types.d.mts:13-20): scalars eagerly, arrays on first access."""
+
+    def __init__(self, handle: int):
+        self._h = handle
+        info = _PlanInfo()
+        _check(lib().amp_plan_get_info(handle, C.byref(info)))
+        self.n = info.n
+        self.nsuper = info.nsuper
+        self.maxFront = info.max_front
+        self.nlevels = info.nlevels
+        self.nnzL = info.nnz_l
+        self.nnzA = info.nnz_a
+        self.nnzLStored = info.nnz_l_stored
+        self.fill = info.fill
+        self.flops = info.flops
+        self.deviceBytes = info.device_bytes
+        self.timing = {"ordering_ms": info.ordering_ms, "symbolic_ms": info.symbolic_ms}
+        buf = C.create_string_buffer(64)
+        _check(lib().amp_plan_fingerprint(handle, buf, 64))
+        self.patternKey = buf.value.decode()
+        self._arrays = {}
+
+    def __getattr__(self, name):
+        if name in FIELDS:
+            if name not in self._arrays:
+                k = FIELDS.index(name)
+                ln = C.c_int64(0)
+                _check(lib().amp_plan_array(self._h, k, None, 0, C.byref(ln)))
+                arr = np.zeros(max(ln.value, 1), np.int64 if name == "Lxp" else np.int32)
+                _check(lib().amp_plan_array(self._h, k, arr.ctypes.data, ln.value, C.byref(ln)))
+                self._arrays[name] = arr[: ln.value]
+            return self._arrays[name]
+        raise AttributeError(name)
+
+    @property
+    def handle(self) -> int:
+        return self._h
+
+    def __del__(self):
+        h = self.__dict__.get("_h")
+        if h and _lib is not None:
+            _lib.amp_plan_destroy(h)
+            self._h = None
+
+
+def analyze(pat, opts: dict | None = None, **kw) -> SymbolicAnalysis:
+    """analyze(pat, {perm, ordering: 'amd' | 'nd' | 'nd3', x, y, z, relax, leaf}) (sparse.mjs:666)."""
+    o = dict(opts or {})
+    o.update(kw)
+    n, rp, ci = _pat(pat)
+    ao = _AnalyzeOpts()
+    ao.relax = 1 if o.get("relax", True) else 0
+    ao.leaf = int(o.get("leaf", 0) or 0)
+    ao.device = int(o.get("device", 0))
+    keep = []
+    perm = o.get("perm")
+    if perm is not None:
+        pa = np.ascontiguousarray(perm, dtype=np.int32)
+        if pa.shape[0] != n:
+            raise AmpError(AMP_BAD_LENGTH, f"analyze: perm has length {pa.shape[0]}, pattern has {n} rows")
+        keep.append(pa)
+        ao.ordering, ao.perm = ORDER_GIVEN, pa.ctypes.data
+    else:
+        ordering = o.get("ordering", "amd")
+        if ordering == "nd":
+            x, y = o.get("x"), o.get("y")
+            if x is None or y is None or len(x) != n or len(y) != n:
+                raise AmpError(AMP_NEED_COORDS, "analyze: ordering nd needs node coordinates x and y of length n")
+            xa, ya = _f64(x), _f64(y)
+            keep += [xa, ya]
+            ao.ordering, ao.x, ao.y = ORDER_ND, xa.ctypes.data, ya.ctypes.data
+        elif ordering == "nd3":
+            x, y, z = o.get("x"), o.get("y"), o.get("z")
+            if any(c is None or len(c) != n for c in (x, y, z)):
+                raise AmpError(AMP_NEED_COORDS, "nd3Order: needs DOF coordinates x, y and z of length n")
+            xa, ya, za = _f64(x), _f64(y), _f64(z)
+            keep += [xa, ya, za]
+            ao.ordering, ao.x, ao.y, ao.z = ORDER_ND3, xa.ctypes.data, ya.ctypes.data, za.ctypes.data
+        elif ordering == "amd":
+            ao.ordering = ORDER_AMD
+        else:
+            raise AmpError(AMP_INVALID, f"analyze: unknown ordering {ordering}")
+    h = C.c_void_p()
+    _check(lib().amp_analyze(n, rp, ci, C.byref(ao), C.byref(h)))
+    return SymbolicAnalysis(h.value)
+
+
+def checkSymbolic(sym: SymbolicAnalysis, pat) -> None:
+    """Throw unless `sym` was analysed from `pat` (sparse.mjs:928-930)."""
+    n, rp, ci = _pat(pat)
+    if sym is None:
+        raise AmpError(AMP_PATTERN_MISMATCH, "symbolic analysis is for a different sparsity pattern")
+    _check(lib().amp_plan_check_pattern(sym.handle, n, rp, ci))
+
+
+# ---- numeric factor ------------------------------------------------------------------------------------------------
+class NumericFactor:
+    """Device factor of one symbolic analysis (NumericFactor, types.d.mts:23; SupernodalLDLT storage)."""
+
+    def __init__(self, sym: SymbolicAnalysis, kind: int = CHOLESKY, precision: int = FP64):
+        self.sym = sym
+        self.kind = kind
+        self.precision = precision
+        self.kernel = "cuda-sm100a"
+        self.ok = False
+        self.nNeg = 0
+        self.nPerturbed = 0
+        self.ms = 0.0
+        self.failColumn = -1
+        fo = _FactorOpts(kind, precision)
+        h = C.c_void_p()
+        _check(lib().amp_factor_create(sym.handle, C.byref(fo), C.byref(h)))
+        self._h = h.value
+
+    @property
+    def handle(self) -> int:
+        return self._h
+
+    def factor(self, values, pivotTol: float = 1e-13, on_device: bool = False) -> bool:
+        res = _FactorResult()
+        if on_device:  # values is a device pointer (int) with the pattern's nnz entries
+            ptr, nv = values
+            _check(lib().amp_factor_numeric(self._h, C.c_void_p(ptr), int(nv), 1, pivotTol, C.byref(res)))
+        else:
+            v = _f64(values)
+            _check(lib().amp_factor_numeric(self._h, v.ctypes.data if v.size else None, v.size, 0, pivotTol,
+                                            C.byref(res)))
+        self.ok = bool(res.ok)
+        self.nNeg, self.nPerturbed, self.ms, self.failColumn = res.n_neg, res.n_perturbed, res.ms, res.fail_column
+        return self.ok
+
+    def solve_block(self, B: np.ndarray) -> np.ndarray:
+        """B: (q, n) FP64 host array; returns X (q, n)."""
+        B = _f64(B)
+        q = B.shape[0] if B.ndim == 2 else 1
+        X = np.empty_like(B)
+        if B.size:
+            _check(lib().amp_solve(self._h, B.ctypes.data, q, X.ctypes.data, 0))
+        elif not self.ok:
+            _check(lib().amp_solve(self._h, None, q, None, 0))
+        return X
+
+    def solve_refined_block(self, B: np.ndarray, maxSteps: int = 3, tol: float = 1e-14):
+        B = _f64(B)
+        q = B.shape[0] if B.ndim == 2 else 1
+        X = np.empty_like(B)
+        st = _RefineStats()
+        ro = _RefineOpts(maxSteps, tol)
+        _check(lib().amp_solve_refined(self._h, B.ctypes.data if B.size else None, q,
+                                       X.ctypes.data if X.size else None, 0, C.byref(ro), C.byref(st)))
+        return X, st.rel_residual, st.steps
+
+    @property
+    def Lx(self) -> np.ndarray:
+        out = np.zeros(max(self.sym.nnzLStored, 1))
+        _check(lib().amp_factor_download(self._h, out.ctypes.data, None))
+        return out[: self.sym.nnzLStored]
+
+    @property
+    def D(self) -> np.ndarray:
+        out = np.zeros(max(self.sym.n, 1))
+        _check(lib().amp_factor_download(self._h, None, out.ctypes.data))
+        return out[: self.sym.n]
+
+    def matVec(self, x) -> np.ndarray:
+        xa = _f64(x)
+        y = np.empty_like(xa)
+        q = xa.shape[0] if xa.ndim == 2 else 1
+        _check(lib().amp_matvec(self._h, xa.ctypes.data, q, y.ctypes.data))
+        return y
+
+    def __del__(self):
+        h = self.__dict__.get("_h")
+        if h and _lib is not None:
+            _lib.amp_factor_destroy(h)
+            self._h = None
+
+
+def _nnz_of(sym: SymbolicAnalysis) -> int:
+    return int(sym.patternKey.split(":")[1])
+
+
+def factorNumeric(sym: SymbolicAnalysis, values, num: NumericFactor | None = None, pat=None,
+                  opts: dict | None = None) -> NumericFactor:
+    """factorNumeric(sym, values, num?, pat?, {factor?}) (sparse.mjs:941): ok = False when not positive definite."""
+    if pat is not None:
+        checkSymbolic(sym, pat)
+    nv = len(values)
+    if nv != _nnz_of(sym):
+        raise AmpError(AMP_BAD_LENGTH, f"factorNumeric: {nv} values for a pattern with {_nnz_of(sym)} entries")
+    if num is None or num.sym is not sym:
+        num = NumericFactor(sym, CHOLESKY, FP64)
+    num.factor(values)
+    return num
+
+
+def solveNumeric(num: NumericFactor, b, out=None) -> np.ndarray:
+    """solveNumeric(num, b, out?) (sparse.mjs:1261)."""
+    if num is None or not num.ok:
+        raise AmpError(AMP_NO_FACTOR, "solveNumeric: no successful numeric factorization")
+    x = num.solve_block(_f64(b).reshape(1, -1)).reshape(-1)
+    if out is not None:
+        out[:] = x
+        return out
+    return x
+
+
+def solveNumericMulti(num: NumericFactor, bs: Sequence, outs=None) -> list:
+    """solveNumericMulti(num, bs[], outs?) (sparse.mjs:1308): one pass over the factor for all vectors."""
+    if num is None or not num.ok:
+        raise AmpError(AMP_NO_FACTOR, "solveNumericMulti: no successful numeric factorization")
+    if len(bs) == 0:
+        return []
+    X = num.solve_block(np.stack([_f64(b) for b in bs]))
+    res = []
+    for k in range(len(bs)):
+        if outs is not None and outs[k] is not None:
+            outs[k][:] = X[k]
+            res.append(outs[k])
+        else:
+            res.append(X[k].copy())
+    return res
+
+
+def matVec(pat, val, x, out=None) -> np.ndarray:
+    """y = A x on full CSR storage (sparse.mjs:219-228), host arithmetic for the caller's convenience."""
+    import scipy.sparse as sp
+    n = int(pat.n)
+    A = sp.csr_matrix((_f64(val), np.asarray(pat.colidx), np.asarray(pat.rowptr)), shape=(n, n))
+    y = A @ _f64(x)
+    if out is not None:
+        out[:] = y
+        return out
+    return y
+
+
+class SparseCholesky:
+    """new SparseCholesky(pat, perm?, {sym, ordering, x, y, factor}) (sparse.mjs:1318-1372)."""
+
+    def __init__(self, pat, perm=None, sym: SymbolicAnalysis | None = None, ordering: str = "amd", x=None, y=None,
+                 z=None, factor=None, precision: int = FP64):
+        t0 = time.perf_counter()
+        self.factorKind = factor
+        if sym is not None:
+            checkSymbolic(sym, pat)
+            self.sym = sym
+        else:
+            self.sym = analyze(pat, {"perm": perm} if perm is not None else {"ordering": ordering, "x": x, "y": y,
+                                                                             "z": z})
+        self.n = int(pat.n)
+        self.perm = self.sym.perm
+        self.nnzL = self.sym.nnzL
+        self.num = None
+        self.ok = False
+        self.precision = precision
+        reused = sym is not None
+        self.timing = {"n": self.n, "nnzA": self.sym.nnzA, "nnzL": self.nnzL, "fill": self.sym.fill,
+                       "flops": self.sym.flops, "nsuper": self.sym.nsuper, "symbolicReused": reused,
+                       "ordering_ms": 0.0 if reused else self.sym.timing["ordering_ms"],
+                       "symbolic_ms": 0.0 if reused else (time.perf_counter() - t0) * 1e3 -
+                       self.sym.timing["ordering_ms"], "factor_ms": 0.0, "nFactor": 0, "solve_ms": 0.0, "nSolve": 0,
+                       "kernel": "cuda-sm100a"}
+
+    def factor(self, values) -> bool:
+        t0 = time.perf_counter()
+        nv = len(values)
+        if nv != _nnz_of(self.sym):
+            raise AmpError(AMP_BAD_LENGTH, f"factorNumeric: {nv} values for a pattern with {_nnz_of(self.sym)} entries")
+        if self.num is None:
+            self.num = NumericFactor(self.sym, CHOLESKY, self.precision)
+        self.ok = self.num.factor(values)
+        self.timing["factor_ms"] += (time.perf_counter() - t0) * 1e3
+        self.timing["nFactor"] += 1
+        return self.ok
+
+    def solve(self, b, out=None) -> np.ndarray:
+        t0 = time.perf_counter()
+        if not self.ok:
+            raise AmpError(AMP_NO_FACTOR, "SparseCholesky: solve without a successful factorization")
+        r = solveNumeric(self.num, b, out)
+        self.timing["solve_ms"] += (time.perf_counter() - t0) * 1e3
+        self.timing["nSolve"] += 1
+        return r
+
+    def solveMany(self, bs, outs=None) -> list:
+        t0 = time.perf_counter()
+        if not self.ok:
+            raise AmpError(AMP_NO_FACTOR, "SparseCholesky: solve without a successful factorization")
+        r = solveNumericMulti(self.num, bs, outs)
+        self.timing["solve_ms"] += (time.perf_counter() - t0) * 1e3
+        self.timing["nSolve"] += len(bs)
+        return r

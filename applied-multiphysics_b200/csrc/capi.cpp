@@ -1,0 +1,559 @@
+// C ABI of libampsolve.so (include/ampsolve.h): plan / factor handles, device memory, and the orchestration of the
+// kernels on one CUDA stream per factor.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ampsolve.h"
+#include "cuda/launch.hpp"
+#include "host/plan.hpp"
+#include "host/symbolic.hpp"
+
+namespace amp {
+void launch_matvec(int n, const int *rowptr, const int *colidx, const double *val, const double *x, double *y, int q,
+                   cudaStream_t st);
+void launch_residual(int n, const int *rowptr, const int *colidx, const double *val, const double *x, const double *b,
+                     double *r, double *norms, int q, cudaStream_t st);
+void launch_axpy(double *x, const double *dx, int64_t len, cudaStream_t st);
+}  // namespace amp
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+struct CudaError {
+  int code;
+};
+
+void ck(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) {
+    g_err = std::string(what) + ": " + cudaGetErrorString(e);
+    throw CudaError{e == cudaErrorMemoryAllocation ? AMP_OOM : AMP_CUDA_ERROR};
+  }
+}
+
+// Device buffer list owned by a handle.
+struct DevMem {
+  std::vector<void *> ptrs;
+  int64_t bytes = 0;
+  template <class T>
+  T *alloc(size_t count) {
+    void *p = nullptr;
+    size_t b = sizeof(T) * (count ? count : 1);
+    ck(cudaMalloc(&p, b), "cudaMalloc");
+    ptrs.push_back(p);
+    bytes += (int64_t)b;
+    return (T *)p;
+  }
+  template <class T>
+  T *upload(const std::vector<T> &v) {
+    T *p = alloc<T>(v.size());
+    if (!v.empty()) ck(cudaMemcpy(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice), "cudaMemcpy H2D");
+    return p;
+  }
+  void release() {
+    for (void *p : ptrs) cudaFree(p);
+    ptrs.clear();
+    bytes = 0;
+  }
+};
+
+}  // namespace
+
+struct amp_plan_s {
+  amp::Symbolic S;
+  amp::Plan P;
+  std::string key;
+  int device = 0;
+  DevMem mem;
+  amp::DevPlan dp{};
+  amp::AsmTask *dAsm = nullptr;
+  amp::PanelTask *dPanel = nullptr;
+  amp::TileTask *dTile = nullptr;
+  int *dRowptr = nullptr, *dColidx = nullptr;
+  std::vector<int> rowptr, colidx;  // host copy of the pattern (uploaded with the schedule)
+  bool uploaded = false;
+  ~amp_plan_s() { mem.release(); }
+};
+
+struct amp_factor_s {
+  amp_plan *plan = nullptr;
+  int kind = AMP_CHOLESKY, precision = AMP_FP64;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  DevMem mem;
+  double *dLx = nullptr, *dU = nullptr, *dD = nullptr, *dValues = nullptr;
+  unsigned long long *dStatus = nullptr;
+  bool ok = false, hasValues = false;
+  // solve workspace (grown on demand)
+  DevMem smem;
+  int qcap = 0;
+  double *dY = nullptr, *dV = nullptr, *dT = nullptr, *dB = nullptr, *dX = nullptr, *dR = nullptr, *dDX = nullptr,
+         *dNorms = nullptr;
+  ~amp_factor_s() {
+    smem.release();
+    mem.release();
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+void upload_plan(amp_plan *pl) {
+  const amp::Plan &P = pl->P;
+  DevMem &m = pl->mem;
+  amp::DevPlan &d = pl->dp;
+  d.n = P.n;
+  d.nsuper = P.nsuper;
+  d.maxFront = P.maxFront;
+  if (P.nsuper == 0) return;
+  d.snF = m.upload(P.snF);
+  d.snNc = m.upload(P.snNc);
+  d.snM = m.upload(P.snM);
+  d.snParent = m.upload(P.snParent);
+  d.snLxp = m.upload(P.snLxp);
+  d.snUoff = m.upload(P.snUoff);
+  d.snTOff = m.upload(P.snTOff);
+  d.chPtr = m.upload(P.chPtr);
+  d.chList = m.upload(P.chList);
+  d.asmColPtr = m.upload(P.asmColPtr);
+  d.asmDst = m.upload(P.asmDst);
+  d.asmSrc = m.upload(P.asmSrc);
+  d.eaPtr = m.upload(P.eaPtr);
+  d.eaMap = m.upload(P.eaMap);
+  d.lvlSn = m.upload(P.lvlSn);
+  d.perm = m.upload(P.perm);
+  d.Sp = m.upload(P.Sp);
+  d.Si = m.upload(P.Si);
+  pl->dAsm = m.upload(P.asmTasks);
+  pl->dPanel = m.upload(P.panelTasks);
+  pl->dTile = m.upload(P.tileTasks);
+}
+
+void ensure_solve_ws(amp_factor *f, int q) {
+  if (q <= f->qcap) return;
+  f->smem.release();
+  const amp::Plan &P = f->plan->P;
+  size_t n = (size_t)P.n;
+  f->dY = f->smem.alloc<double>(n * q);
+  f->dV = f->smem.alloc<double>((size_t)(P.nsuper ? P.Sp[P.nsuper] : 0) * q);
+  f->dT = f->smem.alloc<double>((size_t)P.solveBufDoubles * q);
+  f->dB = f->smem.alloc<double>(n * q);
+  f->dX = f->smem.alloc<double>(n * q);
+  f->dR = f->smem.alloc<double>(n * q);
+  f->dDX = f->smem.alloc<double>(n * q);
+  f->dNorms = f->smem.alloc<double>(2 * (size_t)q);
+  f->qcap = q;
+}
+
+// y (permuted order, q vectors) := A^-1 y in place
+void device_solve_permuted(amp_factor *f, int q) {
+  const amp::Plan &P = f->plan->P;
+  const amp::DevPlan &dp = f->plan->dp;
+  const int64_t Vs = P.nsuper ? P.Sp[P.nsuper] : 0, Ts = P.solveBufDoubles;
+  for (int L = 0; L < P.nlevels; L++)
+    amp::launch_forward(dp.lvlSn + P.lvlPtr[L], P.lvlPtr[L + 1] - P.lvlPtr[L], dp, f->dLx, f->dY, f->dV, f->dT, q, Vs,
+                        Ts, f->stream);
+  for (int L = P.nlevels - 1; L >= 0; L--)
+    amp::launch_backward(dp.lvlSn + P.lvlPtr[L], P.lvlPtr[L + 1] - P.lvlPtr[L], dp, f->dLx, f->dY, q, f->stream);
+}
+
+// x = A^-1 b for device vectors (original order)
+void device_solve(amp_factor *f, const double *dB, double *dX, int q) {
+  const amp::Plan &P = f->plan->P;
+  amp::launch_permute_in(dB, f->dY, f->plan->dp.perm, P.n, q, f->stream);
+  device_solve_permuted(f, q);
+  amp::launch_permute_out(f->dY, dX, f->plan->dp.perm, P.n, q, f->stream);
+}
+
+template <class F>
+int guarded(F &&fn) {
+  try {
+    g_err.clear();
+    return fn();
+  } catch (const CudaError &e) {
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    return fail(AMP_OOM, "host allocation failed");
+  } catch (const std::exception &e) {
+    return fail(AMP_INVALID, e.what());
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *amp_last_error(void) { return g_err.c_str(); }
+
+int amp_amd_order(int32_t n, const int32_t *rowptr, const int32_t *colidx, double dense_factor, int32_t *perm) {
+  return guarded([&] {
+    if (n < 0 || (n > 0 && (!rowptr || !colidx || !perm))) return fail(AMP_INVALID, "amdOrder: invalid arguments");
+    if (!amp::amd_order({n, rowptr, colidx}, dense_factor, perm))
+      return fail(AMP_INVALID, "amdOrder: internal error");
+    return (int)AMP_OK;
+  });
+}
+
+int amp_nd_order(int32_t n, const int32_t *rowptr, const int32_t *colidx, const double *x, const double *y,
+                 int32_t leaf, int32_t *perm) {
+  return guarded([&] {
+    if (n > 0 && (!x || !y)) return fail(AMP_NEED_COORDS, "analyze: ordering nd needs node coordinates x and y of length n");
+    amp::nd_order({n, rowptr, colidx}, x, y, leaf > 0 ? leaf : 48, perm);
+    return (int)AMP_OK;
+  });
+}
+
+int amp_nd3_order(int32_t n, const int32_t *rowptr, const int32_t *colidx, const double *x, const double *y,
+                  const double *z, int32_t leaf, int32_t *perm) {
+  return guarded([&] {
+    if (n > 0 && (!x || !y || !z)) return fail(AMP_NEED_COORDS, "nd3Order: needs DOF coordinates x, y and z of length n");
+    amp::nd3_order({n, rowptr, colidx}, x, y, z, leaf > 0 ? leaf : 2000, perm);
+    return (int)AMP_OK;
+  });
+}
+
+int amp_pattern_fingerprint(int32_t n, const int32_t *rowptr, const int32_t *colidx, char *buf, int32_t buflen) {
+  return guarded([&] {
+    std::string k = amp::pattern_key({n, rowptr, colidx});
+    if (!buf || buflen <= (int32_t)k.size()) return fail(AMP_INVALID, "fingerprint buffer too small");
+    std::memcpy(buf, k.c_str(), k.size() + 1);
+    return (int)AMP_OK;
+  });
+}
+
+int amp_analyze(int32_t n, const int32_t *rowptr, const int32_t *colidx, const amp_analyze_opts *opts,
+                amp_plan **out) {
+  return guarded([&] {
+    if (!out || n < 0 || !rowptr || (n > 0 && !colidx)) return fail(AMP_INVALID, "analyze: invalid arguments");
+    *out = nullptr;
+    amp_analyze_opts o{};
+    o.relax = 1;
+    if (opts) o = *opts;
+    amp::Pattern A{n, rowptr, colidx};
+    const int32_t *perm = nullptr;
+    int ordering = 0;
+    if (o.ordering == AMP_ORDER_GIVEN) {
+      if (!o.perm) return fail(AMP_BAD_LENGTH, "analyze: perm has length 0, pattern has " + std::to_string(n) + " rows");
+      perm = o.perm;
+    } else if (o.ordering == AMP_ORDER_ND) {
+      if (n > 0 && (!o.x || !o.y)) return fail(AMP_NEED_COORDS, "analyze: ordering nd needs node coordinates x and y of length n");
+      ordering = 1;
+    } else if (o.ordering == AMP_ORDER_ND3) {
+      if (n > 0 && (!o.x || !o.y || !o.z)) return fail(AMP_NEED_COORDS, "nd3Order: needs DOF coordinates x, y and z of length n");
+      ordering = 2;
+    } else if (o.ordering != AMP_ORDER_AMD)
+      return fail(AMP_INVALID, "analyze: unknown ordering");
+    auto *pl = new amp_plan_s();
+    pl->device = o.device;
+    try {
+      std::vector<int> permBuf;
+      if (ordering == 1 && o.leaf > 0 && o.leaf != 48) {
+        permBuf.resize(n);
+        amp::nd_order(A, o.x, o.y, o.leaf, permBuf.data());
+        perm = permBuf.data();
+      } else if (ordering == 2 && o.leaf > 0 && o.leaf != 2000) {
+        permBuf.resize(n);
+        amp::nd3_order(A, o.x, o.y, o.z, o.leaf, permBuf.data());
+        perm = permBuf.data();
+      }
+      amp::analyze(A, perm, perm ? 3 : ordering, o.x, o.y, o.z, o.relax != 0, pl->S);
+      amp::build_plan(pl->S, pl->P);
+      pl->key = amp::pattern_key(A);
+      pl->rowptr.assign(rowptr, rowptr + n + 1);
+      pl->colidx.assign(colidx, colidx + (n ? rowptr[n] : 0));
+    } catch (...) {
+      delete pl;
+      throw;
+    }
+    *out = pl;
+    return (int)AMP_OK;
+  });
+}
+
+int amp_plan_get_info(const amp_plan *pl, amp_plan_info *info) {
+  if (!pl || !info) return fail(AMP_INVALID, "null handle");
+  const amp::Symbolic &S = pl->S;
+  info->n = S.n;
+  info->nsuper = S.nsuper;
+  info->max_front = S.maxFront;
+  info->nlevels = pl->P.nlevels;
+  info->nnz_l = S.nnzL;
+  info->nnz_a = S.nnzA;
+  info->nnz_l_stored = S.nnzLStored;
+  info->pattern_nnz = S.patNnz;
+  info->fill = S.fill;
+  info->flops = S.flops;
+  info->ordering_ms = S.ordering_ms;
+  info->symbolic_ms = S.symbolic_ms;
+  info->device_bytes = 8 * (pl->P.nnzLStored + pl->P.arenaDoubles + pl->P.patNnz + S.n) + 4 * (int64_t)(
+      pl->P.asmDst.size() * 2 + pl->P.eaMap.size() + pl->P.Si.size() + pl->rowptr.size() + pl->colidx.size()) +
+      (int64_t)(sizeof(amp::TileTask) * pl->P.tileTasks.size() + sizeof(amp::PanelTask) * pl->P.panelTasks.size());
+  return AMP_OK;
+}
+
+int amp_plan_array(const amp_plan *pl, int field, void *dst, int64_t len, int64_t *out_len) {
+  if (!pl) return fail(AMP_INVALID, "null handle");
+  const amp::Symbolic &S = pl->S;
+  const std::vector<int> *v = nullptr;
+  switch (field) {
+    case AMP_F_PERM: v = &S.perm; break;
+    case AMP_F_PINV: v = &S.pinv; break;
+    case AMP_F_PARENT: v = &S.parent; break;
+    case AMP_F_COLCOUNT: v = &S.colCount; break;
+    case AMP_F_LOWERP: v = &S.lowerP; break;
+    case AMP_F_LOWERI: v = &S.lowerI; break;
+    case AMP_F_LOWERSRC: v = &S.lowerSrc; break;
+    case AMP_F_SUPERSTART: v = &S.superStart; break;
+    case AMP_F_COLSUPER: v = &S.colSuper; break;
+    case AMP_F_SUPERPARENT: v = &S.superParent; break;
+    case AMP_F_CHILDHEAD: v = &S.childHead; break;
+    case AMP_F_CHILDNEXT: v = &S.childNext; break;
+    case AMP_F_SP: v = &S.Sp; break;
+    case AMP_F_SI: v = &S.Si; break;
+    case AMP_F_LXP: {
+      if (out_len) *out_len = (int64_t)S.Lxp.size();
+      if (dst) std::memcpy(dst, S.Lxp.data(), sizeof(int64_t) * std::min<int64_t>(len, S.Lxp.size()));
+      return AMP_OK;
+    }
+    default: return fail(AMP_INVALID, "unknown field");
+  }
+  if (out_len) *out_len = (int64_t)v->size();
+  if (dst) std::memcpy(dst, v->data(), sizeof(int) * std::min<int64_t>(len, v->size()));
+  return AMP_OK;
+}
+
+int amp_plan_fingerprint(const amp_plan *pl, char *buf, int32_t buflen) {
+  if (!pl || !buf || buflen <= (int32_t)pl->key.size()) return fail(AMP_INVALID, "fingerprint buffer too small");
+  std::memcpy(buf, pl->key.c_str(), pl->key.size() + 1);
+  return AMP_OK;
+}
+
+int amp_plan_check_pattern(const amp_plan *pl, int32_t n, const int32_t *rowptr, const int32_t *colidx) {
+  if (!pl) return fail(AMP_INVALID, "null handle");
+  if (n != pl->S.n || amp::pattern_key({n, rowptr, colidx}) != pl->key)
+    return fail(AMP_PATTERN_MISMATCH, "symbolic analysis is for a different sparsity pattern");
+  return AMP_OK;
+}
+
+void amp_plan_destroy(amp_plan *pl) { delete pl; }
+
+int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **out) {
+  return guarded([&] {
+    if (!pl || !out) return fail(AMP_INVALID, "null handle");
+    *out = nullptr;
+    amp_factor_opts o{AMP_CHOLESKY, AMP_FP64};
+    if (opts) o = *opts;
+    if (o.kind != AMP_CHOLESKY) return fail(AMP_INVALID, "factor kind not available in this build");
+    if (o.precision != AMP_FP64) return fail(AMP_INVALID, "precision not available in this build");
+    ck(cudaSetDevice(pl->device), "cudaSetDevice");
+    if (!pl->uploaded) {  // the device schedule is uploaded once, by the first factor of the plan
+      upload_plan(pl);
+      pl->dRowptr = pl->mem.upload(pl->rowptr);
+      pl->dColidx = pl->mem.upload(pl->colidx);
+      pl->uploaded = true;
+    }
+    auto *f = new amp_factor_s();
+    f->plan = pl;
+    f->kind = o.kind;
+    f->precision = o.precision;
+    try {
+      ck(cudaStreamCreateWithFlags(&f->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+      ck(cudaEventCreate(&f->ev0), "cudaEventCreate");
+      ck(cudaEventCreate(&f->ev1), "cudaEventCreate");
+      const amp::Plan &P = pl->P;
+      f->dLx = f->mem.alloc<double>((size_t)P.nnzLStored);
+      f->dU = f->mem.alloc<double>((size_t)P.arenaDoubles);
+      f->dD = f->mem.alloc<double>((size_t)P.n);
+      f->dValues = f->mem.alloc<double>((size_t)P.patNnz);
+      f->dStatus = f->mem.alloc<unsigned long long>(1);
+    } catch (...) {
+      delete f;
+      throw;
+    }
+    *out = f;
+    return (int)AMP_OK;
+  });
+}
+
+int amp_factor_numeric(amp_factor *f, const double *values, int64_t nvalues, int values_on_device, double pivot_tol,
+                       amp_factor_result *res) {
+  return guarded([&] {
+    if (!f) return fail(AMP_INVALID, "null handle");
+    const amp::Plan &P = f->plan->P;
+    if (nvalues != P.patNnz)
+      return fail(AMP_BAD_LENGTH, "factorNumeric: " + std::to_string(nvalues) + " values for a pattern with " +
+                                      std::to_string(P.patNnz) + " entries");
+    (void)pivot_tol;
+    ck(cudaSetDevice(f->plan->device), "cudaSetDevice");
+    f->ok = false;
+    amp_factor_result r{};
+    r.fail_column = -1;
+    if (P.n == 0) {
+      f->ok = true;
+      r.ok = 1;
+      if (res) *res = r;
+      return (int)AMP_OK;
+    }
+    cudaStream_t st = f->stream;
+    if (nvalues > 0)
+      ck(cudaMemcpyAsync(f->dValues, values, sizeof(double) * nvalues,
+                         values_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st),
+         "copy values");
+    f->hasValues = true;
+    ck(cudaMemsetAsync(f->dStatus, 0xff, sizeof(unsigned long long), st), "memset status");
+    ck(cudaEventRecord(f->ev0, st), "event");
+    const amp::DevPlan &dp = f->plan->dp;
+    for (int L = 0; L < P.nlevels; L++) {
+      amp::launch_assemble(f->plan->dAsm + P.asmLvlPtr[L], P.asmLvlPtr[L + 1] - P.asmLvlPtr[L], dp, f->dValues,
+                           f->dLx, f->dU, f->dStatus, st);
+      for (int k = P.lvlStepPtr[L]; k < P.lvlStepPtr[L + 1]; k++) {
+        const amp::StepRange &sr = P.steps[k];
+        amp::launch_panel(f->plan->dPanel + sr.panel0, sr.panel1 - sr.panel0, dp, f->dLx, f->dStatus, st);
+        amp::launch_update(f->plan->dTile + sr.tile0, sr.tile1 - sr.tile0, dp, f->dLx, f->dU, f->dStatus, st);
+      }
+    }
+    ck(cudaGetLastError(), "kernel launch");
+    ck(cudaEventRecord(f->ev1, st), "event");
+    unsigned long long status = 0;
+    ck(cudaMemcpyAsync(&status, f->dStatus, sizeof status, cudaMemcpyDeviceToHost, st), "copy status");
+    ck(cudaStreamSynchronize(st), "factor");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, f->ev0, f->ev1);
+    r.ms = ms;
+    if (status == amp::kStatusOk) {
+      r.ok = 1;
+      f->ok = true;
+    } else {
+      r.ok = 0;
+      r.fail_column = (int32_t)(status >> 32);
+    }
+    if (res) *res = r;
+    return (int)AMP_OK;
+  });
+}
+
+int amp_solve(amp_factor *f, const double *b, int32_t nrhs, double *x, int on_device) {
+  return guarded([&] {
+    if (!f) return fail(AMP_INVALID, "null handle");
+    if (!f->ok) return fail(AMP_NO_FACTOR, "solveNumeric: no successful numeric factorization");
+    const amp::Plan &P = f->plan->P;
+    if (nrhs <= 0 || P.n == 0) return (int)AMP_OK;
+    ck(cudaSetDevice(f->plan->device), "cudaSetDevice");
+    ensure_solve_ws(f, nrhs);
+    size_t bytes = sizeof(double) * (size_t)P.n * nrhs;
+    const double *dB = b;
+    double *dX = x;
+    if (!on_device) {
+      ck(cudaMemcpyAsync(f->dB, b, bytes, cudaMemcpyHostToDevice, f->stream), "copy b");
+      dB = f->dB;
+      dX = f->dX;
+    }
+    device_solve(f, dB, dX, nrhs);
+    ck(cudaGetLastError(), "kernel launch");
+    if (!on_device) ck(cudaMemcpyAsync(x, dX, bytes, cudaMemcpyDeviceToHost, f->stream), "copy x");
+    ck(cudaStreamSynchronize(f->stream), "solve");
+    return (int)AMP_OK;
+  });
+}
+
+int amp_solve_refined(amp_factor *f, const double *b, int32_t nrhs, double *x, int on_device,
+                      const amp_refine_opts *opts, amp_refine_stats *stats) {
+  return guarded([&] {
+    if (!f) return fail(AMP_INVALID, "null handle");
+    if (!f->ok) return fail(AMP_NO_FACTOR, "solveNumeric: no successful numeric factorization");
+    const amp::Plan &P = f->plan->P;
+    amp_refine_opts o{3, 1e-14};
+    if (opts) o = *opts;
+    amp_refine_stats stt{0.0, 0};
+    if (nrhs <= 0 || P.n == 0) {
+      if (stats) *stats = stt;
+      return (int)AMP_OK;
+    }
+    ck(cudaSetDevice(f->plan->device), "cudaSetDevice");
+    ensure_solve_ws(f, nrhs);
+    const int n = P.n;
+    size_t len = (size_t)n * nrhs, bytes = sizeof(double) * len;
+    cudaStream_t st = f->stream;
+    const double *dB = b;
+    double *dX = x;
+    if (!on_device) {
+      ck(cudaMemcpyAsync(f->dB, b, bytes, cudaMemcpyHostToDevice, st), "copy b");
+      dB = f->dB;
+      dX = f->dX;
+    }
+    device_solve(f, dB, dX, nrhs);
+    std::vector<double> norms(2 * (size_t)nrhs);
+    std::vector<char> active(nrhs, 1);
+    double worst = 0;
+    int steps = 0;
+    for (;; steps++) {
+      ck(cudaMemsetAsync(f->dNorms, 0, sizeof(double) * 2 * nrhs, st), "memset");
+      amp::launch_residual(n, f->plan->dRowptr, f->plan->dColidx, f->dValues, dX, dB, f->dR, f->dNorms, nrhs, st);
+      ck(cudaMemcpyAsync(norms.data(), f->dNorms, sizeof(double) * 2 * nrhs, cudaMemcpyDeviceToHost, st), "norms");
+      ck(cudaStreamSynchronize(st), "residual");
+      worst = 0;
+      bool any = false;
+      for (int k = 0; k < nrhs; k++) {
+        double bn = std::sqrt(norms[2 * k + 1]);
+        if (bn == 0 || std::isnan(bn)) bn = 1;
+        double rel = std::sqrt(norms[2 * k]) / bn;
+        worst = std::max(worst, rel);
+        if (!(rel < o.tol)) any = true;
+      }
+      if (!any || steps >= o.max_steps) break;
+      device_solve(f, f->dR, f->dDX, nrhs);
+      amp::launch_axpy(dX, f->dDX, (int64_t)len, st);
+    }
+    ck(cudaGetLastError(), "kernel launch");
+    if (!on_device) ck(cudaMemcpyAsync(x, dX, bytes, cudaMemcpyDeviceToHost, st), "copy x");
+    ck(cudaStreamSynchronize(st), "refine");
+    stt.rel_residual = worst;
+    stt.steps = steps;
+    if (stats) *stats = stt;
+    return (int)AMP_OK;
+  });
+}
+
+int amp_factor_download(const amp_factor *f, double *Lx, double *D) {
+  return guarded([&] {
+    if (!f) return fail(AMP_INVALID, "null handle");
+    const amp::Plan &P = f->plan->P;
+    ck(cudaSetDevice(f->plan->device), "cudaSetDevice");
+    if (Lx && P.nnzLStored) ck(cudaMemcpy(Lx, f->dLx, sizeof(double) * P.nnzLStored, cudaMemcpyDeviceToHost), "copy Lx");
+    if (D && P.n) ck(cudaMemcpy(D, f->dD, sizeof(double) * P.n, cudaMemcpyDeviceToHost), "copy D");
+    return (int)AMP_OK;
+  });
+}
+
+void amp_factor_destroy(amp_factor *f) { delete f; }
+
+int amp_matvec(amp_factor *f, const double *x, int32_t nrhs, double *y) {
+  return guarded([&] {
+    if (!f) return fail(AMP_INVALID, "null handle");
+    if (!f->hasValues) return fail(AMP_NO_FACTOR, "matVec: no values on the device (call amp_factor_numeric first)");
+    const amp::Plan &P = f->plan->P;
+    if (nrhs <= 0 || P.n == 0) return (int)AMP_OK;
+    ck(cudaSetDevice(f->plan->device), "cudaSetDevice");
+    ensure_solve_ws(f, nrhs);
+    size_t bytes = sizeof(double) * (size_t)P.n * nrhs;
+    ck(cudaMemcpyAsync(f->dB, x, bytes, cudaMemcpyHostToDevice, f->stream), "copy x");
+    amp::launch_matvec(P.n, f->plan->dRowptr, f->plan->dColidx, f->dValues, f->dB, f->dX, nrhs, f->stream);
+    ck(cudaMemcpyAsync(y, f->dX, bytes, cudaMemcpyDeviceToHost, f->stream), "copy y");
+    ck(cudaStreamSynchronize(f->stream), "matvec");
+    return (int)AMP_OK;
+  });
+}
+
+}  // extern "C"

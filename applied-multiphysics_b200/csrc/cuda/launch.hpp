@@ -1,0 +1,24 @@
+// Host-callable launchers of the device kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../host/plan.hpp"
+#include "devplan.cuh"
+
+namespace amp {
+
+void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, const double *values, double *Lx,
+                     double *U, const unsigned long long *status, cudaStream_t st);
+void launch_panel(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, unsigned long long *status,
+                  cudaStream_t st);
+void launch_update(const TileTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, double *U,
+                   const unsigned long long *status, cudaStream_t st);
+void launch_permute_in(const double *b, double *y, const int *perm, int n, int q, cudaStream_t st);
+void launch_permute_out(const double *y, double *x, const int *perm, int n, int q, cudaStream_t st);
+void launch_forward(const int *sns, int count, const DevPlan &P, const double *Lx, double *y, double *V, double *T,
+                    int q, int64_t Vstride, int64_t Tstride, cudaStream_t st);
+void launch_backward(const int *sns, int count, const DevPlan &P, const double *Lx, double *y, int q, cudaStream_t st);
+
+}  // namespace amp

@@ -1,0 +1,205 @@
+// Device schedule builder (see plan.hpp).
+#include "plan.hpp"
+
+#include <algorithm>
+#include <map>
+#include <stdexcept>
+
+namespace amp {
+
+namespace {
+
+// Offline first-fit allocator over one arena (offsets in doubles, 256-byte aligned blocks).
+class ArenaPlanner {
+ public:
+  int64_t alloc(int64_t size) {
+    size = (size + 31) & ~int64_t(31);
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second >= size) {
+        int64_t off = it->first, rest = it->second - size;
+        free_.erase(it);
+        if (rest > 0) free_[off + size] = rest;
+        used_[off] = size;
+        return off;
+      }
+    }
+    int64_t off = top_;
+    top_ += size;
+    used_[off] = size;
+    return off;
+  }
+  void release(int64_t off) {
+    auto u = used_.find(off);
+    if (u == used_.end()) throw std::logic_error("arena planner: double free");
+    int64_t size = u->second;
+    used_.erase(u);
+    auto it = free_.emplace(off, size).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+        it = pv;
+      }
+    }
+    if (it->first + it->second == top_) {  // shrink the top
+      top_ = it->first;
+      free_.erase(it);
+    }
+    peak_ = std::max(peak_, top_);
+  }
+  int64_t peak() const { return std::max(peak_, top_); }
+  void note() { peak_ = std::max(peak_, top_); }
+
+ private:
+  std::map<int64_t, int64_t> free_, used_;
+  int64_t top_ = 0, peak_ = 0;
+};
+
+}  // namespace
+
+void build_plan(const Symbolic &S, Plan &P) {
+  P = Plan();
+  const int n = S.n, ns = S.nsuper;
+  P.n = n;
+  P.nsuper = ns;
+  P.maxFront = S.maxFront;
+  P.nnzLStored = S.nnzLStored;
+  P.nnzA = S.nnzA;
+  P.patNnz = S.patNnz;
+  P.flops = S.flops;
+  P.perm = S.perm;
+  P.Sp = S.Sp;
+  P.Si = S.Si;
+  if (ns == 0) {
+    P.lvlPtr.assign(1, 0);
+    P.asmLvlPtr.assign(1, 0);
+    P.lvlStepPtr.assign(1, 0);
+    P.asmPtr.assign(1, 0);
+    return;
+  }
+  P.snF.resize(ns);
+  P.snNc.resize(ns);
+  P.snM.resize(ns);
+  P.snLevel.assign(ns, 0);
+  P.snParent = S.superParent;
+  P.snLxp.assign(S.Lxp.begin(), S.Lxp.begin() + ns);
+  P.snUoff.assign(ns, -1);
+  for (int s = 0; s < ns; s++) {
+    P.snF[s] = S.superStart[s];
+    P.snNc[s] = S.superStart[s + 1] - S.superStart[s];
+    P.snM[s] = S.Sp[s + 1] - S.Sp[s];
+  }
+  // height levels: children always have a smaller index (postorder)
+  for (int s = 0; s < ns; s++)
+    if (S.superParent[s] >= 0) P.snLevel[S.superParent[s]] = std::max(P.snLevel[S.superParent[s]], P.snLevel[s] + 1);
+  P.nlevels = 1 + *std::max_element(P.snLevel.begin(), P.snLevel.end());
+  P.lvlPtr.assign(P.nlevels + 1, 0);
+  for (int s = 0; s < ns; s++) P.lvlPtr[P.snLevel[s] + 1]++;
+  for (int L = 0; L < P.nlevels; L++) P.lvlPtr[L + 1] += P.lvlPtr[L];
+  P.lvlSn.resize(ns);
+  {
+    std::vector<int> fill(P.lvlPtr.begin(), P.lvlPtr.end() - 1);
+    for (int s = 0; s < ns; s++) P.lvlSn[fill[P.snLevel[s]]++] = s;
+  }
+  // children in the reference's order (childHead: decreasing index)
+  P.chPtr.assign(ns + 1, 0);
+  for (int s = 0; s < ns; s++)
+    for (int c = S.childHead[s]; c != -1; c = S.childNext[c]) P.chPtr[s + 1]++;
+  for (int s = 0; s < ns; s++) P.chPtr[s + 1] += P.chPtr[s];
+  P.chList.resize(P.chPtr[ns]);
+  for (int s = 0; s < ns; s++) {
+    int q = P.chPtr[s];
+    for (int c = S.childHead[s]; c != -1; c = S.childNext[c]) P.chList[q++] = c;
+  }
+  // assembly and extend-add maps
+  std::vector<int> rel(n, -1);
+  P.asmPtr.assign(ns + 1, 0);
+  P.asmDst.resize(S.nnzA);
+  P.asmSrc.resize(S.nnzA);
+  P.asmColPtr = S.lowerP;
+  P.eaPtr.assign(ns + 1, 0);
+  for (int s = 0; s < ns; s++) P.eaPtr[s + 1] = P.eaPtr[s] + (P.snParent[s] >= 0 ? P.snM[s] - P.snNc[s] : 0);
+  P.eaMap.resize(P.eaPtr[ns]);
+  for (int s = 0; s < ns; s++) {
+    const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s], r0 = S.Sp[s];
+    for (int r = 0; r < m; r++) rel[S.Si[r0 + r]] = r;
+    P.asmPtr[s] = S.lowerP[f];
+    for (int c = 0; c < nc; c++)
+      for (int p = S.lowerP[f + c]; p < S.lowerP[f + c + 1]; p++) {
+        P.asmDst[p] = rel[S.lowerI[p]] + c * m;
+        P.asmSrc[p] = S.lowerSrc[p];
+      }
+    for (int q = P.chPtr[s]; q < P.chPtr[s + 1]; q++) {
+      int c = P.chList[q];
+      int cr0 = S.Sp[c] + P.snNc[c], mu = P.snM[c] - P.snNc[c];
+      for (int a = 0; a < mu; a++) P.eaMap[P.eaPtr[c] + a] = rel[S.Si[cr0 + a]];
+    }
+  }
+  P.asmPtr[ns] = S.lowerP[n];
+  // U arena by level lifetimes
+  {
+    ArenaPlanner ar;
+    for (int L = 0; L < P.nlevels; L++) {
+      for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
+        int s = P.lvlSn[q];
+        int64_t mu = P.snM[s] - P.snNc[s];
+        if (mu > 0) P.snUoff[s] = ar.alloc(mu * mu);
+      }
+      ar.note();
+      for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
+        int s = P.lvlSn[q];
+        for (int k = P.chPtr[s]; k < P.chPtr[s + 1]; k++) {
+          int c = P.chList[k];
+          if (P.snUoff[c] >= 0) ar.release(P.snUoff[c]);
+        }
+      }
+    }
+    P.arenaDoubles = ar.peak();
+  }
+  // task lists per level
+  P.asmLvlPtr.assign(P.nlevels + 1, 0);
+  P.lvlStepPtr.assign(P.nlevels + 1, 0);
+  for (int L = 0; L < P.nlevels; L++) {
+    int maxSteps = 0;
+    for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
+      int s = P.lvlSn[q];
+      for (int j0 = 0; j0 < P.snM[s]; j0 += kAsmCols) P.asmTasks.push_back({s, j0});
+      maxSteps = std::max(maxSteps, (P.snNc[s] + kPanel - 1) / kPanel);
+    }
+    P.asmLvlPtr[L + 1] = (int64_t)P.asmTasks.size();
+    for (int k = 0; k < maxSteps; k++) {
+      StepRange sr;
+      sr.panel0 = (int64_t)P.panelTasks.size();
+      sr.tile0 = (int64_t)P.tileTasks.size();
+      for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
+        int s = P.lvlSn[q];
+        const int nc = P.snNc[s], m = P.snM[s], c0 = k * kPanel;
+        if (c0 >= nc) continue;
+        const int c1 = std::min(c0 + kPanel, nc);
+        if (c1 >= m)
+          P.panelTasks.push_back({s, c0, m, m});
+        else
+          for (int r0 = c1; r0 < m; r0 += kTrsmRows) P.panelTasks.push_back({s, c0, r0, std::min(r0 + kTrsmRows, m)});
+        const int T = (m - c1 + kTile - 1) / kTile;
+        for (int I = 0; I < T; I++)
+          for (int J = 0; J <= I; J++) P.tileTasks.push_back({s, c0, c1 + kTile * I, c1 + kTile * J});
+      }
+      sr.panel1 = (int64_t)P.panelTasks.size();
+      sr.tile1 = (int64_t)P.tileTasks.size();
+      P.steps.push_back(sr);
+    }
+    P.lvlStepPtr[L + 1] = (int)P.steps.size();
+  }
+  // forward-solve update vectors
+  P.snTOff.assign(ns + 1, 0);
+  for (int s = 0; s < ns; s++) P.snTOff[s + 1] = P.snTOff[s] + (P.snM[s] - P.snNc[s]);
+  P.solveBufDoubles = P.snTOff[ns];
+}
+
+}  // namespace amp

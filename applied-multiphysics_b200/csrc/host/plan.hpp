@@ -1,0 +1,72 @@
+// Device schedule of one symbolic structure: everything the numeric factor and the solves need on the GPU, computed
+// once per pattern on the host (the analogue of the reference's reusable `sym`, sparse.mjs:666-902).
+//
+// Layout in HBM:
+//   Lx       the factor, exactly the reference's layout: supernode s is an m x nc column-major block at Lxp[s]
+//            (rows Si[Sp[s] ..], ld = m). The first nc columns of every frontal matrix live here in place, so no copy
+//            of the factor out of the front is ever made.
+//   U arena  the trailing mu x mu block (mu = m - nc, column-major, ld = mu, lower part used) of every front: the
+//            update (contribution) matrix. Offsets are assigned offline by level lifetimes (allocated at the
+//            supernode's level, released after its parent's level has assembled it).
+// Front entry (i, j), i >= j, of supernode s is Lx[Lxp[s] + j m + i] for j < nc, else U[Uoff[s] + (j-nc) mu + (i-nc)].
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "symbolic.hpp"
+
+namespace amp {
+
+constexpr int kPanel = 64;     // pivot block width of the dense partial factorization
+constexpr int kTile = 64;      // trailing-update tile edge
+constexpr int kAsmCols = 32;   // front columns per assembly task
+constexpr int kTrsmRows = 256; // panel rows per TRSM task
+constexpr int kSmallFront = 0; // fronts with m <= kSmallFront use the one-CTA-per-front kernel (0 = off)
+
+struct PanelTask {  // POTRF of the pivot block [c0, c0 + w) of supernode s and TRSM of rows [r0, r1)
+  int s, c0, r0, r1;
+};
+struct TileTask {  // trailing update tile of supernode s after pivot block c0: rows [i0, i0+64), cols [j0, j0+64)
+  int s, c0, i0, j0;
+};
+struct AsmTask {  // zero + assemble + extend-add front columns [j0, j0 + 32) of supernode s
+  int s, j0;
+};
+
+struct StepRange {
+  int64_t panel0, panel1, tile0, tile1;
+};
+
+struct Plan {
+  int n = 0, nsuper = 0, nlevels = 0, maxFront = 0;
+  int64_t nnzLStored = 0, arenaDoubles = 0, nnzA = 0, patNnz = 0;
+  // per supernode
+  std::vector<int> snF, snNc, snM, snLevel, snParent;
+  std::vector<int64_t> snLxp, snUoff;
+  std::vector<int> chPtr, chList;  // children of s in the reference's extend-add order (childHead chain)
+  // assembly of A: entries of supernode s are [asmPtr[s], asmPtr[s+1]) (= lowerP over its columns)
+  std::vector<int64_t> asmPtr;
+  std::vector<int> asmDst, asmSrc;  // offset in the L panel of s; CSR slot of the value
+  std::vector<int> asmColPtr;       // lowerP relative: column j of s has entries [asmColPtr[f+j], asmColPtr[f+j+1])
+  // extend-add: child c's rows below its block map to parent front positions eaMap[eaPtr[c] + a]
+  std::vector<int64_t> eaPtr;
+  std::vector<int> eaMap;
+  // supernodes by level
+  std::vector<int> lvlPtr, lvlSn;
+  // task lists
+  std::vector<AsmTask> asmTasks;
+  std::vector<int64_t> asmLvlPtr;  // per level
+  std::vector<PanelTask> panelTasks;
+  std::vector<TileTask> tileTasks;
+  std::vector<int> lvlStepPtr;  // per level: steps [lvlStepPtr[L], lvlStepPtr[L+1])
+  std::vector<StepRange> steps;
+  // solve: rows below of each supernode (Si[Sp[s] + nc ..]) and the perm
+  std::vector<int> perm, Sp, Si;
+  int64_t solveBufDoubles = 0;      // sum of mu (per RHS) for the forward update vectors
+  std::vector<int64_t> snTOff;      // offset of supernode s's forward update vector (per RHS)
+  double flops = 0;
+};
+
+void build_plan(const Symbolic &S, Plan &P);
+
+}  // namespace amp

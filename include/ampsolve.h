@@ -1,0 +1,155 @@
+/*
+ * ampsolve.h -- C ABI of the B200-native supernodal sparse direct solver (libampsolve.so).
+ *
+ * Drop-in boundary for the analyze / factor / solve path of jwt625/applied-multiphysics packages/core
+ * (src/la/sparse.mjs, src/la/ldlt.mjs, src/la/order3d.mjs; typed surface src/la/sparse.d.mts and src/la/types.d.mts).
+ * Plain pointers and sizes only. All host pointers are borrowed for the duration of the call.
+ *
+ * Patterns are CSR in full symmetric storage (both triangles, diagonal present, rows sorted ascending), as the
+ * reference's CsrPattern (types.d.mts:6). Values are FP64 aligned with the CSR slots. Permutations are new -> old.
+ * Right-hand sides and solutions: q vectors stored one after another (b[k * n + i]), original ordering.
+ *
+ * Errors: every function returns an amp_status. Misuse that the reference throws on returns a nonzero status whose
+ * amp_last_error() message is the reference's message; numerical failure of a factorization is not an error: it
+ * returns AMP_OK with result.ok = 0 (the reference's ok = false).
+ */
+#ifndef AMPSOLVE_H
+#define AMPSOLVE_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define AMP_API __attribute__((visibility("default")))
+#else
+#define AMP_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  AMP_OK = 0,
+  AMP_NOT_SPD = 1,          /* Cholesky pivot not > 0 (reported through result.ok = 0 by amp_factor_numeric) */
+  AMP_NONFINITE_PIVOT = 2,  /* LDL^T pivot not finite (reported through result.ok = 0) */
+  AMP_PATTERN_MISMATCH = 3, /* 'symbolic analysis is for a different sparsity pattern' (sparse.mjs:929) */
+  AMP_BAD_LENGTH = 4,       /* 'factorNumeric: N values for a pattern with M entries' (sparse.mjs:945), perm length */
+  AMP_NO_FACTOR = 5,        /* 'solveNumeric: no successful numeric factorization' (sparse.mjs:1262) */
+  AMP_NEED_COORDS = 6,      /* 'analyze: ordering nd needs node coordinates x and y of length n' (sparse.mjs:678) */
+  AMP_DEVICE_TIMEOUT = 7,   /* a bounded device wait gave up */
+  AMP_CUDA_ERROR = 8,
+  AMP_OOM = 9,
+  AMP_INVALID = 10          /* invalid argument (null handle, bad option) */
+} amp_status;
+
+typedef enum { AMP_ORDER_AMD = 0, AMP_ORDER_ND = 1, AMP_ORDER_ND3 = 2, AMP_ORDER_GIVEN = 3 } amp_ordering;
+typedef enum { AMP_CHOLESKY = 0, AMP_LDLT = 1 } amp_factor_kind;
+typedef enum { AMP_FP64 = 0, AMP_MIXED = 1 } amp_precision;
+
+typedef struct amp_plan_s amp_plan;     /* symbolic analysis + device schedule of one pattern (reference: sym) */
+typedef struct amp_factor_s amp_factor; /* numeric factor on the device (reference: NumericFactor / SupernodalLDLT) */
+
+/* Options of amp_analyze; replaces analyze(pat, {perm, ordering, x, y, relax}) (sparse.mjs:666, sparse.d.mts:28) and
+ * nd3Order(pat, x, y, z, {leaf}) followed by analyze(pat, {perm}) (order3d.mjs:27). Zero-initialise, then set. */
+typedef struct {
+  int ordering;          /* amp_ordering; AMP_ORDER_AMD by default */
+  int relax;             /* relaxed supernode amalgamation; set 1 for the reference default (relax ?? true) */
+  const int32_t *perm;   /* new -> old, length n, for AMP_ORDER_GIVEN */
+  const double *x, *y, *z;
+  int leaf;              /* ND leaf size; 0 = the reference default (48 for 2D, 2000 for 3D) */
+  int device;            /* CUDA device ordinal */
+} amp_analyze_opts;
+
+/* Scalars of a symbolic analysis (SymbolicAnalysis fields, types.d.mts:13-20). */
+typedef struct {
+  int32_t n, nsuper, max_front, nlevels;
+  int64_t nnz_l, nnz_a, nnz_l_stored, pattern_nnz;
+  double fill, flops, ordering_ms, symbolic_ms;
+  int64_t device_bytes; /* device memory of one factor of this plan (L, update arena, schedule) */
+} amp_plan_info;
+
+/* Array fields of a symbolic analysis for amp_plan_array (int32 unless noted). */
+typedef enum {
+  AMP_F_PERM = 0, AMP_F_PINV, AMP_F_PARENT, AMP_F_COLCOUNT, AMP_F_LOWERP, AMP_F_LOWERI, AMP_F_LOWERSRC,
+  AMP_F_SUPERSTART, AMP_F_COLSUPER, AMP_F_SUPERPARENT, AMP_F_CHILDHEAD, AMP_F_CHILDNEXT, AMP_F_SP, AMP_F_SI,
+  AMP_F_LXP /* int64 */
+} amp_field;
+
+typedef struct {
+  int kind;         /* amp_factor_kind */
+  int precision;    /* amp_precision */
+} amp_factor_opts;
+
+/* Result of a numeric factorization (sparse.mjs factorNumeric ok; ldlt.mjs LdltFactorResult, types.d.mts:26). */
+typedef struct {
+  int32_t ok;
+  int32_t n_neg, n_perturbed;
+  int32_t fail_column;  /* first failing column (permuted order) or -1 */
+  double ms;            /* device time of the factorization */
+} amp_factor_result;
+
+typedef struct {
+  int max_steps;        /* refinement steps (reference default 3) */
+  double tol;           /* stop when ||b - A x|| / ||b|| < tol (reference default 1e-14) */
+} amp_refine_opts;
+
+typedef struct {
+  double rel_residual;  /* max over the right-hand sides */
+  int32_t steps;        /* max over the right-hand sides */
+} amp_refine_stats;
+
+/* ---- orderings (host) ---- */
+/* amdOrder(pat, {denseFactor}) (sparse.mjs:297-592). perm: n entries, new -> old. */
+AMP_API int amp_amd_order(int32_t n, const int32_t *rowptr, const int32_t *colidx, double dense_factor, int32_t *perm);
+/* ndOrder(pat, x, y, leaf) (sparse.mjs:231-283). */
+AMP_API int amp_nd_order(int32_t n, const int32_t *rowptr, const int32_t *colidx, const double *x, const double *y,
+                 int32_t leaf, int32_t *perm);
+/* nd3Order(pat, x, y, z, {leaf}) (order3d.mjs:27-77). */
+AMP_API int amp_nd3_order(int32_t n, const int32_t *rowptr, const int32_t *colidx, const double *x, const double *y,
+                  const double *z, int32_t leaf, int32_t *perm);
+/* patternFingerprint(pat) (sparse.mjs:908-925): writes "n:nnz:hash" (NUL-terminated) into buf. */
+AMP_API int amp_pattern_fingerprint(int32_t n, const int32_t *rowptr, const int32_t *colidx, char *buf, int32_t buflen);
+
+/* ---- symbolic analysis ---- */
+/* analyze(pat, opts) (sparse.mjs:666-902): host symbolic phase, then the device schedule is uploaded. */
+AMP_API int amp_analyze(int32_t n, const int32_t *rowptr, const int32_t *colidx, const amp_analyze_opts *opts,
+                amp_plan **out);
+AMP_API int amp_plan_get_info(const amp_plan *plan, amp_plan_info *info);
+/* Copies one SymbolicAnalysis array (amp_field) into dst (capacity len elements); *out_len = its length. */
+AMP_API int amp_plan_array(const amp_plan *plan, int field, void *dst, int64_t len, int64_t *out_len);
+/* sym.patternKey */
+AMP_API int amp_plan_fingerprint(const amp_plan *plan, char *buf, int32_t buflen);
+/* checkSymbolic(sym, pat) (sparse.mjs:928-930): AMP_PATTERN_MISMATCH when pat is not the analysed pattern. */
+AMP_API int amp_plan_check_pattern(const amp_plan *plan, int32_t n, const int32_t *rowptr, const int32_t *colidx);
+AMP_API void amp_plan_destroy(amp_plan *plan);
+
+/* ---- numeric factorization ---- */
+/* Allocates the device factor of a plan: new SparseCholesky(pat, null, {sym}) storage (sparse.mjs:1318) or
+ * new SupernodalLDLT(sym) (ldlt.mjs:432-448). */
+AMP_API int amp_factor_create(amp_plan *plan, const amp_factor_opts *opts, amp_factor **out);
+/* factorNumeric(sym, values) (sparse.mjs:941) / SupernodalLDLT.factor(values, {pivotTol}) (ldlt.mjs:450).
+ * values: nvalues FP64 in CSR slot order, host memory (values_on_device = 0) or device memory (1). */
+AMP_API int amp_factor_numeric(amp_factor *f, const double *values, int64_t nvalues, int values_on_device, double pivot_tol,
+                       amp_factor_result *result);
+/* solveNumeric / solveNumericMulti (sparse.mjs:1261-1310), SupernodalLDLT.solve / solveMany (ldlt.mjs:565-643).
+ * b, x: nrhs vectors of length n one after another; host (on_device = 0) or device (1) memory. */
+AMP_API int amp_solve(amp_factor *f, const double *b, int32_t nrhs, double *x, int on_device);
+/* solveRefined(pat, values, b, {maxSteps, tol}) (ldlt.mjs:253-275): FP64 iterative refinement against the values
+ * of the last amp_factor_numeric call (the unperturbed matrix). */
+AMP_API int amp_solve_refined(amp_factor *f, const double *b, int32_t nrhs, double *x, int on_device,
+                      const amp_refine_opts *opts, amp_refine_stats *stats);
+/* num.Lx (the m x nc column-major blocks at Lxp) and D (LDL^T) copied to host; either pointer may be null. */
+AMP_API int amp_factor_download(const amp_factor *f, double *Lx, double *D);
+AMP_API void amp_factor_destroy(amp_factor *f);
+
+/* matVec(pat, val, x) (sparse.mjs:219-228) on the device: y = A x for nrhs vectors (host pointers). */
+AMP_API int amp_matvec(amp_factor *f, const double *x, int32_t nrhs, double *y);
+
+/* Message of the last failing call on this thread ("" when none). */
+AMP_API const char *amp_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AMPSOLVE_H */
