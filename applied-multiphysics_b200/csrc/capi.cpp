@@ -93,6 +93,7 @@ struct amp_factor_s {
   DevMem mem;
   double *dLx = nullptr, *dU = nullptr, *dD = nullptr, *dValues = nullptr;
   unsigned long long *dStatus = nullptr;
+  int *dReaders = nullptr;  // per pivot block: row chunks that have read it (reset at every factorization)
   bool ok = false, hasValues = false;
   // solve workspace (grown on demand)
   DevMem smem;
@@ -378,6 +379,7 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
       f->dD = f->mem.alloc<double>((size_t)P.n);
       f->dValues = f->mem.alloc<double>((size_t)P.patNnz);
       f->dStatus = f->mem.alloc<unsigned long long>(1);
+      f->dReaders = f->mem.alloc<int>((size_t)P.panelGroups);
     } catch (...) {
       delete f;
       throw;
@@ -413,6 +415,7 @@ int amp_factor_numeric(amp_factor *f, const double *values, int64_t nvalues, int
          "copy values");
     f->hasValues = true;
     ck(cudaMemsetAsync(f->dStatus, 0xff, sizeof(unsigned long long), st), "memset status");
+    if (P.panelGroups) ck(cudaMemsetAsync(f->dReaders, 0, sizeof(int) * P.panelGroups, st), "memset readers");
     ck(cudaEventRecord(f->ev0, st), "event");
     const amp::DevPlan &dp = f->plan->dp;
     for (int L = 0; L < P.nlevels; L++) {
@@ -420,7 +423,7 @@ int amp_factor_numeric(amp_factor *f, const double *values, int64_t nvalues, int
                            f->dLx, f->dU, f->dStatus, st);
       for (int k = P.lvlStepPtr[L]; k < P.lvlStepPtr[L + 1]; k++) {
         const amp::StepRange &sr = P.steps[k];
-        amp::launch_panel(f->plan->dPanel + sr.panel0, sr.panel1 - sr.panel0, dp, f->dLx, f->dStatus, st);
+        amp::launch_panel(f->plan->dPanel + sr.panel0, sr.panel1 - sr.panel0, dp, f->dLx, f->dReaders, f->dStatus, st);
         amp::launch_update(f->plan->dTile + sr.tile0, sr.tile1 - sr.tile0, dp, f->dLx, f->dU, f->dStatus, st);
       }
     }

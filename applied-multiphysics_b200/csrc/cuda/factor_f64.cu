@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(256) k_assemble(const AsmTask *__restrict__ ta
 // Panel: POTRF of the pivot block + TRSM of a chunk of rows below it
 // ---------------------------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_panel(const PanelTask *__restrict__ tasks, DevPlan P, double *__restrict__ Lx,
-                                               unsigned long long *status) {
+                                               int *__restrict__ readers, unsigned long long *status) {
   if (failed(status)) return;
   const PanelTask t = tasks[blockIdx.x];
   const int s = t.s, c0 = t.c0;
@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(256) k_panel(const PanelTask *__restrict__ tas
   double *Lp = Lx + P.snLxp[s];
   __shared__ double D[kPanel][kPanel + 1];
   __shared__ double invd[kPanel];
-  __shared__ int fail;
+  __shared__ int fail, lastReader;
   const int tid = threadIdx.x;
   if (tid == 0) fail = -1;
   for (int e = tid; e < w * w; e += blockDim.x) {
@@ -103,6 +103,12 @@ __global__ void __launch_bounds__(256) k_panel(const PanelTask *__restrict__ tas
     if (i >= j) D[i][j] = Lp[(int64_t)(c0 + j) * m + (c0 + i)];
   }
   __syncthreads();
+  // Every row chunk factors its own copy of the pivot block; the last chunk to have read the unfactored block writes
+  // the factored one back (no chunk waits for another).
+  if (tid == 0) {
+    __threadfence();
+    lastReader = atomicAdd(readers + t.group, 1) == t.nchunks - 1;
+  }
   for (int k = 0; k < w; k++) {
     if (tid == 0) {
       double d = D[k][k];
@@ -131,7 +137,7 @@ __global__ void __launch_bounds__(256) k_panel(const PanelTask *__restrict__ tas
     return;
   }
   const int c1 = c0 + w;
-  if (t.r0 == c1 || t.r0 == m) {  // the first row chunk writes the factored pivot block back
+  if (lastReader) {
     for (int e = tid; e < w * w; e += blockDim.x) {
       int i = e % w, j = e / w;
       if (i >= j) Lp[(int64_t)(c0 + j) * m + (c0 + i)] = D[i][j];
@@ -313,9 +319,9 @@ void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, con
                      double *U, const unsigned long long *status, cudaStream_t st) {
   if (ntasks > 0) k_assemble<<<(unsigned)ntasks, 256, 0, st>>>(tasks, P, values, Lx, U, status);
 }
-void launch_panel(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, unsigned long long *status,
-                  cudaStream_t st) {
-  if (ntasks > 0) k_panel<<<(unsigned)ntasks, 256, 0, st>>>(tasks, P, Lx, status);
+void launch_panel(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, int *readers,
+                  unsigned long long *status, cudaStream_t st) {
+  if (ntasks > 0) k_panel<<<(unsigned)ntasks, 256, 0, st>>>(tasks, P, Lx, readers, status);
 }
 void launch_update(const TileTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, double *U,
                    const unsigned long long *status, cudaStream_t st) {

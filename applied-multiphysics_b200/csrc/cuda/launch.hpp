@@ -11,8 +11,8 @@ namespace amp {
 
 void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, const double *values, double *Lx,
                      double *U, const unsigned long long *status, cudaStream_t st);
-void launch_panel(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, unsigned long long *status,
-                  cudaStream_t st);
+void launch_panel(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, int *readers,
+                  unsigned long long *status, cudaStream_t st);
 void launch_update(const TileTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, double *U,
                    const unsigned long long *status, cudaStream_t st);
 void launch_permute_in(const double *b, double *y, const int *perm, int n, int q, cudaStream_t st);

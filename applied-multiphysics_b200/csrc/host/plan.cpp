@@ -182,10 +182,14 @@ void build_plan(const Symbolic &S, Plan &P) {
         const int nc = P.snNc[s], m = P.snM[s], c0 = k * kPanel;
         if (c0 >= nc) continue;
         const int c1 = std::min(c0 + kPanel, nc);
+        const int g = P.panelGroups++;
         if (c1 >= m)
-          P.panelTasks.push_back({s, c0, m, m});
-        else
-          for (int r0 = c1; r0 < m; r0 += kTrsmRows) P.panelTasks.push_back({s, c0, r0, std::min(r0 + kTrsmRows, m)});
+          P.panelTasks.push_back({s, c0, m, m, g, 1});
+        else {
+          const int nch = (m - c1 + kTrsmRows - 1) / kTrsmRows;
+          for (int r0 = c1; r0 < m; r0 += kTrsmRows)
+            P.panelTasks.push_back({s, c0, r0, std::min(r0 + kTrsmRows, m), g, nch});
+        }
         const int T = (m - c1 + kTile - 1) / kTile;
         for (int I = 0; I < T; I++)
           for (int J = 0; J <= I; J++) P.tileTasks.push_back({s, c0, c1 + kTile * I, c1 + kTile * J});

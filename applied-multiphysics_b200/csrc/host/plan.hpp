@@ -25,6 +25,7 @@ constexpr int kSmallFront = 0; // fronts with m <= kSmallFront use the one-CTA-p
 
 struct PanelTask {  // POTRF of the pivot block [c0, c0 + w) of supernode s and TRSM of rows [r0, r1)
   int s, c0, r0, r1;
+  int group, nchunks;  // all row chunks of one pivot block share a group; its last reader writes the block back
 };
 struct TileTask {  // trailing update tile of supernode s after pivot block c0: rows [i0, i0+64), cols [j0, j0+64)
   int s, c0, i0, j0;
@@ -57,6 +58,7 @@ struct Plan {
   std::vector<AsmTask> asmTasks;
   std::vector<int64_t> asmLvlPtr;  // per level
   std::vector<PanelTask> panelTasks;
+  int panelGroups = 0;
   std::vector<TileTask> tileTasks;
   std::vector<int> lvlStepPtr;  // per level: steps [lvlStepPtr[L], lvlStepPtr[L+1])
   std::vector<StepRange> steps;
