@@ -59,6 +59,11 @@ class _FactorResult(C.Structure):
                 ("ms", C.c_double)]
 
 
+class _KernelStat(C.Structure):
+    _fields_ = [("name", C.c_char * 24), ("launches", C.c_int32), ("ms", C.c_double), ("flops", C.c_double),
+                ("bytes", C.c_double)]
+
+
 class _RefineOpts(C.Structure):
     _fields_ = [("max_steps", C.c_int), ("tol", C.c_double)]
 
@@ -91,6 +96,8 @@ SIGNATURES = {
     "amp_factor_download": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "amp_factor_destroy": (None, [C.c_void_p]),
     "amp_matvec": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    "amp_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
+    "amp_profile_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
     "amp_last_error": (C.c_char_p, []),
 }
 
@@ -328,6 +335,35 @@ class NumericFactor:
         out = np.zeros(max(self.sym.n, 1))
         _check(lib().amp_factor_download(self._h, None, out.ctypes.data))
         return out[: self.sym.n]
+
+    def profile(self, enable: bool = True) -> None:
+        """Time every kernel launch of the following calls with CUDA events (see profile_read)."""
+        _check(lib().amp_profile_enable(self._h, 1 if enable else 0))
+
+    def profile_read(self) -> list:
+        """Per kernel class: {name, launches, ms, flops, bytes} of the launches since profile(True)."""
+        arr = (_KernelStat * 16)()
+        cnt = C.c_int32(0)
+        _check(lib().amp_profile_read(self._h, arr, 16, C.byref(cnt)))
+        return [{"name": a.name.decode(), "launches": a.launches, "ms": a.ms, "flops": a.flops, "bytes": a.bytes}
+                for a in arr[: cnt.value]]
+
+    def solve_device(self, b_ptr: int, x_ptr: int, q: int = 1) -> None:
+        """x = A^-1 b for device pointers (q vectors of length n one after another)."""
+        _check(lib().amp_solve(self._h, C.c_void_p(b_ptr), q, C.c_void_p(x_ptr), 1))
+
+    def solve_refined_device(self, b_ptr: int, x_ptr: int, q: int = 1, maxSteps: int = 3, tol: float = 1e-14):
+        st = _RefineStats()
+        ro = _RefineOpts(maxSteps, tol)
+        _check(lib().amp_solve_refined(self._h, C.c_void_p(b_ptr), q, C.c_void_p(x_ptr), 1, C.byref(ro), C.byref(st)))
+        return st.rel_residual, st.steps
+
+    def solve_refined_host_pinned(self, b_ptr: int, x_ptr: int, q: int = 1, maxSteps: int = 3, tol: float = 1e-14):
+        """solveRefined with host (pinned) buffers: the library copies b in and x out."""
+        st = _RefineStats()
+        ro = _RefineOpts(maxSteps, tol)
+        _check(lib().amp_solve_refined(self._h, C.c_void_p(b_ptr), q, C.c_void_p(x_ptr), 0, C.byref(ro), C.byref(st)))
+        return st.rel_residual, st.steps
 
     def matVec(self, x) -> np.ndarray:
         xa = _f64(x)

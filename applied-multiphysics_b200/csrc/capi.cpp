@@ -95,12 +95,26 @@ struct amp_factor_s {
   unsigned long long *dStatus = nullptr;
   int *dReaders = nullptr;  // per pivot block: row chunks that have read it (reset at every factorization)
   bool ok = false, hasValues = false;
+  // profiling: events around every launch while enabled
+  bool profiling = false;
+  struct Rec {
+    int kind;
+    cudaEvent_t a, b;
+    double flops, bytes;
+  };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> evPool;
+  size_t evUsed = 0;
+  // the factorization sequence captured once, replayed afterwards
+  cudaGraphExec_t factorGraph = nullptr;
   // solve workspace (grown on demand)
   DevMem smem;
   int qcap = 0;
   double *dY = nullptr, *dV = nullptr, *dT = nullptr, *dB = nullptr, *dX = nullptr, *dR = nullptr, *dDX = nullptr,
          *dNorms = nullptr;
   ~amp_factor_s() {
+    if (factorGraph) cudaGraphExecDestroy(factorGraph);
+    for (auto e : evPool) cudaEventDestroy(e);
     smem.release();
     mem.release();
     if (ev0) cudaEventDestroy(ev0);
@@ -158,24 +172,81 @@ void ensure_solve_ws(amp_factor *f, int q) {
   f->qcap = q;
 }
 
+enum KernelKind { K_ASSEMBLE, K_PANEL, K_UPDATE, K_FORWARD, K_BACKWARD, K_PERMUTE, K_RESIDUAL, K_NKINDS };
+const char *kKindNames[K_NKINDS] = {"assemble", "panel_potrf_trsm", "update_syrk", "solve_forward",
+                                    "solve_backward", "permute", "residual_spmv"};
+
+cudaEvent_t pool_event(amp_factor *f) {
+  if (f->evUsed == f->evPool.size()) {
+    cudaEvent_t e;
+    ck(cudaEventCreate(&e), "cudaEventCreate");
+    f->evPool.push_back(e);
+  }
+  return f->evPool[f->evUsed++];
+}
+
+// Run one launch; while profiling, bracket it with events and record its algorithmic work.
+template <class L>
+void timed(amp_factor *f, int kind, double flops, double bytes, L &&launch) {
+  if (!f->profiling) {
+    launch();
+    return;
+  }
+  amp_factor_s::Rec r{kind, pool_event(f), pool_event(f), flops, bytes};
+  ck(cudaEventRecord(r.a, f->stream), "event");
+  launch();
+  ck(cudaEventRecord(r.b, f->stream), "event");
+  f->recs.push_back(r);
+}
+
+void enqueue_factor(amp_factor *f) {
+  const amp::Plan &P = f->plan->P;
+  const amp::DevPlan &dp = f->plan->dp;
+  cudaStream_t st = f->stream;
+  ck(cudaMemsetAsync(f->dStatus, 0xff, sizeof(unsigned long long), st), "memset status");
+  if (P.panelGroups) ck(cudaMemsetAsync(f->dReaders, 0, sizeof(int) * P.panelGroups, st), "memset readers");
+  for (int L = 0; L < P.nlevels; L++) {
+    timed(f, K_ASSEMBLE, 0.0, P.asmLvlBytes[L], [&] {
+      amp::launch_assemble(f->plan->dAsm + P.asmLvlPtr[L], P.asmLvlPtr[L + 1] - P.asmLvlPtr[L], dp, f->dValues, f->dLx,
+                           f->dU, f->dStatus, st);
+    });
+    for (int k = P.lvlStepPtr[L]; k < P.lvlStepPtr[L + 1]; k++) {
+      const amp::StepRange &sr = P.steps[k];
+      timed(f, K_PANEL, sr.panelFlops, 0.0, [&] {
+        amp::launch_panel(f->plan->dPanel + sr.panel0, sr.panel1 - sr.panel0, dp, f->dLx, f->dReaders, f->dStatus, st);
+      });
+      if (sr.tile1 > sr.tile0)
+        timed(f, K_UPDATE, sr.updateFlops, 0.0, [&] {
+          amp::launch_update(f->plan->dTile + sr.tile0, sr.tile1 - sr.tile0, dp, f->dLx, f->dU, f->dStatus, st);
+        });
+    }
+  }
+}
+
 // y (permuted order, q vectors) := A^-1 y in place
 void device_solve_permuted(amp_factor *f, int q) {
   const amp::Plan &P = f->plan->P;
   const amp::DevPlan &dp = f->plan->dp;
   const int64_t Vs = P.nsuper ? P.Sp[P.nsuper] : 0, Ts = P.solveBufDoubles;
+  const double lbytes = 8.0 * (double)P.nnzLStored * q;  // each sweep reads L once per right-hand side
   for (int L = 0; L < P.nlevels; L++)
-    amp::launch_forward(dp.lvlSn + P.lvlPtr[L], P.lvlPtr[L + 1] - P.lvlPtr[L], dp, f->dLx, f->dY, f->dV, f->dT, q, Vs,
-                        Ts, f->stream);
+    timed(f, K_FORWARD, 0.0, lbytes / P.nlevels, [&] {
+      amp::launch_forward(dp.lvlSn + P.lvlPtr[L], P.lvlPtr[L + 1] - P.lvlPtr[L], dp, f->dLx, f->dY, f->dV, f->dT, q,
+                          Vs, Ts, f->stream);
+    });
   for (int L = P.nlevels - 1; L >= 0; L--)
-    amp::launch_backward(dp.lvlSn + P.lvlPtr[L], P.lvlPtr[L + 1] - P.lvlPtr[L], dp, f->dLx, f->dY, q, f->stream);
+    timed(f, K_BACKWARD, 0.0, lbytes / P.nlevels, [&] {
+      amp::launch_backward(dp.lvlSn + P.lvlPtr[L], P.lvlPtr[L + 1] - P.lvlPtr[L], dp, f->dLx, f->dY, q, f->stream);
+    });
 }
 
 // x = A^-1 b for device vectors (original order)
 void device_solve(amp_factor *f, const double *dB, double *dX, int q) {
   const amp::Plan &P = f->plan->P;
-  amp::launch_permute_in(dB, f->dY, f->plan->dp.perm, P.n, q, f->stream);
+  const double pb = 20.0 * P.n * q;
+  timed(f, K_PERMUTE, 0.0, pb, [&] { amp::launch_permute_in(dB, f->dY, f->plan->dp.perm, P.n, q, f->stream); });
   device_solve_permuted(f, q);
-  amp::launch_permute_out(f->dY, dX, f->plan->dp.perm, P.n, q, f->stream);
+  timed(f, K_PERMUTE, 0.0, pb, [&] { amp::launch_permute_out(f->dY, dX, f->plan->dp.perm, P.n, q, f->stream); });
 }
 
 template <class F>
@@ -380,6 +451,11 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
       f->dValues = f->mem.alloc<double>((size_t)P.patNnz);
       f->dStatus = f->mem.alloc<unsigned long long>(1);
       f->dReaders = f->mem.alloc<int>((size_t)P.panelGroups);
+      static bool attrs = false;
+      if (!attrs) {
+        amp::init_kernel_attributes();
+        attrs = true;
+      }
     } catch (...) {
       delete f;
       throw;
@@ -414,18 +490,19 @@ int amp_factor_numeric(amp_factor *f, const double *values, int64_t nvalues, int
                          values_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st),
          "copy values");
     f->hasValues = true;
-    ck(cudaMemsetAsync(f->dStatus, 0xff, sizeof(unsigned long long), st), "memset status");
-    if (P.panelGroups) ck(cudaMemsetAsync(f->dReaders, 0, sizeof(int) * P.panelGroups, st), "memset readers");
     ck(cudaEventRecord(f->ev0, st), "event");
-    const amp::DevPlan &dp = f->plan->dp;
-    for (int L = 0; L < P.nlevels; L++) {
-      amp::launch_assemble(f->plan->dAsm + P.asmLvlPtr[L], P.asmLvlPtr[L + 1] - P.asmLvlPtr[L], dp, f->dValues,
-                           f->dLx, f->dU, f->dStatus, st);
-      for (int k = P.lvlStepPtr[L]; k < P.lvlStepPtr[L + 1]; k++) {
-        const amp::StepRange &sr = P.steps[k];
-        amp::launch_panel(f->plan->dPanel + sr.panel0, sr.panel1 - sr.panel0, dp, f->dLx, f->dReaders, f->dStatus, st);
-        amp::launch_update(f->plan->dTile + sr.tile0, sr.tile1 - sr.tile0, dp, f->dLx, f->dU, f->dStatus, st);
+    if (f->profiling) {
+      enqueue_factor(f);
+    } else {
+      if (!f->factorGraph) {  // capture the whole sequence once per factor object
+        cudaGraph_t g;
+        ck(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+        enqueue_factor(f);
+        ck(cudaStreamEndCapture(st, &g), "end capture");
+        ck(cudaGraphInstantiate(&f->factorGraph, g, 0), "graph instantiate");
+        cudaGraphDestroy(g);
       }
+      ck(cudaGraphLaunch(f->factorGraph, st), "graph launch");
     }
     ck(cudaGetLastError(), "kernel launch");
     ck(cudaEventRecord(f->ev1, st), "event");
@@ -503,7 +580,9 @@ int amp_solve_refined(amp_factor *f, const double *b, int32_t nrhs, double *x, i
     int steps = 0;
     for (;; steps++) {
       ck(cudaMemsetAsync(f->dNorms, 0, sizeof(double) * 2 * nrhs, st), "memset");
-      amp::launch_residual(n, f->plan->dRowptr, f->plan->dColidx, f->dValues, dX, dB, f->dR, f->dNorms, nrhs, st);
+      timed(f, K_RESIDUAL, 2.0 * P.patNnz * nrhs, (12.0 * P.patNnz + 24.0 * n) * nrhs, [&] {
+        amp::launch_residual(n, f->plan->dRowptr, f->plan->dColidx, f->dValues, dX, dB, f->dR, f->dNorms, nrhs, st);
+      });
       ck(cudaMemcpyAsync(norms.data(), f->dNorms, sizeof(double) * 2 * nrhs, cudaMemcpyDeviceToHost, st), "norms");
       ck(cudaStreamSynchronize(st), "residual");
       worst = 0;
@@ -541,6 +620,41 @@ int amp_factor_download(const amp_factor *f, double *Lx, double *D) {
 }
 
 void amp_factor_destroy(amp_factor *f) { delete f; }
+
+int amp_profile_enable(amp_factor *f, int enable) {
+  if (!f) return fail(AMP_INVALID, "null handle");
+  f->profiling = enable != 0;
+  f->recs.clear();
+  f->evUsed = 0;
+  return AMP_OK;
+}
+
+int amp_profile_read(amp_factor *f, amp_kernel_stat *stats, int32_t cap, int32_t *count) {
+  return guarded([&] {
+    if (!f) return fail(AMP_INVALID, "null handle");
+    ck(cudaStreamSynchronize(f->stream), "sync");
+    std::vector<amp_kernel_stat> acc(K_NKINDS);
+    for (int k = 0; k < K_NKINDS; k++) {
+      std::memset(&acc[k], 0, sizeof(amp_kernel_stat));
+      std::snprintf(acc[k].name, sizeof acc[k].name, "%s", kKindNames[k]);
+    }
+    for (auto &r : f->recs) {
+      float ms = 0;
+      ck(cudaEventElapsedTime(&ms, r.a, r.b), "elapsed");
+      acc[r.kind].launches++;
+      acc[r.kind].ms += ms;
+      acc[r.kind].flops += r.flops;
+      acc[r.kind].bytes += r.bytes;
+    }
+    int c = 0;
+    for (int k = 0; k < K_NKINDS && c < cap; k++)
+      if (acc[k].launches) stats[c++] = acc[k];
+    if (count) *count = c;
+    f->recs.clear();
+    f->evUsed = 0;
+    return (int)AMP_OK;
+  });
+}
 
 int amp_matvec(amp_factor *f, const double *x, int32_t nrhs, double *y) {
   return guarded([&] {

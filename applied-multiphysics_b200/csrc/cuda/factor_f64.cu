@@ -315,6 +315,10 @@ __global__ void __launch_bounds__(256) k_backward(const int *__restrict__ sns, D
 // ---------------------------------------------------------------------------------------------------------------
 // Launchers (host side)
 // ---------------------------------------------------------------------------------------------------------------
+void init_kernel_attributes() {
+  cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kPanel * kLdT * (int)sizeof(double));
+}
+
 void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, const double *values, double *Lx,
                      double *U, const unsigned long long *status, cudaStream_t st) {
   if (ntasks > 0) k_assemble<<<(unsigned)ntasks, 256, 0, st>>>(tasks, P, values, Lx, U, status);
@@ -326,11 +330,6 @@ void launch_panel(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, doub
 void launch_update(const TileTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, double *U,
                    const unsigned long long *status, cudaStream_t st) {
   constexpr int smem = 2 * kPanel * kLdT * (int)sizeof(double);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    attr = true;
-  }
   if (ntasks > 0) k_update<<<(unsigned)ntasks, 128, smem, st>>>(tasks, P, Lx, U, status);
 }
 void launch_permute_in(const double *b, double *y, const int *perm, int n, int q, cudaStream_t st) {

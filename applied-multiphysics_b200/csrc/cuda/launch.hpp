@@ -9,6 +9,8 @@
 
 namespace amp {
 
+void init_kernel_attributes();  // once per process and device, before the first launch
+
 void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, const double *values, double *Lx,
                      double *U, const unsigned long long *status, cudaStream_t st);
 void launch_panel(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, int *readers,

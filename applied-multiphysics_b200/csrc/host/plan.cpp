@@ -164,6 +164,7 @@ void build_plan(const Symbolic &S, Plan &P) {
   }
   // task lists per level
   P.asmLvlPtr.assign(P.nlevels + 1, 0);
+  P.asmLvlBytes.assign(P.nlevels, 0.0);
   P.lvlStepPtr.assign(P.nlevels + 1, 0);
   for (int L = 0; L < P.nlevels; L++) {
     int maxSteps = 0;
@@ -171,10 +172,18 @@ void build_plan(const Symbolic &S, Plan &P) {
       int s = P.lvlSn[q];
       for (int j0 = 0; j0 < P.snM[s]; j0 += kAsmCols) P.asmTasks.push_back({s, j0});
       maxSteps = std::max(maxSteps, (P.snNc[s] + kPanel - 1) / kPanel);
+      // bytes: value + lowerI + lowerSrc per A entry (16); read U + read/write the parent entry per child entry (24)
+      double b = 16.0 * (S.lowerP[P.snF[s] + P.snNc[s]] - S.lowerP[P.snF[s]]);
+      for (int k = P.chPtr[s]; k < P.chPtr[s + 1]; k++) {
+        double mu = P.snM[P.chList[k]] - P.snNc[P.chList[k]];
+        b += 24.0 * mu * (mu + 1) / 2;
+      }
+      P.asmLvlBytes[L] += b;
     }
     P.asmLvlPtr[L + 1] = (int64_t)P.asmTasks.size();
     for (int k = 0; k < maxSteps; k++) {
       StepRange sr;
+      sr.panelFlops = sr.updateFlops = 0;
       sr.panel0 = (int64_t)P.panelTasks.size();
       sr.tile0 = (int64_t)P.tileTasks.size();
       for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
@@ -190,6 +199,9 @@ void build_plan(const Symbolic &S, Plan &P) {
           for (int r0 = c1; r0 < m; r0 += kTrsmRows)
             P.panelTasks.push_back({s, c0, r0, std::min(r0 + kTrsmRows, m), g, nch});
         }
+        const double w = c1 - c0, r = m - c1;
+        sr.panelFlops += w * w * w / 3.0 + r * w * w;  // POTRF + TRSM
+        sr.updateFlops += w * r * (r + 1);             // 2 flops per lower entry per pivot column
         const int T = (m - c1 + kTile - 1) / kTile;
         for (int I = 0; I < T; I++)
           for (int J = 0; J <= I; J++) P.tileTasks.push_back({s, c0, c1 + kTile * I, c1 + kTile * J});

@@ -36,6 +36,7 @@ struct AsmTask {  // zero + assemble + extend-add front columns [j0, j0 + 32) of
 
 struct StepRange {
   int64_t panel0, panel1, tile0, tile1;
+  double panelFlops, updateFlops;  // algorithmic flops of the step's launches
 };
 
 struct Plan {
@@ -57,6 +58,7 @@ struct Plan {
   // task lists
   std::vector<AsmTask> asmTasks;
   std::vector<int64_t> asmLvlPtr;  // per level
+  std::vector<double> asmLvlBytes;  // algorithmic bytes of each level's assembly (A entries + extend-add)
   std::vector<PanelTask> panelTasks;
   int panelGroups = 0;
   std::vector<TileTask> tileTasks;

@@ -1,0 +1,323 @@
+"""Benchmark: factor + solve of the 3D P1 elasticity system (40^3 hexes x 6 Kuhn tets, 201,720 DOFs, x = 0 clamped,
+nested-dissection ordering) on one B200, FP64 and mixed precision + FP64 refinement, to relative residual <= 1e-12.
+
+One step = one numeric factorization + one solve (with refinement) of the seeded system; the symbolic analysis is
+per pattern and is reported separately (symbolic_ms), as the reference reuses it across factorizations.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision fp64|mixed|both]
+
+With --gpus N > 1 (launched by torch.distributed.run) every rank solves its own replica of the system (the path does
+not shard; "replicas only") and rank 0 prints the whole-job throughput. --impl reference times the reference's
+algorithm on the host cores: the oracle (a C restatement of the reference, including an SSE2 restatement of its WASM
+SIMD front kernel) on a bounded sample (one complete subtree of the same factorization), single-threaded because the
+reference is single-threaded by design.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "applied-multiphysics_b200"))
+
+METRIC = "factor+solve TFLOP/s to rel. residual <= 1e-12 (3D P1 elasticity 40^3, 1 x B200)"
+UNIT = "TFLOP/s"
+WORKLOAD = "elastic3d-40: 3D P1 linear elasticity, 40^3 hexes x 6 tets, E=1 nu=0.3, x=0 clamped, nd3Order"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "fallback": True}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = max(mx, float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_system():
+    import workloads as wl
+    return wl.elastic3d(40, seed=2, q=1)
+
+
+def measure_dgemm(torch):
+    """cuBLAS DGEMM 8192^3 (the FP64 roofline denominator; no FP64 figure is in MEASURED_PEAKS.json)."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    b = torch.randn_like(a)
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        a @ b
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 5
+    del a, b
+    torch.cuda.empty_cache()
+    return 2 * 8192 ** 3 / ms / 1e9
+
+
+def cpu_baseline_sample(w, perm, budget_s: float = 15.0):
+    """Oracle (SSE2 restatement of the reference's WASM front kernel) on one complete subtree of the factorization."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    so = orc.analyze(w.pat, perm=perm)
+    # subtree flops
+    ns = so.nsuper
+    sub = np.zeros(ns)
+    cc2 = so.colCount.astype(np.float64) ** 2
+    own = np.add.reduceat(cc2, so.superStart[:-1]) if ns else np.zeros(0)
+    sub[:] = own
+    for s in range(ns):
+        p = so.superParent[s]
+        if p >= 0:
+            sub[p] += sub[s]
+    # calibrate on a small subtree, then pick the largest subtree that fits the budget
+    order = np.argsort(sub)
+    small = int(order[np.searchsorted(sub[order], 2e8)]) if np.any(sub >= 2e8) else int(order[-1])
+    t = time.perf_counter()
+    orc.factor_subtree(so, w.values, small, simd=True)
+    rate = sub[small] / max(time.perf_counter() - t, 1e-6)
+    target = rate * budget_s
+    cand = np.where(sub <= target)[0]
+    root = int(cand[np.argmax(sub[cand])]) if cand.size else small
+    t = time.perf_counter()
+    ok, fl = orc.factor_subtree(so, w.values, root, simd=True)
+    dt = time.perf_counter() - t
+    return {"value": fl / dt / 1e12, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"factor of the subtree of supernode {root} ({fl:.3e} of {so.flops:.3e} flops, "
+                      f"{dt:.1f} s, SSE2 restatement of the reference's WASM front kernel, 1 thread); "
+                      f"extrapolated full factor {so.flops / (fl / dt):.0f} s",
+            "full_factor_s_est": so.flops / (fl / dt)}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    import workloads as wl  # noqa: F401
+    w = make_system()
+    import ampsolve as amp
+    try:
+        perm = amp.nd3Order(w.pat, w.x, w.y, w.z)
+    except Exception:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc
+        perm = orc.nd3_order(w.pat, w.x, w.y, w.z)
+    times, vals = [], []
+    for it in range(args.warmup + args.steps):
+        cb = cpu_baseline_sample(w, perm, budget_s=max(5.0, 60.0 / max(1, args.warmup + args.steps)))
+        if it >= args.warmup:
+            vals.append(cb["value"])
+            times.append(0)
+    v = float(np.median(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": w.n, "nnz": w.pat.nnz, "sample": cb["sample"]},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": cb["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "both"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+    import torch.distributed as dist
+
+    import ampsolve as amp
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    w = make_system()
+    n = w.n
+    t0 = time.perf_counter()
+    sym = amp.analyze(w.pat, ordering="nd3", x=w.x, y=w.y, z=w.z, device=local)
+    symbolic_ms = (time.perf_counter() - t0) * 1e3
+    flops_factor = sym.flops
+    flops_solve = 4.0 * sym.nnzL  # per right-hand side (forward + backward)
+
+    precisions = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    results = {}
+    dev = torch.device("cuda", local)
+    vals_d = torch.from_numpy(w.values).to(dev)
+    b_d = torch.from_numpy(w.rhs[0].copy()).to(dev)
+    x_d = torch.empty_like(b_d)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+    for prec in precisions:
+        num = amp.NumericFactor(sym, amp.CHOLESKY, amp.FP64 if prec == "fp64" else amp.MIXED)
+
+        def step():
+            ok = num.factor((vals_d.data_ptr(), vals_d.numel()), on_device=True)
+            relres, steps = num.solve_refined_device(b_d.data_ptr(), x_d.data_ptr(), 1, maxSteps=10, tol=1e-12)
+            return ok, relres, steps
+
+        for _ in range(args.warmup):
+            ok, relres, irs = step()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        with ClockSampler(local) as clk:
+            for k in range(args.steps):
+                flush.zero_()
+                torch.cuda.synchronize()
+                ev[k][0].record()
+                ok, relres, irs = step()  # synchronous library calls on the factor's own stream
+                ev[k][1].record()
+                torch.cuda.synchronize()
+        ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        # end to end through the C ABI with host buffers (pinned): H2D values + b, D2H x, every step
+        vals_h = torch.from_numpy(w.values).pin_memory()
+        b_h = torch.from_numpy(w.rhs[0].copy()).pin_memory()
+        x_h = torch.empty_like(b_h).pin_memory()
+        e2e = []
+        for k in range(max(2, args.steps)):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            num.factor(vals_h.numpy())
+            rr, ss = num.solve_refined_host_pinned(b_h.data_ptr(), x_h.data_ptr(), 1, 10, 1e-12)
+            e2e.append((time.perf_counter() - t) * 1e3)
+        e2e_ms = float(np.mean(e2e[1:])) if len(e2e) > 1 else e2e[0]
+        if world > 1:
+            t = torch.tensor([e2e_ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        # profile pass: per-kernel device time with CUDA events on the factor's stream
+        num.profile(True)
+        num.factor((vals_d.data_ptr(), vals_d.numel()), on_device=True)
+        num.solve_refined_device(b_d.data_ptr(), x_d.data_ptr(), 1, maxSteps=10, tol=1e-12)
+        prof = num.profile_read()
+        num.profile(False)
+        work = flops_factor + flops_solve * (1 + irs)
+        results[prec] = {"ok": ok, "ms": ms, "relres": relres, "ir_steps": irs, "work": work, "clk": clk.summary(),
+                         "prof": prof, "e2e_ms": e2e_ms, "factor_ms": num.ms}
+        del num
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    head = "mixed" if "mixed" in results else "fp64"
+    R = results[head]
+    pk = peaks()
+    dom = max(R["prof"], key=lambda k: k["ms"])
+    fp64_peak = measure_dgemm(torch)
+    if head == "fp64":
+        peak, bound, punit, note = fp64_peak, "tensor", "TFLOP/s", "measured cuBLAS DGEMM 8192^3 in this run"
+    else:
+        peak, bound, punit, note = pk.get("bf16_tflops_sustained", 1400.0), "tensor", "TFLOP/s", \
+            "MEASURED_PEAKS.json bf16_tflops_sustained (BF16 tensor, 3 products per FP32 update)"
+    if dom["flops"] > 0:
+        achieved = dom["flops"] / (dom["ms"] * 1e-3) / 1e12
+    else:
+        achieved, bound, punit, peak, note = dom["bytes"] / (dom["ms"] * 1e-3) / 1e9, "hbm", "GB/s", pk["hbm_gbs"], \
+            "MEASURED_PEAKS.json hbm_gbs"
+    launches = sum(k["launches"] for k in R["prof"])
+    value = world * R["work"] / (R["ms"] * 1e-3) / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": R["ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if head == "fp64" else "f32+bf16x3 (f64 refinement)", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": n, "nnz": w.pat.nnz, "nnzL": sym.nnzL, "flops_factor": flops_factor,
+                   "maxFront": sym.maxFront, "nsuper": sym.nsuper, "levels": sym.nlevels, "precision": head,
+                   "l2": "flushed between timed steps (256 MB write)", "parallelism": "replicas" if world > 1 else "1 gpu",
+                   "symbolic_ms": symbolic_ms},
+        "relres": R["relres"], "ir_steps": R["ir_steps"], "factor_ms": R["factor_ms"],
+        "e2e": {"value": world * R["work"] / (R["e2e_ms"] * 1e-3) / 1e12, "unit": UNIT,
+                "h2d_bytes_per_step": int(8 * w.pat.nnz + 8 * n), "d2h_bytes_per_step": int(8 * n),
+                "ms_per_step": R["e2e_ms"]},
+        "gpu_launches": int(launches * args.steps),
+        "clocks": R["clk"],
+        "roofline": {"bound": bound, "kernel": dom["name"], "achieved": achieved, "peak": peak, "unit": punit,
+                     "frac": achieved / peak, "traffic": None, "peak_source": note},
+        "kernels": R["prof"],
+        "fp64_dgemm_tflops": fp64_peak,
+    }
+    for p, r in results.items():
+        line[p] = {"ms_per_step": r["ms"], "value": world * r["work"] / (r["ms"] * 1e-3) / 1e12, "relres": r["relres"],
+                   "ir_steps": r["ir_steps"], "factor_ms": r["factor_ms"], "ok": r["ok"]}
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = {k: v for k, v in cpu_baseline_sample(w, sym.perm).items() if k != "full_factor_s_est"}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -142,6 +142,17 @@ AMP_API int amp_solve_refined(amp_factor *f, const double *b, int32_t nrhs, doub
 AMP_API int amp_factor_download(const amp_factor *f, double *Lx, double *D);
 AMP_API void amp_factor_destroy(amp_factor *f);
 
+/* Per-kernel-class device time of the calls made while profiling is on (CUDA events around every launch on the
+ * factor's stream; graphs are not used meanwhile). Algorithmic flops / bytes are the counts the work requires.
+ * Replaces the reference's opt-in timing records (sparse.mjs:20-29 timingSink, SparseCholesky.timing). */
+typedef struct {
+  char name[24];
+  int32_t launches;
+  double ms, flops, bytes;
+} amp_kernel_stat;
+AMP_API int amp_profile_enable(amp_factor *f, int enable);
+AMP_API int amp_profile_read(amp_factor *f, amp_kernel_stat *stats, int32_t cap, int32_t *count);
+
 /* matVec(pat, val, x) (sparse.mjs:219-228) on the device: y = A x for nrhs vectors (host pointers). */
 AMP_API int amp_matvec(amp_factor *f, const double *x, int32_t nrhs, double *y);
 

@@ -1343,8 +1343,17 @@ static int rf_front(double *H, double *W, int m, int nc, int ldlt, double *D, in
 
 /* kind: 0 Cholesky, 1 LDL^T. simd: 0 JS loops only ('blocked'), 1 SSE2 front kernel for m >= 32 ('wasm').
  * Returns 1 ok, 0 numerical failure. Lx has nnzLStored entries; D (LDL^T) has n. stats: nNeg, nPerturbed. */
+ORC_API int orc_factor_range(const orc_sym *S, const double *values, int kind, int simd, double pivotTol, double *Lx,
+                             double *D, int *stats, int s_first, int s_last);
 ORC_API int orc_factor(const orc_sym *S, const double *values, int kind, int simd, double pivotTol, double *Lx,
                        double *D, int *stats) {
+  return orc_factor_range(S, values, kind, simd, pivotTol, Lx, D, stats, 0, S->nsuper - 1);
+}
+
+/* The same multifrontal loop over supernodes s_first .. s_last only: a complete subtree in postorder (s_last its root,
+ * s_first its first descendant). Used to time a bounded sample of a large factorization. */
+ORC_API int orc_factor_range(const orc_sym *S, const double *values, int kind, int simd, double pivotTol, double *Lx,
+                             double *D, int *stats, int s_first, int s_last) {
   int n = S->n, nsuper = S->nsuper, maxFront = S->maxFront;
   stats[0] = stats[1] = 0;
   if (n == 0) return 1;
@@ -1367,7 +1376,7 @@ ORC_API int orc_factor(const orc_sym *S, const double *values, int kind, int sim
   size_t *stackPos = xmalloc(sizeof(size_t) * (nsuper + 1));
   int nsp = 0;
   int nNeg = 0, nPert = 0, ok = 1;
-  for (int s = 0; s < nsuper && ok; s++) {
+  for (int s = s_first; s <= s_last && s < nsuper && ok; s++) {
     int f = S->superStart[s], nc = S->superStart[s + 1] - f;
     int r0 = S->Sp[s], m = S->Sp[s + 1] - r0;
     for (int r = 0; r < m; r++) rel[S->Si[r0 + r]] = r;

@@ -51,6 +51,9 @@ def lib():
         L.orc_sym_arrays.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
         L.orc_factor.restype = C.c_int
         L.orc_factor.argtypes = [C.c_void_p, _f64p, C.c_int, C.c_int, C.c_double, _f64p, _f64p, _i32p]
+        L.orc_factor_range.restype = C.c_int
+        L.orc_factor_range.argtypes = [C.c_void_p, _f64p, C.c_int, C.c_int, C.c_double, _f64p, _f64p, _i32p, C.c_int,
+                                       C.c_int]
         L.orc_solve_chol.argtypes = [C.c_void_p, _f64p, _f64p, _f64p, C.c_int]
         L.orc_solve_ldlt.argtypes = [C.c_void_p, _f64p, _f64p, _f64p, C.c_int, _f64p, C.c_int]
         L.orc_matvec.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p]
@@ -190,6 +193,35 @@ def factor(sym: Symbolic, values, kind: str = "chol", simd: bool = False, pivot_
     ok = lib().orc_factor(sym.handle, v if v.size else np.zeros(1), 0 if kind == "chol" else 1, 1 if simd else 0,
                           pivot_tol, Lx, D, st)
     return bool(ok), Lx[: sym.nnzLStored], (None if kind == "chol" else D[: sym.n]), int(st[0]), int(st[1])
+
+
+def subtree_first(sym: Symbolic, root: int) -> int:
+    """First supernode (in postorder) of the subtree rooted at supernode `root`."""
+    first = root
+    stack = [root]
+    ch = [[] for _ in range(sym.nsuper)]
+    for s in range(sym.nsuper):
+        if sym.superParent[s] >= 0:
+            ch[sym.superParent[s]].append(s)
+    while stack:
+        s = stack.pop()
+        first = min(first, s)
+        stack.extend(ch[s])
+    return first
+
+
+def factor_subtree(sym: Symbolic, values, root: int, kind: str = "chol", simd: bool = True, pivot_tol: float = 1e-13):
+    """Factor only the subtree rooted at supernode `root` (a bounded CPU sample); returns (ok, flops of the sample)."""
+    s0 = subtree_first(sym, root)
+    v = np.ascontiguousarray(values, np.float64)
+    Lx = np.zeros(max(int(sym.nnzLStored), 1), np.float64)
+    D = np.zeros(max(sym.n, 1), np.float64)
+    st = np.zeros(2, np.int32)
+    ok = lib().orc_factor_range(sym.handle, v, 0 if kind == "chol" else 1, 1 if simd else 0, pivot_tol, Lx, D, st,
+                                s0, root)
+    c0, c1 = int(sym.superStart[s0]), int(sym.superStart[root + 1])
+    flops = float(np.sum(sym.colCount[c0:c1].astype(np.float64) ** 2))
+    return bool(ok), flops
 
 
 def solve_chol(sym: Symbolic, Lx, b, simd: bool = False) -> np.ndarray:
