@@ -69,6 +69,10 @@ struct DevMem {
 
 }  // namespace
 
+namespace amp {
+void set_last_error(const std::string &msg) { g_err = msg; }
+}  // namespace amp
+
 struct amp_plan_s {
   amp::Symbolic S;
   amp::Plan P;

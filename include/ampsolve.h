@@ -156,6 +156,17 @@ AMP_API int amp_profile_read(amp_factor *f, amp_kernel_stat *stats, int32_t cap,
 /* matVec(pat, val, x) (sparse.mjs:219-228) on the device: y = A x for nrhs vectors (host pointers). */
 AMP_API int amp_matvec(amp_factor *f, const double *x, int32_t nrhs, double *y);
 
+/* Partial Cholesky of ONE dense front in place, allocating nothing. No counterpart in the reference's API.
+ * For callers that cannot call cudaMalloc: applications that give all device memory to their own pool at start-up,
+ * or that must not let an allocation stall their other streams. F: device pointer to an m x m column-major front
+ * (ld = m, lower part read and written); nc pivot columns are factored (L11, L21 in place) and the trailing
+ * (m - nc) block receives the Schur update. Limit: m <= 16384; larger fronts are rejected with AMP_INVALID.
+ * Scratch: a static device array of 2 KB per GPU that loads the library, kept until exit and shared by every call
+ * (each call resets it); calls that overlap on the GPU race on it. The first call on a device looks up the array's
+ * address with that device current. stream: a cudaStream_t (null = default stream); the call waits for its work.
+ * *fail_column: -1, or the first pivot column that was not positive. */
+AMP_API int amp_front_factor_noalloc(double *F, int32_t m, int32_t nc, void *stream, int32_t *fail_column);
+
 /* Message of the last failing call on this thread ("" when none). */
 AMP_API const char *amp_last_error(void);
 
