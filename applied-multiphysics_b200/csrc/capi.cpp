@@ -83,6 +83,8 @@ struct amp_plan_s {
   amp::AsmTask *dAsm = nullptr;
   amp::PanelTask *dPanel = nullptr;
   amp::TileTask *dTile = nullptr;
+  int4 *dFwdTasks = nullptr, *dBwdTasks = nullptr;
+  int *dBlkOff = nullptr;
   int *dRowptr = nullptr, *dColidx = nullptr;
   std::vector<int> rowptr, colidx;  // host copy of the pattern (uploaded with the schedule)
   bool uploaded = false;
@@ -116,6 +118,9 @@ struct amp_factor_s {
   int qcap = 0;
   double *dY = nullptr, *dV = nullptr, *dT = nullptr, *dB = nullptr, *dX = nullptr, *dR = nullptr, *dDX = nullptr,
          *dNorms = nullptr;
+  int *dFlags = nullptr, *dTickets = nullptr;  // solve block ready flags (epoch-stamped) and per-launch tickets
+  unsigned long long *dSolveStatus = nullptr;
+  int solveEpoch = 0;
   ~amp_factor_s() {
     if (factorGraph) cudaGraphExecDestroy(factorGraph);
     for (auto e : evPool) cudaEventDestroy(e);
@@ -158,6 +163,9 @@ void upload_plan(amp_plan *pl) {
   pl->dAsm = m.upload(P.asmTasks);
   pl->dPanel = m.upload(P.panelTasks);
   pl->dTile = m.upload(P.tileTasks);
+  pl->dFwdTasks = (int4 *)m.upload(P.fwdTasks);
+  pl->dBwdTasks = (int4 *)m.upload(P.bwdTasks);
+  pl->dBlkOff = m.upload(P.blkOff);
 }
 
 void ensure_solve_ws(amp_factor *f, int q) {
@@ -233,15 +241,36 @@ void device_solve_permuted(amp_factor *f, int q) {
   const amp::DevPlan &dp = f->plan->dp;
   const int64_t Vs = P.nsuper ? P.Sp[P.nsuper] : 0, Ts = P.solveBufDoubles;
   const double lbytes = 8.0 * (double)P.nnzLStored * q;  // each sweep reads L once per right-hand side
-  for (int L = 0; L < P.nlevels; L++)
-    timed(f, K_FORWARD, 0.0, lbytes / P.nlevels, [&] {
-      amp::launch_forward(dp.lvlSn + P.lvlPtr[L], P.lvlPtr[L + 1] - P.lvlPtr[L], dp, f->dLx, f->dY, f->dV, f->dT, q,
-                          Vs, Ts, f->stream);
+  cudaStream_t st = f->stream;
+  ck(cudaMemsetAsync(f->dTickets, 0, sizeof(int) * 2 * P.nlevels, st), "memset tickets");
+  ck(cudaMemsetAsync(f->dSolveStatus, 0xff, sizeof(unsigned long long), st), "memset status");
+  const int efwd = 2 * (++f->solveEpoch) - 1, ebwd = 2 * f->solveEpoch;
+  for (int L = 0; L < P.nlevels; L++) {
+    const int cnt = P.lvlPtr[L + 1] - P.lvlPtr[L];
+    const double lvlBytes = lbytes / P.nlevels;
+    timed(f, K_FORWARD, 0.0, 0.0, [&] {
+      amp::launch_fwd_gather(dp.lvlSn + P.lvlPtr[L], cnt, dp, f->dY, f->dV, f->dT, q, Vs, Ts, st);
     });
+    timed(f, K_FORWARD, 0.0, lvlBytes, [&] {
+      amp::launch_fwd_blocks(f->plan->dFwdTasks + P.fwdLvlPtr[L], P.fwdLvlPtr[L + 1] - P.fwdLvlPtr[L],
+                             f->dTickets + L, dp, f->plan->dBlkOff, f->dLx, f->dY, f->dV, f->dT, f->dFlags, efwd, q,
+                             Vs, Ts, f->dSolveStatus, st);
+    });
+  }
   for (int L = P.nlevels - 1; L >= 0; L--)
     timed(f, K_BACKWARD, 0.0, lbytes / P.nlevels, [&] {
-      amp::launch_backward(dp.lvlSn + P.lvlPtr[L], P.lvlPtr[L + 1] - P.lvlPtr[L], dp, f->dLx, f->dY, q, f->stream);
+      amp::launch_bwd_blocks(f->plan->dBwdTasks + P.bwdLvlPtr[L], P.bwdLvlPtr[L + 1] - P.bwdLvlPtr[L],
+                             f->dTickets + P.nlevels + L, dp, f->plan->dBlkOff, f->dLx, f->dY, f->dFlags, ebwd, q,
+                             f->dSolveStatus, st);
     });
+}
+
+// AMP_DEVICE_TIMEOUT when a bounded wait of the last solve gave up (the stream must be synchronised)
+int solve_status(amp_factor *f) {
+  unsigned long long stw = 0;
+  ck(cudaMemcpy(&stw, f->dSolveStatus, sizeof stw, cudaMemcpyDeviceToHost), "copy solve status");
+  if (stw != amp::kStatusOk) return fail(AMP_DEVICE_TIMEOUT, "solve: a device wait timed out");
+  return AMP_OK;
 }
 
 // x = A^-1 b for device vectors (original order)
@@ -455,6 +484,10 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
       f->dValues = f->mem.alloc<double>((size_t)P.patNnz);
       f->dStatus = f->mem.alloc<unsigned long long>(1);
       f->dReaders = f->mem.alloc<int>((size_t)P.panelGroups);
+      f->dFlags = f->mem.alloc<int>((size_t)P.nflags);
+      ck(cudaMemset(f->dFlags, 0, sizeof(int) * std::max(1, P.nflags)), "memset flags");
+      f->dTickets = f->mem.alloc<int>(2 * (size_t)P.nlevels);
+      f->dSolveStatus = f->mem.alloc<unsigned long long>(1);
       static bool attrs = false;
       if (!attrs) {
         amp::init_kernel_attributes();
@@ -548,7 +581,7 @@ int amp_solve(amp_factor *f, const double *b, int32_t nrhs, double *x, int on_de
     ck(cudaGetLastError(), "kernel launch");
     if (!on_device) ck(cudaMemcpyAsync(x, dX, bytes, cudaMemcpyDeviceToHost, f->stream), "copy x");
     ck(cudaStreamSynchronize(f->stream), "solve");
-    return (int)AMP_OK;
+    return solve_status(f);
   });
 }
 
@@ -605,6 +638,7 @@ int amp_solve_refined(amp_factor *f, const double *b, int32_t nrhs, double *x, i
     ck(cudaGetLastError(), "kernel launch");
     if (!on_device) ck(cudaMemcpyAsync(x, dX, bytes, cudaMemcpyDeviceToHost, st), "copy x");
     ck(cudaStreamSynchronize(st), "refine");
+    if (int rc = solve_status(f)) return rc;
     stt.rel_residual = worst;
     stt.steps = steps;
     if (stats) *stats = stt;

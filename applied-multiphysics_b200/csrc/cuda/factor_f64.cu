@@ -136,7 +136,6 @@ __global__ void __launch_bounds__(256) k_panel(const PanelTask *__restrict__ tas
     if (tid == 0) atomicMin(status, status_word(f + c0 + fail, 1, s));
     return;
   }
-  const int c1 = c0 + w;
   if (lastReader) {
     for (int e = tid; e < w * w; e += blockDim.x) {
       int i = e % w, j = e / w;

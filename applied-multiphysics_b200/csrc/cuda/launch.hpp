@@ -22,5 +22,13 @@ void launch_permute_out(const double *y, double *x, const int *perm, int n, int 
 void launch_forward(const int *sns, int count, const DevPlan &P, const double *Lx, double *y, double *V, double *T,
                     int q, int64_t Vstride, int64_t Tstride, cudaStream_t st);
 void launch_backward(const int *sns, int count, const DevPlan &P, const double *Lx, double *y, int q, cudaStream_t st);
+void launch_fwd_gather(const int *sns, int count, const DevPlan &P, const double *y, double *V, const double *T, int q,
+                       int64_t Vstride, int64_t Tstride, cudaStream_t st);
+void launch_fwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const int *blkOff,
+                       const double *Lx, double *y, const double *V, double *T, int *flags, int epoch, int q,
+                       int64_t Vstride, int64_t Tstride, unsigned long long *status, cudaStream_t st);
+void launch_bwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const int *blkOff,
+                       const double *Lx, double *y, int *flags, int epoch, int q, unsigned long long *status,
+                       cudaStream_t st);
 
 }  // namespace amp

@@ -216,6 +216,39 @@ void build_plan(const Symbolic &S, Plan &P) {
   P.snTOff.assign(ns + 1, 0);
   for (int s = 0; s < ns; s++) P.snTOff[s + 1] = P.snTOff[s] + (P.snM[s] - P.snNc[s]);
   P.solveBufDoubles = P.snTOff[ns];
+  // solve block tasks per level (each task only waits for tasks listed before it)
+  constexpr int B = 64;
+  P.blkOff.assign(ns + 1, 0);
+  for (int s = 0; s < ns; s++) P.blkOff[s + 1] = P.blkOff[s] + (P.snNc[s] + B - 1) / B;
+  P.nflags = P.blkOff[ns];
+  P.fwdLvlPtr.assign(P.nlevels + 1, 0);
+  P.bwdLvlPtr.assign(P.nlevels + 1, 0);
+  auto push = [](std::vector<int> &v, int a, int b, int c) {
+    v.push_back(a);
+    v.push_back(b);
+    v.push_back(c);
+    v.push_back(0);
+  };
+  for (int L = 0; L < P.nlevels; L++) {
+    int maxNb = 0;
+    for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) maxNb = std::max(maxNb, (P.snNc[P.lvlSn[q]] + B - 1) / B);
+    for (int blk = 0; blk < maxNb; blk++)
+      for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
+        int s = P.lvlSn[q];
+        if (blk < (P.snNc[s] + B - 1) / B) push(P.fwdTasks, s, blk, 0);
+      }
+    for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
+      int s = P.lvlSn[q], mu = P.snM[s] - P.snNc[s];
+      for (int j = 0; j * B < mu; j++) push(P.fwdTasks, s, j, 1);
+    }
+    P.fwdLvlPtr[L + 1] = (int)(P.fwdTasks.size() / 4);
+    for (int d = 0; d < maxNb; d++)
+      for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
+        int s = P.lvlSn[q], nb = (P.snNc[s] + B - 1) / B;
+        if (d < nb) push(P.bwdTasks, s, nb - 1 - d, 0);
+      }
+    P.bwdLvlPtr[L + 1] = (int)(P.bwdTasks.size() / 4);
+  }
 }
 
 }  // namespace amp

@@ -68,6 +68,11 @@ struct Plan {
   std::vector<int> perm, Sp, Si;
   int64_t solveBufDoubles = 0;      // sum of mu (per RHS) for the forward update vectors
   std::vector<int64_t> snTOff;      // offset of supernode s's forward update vector (per RHS)
+  // block tasks of the solves ({supernode, block, kind, 0}); ready flags per 64-row pivot block
+  std::vector<int> blkOff;          // first flag of supernode s
+  int nflags = 0;
+  std::vector<int> fwdTasks, bwdTasks;  // int4 records, flattened
+  std::vector<int> fwdLvlPtr, bwdLvlPtr;
   double flops = 0;
 };
 
