@@ -13,6 +13,7 @@
 // of length mu to its parent, no atomics), backward per level top-down gathering ancestor values.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "devplan.cuh"
@@ -23,6 +24,21 @@ namespace amp {
 __device__ __forceinline__ double *front_addr(double *Lp, double *Up, int m, int nc, int i, int j) {
   // front entry (i, j), i >= j: first nc columns in the L panel (ld m), the rest in the U block (ld mu)
   return j < nc ? Lp + (int64_t)j * m + i : Up + (int64_t)(j - nc) * (m - nc) + (i - nc);
+}
+
+// 1/d by Newton-Raphson refinement of the FP32 reciprocal (x <- x + x (1 - d x), quadratic convergence: 2^-23 ->
+// 2^-46 -> full double precision). Not correctly rounded (within a few ulp of 1/d); used only for the trailing
+// update scale of the pivot block, where the factor's own rounding dominates. Positive finite d only; other values
+// are rejected by the pivot test before the result is used.
+__device__ __forceinline__ double recip_nr(double d) {
+  if (!(d > 1e-30 && d < 1e30)) return 1.0 / d;  // outside the float range of the first approximation
+  double x = (double)__frcp_rn((float)d);
+  double e = fma(-d, x, 1.0);
+  x = fma(x, e, x);
+  e = fma(-d, x, 1.0);
+  x = fma(x, e, x);
+  e = fma(-d, x, 1.0);
+  return fma(x, e, x);
 }
 
 __device__ __forceinline__ bool failed(const unsigned long long *st) {
@@ -85,8 +101,9 @@ __global__ void __launch_bounds__(256) k_assemble(const AsmTask *__restrict__ ta
 // ---------------------------------------------------------------------------------------------------------------
 // Panel: POTRF of the pivot block + TRSM of a chunk of rows below it
 // ---------------------------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_panel(const PanelTask *__restrict__ tasks, DevPlan P, double *__restrict__ Lx,
-                                               int *__restrict__ readers, unsigned long long *status) {
+__global__ void __launch_bounds__(256, 1) k_panel(const PanelTask *__restrict__ tasks, DevPlan P,
+                                                  double *__restrict__ Lx, int *__restrict__ readers,
+                                                  unsigned long long *status) {
   if (failed(status)) return;
   const PanelTask t = tasks[blockIdx.x];
   const int s = t.s, c0 = t.c0;
@@ -94,13 +111,20 @@ __global__ void __launch_bounds__(256) k_panel(const PanelTask *__restrict__ tas
   const int w = min(kPanel, nc - c0);
   double *Lp = Lx + P.snLxp[s];
   __shared__ double D[kPanel][kPanel + 1];
-  __shared__ double invd[kPanel];
+  __shared__ double invd[kPanel], ivsq[kPanel + 1], pd[kPanel + 1], piv[kPanel];
+  __shared__ unsigned short trail[kPanel * (kPanel - 1) / 2];  // (i, j) of the trailing entries, rightmost column first
+  extern __shared__ double xs[];  // kPanel x 256 staged solutions of the TRSM
   __shared__ int fail, lastReader;
   const int tid = threadIdx.x;
-  if (tid == 0) fail = -1;
-  for (int e = tid; e < w * w; e += blockDim.x) {
-    int i = e % w, j = e / w;
-    if (i >= j) D[i][j] = Lp[(int64_t)(c0 + j) * m + (c0 + i)];
+  // the pivot block (lower part); columns w .. 63 of a short last block are padded with the identity
+  for (int e = tid; e < kPanel * kPanel; e += blockDim.x) {
+    const int i = e & (kPanel - 1), j = e >> 6;
+    if (i >= j) D[i][j] = (i < w) ? Lp[(int64_t)(c0 + j) * m + (c0 + i)] : (i == j ? 1.0 : 0.0);
+  }
+  // trailing-entry list: columns 63, 62, ..., 1, rows j .. 63 within each
+  for (int j = kPanel - 1 - (tid >> 6) ; j >= 1; j -= 4) {
+    const int before = (kPanel - 1 - j) * (kPanel - j) / 2;  // entries of the columns right of j
+    for (int i = j + (tid & 63); i < kPanel; i += 64) trail[before + (i - j)] = (unsigned short)(i | (j << 8));
   }
   __syncthreads();
   // Every row chunk factors its own copy of the pivot block; the last chunk to have read the unfactored block writes
@@ -108,123 +132,214 @@ __global__ void __launch_bounds__(256) k_panel(const PanelTask *__restrict__ tas
   if (tid == 0) {
     __threadfence();
     lastReader = atomicAdd(readers + t.group, 1) == t.nchunks - 1;
+    fail = -1;
+    const double d = D[0][0];
+    if (!(d > 0.0)) fail = 0;
+    pd[0] = d;
+    ivsq[0] = recip_nr(d);
   }
+  __syncthreads();
+  // POTRF, right-looking on the unscaled columns: step k subtracts D[i][k] D[j][k] / d_k from the trailing entries
+  // (i >= j > k), enumerated from the rightmost column so that step k's entries are the first T_k of the list. One
+  // barrier per column; the owner of the next diagonal entry publishes its value and reciprocal (the only quantities
+  // on the column-to-column critical path). The columns are scaled to L once, after the loop.
   for (int k = 0; k < w; k++) {
-    if (tid == 0) {
-      double d = D[k][k];
-      if (!(d > 0.0)) {
-        fail = k;
-      } else {
-        double dk = sqrt(d);
-        D[k][k] = dk;
-        invd[k] = 1.0 / dk;
+    if (fail >= 0) break;  // uniform: written before the barrier that ended the previous step
+    const double iv2 = ivsq[k];
+    const int nk = kPanel - 1 - k;     // trailing columns k+1 .. 63
+    const int Tk = nk * (nk + 1) / 2;  // trailing lower entries
+    for (int e = tid; e < Tk; e += blockDim.x) {
+      const int ij = trail[e], i = ij & 0xff, j = ij >> 8;
+      const double v = D[i][j] - (D[i][k] * D[j][k]) * iv2;
+      D[i][j] = v;
+      if (i == k + 1 && j == k + 1) {  // the next pivot is final now
+        if (!(v > 0.0) && k + 1 < w) fail = k + 1;
+        pd[k + 1] = v;
+        ivsq[k + 1] = recip_nr(v);
       }
     }
     __syncthreads();
-    if (fail >= 0) break;
-    const double iv = invd[k];
-    for (int i = k + 1 + tid; i < w; i += blockDim.x) D[i][k] *= iv;
-    __syncthreads();
-    const int r = w - k - 1;
-    for (int e = tid; e < r * r; e += blockDim.x) {
-      int i = k + 1 + e / r, j = k + 1 + e % r;
-      if (j <= i) D[i][j] -= D[i][k] * D[j][k];
+  }
+  if (fail < 0) {
+    // L = D diag(d)^-1/2: one square root and reciprocal per column, then every entry scaled once
+    if (tid < kPanel) {
+      const double d = tid < w ? pd[tid] : 1.0;
+      const double lk = sqrt(d);
+      piv[tid] = lk;
+      invd[tid] = 1.0 / lk;
     }
     __syncthreads();
+    for (int e = tid; e < kPanel * kPanel; e += blockDim.x) {
+      const int i = e & (kPanel - 1), j = e >> 6;
+      if (i > j) D[i][j] *= invd[j];
+      else if (i == j) D[i][i] = piv[i];
+    }
   }
+  __syncthreads();
   if (fail >= 0) {
     if (tid == 0) atomicMin(status, status_word(f + c0 + fail, 1, s));
     return;
   }
   if (lastReader) {
     for (int e = tid; e < w * w; e += blockDim.x) {
-      int i = e % w, j = e / w;
+      const int i = e % w, j = e / w;
       if (i >= j) Lp[(int64_t)(c0 + j) * m + (c0 + i)] = D[i][j];
     }
   }
-  // TRSM: row r of the panel solves x L11^T = a, thread per row, the row in registers
+  // TRSM: row r of the panel solves x L11^T = a, one thread per row, 16 columns at a time (16 doubles live in
+  // registers); solved columns are staged in shared memory (xs[c][thread]) for the later quarters' updates.
   const int r = t.r0 + tid;
   if (r >= t.r1) return;
-  double x[kPanel];
+  constexpr int Q = 16;
+  double x[Q];
+#pragma unroll 1
+  for (int q0 = 0; q0 < w; q0 += Q) {
 #pragma unroll
-  for (int c = 0; c < kPanel; c++) x[c] = (c < w) ? Lp[(int64_t)(c0 + c) * m + r] : 0.0;
+    for (int c = 0; c < Q; c++) x[c] = (q0 + c < w) ? Lp[(int64_t)(c0 + q0 + c) * m + r] : 0.0;
+#pragma unroll 1
+    for (int k = 0; k < q0; k++) {
+      const double xk = xs[k * 256 + tid];
 #pragma unroll
-  for (int k = 0; k < kPanel; k++) {
-    if (k < w) {
-      x[k] *= invd[k];
+      for (int c = 0; c < Q; c++) x[c] -= xk * D[q0 + c][k];
+    }
 #pragma unroll
-      for (int c = k + 1; c < kPanel; c++)
-        if (c < w) x[c] -= x[k] * D[c][k];
+    for (int k = 0; k < Q; k++) {
+      x[k] *= invd[q0 + k];
+#pragma unroll
+      for (int c = k + 1; c < Q; c++) x[c] -= x[k] * D[q0 + c][q0 + k];
+    }
+#pragma unroll
+    for (int c = 0; c < Q; c++) {
+      if (q0 + c < w) Lp[(int64_t)(c0 + q0 + c) * m + r] = x[c];
+      xs[(q0 + c) * 256 + tid] = x[c];
     }
   }
-#pragma unroll
-  for (int c = 0; c < kPanel; c++)
-    if (c < w) Lp[(int64_t)(c0 + c) * m + r] = x[c];
 }
 
 // ---------------------------------------------------------------------------------------------------------------
-// Trailing update: F[i0:i0+64, j0:j0+64] -= A B^T, A = panel rows i, B = panel rows j, K = pivot block width.
-// 128 threads = 2 x 2 warps of 32 x 32; DMMA m8n8k4 (A row-major 8x4, B col-major 4x8, C 8x8 f64).
+// Trailing update: F[i0:i0+128, j0:j0+64] -= A B^T with A = panel rows i, B = panel rows j, K = pivot block width.
+// Persistent CTAs (two per SM, so one loads while the other computes) walk the step's tiles. The panel rows arrive in
+// shared memory by cp.async; the product runs on the FP64 tensor cores with mma.sync m16n8k16 (fragment layouts of
+// the SM90 FP64 MMA atoms: A (m = g + 8 (v & 1), k = t + 4 (v >> 1)), B (n = g, k = t + 4 v), C (m = g + 8 (v >> 1),
+// n = 2 t + (v & 1)), g = lane / 4, t = lane % 4). 8 warps as 4 (rows) x 2 (cols), 32 x 32 per warp.
 // ---------------------------------------------------------------------------------------------------------------
-__device__ __forceinline__ void dmma_8x8x4(double (&c)[2], double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(c[0]), "+d"(c[1])
-               : "d"(a), "d"(b));
+__device__ __forceinline__ void dmma_16x8x16(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]), "d"(b[1]),
+        "d"(b[2]), "d"(b[3]));
 }
 
-constexpr int kLdT = kTile + 4;  // 68 doubles: conflict-free fragment loads
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  const int bytes = valid ? 8 : 0;  // zero-fill when out of range
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
-__global__ void __launch_bounds__(128) k_update(const TileTask *__restrict__ tasks, DevPlan P, double *__restrict__ Lx,
-                                                double *__restrict__ U, const unsigned long long *status) {
+constexpr int kLdA = kTileM + 4;  // 132 doubles (== 4 mod 16): conflict-free fragment loads
+constexpr int kLdB = kTile + 4;   // 68 doubles
+constexpr int kStage = kPanel * kLdA + kPanel * kLdB;  // doubles per pipeline stage
+constexpr int kUpdateSmem = 2 * kStage * (int)sizeof(double);
+
+__device__ __forceinline__ void tile_loads(const TileTask &t, const double *Lx, double *stage) {
+  const int wk = (t.w + 15) & ~15;
+  const double *Lp = Lx + t.lp;
+  double *As = stage, *Bs = stage + kPanel * kLdA;
+  for (int e = threadIdx.x; e < wk * kTileM; e += blockDim.x) {
+    const int k = e >> 7, i = e & (kTileM - 1), r = t.i0 + i;
+    const bool ok = k < t.w && r < t.m;
+    cp_async8(As + k * kLdA + i, ok ? Lp + (int64_t)(t.c0 + k) * t.m + r : Lp, ok);
+  }
+  for (int e = threadIdx.x; e < wk * kTile; e += blockDim.x) {
+    const int k = e >> 6, i = e & (kTile - 1), r = t.j0 + i;
+    const bool ok = k < t.w && r < t.m;
+    cp_async8(Bs + k * kLdB + i, ok ? Lp + (int64_t)(t.c0 + k) * t.m + r : Lp, ok);
+  }
+}
+
+__global__ void __launch_bounds__(256, 1) k_update(const TileTask *__restrict__ tasks, int ntasks,
+                                                   double *__restrict__ Lx, double *__restrict__ U,
+                                                   const unsigned long long *status) {
   if (failed(status)) return;
-  const TileTask t = tasks[blockIdx.x];
-  const int s = t.s, c0 = t.c0, i0 = t.i0, j0 = t.j0;
-  const int nc = P.snNc[s], m = P.snM[s];
-  const int w = min(kPanel, nc - c0);
-  const int wp = (w + 3) & ~3;
-  double *Lp = Lx + P.snLxp[s];
-  double *Up = (m > nc) ? U + P.snUoff[s] : nullptr;
   extern __shared__ double smem_upd[];
-  double(*As)[kLdT] = reinterpret_cast<double(*)[kLdT]>(smem_upd);
-  double(*Bs)[kLdT] = reinterpret_cast<double(*)[kLdT]>(smem_upd + kPanel * kLdT);
-  const int tid = threadIdx.x;
-  for (int e = tid; e < wp * kTile; e += blockDim.x) {
-    const int k = e / kTile, i = e % kTile;
-    const int ri = i0 + i, rj = j0 + i;
-    const double *col = Lp + (int64_t)(c0 + k) * m;
-    As[k][i] = (k < w && ri < m) ? col[ri] : 0.0;
-    Bs[k][i] = (k < w && rj < m) ? col[rj] : 0.0;
-  }
-  __syncthreads();
-  const int warp = tid >> 5, lane = tid & 31;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
-  const int gid = lane >> 2, t4 = lane & 3;
-  double acc[4][4][2];
+  const int g = lane >> 2, t4 = lane & 3;
+  int t = blockIdx.x;
+  if (t >= ntasks) return;
+  TileTask cur = tasks[t];
+  TileTask nxt = cur;
+  if (t + (int)gridDim.x < ntasks) nxt = tasks[t + gridDim.x];
+  int stage = 0;
+  tile_loads(cur, Lx, smem_upd);
+  cp_async_commit();
+  for (; t < ntasks; t += gridDim.x) {
+    const bool hasNext = t + (int)gridDim.x < ntasks;
+    // record two tiles ahead, the next tile's panel rows, and this tile's C, all in flight during the MMAs
+    TileTask after = nxt;
+    if (t + 2 * (int)gridDim.x < ntasks) after = tasks[t + 2 * gridDim.x];
+    if (hasNext) tile_loads(nxt, Lx, smem_upd + (stage ^ 1) * kStage);
+    cp_async_commit();
+    const int m = cur.m, nc = cur.nc;
+    double *Lp = Lx + cur.lp;
+    double *Up = cur.up >= 0 ? U + cur.up : nullptr;
+    double cpre[2][4][4];
 #pragma unroll
-  for (int a = 0; a < 4; a++)
+    for (int a = 0; a < 2; a++)
 #pragma unroll
-    for (int b = 0; b < 4; b++) acc[a][b][0] = acc[a][b][1] = 0.0;
-  for (int kk = 0; kk < wp; kk += 4) {
-    double af[4], bf[4];
+      for (int b = 0; b < 4; b++)
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-      af[q] = As[kk + t4][wr + 8 * q + gid];
-      bf[q] = Bs[kk + t4][wc + 8 * q + gid];
-    }
+        for (int v = 0; v < 4; v++) {
+          const int i = cur.i0 + wr + 16 * a + g + 8 * (v >> 1), j = cur.j0 + wc + 8 * b + 2 * t4 + (v & 1);
+          cpre[a][b][v] = (i < m && j < m && i >= j) ? *front_addr(Lp, Up, m, nc, i, j) : 0.0;
+        }
+    if (hasNext) cp_async_wait<1>(); else cp_async_wait<0>();
+    __syncthreads();
+    const double *As = smem_upd + stage * kStage, *Bs = As + kPanel * kLdA;
+    const int wk = (cur.w + 15) & ~15;
+    double acc[2][4][4];
 #pragma unroll
-    for (int a = 0; a < 4; a++)
+    for (int a = 0; a < 2; a++)
 #pragma unroll
-      for (int b = 0; b < 4; b++) dmma_8x8x4(acc[a][b], af[a], bf[b]);
-  }
+      for (int b = 0; b < 4; b++)
 #pragma unroll
-  for (int a = 0; a < 4; a++)
+        for (int v = 0; v < 4; v++) acc[a][b][v] = 0.0;
+    for (int kk = 0; kk < wk; kk += 16) {
+      double bf[4][4];
 #pragma unroll
-    for (int b = 0; b < 4; b++)
+      for (int b = 0; b < 4; b++)
 #pragma unroll
-      for (int v = 0; v < 2; v++) {
-        const int i = i0 + wr + 8 * a + gid, j = j0 + wc + 8 * b + 2 * t4 + v;
-        if (i < m && j < m && i >= j) *front_addr(Lp, Up, m, nc, i, j) -= acc[a][b][v];
+        for (int v = 0; v < 4; v++) bf[b][v] = Bs[(kk + t4 + 4 * v) * kLdB + wc + 8 * b + g];
+#pragma unroll
+      for (int a = 0; a < 2; a++) {
+        double af[8];
+#pragma unroll
+        for (int v = 0; v < 8; v++) af[v] = As[(kk + t4 + 4 * (v >> 1)) * kLdA + wr + 16 * a + g + 8 * (v & 1)];
+#pragma unroll
+        for (int b = 0; b < 4; b++) dmma_16x8x16(acc[a][b], af, bf[b]);
       }
+    }
+    __syncthreads();  // this stage is free for the tile after next
+#pragma unroll
+    for (int a = 0; a < 2; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+          const int i = cur.i0 + wr + 16 * a + g + 8 * (v >> 1), j = cur.j0 + wc + 8 * b + 2 * t4 + (v & 1);
+          if (i < m && j < m && i >= j) *front_addr(Lp, Up, m, nc, i, j) = cpre[a][b][v] - acc[a][b][v];
+        }
+    stage ^= 1;
+    cur = nxt;
+    nxt = after;
+  }
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -314,8 +429,14 @@ __global__ void __launch_bounds__(256) k_backward(const int *__restrict__ sns, D
 // ---------------------------------------------------------------------------------------------------------------
 // Launchers (host side)
 // ---------------------------------------------------------------------------------------------------------------
+static int g_num_sms = 148;
+constexpr int kPanelSmem = kPanel * 256 * (int)sizeof(double);
 void init_kernel_attributes() {
-  cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kPanel * kLdT * (int)sizeof(double));
+  cudaFuncSetAttribute(k_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmem);
+  cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, kUpdateSmem);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
 }
 
 void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, const double *values, double *Lx,
@@ -324,12 +445,13 @@ void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, con
 }
 void launch_panel(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, int *readers,
                   unsigned long long *status, cudaStream_t st) {
-  if (ntasks > 0) k_panel<<<(unsigned)ntasks, 256, 0, st>>>(tasks, P, Lx, readers, status);
+  if (ntasks > 0) k_panel<<<(unsigned)ntasks, 256, kPanelSmem, st>>>(tasks, P, Lx, readers, status);
 }
 void launch_update(const TileTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, double *U,
                    const unsigned long long *status, cudaStream_t st) {
-  constexpr int smem = 2 * kPanel * kLdT * (int)sizeof(double);
-  if (ntasks > 0) k_update<<<(unsigned)ntasks, 128, smem, st>>>(tasks, P, Lx, U, status);
+  (void)P;
+  const int grid = (int)std::min<int64_t>(ntasks, g_num_sms);
+  if (ntasks > 0) k_update<<<grid, 256, kUpdateSmem, st>>>(tasks, (int)ntasks, Lx, U, status);
 }
 void launch_permute_in(const double *b, double *y, const int *perm, int n, int q, cudaStream_t st) {
   int64_t tot = (int64_t)n * q;

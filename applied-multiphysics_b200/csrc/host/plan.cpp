@@ -202,9 +202,10 @@ void build_plan(const Symbolic &S, Plan &P) {
         const double w = c1 - c0, r = m - c1;
         sr.panelFlops += w * w * w / 3.0 + r * w * w;  // POTRF + TRSM
         sr.updateFlops += w * r * (r + 1);             // 2 flops per lower entry per pivot column
-        const int T = (m - c1 + kTile - 1) / kTile;
-        for (int I = 0; I < T; I++)
-          for (int J = 0; J <= I; J++) P.tileTasks.push_back({s, c0, c1 + kTile * I, c1 + kTile * J});
+        // tiles holding at least one lower entry: rows [i0, i0 + 128) x cols [j0, j0 + 64) with i0 + 127 >= j0
+        for (int j0 = c1; j0 < m; j0 += kTile)
+          for (int i0 = c1 + ((j0 - c1) / kTileM) * kTileM; i0 < m; i0 += kTileM)
+            P.tileTasks.push_back({(long long)P.snLxp[s], (long long)P.snUoff[s], m, nc, c0, c1 - c0, i0, j0});
       }
       sr.panel1 = (int64_t)P.panelTasks.size();
       sr.tile1 = (int64_t)P.tileTasks.size();

@@ -18,7 +18,8 @@
 namespace amp {
 
 constexpr int kPanel = 64;     // pivot block width of the dense partial factorization
-constexpr int kTile = 64;      // trailing-update tile edge
+constexpr int kTile = 64;      // trailing-update tile columns
+constexpr int kTileM = 128;    // trailing-update tile rows
 constexpr int kAsmCols = 32;   // front columns per assembly task
 constexpr int kTrsmRows = 256; // panel rows per TRSM task
 constexpr int kSmallFront = 0; // fronts with m <= kSmallFront use the one-CTA-per-front kernel (0 = off)
@@ -27,8 +28,9 @@ struct PanelTask {  // POTRF of the pivot block [c0, c0 + w) of supernode s and 
   int s, c0, r0, r1;
   int group, nchunks;  // all row chunks of one pivot block share a group; its last reader writes the block back
 };
-struct TileTask {  // trailing update tile of supernode s after pivot block c0: rows [i0, i0+64), cols [j0, j0+64)
-  int s, c0, i0, j0;
+struct TileTask {  // trailing update tile: rows [i0, i0+128) x cols [j0, j0+64) of a front, K = pivot columns [c0, c0+w)
+  long long lp, up;      // offsets of the front's L panel (Lx) and update block (U arena, -1 if none)
+  int m, nc, c0, w, i0, j0;
 };
 struct AsmTask {  // zero + assemble + extend-add front columns [j0, j0 + 32) of supernode s
   int s, j0;
