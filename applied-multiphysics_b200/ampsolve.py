@@ -98,6 +98,8 @@ SIGNATURES = {
     "amp_matvec": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "amp_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
     "amp_profile_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
+    "amp_profile_launches": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                       C.POINTER(C.c_int32)]),
     "amp_last_error": (C.c_char_p, []),
 }
 
@@ -339,6 +341,16 @@ class NumericFactor:
     def profile(self, enable: bool = True) -> None:
         """Time every kernel launch of the following calls with CUDA events (see profile_read)."""
         _check(lib().amp_profile_enable(self._h, 1 if enable else 0))
+
+    def profile_launches(self, cap: int = 100000):
+        """(kinds, ms, flops) arrays of the individual launches since profile(True); call before profile_read."""
+        kinds = np.zeros(cap, np.int32)
+        ms = np.zeros(cap)
+        fl = np.zeros(cap)
+        cnt = C.c_int32(0)
+        _check(lib().amp_profile_launches(self._h, kinds.ctypes.data, ms.ctypes.data, fl.ctypes.data, cap,
+                                          C.byref(cnt)))
+        return kinds[: cnt.value], ms[: cnt.value], fl[: cnt.value]
 
     def profile_read(self) -> list:
         """Per kernel class: {name, launches, ms, flops, bytes} of the launches since profile(True)."""

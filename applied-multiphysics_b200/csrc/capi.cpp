@@ -82,7 +82,7 @@ struct amp_plan_s {
   amp::DevPlan dp{};
   amp::AsmTask *dAsm = nullptr;
   amp::PanelTask *dPanel = nullptr;
-  amp::TileTask *dTile = nullptr;
+  amp::TileTask *dTile = nullptr, *dUTile = nullptr;
   int4 *dFwdTasks = nullptr, *dBwdTasks = nullptr;
   int *dBlkOff = nullptr;
   int *dRowptr = nullptr, *dColidx = nullptr;
@@ -163,6 +163,7 @@ void upload_plan(amp_plan *pl) {
   pl->dAsm = m.upload(P.asmTasks);
   pl->dPanel = m.upload(P.panelTasks);
   pl->dTile = m.upload(P.tileTasks);
+  pl->dUTile = m.upload(P.uTasks);
   pl->dFwdTasks = (int4 *)m.upload(P.fwdTasks);
   pl->dBwdTasks = (int4 *)m.upload(P.bwdTasks);
   pl->dBlkOff = m.upload(P.blkOff);
@@ -232,6 +233,11 @@ void enqueue_factor(amp_factor *f) {
           amp::launch_update(f->plan->dTile + sr.tile0, sr.tile1 - sr.tile0, dp, f->dLx, f->dU, f->dStatus, st);
         });
     }
+    if (P.uLvlPtr[L + 1] > P.uLvlPtr[L])
+      timed(f, K_UPDATE, P.uLvlFlops[L], 0.0, [&] {
+        amp::launch_update(f->plan->dUTile + P.uLvlPtr[L], P.uLvlPtr[L + 1] - P.uLvlPtr[L], dp, f->dLx, f->dU,
+                           f->dStatus, st);
+      });
   }
 }
 
@@ -665,6 +671,25 @@ int amp_profile_enable(amp_factor *f, int enable) {
   f->recs.clear();
   f->evUsed = 0;
   return AMP_OK;
+}
+
+int amp_profile_launches(amp_factor *f, int32_t *kinds, double *ms, double *flops, int32_t cap, int32_t *count) {
+  return guarded([&] {
+    if (!f) return fail(AMP_INVALID, "null handle");
+    ck(cudaStreamSynchronize(f->stream), "sync");
+    int c = 0;
+    for (auto &r : f->recs) {
+      if (c >= cap) break;
+      float t = 0;
+      ck(cudaEventElapsedTime(&t, r.a, r.b), "elapsed");
+      kinds[c] = r.kind;
+      ms[c] = t;
+      flops[c] = r.flops;
+      c++;
+    }
+    if (count) *count = c;
+    return (int)AMP_OK;
+  });
 }
 
 int amp_profile_read(amp_factor *f, amp_kernel_stat *stats, int32_t cap, int32_t *count) {

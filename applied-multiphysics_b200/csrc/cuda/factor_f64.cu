@@ -248,22 +248,35 @@ constexpr int kLdB = kTile + 4;   // 68 doubles
 constexpr int kStage = kPanel * kLdA + kPanel * kLdB;  // doubles per pipeline stage
 constexpr int kUpdateSmem = 2 * kStage * (int)sizeof(double);
 
-__device__ __forceinline__ void tile_loads(const TileTask &t, const double *Lx, double *stage) {
-  const int wk = (t.w + 15) & ~15;
+// Panel rows of one tile and one 64-column chunk of its K range into a pipeline stage. Thread t owns one row of A
+// (t % 128) and of B (t % 64) and walks the pivot columns with a pointer step of 2 m (A) or 4 m (B).
+__device__ __forceinline__ void tile_loads(const TileTask &t, int chunk, const double *Lx, double *stage) {
+  const int kc = t.c0 + chunk * kPanel, kw = min(kPanel, t.w - chunk * kPanel), wk = (kw + 15) & ~15;
   const double *Lp = Lx + t.lp;
-  double *As = stage, *Bs = stage + kPanel * kLdA;
-  for (int e = threadIdx.x; e < wk * kTileM; e += blockDim.x) {
-    const int k = e >> 7, i = e & (kTileM - 1), r = t.i0 + i;
-    const bool ok = k < t.w && r < t.m;
-    cp_async8(As + k * kLdA + i, ok ? Lp + (int64_t)(t.c0 + k) * t.m + r : Lp, ok);
+  const int tid = threadIdx.x;
+  {
+    const int i = tid & (kTileM - 1), k0 = tid >> 7, r = t.i0 + i;
+    const bool rowok = r < t.m;
+    const double *src = Lp + (int64_t)(kc + k0) * t.m + (rowok ? r : 0);
+    double *dst = stage + k0 * kLdA + i;
+    const int64_t step = 2 * (int64_t)t.m;
+#pragma unroll 4
+    for (int k = k0; k < wk; k += 2, src += step, dst += 2 * kLdA) cp_async8(dst, rowok && k < kw ? src : Lp, rowok && k < kw);
   }
-  for (int e = threadIdx.x; e < wk * kTile; e += blockDim.x) {
-    const int k = e >> 6, i = e & (kTile - 1), r = t.j0 + i;
-    const bool ok = k < t.w && r < t.m;
-    cp_async8(Bs + k * kLdB + i, ok ? Lp + (int64_t)(t.c0 + k) * t.m + r : Lp, ok);
+  {
+    const int i = tid & (kTile - 1), k0 = tid >> 6, r = t.j0 + i;
+    const bool rowok = r < t.m;
+    const double *src = Lp + (int64_t)(kc + k0) * t.m + (rowok ? r : 0);
+    double *dst = stage + kPanel * kLdA + k0 * kLdB + i;
+    const int64_t step = 4 * (int64_t)t.m;
+#pragma unroll 4
+    for (int k = k0; k < wk; k += 4, src += step, dst += 4 * kLdB) cp_async8(dst, rowok && k < kw ? src : Lp, rowok && k < kw);
   }
 }
 
+// Update tiles F[i0:i0+128, j0:j0+64] -= A B^T, K = w pivot columns in 64-column chunks. Persistent CTAs walk
+// (tile, chunk) items; the next item's panel rows stream into the other stage while the current one runs on the
+// FP64 tensor cores; the C tile is read once (prefetched into registers during its first chunk) and written once.
 __global__ void __launch_bounds__(256, 1) k_update(const TileTask *__restrict__ tasks, int ntasks,
                                                    double *__restrict__ Lx, double *__restrict__ U,
                                                    const unsigned long long *status) {
@@ -275,70 +288,94 @@ __global__ void __launch_bounds__(256, 1) k_update(const TileTask *__restrict__ 
   int t = blockIdx.x;
   if (t >= ntasks) return;
   TileTask cur = tasks[t];
-  TileTask nxt = cur;
-  if (t + (int)gridDim.x < ntasks) nxt = tasks[t + gridDim.x];
+  TileTask nxtTask = cur;
+  if (t + (int)gridDim.x < ntasks) nxtTask = tasks[t + gridDim.x];
+  int chunk = 0, nch = (cur.w + kPanel - 1) / kPanel;
   int stage = 0;
-  tile_loads(cur, Lx, smem_upd);
+  tile_loads(cur, 0, Lx, smem_upd);
   cp_async_commit();
-  for (; t < ntasks; t += gridDim.x) {
-    const bool hasNext = t + (int)gridDim.x < ntasks;
-    // record two tiles ahead, the next tile's panel rows, and this tile's C, all in flight during the MMAs
-    TileTask after = nxt;
-    if (t + 2 * (int)gridDim.x < ntasks) after = tasks[t + 2 * gridDim.x];
-    if (hasNext) tile_loads(nxt, Lx, smem_upd + (stage ^ 1) * kStage);
+  double *cp[4][2];
+  int jj[4][2], ii[2][2];
+  double cpre[2][4][4], acc[2][4][4];
+  bool newTile = true;
+  while (true) {
+    // the next (tile, chunk) item
+    const bool sameTile = chunk + 1 < nch;
+    const bool hasNext = sameTile || t + (int)gridDim.x < ntasks;
+    if (hasNext) tile_loads(sameTile ? cur : nxtTask, sameTile ? chunk + 1 : 0, Lx, smem_upd + (stage ^ 1) * kStage);
     cp_async_commit();
-    const int m = cur.m, nc = cur.nc;
-    double *Lp = Lx + cur.lp;
-    double *Up = cur.up >= 0 ? U + cur.up : nullptr;
-    double cpre[2][4][4];
-#pragma unroll
-    for (int a = 0; a < 2; a++)
+    const int m = cur.m, nc = cur.nc, mu = m - nc;
+    if (newTile) {
+      // this thread's 8 columns (base pointers indexed by the front row) and 4 rows of the C tile; C prefetch
+      double *Lp = Lx + cur.lp;
+      double *Up = cur.up >= 0 ? U + cur.up : Lp;
 #pragma unroll
       for (int b = 0; b < 4; b++)
 #pragma unroll
-        for (int v = 0; v < 4; v++) {
-          const int i = cur.i0 + wr + 16 * a + g + 8 * (v >> 1), j = cur.j0 + wc + 8 * b + 2 * t4 + (v & 1);
-          cpre[a][b][v] = (i < m && j < m && i >= j) ? *front_addr(Lp, Up, m, nc, i, j) : 0.0;
+        for (int u = 0; u < 2; u++) {
+          const int j = cur.j0 + wc + 8 * b + 2 * t4 + u;
+          jj[b][u] = j < cur.jend ? j : 0x3fffffff;  // columns beyond jend are masked
+          cp[b][u] = j < nc ? Lp + (int64_t)j * m : Up + (int64_t)(j - nc) * mu - nc;
         }
+#pragma unroll
+      for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) ii[a][h] = cur.i0 + wr + 16 * a + g + 8 * h;
+#pragma unroll
+      for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++)
+#pragma unroll
+          for (int v = 0; v < 4; v++) {
+            const int i = ii[a][v >> 1], j = jj[b][v & 1];
+            cpre[a][b][v] = (i < m && i >= j) ? cp[b][v & 1][i] : 0.0;
+            acc[a][b][v] = 0.0;
+          }
+      newTile = false;
+    }
     if (hasNext) cp_async_wait<1>(); else cp_async_wait<0>();
     __syncthreads();
-    const double *As = smem_upd + stage * kStage, *Bs = As + kPanel * kLdA;
-    const int wk = (cur.w + 15) & ~15;
-    double acc[2][4][4];
-#pragma unroll
-    for (int a = 0; a < 2; a++)
-#pragma unroll
-      for (int b = 0; b < 4; b++)
-#pragma unroll
-        for (int v = 0; v < 4; v++) acc[a][b][v] = 0.0;
+    const double *As = smem_upd + stage * kStage + wr + g, *Bs = smem_upd + stage * kStage + kPanel * kLdA + wc + g;
+    const int kw = min(kPanel, cur.w - chunk * kPanel), wk = (kw + 15) & ~15;
     for (int kk = 0; kk < wk; kk += 16) {
+      const double *Ak = As + (kk + t4) * kLdA, *Bk = Bs + (kk + t4) * kLdB;
       double bf[4][4];
 #pragma unroll
       for (int b = 0; b < 4; b++)
 #pragma unroll
-        for (int v = 0; v < 4; v++) bf[b][v] = Bs[(kk + t4 + 4 * v) * kLdB + wc + 8 * b + g];
+        for (int v = 0; v < 4; v++) bf[b][v] = Bk[4 * v * kLdB + 8 * b];
 #pragma unroll
       for (int a = 0; a < 2; a++) {
         double af[8];
 #pragma unroll
-        for (int v = 0; v < 8; v++) af[v] = As[(kk + t4 + 4 * (v >> 1)) * kLdA + wr + 16 * a + g + 8 * (v & 1)];
+        for (int v = 0; v < 8; v++) af[v] = Ak[4 * (v >> 1) * kLdA + 16 * a + 8 * (v & 1)];
 #pragma unroll
         for (int b = 0; b < 4; b++) dmma_16x8x16(acc[a][b], af, bf[b]);
       }
     }
-    __syncthreads();  // this stage is free for the tile after next
+    __syncthreads();  // this stage is free for the item after next
+    stage ^= 1;
+    if (sameTile) {
+      chunk++;
+      continue;
+    }
+    // last chunk of the tile: write C once
 #pragma unroll
     for (int a = 0; a < 2; a++)
 #pragma unroll
       for (int b = 0; b < 4; b++)
 #pragma unroll
         for (int v = 0; v < 4; v++) {
-          const int i = cur.i0 + wr + 16 * a + g + 8 * (v >> 1), j = cur.j0 + wc + 8 * b + 2 * t4 + (v & 1);
-          if (i < m && j < m && i >= j) *front_addr(Lp, Up, m, nc, i, j) = cpre[a][b][v] - acc[a][b][v];
+          const int i = ii[a][v >> 1], j = jj[b][v & 1];
+          if (i < m && i >= j) cp[b][v & 1][i] = cpre[a][b][v] - acc[a][b][v];
         }
-    stage ^= 1;
-    cur = nxt;
-    nxt = after;
+    if (!hasNext) break;
+    t += gridDim.x;
+    cur = nxtTask;
+    if (t + (int)gridDim.x < ntasks) nxtTask = tasks[t + gridDim.x];
+    chunk = 0;
+    nch = (cur.w + kPanel - 1) / kPanel;
+    newTile = true;
   }
 }
 

@@ -165,6 +165,7 @@ void build_plan(const Symbolic &S, Plan &P) {
   // task lists per level
   P.asmLvlPtr.assign(P.nlevels + 1, 0);
   P.asmLvlBytes.assign(P.nlevels, 0.0);
+  P.uLvlPtr.assign(1, 0);
   P.lvlStepPtr.assign(P.nlevels + 1, 0);
   for (int L = 0; L < P.nlevels; L++) {
     int maxSteps = 0;
@@ -199,19 +200,33 @@ void build_plan(const Symbolic &S, Plan &P) {
           for (int r0 = c1; r0 < m; r0 += kTrsmRows)
             P.panelTasks.push_back({s, c0, r0, std::min(r0 + kTrsmRows, m), g, nch});
         }
-        const double w = c1 - c0, r = m - c1;
+        // trailing update restricted to the remaining pivot columns [c1, nc): rows [c1, m) x cols [c1, nc)
+        const double w = c1 - c0, r = m - c1, pc = nc - c1;
         sr.panelFlops += w * w * w / 3.0 + r * w * w;  // POTRF + TRSM
-        sr.updateFlops += w * r * (r + 1);             // 2 flops per lower entry per pivot column
-        // tiles holding at least one lower entry: rows [i0, i0 + 128) x cols [j0, j0 + 64) with i0 + 127 >= j0
-        for (int j0 = c1; j0 < m; j0 += kTile)
+        sr.updateFlops += w * pc * (2 * r - pc + 1);    // 2 flops per lower entry of the trapezoid per pivot column
+        for (int j0 = c1; j0 < nc; j0 += kTile)
           for (int i0 = c1 + ((j0 - c1) / kTileM) * kTileM; i0 < m; i0 += kTileM)
-            P.tileTasks.push_back({(long long)P.snLxp[s], (long long)P.snUoff[s], m, nc, c0, c1 - c0, i0, j0});
+            P.tileTasks.push_back({(long long)P.snLxp[s], (long long)P.snUoff[s], m, nc, c0, c1 - c0, i0, j0, nc, 0});
       }
       sr.panel1 = (int64_t)P.panelTasks.size();
       sr.tile1 = (int64_t)P.tileTasks.size();
       P.steps.push_back(sr);
     }
     P.lvlStepPtr[L + 1] = (int)P.steps.size();
+    // update blocks of the level's fronts: one long-K pass each
+    double uf = 0;
+    for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
+      int s = P.lvlSn[q];
+      const int nc = P.snNc[s], m = P.snM[s];
+      if (m <= nc) continue;
+      const double mu = m - nc;
+      uf += (double)nc * mu * (mu + 1);
+      for (int j0 = nc; j0 < m; j0 += kTile)
+        for (int i0 = nc + ((j0 - nc) / kTileM) * kTileM; i0 < m; i0 += kTileM)
+          P.uTasks.push_back({(long long)P.snLxp[s], (long long)P.snUoff[s], m, nc, 0, nc, i0, j0, m, 0});
+    }
+    P.uLvlPtr.push_back((int64_t)P.uTasks.size());
+    P.uLvlFlops.push_back(uf);
   }
   // forward-solve update vectors
   P.snTOff.assign(ns + 1, 0);

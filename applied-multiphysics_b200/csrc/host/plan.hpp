@@ -28,9 +28,9 @@ struct PanelTask {  // POTRF of the pivot block [c0, c0 + w) of supernode s and 
   int s, c0, r0, r1;
   int group, nchunks;  // all row chunks of one pivot block share a group; its last reader writes the block back
 };
-struct TileTask {  // trailing update tile: rows [i0, i0+128) x cols [j0, j0+64) of a front, K = pivot columns [c0, c0+w)
+struct TileTask {  // update tile: rows [i0, i0+128) x cols [j0, min(j0+64, jend)) of a front, K = columns [c0, c0+w)
   long long lp, up;      // offsets of the front's L panel (Lx) and update block (U arena, -1 if none)
-  int m, nc, c0, w, i0, j0;
+  int m, nc, c0, w, i0, j0, jend, pad;
 };
 struct AsmTask {  // zero + assemble + extend-add front columns [j0, j0 + 32) of supernode s
   int s, j0;
@@ -40,6 +40,8 @@ struct StepRange {
   int64_t panel0, panel1, tile0, tile1;
   double panelFlops, updateFlops;  // algorithmic flops of the step's launches
 };
+// The update block of every front receives its whole Schur update once, after the panel steps of its level:
+// U -= L21 L21^T with K = nc (tiles over the lower triangle of [nc, m)^2).
 
 struct Plan {
   int n = 0, nsuper = 0, nlevels = 0, maxFront = 0;
@@ -65,6 +67,9 @@ struct Plan {
   int panelGroups = 0;
   std::vector<TileTask> tileTasks;
   std::vector<int> lvlStepPtr;  // per level: steps [lvlStepPtr[L], lvlStepPtr[L+1])
+  std::vector<TileTask> uTasks;  // long-K update-block tiles, per level [uLvlPtr[L], uLvlPtr[L+1])
+  std::vector<int64_t> uLvlPtr;
+  std::vector<double> uLvlFlops;
   std::vector<StepRange> steps;
   // solve: rows below of each supernode (Si[Sp[s] + nc ..]) and the perm
   std::vector<int> perm, Sp, Si;

@@ -152,6 +152,10 @@ typedef struct {
 } amp_kernel_stat;
 AMP_API int amp_profile_enable(amp_factor *f, int enable);
 AMP_API int amp_profile_read(amp_factor *f, amp_kernel_stat *stats, int32_t cap, int32_t *count);
+/* The individual launches behind amp_profile_read (call before it; it clears the records): kernel class index (order
+ * of amp_profile_read's names: assemble, panel, update, forward, backward, permute, residual), device ms, flops. */
+AMP_API int amp_profile_launches(amp_factor *f, int32_t *kinds, double *ms, double *flops, int32_t cap,
+                                 int32_t *count);
 
 /* matVec(pat, val, x) (sparse.mjs:219-228) on the device: y = A x for nrhs vectors (host pointers). */
 AMP_API int amp_matvec(amp_factor *f, const double *x, int32_t nrhs, double *y);
