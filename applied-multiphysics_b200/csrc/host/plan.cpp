@@ -200,13 +200,24 @@ void build_plan(const Symbolic &S, Plan &P) {
           for (int r0 = c1; r0 < m; r0 += kTrsmRows)
             P.panelTasks.push_back({s, c0, r0, std::min(r0 + kTrsmRows, m), g, nch});
         }
-        // trailing update restricted to the remaining pivot columns [c1, nc): rows [c1, m) x cols [c1, nc)
-        const double w = c1 - c0, r = m - c1, pc = nc - c1;
+        // Pivot blocks are grouped by kGroup: after block b of group [g0, g1) only the group's remaining columns are
+        // updated (narrow, K = 64); after the group's last block the pivot columns right of the group receive the
+        // whole group at once (wide, K = g1 - g0). The update block waits for the long-K pass after the level.
+        const int g0 = (c0 / (kGroup * kPanel)) * (kGroup * kPanel), g1 = std::min(nc, g0 + kGroup * kPanel);
+        const double w = c1 - c0, r = m - c1;
         sr.panelFlops += w * w * w / 3.0 + r * w * w;  // POTRF + TRSM
-        sr.updateFlops += w * pc * (2 * r - pc + 1);    // 2 flops per lower entry of the trapezoid per pivot column
-        for (int j0 = c1; j0 < nc; j0 += kTile)
-          for (int i0 = c1 + ((j0 - c1) / kTileM) * kTileM; i0 < m; i0 += kTileM)
-            P.tileTasks.push_back({(long long)P.snLxp[s], (long long)P.snUoff[s], m, nc, c0, c1 - c0, i0, j0, nc, 0});
+        auto trap = [m](double a, double b) { return (b - a) * m - (a + b - 1) * (b - a) / 2; };  // lower entries
+        if (c1 < g1) {
+          sr.updateFlops += 2 * w * trap(c1, g1);
+          for (int j0 = c1; j0 < g1; j0 += kTile)
+            for (int i0 = c1 + ((j0 - c1) / kTileM) * kTileM; i0 < m; i0 += kTileM)
+              P.tileTasks.push_back({(long long)P.snLxp[s], (long long)P.snUoff[s], m, nc, c0, c1 - c0, i0, j0, g1, 0});
+        } else if (g1 < nc) {
+          sr.updateFlops += 2.0 * (g1 - g0) * trap(g1, nc);
+          for (int j0 = g1; j0 < nc; j0 += kTile)
+            for (int i0 = g1 + ((j0 - g1) / kTileM) * kTileM; i0 < m; i0 += kTileM)
+              P.tileTasks.push_back({(long long)P.snLxp[s], (long long)P.snUoff[s], m, nc, g0, g1 - g0, i0, j0, nc, 0});
+        }
       }
       sr.panel1 = (int64_t)P.panelTasks.size();
       sr.tile1 = (int64_t)P.tileTasks.size();

@@ -18,6 +18,7 @@
 namespace amp {
 
 constexpr int kPanel = 64;     // pivot block width of the dense partial factorization
+constexpr int kGroup = 4;      // pivot blocks whose update of the columns right of them is applied together
 constexpr int kTile = 64;      // trailing-update tile columns
 constexpr int kTileM = 128;    // trailing-update tile rows
 constexpr int kAsmCols = 32;   // front columns per assembly task
