@@ -1,5 +1,6 @@
 // C ABI of libampsolve.so (include/ampsolve.h): plan / factor handles, device memory, and the orchestration of the
 // kernels on one CUDA stream per factor.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -83,6 +84,7 @@ struct amp_plan_s {
   amp::AsmTask *dAsm = nullptr;
   amp::PanelTask *dPanel = nullptr;
   amp::TileTask *dTile = nullptr, *dUTile = nullptr;
+  amp::MixTask *dMixTile = nullptr, *dMixU = nullptr;
   int4 *dFwdTasks = nullptr, *dBwdTasks = nullptr;
   int *dBlkOff = nullptr;
   int *dRowptr = nullptr, *dColidx = nullptr;
@@ -98,6 +100,8 @@ struct amp_factor_s {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   DevMem mem;
   double *dLx = nullptr, *dU = nullptr, *dD = nullptr, *dValues = nullptr;
+  float *dL32 = nullptr, *dU32 = nullptr;           // mixed precision: FP32 factor and update arena
+  __nv_bfloat16 *dShi = nullptr, *dSlo = nullptr;   // BF16 split columns of the factored pivot blocks
   unsigned long long *dStatus = nullptr;
   int *dReaders = nullptr;  // per pivot block: row chunks that have read it (reset at every factorization)
   bool ok = false, hasValues = false;
@@ -149,6 +153,7 @@ void upload_plan(amp_plan *pl) {
   d.snLxp = m.upload(P.snLxp);
   d.snUoff = m.upload(P.snUoff);
   d.snTOff = m.upload(P.snTOff);
+  d.snSp = m.upload(P.snSp);
   d.chPtr = m.upload(P.chPtr);
   d.chList = m.upload(P.chList);
   d.asmColPtr = m.upload(P.asmColPtr);
@@ -164,6 +169,8 @@ void upload_plan(amp_plan *pl) {
   pl->dPanel = m.upload(P.panelTasks);
   pl->dTile = m.upload(P.tileTasks);
   pl->dUTile = m.upload(P.uTasks);
+  pl->dMixTile = m.upload(P.mixTiles);
+  pl->dMixU = m.upload(P.mixUTasks);
   pl->dFwdTasks = (int4 *)m.upload(P.fwdTasks);
   pl->dBwdTasks = (int4 *)m.upload(P.bwdTasks);
   pl->dBlkOff = m.upload(P.blkOff);
@@ -218,15 +225,44 @@ void enqueue_factor(amp_factor *f) {
   cudaStream_t st = f->stream;
   ck(cudaMemsetAsync(f->dStatus, 0xff, sizeof(unsigned long long), st), "memset status");
   if (P.panelGroups) ck(cudaMemsetAsync(f->dReaders, 0, sizeof(int) * P.panelGroups, st), "memset readers");
+  if (f->precision == AMP_MIXED) {
+    for (int L = 0; L < P.nlevels; L++) {
+      timed(f, K_ASSEMBLE, 0.0, P.asmLvlBytes[L] / 2, [&] {
+        amp::launch_assemble<float>(f->plan->dAsm + P.asmLvlPtr[L], P.asmLvlPtr[L + 1] - P.asmLvlPtr[L], dp,
+                                    f->dValues, f->dL32, f->dU32, f->dStatus, st);
+      });
+      for (int k = P.lvlStepPtr[L]; k < P.lvlStepPtr[L + 1]; k++) {
+        const amp::StepRange &sr = P.steps[k];
+        timed(f, K_PANEL, sr.panelFlops, 0.0, [&] {
+          amp::launch_panel<float>(f->plan->dPanel + sr.panel0, sr.panel1 - sr.panel0, dp, f->dL32, f->dReaders,
+                                   f->dStatus, f->dShi, f->dSlo, st);
+        });
+        const int64_t t0 = P.mixStepPtr[k], t1 = P.mixStepPtr[k + 1];
+        if (t1 > t0)
+          timed(f, K_UPDATE, sr.updateFlops, 0.0, [&] {
+            amp::launch_update_mx(f->plan->dMixTile + t0, t1 - t0, f->dL32, f->dU32, f->dShi, f->dSlo, f->dStatus,
+                                  amp::num_sms(), st);
+          });
+      }
+      const int64_t u0 = P.mixULvlPtr[L], u1 = P.mixULvlPtr[L + 1];
+      if (u1 > u0)
+        timed(f, K_UPDATE, P.uLvlFlops[L], 0.0, [&] {
+          amp::launch_update_mx(f->plan->dMixU + u0, u1 - u0, f->dL32, f->dU32, f->dShi, f->dSlo, f->dStatus,
+                                amp::num_sms(), st);
+        });
+    }
+    return;
+  }
   for (int L = 0; L < P.nlevels; L++) {
     timed(f, K_ASSEMBLE, 0.0, P.asmLvlBytes[L], [&] {
-      amp::launch_assemble(f->plan->dAsm + P.asmLvlPtr[L], P.asmLvlPtr[L + 1] - P.asmLvlPtr[L], dp, f->dValues, f->dLx,
-                           f->dU, f->dStatus, st);
+      amp::launch_assemble<double>(f->plan->dAsm + P.asmLvlPtr[L], P.asmLvlPtr[L + 1] - P.asmLvlPtr[L], dp,
+                                   f->dValues, f->dLx, f->dU, f->dStatus, st);
     });
     for (int k = P.lvlStepPtr[L]; k < P.lvlStepPtr[L + 1]; k++) {
       const amp::StepRange &sr = P.steps[k];
       timed(f, K_PANEL, sr.panelFlops, 0.0, [&] {
-        amp::launch_panel(f->plan->dPanel + sr.panel0, sr.panel1 - sr.panel0, dp, f->dLx, f->dReaders, f->dStatus, st);
+        amp::launch_panel<double>(f->plan->dPanel + sr.panel0, sr.panel1 - sr.panel0, dp, f->dLx, f->dReaders,
+                                  f->dStatus, nullptr, nullptr, st);
       });
       if (sr.tile1 > sr.tile0)
         timed(f, K_UPDATE, sr.updateFlops, 0.0, [&] {
@@ -246,7 +282,7 @@ void device_solve_permuted(amp_factor *f, int q) {
   const amp::Plan &P = f->plan->P;
   const amp::DevPlan &dp = f->plan->dp;
   const int64_t Vs = P.nsuper ? P.Sp[P.nsuper] : 0, Ts = P.solveBufDoubles;
-  const double lbytes = 8.0 * (double)P.nnzLStored * q;  // each sweep reads L once per right-hand side
+  const double lbytes = (f->dL32 ? 4.0 : 8.0) * (double)P.nnzLStored * q;  // each sweep reads L once per RHS
   cudaStream_t st = f->stream;
   ck(cudaMemsetAsync(f->dTickets, 0, sizeof(int) * 2 * P.nlevels, st), "memset tickets");
   ck(cudaMemsetAsync(f->dSolveStatus, 0xff, sizeof(unsigned long long), st), "memset status");
@@ -258,16 +294,26 @@ void device_solve_permuted(amp_factor *f, int q) {
       amp::launch_fwd_gather(dp.lvlSn + P.lvlPtr[L], cnt, dp, f->dY, f->dV, f->dT, q, Vs, Ts, st);
     });
     timed(f, K_FORWARD, 0.0, lvlBytes, [&] {
-      amp::launch_fwd_blocks(f->plan->dFwdTasks + P.fwdLvlPtr[L], P.fwdLvlPtr[L + 1] - P.fwdLvlPtr[L],
-                             f->dTickets + L, dp, f->plan->dBlkOff, f->dLx, f->dY, f->dV, f->dT, f->dFlags, efwd, q,
-                             Vs, Ts, f->dSolveStatus, st);
+      if (f->dL32)
+        amp::launch_fwd_blocks<float>(f->plan->dFwdTasks + P.fwdLvlPtr[L], P.fwdLvlPtr[L + 1] - P.fwdLvlPtr[L],
+                                      f->dTickets + L, dp, f->plan->dBlkOff, f->dL32, f->dY, f->dV, f->dT, f->dFlags,
+                                      efwd, q, Vs, Ts, f->dSolveStatus, st);
+      else
+        amp::launch_fwd_blocks<double>(f->plan->dFwdTasks + P.fwdLvlPtr[L], P.fwdLvlPtr[L + 1] - P.fwdLvlPtr[L],
+                                       f->dTickets + L, dp, f->plan->dBlkOff, f->dLx, f->dY, f->dV, f->dT, f->dFlags,
+                                       efwd, q, Vs, Ts, f->dSolveStatus, st);
     });
   }
   for (int L = P.nlevels - 1; L >= 0; L--)
     timed(f, K_BACKWARD, 0.0, lbytes / P.nlevels, [&] {
-      amp::launch_bwd_blocks(f->plan->dBwdTasks + P.bwdLvlPtr[L], P.bwdLvlPtr[L + 1] - P.bwdLvlPtr[L],
-                             f->dTickets + P.nlevels + L, dp, f->plan->dBlkOff, f->dLx, f->dY, f->dFlags, ebwd, q,
-                             f->dSolveStatus, st);
+      if (f->dL32)
+        amp::launch_bwd_blocks<float>(f->plan->dBwdTasks + P.bwdLvlPtr[L], P.bwdLvlPtr[L + 1] - P.bwdLvlPtr[L],
+                                      f->dTickets + P.nlevels + L, dp, f->plan->dBlkOff, f->dL32, f->dY, f->dFlags,
+                                      ebwd, q, f->dSolveStatus, st);
+      else
+        amp::launch_bwd_blocks<double>(f->plan->dBwdTasks + P.bwdLvlPtr[L], P.bwdLvlPtr[L + 1] - P.bwdLvlPtr[L],
+                                       f->dTickets + P.nlevels + L, dp, f->plan->dBlkOff, f->dLx, f->dY, f->dFlags,
+                                       ebwd, q, f->dSolveStatus, st);
     });
 }
 
@@ -467,7 +513,7 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
     amp_factor_opts o{AMP_CHOLESKY, AMP_FP64};
     if (opts) o = *opts;
     if (o.kind != AMP_CHOLESKY) return fail(AMP_INVALID, "factor kind not available in this build");
-    if (o.precision != AMP_FP64) return fail(AMP_INVALID, "precision not available in this build");
+    if (o.precision != AMP_FP64 && o.precision != AMP_MIXED) return fail(AMP_INVALID, "unknown precision");
     ck(cudaSetDevice(pl->device), "cudaSetDevice");
     if (!pl->uploaded) {  // the device schedule is uploaded once, by the first factor of the plan
       upload_plan(pl);
@@ -484,8 +530,15 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
       ck(cudaEventCreate(&f->ev0), "cudaEventCreate");
       ck(cudaEventCreate(&f->ev1), "cudaEventCreate");
       const amp::Plan &P = pl->P;
-      f->dLx = f->mem.alloc<double>((size_t)P.nnzLStored);
-      f->dU = f->mem.alloc<double>((size_t)P.arenaDoubles);
+      if (o.precision == AMP_FP64) {
+        f->dLx = f->mem.alloc<double>((size_t)P.nnzLStored);
+        f->dU = f->mem.alloc<double>((size_t)P.arenaDoubles);
+      } else {
+        f->dL32 = f->mem.alloc<float>((size_t)P.nnzLStored);
+        f->dU32 = f->mem.alloc<float>((size_t)P.arenaDoubles);
+        f->dShi = f->mem.alloc<__nv_bfloat16>((size_t)P.splitElems);
+        f->dSlo = f->mem.alloc<__nv_bfloat16>((size_t)P.splitElems);
+      }
       f->dD = f->mem.alloc<double>((size_t)P.n);
       f->dValues = f->mem.alloc<double>((size_t)P.patNnz);
       f->dStatus = f->mem.alloc<unsigned long long>(1);
@@ -657,7 +710,13 @@ int amp_factor_download(const amp_factor *f, double *Lx, double *D) {
     if (!f) return fail(AMP_INVALID, "null handle");
     const amp::Plan &P = f->plan->P;
     ck(cudaSetDevice(f->plan->device), "cudaSetDevice");
-    if (Lx && P.nnzLStored) ck(cudaMemcpy(Lx, f->dLx, sizeof(double) * P.nnzLStored, cudaMemcpyDeviceToHost), "copy Lx");
+    if (Lx && P.nnzLStored && f->dLx)
+      ck(cudaMemcpy(Lx, f->dLx, sizeof(double) * P.nnzLStored, cudaMemcpyDeviceToHost), "copy Lx");
+    if (Lx && P.nnzLStored && f->dL32) {
+      std::vector<float> tmp(P.nnzLStored);
+      ck(cudaMemcpy(tmp.data(), f->dL32, sizeof(float) * P.nnzLStored, cudaMemcpyDeviceToHost), "copy Lx");
+      for (int64_t i = 0; i < P.nnzLStored; i++) Lx[i] = tmp[i];
+    }
     if (D && P.n) ck(cudaMemcpy(D, f->dD, sizeof(double) * P.n, cudaMemcpyDeviceToHost), "copy D");
     return (int)AMP_OK;
   });

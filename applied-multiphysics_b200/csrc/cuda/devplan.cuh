@@ -7,7 +7,7 @@ namespace amp {
 struct DevPlan {
   int n, nsuper, maxFront;
   const int *snF, *snNc, *snM, *snParent;
-  const int64_t *snLxp, *snUoff, *snTOff;
+  const int64_t *snLxp, *snUoff, *snTOff, *snSp;
   const int *chPtr, *chList;
   const int *asmColPtr, *asmDst, *asmSrc;
   const int64_t *eaPtr;

@@ -11,6 +11,7 @@
 //               covering both the remaining pivot columns (in Lx) and the update block (in the U arena).
 // The solves run the multifrontal vector form: forward per level bottom-up (each supernode passes one update vector
 // of length mu to its parent, no atomics), backward per level top-down gathering ancestor values.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -21,7 +22,8 @@
 
 namespace amp {
 
-__device__ __forceinline__ double *front_addr(double *Lp, double *Up, int m, int nc, int i, int j) {
+template <class T>
+__device__ __forceinline__ T *front_addr(T *Lp, T *Up, int m, int nc, int i, int j) {
   // front entry (i, j), i >= j: first nc columns in the L panel (ld m), the rest in the U block (ld mu)
   return j < nc ? Lp + (int64_t)j * m + i : Up + (int64_t)(j - nc) * (m - nc) + (i - nc);
 }
@@ -48,25 +50,26 @@ __device__ __forceinline__ bool failed(const unsigned long long *st) {
 // ---------------------------------------------------------------------------------------------------------------
 // Assembly + extend-add
 // ---------------------------------------------------------------------------------------------------------------
+template <class T>
 __global__ void __launch_bounds__(256) k_assemble(const AsmTask *__restrict__ tasks, DevPlan P,
-                                                  const double *__restrict__ values, double *__restrict__ Lx,
-                                                  double *__restrict__ U, const unsigned long long *status) {
+                                                  const double *__restrict__ values, T *__restrict__ Lx,
+                                                  T *__restrict__ U, const unsigned long long *status) {
   if (failed(status)) return;
   const AsmTask t = tasks[blockIdx.x];
   const int s = t.s, j0 = t.j0;
   const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
   const int jend = min(j0 + kAsmCols, m);
-  double *Lp = Lx + P.snLxp[s];
-  double *Up = (m > nc) ? U + P.snUoff[s] : nullptr;
+  T *Lp = Lx + P.snLxp[s];
+  T *Up = (m > nc) ? U + P.snUoff[s] : nullptr;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   // 1. zero the lower part of the owned columns
   for (int j = j0 + warp; j < jend; j += nwarps)
-    for (int i = j + lane; i < m; i += 32) *front_addr(Lp, Up, m, nc, i, j) = 0.0;
+    for (int i = j + lane; i < m; i += 32) *front_addr(Lp, Up, m, nc, i, j) = T(0);
   __syncthreads();
   // 2. A's entries of the owned pivot columns (each (row, col) once)
   for (int j = j0 + warp; j < min(jend, nc); j += nwarps) {
     const int p0 = P.asmColPtr[f + j], p1 = P.asmColPtr[f + j + 1];
-    for (int p = p0 + lane; p < p1; p += 32) Lp[P.asmDst[p]] += values[P.asmSrc[p]];
+    for (int p = p0 + lane; p < p1; p += 32) Lp[P.asmDst[p]] += (T)values[P.asmSrc[p]];
   }
   __syncthreads();
   // 3. children, one after another (stack order of the reference)
@@ -75,7 +78,7 @@ __global__ void __launch_bounds__(256) k_assemble(const AsmTask *__restrict__ ta
     const int muc = P.snM[c] - P.snNc[c];
     if (muc <= 0) continue;
     const int *map = P.eaMap + P.eaPtr[c];
-    const double *Uc = U + P.snUoff[c];
+    const T *Uc = U + P.snUoff[c];
     // child columns b mapping into [j0, jend): map is increasing
     int lo = 0, hi = muc;
     while (lo < hi) {
@@ -91,7 +94,7 @@ __global__ void __launch_bounds__(256) k_assemble(const AsmTask *__restrict__ ta
     const int b1 = lo;
     for (int b = b0 + warp; b < b1; b += nwarps) {
       const int jj = map[b];
-      const double *col = Uc + (int64_t)b * muc;
+      const T *col = Uc + (int64_t)b * muc;
       for (int a = b + lane; a < muc; a += 32) *front_addr(Lp, Up, m, nc, map[a], jj) += col[a];
     }
     __syncthreads();
@@ -101,25 +104,33 @@ __global__ void __launch_bounds__(256) k_assemble(const AsmTask *__restrict__ ta
 // ---------------------------------------------------------------------------------------------------------------
 // Panel: POTRF of the pivot block + TRSM of a chunk of rows below it
 // ---------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ double recip_t(double d) { return recip_nr(d); }
+__device__ __forceinline__ float recip_t(float d) { return __frcp_rn(d); }
+
+// T = double: the FP64 factor. T = float: the mixed-precision factor; the solved panel rows are also written as BF16
+// hi / lo pairs (hi = bf16(x), lo = bf16(x - hi)) into the split columns read by the tensor-core updates.
+template <class T>
 __global__ void __launch_bounds__(256, 1) k_panel(const PanelTask *__restrict__ tasks, DevPlan P,
-                                                  double *__restrict__ Lx, int *__restrict__ readers,
-                                                  unsigned long long *status) {
+                                                  T *__restrict__ Lx, int *__restrict__ readers,
+                                                  unsigned long long *status, __nv_bfloat16 *__restrict__ Shi,
+                                                  __nv_bfloat16 *__restrict__ Slo) {
   if (failed(status)) return;
   const PanelTask t = tasks[blockIdx.x];
   const int s = t.s, c0 = t.c0;
   const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
   const int w = min(kPanel, nc - c0);
-  double *Lp = Lx + P.snLxp[s];
-  __shared__ double D[kPanel][kPanel + 1];
-  __shared__ double invd[kPanel], ivsq[kPanel + 1], pd[kPanel + 1], piv[kPanel];
+  T *Lp = Lx + P.snLxp[s];
+  __shared__ T D[kPanel][kPanel + 1];
+  __shared__ T invd[kPanel], ivsq[kPanel + 1], pd[kPanel + 1], piv[kPanel];
   __shared__ unsigned short trail[kPanel * (kPanel - 1) / 2];  // (i, j) of the trailing entries, rightmost column first
-  extern __shared__ double xs[];  // kPanel x 256 staged solutions of the TRSM
+  extern __shared__ __align__(16) unsigned char xs_raw[];
+  T *xs = reinterpret_cast<T *>(xs_raw);  // kPanel x 256 staged solutions of the TRSM
   __shared__ int fail, lastReader;
   const int tid = threadIdx.x;
   // the pivot block (lower part); columns w .. 63 of a short last block are padded with the identity
   for (int e = tid; e < kPanel * kPanel; e += blockDim.x) {
     const int i = e & (kPanel - 1), j = e >> 6;
-    if (i >= j) D[i][j] = (i < w) ? Lp[(int64_t)(c0 + j) * m + (c0 + i)] : (i == j ? 1.0 : 0.0);
+    if (i >= j) D[i][j] = (i < w) ? Lp[(int64_t)(c0 + j) * m + (c0 + i)] : (i == j ? T(1) : T(0));
   }
   // trailing-entry list: columns 63, 62, ..., 1, rows j .. 63 within each
   for (int j = kPanel - 1 - (tid >> 6) ; j >= 1; j -= 4) {
@@ -133,10 +144,10 @@ __global__ void __launch_bounds__(256, 1) k_panel(const PanelTask *__restrict__ 
     __threadfence();
     lastReader = atomicAdd(readers + t.group, 1) == t.nchunks - 1;
     fail = -1;
-    const double d = D[0][0];
-    if (!(d > 0.0)) fail = 0;
+    const T d = D[0][0];
+    if (!(d > T(0))) fail = 0;
     pd[0] = d;
-    ivsq[0] = recip_nr(d);
+    ivsq[0] = recip_t(d);
   }
   __syncthreads();
   // POTRF, right-looking on the unscaled columns: step k subtracts D[i][k] D[j][k] / d_k from the trailing entries
@@ -145,17 +156,17 @@ __global__ void __launch_bounds__(256, 1) k_panel(const PanelTask *__restrict__ 
   // on the column-to-column critical path). The columns are scaled to L once, after the loop.
   for (int k = 0; k < w; k++) {
     if (fail >= 0) break;  // uniform: written before the barrier that ended the previous step
-    const double iv2 = ivsq[k];
+    const T iv2 = ivsq[k];
     const int nk = kPanel - 1 - k;     // trailing columns k+1 .. 63
     const int Tk = nk * (nk + 1) / 2;  // trailing lower entries
     for (int e = tid; e < Tk; e += blockDim.x) {
       const int ij = trail[e], i = ij & 0xff, j = ij >> 8;
-      const double v = D[i][j] - (D[i][k] * D[j][k]) * iv2;
+      const T v = D[i][j] - (D[i][k] * D[j][k]) * iv2;
       D[i][j] = v;
       if (i == k + 1 && j == k + 1) {  // the next pivot is final now
-        if (!(v > 0.0) && k + 1 < w) fail = k + 1;
+        if (!(v > T(0)) && k + 1 < w) fail = k + 1;
         pd[k + 1] = v;
-        ivsq[k + 1] = recip_nr(v);
+        ivsq[k + 1] = recip_t(v);
       }
     }
     __syncthreads();
@@ -163,10 +174,10 @@ __global__ void __launch_bounds__(256, 1) k_panel(const PanelTask *__restrict__ 
   if (fail < 0) {
     // L = D diag(d)^-1/2: one square root and reciprocal per column, then every entry scaled once
     if (tid < kPanel) {
-      const double d = tid < w ? pd[tid] : 1.0;
-      const double lk = sqrt(d);
+      const T d = tid < w ? pd[tid] : T(1);
+      const T lk = sqrt(d);
       piv[tid] = lk;
-      invd[tid] = 1.0 / lk;
+      invd[tid] = T(1) / lk;
     }
     __syncthreads();
     for (int e = tid; e < kPanel * kPanel; e += blockDim.x) {
@@ -191,14 +202,14 @@ __global__ void __launch_bounds__(256, 1) k_panel(const PanelTask *__restrict__ 
   const int r = t.r0 + tid;
   if (r >= t.r1) return;
   constexpr int Q = 16;
-  double x[Q];
+  T x[Q];
 #pragma unroll 1
   for (int q0 = 0; q0 < w; q0 += Q) {
 #pragma unroll
-    for (int c = 0; c < Q; c++) x[c] = (q0 + c < w) ? Lp[(int64_t)(c0 + q0 + c) * m + r] : 0.0;
+    for (int c = 0; c < Q; c++) x[c] = (q0 + c < w) ? Lp[(int64_t)(c0 + q0 + c) * m + r] : T(0);
 #pragma unroll 1
     for (int k = 0; k < q0; k++) {
-      const double xk = xs[k * 256 + tid];
+      const T xk = xs[k * 256 + tid];
 #pragma unroll
       for (int c = 0; c < Q; c++) x[c] -= xk * D[q0 + c][k];
     }
@@ -210,7 +221,15 @@ __global__ void __launch_bounds__(256, 1) k_panel(const PanelTask *__restrict__ 
     }
 #pragma unroll
     for (int c = 0; c < Q; c++) {
-      if (q0 + c < w) Lp[(int64_t)(c0 + q0 + c) * m + r] = x[c];
+      if (q0 + c < w) {
+        Lp[(int64_t)(c0 + q0 + c) * m + r] = x[c];
+        if (Shi) {
+          const int64_t g = P.snSp[s] + (int64_t)(c0 + q0 + c) * ((m + 7) & ~7) + r;
+          const __nv_bfloat16 hi = __float2bfloat16_rn((float)x[c]);
+          Shi[g] = hi;
+          Slo[g] = __float2bfloat16_rn((float)x[c] - __bfloat162float(hi));
+        }
+      }
       xs[(q0 + c) * 256 + tid] = x[c];
     }
   }
@@ -468,22 +487,37 @@ __global__ void __launch_bounds__(256) k_backward(const int *__restrict__ sns, D
 // ---------------------------------------------------------------------------------------------------------------
 static int g_num_sms = 148;
 constexpr int kPanelSmem = kPanel * 256 * (int)sizeof(double);
+void init_mixed_attributes();
 void init_kernel_attributes() {
-  cudaFuncSetAttribute(k_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmem);
+  cudaFuncSetAttribute(k_panel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmem);
+  cudaFuncSetAttribute(k_panel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmem / 2);
+  init_mixed_attributes();
   cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, kUpdateSmem);
   int dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
 }
 
-void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, const double *values, double *Lx,
-                     double *U, const unsigned long long *status, cudaStream_t st) {
-  if (ntasks > 0) k_assemble<<<(unsigned)ntasks, 256, 0, st>>>(tasks, P, values, Lx, U, status);
+template <class T>
+void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, const double *values, T *Lx, T *U,
+                     const unsigned long long *status, cudaStream_t st) {
+  if (ntasks > 0) k_assemble<T><<<(unsigned)ntasks, 256, 0, st>>>(tasks, P, values, Lx, U, status);
 }
-void launch_panel(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, int *readers,
-                  unsigned long long *status, cudaStream_t st) {
-  if (ntasks > 0) k_panel<<<(unsigned)ntasks, 256, kPanelSmem, st>>>(tasks, P, Lx, readers, status);
+template void launch_assemble<double>(const AsmTask *, int64_t, const DevPlan &, const double *, double *, double *,
+                                      const unsigned long long *, cudaStream_t);
+template void launch_assemble<float>(const AsmTask *, int64_t, const DevPlan &, const double *, float *, float *,
+                                     const unsigned long long *, cudaStream_t);
+template <class T>
+void launch_panel(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, T *Lx, int *readers,
+                  unsigned long long *status, __nv_bfloat16 *Shi, __nv_bfloat16 *Slo, cudaStream_t st) {
+  if (ntasks > 0)
+    k_panel<T><<<(unsigned)ntasks, 256, kPanel * 256 * (int)sizeof(T), st>>>(tasks, P, Lx, readers, status, Shi, Slo);
 }
+template void launch_panel<double>(const PanelTask *, int64_t, const DevPlan &, double *, int *, unsigned long long *,
+                                   __nv_bfloat16 *, __nv_bfloat16 *, cudaStream_t);
+template void launch_panel<float>(const PanelTask *, int64_t, const DevPlan &, float *, int *, unsigned long long *,
+                                  __nv_bfloat16 *, __nv_bfloat16 *, cudaStream_t);
+int num_sms() { return g_num_sms; }
 void launch_update(const TileTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, double *U,
                    const unsigned long long *status, cudaStream_t st) {
   (void)P;

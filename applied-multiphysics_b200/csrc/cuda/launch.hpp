@@ -1,5 +1,6 @@
 // Host-callable launchers of the device kernels.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -11,10 +12,15 @@ namespace amp {
 
 void init_kernel_attributes();  // once per process and device, before the first launch
 
-void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, const double *values, double *Lx,
-                     double *U, const unsigned long long *status, cudaStream_t st);
-void launch_panel(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, int *readers,
-                  unsigned long long *status, cudaStream_t st);
+template <class T>
+void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, const double *values, T *Lx, T *U,
+                     const unsigned long long *status, cudaStream_t st);
+template <class T>
+void launch_panel(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, T *Lx, int *readers,
+                  unsigned long long *status, __nv_bfloat16 *Shi, __nv_bfloat16 *Slo, cudaStream_t st);
+void launch_update_mx(const MixTask *tasks, int64_t ntasks, float *L32, float *U32, const __nv_bfloat16 *Shi,
+                      const __nv_bfloat16 *Slo, unsigned long long *status, int num_sms, cudaStream_t st);
+int num_sms();
 void launch_update(const TileTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, double *U,
                    const unsigned long long *status, cudaStream_t st);
 void launch_permute_in(const double *b, double *y, const int *perm, int n, int q, cudaStream_t st);
@@ -24,11 +30,13 @@ void launch_forward(const int *sns, int count, const DevPlan &P, const double *L
 void launch_backward(const int *sns, int count, const DevPlan &P, const double *Lx, double *y, int q, cudaStream_t st);
 void launch_fwd_gather(const int *sns, int count, const DevPlan &P, const double *y, double *V, const double *T, int q,
                        int64_t Vstride, int64_t Tstride, cudaStream_t st);
+template <class TL>
 void launch_fwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const int *blkOff,
-                       const double *Lx, double *y, const double *V, double *T, int *flags, int epoch, int q,
+                       const TL *Lx, double *y, const double *V, double *T, int *flags, int epoch, int q,
                        int64_t Vstride, int64_t Tstride, unsigned long long *status, cudaStream_t st);
+template <class TL>
 void launch_bwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const int *blkOff,
-                       const double *Lx, double *y, int *flags, int epoch, int q, unsigned long long *status,
+                       const TL *Lx, double *y, int *flags, int epoch, int q, unsigned long long *status,
                        cudaStream_t st);
 
 }  // namespace amp

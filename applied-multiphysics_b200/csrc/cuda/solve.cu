@@ -75,9 +75,10 @@ __global__ void __launch_bounds__(256) k_fwd_gather(const int *__restrict__ sns,
 
 // ---- forward block tasks -----------------------------------------------------------------------------------------
 // task: .x supernode, .y block, .z kind (0 diagonal, 1 below)
+template <class TL>
 __global__ void __launch_bounds__(256) k_fwd_blocks(const int4 *__restrict__ tasks, int ntasks, int *__restrict__ ticket,
                                                     DevPlan P, const int *__restrict__ blkOff,
-                                                    const double *__restrict__ Lx, double *__restrict__ y,
+                                                    const TL *__restrict__ Lx, double *__restrict__ y,
                                                     const double *__restrict__ V, double *__restrict__ T,
                                                     int *__restrict__ flags, int epoch, int q, int64_t Vstride,
                                                     int64_t Tstride, unsigned long long *status) {
@@ -90,7 +91,7 @@ __global__ void __launch_bounds__(256) k_fwd_blocks(const int4 *__restrict__ tas
   const int4 t = tasks[tk];
   const int s = t.x, blk = t.y, below = t.z;
   const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s], mu = m - nc;
-  const double *Lp = Lx + P.snLxp[s];
+  const TL *Lp = Lx + P.snLxp[s];
   const int r0 = below ? nc + blk * kSB : blk * kSB;
   const int rows = below ? min(kSB, mu - blk * kSB) : min(kSB, nc - blk * kSB);
   const int ncols = below ? nc : blk * kSB;  // columns of L to the left of the diagonal block / all pivot columns
@@ -108,7 +109,7 @@ __global__ void __launch_bounds__(256) k_fwd_blocks(const int4 *__restrict__ tas
       }
       const int c1 = min(ncols, (cb + 1) * kSB);
       if (row < rows)
-        for (int c = cb * kSB + part; c < c1; c += 4) acc += Lp[(int64_t)c * m + r0 + row] * __ldcg(yk + c);
+        for (int c = cb * kSB + part; c < c1; c += 4) acc += (double)Lp[(int64_t)c * m + r0 + row] * __ldcg(yk + c);
     }
     red[part][row] = acc;
     __syncthreads();
@@ -126,7 +127,7 @@ __global__ void __launch_bounds__(256) k_fwd_blocks(const int4 *__restrict__ tas
       if (k == 0) {
         for (int e = tid; e < rows * rows; e += blockDim.x) {
           int i = e % rows, j = e / rows;
-          if (i >= j) Lkk[i][j] = Lp[(int64_t)(r0 + j) * m + r0 + i];
+          if (i >= j) Lkk[i][j] = (double)Lp[(int64_t)(r0 + j) * m + r0 + i];
         }
         __syncthreads();
       }
@@ -156,9 +157,10 @@ __global__ void __launch_bounds__(256) k_fwd_blocks(const int4 *__restrict__ tas
 
 // ---- backward block tasks ----------------------------------------------------------------------------------------
 // task: .x supernode, .y column block (tasks of a supernode listed from the last block down)
+template <class TL>
 __global__ void __launch_bounds__(256) k_bwd_blocks(const int4 *__restrict__ tasks, int ntasks, int *__restrict__ ticket,
                                                     DevPlan P, const int *__restrict__ blkOff,
-                                                    const double *__restrict__ Lx, double *__restrict__ y,
+                                                    const TL *__restrict__ Lx, double *__restrict__ y,
                                                     int *__restrict__ flags, int epoch, int q,
                                                     unsigned long long *status) {
   __shared__ int tk, waitOk;
@@ -170,7 +172,7 @@ __global__ void __launch_bounds__(256) k_bwd_blocks(const int4 *__restrict__ tas
   const int4 t = tasks[tk];
   const int s = t.x, blk = t.y;
   const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
-  const double *Lp = Lx + P.snLxp[s];
+  const TL *Lp = Lx + P.snLxp[s];
   const int *rowsOf = P.Si + P.Sp[s];
   const int c0 = blk * kSB, w = min(kSB, nc - c0), nb = (nc + kSB - 1) / kSB;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -187,7 +189,7 @@ __global__ void __launch_bounds__(256) k_bwd_blocks(const int4 *__restrict__ tas
 #pragma unroll
       for (int u = 0; u < 8; u++) {
         const int c = warp + 8 * u;
-        if (c < w) acc[u] += Lp[(int64_t)(c0 + c) * m + r] * xr;
+        if (c < w) acc[u] += (double)Lp[(int64_t)(c0 + c) * m + r] * xr;
       }
     }
     // later pivot blocks of this supernode, as they become final
@@ -203,7 +205,7 @@ __global__ void __launch_bounds__(256) k_bwd_blocks(const int4 *__restrict__ tas
 #pragma unroll
         for (int u = 0; u < 8; u++) {
           const int c = warp + 8 * u;
-          if (c < w) acc[u] += Lp[(int64_t)(c0 + c) * m + r] * xr;
+          if (c < w) acc[u] += (double)Lp[(int64_t)(c0 + c) * m + r] * xr;
         }
       }
     }
@@ -217,7 +219,7 @@ __global__ void __launch_bounds__(256) k_bwd_blocks(const int4 *__restrict__ tas
     if (k == 0) {
       for (int e = tid; e < w * w; e += blockDim.x) {
         int i = e % w, j = e / w;
-        if (i >= j) Lkk[i][j] = Lp[(int64_t)(c0 + j) * m + c0 + i];
+        if (i >= j) Lkk[i][j] = (double)Lp[(int64_t)(c0 + j) * m + c0 + i];
       }
     }
     __syncthreads();
@@ -250,18 +252,30 @@ void launch_fwd_gather(const int *sns, int count, const DevPlan &P, const double
                        int64_t Vstride, int64_t Tstride, cudaStream_t st) {
   if (count > 0) k_fwd_gather<<<count, 256, 0, st>>>(sns, P, y, V, T, q, Vstride, Tstride);
 }
+template <class TL>
 void launch_fwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const int *blkOff,
-                       const double *Lx, double *y, const double *V, double *T, int *flags, int epoch, int q,
+                       const TL *Lx, double *y, const double *V, double *T, int *flags, int epoch, int q,
                        int64_t Vstride, int64_t Tstride, unsigned long long *status, cudaStream_t st) {
   if (ntasks > 0)
-    k_fwd_blocks<<<ntasks, 256, 0, st>>>(tasks, ntasks, ticket, P, blkOff, Lx, y, V, T, flags, epoch, q, Vstride,
-                                         Tstride, status);
+    k_fwd_blocks<TL><<<ntasks, 256, 0, st>>>(tasks, ntasks, ticket, P, blkOff, Lx, y, V, T, flags, epoch, q, Vstride,
+                                             Tstride, status);
 }
+template <class TL>
 void launch_bwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const int *blkOff,
-                       const double *Lx, double *y, int *flags, int epoch, int q, unsigned long long *status,
+                       const TL *Lx, double *y, int *flags, int epoch, int q, unsigned long long *status,
                        cudaStream_t st) {
   if (ntasks > 0)
-    k_bwd_blocks<<<ntasks, 256, 0, st>>>(tasks, ntasks, ticket, P, blkOff, Lx, y, flags, epoch, q, status);
+    k_bwd_blocks<TL><<<ntasks, 256, 0, st>>>(tasks, ntasks, ticket, P, blkOff, Lx, y, flags, epoch, q, status);
 }
+template void launch_fwd_blocks<double>(const int4 *, int, int *, const DevPlan &, const int *, const double *,
+                                        double *, const double *, double *, int *, int, int, int64_t, int64_t,
+                                        unsigned long long *, cudaStream_t);
+template void launch_fwd_blocks<float>(const int4 *, int, int *, const DevPlan &, const int *, const float *, double *,
+                                       const double *, double *, int *, int, int, int64_t, int64_t,
+                                       unsigned long long *, cudaStream_t);
+template void launch_bwd_blocks<double>(const int4 *, int, int *, const DevPlan &, const int *, const double *,
+                                        double *, int *, int, int, unsigned long long *, cudaStream_t);
+template void launch_bwd_blocks<float>(const int4 *, int, int *, const DevPlan &, const int *, const float *, double *,
+                                       int *, int, int, unsigned long long *, cudaStream_t);
 
 }  // namespace amp

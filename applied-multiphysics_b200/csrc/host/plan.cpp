@@ -162,6 +162,20 @@ void build_plan(const Symbolic &S, Plan &P) {
     }
     P.arenaDoubles = ar.peak();
   }
+  // BF16 split storage of the pivot columns (mixed precision): ld = round_up(m, 8), 16-byte aligned columns
+  P.snSp.assign(ns + 1, 0);
+  for (int s = 0; s < ns; s++) P.snSp[s + 1] = P.snSp[s] + (int64_t)((P.snM[s] + 7) & ~7) * P.snNc[s];
+  P.splitElems = P.snSp[ns];
+  // mixed-precision tiles (128 x 256, starts aligned down to 8, masked by ilo / jlo / jend) of a region
+  auto emitMix = [&](std::vector<MixTask> &out, int s, int rlo, int clo, int chi, int kc0, int kw) {
+    const int m = P.snM[s], nc = P.snNc[s];
+    for (int j0 = clo & ~7; j0 < chi; j0 += 256)
+      for (int i0 = std::max(rlo, j0) & ~7; i0 < m; i0 += 128)
+        out.push_back({(long long)P.snLxp[s], (long long)P.snUoff[s], (long long)P.snSp[s], m, nc, (m + 7) & ~7, kc0,
+                       kw, i0, j0, rlo, clo, chi, 0});
+  };
+  P.mixStepPtr.assign(1, 0);
+  P.mixULvlPtr.assign(1, 0);
   // task lists per level
   P.asmLvlPtr.assign(P.nlevels + 1, 0);
   P.asmLvlBytes.assign(P.nlevels, 0.0);
@@ -207,6 +221,10 @@ void build_plan(const Symbolic &S, Plan &P) {
         const double w = c1 - c0, r = m - c1;
         sr.panelFlops += w * w * w / 3.0 + r * w * w;  // POTRF + TRSM
         auto trap = [m](double a, double b) { return (b - a) * m - (a + b - 1) * (b - a) / 2; };  // lower entries
+        if (c1 < g1)
+          emitMix(P.mixTiles, s, c1, c1, g1, c0, c1 - c0);
+        else if (g1 < nc)
+          emitMix(P.mixTiles, s, g1, g1, nc, g0, g1 - g0);
         if (c1 < g1) {
           sr.updateFlops += 2 * w * trap(c1, g1);
           for (int j0 = c1; j0 < g1; j0 += kTile)
@@ -222,6 +240,7 @@ void build_plan(const Symbolic &S, Plan &P) {
       sr.panel1 = (int64_t)P.panelTasks.size();
       sr.tile1 = (int64_t)P.tileTasks.size();
       P.steps.push_back(sr);
+      P.mixStepPtr.push_back((int64_t)P.mixTiles.size());
     }
     P.lvlStepPtr[L + 1] = (int)P.steps.size();
     // update blocks of the level's fronts: one long-K pass each
@@ -235,7 +254,9 @@ void build_plan(const Symbolic &S, Plan &P) {
       for (int j0 = nc; j0 < m; j0 += kTile)
         for (int i0 = nc + ((j0 - nc) / kTileM) * kTileM; i0 < m; i0 += kTileM)
           P.uTasks.push_back({(long long)P.snLxp[s], (long long)P.snUoff[s], m, nc, 0, nc, i0, j0, m, 0});
+      emitMix(P.mixUTasks, s, nc, nc, m, 0, nc);
     }
+    P.mixULvlPtr.push_back((int64_t)P.mixUTasks.size());
     P.uLvlPtr.push_back((int64_t)P.uTasks.size());
     P.uLvlFlops.push_back(uf);
   }

@@ -33,6 +33,13 @@ struct TileTask {  // update tile: rows [i0, i0+128) x cols [j0, min(j0+64, jend
   long long lp, up;      // offsets of the front's L panel (Lx) and update block (U arena, -1 if none)
   int m, nc, c0, w, i0, j0, jend, pad;
 };
+struct MixTask {  // mixed-precision update tile (128 x 256, 8-aligned start) of a front with FP32 storage
+  long long lp, up, sp;      // FP32 L panel, FP32 update block (-1 if none), BF16 split columns (ld per front)
+  int m, nc, ld, c0, w;      // K = pivot columns [c0, c0 + w)
+  int i0, j0;                // tile origin (multiples of 8)
+  int ilo, jlo, jend;        // rows >= ilo, columns in [jlo, jend) are updated
+  int pad;
+};
 struct AsmTask {  // zero + assemble + extend-add front columns [j0, j0 + 32) of supernode s
   int s, j0;
 };
@@ -69,6 +76,11 @@ struct Plan {
   std::vector<TileTask> tileTasks;
   std::vector<int> lvlStepPtr;  // per level: steps [lvlStepPtr[L], lvlStepPtr[L+1])
   std::vector<TileTask> uTasks;  // long-K update-block tiles, per level [uLvlPtr[L], uLvlPtr[L+1])
+  // mixed precision: the same steps with 128 x 256 tiles; BF16 split storage of the pivot columns
+  std::vector<MixTask> mixTiles, mixUTasks;
+  std::vector<int64_t> mixStepPtr, mixULvlPtr;  // per step / per level
+  std::vector<int64_t> snSp;  // split-column offset of supernode s (ld = round_up(m, 8) per front)
+  int64_t splitElems = 0;
   std::vector<int64_t> uLvlPtr;
   std::vector<double> uLvlFlops;
   std::vector<StepRange> steps;
