@@ -85,7 +85,7 @@ struct amp_plan_s {
   amp::PanelTask *dPanel = nullptr;
   amp::TileTask *dTile = nullptr, *dUTile = nullptr;
   amp::MixTask *dMixTile = nullptr, *dMixU = nullptr;
-  int4 *dFwdTasks = nullptr, *dBwdTasks = nullptr;
+  int4 *dFwdTasks = nullptr, *dBwdTasks = nullptr, *dBwdAll = nullptr;
   int *dBlkOff = nullptr;
   int *dRowptr = nullptr, *dColidx = nullptr;
   std::vector<int> rowptr, colidx;  // host copy of the pattern (uploaded with the schedule)
@@ -123,6 +123,7 @@ struct amp_factor_s {
   double *dY = nullptr, *dV = nullptr, *dT = nullptr, *dB = nullptr, *dX = nullptr, *dR = nullptr, *dDX = nullptr,
          *dNorms = nullptr;
   int *dFlags = nullptr, *dTickets = nullptr;  // solve block ready flags (epoch-stamped) and per-launch tickets
+  int *dDone = nullptr;                         // forward: finished below tasks per supernode
   unsigned long long *dSolveStatus = nullptr;
   int solveEpoch = 0;
   ~amp_factor_s() {
@@ -173,6 +174,7 @@ void upload_plan(amp_plan *pl) {
   pl->dMixU = m.upload(P.mixUTasks);
   pl->dFwdTasks = (int4 *)m.upload(P.fwdTasks);
   pl->dBwdTasks = (int4 *)m.upload(P.bwdTasks);
+  pl->dBwdAll = (int4 *)m.upload(P.bwdAll);
   pl->dBlkOff = m.upload(P.blkOff);
 }
 
@@ -284,37 +286,27 @@ void device_solve_permuted(amp_factor *f, int q) {
   const int64_t Vs = P.nsuper ? P.Sp[P.nsuper] : 0, Ts = P.solveBufDoubles;
   const double lbytes = (f->dL32 ? 4.0 : 8.0) * (double)P.nnzLStored * q;  // each sweep reads L once per RHS
   cudaStream_t st = f->stream;
-  ck(cudaMemsetAsync(f->dTickets, 0, sizeof(int) * 2 * P.nlevels, st), "memset tickets");
+  ck(cudaMemsetAsync(f->dTickets, 0, sizeof(int) * 2, st), "memset tickets");
+  ck(cudaMemsetAsync(f->dDone, 0, sizeof(int) * std::max(1, P.nsuper), st), "memset done");
   ck(cudaMemsetAsync(f->dSolveStatus, 0xff, sizeof(unsigned long long), st), "memset status");
   const int efwd = 2 * (++f->solveEpoch) - 1, ebwd = 2 * f->solveEpoch;
-  for (int L = 0; L < P.nlevels; L++) {
-    const int cnt = P.lvlPtr[L + 1] - P.lvlPtr[L];
-    const double lvlBytes = lbytes / P.nlevels;
-    timed(f, K_FORWARD, 0.0, 0.0, [&] {
-      amp::launch_fwd_gather(dp.lvlSn + P.lvlPtr[L], cnt, dp, f->dY, f->dV, f->dT, q, Vs, Ts, st);
-    });
-    timed(f, K_FORWARD, 0.0, lvlBytes, [&] {
-      if (f->dL32)
-        amp::launch_fwd_blocks<float>(f->plan->dFwdTasks + P.fwdLvlPtr[L], P.fwdLvlPtr[L + 1] - P.fwdLvlPtr[L],
-                                      f->dTickets + L, dp, f->plan->dBlkOff, f->dL32, f->dY, f->dV, f->dT, f->dFlags,
-                                      efwd, q, Vs, Ts, f->dSolveStatus, st);
-      else
-        amp::launch_fwd_blocks<double>(f->plan->dFwdTasks + P.fwdLvlPtr[L], P.fwdLvlPtr[L + 1] - P.fwdLvlPtr[L],
-                                       f->dTickets + L, dp, f->plan->dBlkOff, f->dLx, f->dY, f->dV, f->dT, f->dFlags,
-                                       efwd, q, Vs, Ts, f->dSolveStatus, st);
-    });
-  }
-  for (int L = P.nlevels - 1; L >= 0; L--)
-    timed(f, K_BACKWARD, 0.0, lbytes / P.nlevels, [&] {
-      if (f->dL32)
-        amp::launch_bwd_blocks<float>(f->plan->dBwdTasks + P.bwdLvlPtr[L], P.bwdLvlPtr[L + 1] - P.bwdLvlPtr[L],
-                                      f->dTickets + P.nlevels + L, dp, f->plan->dBlkOff, f->dL32, f->dY, f->dFlags,
-                                      ebwd, q, f->dSolveStatus, st);
-      else
-        amp::launch_bwd_blocks<double>(f->plan->dBwdTasks + P.bwdLvlPtr[L], P.bwdLvlPtr[L + 1] - P.bwdLvlPtr[L],
-                                       f->dTickets + P.nlevels + L, dp, f->plan->dBlkOff, f->dLx, f->dY, f->dFlags,
-                                       ebwd, q, f->dSolveStatus, st);
-    });
+  const int nf = P.fwdLvlPtr[P.nlevels], nb = (int)(P.bwdAll.size() / 4);
+  timed(f, K_FORWARD, 0.0, lbytes, [&] {
+    if (f->dL32)
+      amp::launch_fwd_blocks<float>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->plan->dBlkOff, f->dL32, f->dY, f->dV,
+                                    f->dT, f->dFlags, efwd, f->dDone, q, Vs, Ts, f->dSolveStatus, st);
+    else
+      amp::launch_fwd_blocks<double>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->plan->dBlkOff, f->dLx, f->dY, f->dV,
+                                     f->dT, f->dFlags, efwd, f->dDone, q, Vs, Ts, f->dSolveStatus, st);
+  });
+  timed(f, K_BACKWARD, 0.0, lbytes, [&] {
+    if (f->dL32)
+      amp::launch_bwd_blocks<float>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->plan->dBlkOff, f->dL32, f->dY,
+                                    f->dFlags, ebwd, q, f->dSolveStatus, st);
+    else
+      amp::launch_bwd_blocks<double>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->plan->dBlkOff, f->dLx, f->dY,
+                                     f->dFlags, ebwd, q, f->dSolveStatus, st);
+  });
 }
 
 // AMP_DEVICE_TIMEOUT when a bounded wait of the last solve gave up (the stream must be synchronised)
@@ -545,7 +537,8 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
       f->dReaders = f->mem.alloc<int>((size_t)P.panelGroups);
       f->dFlags = f->mem.alloc<int>((size_t)P.nflags);
       ck(cudaMemset(f->dFlags, 0, sizeof(int) * std::max(1, P.nflags)), "memset flags");
-      f->dTickets = f->mem.alloc<int>(2 * (size_t)P.nlevels);
+      f->dTickets = f->mem.alloc<int>(2);
+      f->dDone = f->mem.alloc<int>((size_t)std::max(1, P.nsuper));
       f->dSolveStatus = f->mem.alloc<unsigned long long>(1);
       static bool attrs = false;
       if (!attrs) {

@@ -32,7 +32,7 @@ void launch_fwd_gather(const int *sns, int count, const DevPlan &P, const double
                        int64_t Vstride, int64_t Tstride, cudaStream_t st);
 template <class TL>
 void launch_fwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const int *blkOff,
-                       const TL *Lx, double *y, const double *V, double *T, int *flags, int epoch, int q,
+                       const TL *Lx, double *y, double *V, double *T, int *flags, int epoch, int *done, int q,
                        int64_t Vstride, int64_t Tstride, unsigned long long *status, cudaStream_t st);
 template <class TL>
 void launch_bwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const int *blkOff,

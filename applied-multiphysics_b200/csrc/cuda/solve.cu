@@ -48,6 +48,19 @@ __device__ bool wait_flag(const int *flag, int epoch, unsigned long long *status
   return true;
 }
 
+// Wait until *cnt == need; false on time-out (status set).
+__device__ bool wait_count(const int *cnt, int need, unsigned long long *status, int s) {
+  long long spins = 0;
+  while (ld_acquire(cnt) < need) {
+    if (++spins > kSpinLimit) {
+      atomicMin(status, status_word(0x7fffffff, 3, s));
+      return false;
+    }
+    __nanosleep(64);
+  }
+  return true;
+}
+
 // ---- forward gather ----------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_fwd_gather(const int *__restrict__ sns, DevPlan P, const double *__restrict__ y,
                                                     double *__restrict__ V, const double *__restrict__ T, int q,
@@ -75,13 +88,18 @@ __global__ void __launch_bounds__(256) k_fwd_gather(const int *__restrict__ sns,
 
 // ---- forward block tasks -----------------------------------------------------------------------------------------
 // task: .x supernode, .y block, .z kind (0 diagonal, 1 below)
+// One launch for the whole sweep: tasks are listed level by level (leaves first), so every wait below is on a task
+// with an earlier ticket. The first diagonal task of a supernode waits for its children's pass-up vectors (their
+// below tasks count themselves in done[]) and gathers its front vector; every below task counts itself when its
+// part of the pass-up vector is written.
 template <class TL>
 __global__ void __launch_bounds__(256) k_fwd_blocks(const int4 *__restrict__ tasks, int ntasks, int *__restrict__ ticket,
                                                     DevPlan P, const int *__restrict__ blkOff,
                                                     const TL *__restrict__ Lx, double *__restrict__ y,
-                                                    const double *__restrict__ V, double *__restrict__ T,
-                                                    int *__restrict__ flags, int epoch, int q, int64_t Vstride,
-                                                    int64_t Tstride, unsigned long long *status) {
+                                                    double *__restrict__ V, double *__restrict__ T,
+                                                    int *__restrict__ flags, int epoch, int *__restrict__ done,
+                                                    int q, int64_t Vstride, int64_t Tstride,
+                                                    unsigned long long *status) {
   __shared__ int tk, waitOk;
   __shared__ double red[4][kSB];
   __shared__ double Lkk[kSB][kSB + 1];
@@ -97,6 +115,34 @@ __global__ void __launch_bounds__(256) k_fwd_blocks(const int4 *__restrict__ tas
   const int ncols = below ? nc : blk * kSB;  // columns of L to the left of the diagonal block / all pivot columns
   const int tid = threadIdx.x, row = tid & (kSB - 1), part = tid >> 6;
   int *myflags = flags + blkOff[s];
+  if (!below && blk == 0) {
+    // children's pass-up vectors complete?
+    for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
+      const int c = P.chList[qq];
+      const int need = (P.snM[c] - P.snNc[c] + kSB - 1) / kSB;
+      if (tid == 0) waitOk = wait_count(done + c, need, status, s);
+      __syncthreads();
+      if (!waitOk) return;
+    }
+    // gather v_s = [y(f .. f + nc); 0] + children's pass-up vectors (the reference's child order)
+    for (int k = 0; k < q; k++) {
+      double *v = V + (int64_t)k * Vstride + P.Sp[s];
+      const double *yk = y + (int64_t)k * P.n;
+      for (int r = tid; r < m; r += blockDim.x) v[r] = r < nc ? yk[f + r] : 0.0;
+    }
+    __syncthreads();
+    for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
+      const int c = P.chList[qq];
+      const int muc = P.snM[c] - P.snNc[c];
+      const int *map = P.eaMap + P.eaPtr[c];
+      for (int k = 0; k < q; k++) {
+        double *v = V + (int64_t)k * Vstride + P.Sp[s];
+        const double *tc = T + (int64_t)k * Tstride + P.snTOff[c];
+        for (int a = tid; a < muc; a += blockDim.x) v[map[a]] += __ldcg(tc + a);
+      }
+      __syncthreads();
+    }
+  }
   for (int k = 0; k < q; k++) {
     const double *yk = y + (int64_t)k * P.n + f;
     double acc = 0.0;
@@ -116,7 +162,7 @@ __global__ void __launch_bounds__(256) k_fwd_blocks(const int4 *__restrict__ tas
     if (tid < kSB) {
       double sum = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
       const double *vk = V + (int64_t)k * Vstride + P.Sp[s];
-      red[0][tid] = tid < rows ? vk[r0 + tid] - sum : 0.0;
+      red[0][tid] = tid < rows ? __ldcg(vk + r0 + tid) - sum : 0.0;
     }
     __syncthreads();
     if (below) {
@@ -149,9 +195,13 @@ __global__ void __launch_bounds__(256) k_fwd_blocks(const int4 *__restrict__ tas
       __syncthreads();
     }
   }
-  if (!below && tid == 0) {
+  __syncthreads();
+  if (tid == 0) {
     __threadfence();
-    st_release(myflags + blk, epoch);
+    if (below)
+      atomicAdd(done + s, 1);
+    else
+      st_release(myflags + blk, epoch);
   }
 }
 
@@ -177,6 +227,14 @@ __global__ void __launch_bounds__(256) k_bwd_blocks(const int4 *__restrict__ tas
   const int c0 = blk * kSB, w = min(kSB, nc - c0), nb = (nc + kSB - 1) / kSB;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   int *myflags = flags + blkOff[s];
+  // one launch for the whole sweep (levels top-down): the rows below this supernode are final once its parent's
+  // first pivot block (the parent's last backward task) is
+  const int par = P.snParent[s];
+  if (par >= 0) {
+    if (tid == 0) waitOk = wait_flag(flags + blkOff[par], epoch, status, s);
+    __syncthreads();
+    if (!waitOk) return;
+  }
   for (int k = 0; k < q; k++) {
     double *yk = y + (int64_t)k * P.n;
     // each warp owns columns c0 + warp, c0 + warp + 8, ...; lanes walk the rows below the diagonal block
@@ -254,11 +312,11 @@ void launch_fwd_gather(const int *sns, int count, const DevPlan &P, const double
 }
 template <class TL>
 void launch_fwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const int *blkOff,
-                       const TL *Lx, double *y, const double *V, double *T, int *flags, int epoch, int q,
+                       const TL *Lx, double *y, double *V, double *T, int *flags, int epoch, int *done, int q,
                        int64_t Vstride, int64_t Tstride, unsigned long long *status, cudaStream_t st) {
   if (ntasks > 0)
-    k_fwd_blocks<TL><<<ntasks, 256, 0, st>>>(tasks, ntasks, ticket, P, blkOff, Lx, y, V, T, flags, epoch, q, Vstride,
-                                             Tstride, status);
+    k_fwd_blocks<TL><<<ntasks, 256, 0, st>>>(tasks, ntasks, ticket, P, blkOff, Lx, y, V, T, flags, epoch, done, q,
+                                             Vstride, Tstride, status);
 }
 template <class TL>
 void launch_bwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const int *blkOff,
@@ -268,10 +326,10 @@ void launch_bwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan
     k_bwd_blocks<TL><<<ntasks, 256, 0, st>>>(tasks, ntasks, ticket, P, blkOff, Lx, y, flags, epoch, q, status);
 }
 template void launch_fwd_blocks<double>(const int4 *, int, int *, const DevPlan &, const int *, const double *,
-                                        double *, const double *, double *, int *, int, int, int64_t, int64_t,
+                                        double *, double *, double *, int *, int, int *, int, int64_t, int64_t,
                                         unsigned long long *, cudaStream_t);
 template void launch_fwd_blocks<float>(const int4 *, int, int *, const DevPlan &, const int *, const float *, double *,
-                                       const double *, double *, int *, int, int, int64_t, int64_t,
+                                       double *, double *, int *, int, int *, int, int64_t, int64_t,
                                        unsigned long long *, cudaStream_t);
 template void launch_bwd_blocks<double>(const int4 *, int, int *, const DevPlan &, const int *, const double *,
                                         double *, int *, int, int, unsigned long long *, cudaStream_t);

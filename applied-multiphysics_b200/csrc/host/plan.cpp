@@ -297,6 +297,11 @@ void build_plan(const Symbolic &S, Plan &P) {
       }
     P.bwdLvlPtr[L + 1] = (int)(P.bwdTasks.size() / 4);
   }
+  // the whole backward sweep in one launch: levels top-down
+  P.bwdAll.clear();
+  for (int L = P.nlevels - 1; L >= 0; L--)
+    P.bwdAll.insert(P.bwdAll.end(), P.bwdTasks.begin() + 4 * (size_t)P.bwdLvlPtr[L],
+                    P.bwdTasks.begin() + 4 * (size_t)P.bwdLvlPtr[L + 1]);
 }
 
 }  // namespace amp

@@ -93,6 +93,7 @@ struct Plan {
   int nflags = 0;
   std::vector<int> fwdTasks, bwdTasks;  // int4 records, flattened
   std::vector<int> fwdLvlPtr, bwdLvlPtr;
+  std::vector<int> bwdAll;  // backward tasks of all levels, top-down (one launch)
   double flops = 0;
 };
 
