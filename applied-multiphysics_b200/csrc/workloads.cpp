@@ -396,13 +396,16 @@ WL_API amp_workload *amp_wl_elastic3d(int N, double E, double nu, uint32_t seed,
         for (int k = 0; k < 6; k++) s += D[i][k] * B[k][c];
         DB[i][c] = s;
       }
-    for (int r = 0; r < 12; r++) {
-      int row = 3 * t[r / 3] + r % 3;
-      for (int c = 0; c < 12; c++) {
+    double Ke[12][12];  // exactly symmetric: upper triangle computed, lower mirrored
+    for (int r = 0; r < 12; r++)
+      for (int c = r; c < 12; c++) {
         double s = 0;
         for (int k = 0; k < 6; k++) s += B[k][r] * DB[k][c];
-        val[entry_index(P, row, 3 * t[c / 3] + c % 3)] += V * s;
+        Ke[r][c] = Ke[c][r] = V * s;
       }
+    for (int r = 0; r < 12; r++) {
+      int row = 3 * t[r / 3] + r % 3;
+      for (int c = 0; c < 12; c++) val[entry_index(P, row, 3 * t[c / 3] + c % 3)] += Ke[r][c];
     }
   }
   int n = P.n;
