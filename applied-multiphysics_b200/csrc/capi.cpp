@@ -1,11 +1,13 @@
 // C ABI of libampsolve.so (include/ampsolve.h): plan / factor handles, device memory, and the orchestration of the
 // kernels on one CUDA stream per factor.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -74,6 +76,47 @@ namespace amp {
 void set_last_error(const std::string &msg) { g_err = msg; }
 }  // namespace amp
 
+namespace {
+// TMA descriptors of the BF16 split columns, two per supernode that has mixed-precision update tiles (hi, lo): the
+// front's m x nc column-major block (ld = round_up(m, 8)) as a 2D tensor {rows, columns}, 64 x 64 boxes with the
+// 128-byte swizzle; reads past m rows or nc columns return zeros, which is how partial tiles and K chunks are padded.
+std::vector<CUtensorMap> split_tensor_maps(const amp::Plan &P, const __nv_bfloat16 *Shi, const __nv_bfloat16 *Slo) {
+  using Encode = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                              const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static Encode encode = nullptr;
+  if (!encode) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    ck(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q), "cudaGetDriverEntryPoint");
+    if (!fn || q != cudaDriverEntryPointSuccess) throw std::runtime_error("cuTensorMapEncodeTiled not available");
+    encode = (Encode)fn;
+  }
+  std::vector<char> need(P.nsuper, 0);
+  for (const auto *v : {&P.mixTiles, &P.mixUTasks})
+    for (const amp::MixTask &t : *v) need[t.s] = 1;
+  std::vector<CUtensorMap> maps(2 * (size_t)std::max(1, P.nsuper));
+  std::memset(maps.data(), 0, sizeof(CUtensorMap) * maps.size());
+  for (int s = 0; s < P.nsuper; s++) {
+    if (!need[s]) continue;
+    const int m = P.snM[s], nc = P.snNc[s], ld = (m + 7) & ~7;
+    const cuuint64_t dims[2] = {(cuuint64_t)m, (cuuint64_t)nc};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    const cuuint32_t box[2] = {64, 64}, estr[2] = {1, 1};
+    for (int h = 0; h < 2; h++) {
+      const __nv_bfloat16 *base = (h ? Slo : Shi) + P.snSp[s];
+      CUresult r = encode(&maps[2 * s + h], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void *)base, dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS)
+        throw std::runtime_error("cuTensorMapEncodeTiled failed for supernode " + std::to_string(s) + " (error " +
+                                 std::to_string((int)r) + ")");
+    }
+  }
+  return maps;
+}
+}  // namespace
+
 struct amp_plan_s {
   amp::Symbolic S;
   amp::Plan P;
@@ -102,6 +145,7 @@ struct amp_factor_s {
   double *dLx = nullptr, *dU = nullptr, *dD = nullptr, *dValues = nullptr;
   float *dL32 = nullptr, *dU32 = nullptr;           // mixed precision: FP32 factor and update arena
   __nv_bfloat16 *dShi = nullptr, *dSlo = nullptr;   // BF16 split columns of the factored pivot blocks
+  CUtensorMap *dMaps = nullptr;                     // per supernode: TMA descriptors of its hi / lo split columns
   unsigned long long *dStatus = nullptr;
   int *dReaders = nullptr;  // per pivot block: row chunks that have read it (reset at every factorization)
   bool ok = false, hasValues = false;
@@ -242,14 +286,14 @@ void enqueue_factor(amp_factor *f) {
         const int64_t t0 = P.mixStepPtr[k], t1 = P.mixStepPtr[k + 1];
         if (t1 > t0)
           timed(f, K_UPDATE, sr.updateFlops, 0.0, [&] {
-            amp::launch_update_mx(f->plan->dMixTile + t0, t1 - t0, f->dL32, f->dU32, f->dShi, f->dSlo, f->dStatus,
+            amp::launch_update_mx(f->plan->dMixTile + t0, t1 - t0, f->dMaps, f->dL32, f->dU32, f->dStatus,
                                   amp::num_sms(), st);
           });
       }
       const int64_t u0 = P.mixULvlPtr[L], u1 = P.mixULvlPtr[L + 1];
       if (u1 > u0)
         timed(f, K_UPDATE, P.uLvlFlops[L], 0.0, [&] {
-          amp::launch_update_mx(f->plan->dMixU + u0, u1 - u0, f->dL32, f->dU32, f->dShi, f->dSlo, f->dStatus,
+          amp::launch_update_mx(f->plan->dMixU + u0, u1 - u0, f->dMaps, f->dL32, f->dU32, f->dStatus,
                                 amp::num_sms(), st);
         });
     }
@@ -530,6 +574,7 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
         f->dU32 = f->mem.alloc<float>((size_t)P.arenaDoubles);
         f->dShi = f->mem.alloc<__nv_bfloat16>((size_t)P.splitElems);
         f->dSlo = f->mem.alloc<__nv_bfloat16>((size_t)P.splitElems);
+        f->dMaps = f->mem.upload(split_tensor_maps(P, f->dShi, f->dSlo));
       }
       f->dD = f->mem.alloc<double>((size_t)P.n);
       f->dValues = f->mem.alloc<double>((size_t)P.patNnz);

@@ -1,6 +1,7 @@
 // Host-callable launchers of the device kernels.
 #pragma once
 #include <cuda_bf16.h>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -18,8 +19,8 @@ void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, con
 template <class T>
 void launch_panel(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, T *Lx, int *readers,
                   unsigned long long *status, __nv_bfloat16 *Shi, __nv_bfloat16 *Slo, cudaStream_t st);
-void launch_update_mx(const MixTask *tasks, int64_t ntasks, float *L32, float *U32, const __nv_bfloat16 *Shi,
-                      const __nv_bfloat16 *Slo, unsigned long long *status, int num_sms, cudaStream_t st);
+void launch_update_mx(const MixTask *tasks, int64_t ntasks, const CUtensorMap *maps, float *L32, float *U32,
+                      unsigned long long *status, int num_sms, cudaStream_t st);
 int num_sms();
 void launch_update(const TileTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, double *U,
                    const unsigned long long *status, cudaStream_t st);

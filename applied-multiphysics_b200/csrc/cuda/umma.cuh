@@ -23,6 +23,16 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo_bytes
   return d;                // base offset 0, lbo mode 0, layout type 0 (no swizzle)
 }
 
+// MN-major operand with the 128-byte swizzle (layout type 2), as TMA writes it for a box whose inner extent is 64
+// 16-bit elements: each K row of a 64-element MN block is 128 bytes, 8 K rows form a 1 KB swizzle atom.
+//   LBO = byte stride between 64-element MN blocks, SBO = byte stride between groups of 8 K rows.
+// The start address must keep the 1 KB atom phase (advance by multiples of 1 KB), base offset 0.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+  uint64_t d = smem_desc(saddr, lbo_bytes, sbo_bytes);
+  d |= (uint64_t)2 << 61;
+  return d;
+}
+
 constexpr uint32_t idesc_bf16_f32_mn(int M, int N) {
   return (1u << 4)                   // D format F32
          | (1u << 7) | (1u << 10)    // A, B format BF16
@@ -49,6 +59,25 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
     if (i > 64) __nanosleep(128);
   }
   return false;
+}
+
+// Arrive once and add `bytes` to the transaction count the current phase waits for (the TMA loads complete it).
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// 2D tiled TMA load of one box into this CTA's shared memory, completing on `bar` (no multicast). The tensor map
+// lives in global memory, written by the host before the launch. x is the innermost (contiguous) coordinate and must
+// be a multiple of 8 for 16-bit data; coordinates past the tensor's extent read zeros.
+__device__ __forceinline__ void tma_load_2d(void *dst, const void *tmap, int x, int y, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::
+          "r"(smem_u32(dst)),
+      "l"(tmap), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
 }
 
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }

@@ -5,12 +5,18 @@
 // kernel, into the split buffers) and A B^T ~= Ahi Bhi^T + Ahi Blo^T + Alo Bhi^T with FP32 accumulation in tensor
 // memory (the dropped Alo Blo^T term is ~2^-16 relative).
 //
-// One CTA per SM (persistent), 4 warps. Per (tile, 64-column K chunk) item all threads stream the chunk's hi/lo
-// operands into one of two shared-memory stages with 16-byte cp.async (MN-major, no-swizzle UMMA layout); thread 0
-// then issues 4 K-steps x 3 UMMAs (M = 128, N = 256, K = 16) and commits them to the stage's mbarrier, so the next
-// chunk loads while the tensor core works. After a tile's last chunk every warp reads its 32 accumulator lanes from
-// tensor memory (tcgen05.ld) and updates its 32 rows of C. Every mbarrier wait is bounded; on time-out the kernel
-// records a device-timeout status and leaves (after waiting, bounded, for its own MMAs), freeing its tensor memory.
+// Persistent, one CTA per SM, warp-specialised:
+//   warp 0      TMA producer: per 64-column K chunk, 12 boxes of 64 rows x 64 columns (A and B, hi and lo) from the
+//               front's 2D tensor maps into one of two 96 KB shared-memory stages (128-byte swizzle, zero fill past
+//               the front's rows and pivot columns), completing on the stage's `full` barrier;
+//   warp 1      MMA issuer: 4 K-steps x 3 UMMAs (M = 128, N = 256, K = 16) per chunk into one of two TMEM
+//               accumulators (2 x 256 columns), `empty` commit per stage, `accFull` commit per tile;
+//   warps 2-9   epilogue: 4 lane quadrants x 2 column halves; tcgen05.ld the accumulator, release it (`accEmpty`),
+//               then subtract it from the FP32 front (masked to the task's rows, columns and the lower triangle).
+// The epilogue of tile t overlaps the loads and MMAs of tile t + 1. Every wait is bounded: on time-out the waiting
+// role raises a shared abort flag and a device-timeout status, the other roles see the flag and leave, and before
+// the tensor memory is freed the producer waits (bounded) for its own loads and the MMA warp for its own MMAs.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -24,161 +30,206 @@ namespace amp {
 
 namespace {
 constexpr int kM = 128, kN = 256, kK = 64;
-// Layout per 16-column K step: [K step][MN core block][K half][8 rows x 16 bytes]. The two K halves of an MN block
-// are adjacent (LBO = 128 B) and MN blocks are 256 B apart (SBO), so one MMA's operand stays inside its K-step slab.
-constexpr uint32_t kLbo = 128, kSbo = 256;
-constexpr uint32_t kStepA = (kM / 8) * 256, kStepB = (kN / 8) * 256;  // bytes per K step
-constexpr int kBytesA = kM * kK * 2, kBytesB = kN * kK * 2;          // one of hi / lo
-constexpr int kStageBytes = 2 * kBytesA + 2 * kBytesB;              // 96 KB
+constexpr int kBox = 64;                                  // rows per TMA box (128 bytes of BF16)
+constexpr uint32_t kBoxBytes = kBox * kK * 2;             // 8 KB
+constexpr uint32_t kABytes = kM * kK * 2;                 // 16 KB (hi or lo)
+constexpr uint32_t kBBytes = kN * kK * 2;                 // 32 KB
+constexpr uint32_t kStageBytes = 2 * kABytes + 2 * kBBytes;  // 96 KB
+constexpr int kStages = 2;
+constexpr uint32_t kLbo = kBoxBytes;                      // between 64-row MN blocks
+constexpr uint32_t kSbo = 8 * 128;                        // between groups of 8 K rows
+constexpr uint32_t kKStep = 16 * 128;                     // one K16 step (2 groups of 8 K rows)
+constexpr int kEpiPerQuad = 2;                           // epilogue warps per TMEM lane quadrant
+constexpr int kEpiWarps = 4 * kEpiPerQuad;
+constexpr int kThreads = 32 * (2 + kEpiWarps);
+constexpr uint32_t kTmemCols = 2 * kN;
 constexpr uint32_t kIdesc = umma::idesc_bf16_f32_mn(kM, kN);
+constexpr long long kSpin = 1ll << 22;                    // ~0.5 s with back-off
 }  // namespace
 
-constexpr int kMixedSmem = 2 * kStageBytes + 1024;
+constexpr int kMixedSmem = kStages * kStageBytes + 1024;
 
-__device__ __forceinline__ void mx_fill(const MixTask &t, int chunk, const __nv_bfloat16 *Shi,
-                                        const __nv_bfloat16 *Slo, uint8_t *stage) {
-  const int kc = t.c0 + chunk * kK, kw = min(kK, t.w - chunk * kK);
-  const uint32_t sa = umma::smem_u32(stage);
-  const int tid = threadIdx.x;
-  // A: 16 row-units x 64 columns = 1024 16-byte units per hi / lo; unit u -> (mb = u % 16, k = u / 16)
-#pragma unroll 2
-  for (int u = tid; u < (kM / 8) * kK; u += 128) {
-    const int mb = u & 15, k = u >> 4, r = t.i0 + 8 * mb;
-    const bool ok = k < kw && r < t.ld;
-    const int64_t g = t.sp + (int64_t)(kc + (ok ? k : 0)) * t.ld + (ok ? r : 0);
-    const uint32_t off = (k >> 4) * kStepA + mb * kSbo + ((k >> 3) & 1) * kLbo + (k & 7) * 16;
-    umma::cp_async16(sa + off, Shi + g, ok);
-    umma::cp_async16(sa + kBytesA + off, Slo + g, ok);
+struct MxShared {
+  uint64_t full[kStages], empty[kStages], accFull[2], accEmpty[2], drain;
+  uint32_t tmem;
+  int abort;
+};
+
+// Bounded wait that also gives up when another role raised the abort flag. false: aborted or timed out.
+__device__ __forceinline__ bool mx_wait(uint64_t *bar, uint32_t parity, MxShared &sh, unsigned long long *status) {
+  for (long long i = 0; i < kSpin; i++) {
+    if (umma::mbar_try_wait(bar, parity)) return true;
+    if (*(volatile int *)&sh.abort) return false;
+    if (i > 64) __nanosleep(128);
   }
-  // B: 32 row-units x 64 columns
-#pragma unroll 2
-  for (int u = tid; u < (kN / 8) * kK; u += 128) {
-    const int nb = u & 31, k = u >> 5, r = t.j0 + 8 * nb;
-    const bool ok = k < kw && r < t.ld;
-    const int64_t g = t.sp + (int64_t)(kc + (ok ? k : 0)) * t.ld + (ok ? r : 0);
-    const uint32_t off = (k >> 4) * kStepB + nb * kSbo + ((k >> 3) & 1) * kLbo + (k & 7) * 16;
-    umma::cp_async16(sa + 2 * kBytesA + off, Shi + g, ok);
-    umma::cp_async16(sa + 2 * kBytesA + kBytesB + off, Slo + g, ok);
-  }
-  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+  *(volatile int *)&sh.abort = 1;
+  atomicMin(status, status_word(0x7fffffff, 3, 0));
+  return false;
 }
 
-__global__ void __launch_bounds__(128, 1) k_update_mx(const MixTask *__restrict__ tasks, int ntasks,
-                                                      float *__restrict__ L32, float *__restrict__ U32,
-                                                      const __nv_bfloat16 *__restrict__ Shi,
-                                                      const __nv_bfloat16 *__restrict__ Slo,
-                                                      unsigned long long *status) {
+__global__ void __launch_bounds__(kThreads, 1) k_update_mx(const MixTask *__restrict__ tasks, int ntasks,
+                                                           const CUtensorMap *__restrict__ maps,
+                                                           float *__restrict__ L32, float *__restrict__ U32,
+                                                           unsigned long long *status) {
   extern __shared__ __align__(1024) uint8_t smem_mx[];
-  __shared__ uint64_t bar[2];
-  __shared__ uint32_t tmem_slot;
-  __shared__ int abort_flag;
+  __shared__ MxShared sh;
   if (*(volatile unsigned long long *)status != kStatusOk) return;
   if ((int)blockIdx.x >= ntasks) return;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  uint8_t *stages = smem_mx + ((1024 - (umma::smem_u32(smem_mx) & 1023)) & 1023);  // 1 KB aligned
-  if (warp == 0) umma::tmem_alloc(&tmem_slot, kN);
-  if (tid == 0) {
-    umma::mbar_init(&bar[0], 1);
-    umma::mbar_init(&bar[1], 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint8_t *stages = smem_mx + ((1024 - (umma::smem_u32(smem_mx) & 1023)) & 1023);  // 1 KB aligned (swizzle atom)
+  if (warp == 1) umma::tmem_alloc(&sh.tmem, kTmemCols);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; s++) {
+      umma::mbar_init(&sh.full[s], 1);
+      umma::mbar_init(&sh.empty[s], 1);
+    }
+    for (int a = 0; a < 2; a++) {
+      umma::mbar_init(&sh.accFull[a], 1);
+      umma::mbar_init(&sh.accEmpty[a], kEpiWarps);
+    }
+    umma::mbar_init(&sh.drain, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    abort_flag = 0;
+    sh.abort = 0;
   }
   umma::tc_fence_before();
   __syncthreads();
   umma::tc_fence_after();
-  const uint32_t tmem = tmem_slot;
-  uint32_t phase[2] = {0, 0};
-  bool pending[2] = {false, false};
-  int item = 0;
-  bool failedWait = false;  // block-uniform
-  auto consume = [&](int s) -> bool {  // wait for the MMAs committed on stage s (bounded)
-    if (!pending[s]) return true;
-    const bool ok = umma::mbar_wait(&bar[s], phase[s]);
-    phase[s] ^= 1;
-    pending[s] = false;
-    return ok;
-  };
-  for (int t = blockIdx.x; t < ntasks && !failedWait; t += gridDim.x) {
-    const MixTask tk = tasks[t];
-    const int nch = (tk.w + kK - 1) / kK;
-    for (int c = 0; c < nch; c++, item++) {
-      const int s = item & 1;
-      if (__syncthreads_or(!consume(s))) {  // block-uniform decision
-        failedWait = true;
-        break;
-      }
-      uint8_t *st = stages + s * kStageBytes;
-      mx_fill(tk, c, Shi, Slo, st);
-      umma::fence_async_smem();
-      umma::tc_fence_before();
-      __syncthreads();
-      if (tid == 0) {
-        umma::tc_fence_after();
-        const uint32_t sa = umma::smem_u32(st);
-        const int kw = min(kK, tk.w - c * kK);
-        for (int kk = 0; kk * 16 < kw; kk++) {
-          const uint32_t ao = kk * kStepA, bo = kk * kStepB;
-          const uint64_t ahi = umma::smem_desc(sa + ao, kLbo, kSbo);
-          const uint64_t alo = umma::smem_desc(sa + kBytesA + ao, kLbo, kSbo);
-          const uint64_t bhi = umma::smem_desc(sa + 2 * kBytesA + bo, kLbo, kSbo);
-          const uint64_t blo = umma::smem_desc(sa + 2 * kBytesA + kBytesB + bo, kLbo, kSbo);
-          umma::mma_bf16(tmem, ahi, bhi, kIdesc, c > 0 || kk > 0);
-          umma::mma_bf16(tmem, ahi, blo, kIdesc, true);
-          umma::mma_bf16(tmem, alo, bhi, kIdesc, true);
-        }
-        umma::mma_commit(&bar[s]);
-      }
-      pending[s] = true;
-    }
-    if (failedWait) break;
-    // all MMAs of the tile: the last commit covers every earlier one
-    const int last = (item - 1) & 1;
-    const bool ok1 = consume(last), ok2 = consume(last ^ 1);
-    if (__syncthreads_or(!(ok1 && ok2))) {
-      failedWait = true;
-      break;
-    }
-    umma::tc_fence_after();
-    // epilogue: warp w owns accumulator lanes (tile rows) 32w .. 32w + 31
-    const int i = tk.i0 + 32 * warp + lane, m = tk.m, nc = tk.nc, mu = m - nc;
-    float *Lp = L32 + tk.lp;
-    float *Up = tk.up >= 0 ? U32 + tk.up : Lp;
-    const bool rowok = i >= tk.ilo && i < m;
-    for (int cc = 0; cc < kN / 32; cc++) {
-      float v[32];
-      umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + cc * 32, v);
-      if (!rowok) continue;
+  const uint32_t tmem = sh.tmem;
+
+  if (warp == 0) {
+    if (lane == 0) {  // ---- TMA producer
+      int it = 0;
+      for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
+        const MixTask tk = tasks[t];
+        const CUtensorMap *mhi = maps + 2 * tk.s, *mlo = mhi + 1;
+        const int nch = (tk.w + kK - 1) / kK;
+        bool ok = true;
+        for (int c = 0; c < nch; c++, it++) {
+          const int s = it % kStages;
+          const uint32_t n = it / kStages;
+          if (!mx_wait(&sh.empty[s], (n & 1) ^ 1, sh, status)) {
+            ok = false;
+            break;
+          }
+          uint8_t *st = stages + s * kStageBytes;
+          umma::mbar_arrive_expect_tx(&sh.full[s], kStageBytes);
+          const int kc = tk.c0 + c * kK;
 #pragma unroll
-      for (int x = 0; x < 32; x++) {
-        const int j = tk.j0 + cc * 32 + x;
-        if (j >= tk.jlo && j < tk.jend && i >= j) {
-          float *p = j < nc ? Lp + (int64_t)j * m + i : Up + (int64_t)(j - nc) * mu + (i - nc);
-          *p -= v[x];
+          for (int b = 0; b < kM / kBox; b++) {
+            umma::tma_load_2d(st + b * kBoxBytes, mhi, tk.i0 + kBox * b, kc, &sh.full[s]);
+            umma::tma_load_2d(st + kABytes + b * kBoxBytes, mlo, tk.i0 + kBox * b, kc, &sh.full[s]);
+          }
+#pragma unroll
+          for (int b = 0; b < kN / kBox; b++) {
+            umma::tma_load_2d(st + 2 * kABytes + b * kBoxBytes, mhi, tk.j0 + kBox * b, kc, &sh.full[s]);
+            umma::tma_load_2d(st + 2 * kABytes + kBBytes + b * kBoxBytes, mlo, tk.j0 + kBox * b, kc, &sh.full[s]);
+          }
         }
+        if (!ok) break;
+      }
+      // let the last loads land before the CTA can exit (bounded, also after an abort)
+      for (int q = it > kStages ? it - kStages : 0; q < it; q++)
+        umma::mbar_wait(&sh.full[q % kStages], (q / kStages) & 1);
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0) {  // ---- MMA issuer
+      int it = 0, tl = 0;
+      for (int t = blockIdx.x; t < ntasks; t += gridDim.x, tl++) {
+        const MixTask tk = tasks[t];
+        const int nch = (tk.w + kK - 1) / kK;
+        const int a = tl & 1;
+        if (!mx_wait(&sh.accEmpty[a], ((tl >> 1) & 1) ^ 1, sh, status)) break;
+        umma::tc_fence_after();
+        const uint32_t d = tmem + a * kN;
+        bool ok = true;
+        for (int c = 0; c < nch; c++, it++) {
+          const int s = it % kStages;
+          if (!mx_wait(&sh.full[s], (it / kStages) & 1, sh, status)) {
+            ok = false;
+            break;
+          }
+          umma::tc_fence_after();
+          const uint32_t sa = umma::smem_u32(stages + s * kStageBytes);
+          const int kw = min(kK, tk.w - c * kK);
+          for (int kk = 0; kk * 16 < kw; kk++) {
+            const uint64_t ahi = umma::smem_desc_sw128(sa + kk * kKStep, kLbo, kSbo);
+            const uint64_t alo = umma::smem_desc_sw128(sa + kABytes + kk * kKStep, kLbo, kSbo);
+            const uint64_t bhi = umma::smem_desc_sw128(sa + 2 * kABytes + kk * kKStep, kLbo, kSbo);
+            const uint64_t blo = umma::smem_desc_sw128(sa + 2 * kABytes + kBBytes + kk * kKStep, kLbo, kSbo);
+            umma::mma_bf16(d, ahi, bhi, kIdesc, c > 0 || kk > 0);
+            umma::mma_bf16(d, ahi, blo, kIdesc, true);
+            umma::mma_bf16(d, alo, bhi, kIdesc, true);
+          }
+          umma::mma_commit(&sh.empty[s]);  // the stage is free once these MMAs have read it
+        }
+        if (!ok) break;
+        umma::mma_commit(&sh.accFull[a]);  // accumulator complete
+      }
+      umma::mma_commit(&sh.drain);  // all MMAs of this CTA done before the tensor memory is freed
+      umma::mbar_wait(&sh.drain, 0);
+    }
+    __syncwarp();
+  } else {  // ---- epilogue: quadrant q of the TMEM lanes (rows), column quarter h
+    const int ew = warp - 2, q = warp & 3, h = ew >> 2;
+    int tl = 0;
+    for (int t = blockIdx.x; t < ntasks; t += gridDim.x, tl++) {
+      const MixTask tk = tasks[t];
+      const int a = tl & 1;
+      bool ok = true;
+      if (lane == 0) ok = mx_wait(&sh.accFull[a], (tl >> 1) & 1, sh, status);
+      if (!__shfl_sync(0xffffffffu, ok ? 1 : 0, 0)) break;
+      umma::tc_fence_after();
+      const int i = tk.i0 + 32 * q + lane, m = tk.m, nc = tk.nc, mu = m - nc;
+      const bool rowok = i >= tk.ilo && i < m;
+      float *Lp = L32 + tk.lp;
+      float *Up = tk.up >= 0 ? U32 + tk.up : Lp;
+      constexpr int kChunks = kN / kEpiPerQuad / 32;
+#pragma unroll 1
+      for (int cc = 0; cc < kChunks; cc++) {
+        const int col0 = h * (kN / kEpiPerQuad) + cc * 32;
+        float v[32];
+        umma::tmem_ld32(tmem + a * kN + ((uint32_t)(32 * q) << 16) + col0, v);
+        if (cc == kChunks - 1) {  // accumulator fully read: hand it back to the MMA warp
+          umma::tc_fence_before();
+          __syncwarp();
+          if (lane == 0) umma::mbar_arrive(&sh.accEmpty[a]);
+        }
+        if (!rowok) continue;
+        const int j0 = tk.j0 + col0;
+        const int jl = max(tk.jlo, j0), jh = min(min(tk.jend, i + 1), j0 + 32);  // columns of this row to update
+        if (jl >= jh) continue;
+        const uint32_t msk = (jh - j0 == 32 ? 0xffffffffu : ((1u << (jh - j0)) - 1)) & ~((1u << (jl - j0)) - 1);
+        auto addr = [&](int x) {
+          const int j = j0 + x;
+          return j < nc ? Lp + (int64_t)j * m + i : Up + (int64_t)(j - nc) * mu + (i - nc);
+        };
+        float c[32];
+#pragma unroll
+        for (int x = 0; x < 32; x++) c[x] = (msk >> x) & 1 ? *addr(x) : 0.f;
+#pragma unroll
+        for (int x = 0; x < 32; x++)
+          if ((msk >> x) & 1) *addr(x) = c[x] - v[x];
       }
     }
-    umma::tc_fence_before();
-    __syncthreads();  // accumulators read before the next tile's first MMA overwrites them
-  }
-  if (failedWait) {
-    if (tid == 0) atomicMin(status, status_word(0x7fffffff, 3, 0));
-    consume(0);  // bounded: let our own MMAs finish before freeing tensor memory
-    consume(1);
   }
   umma::tc_fence_before();
   __syncthreads();
-  if (warp == 0) umma::tmem_dealloc(tmem, kN);
+  if (warp == 1) {
+    umma::tc_fence_after();
+    umma::tmem_dealloc(tmem, kTmemCols);
+  }
 }
 
 void init_mixed_attributes() {
   cudaFuncSetAttribute(k_update_mx, cudaFuncAttributeMaxDynamicSharedMemorySize, kMixedSmem);
 }
 
-void launch_update_mx(const MixTask *tasks, int64_t ntasks, float *L32, float *U32, const __nv_bfloat16 *Shi,
-                      const __nv_bfloat16 *Slo, unsigned long long *status, int num_sms, cudaStream_t st) {
+void launch_update_mx(const MixTask *tasks, int64_t ntasks, const CUtensorMap *maps, float *L32, float *U32,
+                      unsigned long long *status, int num_sms, cudaStream_t st) {
   if (ntasks <= 0) return;
   const int grid = (int)(ntasks < num_sms ? ntasks : num_sms);
-  k_update_mx<<<grid, 128, kMixedSmem, st>>>(tasks, (int)ntasks, L32, U32, Shi, Slo, status);
+  k_update_mx<<<grid, kThreads, kMixedSmem, st>>>(tasks, (int)ntasks, maps, L32, U32, status);
 }
 
 }  // namespace amp

@@ -172,7 +172,7 @@ void build_plan(const Symbolic &S, Plan &P) {
     for (int j0 = clo & ~7; j0 < chi; j0 += 256)
       for (int i0 = std::max(rlo, j0) & ~7; i0 < m; i0 += 128)
         out.push_back({(long long)P.snLxp[s], (long long)P.snUoff[s], (long long)P.snSp[s], m, nc, (m + 7) & ~7, kc0,
-                       kw, i0, j0, rlo, clo, chi, 0});
+                       kw, i0, j0, rlo, clo, chi, s});
   };
   P.mixStepPtr.assign(1, 0);
   P.mixULvlPtr.assign(1, 0);

@@ -38,7 +38,7 @@ struct MixTask {  // mixed-precision update tile (128 x 256, 8-aligned start) of
   int m, nc, ld, c0, w;      // K = pivot columns [c0, c0 + w)
   int i0, j0;                // tile origin (multiples of 8)
   int ilo, jlo, jend;        // rows >= ilo, columns in [jlo, jend) are updated
-  int pad;
+  int s;                     // supernode (selects the front's TMA descriptors of the split columns)
 };
 struct AsmTask {  // zero + assemble + extend-add front columns [j0, j0 + 32) of supernode s
   int s, j0;
