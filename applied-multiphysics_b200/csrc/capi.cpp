@@ -77,6 +77,9 @@ void set_last_error(const std::string &msg) { g_err = msg; }
 }  // namespace amp
 
 namespace {
+// elements of the diagonal-block inverses (none for an empty pattern, whose plan has no per-block arrays)
+int64_t inv_elems(const amp::Plan &P) { return P.invOff.empty() ? 0 : P.invOff[P.nflags]; }
+
 // TMA descriptors of the BF16 split columns, two per supernode that has mixed-precision update tiles (hi, lo): the
 // front's m x nc column-major block (ld = round_up(m, 8)) as a 2D tensor {rows, columns}, 64 x 64 boxes with the
 // 128-byte swizzle; reads past m rows or nc columns return zeros, which is how partial tiles and K chunks are padded.
@@ -129,7 +132,6 @@ struct amp_plan_s {
   amp::TileTask *dTile = nullptr, *dUTile = nullptr;
   amp::MixTask *dMixTile = nullptr, *dMixU = nullptr;
   int4 *dFwdTasks = nullptr, *dBwdTasks = nullptr, *dBwdAll = nullptr;
-  int *dBlkOff = nullptr;
   int *dRowptr = nullptr, *dColidx = nullptr;
   std::vector<int> rowptr, colidx;  // host copy of the pattern (uploaded with the schedule)
   bool uploaded = false;
@@ -144,6 +146,8 @@ struct amp_factor_s {
   DevMem mem;
   double *dLx = nullptr, *dU = nullptr, *dD = nullptr, *dValues = nullptr;
   float *dL32 = nullptr, *dU32 = nullptr;           // mixed precision: FP32 factor and update arena
+  double *dInv = nullptr;                           // inverses of the 64-column diagonal blocks (FP64 factor)
+  float *dInv32 = nullptr;                          // the same for the FP32 factor
   __nv_bfloat16 *dShi = nullptr, *dSlo = nullptr;   // BF16 split columns of the factored pivot blocks
   CUtensorMap *dMaps = nullptr;                     // per supernode: TMA descriptors of its hi / lo split columns
   unsigned long long *dStatus = nullptr;
@@ -210,6 +214,8 @@ void upload_plan(amp_plan *pl) {
   d.perm = m.upload(P.perm);
   d.Sp = m.upload(P.Sp);
   d.Si = m.upload(P.Si);
+  d.blkOff = m.upload(P.blkOff);
+  d.invOff = m.upload(P.invOff);
   pl->dAsm = m.upload(P.asmTasks);
   pl->dPanel = m.upload(P.panelTasks);
   pl->dTile = m.upload(P.tileTasks);
@@ -219,7 +225,6 @@ void upload_plan(amp_plan *pl) {
   pl->dFwdTasks = (int4 *)m.upload(P.fwdTasks);
   pl->dBwdTasks = (int4 *)m.upload(P.bwdTasks);
   pl->dBwdAll = (int4 *)m.upload(P.bwdAll);
-  pl->dBlkOff = m.upload(P.blkOff);
 }
 
 void ensure_solve_ws(amp_factor *f, int q) {
@@ -238,9 +243,9 @@ void ensure_solve_ws(amp_factor *f, int q) {
   f->qcap = q;
 }
 
-enum KernelKind { K_ASSEMBLE, K_PANEL, K_UPDATE, K_FORWARD, K_BACKWARD, K_PERMUTE, K_RESIDUAL, K_NKINDS };
+enum KernelKind { K_ASSEMBLE, K_PANEL, K_UPDATE, K_FORWARD, K_BACKWARD, K_PERMUTE, K_RESIDUAL, K_DIAGINV, K_NKINDS };
 const char *kKindNames[K_NKINDS] = {"assemble", "panel_potrf_trsm", "update_syrk", "solve_forward",
-                                    "solve_backward", "permute", "residual_spmv"};
+                                    "solve_backward", "permute", "residual_spmv", "diag_inverse"};
 
 cudaEvent_t pool_event(amp_factor *f) {
   if (f->evUsed == f->evPool.size()) {
@@ -297,6 +302,9 @@ void enqueue_factor(amp_factor *f) {
                                 amp::num_sms(), st);
         });
     }
+    if (P.nflags)
+      timed(f, K_DIAGINV, 0.0, 8.0 * (double)inv_elems(P),
+            [&] { amp::launch_diag_inv<float>(dp, P.nflags, f->dL32, f->dInv32, st); });
     return;
   }
   for (int L = 0; L < P.nlevels; L++) {
@@ -321,6 +329,9 @@ void enqueue_factor(amp_factor *f) {
                            f->dStatus, st);
       });
   }
+  if (P.nflags)
+    timed(f, K_DIAGINV, 0.0, 16.0 * (double)inv_elems(P),
+          [&] { amp::launch_diag_inv<double>(dp, P.nflags, f->dLx, f->dInv, st); });
 }
 
 // y (permuted order, q vectors) := A^-1 y in place
@@ -337,19 +348,19 @@ void device_solve_permuted(amp_factor *f, int q) {
   const int nf = P.fwdLvlPtr[P.nlevels], nb = (int)(P.bwdAll.size() / 4);
   timed(f, K_FORWARD, 0.0, lbytes, [&] {
     if (f->dL32)
-      amp::launch_fwd_blocks<float>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->plan->dBlkOff, f->dL32, f->dY, f->dV,
-                                    f->dT, f->dFlags, efwd, f->dDone, q, Vs, Ts, f->dSolveStatus, st);
+      amp::launch_fwd_blocks<float>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->dL32, f->dInv32, f->dY, f->dV, f->dT,
+                                    f->dFlags, efwd, f->dDone, q, Vs, Ts, f->dSolveStatus, st);
     else
-      amp::launch_fwd_blocks<double>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->plan->dBlkOff, f->dLx, f->dY, f->dV,
-                                     f->dT, f->dFlags, efwd, f->dDone, q, Vs, Ts, f->dSolveStatus, st);
+      amp::launch_fwd_blocks<double>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->dLx, f->dInv, f->dY, f->dV, f->dT,
+                                     f->dFlags, efwd, f->dDone, q, Vs, Ts, f->dSolveStatus, st);
   });
   timed(f, K_BACKWARD, 0.0, lbytes, [&] {
     if (f->dL32)
-      amp::launch_bwd_blocks<float>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->plan->dBlkOff, f->dL32, f->dY,
-                                    f->dFlags, ebwd, q, f->dSolveStatus, st);
+      amp::launch_bwd_blocks<float>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dL32, f->dInv32, f->dY, f->dFlags,
+                                    ebwd, q, f->dSolveStatus, st);
     else
-      amp::launch_bwd_blocks<double>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->plan->dBlkOff, f->dLx, f->dY,
-                                     f->dFlags, ebwd, q, f->dSolveStatus, st);
+      amp::launch_bwd_blocks<double>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dLx, f->dInv, f->dY, f->dFlags,
+                                     ebwd, q, f->dSolveStatus, st);
   });
 }
 
@@ -569,9 +580,11 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
       if (o.precision == AMP_FP64) {
         f->dLx = f->mem.alloc<double>((size_t)P.nnzLStored);
         f->dU = f->mem.alloc<double>((size_t)P.arenaDoubles);
+        f->dInv = f->mem.alloc<double>((size_t)inv_elems(P));
       } else {
         f->dL32 = f->mem.alloc<float>((size_t)P.nnzLStored);
         f->dU32 = f->mem.alloc<float>((size_t)P.arenaDoubles);
+        f->dInv32 = f->mem.alloc<float>((size_t)inv_elems(P));
         f->dShi = f->mem.alloc<__nv_bfloat16>((size_t)P.splitElems);
         f->dSlo = f->mem.alloc<__nv_bfloat16>((size_t)P.splitElems);
         f->dMaps = f->mem.upload(split_tensor_maps(P, f->dShi, f->dSlo));

@@ -14,6 +14,8 @@ struct DevPlan {
   const int *eaMap;
   const int *lvlSn;
   const int *perm, *Sp, *Si;
+  const int *blkOff;       // first 64-column diagonal block of supernode s (nsuper + 1)
+  const int64_t *invOff;   // offset of the inverse of each diagonal block (w x w, column-major)
 };
 
 // Failure record: the lowest failing global column wins (atomicMin), code in the low bits.

@@ -417,81 +417,18 @@ __global__ void k_permute_out(const double *__restrict__ y, double *__restrict__
   x[(int64_t)k * n + perm[i]] = y[idx];
 }
 
-// Forward: one CTA per supernode of the level. V: per-supernode front vectors (offset Sp[s], length m, per RHS
-// stride Vstride); T: pass-up vectors (offset snTOff[s], length mu, per RHS stride Tstride).
-__global__ void __launch_bounds__(256) k_forward(const int *__restrict__ sns, DevPlan P, const double *__restrict__ Lx,
-                                                 double *__restrict__ y, double *__restrict__ V, double *__restrict__ T,
-                                                 int q, int64_t Vstride, int64_t Tstride) {
-  const int s = sns[blockIdx.x];
-  const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s], mu = m - nc;
-  const double *Lp = Lx + P.snLxp[s];
-  for (int k = 0; k < q; k++) {
-    double *v = V + (int64_t)k * Vstride + P.Sp[s];
-    double *yk = y + (int64_t)k * P.n;
-    for (int r = threadIdx.x; r < m; r += blockDim.x) v[r] = r < nc ? yk[f + r] : 0.0;
-    __syncthreads();
-    for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
-      const int c = P.chList[qq];
-      const int muc = P.snM[c] - P.snNc[c];
-      const int *map = P.eaMap + P.eaPtr[c];
-      const double *tc = T + (int64_t)k * Tstride + P.snTOff[c];
-      for (int a = threadIdx.x; a < muc; a += blockDim.x) v[map[a]] += tc[a];
-      __syncthreads();
-    }
-    for (int c = 0; c < nc; c++) {
-      const double *col = Lp + (int64_t)c * m;
-      const double yc = v[c] / col[c];
-      __syncthreads();
-      if (threadIdx.x == 0) v[c] = yc;
-      for (int r = c + 1 + threadIdx.x; r < m; r += blockDim.x) v[r] -= col[r] * yc;
-      __syncthreads();
-    }
-    for (int r = threadIdx.x; r < nc; r += blockDim.x) yk[f + r] = v[r];
-    double *ts = T + (int64_t)k * Tstride + P.snTOff[s];
-    for (int r = threadIdx.x; r < mu; r += blockDim.x) ts[r] = v[nc + r];
-    __syncthreads();
-  }
-}
-
-// Backward: one CTA per supernode of the level (levels top-down); ancestors' x are final.
-__global__ void __launch_bounds__(256) k_backward(const int *__restrict__ sns, DevPlan P, const double *__restrict__ Lx,
-                                                  double *__restrict__ y, int q) {
-  const int s = sns[blockIdx.x];
-  const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
-  const double *Lp = Lx + P.snLxp[s];
-  const int *rows = P.Si + P.Sp[s];
-  __shared__ double red[256 / 32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int k = 0; k < q; k++) {
-    double *yk = y + (int64_t)k * P.n;
-    for (int c = nc - 1; c >= 0; c--) {
-      const double *col = Lp + (int64_t)c * m;
-      double part = 0.0;
-      for (int r = c + 1 + threadIdx.x; r < m; r += blockDim.x) part += col[r] * yk[rows[r]];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
-      if (lane == 0) red[warp] = part;
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double sum = 0.0;
-        for (int wv = 0; wv < nw; wv++) sum += red[wv];
-        yk[f + c] = (yk[f + c] - sum) / col[c];
-      }
-      __syncthreads();
-    }
-  }
-}
-
 // ---------------------------------------------------------------------------------------------------------------
 // Launchers (host side)
 // ---------------------------------------------------------------------------------------------------------------
 static int g_num_sms = 148;
 constexpr int kPanelSmem = kPanel * 256 * (int)sizeof(double);
 void init_mixed_attributes();
+void init_solve_attributes();
 void init_kernel_attributes() {
   cudaFuncSetAttribute(k_panel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmem);
   cudaFuncSetAttribute(k_panel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmem / 2);
   init_mixed_attributes();
+  init_solve_attributes();
   cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, kUpdateSmem);
   int dev = 0;
   cudaGetDevice(&dev);
@@ -532,12 +469,4 @@ void launch_permute_out(const double *y, double *x, const int *perm, int n, int 
   int64_t tot = (int64_t)n * q;
   if (tot > 0) k_permute_out<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(y, x, perm, n, q);
 }
-void launch_forward(const int *sns, int count, const DevPlan &P, const double *Lx, double *y, double *V, double *T,
-                    int q, int64_t Vstride, int64_t Tstride, cudaStream_t st) {
-  if (count > 0) k_forward<<<count, 256, 0, st>>>(sns, P, Lx, y, V, T, q, Vstride, Tstride);
-}
-void launch_backward(const int *sns, int count, const DevPlan &P, const double *Lx, double *y, int q, cudaStream_t st) {
-  if (count > 0) k_backward<<<count, 256, 0, st>>>(sns, P, Lx, y, q);
-}
-
 }  // namespace amp

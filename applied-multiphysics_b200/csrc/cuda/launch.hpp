@@ -26,18 +26,14 @@ void launch_update(const TileTask *tasks, int64_t ntasks, const DevPlan &P, doub
                    const unsigned long long *status, cudaStream_t st);
 void launch_permute_in(const double *b, double *y, const int *perm, int n, int q, cudaStream_t st);
 void launch_permute_out(const double *y, double *x, const int *perm, int n, int q, cudaStream_t st);
-void launch_forward(const int *sns, int count, const DevPlan &P, const double *Lx, double *y, double *V, double *T,
-                    int q, int64_t Vstride, int64_t Tstride, cudaStream_t st);
-void launch_backward(const int *sns, int count, const DevPlan &P, const double *Lx, double *y, int q, cudaStream_t st);
-void launch_fwd_gather(const int *sns, int count, const DevPlan &P, const double *y, double *V, const double *T, int q,
-                       int64_t Vstride, int64_t Tstride, cudaStream_t st);
 template <class TL>
-void launch_fwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const int *blkOff,
-                       const TL *Lx, double *y, double *V, double *T, int *flags, int epoch, int *done, int q,
-                       int64_t Vstride, int64_t Tstride, unsigned long long *status, cudaStream_t st);
+void launch_diag_inv(const DevPlan &P, int nblocks, const TL *Lx, TL *Inv, cudaStream_t st);
 template <class TL>
-void launch_bwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const int *blkOff,
-                       const TL *Lx, double *y, int *flags, int epoch, int q, unsigned long long *status,
-                       cudaStream_t st);
+void launch_fwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
+                       double *y, double *V, double *T, int *flags, int epoch, int *done, int q, int64_t Vstride,
+                       int64_t Tstride, unsigned long long *status, cudaStream_t st);
+template <class TL>
+void launch_bwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
+                       double *y, int *flags, int epoch, int q, unsigned long long *status, cudaStream_t st);
 
 }  // namespace amp

@@ -1,19 +1,23 @@
 // Supernodal triangular solves on sm_100a (sparse.mjs solveNumeric :1261-1305, supernodalSolve :1200-1258).
 //
-// Multifrontal vector form, one level of the supernodal tree per launch:
-//   forward (levels bottom-up)
-//     k_fwd_gather  v_s = [y(f .. f+nc); 0] + the children's pass-up vectors (extend-add in the reference's child
-//                   order; one CTA per supernode, so no atomics)
-//     k_fwd_blocks  tasks over 64-row blocks: diagonal block k computes v_k - L[k, 0:k] y(0:k) (row-block dot
-//                   products) and solves with L_kk; below block j computes the pass-up vector
-//                   u_j = v_j - L[j, 0:nc] y (read by the parent's gather)
-//   backward (levels top-down)
-//     k_bwd_blocks  column block k (reverse order): x_k = L_kk^-T (y_k - L[rows below k, k]^T x(rows)), the rows below
-//                   the supernode gathered from the ancestors' final values
-// Every L element is read once per sweep. Tasks inside a launch depend on earlier blocks of the same supernode: a
-// CTA takes the next task with an atomic ticket (so it only ever waits for tasks already taken by running or finished
-// CTAs) and waits on per-block ready flags with a bounded spin; on time-out it records AMP_DEVICE_TIMEOUT in the
-// status word and returns.
+// Multifrontal vector form, each sweep one launch over 64-row block tasks:
+//   forward (tasks listed level by level, leaves first)
+//     diagonal task (s, k)  block 0 first gathers v_s = [y(f .. f+nc); 0] + the children's pass-up vectors (extend-add
+//                           in the reference's child order); then r_k = v_k - L[k, 0:k] y(0:k) (row-block dot products)
+//                           and y_k = L_kk^-1 r_k as a 64 x 64 product with the precomputed inverse block
+//     below task (s, j)     the pass-up vector u_j = v_j - L[j, 0:nc] y (read by the parent's gather)
+//   backward (tasks listed level by level, root first; blocks of a supernode from the last down)
+//     x_k = L_kk^-T (y_k - L[rows below k, k]^T x(rows)), the rows below the supernode gathered from the ancestors'
+//     final values
+// Every L element is read once per sweep. A CTA takes the next task with an atomic ticket (so it only ever waits for
+// tasks already taken by running or finished CTAs) and waits on per-block ready flags with a bounded spin; on
+// time-out it records AMP_DEVICE_TIMEOUT in the status word and returns. The L values a task needs from a block are
+// loaded before it waits for that block's flag, so the dependency chain through a large supernode costs a flag
+// round trip, 64 y values and a 64 x 64 product per block.
+//
+// The inverses of the diagonal blocks are computed once per factorization (k_diag_inv): column j of X = L_kk^-1 by
+// forward substitution, X(j, j) = 1 / L(j, j), X(i, j) = -(sum_{t=j}^{i-1} L(i, t) X(t, j)) X(i, i). Solving with X
+// instead of by substitution changes the result by rounding only (the FP64 path stays within 1e-12 of the oracle).
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -23,7 +27,7 @@
 
 namespace amp {
 
-constexpr int kSB = 64;                 // solve block rows
+constexpr int kSB = 64;                      // solve block rows
 constexpr long long kSpinLimit = 1ll << 24;  // ~ seconds with the back-off below
 
 __device__ __forceinline__ int ld_acquire(const int *p) {
@@ -34,6 +38,9 @@ __device__ __forceinline__ int ld_acquire(const int *p) {
 __device__ __forceinline__ void st_release(int *p, int v) {
   asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ void red_release_add(int *p, int v) {
+  asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
 // Wait until flag == epoch; false on time-out (status set).
 __device__ bool wait_flag(const int *flag, int epoch, unsigned long long *status, int s) {
@@ -43,7 +50,7 @@ __device__ bool wait_flag(const int *flag, int epoch, unsigned long long *status
       atomicMin(status, status_word(0x7fffffff, 3, s));
       return false;
     }
-    __nanosleep(64);
+    __nanosleep(32);
   }
   return true;
 }
@@ -56,33 +63,43 @@ __device__ bool wait_count(const int *cnt, int need, unsigned long long *status,
       atomicMin(status, status_word(0x7fffffff, 3, s));
       return false;
     }
-    __nanosleep(64);
+    __nanosleep(32);
   }
   return true;
 }
 
-// ---- forward gather ----------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_fwd_gather(const int *__restrict__ sns, DevPlan P, const double *__restrict__ y,
-                                                    double *__restrict__ V, const double *__restrict__ T, int q,
-                                                    int64_t Vstride, int64_t Tstride) {
-  const int s = sns[blockIdx.x];
-  const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
-  for (int k = 0; k < q; k++) {
-    double *v = V + (int64_t)k * Vstride + P.Sp[s];
-    const double *yk = y + (int64_t)k * P.n;
-    for (int r = threadIdx.x; r < m; r += blockDim.x) v[r] = r < nc ? yk[f + r] : 0.0;
+// ---- inverses of the diagonal blocks -----------------------------------------------------------------------------
+// One CTA per 64-column block b of the pivot columns (all supernodes): X = L_kk^-1, w x w column-major, lower part.
+// Thread j computes column j; L is read through the read-only cache.
+template <class TL>
+__global__ void __launch_bounds__(kSB) k_diag_inv(DevPlan P, const TL *__restrict__ Lx, TL *__restrict__ Inv) {
+  __shared__ double Xs[kSB][kSB + 1];
+  __shared__ double dinv[kSB];
+  const int b = blockIdx.x;
+  int lo = 0, hi = P.nsuper;  // supernode s with blkOff[s] <= b < blkOff[s + 1]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (P.blkOff[mid] <= b) lo = mid; else hi = mid;
+  }
+  const int s = lo, c0 = (b - P.blkOff[s]) * kSB;
+  const int m = P.snM[s], w = min(kSB, P.snNc[s] - c0);
+  const TL *Lb = Lx + P.snLxp[s] + (int64_t)c0 * m + c0;  // L_kk(i, t) = Lb[t m + i]
+  const int j = threadIdx.x;
+  if (j < w) dinv[j] = 1.0 / (double)__ldg(Lb + (int64_t)j * m + j);
+  __syncthreads();
+  if (j < w) {
+    Xs[j][j] = dinv[j];
+    for (int i = j + 1; i < w; i++) {
+      double acc = 0.0;
+      for (int t = j; t < i; t++) acc += (double)__ldg(Lb + (int64_t)t * m + i) * Xs[t][j];
+      Xs[i][j] = -acc * dinv[i];
+    }
   }
   __syncthreads();
-  for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
-    const int c = P.chList[qq];
-    const int muc = P.snM[c] - P.snNc[c];
-    const int *map = P.eaMap + P.eaPtr[c];
-    for (int k = 0; k < q; k++) {
-      double *v = V + (int64_t)k * Vstride + P.Sp[s];
-      const double *tc = T + (int64_t)k * Tstride + P.snTOff[c];
-      for (int a = threadIdx.x; a < muc; a += blockDim.x) v[map[a]] += tc[a];
-    }
-    __syncthreads();
+  TL *X = Inv + P.invOff[b];
+  for (int e = threadIdx.x; e < w * w; e += kSB) {
+    const int i = e % w, jj = e / w;
+    X[e] = (TL)(i >= jj ? Xs[i][jj] : 0.0);
   }
 }
 
@@ -93,16 +110,16 @@ __global__ void __launch_bounds__(256) k_fwd_gather(const int *__restrict__ sns,
 // below tasks count themselves in done[]) and gathers its front vector; every below task counts itself when its
 // part of the pass-up vector is written.
 template <class TL>
-__global__ void __launch_bounds__(256) k_fwd_blocks(const int4 *__restrict__ tasks, int ntasks, int *__restrict__ ticket,
-                                                    DevPlan P, const int *__restrict__ blkOff,
-                                                    const TL *__restrict__ Lx, double *__restrict__ y,
-                                                    double *__restrict__ V, double *__restrict__ T,
-                                                    int *__restrict__ flags, int epoch, int *__restrict__ done,
-                                                    int q, int64_t Vstride, int64_t Tstride,
+__global__ void __launch_bounds__(256, 3) k_fwd_blocks(const int4 *__restrict__ tasks, int ntasks, int *__restrict__ ticket,
+                                                    DevPlan P, const TL *__restrict__ Lx, const TL *__restrict__ Inv,
+                                                    double *__restrict__ y, double *__restrict__ V,
+                                                    double *__restrict__ T, int *__restrict__ flags, int epoch,
+                                                    int *__restrict__ done, int q, int64_t Vstride, int64_t Tstride,
                                                     unsigned long long *status) {
   __shared__ int tk, waitOk;
   __shared__ double red[4][kSB];
-  __shared__ double Lkk[kSB][kSB + 1];
+  __shared__ double rk[kSB];
+  __shared__ double Xs[kSB][kSB + 1];
   if (threadIdx.x == 0) tk = atomicAdd(ticket, 1);
   __syncthreads();
   if (tk >= ntasks) return;
@@ -114,7 +131,12 @@ __global__ void __launch_bounds__(256) k_fwd_blocks(const int4 *__restrict__ tas
   const int rows = below ? min(kSB, mu - blk * kSB) : min(kSB, nc - blk * kSB);
   const int ncols = below ? nc : blk * kSB;  // columns of L to the left of the diagonal block / all pivot columns
   const int tid = threadIdx.x, row = tid & (kSB - 1), part = tid >> 6;
-  int *myflags = flags + blkOff[s];
+  const bool rowok = row < rows;
+  int *myflags = flags + P.blkOff[s];
+  if (!below) {  // inverse of the diagonal block, needed at the end
+    const TL *X = Inv + P.invOff[P.blkOff[s] + blk];
+    for (int e = tid; e < rows * rows; e += blockDim.x) Xs[e % rows][e / rows] = (double)X[e];
+  }
   if (!below && blk == 0) {
     // children's pass-up vectors complete?
     for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
@@ -143,63 +165,70 @@ __global__ void __launch_bounds__(256) k_fwd_blocks(const int4 *__restrict__ tas
       __syncthreads();
     }
   }
+  const int ncb = (ncols + kSB - 1) / kSB;
   for (int k = 0; k < q; k++) {
     const double *yk = y + (int64_t)k * P.n + f;
-    double acc = 0.0;
-    // row-block dot products over the columns of the blocks this one depends on, waiting for each block
-    for (int cb = 0; cb * kSB < ncols; cb++) {
+    double acc = 0.0, vreg = 0.0;
+    // v rows of this block: final once the supernode's first diagonal block is (it gathers them)
+    auto loadV = [&] {
+      if (tid < rows) vreg = __ldcg(V + (int64_t)k * Vstride + P.Sp[s] + r0 + tid);
+    };
+    if (ncb == 0 || k > 0) loadV();
+    // row-block dot products over the columns of the blocks this one depends on; the L values of a block are loaded
+    // before waiting for its flag (thread: row `row`, columns part, part + 4, ... of the block)
+    TL lv[16];
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+      const int c = part + 4 * u;
+      lv[u] = (rowok && c < ncols) ? Lp[(int64_t)c * m + r0 + row] : (TL)0;
+    }
+    for (int cb = 0; cb < ncb; cb++) {
+      TL ln[16];
+      const int cn = (cb + 1) * kSB;
+#pragma unroll
+      for (int u = 0; u < 16; u++) {
+        const int c = cn + part + 4 * u;
+        ln[u] = (rowok && c < ncols) ? Lp[(int64_t)c * m + r0 + row] : (TL)0;
+      }
       if (k == 0) {
         if (tid == 0) waitOk = wait_flag(myflags + cb, epoch, status, s);
         __syncthreads();
         if (!waitOk) return;  // block-uniform
+        if (cb == 0) loadV();
       }
-      const int c1 = min(ncols, (cb + 1) * kSB);
-      if (row < rows)
-        for (int c = cb * kSB + part; c < c1; c += 4) acc += (double)Lp[(int64_t)c * m + r0 + row] * __ldcg(yk + c);
+      const int cbase = cb * kSB;
+#pragma unroll
+      for (int u = 0; u < 16; u++) {
+        const int c = cbase + part + 4 * u;
+        if (c < ncols) acc += (double)lv[u] * __ldcg(yk + c);
+      }
+#pragma unroll
+      for (int u = 0; u < 16; u++) lv[u] = ln[u];
     }
     red[part][row] = acc;
     __syncthreads();
     if (tid < kSB) {
-      double sum = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
-      const double *vk = V + (int64_t)k * Vstride + P.Sp[s];
-      red[0][tid] = tid < rows ? __ldcg(vk + r0 + tid) - sum : 0.0;
+      const double sum = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
+      rk[tid] = tid < rows ? vreg - sum : 0.0;
     }
     __syncthreads();
     if (below) {
       double *tk_out = T + (int64_t)k * Tstride + P.snTOff[s];
-      if (tid < rows) tk_out[blk * kSB + tid] = red[0][tid];
+      if (tid < rows) tk_out[blk * kSB + tid] = rk[tid];
     } else {
-      // solve L_kk y_k = v_k with one warp: lane i owns rows i and i + 32
-      if (k == 0) {
-        for (int e = tid; e < rows * rows; e += blockDim.x) {
-          int i = e % rows, j = e / rows;
-          if (i >= j) Lkk[i][j] = (double)Lp[(int64_t)(r0 + j) * m + r0 + i];
-        }
-        __syncthreads();
-      }
-      if (tid < 32) {
-        double v0 = red[0][tid], v1 = red[0][tid + 32];
-        for (int j = 0; j < rows; j++) {
-          double vj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
-          double yj = vj / Lkk[j][j];
-          if (tid == (j & 31)) {
-            if (j < 32) v0 = yj; else v1 = yj;
-          }
-          if (tid > j && tid < rows) v0 -= Lkk[tid][j] * yj;
-          if (tid + 32 > j && tid + 32 < rows) v1 -= Lkk[tid + 32][j] * yj;
-        }
-        double *yo = y + (int64_t)k * P.n + f + r0;
-        if (tid < rows) yo[tid] = v0;
-        if (tid + 32 < rows) yo[tid + 32] = v1;
-      }
+      // y_k = X r_k, X = L_kk^-1 lower triangular: thread (row, part) sums columns part, part + 4, ... <= row
+      double a2 = 0.0;
+      if (rowok)
+        for (int c = part; c <= row; c += 4) a2 += Xs[row][c] * rk[c];
+      red[part][row] = a2;
       __syncthreads();
+      if (tid < rows) y[(int64_t)k * P.n + f + r0 + tid] = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
     }
+    __syncthreads();
   }
-  __syncthreads();
-  if (tid == 0) {
-    __threadfence();
+  if (tid == 0) {  // after the barrier: the CTA's stores are ordered before the release / the counted arrival
     if (below)
-      atomicAdd(done + s, 1);
+      red_release_add(done + s, 1);
     else
       st_release(myflags + blk, epoch);
   }
@@ -207,15 +236,24 @@ __global__ void __launch_bounds__(256) k_fwd_blocks(const int4 *__restrict__ tas
 
 // ---- backward block tasks ----------------------------------------------------------------------------------------
 // task: .x supernode, .y column block (tasks of a supernode listed from the last block down)
+// r_k = y_k - L[rows below the block, k]^T x(rows): the rows below the supernode (ancestors, final once the parent's
+// first pivot block is) and the later pivot blocks except the next one accumulate in registers (warps own columns,
+// lanes walk rows) and are reduced before the last wait; the next block's L tile is staged in shared memory and
+// read column-wise after its flag, so the chain step is a 64 x 64 product, a reduction and the inverse product.
+constexpr int kBwdSmem = 2 * kSB * (kSB + 1) * (int)sizeof(double);
 template <class TL>
-__global__ void __launch_bounds__(256) k_bwd_blocks(const int4 *__restrict__ tasks, int ntasks, int *__restrict__ ticket,
-                                                    DevPlan P, const int *__restrict__ blkOff,
-                                                    const TL *__restrict__ Lx, double *__restrict__ y,
-                                                    int *__restrict__ flags, int epoch, int q,
+__global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ tasks, int ntasks, int *__restrict__ ticket,
+                                                    DevPlan P, const TL *__restrict__ Lx, const TL *__restrict__ Inv,
+                                                    double *__restrict__ y, int *__restrict__ flags, int epoch, int q,
                                                     unsigned long long *status) {
   __shared__ int tk, waitOk;
-  __shared__ double red[8][kSB];
-  __shared__ double Lkk[kSB][kSB + 1];
+  __shared__ double red[4][kSB];
+  __shared__ double red0[kSB];
+  __shared__ double xs[kSB];
+  __shared__ double rk[kSB];
+  extern __shared__ double bwd_dyn[];
+  double(*Xs)[kSB + 1] = reinterpret_cast<double(*)[kSB + 1]>(bwd_dyn);            // L_kk^-1
+  double(*Lf)[kSB + 1] = reinterpret_cast<double(*)[kSB + 1]>(bwd_dyn + kSB * (kSB + 1));  // next block, [row][col]
   if (threadIdx.x == 0) tk = atomicAdd(ticket, 1);
   __syncthreads();
   if (tk >= ntasks) return;
@@ -226,18 +264,28 @@ __global__ void __launch_bounds__(256) k_bwd_blocks(const int4 *__restrict__ tas
   const int *rowsOf = P.Si + P.Sp[s];
   const int c0 = blk * kSB, w = min(kSB, nc - c0), nb = (nc + kSB - 1) / kSB;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  int *myflags = flags + blkOff[s];
+  const bool hasNext = blk + 1 < nb;
+  const int rn = (blk + 1) * kSB, wn = hasNext ? min(kSB, nc - rn) : 0;  // the next pivot block: rows [rn, rn + wn)
+  int *myflags = flags + P.blkOff[s];
+  {
+    const TL *X = Inv + P.invOff[P.blkOff[s] + blk];
+    for (int e = tid; e < w * w; e += blockDim.x) Xs[e % w][e / w] = (double)X[e];
+    // next block's tile: Lf[r][c] = L(rn + r, c0 + c); coalesced along r
+    for (int e = tid; e < kSB * kSB; e += blockDim.x) {
+      const int r = e & (kSB - 1), c = e >> 6;
+      Lf[r][c] = (r < wn && c < w) ? (double)Lp[(int64_t)(c0 + c) * m + rn + r] : 0.0;
+    }
+  }
   // one launch for the whole sweep (levels top-down): the rows below this supernode are final once its parent's
   // first pivot block (the parent's last backward task) is
   const int par = P.snParent[s];
   if (par >= 0) {
-    if (tid == 0) waitOk = wait_flag(flags + blkOff[par], epoch, status, s);
+    if (tid == 0) waitOk = wait_flag(flags + P.blkOff[par], epoch, status, s);
     __syncthreads();
     if (!waitOk) return;
   }
   for (int k = 0; k < q; k++) {
     double *yk = y + (int64_t)k * P.n;
-    // each warp owns columns c0 + warp, c0 + warp + 8, ...; lanes walk the rows below the diagonal block
     double acc[8];
 #pragma unroll
     for (int u = 0; u < 8; u++) acc[u] = 0.0;
@@ -250,90 +298,117 @@ __global__ void __launch_bounds__(256) k_bwd_blocks(const int4 *__restrict__ tas
         if (c < w) acc[u] += (double)Lp[(int64_t)(c0 + c) * m + r] * xr;
       }
     }
-    // later pivot blocks of this supernode, as they become final
-    for (int rb = nb - 1; rb > blk; rb--) {
+    // pivot blocks after the next one, as they become final; a block's L values are loaded before its wait
+    TL lv[2][8];
+    auto load_block = [&](int rb, TL (&dst)[2][8]) {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int r = rb * kSB + lane + 32 * h;
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const int c = warp + 8 * u;
+          dst[h][u] = (rb > blk + 1 && r < nc && c < w) ? Lp[(int64_t)(c0 + c) * m + r] : (TL)0;
+        }
+      }
+    };
+    load_block(nb - 1, lv);
+    for (int rb = nb - 1; rb > blk + 1; rb--) {
+      TL ln[2][8];
+      load_block(rb - 1, ln);
       if (k == 0) {
         if (tid == 0) waitOk = wait_flag(myflags + rb, epoch, status, s);
         __syncthreads();
         if (!waitOk) return;  // block-uniform
       }
-      const int rr1 = min(nc, (rb + 1) * kSB);
-      for (int r = rb * kSB + lane; r < rr1; r += 32) {
-        const double xr = __ldcg(yk + f + r);
 #pragma unroll
-        for (int u = 0; u < 8; u++) {
-          const int c = warp + 8 * u;
-          if (c < w) acc[u] += (double)Lp[(int64_t)(c0 + c) * m + r] * xr;
-        }
+      for (int h = 0; h < 2; h++) {
+        const int r = rb * kSB + lane + 32 * h;
+        const double xr = r < nc ? __ldcg(yk + f + r) : 0.0;
+#pragma unroll
+        for (int u = 0; u < 8; u++) acc[u] += (double)lv[h][u] * xr;
       }
+#pragma unroll
+      for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int u = 0; u < 8; u++) lv[h][u] = ln[h][u];
     }
 #pragma unroll
     for (int u = 0; u < 8; u++) {
       double v = acc[u];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-      if (lane == 0) red[0][warp + 8 * u] = v;
+      if (lane == 0) red0[warp + 8 * u] = v;
     }
-    if (k == 0) {
-      for (int e = tid; e < w * w; e += blockDim.x) {
-        int i = e % w, j = e / w;
-        if (i >= j) Lkk[i][j] = (double)Lp[(int64_t)(c0 + j) * m + c0 + i];
-      }
+    double yv = 0.0;
+    if (tid < w) yv = yk[f + c0 + tid];
+    // the chain step: wait for the next block, then its contribution from the staged tile
+    if (hasNext && k == 0) {
+      if (tid == 0) waitOk = wait_flag(myflags + blk + 1, epoch, status, s);
+      __syncthreads();
+      if (!waitOk) return;  // block-uniform
+    }
+    if (tid < kSB) xs[tid] = tid < wn ? __ldcg(yk + f + rn + tid) : 0.0;
+    __syncthreads();
+    {
+      const int c = tid & (kSB - 1), part = tid >> 6;
+      double a2 = 0.0;
+#pragma unroll 4
+      for (int r = part; r < wn; r += 4) a2 += Lf[r][c] * xs[r];
+      red[part][c] = a2;
     }
     __syncthreads();
-    // x_k = L_kk^-T (y_k - sum): upper-triangular solve with one warp, rows i and i + 32 per lane
-    if (tid < 32) {
-      double *yb = yk + f + c0;
-      double w0 = tid < w ? yb[tid] - red[0][tid] : 0.0;
-      double w1 = tid + 32 < w ? yb[tid + 32] - red[0][tid + 32] : 0.0;
-      for (int j = w - 1; j >= 0; j--) {
-        double wj = __shfl_sync(0xffffffffu, j < 32 ? w0 : w1, j & 31);
-        double xj = wj / Lkk[j][j];
-        if (tid == (j & 31)) {
-          if (j < 32) w0 = xj; else w1 = xj;
-        }
-        if (tid < j) w0 -= Lkk[j][tid] * xj;
-        if (tid + 32 < j) w1 -= Lkk[j][tid + 32] * xj;
-      }
-      if (tid < w) yb[tid] = w0;
-      if (tid + 32 < w) yb[tid + 32] = w1;
+    if (tid < kSB)
+      rk[tid] = tid < w ? yv - red0[tid] - ((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid])) : 0.0;
+    __syncthreads();
+    // x_k = X^T r_k, X = L_kk^-1 lower triangular: thread (row i, part) sums X(j, i) r(j) over j = i + part, +4 ...
+    {
+      const int i = tid & (kSB - 1), part = tid >> 6;
+      double a2 = 0.0;
+      if (i < w)
+        for (int j = i + part; j < w; j += 4) a2 += Xs[j][i] * rk[j];
+      red[part][i] = a2;
     }
     __syncthreads();
+    if (tid < w) yk[f + c0 + tid] = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
+    __syncthreads();
   }
-  if (tid == 0) {
-    __threadfence();
-    st_release(myflags + blk, epoch);
-  }
+  if (tid == 0) st_release(myflags + blk, epoch);  // after the barrier: the CTA's stores of x_k are ordered before
 }
 
-void launch_fwd_gather(const int *sns, int count, const DevPlan &P, const double *y, double *V, const double *T, int q,
-                       int64_t Vstride, int64_t Tstride, cudaStream_t st) {
-  if (count > 0) k_fwd_gather<<<count, 256, 0, st>>>(sns, P, y, V, T, q, Vstride, Tstride);
+void init_solve_attributes() {
+  cudaFuncSetAttribute(k_bwd_blocks<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBwdSmem);
+  cudaFuncSetAttribute(k_bwd_blocks<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBwdSmem);
+}
+
+template <class TL>
+void launch_diag_inv(const DevPlan &P, int nblocks, const TL *Lx, TL *Inv, cudaStream_t st) {
+  if (nblocks > 0) k_diag_inv<TL><<<nblocks, kSB, 0, st>>>(P, Lx, Inv);
 }
 template <class TL>
-void launch_fwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const int *blkOff,
-                       const TL *Lx, double *y, double *V, double *T, int *flags, int epoch, int *done, int q,
-                       int64_t Vstride, int64_t Tstride, unsigned long long *status, cudaStream_t st) {
+void launch_fwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
+                       double *y, double *V, double *T, int *flags, int epoch, int *done, int q, int64_t Vstride,
+                       int64_t Tstride, unsigned long long *status, cudaStream_t st) {
   if (ntasks > 0)
-    k_fwd_blocks<TL><<<ntasks, 256, 0, st>>>(tasks, ntasks, ticket, P, blkOff, Lx, y, V, T, flags, epoch, done, q,
+    k_fwd_blocks<TL><<<ntasks, 256, 0, st>>>(tasks, ntasks, ticket, P, Lx, Inv, y, V, T, flags, epoch, done, q,
                                              Vstride, Tstride, status);
 }
 template <class TL>
-void launch_bwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const int *blkOff,
-                       const TL *Lx, double *y, int *flags, int epoch, int q, unsigned long long *status,
-                       cudaStream_t st) {
+void launch_bwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
+                       double *y, int *flags, int epoch, int q, unsigned long long *status, cudaStream_t st) {
   if (ntasks > 0)
-    k_bwd_blocks<TL><<<ntasks, 256, 0, st>>>(tasks, ntasks, ticket, P, blkOff, Lx, y, flags, epoch, q, status);
+    k_bwd_blocks<TL><<<ntasks, 256, kBwdSmem, st>>>(tasks, ntasks, ticket, P, Lx, Inv, y, flags, epoch, q, status);
 }
-template void launch_fwd_blocks<double>(const int4 *, int, int *, const DevPlan &, const int *, const double *,
+template void launch_diag_inv<double>(const DevPlan &, int, const double *, double *, cudaStream_t);
+template void launch_diag_inv<float>(const DevPlan &, int, const float *, float *, cudaStream_t);
+template void launch_fwd_blocks<double>(const int4 *, int, int *, const DevPlan &, const double *, const double *,
                                         double *, double *, double *, int *, int, int *, int, int64_t, int64_t,
                                         unsigned long long *, cudaStream_t);
-template void launch_fwd_blocks<float>(const int4 *, int, int *, const DevPlan &, const int *, const float *, double *,
-                                       double *, double *, int *, int, int *, int, int64_t, int64_t,
+template void launch_fwd_blocks<float>(const int4 *, int, int *, const DevPlan &, const float *, const float *,
+                                       double *, double *, double *, int *, int, int *, int, int64_t, int64_t,
                                        unsigned long long *, cudaStream_t);
-template void launch_bwd_blocks<double>(const int4 *, int, int *, const DevPlan &, const int *, const double *,
+template void launch_bwd_blocks<double>(const int4 *, int, int *, const DevPlan &, const double *, const double *,
                                         double *, int *, int, int, unsigned long long *, cudaStream_t);
-template void launch_bwd_blocks<float>(const int4 *, int, int *, const DevPlan &, const int *, const float *, double *,
-                                       int *, int, int, unsigned long long *, cudaStream_t);
+template void launch_bwd_blocks<float>(const int4 *, int, int *, const DevPlan &, const float *, const float *,
+                                       double *, int *, int, int, unsigned long long *, cudaStream_t);
 
 }  // namespace amp

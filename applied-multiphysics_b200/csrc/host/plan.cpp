@@ -269,6 +269,12 @@ void build_plan(const Symbolic &S, Plan &P) {
   P.blkOff.assign(ns + 1, 0);
   for (int s = 0; s < ns; s++) P.blkOff[s + 1] = P.blkOff[s] + (P.snNc[s] + B - 1) / B;
   P.nflags = P.blkOff[ns];
+  P.invOff.assign(P.nflags + 1, 0);
+  for (int s = 0; s < ns; s++)
+    for (int b = 0; b * B < P.snNc[s]; b++) {
+      const int64_t w = std::min(B, P.snNc[s] - b * B);
+      P.invOff[P.blkOff[s] + b + 1] = P.invOff[P.blkOff[s] + b] + w * w;
+    }
   P.fwdLvlPtr.assign(P.nlevels + 1, 0);
   P.bwdLvlPtr.assign(P.nlevels + 1, 0);
   auto push = [](std::vector<int> &v, int a, int b, int c) {

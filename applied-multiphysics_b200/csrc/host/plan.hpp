@@ -91,6 +91,7 @@ struct Plan {
   // block tasks of the solves ({supernode, block, kind, 0}); ready flags per 64-row pivot block
   std::vector<int> blkOff;          // first flag of supernode s
   int nflags = 0;
+  std::vector<int64_t> invOff;      // per diagonal block (flag index): offset of its w x w inverse; [nflags] = total
   std::vector<int> fwdTasks, bwdTasks;  // int4 records, flattened
   std::vector<int> fwdLvlPtr, bwdLvlPtr;
   std::vector<int> bwdAll;  // backward tasks of all levels, top-down (one launch)
