@@ -26,9 +26,9 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "applied-multiphysics_b200"))
 
-METRIC = "factor+solve TFLOP/s to rel. residual <= 1e-12 (3D P1 elasticity 40^3, 1 x B200)"
+METRIC = "factor+solve TFLOP/s to rel. residual <= 1e-12 (3D P1 elasticity {N}^3, 1 x B200)"
 UNIT = "TFLOP/s"
-WORKLOAD = "elastic3d-40: 3D P1 linear elasticity, 40^3 hexes x 6 tets, E=1 nu=0.3, x=0 clamped, nd3Order"
+WORKLOAD = "elastic3d-{N}: 3D P1 linear elasticity, {N}^3 hexes x 6 tets, E=1 nu=0.3, x=0 clamped, nd3Order"
 
 
 def peaks():
@@ -90,14 +90,34 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_system():
+def make_system(size: int = 40):
     import workloads as wl
-    return wl.elastic3d(40, seed=2, q=1)
+    return wl.elastic3d(size, seed=2, q=1)
 
 
 def measure_dgemm(torch):
     """cuBLAS DGEMM 8192^3 (the FP64 roofline denominator; no FP64 figure is in MEASURED_PEAKS.json)."""
     a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    b = torch.randn_like(a)
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        a @ b
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 5
+    del a, b
+    torch.cuda.empty_cache()
+    return 2 * 8192 ** 3 / ms / 1e9
+
+
+def measure_sgemm(torch):
+    """cuBLAS SGEMM 8192^3 with TF32 off: the FP32 CUDA-core denominator for the FP32 panel kernel."""
+    torch.backends.cuda.matmul.allow_tf32 = False
+    a = torch.randn(8192, 8192, dtype=torch.float32, device="cuda")
     b = torch.randn_like(a)
     for _ in range(2):
         a @ b
@@ -152,7 +172,7 @@ def run_reference(args, rank):
     if rank != 0:
         return
     import workloads as wl  # noqa: F401
-    w = make_system()
+    w = make_system(args.size)
     import ampsolve as amp
     try:
         perm = amp.nd3Order(w.pat, w.x, w.y, w.z)
@@ -167,10 +187,11 @@ def run_reference(args, rank):
             vals.append(cb["value"])
             times.append(0)
     v = float(np.median(vals))
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+    line = {"impl": "reference", "metric": METRIC.format(N=args.size), "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n": w.n, "nnz": w.pat.nnz, "sample": cb["sample"]},
+            "config": {"workload": WORKLOAD.format(N=args.size), "n": w.n, "nnz": w.pat.nnz, "sample": cb["sample"]},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": cb["sample"]},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -182,8 +203,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "both"])
+    ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--size", type=int, default=40, help="hexes per side (40 = the benchmark; smaller for profiling)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -200,7 +222,7 @@ def main():
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    w = make_system()
+    w = make_system(args.size)
     n = w.n
     t0 = time.perf_counter()
     sym = amp.analyze(w.pat, ordering="nd3", x=w.x, y=w.y, z=w.z, device=local)
@@ -250,10 +272,13 @@ def main():
         for k in range(max(2, args.steps)):
             flush.zero_()
             torch.cuda.synchronize()
-            t = time.perf_counter()
-            num.factor(vals_h.numpy())
-            rr, ss = num.solve_refined_host_pinned(b_h.data_ptr(), x_h.data_ptr(), 1, 10, 1e-12)
-            e2e.append((time.perf_counter() - t) * 1e3)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            num.factor(vals_h.numpy())  # H2D of the values inside the call
+            rr, ss = num.solve_refined_host_pinned(b_h.data_ptr(), x_h.data_ptr(), 1, 10, 1e-12)  # H2D b, D2H x
+            b.record()
+            torch.cuda.synchronize()
+            e2e.append(a.elapsed_time(b))
         e2e_ms = float(np.mean(e2e[1:])) if len(e2e) > 1 else e2e[0]
         if world > 1:
             t = torch.tensor([e2e_ms], device=dev)
@@ -265,7 +290,7 @@ def main():
         num.solve_refined_device(b_d.data_ptr(), x_d.data_ptr(), 1, maxSteps=10, tol=1e-12)
         prof = num.profile_read()
         num.profile(False)
-        work = flops_factor + flops_solve * (1 + irs)
+        work = flops_factor + flops_solve  # the same algorithmic work for both precisions: factor + one solve
         results[prec] = {"ok": ok, "ms": ms, "relres": relres, "ir_steps": irs, "work": work, "clk": clk.summary(),
                          "prof": prof, "e2e_ms": e2e_ms, "factor_ms": num.ms}
         del num
@@ -278,11 +303,14 @@ def main():
     pk = peaks()
     dom = max(R["prof"], key=lambda k: k["ms"])
     fp64_peak = measure_dgemm(torch)
-    if head == "fp64":
-        peak, bound, punit, note = fp64_peak, "tensor", "TFLOP/s", "measured cuBLAS DGEMM 8192^3 in this run"
-    else:
+    fp32_peak = measure_sgemm(torch)
+    if dom["flops"] > 0 and dom["name"] == "update_syrk" and head == "mixed":
         peak, bound, punit, note = pk.get("bf16_tflops_sustained", 1400.0), "tensor", "TFLOP/s", \
-            "MEASURED_PEAKS.json bf16_tflops_sustained (BF16 tensor, 3 products per FP32 update)"
+            "MEASURED_PEAKS.json bf16_tflops_sustained (BF16 tensor; 3 products per FP32 update counted once)"
+    elif dom["flops"] > 0 and head == "mixed":
+        peak, bound, punit, note = fp32_peak, "tensor", "TFLOP/s", "measured cuBLAS SGEMM 8192^3 (no TF32) in this run"
+    elif dom["flops"] > 0:
+        peak, bound, punit, note = fp64_peak, "tensor", "TFLOP/s", "measured cuBLAS DGEMM 8192^3 in this run"
     if dom["flops"] > 0:
         achieved = dom["flops"] / (dom["ms"] * 1e-3) / 1e12
     else:
@@ -291,10 +319,12 @@ def main():
     launches = sum(k["launches"] for k in R["prof"])
     value = world * R["work"] / (R["ms"] * 1e-3) / 1e12
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "metric": METRIC.format(N=args.size), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup,
         "ms_per_step": R["ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if head == "fp64" else "f32+bf16x3 (f64 refinement)", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n": n, "nnz": w.pat.nnz, "nnzL": sym.nnzL, "flops_factor": flops_factor,
+        "config": {"workload": WORKLOAD.format(N=args.size), "n": n, "nnz": w.pat.nnz, "nnzL": sym.nnzL,
+                   "flops_factor": flops_factor,
                    "maxFront": sym.maxFront, "nsuper": sym.nsuper, "levels": sym.nlevels, "precision": head,
                    "l2": "flushed between timed steps (256 MB write)", "parallelism": "replicas" if world > 1 else "1 gpu",
                    "symbolic_ms": symbolic_ms},
@@ -308,6 +338,7 @@ def main():
                      "frac": achieved / peak, "traffic": None, "peak_source": note},
         "kernels": R["prof"],
         "fp64_dgemm_tflops": fp64_peak,
+        "fp32_sgemm_tflops": fp32_peak,
     }
     for p, r in results.items():
         line[p] = {"ms_per_step": r["ms"], "value": world * r["work"] / (r["ms"] * 1e-3) / 1e12, "relres": r["relres"],
