@@ -9,11 +9,11 @@
 //   backward (tasks listed level by level, root first; blocks of a supernode from the last down)
 //     x_k = L_kk^-T (y_k - L[rows below k, k]^T x(rows)), the rows below the supernode gathered from the ancestors'
 //     final values
-// Every L element is read once per sweep. A CTA takes the next task with an atomic ticket (so it only ever waits for
-// tasks already taken by running or finished CTAs) and waits on per-block ready flags with a bounded spin; on
-// time-out it records AMP_DEVICE_TIMEOUT in the status word and returns. The L values a task needs from a block are
-// loaded before it waits for that block's flag, so the dependency chain through a large supernode costs a flag
-// round trip, 64 y values and a 64 x 64 product per block.
+// Every L element is read once per sweep. Persistent CTAs (3 per SM) take the next task with an atomic ticket (so a
+// task only ever waits for tasks already taken by running or finished CTAs) and wait on per-block ready flags with a
+// bounded spin; on time-out a CTA records AMP_DEVICE_TIMEOUT in the status word and returns. The L values a task
+// needs from a block are loaded before it waits for that block's flag, so the dependency chain through a large
+// supernode costs a flag round trip, 64 y values and a 64 x 64 product per block.
 //
 // The inverses of the diagonal blocks are computed once per factorization (k_diag_inv): column j of X = L_kk^-1 by
 // forward substitution, X(j, j) = 1 / L(j, j), X(i, j) = -(sum_{t=j}^{i-1} L(i, t) X(t, j)) X(i, i). Solving with X
@@ -120,117 +120,125 @@ __global__ void __launch_bounds__(256, 3) k_fwd_blocks(const int4 *__restrict__ 
   __shared__ double red[4][kSB];
   __shared__ double rk[kSB];
   __shared__ double Xs[kSB][kSB + 1];
-  if (threadIdx.x == 0) tk = atomicAdd(ticket, 1);
-  __syncthreads();
-  if (tk >= ntasks) return;
-  const int4 t = tasks[tk];
-  const int s = t.x, blk = t.y, below = t.z;
-  const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s], mu = m - nc;
-  const TL *Lp = Lx + P.snLxp[s];
-  const int r0 = below ? nc + blk * kSB : blk * kSB;
-  const int rows = below ? min(kSB, mu - blk * kSB) : min(kSB, nc - blk * kSB);
-  const int ncols = below ? nc : blk * kSB;  // columns of L to the left of the diagonal block / all pivot columns
-  const int tid = threadIdx.x, row = tid & (kSB - 1), part = tid >> 6;
-  const bool rowok = row < rows;
-  int *myflags = flags + P.blkOff[s];
-  if (!below) {  // inverse of the diagonal block, needed at the end
-    const TL *X = Inv + P.invOff[P.blkOff[s] + blk];
-    for (int e = tid; e < rows * rows; e += blockDim.x) Xs[e % rows][e / rows] = (double)X[e];
-  }
-  if (!below && blk == 0) {
-    // children's pass-up vectors complete?
-    for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
-      const int c = P.chList[qq];
-      const int need = (P.snM[c] - P.snNc[c] + kSB - 1) / kSB;
-      if (tid == 0) waitOk = wait_count(done + c, need, status, s);
-      __syncthreads();
-      if (!waitOk) return;
+  // persistent: take tickets until the list is exhausted (a task only waits for earlier tickets)
+  auto run = [&](const int tkv) -> bool {
+    const int4 t = tasks[tkv];
+    const int s = t.x, blk = t.y, below = t.z;
+    const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s], mu = m - nc;
+    const TL *Lp = Lx + P.snLxp[s];
+    const int r0 = below ? nc + blk * kSB : blk * kSB;
+    const int rows = below ? min(kSB, mu - blk * kSB) : min(kSB, nc - blk * kSB);
+    const int ncols = below ? nc : blk * kSB;  // columns of L to the left of the diagonal block / all pivot columns
+    const int tid = threadIdx.x, row = tid & (kSB - 1), part = tid >> 6;
+    const bool rowok = row < rows;
+    int *myflags = flags + P.blkOff[s];
+    if (!below) {  // inverse of the diagonal block, needed at the end
+      const TL *X = Inv + P.invOff[P.blkOff[s] + blk];
+      for (int e = tid; e < rows * rows; e += blockDim.x) Xs[e % rows][e / rows] = (double)X[e];
     }
-    // gather v_s = [y(f .. f + nc); 0] + children's pass-up vectors (the reference's child order)
-    for (int k = 0; k < q; k++) {
-      double *v = V + (int64_t)k * Vstride + P.Sp[s];
-      const double *yk = y + (int64_t)k * P.n;
-      for (int r = tid; r < m; r += blockDim.x) v[r] = r < nc ? yk[f + r] : 0.0;
-    }
-    __syncthreads();
-    for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
-      const int c = P.chList[qq];
-      const int muc = P.snM[c] - P.snNc[c];
-      const int *map = P.eaMap + P.eaPtr[c];
+    if (!below && blk == 0) {
+      // children's pass-up vectors complete?
+      for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
+        const int c = P.chList[qq];
+        const int need = (P.snM[c] - P.snNc[c] + kSB - 1) / kSB;
+        if (tid == 0) waitOk = wait_count(done + c, need, status, s);
+        __syncthreads();
+        if (!waitOk) return false;
+      }
+      // gather v_s = [y(f .. f + nc); 0] + children's pass-up vectors (the reference's child order)
       for (int k = 0; k < q; k++) {
         double *v = V + (int64_t)k * Vstride + P.Sp[s];
-        const double *tc = T + (int64_t)k * Tstride + P.snTOff[c];
-        for (int a = tid; a < muc; a += blockDim.x) v[map[a]] += __ldcg(tc + a);
+        const double *yk = y + (int64_t)k * P.n;
+        for (int r = tid; r < m; r += blockDim.x) v[r] = r < nc ? yk[f + r] : 0.0;
       }
       __syncthreads();
-    }
-  }
-  const int ncb = (ncols + kSB - 1) / kSB;
-  for (int k = 0; k < q; k++) {
-    const double *yk = y + (int64_t)k * P.n + f;
-    double acc = 0.0, vreg = 0.0;
-    // v rows of this block: final once the supernode's first diagonal block is (it gathers them)
-    auto loadV = [&] {
-      if (tid < rows) vreg = __ldcg(V + (int64_t)k * Vstride + P.Sp[s] + r0 + tid);
-    };
-    if (ncb == 0 || k > 0) loadV();
-    // row-block dot products over the columns of the blocks this one depends on; the L values of a block are loaded
-    // before waiting for its flag (thread: row `row`, columns part, part + 4, ... of the block)
-    TL lv[16];
-#pragma unroll
-    for (int u = 0; u < 16; u++) {
-      const int c = part + 4 * u;
-      lv[u] = (rowok && c < ncols) ? Lp[(int64_t)c * m + r0 + row] : (TL)0;
-    }
-    for (int cb = 0; cb < ncb; cb++) {
-      TL ln[16];
-      const int cn = (cb + 1) * kSB;
-#pragma unroll
-      for (int u = 0; u < 16; u++) {
-        const int c = cn + part + 4 * u;
-        ln[u] = (rowok && c < ncols) ? Lp[(int64_t)c * m + r0 + row] : (TL)0;
-      }
-      if (k == 0) {
-        if (tid == 0) waitOk = wait_flag(myflags + cb, epoch, status, s);
+      for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
+        const int c = P.chList[qq];
+        const int muc = P.snM[c] - P.snNc[c];
+        const int *map = P.eaMap + P.eaPtr[c];
+        for (int k = 0; k < q; k++) {
+          double *v = V + (int64_t)k * Vstride + P.Sp[s];
+          const double *tc = T + (int64_t)k * Tstride + P.snTOff[c];
+          for (int a = tid; a < muc; a += blockDim.x) v[map[a]] += __ldcg(tc + a);
+        }
         __syncthreads();
-        if (!waitOk) return;  // block-uniform
-        if (cb == 0) loadV();
       }
-      const int cbase = cb * kSB;
-#pragma unroll
+    }
+    const int ncb = (ncols + kSB - 1) / kSB;
+    for (int k = 0; k < q; k++) {
+      const double *yk = y + (int64_t)k * P.n + f;
+      double acc = 0.0, vreg = 0.0;
+      // v rows of this block: final once the supernode's first diagonal block is (it gathers them)
+      auto loadV = [&] {
+        if (tid < rows) vreg = __ldcg(V + (int64_t)k * Vstride + P.Sp[s] + r0 + tid);
+      };
+      if (ncb == 0 || k > 0) loadV();
+      // row-block dot products over the columns of the blocks this one depends on; the L values of a block are loaded
+      // before waiting for its flag (thread: row `row`, columns part, part + 4, ... of the block)
+      TL lv[16];
+  #pragma unroll
       for (int u = 0; u < 16; u++) {
-        const int c = cbase + part + 4 * u;
-        if (c < ncols) acc += (double)lv[u] * __ldcg(yk + c);
+        const int c = part + 4 * u;
+        lv[u] = (rowok && c < ncols) ? Lp[(int64_t)c * m + r0 + row] : (TL)0;
       }
-#pragma unroll
-      for (int u = 0; u < 16; u++) lv[u] = ln[u];
-    }
-    red[part][row] = acc;
-    __syncthreads();
-    if (tid < kSB) {
-      const double sum = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
-      rk[tid] = tid < rows ? vreg - sum : 0.0;
-    }
-    __syncthreads();
-    if (below) {
-      double *tk_out = T + (int64_t)k * Tstride + P.snTOff[s];
-      if (tid < rows) tk_out[blk * kSB + tid] = rk[tid];
-    } else {
-      // y_k = X r_k, X = L_kk^-1 lower triangular: thread (row, part) sums columns part, part + 4, ... <= row
-      double a2 = 0.0;
-      if (rowok)
-        for (int c = part; c <= row; c += 4) a2 += Xs[row][c] * rk[c];
-      red[part][row] = a2;
+      for (int cb = 0; cb < ncb; cb++) {
+        TL ln[16];
+        const int cn = (cb + 1) * kSB;
+  #pragma unroll
+        for (int u = 0; u < 16; u++) {
+          const int c = cn + part + 4 * u;
+          ln[u] = (rowok && c < ncols) ? Lp[(int64_t)c * m + r0 + row] : (TL)0;
+        }
+        if (k == 0) {
+          if (tid == 0) waitOk = wait_flag(myflags + cb, epoch, status, s);
+          __syncthreads();
+          if (!waitOk) return false;  // block-uniform
+          if (cb == 0) loadV();
+        }
+        const int cbase = cb * kSB;
+  #pragma unroll
+        for (int u = 0; u < 16; u++) {
+          const int c = cbase + part + 4 * u;
+          if (c < ncols) acc += (double)lv[u] * __ldcg(yk + c);
+        }
+  #pragma unroll
+        for (int u = 0; u < 16; u++) lv[u] = ln[u];
+      }
+      red[part][row] = acc;
       __syncthreads();
-      if (tid < rows) y[(int64_t)k * P.n + f + r0 + tid] = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
+      if (tid < kSB) {
+        const double sum = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
+        rk[tid] = tid < rows ? vreg - sum : 0.0;
+      }
+      __syncthreads();
+      if (below) {
+        double *tk_out = T + (int64_t)k * Tstride + P.snTOff[s];
+        if (tid < rows) tk_out[blk * kSB + tid] = rk[tid];
+      } else {
+        // y_k = X r_k, X = L_kk^-1 lower triangular: thread (row, part) sums columns part, part + 4, ... <= row
+        double a2 = 0.0;
+        if (rowok)
+          for (int c = part; c <= row; c += 4) a2 += Xs[row][c] * rk[c];
+        red[part][row] = a2;
+        __syncthreads();
+        if (tid < rows) y[(int64_t)k * P.n + f + r0 + tid] = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
+      }
+      __syncthreads();
     }
+    if (tid == 0) {  // after the barrier: the CTA's stores are ordered before the release / the counted arrival
+      if (below)
+        red_release_add(done + s, 1);
+      else
+        st_release(myflags + blk, epoch);
+    }
+    return true;
+  };
+  for (;;) {
+    if (threadIdx.x == 0) tk = atomicAdd(ticket, 1);
     __syncthreads();
-  }
-  if (tid == 0) {  // after the barrier: the CTA's stores are ordered before the release / the counted arrival
-    if (below)
-      red_release_add(done + s, 1);
-    else
-      st_release(myflags + blk, epoch);
+    const int mine = tk;
+    __syncthreads();
+    if (mine >= ntasks || !run(mine)) return;
   }
 }
 
@@ -254,131 +262,143 @@ __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ 
   extern __shared__ double bwd_dyn[];
   double(*Xs)[kSB + 1] = reinterpret_cast<double(*)[kSB + 1]>(bwd_dyn);            // L_kk^-1
   double(*Lf)[kSB + 1] = reinterpret_cast<double(*)[kSB + 1]>(bwd_dyn + kSB * (kSB + 1));  // next block, [row][col]
-  if (threadIdx.x == 0) tk = atomicAdd(ticket, 1);
-  __syncthreads();
-  if (tk >= ntasks) return;
-  const int4 t = tasks[tk];
-  const int s = t.x, blk = t.y;
-  const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
-  const TL *Lp = Lx + P.snLxp[s];
-  const int *rowsOf = P.Si + P.Sp[s];
-  const int c0 = blk * kSB, w = min(kSB, nc - c0), nb = (nc + kSB - 1) / kSB;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const bool hasNext = blk + 1 < nb;
-  const int rn = (blk + 1) * kSB, wn = hasNext ? min(kSB, nc - rn) : 0;  // the next pivot block: rows [rn, rn + wn)
-  int *myflags = flags + P.blkOff[s];
-  {
-    const TL *X = Inv + P.invOff[P.blkOff[s] + blk];
-    for (int e = tid; e < w * w; e += blockDim.x) Xs[e % w][e / w] = (double)X[e];
-    // next block's tile: Lf[r][c] = L(rn + r, c0 + c); coalesced along r
-    for (int e = tid; e < kSB * kSB; e += blockDim.x) {
-      const int r = e & (kSB - 1), c = e >> 6;
-      Lf[r][c] = (r < wn && c < w) ? (double)Lp[(int64_t)(c0 + c) * m + rn + r] : 0.0;
-    }
-  }
-  // one launch for the whole sweep (levels top-down): the rows below this supernode are final once its parent's
-  // first pivot block (the parent's last backward task) is
-  const int par = P.snParent[s];
-  if (par >= 0) {
-    if (tid == 0) waitOk = wait_flag(flags + P.blkOff[par], epoch, status, s);
-    __syncthreads();
-    if (!waitOk) return;
-  }
-  for (int k = 0; k < q; k++) {
-    double *yk = y + (int64_t)k * P.n;
-    double acc[8];
-#pragma unroll
-    for (int u = 0; u < 8; u++) acc[u] = 0.0;
-    // rows of the supernode below its pivot columns: ancestors, final
-    for (int r = nc + lane; r < m; r += 32) {
-      const double xr = __ldcg(yk + rowsOf[r]);
-#pragma unroll
-      for (int u = 0; u < 8; u++) {
-        const int c = warp + 8 * u;
-        if (c < w) acc[u] += (double)Lp[(int64_t)(c0 + c) * m + r] * xr;
+  // persistent: take tickets until the list is exhausted (a task only waits for earlier tickets)
+  auto run = [&](const int tkv) -> bool {
+    const int4 t = tasks[tkv];
+    const int s = t.x, blk = t.y;
+    const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
+    const TL *Lp = Lx + P.snLxp[s];
+    const int *rowsOf = P.Si + P.Sp[s];
+    const int c0 = blk * kSB, w = min(kSB, nc - c0), nb = (nc + kSB - 1) / kSB;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const bool hasNext = blk + 1 < nb;
+    const int rn = (blk + 1) * kSB, wn = hasNext ? min(kSB, nc - rn) : 0;  // the next pivot block: rows [rn, rn + wn)
+    int *myflags = flags + P.blkOff[s];
+    {
+      const TL *X = Inv + P.invOff[P.blkOff[s] + blk];
+      for (int e = tid; e < w * w; e += blockDim.x) Xs[e % w][e / w] = (double)X[e];
+      // next block's tile: Lf[r][c] = L(rn + r, c0 + c); coalesced along r
+      for (int e = tid; e < kSB * kSB; e += blockDim.x) {
+        const int r = e & (kSB - 1), c = e >> 6;
+        Lf[r][c] = (r < wn && c < w) ? (double)Lp[(int64_t)(c0 + c) * m + rn + r] : 0.0;
       }
     }
-    // pivot blocks after the next one, as they become final; a block's L values are loaded before its wait
-    TL lv[2][8];
-    auto load_block = [&](int rb, TL (&dst)[2][8]) {
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const int r = rb * kSB + lane + 32 * h;
-#pragma unroll
+    // one launch for the whole sweep (levels top-down): the rows below this supernode are final once its parent's
+    // first pivot block (the parent's last backward task) is
+    const int par = P.snParent[s];
+    if (par >= 0) {
+      if (tid == 0) waitOk = wait_flag(flags + P.blkOff[par], epoch, status, s);
+      __syncthreads();
+      if (!waitOk) return false;
+    }
+    for (int k = 0; k < q; k++) {
+      double *yk = y + (int64_t)k * P.n;
+      double acc[8];
+  #pragma unroll
+      for (int u = 0; u < 8; u++) acc[u] = 0.0;
+      // rows of the supernode below its pivot columns: ancestors, final
+      for (int r = nc + lane; r < m; r += 32) {
+        const double xr = __ldcg(yk + rowsOf[r]);
+  #pragma unroll
         for (int u = 0; u < 8; u++) {
           const int c = warp + 8 * u;
-          dst[h][u] = (rb > blk + 1 && r < nc && c < w) ? Lp[(int64_t)(c0 + c) * m + r] : (TL)0;
+          if (c < w) acc[u] += (double)Lp[(int64_t)(c0 + c) * m + r] * xr;
         }
       }
-    };
-    load_block(nb - 1, lv);
-    for (int rb = nb - 1; rb > blk + 1; rb--) {
-      TL ln[2][8];
-      load_block(rb - 1, ln);
-      if (k == 0) {
-        if (tid == 0) waitOk = wait_flag(myflags + rb, epoch, status, s);
+      // pivot blocks after the next one, as they become final; a block's L values are loaded before its wait
+      TL lv[2][8];
+      auto load_block = [&](int rb, TL (&dst)[2][8]) {
+  #pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int r = rb * kSB + lane + 32 * h;
+  #pragma unroll
+          for (int u = 0; u < 8; u++) {
+            const int c = warp + 8 * u;
+            dst[h][u] = (rb > blk + 1 && r < nc && c < w) ? Lp[(int64_t)(c0 + c) * m + r] : (TL)0;
+          }
+        }
+      };
+      load_block(nb - 1, lv);
+      for (int rb = nb - 1; rb > blk + 1; rb--) {
+        TL ln[2][8];
+        load_block(rb - 1, ln);
+        if (k == 0) {
+          if (tid == 0) waitOk = wait_flag(myflags + rb, epoch, status, s);
+          __syncthreads();
+          if (!waitOk) return false;  // block-uniform
+        }
+  #pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int r = rb * kSB + lane + 32 * h;
+          const double xr = r < nc ? __ldcg(yk + f + r) : 0.0;
+  #pragma unroll
+          for (int u = 0; u < 8; u++) acc[u] += (double)lv[h][u] * xr;
+        }
+  #pragma unroll
+        for (int h = 0; h < 2; h++)
+  #pragma unroll
+          for (int u = 0; u < 8; u++) lv[h][u] = ln[h][u];
+      }
+  #pragma unroll
+      for (int u = 0; u < 8; u++) {
+        double v = acc[u];
+  #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red0[warp + 8 * u] = v;
+      }
+      double yv = 0.0;
+      if (tid < w) yv = yk[f + c0 + tid];
+      // the chain step: wait for the next block, then its contribution from the staged tile
+      if (hasNext && k == 0) {
+        if (tid == 0) waitOk = wait_flag(myflags + blk + 1, epoch, status, s);
         __syncthreads();
-        if (!waitOk) return;  // block-uniform
+        if (!waitOk) return false;  // block-uniform
       }
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const int r = rb * kSB + lane + 32 * h;
-        const double xr = r < nc ? __ldcg(yk + f + r) : 0.0;
-#pragma unroll
-        for (int u = 0; u < 8; u++) acc[u] += (double)lv[h][u] * xr;
-      }
-#pragma unroll
-      for (int h = 0; h < 2; h++)
-#pragma unroll
-        for (int u = 0; u < 8; u++) lv[h][u] = ln[h][u];
-    }
-#pragma unroll
-    for (int u = 0; u < 8; u++) {
-      double v = acc[u];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-      if (lane == 0) red0[warp + 8 * u] = v;
-    }
-    double yv = 0.0;
-    if (tid < w) yv = yk[f + c0 + tid];
-    // the chain step: wait for the next block, then its contribution from the staged tile
-    if (hasNext && k == 0) {
-      if (tid == 0) waitOk = wait_flag(myflags + blk + 1, epoch, status, s);
+      if (tid < kSB) xs[tid] = tid < wn ? __ldcg(yk + f + rn + tid) : 0.0;
       __syncthreads();
-      if (!waitOk) return;  // block-uniform
+      {
+        const int c = tid & (kSB - 1), part = tid >> 6;
+        double a2 = 0.0;
+  #pragma unroll 4
+        for (int r = part; r < wn; r += 4) a2 += Lf[r][c] * xs[r];
+        red[part][c] = a2;
+      }
+      __syncthreads();
+      if (tid < kSB)
+        rk[tid] = tid < w ? yv - red0[tid] - ((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid])) : 0.0;
+      __syncthreads();
+      // x_k = X^T r_k, X = L_kk^-1 lower triangular: thread (row i, part) sums X(j, i) r(j) over j = i + part, +4 ...
+      {
+        const int i = tid & (kSB - 1), part = tid >> 6;
+        double a2 = 0.0;
+        if (i < w)
+          for (int j = i + part; j < w; j += 4) a2 += Xs[j][i] * rk[j];
+        red[part][i] = a2;
+      }
+      __syncthreads();
+      if (tid < w) yk[f + c0 + tid] = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
+      __syncthreads();
     }
-    if (tid < kSB) xs[tid] = tid < wn ? __ldcg(yk + f + rn + tid) : 0.0;
+    if (tid == 0) st_release(myflags + blk, epoch);  // after the barrier: the CTA's stores of x_k are ordered before
+    return true;
+  };
+  for (;;) {
+    if (threadIdx.x == 0) tk = atomicAdd(ticket, 1);
     __syncthreads();
-    {
-      const int c = tid & (kSB - 1), part = tid >> 6;
-      double a2 = 0.0;
-#pragma unroll 4
-      for (int r = part; r < wn; r += 4) a2 += Lf[r][c] * xs[r];
-      red[part][c] = a2;
-    }
+    const int mine = tk;
     __syncthreads();
-    if (tid < kSB)
-      rk[tid] = tid < w ? yv - red0[tid] - ((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid])) : 0.0;
-    __syncthreads();
-    // x_k = X^T r_k, X = L_kk^-1 lower triangular: thread (row i, part) sums X(j, i) r(j) over j = i + part, +4 ...
-    {
-      const int i = tid & (kSB - 1), part = tid >> 6;
-      double a2 = 0.0;
-      if (i < w)
-        for (int j = i + part; j < w; j += 4) a2 += Xs[j][i] * rk[j];
-      red[part][i] = a2;
-    }
-    __syncthreads();
-    if (tid < w) yk[f + c0 + tid] = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
-    __syncthreads();
+    if (mine >= ntasks || !run(mine)) return;
   }
-  if (tid == 0) st_release(myflags + blk, epoch);  // after the barrier: the CTA's stores of x_k are ordered before
 }
 
 void init_solve_attributes() {
   cudaFuncSetAttribute(k_bwd_blocks<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBwdSmem);
   cudaFuncSetAttribute(k_bwd_blocks<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBwdSmem);
 }
+
+int num_sms();
+// persistent solve grids: 3 CTAs per SM (the kernels' launch bounds)
+static int solve_grid(int ntasks) { return ntasks < 3 * num_sms() ? ntasks : 3 * num_sms(); }
 
 template <class TL>
 void launch_diag_inv(const DevPlan &P, int nblocks, const TL *Lx, TL *Inv, cudaStream_t st) {
@@ -389,14 +409,14 @@ void launch_fwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan
                        double *y, double *V, double *T, int *flags, int epoch, int *done, int q, int64_t Vstride,
                        int64_t Tstride, unsigned long long *status, cudaStream_t st) {
   if (ntasks > 0)
-    k_fwd_blocks<TL><<<ntasks, 256, 0, st>>>(tasks, ntasks, ticket, P, Lx, Inv, y, V, T, flags, epoch, done, q,
+    k_fwd_blocks<TL><<<solve_grid(ntasks), 256, 0, st>>>(tasks, ntasks, ticket, P, Lx, Inv, y, V, T, flags, epoch, done, q,
                                              Vstride, Tstride, status);
 }
 template <class TL>
 void launch_bwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
                        double *y, int *flags, int epoch, int q, unsigned long long *status, cudaStream_t st) {
   if (ntasks > 0)
-    k_bwd_blocks<TL><<<ntasks, 256, kBwdSmem, st>>>(tasks, ntasks, ticket, P, Lx, Inv, y, flags, epoch, q, status);
+    k_bwd_blocks<TL><<<solve_grid(ntasks), 256, kBwdSmem, st>>>(tasks, ntasks, ticket, P, Lx, Inv, y, flags, epoch, q, status);
 }
 template void launch_diag_inv<double>(const DevPlan &, int, const double *, double *, cudaStream_t);
 template void launch_diag_inv<float>(const DevPlan &, int, const float *, float *, cudaStream_t);
