@@ -505,3 +505,67 @@ class SparseCholesky:
         self.timing["solve_ms"] += (time.perf_counter() - t0) * 1e3
         self.timing["nSolve"] += len(bs)
         return r
+
+
+class SupernodalLDLT:
+    """Real symmetric LDL^T over a supernodal analysis: 1x1 pivots with static perturbation (|d| < tau -> +-tau,
+    tau = pivotTol * max |A(i, i)|), inertia and refinement (ldlt.mjs:431-645). Factor and solves run on the GPU."""
+
+    def __init__(self, sym: SymbolicAnalysis, factor=None):
+        self.sym = sym
+        self.factorKind = factor
+        self.kernel = "cuda-sm100a"
+        self.num = NumericFactor(sym, LDLT, FP64)
+        self.nnzL = sym.nnzL
+        self.nNeg = 0
+        self.nPerturbed = 0
+        self.ok = False
+
+    def factor(self, values, pivotTol: float = 1e-13) -> dict:
+        nv = len(values)
+        if nv != _nnz_of(self.sym):
+            raise AmpError(AMP_BAD_LENGTH, f"factorNumeric: {nv} values for a pattern with {_nnz_of(self.sym)} entries")
+        self.ok = self.num.factor(values, pivotTol=pivotTol)
+        self.nNeg, self.nPerturbed = self.num.nNeg, self.num.nPerturbed
+        return {"ok": self.ok, "nNeg": self.nNeg, "nPerturbed": self.nPerturbed, "ms": self.num.ms}
+
+    @property
+    def Lx(self) -> np.ndarray:
+        return self.num.Lx
+
+    @property
+    def D(self) -> np.ndarray:
+        return self.num.D
+
+    def _need(self):
+        if not self.ok:
+            raise AmpError(AMP_NO_FACTOR, "solveNumeric: no successful numeric factorization")
+
+    def solve(self, b, out=None) -> np.ndarray:
+        self._need()
+        x = self.num.solve_block(_f64(b)[None, :])[0]
+        if out is not None:
+            out[:] = x
+            return out
+        return x
+
+    def solveMany(self, b, q: int, out=None) -> np.ndarray:
+        """q right-hand sides stored one after another in b (b[k n + i]); one device pass per sweep for all q."""
+        self._need()
+        n = self.sym.n
+        x = self.num.solve_block(_f64(b).reshape(q, n)).reshape(q * n)
+        if out is not None:
+            out[:] = x
+            return out
+        return x
+
+    def solveRefined(self, pat, values, b, maxSteps: int = 3, tol: float = 1e-14) -> dict:
+        """Refinement against the factored (unperturbed) matrix: r = b - A x, x += solve(r) (ldlt.mjs:253-275).
+        `pat` / `values` must be the pattern and values that were factored; the residual runs on the device copy."""
+        self._need()
+        checkSymbolic(self.sym, pat)
+        if len(values) != _nnz_of(self.sym):
+            raise AmpError(AMP_BAD_LENGTH, f"solveRefined: {len(values)} values for a pattern with "
+                                           f"{_nnz_of(self.sym)} entries")
+        X, rel, steps = self.num.solve_refined_block(_f64(b)[None, :], maxSteps=maxSteps, tol=tol)
+        return {"x": X[0], "relResidual": rel, "steps": steps}

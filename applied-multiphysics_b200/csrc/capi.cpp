@@ -146,6 +146,9 @@ struct amp_factor_s {
   DevMem mem;
   double *dLx = nullptr, *dU = nullptr, *dD = nullptr, *dValues = nullptr;
   float *dL32 = nullptr, *dU32 = nullptr;           // mixed precision: FP32 factor and update arena
+  double *dW = nullptr;                             // LDL^T: L21 D of every front (the update's A operand)
+  double *dScal = nullptr;                          // LDL^T: pivotTol, tau
+  int *dCounts = nullptr;                           // LDL^T: nNeg, nPerturbed
   double *dInv = nullptr;                           // inverses of the 64-column diagonal blocks (FP64 factor)
   float *dInv32 = nullptr;                          // the same for the FP32 factor
   __nv_bfloat16 *dShi = nullptr, *dSlo = nullptr;   // BF16 split columns of the factored pivot blocks
@@ -216,6 +219,7 @@ void upload_plan(amp_plan *pl) {
   d.Si = m.upload(P.Si);
   d.blkOff = m.upload(P.blkOff);
   d.invOff = m.upload(P.invOff);
+  d.diagSlot = m.upload(P.diagSlot);
   pl->dAsm = m.upload(P.asmTasks);
   pl->dPanel = m.upload(P.panelTasks);
   pl->dTile = m.upload(P.tileTasks);
@@ -286,7 +290,7 @@ void enqueue_factor(amp_factor *f) {
         const amp::StepRange &sr = P.steps[k];
         timed(f, K_PANEL, sr.panelFlops, 0.0, [&] {
           amp::launch_panel<float>(f->plan->dPanel + sr.panel0, sr.panel1 - sr.panel0, dp, f->dL32, f->dReaders,
-                                   f->dStatus, f->dShi, f->dSlo, st);
+                                   f->dStatus, f->dShi, f->dSlo, amp::LdltArgs<float>{}, st);
         });
         const int64_t t0 = P.mixStepPtr[k], t1 = P.mixStepPtr[k + 1];
         if (t1 > t0)
@@ -307,6 +311,13 @@ void enqueue_factor(amp_factor *f) {
             [&] { amp::launch_diag_inv<float>(dp, P.nflags, f->dL32, f->dInv32, st); });
     return;
   }
+  const bool ldlt = f->kind == AMP_LDLT;
+  const amp::LdltArgs<double> ld = ldlt ? amp::LdltArgs<double>{f->dScal, f->dCounts, f->dW, f->dD}
+                                        : amp::LdltArgs<double>{};
+  if (ldlt) {
+    ck(cudaMemsetAsync(f->dCounts, 0, 2 * sizeof(int), st), "memset counts");
+    amp::launch_ldlt_tau(f->dValues, dp, f->dScal, st);
+  }
   for (int L = 0; L < P.nlevels; L++) {
     timed(f, K_ASSEMBLE, 0.0, P.asmLvlBytes[L], [&] {
       amp::launch_assemble<double>(f->plan->dAsm + P.asmLvlPtr[L], P.asmLvlPtr[L + 1] - P.asmLvlPtr[L], dp,
@@ -316,16 +327,17 @@ void enqueue_factor(amp_factor *f) {
       const amp::StepRange &sr = P.steps[k];
       timed(f, K_PANEL, sr.panelFlops, 0.0, [&] {
         amp::launch_panel<double>(f->plan->dPanel + sr.panel0, sr.panel1 - sr.panel0, dp, f->dLx, f->dReaders,
-                                  f->dStatus, nullptr, nullptr, st);
+                                  f->dStatus, nullptr, nullptr, ld, st);
       });
       if (sr.tile1 > sr.tile0)
         timed(f, K_UPDATE, sr.updateFlops, 0.0, [&] {
-          amp::launch_update(f->plan->dTile + sr.tile0, sr.tile1 - sr.tile0, dp, f->dLx, f->dU, f->dStatus, st);
+          amp::launch_update(f->plan->dTile + sr.tile0, sr.tile1 - sr.tile0, dp, f->dLx, f->dU, ld.W, f->dStatus,
+                             st);
         });
     }
     if (P.uLvlPtr[L + 1] > P.uLvlPtr[L])
       timed(f, K_UPDATE, P.uLvlFlops[L], 0.0, [&] {
-        amp::launch_update(f->plan->dUTile + P.uLvlPtr[L], P.uLvlPtr[L + 1] - P.uLvlPtr[L], dp, f->dLx, f->dU,
+        amp::launch_update(f->plan->dUTile + P.uLvlPtr[L], P.uLvlPtr[L + 1] - P.uLvlPtr[L], dp, f->dLx, f->dU, ld.W,
                            f->dStatus, st);
       });
   }
@@ -356,11 +368,12 @@ void device_solve_permuted(amp_factor *f, int q) {
   });
   timed(f, K_BACKWARD, 0.0, lbytes, [&] {
     if (f->dL32)
-      amp::launch_bwd_blocks<float>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dL32, f->dInv32, f->dY, f->dFlags,
-                                    ebwd, q, f->dSolveStatus, st);
+      amp::launch_bwd_blocks<float>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dL32, f->dInv32, nullptr, f->dY,
+                                    f->dFlags, ebwd, q, f->dSolveStatus, st);
     else
-      amp::launch_bwd_blocks<double>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dLx, f->dInv, f->dY, f->dFlags,
-                                     ebwd, q, f->dSolveStatus, st);
+      amp::launch_bwd_blocks<double>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dLx, f->dInv,
+                                     f->kind == AMP_LDLT ? f->dD : nullptr, f->dY, f->dFlags, ebwd, q,
+                                     f->dSolveStatus, st);
   });
 }
 
@@ -559,8 +572,10 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
     *out = nullptr;
     amp_factor_opts o{AMP_CHOLESKY, AMP_FP64};
     if (opts) o = *opts;
-    if (o.kind != AMP_CHOLESKY) return fail(AMP_INVALID, "factor kind not available in this build");
+    if (o.kind != AMP_CHOLESKY && o.kind != AMP_LDLT) return fail(AMP_INVALID, "unknown factor kind");
     if (o.precision != AMP_FP64 && o.precision != AMP_MIXED) return fail(AMP_INVALID, "unknown precision");
+    if (o.kind == AMP_LDLT && o.precision != AMP_FP64)
+      return fail(AMP_INVALID, "LDL^T is available in FP64 only in this build");
     ck(cudaSetDevice(pl->device), "cudaSetDevice");
     if (!pl->uploaded) {  // the device schedule is uploaded once, by the first factor of the plan
       upload_plan(pl);
@@ -581,6 +596,11 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
         f->dLx = f->mem.alloc<double>((size_t)P.nnzLStored);
         f->dU = f->mem.alloc<double>((size_t)P.arenaDoubles);
         f->dInv = f->mem.alloc<double>((size_t)inv_elems(P));
+        if (o.kind == AMP_LDLT) {
+          f->dW = f->mem.alloc<double>((size_t)P.nnzLStored);
+          f->dScal = f->mem.alloc<double>(2);
+          f->dCounts = f->mem.alloc<int>(2);
+        }
       } else {
         f->dL32 = f->mem.alloc<float>((size_t)P.nnzLStored);
         f->dU32 = f->mem.alloc<float>((size_t)P.arenaDoubles);
@@ -620,7 +640,6 @@ int amp_factor_numeric(amp_factor *f, const double *values, int64_t nvalues, int
     if (nvalues != P.patNnz)
       return fail(AMP_BAD_LENGTH, "factorNumeric: " + std::to_string(nvalues) + " values for a pattern with " +
                                       std::to_string(P.patNnz) + " entries");
-    (void)pivot_tol;
     ck(cudaSetDevice(f->plan->device), "cudaSetDevice");
     f->ok = false;
     amp_factor_result r{};
@@ -637,6 +656,8 @@ int amp_factor_numeric(amp_factor *f, const double *values, int64_t nvalues, int
                          values_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st),
          "copy values");
     f->hasValues = true;
+    if (f->kind == AMP_LDLT)  // read by the tau kernel at the start of the captured sequence
+      ck(cudaMemcpyAsync(f->dScal, &pivot_tol, sizeof(double), cudaMemcpyHostToDevice, st), "copy pivotTol");
     ck(cudaEventRecord(f->ev0, st), "event");
     if (f->profiling) {
       enqueue_factor(f);
@@ -654,8 +675,13 @@ int amp_factor_numeric(amp_factor *f, const double *values, int64_t nvalues, int
     ck(cudaGetLastError(), "kernel launch");
     ck(cudaEventRecord(f->ev1, st), "event");
     unsigned long long status = 0;
+    int counts[2] = {0, 0};
     ck(cudaMemcpyAsync(&status, f->dStatus, sizeof status, cudaMemcpyDeviceToHost, st), "copy status");
+    if (f->kind == AMP_LDLT)
+      ck(cudaMemcpyAsync(counts, f->dCounts, sizeof counts, cudaMemcpyDeviceToHost, st), "copy counts");
     ck(cudaStreamSynchronize(st), "factor");
+    r.n_neg = counts[0];
+    r.n_perturbed = counts[1];
     float ms = 0;
     cudaEventElapsedTime(&ms, f->ev0, f->ev1);
     r.ms = ms;

@@ -16,6 +16,16 @@ struct DevPlan {
   const int *perm, *Sp, *Si;
   const int *blkOff;       // first 64-column diagonal block of supernode s (nsuper + 1)
   const int64_t *invOff;   // offset of the inverse of each diagonal block (w x w, column-major)
+  const int *diagSlot;     // CSR slot of A(i, i), original row i (the LDL^T pivot scale)
+};
+
+// LDL^T variant of the panel and update kernels (ldlt.mjs:450-562); all null for Cholesky.
+template <class T>
+struct LdltArgs {
+  const double *scal;  // [0] pivotTol (copied per factorization), [1] tau = pivotTol * max |A(i, i)| (device)
+  int *counts;         // [0] nNeg, [1] nPerturbed
+  T *W;                // L21 D (rows of the solved panel times the pivots): the A operand of the update
+  double *D;           // the pivots, permuted order
 };
 
 // Failure record: the lowest failing global column wins (atomicMin), code in the low bits.

@@ -1,16 +1,15 @@
-// FP64 multifrontal numeric factorization (Cholesky) and supernodal solves on sm_100a.
+// Multifrontal numeric factorization on sm_100a: Cholesky (FP64, or FP32 fronts for the mixed-precision path) and
+// LDL^T with static pivot perturbation (FP64).
 //
 // Per level of the supernodal tree (leaves first):
 //   k_assemble  zero the front, scatter A's entries (sparse.mjs:965-973) and extend-add the children's update
 //               matrices in the reference's child order (sparse.mjs:974-985). One CTA owns a block of 32 front
 //               columns, so every entry has a single writer and the summation order is the reference's.
 //   per pivot block of 64 columns:
-//     k_panel   POTRF of the 64 x 64 diagonal block in shared memory (pivot test d > 0, sqrt, multiply by 1/dk as
-//               sparse.mjs:1151-1156) and TRSM of 256 panel rows per CTA (rows held in registers).
-//     k_update  trailing update F -= L21 L21^T on 64 x 64 lower tiles with FP64 tensor-core MMA (DMMA m8n8k4),
-//               covering both the remaining pivot columns (in Lx) and the update block (in the U arena).
-// The solves run the multifrontal vector form: forward per level bottom-up (each supernode passes one update vector
-// of length mu to its parent, no atomics), backward per level top-down gathering ancestor values.
+//     k_panel   POTRF (or LDL^T) of the 64 x 64 diagonal block in shared memory and TRSM of 256 panel rows per CTA.
+//     k_update  FP64 trailing update F -= A B^T (A = L21, or L21 D for LDL^T; B = L21) on 128 x 64 tiles with the
+//               FP64 tensor-core MMA (mma.sync m16n8k16), covering the remaining pivot columns (in Lx) and the update
+//               block (in the U arena). The mixed-precision update is k_update_mx (update_bf16x3.cu).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -41,6 +40,41 @@ __device__ __forceinline__ double recip_nr(double d) {
   x = fma(x, e, x);
   e = fma(-d, x, 1.0);
   return fma(x, e, x);
+}
+
+// Static pivot perturbation of LDL^T (ldlt.mjs:513-522): |d| < tau (or NaN) becomes -tau / +tau by the sign of d,
+// a non-finite small pivot fails the factorization. flags: bit 0 negative pivot, bit 1 perturbed. false = failure.
+template <class T>
+__device__ __forceinline__ bool ldlt_pivot(T &d, T tau, unsigned char &flags) {
+  flags = 0;
+  if (!(fabs(d) >= tau)) {
+    if (!isfinite(d)) return false;
+    d = d < T(0) ? -tau : tau;
+    flags = 2;
+  }
+  if (d < T(0)) flags |= 1;
+  return true;
+}
+
+// tau = pivotTol * max |A(i, i)| (1 when that maximum is 0 or not a number, ldlt.mjs:419-424). One CTA.
+__global__ void __launch_bounds__(1024) k_ldlt_tau(const double *__restrict__ values, const int *__restrict__ diagSlot,
+                                                    int n, double *scal) {
+  __shared__ double red[32];
+  double mx = 0.0;
+  bool nan = false;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const double a = fabs(values[diagSlot[i]]);
+    if (a != a) nan = true;
+    mx = fmax(mx, a);
+  }
+  nan = __syncthreads_or(nan);
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) mx = fmax(mx, red[w]);
+    scal[1] = scal[0] * ((mx > 0.0 && !nan) ? mx : 1.0);
+  }
 }
 
 __device__ __forceinline__ bool failed(const unsigned long long *st) {
@@ -109,11 +143,14 @@ __device__ __forceinline__ float recip_t(float d) { return __frcp_rn(d); }
 
 // T = double: the FP64 factor. T = float: the mixed-precision factor; the solved panel rows are also written as BF16
 // hi / lo pairs (hi = bf16(x), lo = bf16(x - hi)) into the split columns read by the tensor-core updates.
+// LDL^T (ld.scal != null): the same right-looking unscaled form, whose columns hold L D and whose pivots are D;
+// the pivots are perturbed as they become final, L = (L D) D^-1 with a unit diagonal is written back, D goes to
+// ld.D, and the TRSM rows are written both as L21 (Lx) and as L21 D (ld.W) for the update.
 template <class T>
 __global__ void __launch_bounds__(256, 1) k_panel(const PanelTask *__restrict__ tasks, DevPlan P,
                                                   T *__restrict__ Lx, int *__restrict__ readers,
                                                   unsigned long long *status, __nv_bfloat16 *__restrict__ Shi,
-                                                  __nv_bfloat16 *__restrict__ Slo) {
+                                                  __nv_bfloat16 *__restrict__ Slo, LdltArgs<T> ld) {
   if (failed(status)) return;
   const PanelTask t = tasks[blockIdx.x];
   const int s = t.s, c0 = t.c0;
@@ -125,8 +162,11 @@ __global__ void __launch_bounds__(256, 1) k_panel(const PanelTask *__restrict__ 
   __shared__ unsigned short trail[kPanel * (kPanel - 1) / 2];  // (i, j) of the trailing entries, rightmost column first
   extern __shared__ __align__(16) unsigned char xs_raw[];
   T *xs = reinterpret_cast<T *>(xs_raw);  // kPanel x 256 staged solutions of the TRSM
-  __shared__ int fail, lastReader;
+  __shared__ int fail, failCode, lastReader;
+  __shared__ unsigned char pflag[kPanel];
   const int tid = threadIdx.x;
+  const bool ldlt = ld.scal != nullptr;
+  const T tau = ldlt ? (T)ld.scal[1] : T(0);
   // the pivot block (lower part); columns w .. 63 of a short last block are padded with the identity
   for (int e = tid; e < kPanel * kPanel; e += blockDim.x) {
     const int i = e & (kPanel - 1), j = e >> 6;
@@ -144,10 +184,18 @@ __global__ void __launch_bounds__(256, 1) k_panel(const PanelTask *__restrict__ 
     __threadfence();
     lastReader = atomicAdd(readers + t.group, 1) == t.nchunks - 1;
     fail = -1;
-    const T d = D[0][0];
-    if (!(d > T(0))) fail = 0;
+    failCode = 1;
+    T d = D[0][0];
+    if (ldlt) {
+      if (!ldlt_pivot(d, tau, pflag[0])) {
+        fail = 0;
+        failCode = 2;
+      }
+    } else if (!(d > T(0))) {
+      fail = 0;
+    }
     pd[0] = d;
-    ivsq[0] = recip_t(d);
+    ivsq[0] = ldlt ? T(1) / d : recip_t(d);
   }
   __syncthreads();
   // POTRF, right-looking on the unscaled columns: step k subtracts D[i][k] D[j][k] / d_k from the trailing entries
@@ -164,14 +212,30 @@ __global__ void __launch_bounds__(256, 1) k_panel(const PanelTask *__restrict__ 
       const T v = D[i][j] - (D[i][k] * D[j][k]) * iv2;
       D[i][j] = v;
       if (i == k + 1 && j == k + 1) {  // the next pivot is final now
-        if (!(v > T(0)) && k + 1 < w) fail = k + 1;
-        pd[k + 1] = v;
-        ivsq[k + 1] = recip_t(v);
+        T d = v;
+        if (ldlt) {
+          if (k + 1 < w && !ldlt_pivot(d, tau, pflag[k + 1])) {
+            fail = k + 1;
+            failCode = 2;
+          }
+          ivsq[k + 1] = T(1) / d;
+        } else {
+          if (!(v > T(0)) && k + 1 < w) fail = k + 1;
+          ivsq[k + 1] = recip_t(v);
+        }
+        pd[k + 1] = d;
       }
     }
     __syncthreads();
   }
-  if (fail < 0) {
+  if (fail < 0 && ldlt) {
+    // LDL^T: D keeps L D (used by the TRSM below as is); pivots and their reciprocals
+    if (tid < kPanel) {
+      const T d = tid < w ? pd[tid] : T(1);
+      piv[tid] = d;
+      invd[tid] = T(1) / d;
+    }
+  } else if (fail < 0) {
     // L = D diag(d)^-1/2: one square root and reciprocal per column, then every entry scaled once
     if (tid < kPanel) {
       const T d = tid < w ? pd[tid] : T(1);
@@ -188,13 +252,27 @@ __global__ void __launch_bounds__(256, 1) k_panel(const PanelTask *__restrict__ 
   }
   __syncthreads();
   if (fail >= 0) {
-    if (tid == 0) atomicMin(status, status_word(f + c0 + fail, 1, s));
+    if (tid == 0) atomicMin(status, status_word(f + c0 + fail, failCode, s));
     return;
   }
   if (lastReader) {
-    for (int e = tid; e < w * w; e += blockDim.x) {
-      const int i = e % w, j = e / w;
-      if (i >= j) Lp[(int64_t)(c0 + j) * m + (c0 + i)] = D[i][j];
+    if (ldlt) {
+      for (int e = tid; e < w * w; e += blockDim.x) {
+        const int i = e % w, j = e / w;
+        if (i >= j) Lp[(int64_t)(c0 + j) * m + (c0 + i)] = i == j ? T(1) : D[i][j] * invd[j];
+      }
+      if (tid < w) ld.D[f + c0 + tid] = (double)piv[tid];
+      if (tid == 0) {
+        int neg = 0, pert = 0;
+        for (int k = 0; k < w; k++) neg += pflag[k] & 1, pert += pflag[k] >> 1;
+        atomicAdd(ld.counts, neg);
+        atomicAdd(ld.counts + 1, pert);
+      }
+    } else {
+      for (int e = tid; e < w * w; e += blockDim.x) {
+        const int i = e % w, j = e / w;
+        if (i >= j) Lp[(int64_t)(c0 + j) * m + (c0 + i)] = D[i][j];
+      }
     }
   }
   // TRSM: row r of the panel solves x L11^T = a, one thread per row, 16 columns at a time (16 doubles live in
@@ -223,6 +301,7 @@ __global__ void __launch_bounds__(256, 1) k_panel(const PanelTask *__restrict__ 
     for (int c = 0; c < Q; c++) {
       if (q0 + c < w) {
         Lp[(int64_t)(c0 + q0 + c) * m + r] = x[c];
+        if (ldlt) ld.W[P.snLxp[s] + (int64_t)(c0 + q0 + c) * m + r] = x[c] * piv[q0 + c];
         if (Shi) {
           const int64_t g = P.snSp[s] + (int64_t)(c0 + q0 + c) * ((m + 7) & ~7) + r;
           const __nv_bfloat16 hi = __float2bfloat16_rn((float)x[c]);
@@ -269,18 +348,20 @@ constexpr int kUpdateSmem = 2 * kStage * (int)sizeof(double);
 
 // Panel rows of one tile and one 64-column chunk of its K range into a pipeline stage. Thread t owns one row of A
 // (t % 128) and of B (t % 64) and walks the pivot columns with a pointer step of 2 m (A) or 4 m (B).
-__device__ __forceinline__ void tile_loads(const TileTask &t, int chunk, const double *Lx, double *stage) {
+__device__ __forceinline__ void tile_loads(const TileTask &t, int chunk, const double *Ax, const double *Lx,
+                                           double *stage) {
   const int kc = t.c0 + chunk * kPanel, kw = min(kPanel, t.w - chunk * kPanel), wk = (kw + 15) & ~15;
-  const double *Lp = Lx + t.lp;
+  const double *Ap = Ax + t.lp, *Lp = Lx + t.lp;
   const int tid = threadIdx.x;
   {
     const int i = tid & (kTileM - 1), k0 = tid >> 7, r = t.i0 + i;
     const bool rowok = r < t.m;
-    const double *src = Lp + (int64_t)(kc + k0) * t.m + (rowok ? r : 0);
+    const double *src = Ap + (int64_t)(kc + k0) * t.m + (rowok ? r : 0);
     double *dst = stage + k0 * kLdA + i;
     const int64_t step = 2 * (int64_t)t.m;
 #pragma unroll 4
-    for (int k = k0; k < wk; k += 2, src += step, dst += 2 * kLdA) cp_async8(dst, rowok && k < kw ? src : Lp, rowok && k < kw);
+    for (int k = k0; k < wk; k += 2, src += step, dst += 2 * kLdA)
+      cp_async8(dst, rowok && k < kw ? src : Ap, rowok && k < kw);
   }
   {
     const int i = tid & (kTile - 1), k0 = tid >> 6, r = t.j0 + i;
@@ -289,7 +370,8 @@ __device__ __forceinline__ void tile_loads(const TileTask &t, int chunk, const d
     double *dst = stage + kPanel * kLdA + k0 * kLdB + i;
     const int64_t step = 4 * (int64_t)t.m;
 #pragma unroll 4
-    for (int k = k0; k < wk; k += 4, src += step, dst += 4 * kLdB) cp_async8(dst, rowok && k < kw ? src : Lp, rowok && k < kw);
+    for (int k = k0; k < wk; k += 4, src += step, dst += 4 * kLdB)
+      cp_async8(dst, rowok && k < kw ? src : Lp, rowok && k < kw);
   }
 }
 
@@ -298,8 +380,9 @@ __device__ __forceinline__ void tile_loads(const TileTask &t, int chunk, const d
 // FP64 tensor cores; the C tile is read once (prefetched into registers during its first chunk) and written once.
 __global__ void __launch_bounds__(256, 1) k_update(const TileTask *__restrict__ tasks, int ntasks,
                                                    double *__restrict__ Lx, double *__restrict__ U,
-                                                   const unsigned long long *status) {
+                                                   const double *__restrict__ W, const unsigned long long *status) {
   if (failed(status)) return;
+  const double *Ax = W ? W : Lx;  // LDL^T: A = L21 D
   extern __shared__ double smem_upd[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
@@ -311,7 +394,7 @@ __global__ void __launch_bounds__(256, 1) k_update(const TileTask *__restrict__ 
   if (t + (int)gridDim.x < ntasks) nxtTask = tasks[t + gridDim.x];
   int chunk = 0, nch = (cur.w + kPanel - 1) / kPanel;
   int stage = 0;
-  tile_loads(cur, 0, Lx, smem_upd);
+  tile_loads(cur, 0, Ax, Lx, smem_upd);
   cp_async_commit();
   double *cp[4][2];
   int jj[4][2], ii[2][2];
@@ -321,7 +404,8 @@ __global__ void __launch_bounds__(256, 1) k_update(const TileTask *__restrict__ 
     // the next (tile, chunk) item
     const bool sameTile = chunk + 1 < nch;
     const bool hasNext = sameTile || t + (int)gridDim.x < ntasks;
-    if (hasNext) tile_loads(sameTile ? cur : nxtTask, sameTile ? chunk + 1 : 0, Lx, smem_upd + (stage ^ 1) * kStage);
+    if (hasNext)
+      tile_loads(sameTile ? cur : nxtTask, sameTile ? chunk + 1 : 0, Ax, Lx, smem_upd + (stage ^ 1) * kStage);
     cp_async_commit();
     const int m = cur.m, nc = cur.nc, mu = m - nc;
     if (newTile) {
@@ -446,20 +530,25 @@ template void launch_assemble<float>(const AsmTask *, int64_t, const DevPlan &, 
                                      const unsigned long long *, cudaStream_t);
 template <class T>
 void launch_panel(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, T *Lx, int *readers,
-                  unsigned long long *status, __nv_bfloat16 *Shi, __nv_bfloat16 *Slo, cudaStream_t st) {
+                  unsigned long long *status, __nv_bfloat16 *Shi, __nv_bfloat16 *Slo, const LdltArgs<T> &ld,
+                  cudaStream_t st) {
   if (ntasks > 0)
-    k_panel<T><<<(unsigned)ntasks, 256, kPanel * 256 * (int)sizeof(T), st>>>(tasks, P, Lx, readers, status, Shi, Slo);
+    k_panel<T><<<(unsigned)ntasks, 256, kPanel * 256 * (int)sizeof(T), st>>>(tasks, P, Lx, readers, status, Shi, Slo,
+                                                                            ld);
 }
 template void launch_panel<double>(const PanelTask *, int64_t, const DevPlan &, double *, int *, unsigned long long *,
-                                   __nv_bfloat16 *, __nv_bfloat16 *, cudaStream_t);
+                                   __nv_bfloat16 *, __nv_bfloat16 *, const LdltArgs<double> &, cudaStream_t);
 template void launch_panel<float>(const PanelTask *, int64_t, const DevPlan &, float *, int *, unsigned long long *,
-                                  __nv_bfloat16 *, __nv_bfloat16 *, cudaStream_t);
+                                  __nv_bfloat16 *, __nv_bfloat16 *, const LdltArgs<float> &, cudaStream_t);
+void launch_ldlt_tau(const double *values, const DevPlan &P, double *scal, cudaStream_t st) {
+  k_ldlt_tau<<<1, 1024, 0, st>>>(values, P.diagSlot, P.n, scal);
+}
 int num_sms() { return g_num_sms; }
-void launch_update(const TileTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, double *U,
+void launch_update(const TileTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, double *U, const double *W,
                    const unsigned long long *status, cudaStream_t st) {
   (void)P;
   const int grid = (int)std::min<int64_t>(ntasks, g_num_sms);
-  if (ntasks > 0) k_update<<<grid, 256, kUpdateSmem, st>>>(tasks, (int)ntasks, Lx, U, status);
+  if (ntasks > 0) k_update<<<grid, 256, kUpdateSmem, st>>>(tasks, (int)ntasks, Lx, U, W, status);
 }
 void launch_permute_in(const double *b, double *y, const int *perm, int n, int q, cudaStream_t st) {
   int64_t tot = (int64_t)n * q;

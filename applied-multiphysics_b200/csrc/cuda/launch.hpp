@@ -18,11 +18,13 @@ void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, con
                      const unsigned long long *status, cudaStream_t st);
 template <class T>
 void launch_panel(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, T *Lx, int *readers,
-                  unsigned long long *status, __nv_bfloat16 *Shi, __nv_bfloat16 *Slo, cudaStream_t st);
+                  unsigned long long *status, __nv_bfloat16 *Shi, __nv_bfloat16 *Slo, const LdltArgs<T> &ld,
+                  cudaStream_t st);
+void launch_ldlt_tau(const double *values, const DevPlan &P, double *scal, cudaStream_t st);
 void launch_update_mx(const MixTask *tasks, int64_t ntasks, const CUtensorMap *maps, float *L32, float *U32,
                       unsigned long long *status, int num_sms, cudaStream_t st);
 int num_sms();
-void launch_update(const TileTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, double *U,
+void launch_update(const TileTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, double *U, const double *W,
                    const unsigned long long *status, cudaStream_t st);
 void launch_permute_in(const double *b, double *y, const int *perm, int n, int q, cudaStream_t st);
 void launch_permute_out(const double *y, double *x, const int *perm, int n, int q, cudaStream_t st);
@@ -34,6 +36,7 @@ void launch_fwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan
                        int64_t Tstride, unsigned long long *status, cudaStream_t st);
 template <class TL>
 void launch_bwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
-                       double *y, int *flags, int epoch, int q, unsigned long long *status, cudaStream_t st);
+                       const double *Dpiv, double *y, int *flags, int epoch, int q, unsigned long long *status,
+                       cudaStream_t st);
 
 }  // namespace amp

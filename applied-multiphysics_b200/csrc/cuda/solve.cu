@@ -252,7 +252,8 @@ constexpr int kBwdSmem = 2 * kSB * (kSB + 1) * (int)sizeof(double);
 template <class TL>
 __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ tasks, int ntasks, int *__restrict__ ticket,
                                                     DevPlan P, const TL *__restrict__ Lx, const TL *__restrict__ Inv,
-                                                    double *__restrict__ y, int *__restrict__ flags, int epoch, int q,
+                                                    const double *__restrict__ Dpiv, double *__restrict__ y,
+                                                    int *__restrict__ flags, int epoch, int q,
                                                     unsigned long long *status) {
   __shared__ int tk, waitOk;
   __shared__ double red[4][kSB];
@@ -346,8 +347,8 @@ __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ 
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         if (lane == 0) red0[warp + 8 * u] = v;
       }
-      double yv = 0.0;
-      if (tid < w) yv = yk[f + c0 + tid];
+      double yv = 0.0;  // LDL^T: y /= D before the backward sweep (ldlt.mjs:629)
+      if (tid < w) yv = Dpiv ? yk[f + c0 + tid] / Dpiv[f + c0 + tid] : yk[f + c0 + tid];
       // the chain step: wait for the next block, then its contribution from the staged tile
       if (hasNext && k == 0) {
         if (tid == 0) waitOk = wait_flag(myflags + blk + 1, epoch, status, s);
@@ -414,9 +415,11 @@ void launch_fwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan
 }
 template <class TL>
 void launch_bwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
-                       double *y, int *flags, int epoch, int q, unsigned long long *status, cudaStream_t st) {
+                       const double *Dpiv, double *y, int *flags, int epoch, int q, unsigned long long *status,
+                       cudaStream_t st) {
   if (ntasks > 0)
-    k_bwd_blocks<TL><<<solve_grid(ntasks), 256, kBwdSmem, st>>>(tasks, ntasks, ticket, P, Lx, Inv, y, flags, epoch, q, status);
+    k_bwd_blocks<TL><<<solve_grid(ntasks), 256, kBwdSmem, st>>>(tasks, ntasks, ticket, P, Lx, Inv, Dpiv, y, flags,
+                                                                 epoch, q, status);
 }
 template void launch_diag_inv<double>(const DevPlan &, int, const double *, double *, cudaStream_t);
 template void launch_diag_inv<float>(const DevPlan &, int, const float *, float *, cudaStream_t);
@@ -427,8 +430,8 @@ template void launch_fwd_blocks<float>(const int4 *, int, int *, const DevPlan &
                                        double *, double *, double *, int *, int, int *, int, int64_t, int64_t,
                                        unsigned long long *, cudaStream_t);
 template void launch_bwd_blocks<double>(const int4 *, int, int *, const DevPlan &, const double *, const double *,
-                                        double *, int *, int, int, unsigned long long *, cudaStream_t);
+                                        const double *, double *, int *, int, int, unsigned long long *, cudaStream_t);
 template void launch_bwd_blocks<float>(const int4 *, int, int *, const DevPlan &, const float *, const float *,
-                                       double *, int *, int, int, unsigned long long *, cudaStream_t);
+                                       const double *, double *, int *, int, int, unsigned long long *, cudaStream_t);
 
 }  // namespace amp

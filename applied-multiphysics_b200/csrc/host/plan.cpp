@@ -269,6 +269,10 @@ void build_plan(const Symbolic &S, Plan &P) {
   P.blkOff.assign(ns + 1, 0);
   for (int s = 0; s < ns; s++) P.blkOff[s + 1] = P.blkOff[s] + (P.snNc[s] + B - 1) / B;
   P.nflags = P.blkOff[ns];
+  P.diagSlot.clear();
+  for (int j = 0; j < S.n; j++)
+    for (int p = S.lowerP[j]; p < S.lowerP[j + 1]; p++)
+      if (S.lowerI[p] == j) P.diagSlot.push_back(S.lowerSrc[p]);
   P.invOff.assign(P.nflags + 1, 0);
   for (int s = 0; s < ns; s++)
     for (int b = 0; b * B < P.snNc[s]; b++) {

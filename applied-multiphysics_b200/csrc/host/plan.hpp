@@ -92,6 +92,7 @@ struct Plan {
   std::vector<int> blkOff;          // first flag of supernode s
   int nflags = 0;
   std::vector<int64_t> invOff;      // per diagonal block (flag index): offset of its w x w inverse; [nflags] = total
+  std::vector<int> diagSlot;        // CSR slot of each diagonal entry of A (LDL^T pivot scale)
   std::vector<int> fwdTasks, bwdTasks;  // int4 records, flattened
   std::vector<int> fwdLvlPtr, bwdLvlPtr;
   std::vector<int> bwdAll;  // backward tasks of all levels, top-down (one launch)

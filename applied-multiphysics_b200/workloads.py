@@ -111,8 +111,17 @@ def heat3d_p2(N: int = 48, nsph: int = 64, radius: float = 0.05, seed: int = 4, 
     return _take(f"heat3d-p2-{N}", lib().amp_wl_heat3d_p2(N, nsph, radius, seed, q))
 
 
-def maxwell3d(N: int = 32, nbox: int = 8, eps_in: float = 12.0, k2: float = 0.0, seed: int = 5, q: int = 64) -> Workload:
-    """Lowest-order Nedelec curl-curl - k2 eps_r mass on N^3 hexes x 6 tets, PEC boundary, port-like RHS."""
+# k^2 of the 32^3 driven Maxwell system: midway between its 10th (34.3115) and 11th (36.2170) nonzero eigenvalues,
+# found by inertia bisection with the GPU LDL^T (maxwell_k2.py 32, on a B200).
+MAXWELL_K2_32 = 35.2642118891234
+
+
+def maxwell3d(N: int = 32, nbox: int = 8, eps_in: float = 12.0, k2: float | None = None, seed: int = 5,
+              q: int = 64) -> Workload:
+    """Lowest-order Nedelec curl-curl - k2 eps_r mass on N^3 hexes x 6 tets, PEC boundary, port-like RHS.
+    k2 defaults to MAXWELL_K2_32 for N = 32 (indefinite: 10 eigenvalues below it besides the gradient null space)."""
+    if k2 is None:
+        k2 = MAXWELL_K2_32 if N == 32 else 0.0
     return _take(f"maxwell3d-{N}", lib().amp_wl_maxwell3d(N, nbox, eps_in, k2, seed, q))
 
 

@@ -76,7 +76,7 @@ typedef enum {
 } amp_field;
 
 typedef struct {
-  int kind;         /* amp_factor_kind */
+  int kind;         /* amp_factor_kind; AMP_LDLT requires AMP_FP64 */
   int precision;    /* amp_precision */
 } amp_factor_opts;
 
@@ -128,7 +128,9 @@ AMP_API void amp_plan_destroy(amp_plan *plan);
  * new SupernodalLDLT(sym) (ldlt.mjs:432-448). */
 AMP_API int amp_factor_create(amp_plan *plan, const amp_factor_opts *opts, amp_factor **out);
 /* factorNumeric(sym, values) (sparse.mjs:941) / SupernodalLDLT.factor(values, {pivotTol}) (ldlt.mjs:450).
- * values: nvalues FP64 in CSR slot order, host memory (values_on_device = 0) or device memory (1). */
+ * values: nvalues FP64 in CSR slot order, host memory (values_on_device = 0) or device memory (1).
+ * LDL^T: pivots with |d| < pivot_tol * max |A(i, i)| become +-that bound (counted in n_perturbed); n_neg counts the
+ * negative pivots (the inertia); a non-finite small pivot gives ok = 0. pivot_tol is ignored for Cholesky. */
 AMP_API int amp_factor_numeric(amp_factor *f, const double *values, int64_t nvalues, int values_on_device, double pivot_tol,
                        amp_factor_result *result);
 /* solveNumeric / solveNumericMulti (sparse.mjs:1261-1310), SupernodalLDLT.solve / solveMany (ldlt.mjs:565-643).
