@@ -59,6 +59,14 @@ class _FactorResult(C.Structure):
                 ("ms", C.c_double)]
 
 
+class _GmresOpts(C.Structure):
+    _fields_ = [("tol", C.c_double), ("restart", C.c_int32), ("max_iter", C.c_int32)]
+
+
+class _GmresStats(C.Structure):
+    _fields_ = [("rel_residual", C.c_double), ("iterations", C.c_int32), ("converged", C.c_int32)]
+
+
 class _KernelStat(C.Structure):
     _fields_ = [("name", C.c_char * 24), ("launches", C.c_int32), ("ms", C.c_double), ("flops", C.c_double),
                 ("bytes", C.c_double)]
@@ -93,6 +101,8 @@ SIGNATURES = {
     "amp_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int]),
     "amp_solve_refined": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int, C.POINTER(_RefineOpts),
                                     C.POINTER(_RefineStats)]),
+    "amp_solve_gmres": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(_GmresOpts),
+                                  C.POINTER(_GmresStats)]),
     "amp_factor_download": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "amp_factor_destroy": (None, [C.c_void_p]),
     "amp_matvec": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
@@ -326,6 +336,17 @@ class NumericFactor:
                                        X.ctypes.data if X.size else None, 0, C.byref(ro), C.byref(st)))
         return X, st.rel_residual, st.steps
 
+    def solve_gmres(self, b, tol: float = 1e-10, restart: int = 40, maxIter: int = 400) -> dict:
+        """gmres(A, precond = this factor's solve, b, {tol, restart, maxIter}) (gmres-real.mjs:31-105) on the device,
+        from x0 = 0: GMRES-based refinement with a mixed-precision factor. Returns {x, iterations, relres,
+        converged} as the reference does."""
+        bb = _f64(b)
+        x = np.empty_like(bb)
+        st = _GmresStats()
+        _check(lib().amp_solve_gmres(self._h, bb.ctypes.data if bb.size else None, x.ctypes.data if x.size else None,
+                                     0, C.byref(_GmresOpts(tol, restart, maxIter)), C.byref(st)))
+        return {"x": x, "iterations": st.iterations, "relres": st.rel_residual, "converged": bool(st.converged)}
+
     @property
     def Lx(self) -> np.ndarray:
         out = np.zeros(max(self.sym.nnzLStored, 1))
@@ -511,11 +532,11 @@ class SupernodalLDLT:
     """Real symmetric LDL^T over a supernodal analysis: 1x1 pivots with static perturbation (|d| < tau -> +-tau,
     tau = pivotTol * max |A(i, i)|), inertia and refinement (ldlt.mjs:431-645). Factor and solves run on the GPU."""
 
-    def __init__(self, sym: SymbolicAnalysis, factor=None):
+    def __init__(self, sym: SymbolicAnalysis, factor=None, precision: int = FP64):
         self.sym = sym
         self.factorKind = factor
         self.kernel = "cuda-sm100a"
-        self.num = NumericFactor(sym, LDLT, FP64)
+        self.num = NumericFactor(sym, LDLT, precision)
         self.nnzL = sym.nnzL
         self.nNeg = 0
         self.nPerturbed = 0
@@ -569,3 +590,9 @@ class SupernodalLDLT:
                                            f"{_nnz_of(self.sym)} entries")
         X, rel, steps = self.num.solve_refined_block(_f64(b)[None, :], maxSteps=maxSteps, tol=tol)
         return {"x": X[0], "relResidual": rel, "steps": steps}
+
+    def solveGmres(self, b, tol: float = 1e-10, restart: int = 40, maxIter: int = 400) -> dict:
+        """FP64 GMRES on the factored matrix preconditioned by this factor (GMRES-IR for a mixed-precision factor of
+        an indefinite matrix, gmres-real.mjs:31-105)."""
+        self._need()
+        return self.num.solve_gmres(b, tol=tol, restart=restart, maxIter=maxIter)

@@ -22,6 +22,12 @@ void launch_matvec(int n, const int *rowptr, const int *colidx, const double *va
 void launch_residual(int n, const int *rowptr, const int *colidx, const double *val, const double *x, const double *b,
                      double *r, double *norms, int q, cudaStream_t st);
 void launch_axpy(double *x, const double *dx, int64_t len, cudaStream_t st);
+void launch_dots(const double *V, int nv, int64_t n, const double *w, double *partial, double *out, cudaStream_t st);
+void launch_gs_update(double *w, const double *V, const double *h, int nv, int64_t n, cudaStream_t st);
+void launch_combine_add(double *x, const double *Z, const double *y, int nv, int64_t n, cudaStream_t st);
+void launch_scale_to(double *v, const double *w, double a, int64_t n, cudaStream_t st);
+void launch_sub_from(double *r, const double *b, const double *y, int64_t n, cudaStream_t st);
+int dot_partials();
 }  // namespace amp
 
 namespace {
@@ -68,6 +74,10 @@ struct DevMem {
     ptrs.clear();
     bytes = 0;
   }
+  DevMem() = default;
+  DevMem(const DevMem &) = delete;
+  DevMem &operator=(const DevMem &) = delete;
+  ~DevMem() { release(); }
 };
 
 }  // namespace
@@ -83,7 +93,10 @@ int64_t inv_elems(const amp::Plan &P) { return P.invOff.empty() ? 0 : P.invOff[P
 // TMA descriptors of the BF16 split columns, two per supernode that has mixed-precision update tiles (hi, lo): the
 // front's m x nc column-major block (ld = round_up(m, 8)) as a 2D tensor {rows, columns}, 64 x 64 boxes with the
 // 128-byte swizzle; reads past m rows or nc columns return zeros, which is how partial tiles and K chunks are padded.
-std::vector<CUtensorMap> split_tensor_maps(const amp::Plan &P, const __nv_bfloat16 *Shi, const __nv_bfloat16 *Slo) {
+// Four per supernode: the A operand (hi, lo) and the B operand (hi, lo); for Cholesky A and B are the same columns,
+// for LDL^T A is the split of L21 D and B the split of L21.
+std::vector<CUtensorMap> split_tensor_maps(const amp::Plan &P, const __nv_bfloat16 *Ahi, const __nv_bfloat16 *Alo,
+                                           const __nv_bfloat16 *Bhi, const __nv_bfloat16 *Blo) {
   using Encode = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                               const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                               CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -98,7 +111,7 @@ std::vector<CUtensorMap> split_tensor_maps(const amp::Plan &P, const __nv_bfloat
   std::vector<char> need(P.nsuper, 0);
   for (const auto *v : {&P.mixTiles, &P.mixUTasks})
     for (const amp::MixTask &t : *v) need[t.s] = 1;
-  std::vector<CUtensorMap> maps(2 * (size_t)std::max(1, P.nsuper));
+  std::vector<CUtensorMap> maps(4 * (size_t)std::max(1, P.nsuper));
   std::memset(maps.data(), 0, sizeof(CUtensorMap) * maps.size());
   for (int s = 0; s < P.nsuper; s++) {
     if (!need[s]) continue;
@@ -106,9 +119,10 @@ std::vector<CUtensorMap> split_tensor_maps(const amp::Plan &P, const __nv_bfloat
     const cuuint64_t dims[2] = {(cuuint64_t)m, (cuuint64_t)nc};
     const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
     const cuuint32_t box[2] = {64, 64}, estr[2] = {1, 1};
-    for (int h = 0; h < 2; h++) {
-      const __nv_bfloat16 *base = (h ? Slo : Shi) + P.snSp[s];
-      CUresult r = encode(&maps[2 * s + h], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void *)base, dims, strides, box, estr,
+    const __nv_bfloat16 *bases[4] = {Ahi, Alo, Bhi, Blo};
+    for (int h = 0; h < 4; h++) {
+      const __nv_bfloat16 *base = bases[h] + P.snSp[s];
+      CUresult r = encode(&maps[4 * s + h], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void *)base, dims, strides, box, estr,
                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
       if (r != CUDA_SUCCESS)
@@ -152,7 +166,8 @@ struct amp_factor_s {
   double *dInv = nullptr;                           // inverses of the 64-column diagonal blocks (FP64 factor)
   float *dInv32 = nullptr;                          // the same for the FP32 factor
   __nv_bfloat16 *dShi = nullptr, *dSlo = nullptr;   // BF16 split columns of the factored pivot blocks
-  CUtensorMap *dMaps = nullptr;                     // per supernode: TMA descriptors of its hi / lo split columns
+  __nv_bfloat16 *dWhi = nullptr, *dWlo = nullptr;   // mixed LDL^T: BF16 split of L21 D
+  CUtensorMap *dMaps = nullptr;                     // per supernode: TMA descriptors of the split A and B operands
   unsigned long long *dStatus = nullptr;
   int *dReaders = nullptr;  // per pivot block: row chunks that have read it (reset at every factorization)
   bool ok = false, hasValues = false;
@@ -175,6 +190,10 @@ struct amp_factor_s {
          *dNorms = nullptr;
   int *dFlags = nullptr, *dTickets = nullptr;  // solve block ready flags (epoch-stamped) and per-launch tickets
   int *dDone = nullptr;                         // forward: finished below tasks per supernode
+  DevMem gmem;                                  // GMRES workspace (Krylov and preconditioned bases), grown on demand
+  int gmresCap = 0;
+  double *gV = nullptr, *gZ = nullptr, *gR = nullptr, *gW = nullptr, *gX = nullptr, *gB = nullptr, *gPart = nullptr,
+         *gH = nullptr;
   unsigned long long *dSolveStatus = nullptr;
   int solveEpoch = 0;
   ~amp_factor_s() {
@@ -281,6 +300,12 @@ void enqueue_factor(amp_factor *f) {
   ck(cudaMemsetAsync(f->dStatus, 0xff, sizeof(unsigned long long), st), "memset status");
   if (P.panelGroups) ck(cudaMemsetAsync(f->dReaders, 0, sizeof(int) * P.panelGroups, st), "memset readers");
   if (f->precision == AMP_MIXED) {
+    amp::LdltArgs<float> ld32{};
+    if (f->kind == AMP_LDLT) {
+      ld32 = amp::LdltArgs<float>{f->dScal, f->dCounts, nullptr, f->dD, f->dWhi, f->dWlo};
+      ck(cudaMemsetAsync(f->dCounts, 0, 2 * sizeof(int), st), "memset counts");
+      amp::launch_ldlt_tau(f->dValues, dp, f->dScal, st);
+    }
     for (int L = 0; L < P.nlevels; L++) {
       timed(f, K_ASSEMBLE, 0.0, P.asmLvlBytes[L] / 2, [&] {
         amp::launch_assemble<float>(f->plan->dAsm + P.asmLvlPtr[L], P.asmLvlPtr[L + 1] - P.asmLvlPtr[L], dp,
@@ -290,7 +315,7 @@ void enqueue_factor(amp_factor *f) {
         const amp::StepRange &sr = P.steps[k];
         timed(f, K_PANEL, sr.panelFlops, 0.0, [&] {
           amp::launch_panel<float>(f->plan->dPanel + sr.panel0, sr.panel1 - sr.panel0, dp, f->dL32, f->dReaders,
-                                   f->dStatus, f->dShi, f->dSlo, amp::LdltArgs<float>{}, st);
+                                   f->dStatus, f->dShi, f->dSlo, ld32, st);
         });
         const int64_t t0 = P.mixStepPtr[k], t1 = P.mixStepPtr[k + 1];
         if (t1 > t0)
@@ -312,7 +337,7 @@ void enqueue_factor(amp_factor *f) {
     return;
   }
   const bool ldlt = f->kind == AMP_LDLT;
-  const amp::LdltArgs<double> ld = ldlt ? amp::LdltArgs<double>{f->dScal, f->dCounts, f->dW, f->dD}
+  const amp::LdltArgs<double> ld = ldlt ? amp::LdltArgs<double>{f->dScal, f->dCounts, f->dW, f->dD, nullptr, nullptr}
                                         : amp::LdltArgs<double>{};
   if (ldlt) {
     ck(cudaMemsetAsync(f->dCounts, 0, 2 * sizeof(int), st), "memset counts");
@@ -368,8 +393,9 @@ void device_solve_permuted(amp_factor *f, int q) {
   });
   timed(f, K_BACKWARD, 0.0, lbytes, [&] {
     if (f->dL32)
-      amp::launch_bwd_blocks<float>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dL32, f->dInv32, nullptr, f->dY,
-                                    f->dFlags, ebwd, q, f->dSolveStatus, st);
+      amp::launch_bwd_blocks<float>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dL32, f->dInv32,
+                                    f->kind == AMP_LDLT ? f->dD : nullptr, f->dY, f->dFlags, ebwd, q,
+                                    f->dSolveStatus, st);
     else
       amp::launch_bwd_blocks<double>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dLx, f->dInv,
                                      f->kind == AMP_LDLT ? f->dD : nullptr, f->dY, f->dFlags, ebwd, q,
@@ -574,8 +600,6 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
     if (opts) o = *opts;
     if (o.kind != AMP_CHOLESKY && o.kind != AMP_LDLT) return fail(AMP_INVALID, "unknown factor kind");
     if (o.precision != AMP_FP64 && o.precision != AMP_MIXED) return fail(AMP_INVALID, "unknown precision");
-    if (o.kind == AMP_LDLT && o.precision != AMP_FP64)
-      return fail(AMP_INVALID, "LDL^T is available in FP64 only in this build");
     ck(cudaSetDevice(pl->device), "cudaSetDevice");
     if (!pl->uploaded) {  // the device schedule is uploaded once, by the first factor of the plan
       upload_plan(pl);
@@ -607,7 +631,15 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
         f->dInv32 = f->mem.alloc<float>((size_t)inv_elems(P));
         f->dShi = f->mem.alloc<__nv_bfloat16>((size_t)P.splitElems);
         f->dSlo = f->mem.alloc<__nv_bfloat16>((size_t)P.splitElems);
-        f->dMaps = f->mem.upload(split_tensor_maps(P, f->dShi, f->dSlo));
+        if (o.kind == AMP_LDLT) {
+          f->dWhi = f->mem.alloc<__nv_bfloat16>((size_t)P.splitElems);
+          f->dWlo = f->mem.alloc<__nv_bfloat16>((size_t)P.splitElems);
+          f->dScal = f->mem.alloc<double>(2);
+          f->dCounts = f->mem.alloc<int>(2);
+          f->dMaps = f->mem.upload(split_tensor_maps(P, f->dWhi, f->dWlo, f->dShi, f->dSlo));
+        } else {
+          f->dMaps = f->mem.upload(split_tensor_maps(P, f->dShi, f->dSlo, f->dShi, f->dSlo));
+        }
       }
       f->dD = f->mem.alloc<double>((size_t)P.n);
       f->dValues = f->mem.alloc<double>((size_t)P.patNnz);
@@ -778,6 +810,129 @@ int amp_solve_refined(amp_factor *f, const double *b, int32_t nrhs, double *x, i
     stt.rel_residual = worst;
     stt.steps = steps;
     if (stats) *stats = stt;
+    return (int)AMP_OK;
+  });
+}
+
+int amp_solve_gmres(amp_factor *f, const double *b, double *x, int on_device, const amp_gmres_opts *opts,
+                    amp_gmres_stats *stats) {
+  return guarded([&] {
+    if (!f) return fail(AMP_INVALID, "null handle");
+    if (!f->ok) return fail(AMP_NO_FACTOR, "solveNumeric: no successful numeric factorization");
+    amp_gmres_opts o{1e-10, 40, 400};
+    if (opts) o = *opts;
+    if (o.restart < 1 || o.max_iter < 0) return fail(AMP_INVALID, "gmres: restart >= 1 and maxIter >= 0 required");
+    const amp::Plan &P = f->plan->P;
+    const int64_t n = P.n;
+    amp_gmres_stats res{0.0, 0, 1};
+    if (n == 0) {
+      if (stats) *stats = res;
+      return (int)AMP_OK;
+    }
+    ck(cudaSetDevice(f->plan->device), "cudaSetDevice");
+    ensure_solve_ws(f, 1);
+    cudaStream_t st = f->stream;
+    const int m = o.restart;
+    // workspace (kept by the factor): V (m + 1 vectors), Z (m), r, w, x, b, dot partials and results
+    if (m > f->gmresCap) {
+      f->gmem.release();
+      f->gV = f->gmem.alloc<double>((size_t)(m + 1) * n);
+      f->gZ = f->gmem.alloc<double>((size_t)m * n);
+      f->gR = f->gmem.alloc<double>((size_t)n);
+      f->gW = f->gmem.alloc<double>((size_t)n);
+      f->gX = f->gmem.alloc<double>((size_t)n);
+      f->gB = f->gmem.alloc<double>((size_t)n);
+      f->gPart = f->gmem.alloc<double>((size_t)(m + 1) * amp::dot_partials());
+      f->gH = f->gmem.alloc<double>((size_t)m + 1);
+      f->gmresCap = m;
+    }
+    double *V = f->gV, *Z = f->gZ, *r = f->gR, *w = f->gW, *xb = f->gX, *bb = f->gB, *part = f->gPart, *dh = f->gH;
+    ck(cudaMemcpyAsync(bb, b, sizeof(double) * n, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st),
+       "copy b");
+    ck(cudaMemsetAsync(xb, 0, sizeof(double) * n, st), "zero x");
+    std::vector<double> h(m + 1), H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
+    auto dots = [&](const double *Vs, int nv, const double *v) {  // h[0..nv) = Vs[j] . v (synchronises)
+      amp::launch_dots(Vs, nv, n, v, part, dh, st);
+      ck(cudaMemcpyAsync(h.data(), dh, sizeof(double) * nv, cudaMemcpyDeviceToHost, st), "dots");
+      ck(cudaStreamSynchronize(st), "dots");
+    };
+    auto residual = [&]() {  // r = b - A x, returns ||r||
+      amp::launch_matvec((int)n, f->plan->dRowptr, f->plan->dColidx, f->dValues, xb, w, 1, st);
+      amp::launch_sub_from(r, bb, w, n, st);
+      dots(r, 1, r);
+      return std::sqrt(h[0]);
+    };
+    auto precond = [&](const double *v, double *z) {  // z = M^-1 v (the factor's solve)
+      device_solve(f, v, z, 1);
+      ck(cudaGetLastError(), "kernel launch");
+    };
+    dots(bb, 1, bb);
+    double bnorm = std::sqrt(h[0]);
+    if (bnorm == 0) bnorm = 1;
+    ck(cudaMemcpyAsync(r, bb, sizeof(double) * n, cudaMemcpyDeviceToDevice, st), "r = b");
+    double beta = bnorm == 1 && h[0] == 0 ? 0.0 : std::sqrt(h[0]);
+    double relres = beta / bnorm;
+    int iters = 0;
+    while (relres > o.tol && iters < o.max_iter) {
+      amp::launch_scale_to(V, r, 1.0 / beta, n, st);
+      std::fill(g.begin(), g.end(), 0.0);
+      g[0] = beta;
+      int k = 0;
+      for (; k < m && iters < o.max_iter; k++) {
+        iters++;
+        precond(V + (int64_t)k * n, Z + (int64_t)k * n);
+        amp::launch_matvec((int)n, f->plan->dRowptr, f->plan->dColidx, f->dValues, Z + (int64_t)k * n, w, 1, st);
+        // classical Gram-Schmidt twice (as stable as modified Gram-Schmidt, two reductions per iteration)
+        for (int j = 0; j <= k; j++) H[(size_t)j * m + k] = 0.0;
+        for (int pass = 0; pass < 2; pass++) {
+          dots(V, k + 1, w);
+          ck(cudaMemcpyAsync(dh, h.data(), sizeof(double) * (k + 1), cudaMemcpyHostToDevice, st), "h");
+          amp::launch_gs_update(w, V, dh, k + 1, n, st);
+          for (int j = 0; j <= k; j++) H[(size_t)j * m + k] += h[j];
+        }
+        dots(w, 1, w);
+        const double hn = std::sqrt(h[0]);
+        H[(size_t)(k + 1) * m + k] = hn;
+        if (hn > 0) amp::launch_scale_to(V + (int64_t)(k + 1) * n, w, 1.0 / hn, n, st);
+        for (int j = 0; j < k; j++) {  // apply the previous Givens rotations
+          const double a = H[(size_t)j * m + k], c = H[(size_t)(j + 1) * m + k];
+          H[(size_t)j * m + k] = cs[j] * a + sn[j] * c;
+          H[(size_t)(j + 1) * m + k] = -sn[j] * a + cs[j] * c;
+        }
+        const double a = H[(size_t)k * m + k], c = H[(size_t)(k + 1) * m + k];
+        double d = std::hypot(a, c);
+        if (d == 0) d = 1e-300;
+        cs[k] = a / d;
+        sn[k] = c / d;
+        H[(size_t)k * m + k] = d;
+        H[(size_t)(k + 1) * m + k] = 0.0;
+        g[k + 1] = -sn[k] * g[k];
+        g[k] = cs[k] * g[k];
+        relres = std::fabs(g[k + 1]) / bnorm;
+        if (relres <= o.tol || hn == 0) {
+          k++;
+          break;
+        }
+      }
+      for (int i = k - 1; i >= 0; i--) {  // back substitution, then x += Z y
+        double s = g[i];
+        for (int j = i + 1; j < k; j++) s -= H[(size_t)i * m + j] * y[j];
+        y[i] = s / H[(size_t)i * m + i];
+      }
+      ck(cudaMemcpyAsync(dh, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st), "y");
+      amp::launch_combine_add(xb, Z, dh, k, n, st);
+      if (relres <= o.tol || iters >= o.max_iter) break;
+      beta = residual();
+      relres = beta / bnorm;
+    }
+    res.rel_residual = residual() / bnorm;
+    res.iterations = iters;
+    res.converged = res.rel_residual <= std::max(o.tol * 10, 1e-14);
+    ck(cudaMemcpyAsync(x, xb, sizeof(double) * n, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st),
+       "copy x");
+    ck(cudaStreamSynchronize(st), "gmres");
+    if (int rc = solve_status(f)) return rc;
+    if (stats) *stats = res;
     return (int)AMP_OK;
   });
 }

@@ -1,5 +1,7 @@
 // Device-side view of a plan (plain pointers into device memory; passed by value to every kernel).
 #pragma once
+#include <cuda_bf16.h>
+
 #include <cstdint>
 
 namespace amp {
@@ -24,8 +26,9 @@ template <class T>
 struct LdltArgs {
   const double *scal;  // [0] pivotTol (copied per factorization), [1] tau = pivotTol * max |A(i, i)| (device)
   int *counts;         // [0] nNeg, [1] nPerturbed
-  T *W;                // L21 D (rows of the solved panel times the pivots): the A operand of the update
+  T *W;                // L21 D (rows of the solved panel times the pivots): the A operand of the FP64 update
   double *D;           // the pivots, permuted order
+  __nv_bfloat16 *Whi, *Wlo;  // mixed precision: BF16 split of L21 D (the A operand of the tensor-core update)
 };
 
 // Failure record: the lowest failing global column wins (atomicMin), code in the low bits.

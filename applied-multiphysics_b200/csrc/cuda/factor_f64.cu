@@ -301,12 +301,18 @@ __global__ void __launch_bounds__(256, 1) k_panel(const PanelTask *__restrict__ 
     for (int c = 0; c < Q; c++) {
       if (q0 + c < w) {
         Lp[(int64_t)(c0 + q0 + c) * m + r] = x[c];
-        if (ldlt) ld.W[P.snLxp[s] + (int64_t)(c0 + q0 + c) * m + r] = x[c] * piv[q0 + c];
+        const T wv = ldlt ? x[c] * piv[q0 + c] : T(0);
+        if (ldlt && ld.W) ld.W[P.snLxp[s] + (int64_t)(c0 + q0 + c) * m + r] = wv;
         if (Shi) {
           const int64_t g = P.snSp[s] + (int64_t)(c0 + q0 + c) * ((m + 7) & ~7) + r;
           const __nv_bfloat16 hi = __float2bfloat16_rn((float)x[c]);
           Shi[g] = hi;
           Slo[g] = __float2bfloat16_rn((float)x[c] - __bfloat162float(hi));
+          if (ldlt) {
+            const __nv_bfloat16 whi = __float2bfloat16_rn((float)wv);
+            ld.Whi[g] = whi;
+            ld.Wlo[g] = __float2bfloat16_rn((float)wv - __bfloat162float(whi));
+          }
         }
       }
       xs[(q0 + c) * 256 + tid] = x[c];

@@ -20,25 +20,59 @@ __global__ void k_matvec(int n, const int *__restrict__ rowptr, const int *__res
   if (lane == 0) y[(int64_t)k * n + i] = s;
 }
 
-// r = b - A x; norms[2k] += ||r_k||^2, norms[2k+1] += ||b_k||^2 (zeroed by the caller)
-__global__ void k_residual(int n, const int *__restrict__ rowptr, const int *__restrict__ colidx,
-                           const double *__restrict__ val, const double *__restrict__ x, const double *__restrict__ b,
-                           double *__restrict__ r, double *__restrict__ norms, int q) {
-  const int lane = threadIdx.x & 31;
+// r = b - A x; norms[2k] += ||r_k||^2, norms[2k+1] += ||b_k||^2 (zeroed by the caller). One warp per row; the
+// squares are summed per block in shared memory and added with one atomic pair per block and vector.
+__global__ void __launch_bounds__(256) k_residual(int n, const int *__restrict__ rowptr, const int *__restrict__ colidx,
+                                                  const double *__restrict__ val, const double *__restrict__ x,
+                                                  const double *__restrict__ b, double *__restrict__ r,
+                                                  double *__restrict__ norms, int q) {
+  __shared__ double rr[8], bb[8];
+  __shared__ int kk[8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (row >= (int64_t)n * q) return;
-  const int k = (int)(row / n), i = (int)(row % n);
-  const double *xk = x + (int64_t)k * n;
-  double s = 0.0;
-  for (int p = rowptr[i] + lane; p < rowptr[i + 1]; p += 32) s += val[p] * xk[colidx[p]];
+  double ri2 = 0.0, bi2 = 0.0;
+  int k = -1;
+  if (row < (int64_t)n * q) {
+    k = (int)(row / n);
+    const int i = (int)(row % n);
+    const double *xk = x + (int64_t)k * n;
+    double s = 0.0;
+    for (int p = rowptr[i] + lane; p < rowptr[i + 1]; p += 32) s += val[p] * xk[colidx[p]];
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+      const double bi = b[(int64_t)k * n + i];
+      const double ri = bi - s;
+      r[(int64_t)k * n + i] = ri;
+      ri2 = ri * ri;
+      bi2 = bi * bi;
+    }
+  }
   if (lane == 0) {
-    const double bi = b[(int64_t)k * n + i];
-    const double ri = bi - s;
-    r[(int64_t)k * n + i] = ri;
-    atomicAdd(norms + 2 * k, ri * ri);
-    atomicAdd(norms + 2 * k + 1, bi * bi);
+    rr[warp] = ri2;
+    bb[warp] = bi2;
+    kk[warp] = k;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {  // consecutive rows: one atomic pair per run of rows of the same vector
+    int cur = -1;
+    double a = 0.0, c = 0.0;
+    for (int w = 0; w < 8; w++) {
+      if (kk[w] != cur) {
+        if (cur >= 0) {
+          atomicAdd(norms + 2 * cur, a);
+          atomicAdd(norms + 2 * cur + 1, c);
+        }
+        cur = kk[w];
+        a = c = 0.0;
+      }
+      a += rr[w];
+      c += bb[w];
+    }
+    if (cur >= 0) {
+      atomicAdd(norms + 2 * cur, a);
+      atomicAdd(norms + 2 * cur + 1, c);
+    }
   }
 }
 

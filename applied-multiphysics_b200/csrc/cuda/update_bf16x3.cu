@@ -1,9 +1,10 @@
 // Mixed-precision trailing / update-block tiles on the 5th-generation tensor cores (tcgen05, sm_100a).
 //
-// C[i0:i0+128, j0:j0+256] -= A B^T in FP32, where A and B are rows of the factored pivot columns of a front and the
-// product runs as BF16x3: every FP32 value x is carried as hi = bf16(x), lo = bf16(x - hi) (split once, by the panel
-// kernel, into the split buffers) and A B^T ~= Ahi Bhi^T + Ahi Blo^T + Alo Bhi^T with FP32 accumulation in tensor
-// memory (the dropped Alo Blo^T term is ~2^-16 relative).
+// C[i0:i0+128, j0:j0+256] -= A B^T in FP32, where A and B are rows of the factored pivot columns of a front (for
+// LDL^T, A holds those rows times the pivots, L21 D) and the product runs as BF16x3: every FP32 value x is carried
+// as hi = bf16(x), lo = bf16(x - hi) (split once, by the panel kernel, into the split buffers) and
+// A B^T ~= Ahi Bhi^T + Ahi Blo^T + Alo Bhi^T with FP32 accumulation in tensor memory (the dropped Alo Blo^T term is
+// ~2^-16 relative).
 //
 // Persistent, one CTA per SM, warp-specialised:
 //   warp 0      TMA producer: per 64-column K chunk, 12 boxes of 64 rows x 64 columns (A and B, hi and lo) from the
@@ -101,7 +102,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_update_mx(const MixTask *__rest
       int it = 0;
       for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
         const MixTask tk = tasks[t];
-        const CUtensorMap *mhi = maps + 2 * tk.s, *mlo = mhi + 1;
+        const CUtensorMap *ahi = maps + 4 * tk.s, *alo = ahi + 1, *bhi = ahi + 2, *blo = ahi + 3;
         const int nch = (tk.w + kK - 1) / kK;
         bool ok = true;
         for (int c = 0; c < nch; c++, it++) {
@@ -116,13 +117,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_update_mx(const MixTask *__rest
           const int kc = tk.c0 + c * kK;
 #pragma unroll
           for (int b = 0; b < kM / kBox; b++) {
-            umma::tma_load_2d(st + b * kBoxBytes, mhi, tk.i0 + kBox * b, kc, &sh.full[s]);
-            umma::tma_load_2d(st + kABytes + b * kBoxBytes, mlo, tk.i0 + kBox * b, kc, &sh.full[s]);
+            umma::tma_load_2d(st + b * kBoxBytes, ahi, tk.i0 + kBox * b, kc, &sh.full[s]);
+            umma::tma_load_2d(st + kABytes + b * kBoxBytes, alo, tk.i0 + kBox * b, kc, &sh.full[s]);
           }
 #pragma unroll
           for (int b = 0; b < kN / kBox; b++) {
-            umma::tma_load_2d(st + 2 * kABytes + b * kBoxBytes, mhi, tk.j0 + kBox * b, kc, &sh.full[s]);
-            umma::tma_load_2d(st + 2 * kABytes + kBBytes + b * kBoxBytes, mlo, tk.j0 + kBox * b, kc, &sh.full[s]);
+            umma::tma_load_2d(st + 2 * kABytes + b * kBoxBytes, bhi, tk.j0 + kBox * b, kc, &sh.full[s]);
+            umma::tma_load_2d(st + 2 * kABytes + kBBytes + b * kBoxBytes, blo, tk.j0 + kBox * b, kc, &sh.full[s]);
           }
         }
         if (!ok) break;

@@ -138,3 +138,22 @@ def hex_q1(nx: int = 6, ny: int = 5, nz: int = 4) -> Workload:
 def chain(n: int, diag: float = 2.0, off: float = -1.0) -> Workload:
     """1D chain tridiag(off, diag, off) of the reference's core-solvers tests."""
     return _take("chain", lib().amp_wl_chain(n, diag, off))
+
+
+def heat2d_batch_sizes(count: int = 256, seed: int = 3) -> list[tuple[int, int]]:
+    """(N, q) of the batched 2D heat set: N ~ U{16..128} cells per side, q ~ U{1..64} right-hand sides, from the
+    uint32 LCG s = s * 1664525 + 1013904223."""
+    s = seed & 0xFFFFFFFF
+    out = []
+    for _ in range(count):
+        s = (s * 1664525 + 1013904223) & 0xFFFFFFFF
+        N = 16 + (s >> 8) % 113
+        s = (s * 1664525 + 1013904223) & 0xFFFFFFFF
+        q = 1 + (s >> 8) % 64
+        out.append((int(N), int(q)))
+    return out
+
+
+def heat2d_batch(count: int = 256, seed: int = 3) -> list[Workload]:
+    """The batched 2D heat set: `count` lognormal-conductivity P1 problems of uneven size with q_i seeded RHS each."""
+    return [heat2d_lognormal(N, seed * 1000 + i, q) for i, (N, q) in enumerate(heat2d_batch_sizes(count, seed))]

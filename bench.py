@@ -26,9 +26,25 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "applied-multiphysics_b200"))
 
-METRIC = "factor+solve TFLOP/s to rel. residual <= 1e-12 (3D P1 elasticity {N}^3, 1 x B200)"
+METRIC = "factor+solve TFLOP/s to rel. residual <= 1e-12 ({title}, 1 x B200)"
 UNIT = "TFLOP/s"
-WORKLOAD = "elastic3d-{N}: 3D P1 linear elasticity, {N}^3 hexes x 6 tets, E=1 nu=0.3, x=0 clamped, nd3Order"
+# the benchmark systems: elasticity (the headline), P2 heat and Nedelec Maxwell (indefinite, LDL^T)
+SYSTEMS = {
+    "elastic3d": {"size": 40, "title": "3D P1 elasticity {N}^3", "kind": "chol",
+                  "desc": "elastic3d-{N}: 3D P1 linear elasticity, {N}^3 hexes x 6 tets, E=1 nu=0.3, x=0 clamped, "
+                          "nd3Order"},
+    "heat3d_p2": {"size": 48, "title": "3D P2 heat {N}^3", "kind": "chol",
+                  "desc": "heat3d-p2-{N}: 3D P2 (tet10) heat, {N}^3 hexes x 6 tets, k=100 in 64 seeded spheres "
+                          "(r=0.05) else 1, Dirichlet x=0 and x=1, nd3Order"},
+    "heat2d_batch": {"size": 256, "title": "batched 2D P1 heat, {N} problems", "kind": "batch",
+                     "desc": "heat2d-batch-{N}: {N} P1 heat problems on unit squares, N ~ U{{16..128}} cells per side, "
+                             "lognormal(0,1) conductivity, Dirichlet, 1-64 RHS each; AMD per matrix, one "
+                             "block-diagonal factorization"},
+    "maxwell3d": {"size": 32, "title": "3D Nedelec Maxwell {N}^3, LDL^T", "kind": "ldlt",
+                  "desc": "maxwell3d-{N}: lowest-order Nedelec curl-curl - k^2 eps_r mass, {N}^3 hexes x 6 tets, "
+                          "eps_r=12 in 8 seeded boxes, PEC, k^2 between the 10th and 11th eigenvalues, nd3Order on "
+                          "edge midpoints"},
+}
 
 
 def peaks():
@@ -90,8 +106,34 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_system(size: int = 40):
+class _Batch:
+    """The batched heat set as one block-diagonal system (pattern, values, q_max RHS) with per-matrix AMD orders."""
+
+    def __init__(self, count: int):
+        import workloads as wl
+        import ampsolve as amp
+        import batch
+        ws = wl.heat2d_batch(count)
+        self.pat, offs, _ = batch.block_diagonal([w.pat for w in ws])
+        self.values = np.concatenate([w.values for w in ws])
+        q = max(w.rhs.shape[0] for w in ws)
+        self.rhs = np.zeros((q, self.pat.n))
+        for i, w in enumerate(ws):
+            self.rhs[: w.rhs.shape[0], offs[i]: offs[i + 1]] = w.rhs
+        self.perm = np.concatenate([amp.amdOrder(w.pat) + offs[i] for i, w in enumerate(ws)]).astype(np.int32)
+        self.offs, self.q = offs, [w.rhs.shape[0] for w in ws]
+        self.n = self.pat.n
+        self.x = self.y = self.z = None
+
+
+def make_system(name: str = "elastic3d", size: int = 40):
     import workloads as wl
+    if name == "heat2d_batch":
+        return _Batch(size)
+    if name == "heat3d_p2":
+        return wl.heat3d_p2(size, q=1)
+    if name == "maxwell3d":
+        return wl.maxwell3d(size, q=1)
     return wl.elastic3d(size, seed=2, q=1)
 
 
@@ -134,10 +176,16 @@ def measure_sgemm(torch):
     return 2 * 8192 ** 3 / ms / 1e9
 
 
-def cpu_baseline_sample(w, perm, budget_s: float = 15.0):
-    """Oracle (SSE2 restatement of the reference's WASM front kernel) on one complete subtree of the factorization."""
+def cpu_baseline_sample(w, perm, budget_s: float = 15.0, kind: str = "chol"):
+    """Oracle (SSE2 restatement of the reference's WASM front kernel) on one complete subtree of the factorization,
+    pinned to one core (the reference's solver is single-threaded)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
+    try:
+        keep = os.sched_getaffinity(0)
+        os.sched_setaffinity(0, {min(keep)})
+    except (AttributeError, OSError):
+        keep = None
     so = orc.analyze(w.pat, perm=perm)
     # subtree flops
     ns = so.nsuper
@@ -153,17 +201,19 @@ def cpu_baseline_sample(w, perm, budget_s: float = 15.0):
     order = np.argsort(sub)
     small = int(order[np.searchsorted(sub[order], 2e8)]) if np.any(sub >= 2e8) else int(order[-1])
     t = time.perf_counter()
-    orc.factor_subtree(so, w.values, small, simd=True)
+    orc.factor_subtree(so, w.values, small, kind=kind, simd=True)
     rate = sub[small] / max(time.perf_counter() - t, 1e-6)
     target = rate * budget_s
     cand = np.where(sub <= target)[0]
     root = int(cand[np.argmax(sub[cand])]) if cand.size else small
     t = time.perf_counter()
-    ok, fl = orc.factor_subtree(so, w.values, root, simd=True)
+    ok, fl = orc.factor_subtree(so, w.values, root, kind=kind, simd=True)
     dt = time.perf_counter() - t
+    if keep:
+        os.sched_setaffinity(0, keep)
     return {"value": fl / dt / 1e12, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"factor of the subtree of supernode {root} ({fl:.3e} of {so.flops:.3e} flops, "
-                      f"{dt:.1f} s, SSE2 restatement of the reference's WASM front kernel, 1 thread); "
+                      f"{dt:.1f} s, SSE2 restatement of the reference's WASM front kernel, 1 pinned thread); "
                       f"extrapolated full factor {so.flops / (fl / dt):.0f} s",
             "full_factor_s_est": so.flops / (fl / dt)}
 
@@ -172,26 +222,27 @@ def run_reference(args, rank):
     if rank != 0:
         return
     import workloads as wl  # noqa: F401
-    w = make_system(args.size)
+    w = make_system(args.workload, args.size)
     import ampsolve as amp
     try:
-        perm = amp.nd3Order(w.pat, w.x, w.y, w.z)
+        perm = w.perm if isinstance(w, _Batch) else amp.nd3Order(w.pat, w.x, w.y, w.z)
     except Exception:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as orc
         perm = orc.nd3_order(w.pat, w.x, w.y, w.z)
     times, vals = [], []
     for it in range(args.warmup + args.steps):
-        cb = cpu_baseline_sample(w, perm, budget_s=max(5.0, 60.0 / max(1, args.warmup + args.steps)))
+        cb = cpu_baseline_sample(w, perm, budget_s=max(5.0, 60.0 / max(1, args.warmup + args.steps)),
+                                 kind="ldlt" if args.ldlt else "chol")
         if it >= args.warmup:
             vals.append(cb["value"])
             times.append(0)
     v = float(np.median(vals))
-    line = {"impl": "reference", "metric": METRIC.format(N=args.size), "value": v, "unit": UNIT, "n_gpus": args.gpus,
+    line = {"impl": "reference", "metric": args.metric, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD.format(N=args.size), "n": w.n, "nnz": w.pat.nnz, "sample": cb["sample"]},
+            "config": {"workload": args.desc, "n": w.n, "nnz": w.pat.nnz, "sample": cb["sample"]},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": cb["sample"]},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -205,8 +256,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--size", type=int, default=40, help="hexes per side (40 = the benchmark; smaller for profiling)")
+    ap.add_argument("--workload", default="elastic3d", choices=sorted(SYSTEMS))
+    ap.add_argument("--size", type=int, default=0, help="hexes per side (0 = the system's benchmark size)")
     args = ap.parse_args()
+    sysinfo = SYSTEMS[args.workload]
+    args.size = args.size or sysinfo["size"]
+    args.metric = METRIC.format(title=sysinfo["title"].format(N=args.size))
+    args.desc = sysinfo["desc"].format(N=args.size)
+    args.ldlt = sysinfo["kind"] == "ldlt"
+    if args.ldlt:  # LDL^T runs in FP64 only
+        args.precision = "fp64"
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -222,27 +281,35 @@ def main():
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    w = make_system(args.size)
+    w = make_system(args.workload, args.size)
     n = w.n
     t0 = time.perf_counter()
-    sym = amp.analyze(w.pat, ordering="nd3", x=w.x, y=w.y, z=w.z, device=local)
+    if isinstance(w, _Batch):
+        sym = amp.analyze(w.pat, perm=w.perm, device=local)
+    else:
+        sym = amp.analyze(w.pat, ordering="nd3", x=w.x, y=w.y, z=w.z, device=local)
     symbolic_ms = (time.perf_counter() - t0) * 1e3
     flops_factor = sym.flops
     flops_solve = 4.0 * sym.nnzL  # per right-hand side (forward + backward)
+    nq = 1
+    if isinstance(w, _Batch):  # every matrix solves its own q_i vectors: 4 nnzL_i q_i
+        cc = sym.colCount.astype(np.float64)
+        flops_solve = sum(4.0 * cc[w.offs[i]: w.offs[i + 1]].sum() * qi for i, qi in enumerate(w.q))
+        nq = w.rhs.shape[0]
 
     precisions = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
     results = {}
     dev = torch.device("cuda", local)
     vals_d = torch.from_numpy(w.values).to(dev)
-    b_d = torch.from_numpy(w.rhs[0].copy()).to(dev)
+    b_d = torch.from_numpy(np.ascontiguousarray(w.rhs[:nq]).reshape(-1)).to(dev)
     x_d = torch.empty_like(b_d)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
     for prec in precisions:
-        num = amp.NumericFactor(sym, amp.CHOLESKY, amp.FP64 if prec == "fp64" else amp.MIXED)
+        num = amp.NumericFactor(sym, amp.LDLT if args.ldlt else amp.CHOLESKY, amp.FP64 if prec == "fp64" else amp.MIXED)
 
         def step():
             ok = num.factor((vals_d.data_ptr(), vals_d.numel()), on_device=True)
-            relres, steps = num.solve_refined_device(b_d.data_ptr(), x_d.data_ptr(), 1, maxSteps=10, tol=1e-12)
+            relres, steps = num.solve_refined_device(b_d.data_ptr(), x_d.data_ptr(), nq, maxSteps=10, tol=1e-12)
             return ok, relres, steps
 
         for _ in range(args.warmup):
@@ -266,7 +333,7 @@ def main():
             ms = float(t.item())
         # end to end through the C ABI with host buffers (pinned): H2D values + b, D2H x, every step
         vals_h = torch.from_numpy(w.values).pin_memory()
-        b_h = torch.from_numpy(w.rhs[0].copy()).pin_memory()
+        b_h = torch.from_numpy(np.ascontiguousarray(w.rhs[:nq]).reshape(-1)).pin_memory()
         x_h = torch.empty_like(b_h).pin_memory()
         e2e = []
         for k in range(max(2, args.steps)):
@@ -275,7 +342,7 @@ def main():
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record()
             num.factor(vals_h.numpy())  # H2D of the values inside the call
-            rr, ss = num.solve_refined_host_pinned(b_h.data_ptr(), x_h.data_ptr(), 1, 10, 1e-12)  # H2D b, D2H x
+            rr, ss = num.solve_refined_host_pinned(b_h.data_ptr(), x_h.data_ptr(), nq, 10, 1e-12)  # H2D b, D2H x
             b.record()
             torch.cuda.synchronize()
             e2e.append(a.elapsed_time(b))
@@ -287,7 +354,7 @@ def main():
         # profile pass: per-kernel device time with CUDA events on the factor's stream
         num.profile(True)
         num.factor((vals_d.data_ptr(), vals_d.numel()), on_device=True)
-        num.solve_refined_device(b_d.data_ptr(), x_d.data_ptr(), 1, maxSteps=10, tol=1e-12)
+        num.solve_refined_device(b_d.data_ptr(), x_d.data_ptr(), nq, maxSteps=10, tol=1e-12)
         prof = num.profile_read()
         num.profile(False)
         work = flops_factor + flops_solve  # the same algorithmic work for both precisions: factor + one solve
@@ -319,18 +386,18 @@ def main():
     launches = sum(k["launches"] for k in R["prof"])
     value = world * R["work"] / (R["ms"] * 1e-3) / 1e12
     line = {
-        "metric": METRIC.format(N=args.size), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": args.metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup,
         "ms_per_step": R["ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if head == "fp64" else "f32+bf16x3 (f64 refinement)", "data": "synthetic",
-        "config": {"workload": WORKLOAD.format(N=args.size), "n": n, "nnz": w.pat.nnz, "nnzL": sym.nnzL,
+        "config": {"workload": args.desc, "n": n, "nnz": w.pat.nnz, "nnzL": sym.nnzL,
                    "flops_factor": flops_factor,
                    "maxFront": sym.maxFront, "nsuper": sym.nsuper, "levels": sym.nlevels, "precision": head,
                    "l2": "flushed between timed steps (256 MB write)", "parallelism": "replicas" if world > 1 else "1 gpu",
                    "symbolic_ms": symbolic_ms},
         "relres": R["relres"], "ir_steps": R["ir_steps"], "factor_ms": R["factor_ms"],
         "e2e": {"value": world * R["work"] / (R["e2e_ms"] * 1e-3) / 1e12, "unit": UNIT,
-                "h2d_bytes_per_step": int(8 * w.pat.nnz + 8 * n), "d2h_bytes_per_step": int(8 * n),
+                "h2d_bytes_per_step": int(8 * w.pat.nnz + 8 * n * nq), "d2h_bytes_per_step": int(8 * n * nq),
                 "ms_per_step": R["e2e_ms"]},
         "gpu_launches": int(launches * args.steps),
         "clocks": R["clk"],
@@ -344,7 +411,8 @@ def main():
         line[p] = {"ms_per_step": r["ms"], "value": world * r["work"] / (r["ms"] * 1e-3) / 1e12, "relres": r["relres"],
                    "ir_steps": r["ir_steps"], "factor_ms": r["factor_ms"], "ok": r["ok"]}
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = {k: v for k, v in cpu_baseline_sample(w, sym.perm).items() if k != "full_factor_s_est"}
+        cb = cpu_baseline_sample(w, sym.perm, kind="ldlt" if args.ldlt else "chol")
+        line["cpu_baseline"] = {k: v for k, v in cb.items() if k != "full_factor_s_est"}
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -98,6 +98,18 @@ typedef struct {
   int32_t steps;        /* max over the right-hand sides */
 } amp_refine_stats;
 
+typedef struct {
+  double tol;           /* stop when the residual estimate / ||b|| <= tol (reference default 1e-10) */
+  int32_t restart;      /* Krylov vectors per cycle (reference default 40) */
+  int32_t max_iter;     /* total iterations (reference default 400) */
+} amp_gmres_opts;
+
+typedef struct {
+  double rel_residual;  /* true ||b - A x|| / ||b|| of the returned x */
+  int32_t iterations;
+  int32_t converged;    /* rel_residual <= max(10 tol, 1e-14), as the reference reports */
+} amp_gmres_stats;
+
 /* ---- orderings (host) ---- */
 /* amdOrder(pat, {denseFactor}) (sparse.mjs:297-592). perm: n entries, new -> old. */
 AMP_API int amp_amd_order(int32_t n, const int32_t *rowptr, const int32_t *colidx, double dense_factor, int32_t *perm);
@@ -140,6 +152,11 @@ AMP_API int amp_solve(amp_factor *f, const double *b, int32_t nrhs, double *x, i
  * of the last amp_factor_numeric call (the unperturbed matrix). */
 AMP_API int amp_solve_refined(amp_factor *f, const double *b, int32_t nrhs, double *x, int on_device,
                       const amp_refine_opts *opts, amp_refine_stats *stats);
+/* gmres(matvec, precond, b, {tol, restart, maxIter}) (gmres-real.mjs:31-105) with matvec = the factored matrix (FP64
+ * CSR on the device) and precond = this factor's solve: restarted, right-preconditioned GMRES from x0 = 0, so with a
+ * mixed-precision factor it is GMRES-based iterative refinement. One right-hand side; b, x host or device memory. */
+AMP_API int amp_solve_gmres(amp_factor *f, const double *b, double *x, int on_device, const amp_gmres_opts *opts,
+                    amp_gmres_stats *stats);
 /* num.Lx (the m x nc column-major blocks at Lxp) and D (LDL^T) copied to host; either pointer may be null. */
 AMP_API int amp_factor_download(const amp_factor *f, double *Lx, double *D);
 AMP_API void amp_factor_destroy(amp_factor *f);

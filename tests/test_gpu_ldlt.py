@@ -46,6 +46,10 @@ def shifted(w, sigma):
     return v
 
 
+def relres(pat, vals, x, b):
+    return float(np.linalg.norm(O.matvec(pat, vals, x) - b) / np.linalg.norm(b))
+
+
 def lower_parts(sym, Lx):
     out = []
     for s in range(sym.nsuper):
@@ -143,3 +147,42 @@ def test_ldlt_nonfinite_pivot_fails_and_solve_raises():
     with pytest.raises(A.AmpError, match="no successful numeric factorization"):
         f.solve(np.ones(w.n))
     assert f.factor(shifted(w, 30.0))["ok"]  # the same object factors again
+
+
+# ---- mixed precision (FP32 fronts, BF16x3 tensor-core updates) + FP64 GMRES-IR (gmres-real.mjs:31-105) ----------
+MIXED_CASES = [
+    ("grid27-10-shift30", lambda: W.grid27(10, 10, 10, sym=True), 30.0, {}),
+    ("maxwell3d-8-k2", lambda: W.maxwell3d(8, 2, 12.0, 40.0, 5, 1), 0.0, {"ordering": "nd3"}),
+    ("elastic3d-12-shift", lambda: W.elastic3d(12), None, {"ordering": "nd3"}),
+]
+
+
+@pytest.mark.parametrize("name,make,sigma,kw", MIXED_CASES, ids=[c[0] for c in MIXED_CASES])
+def test_mixed_ldlt_gmres_ir(name, make, sigma, kw):
+    w = make()
+    if sigma is None:
+        sigma = 0.05 * float(np.median(w.values[diag_slots(w.pat)]))
+    if kw.get("ordering") == "nd3":
+        kw = dict(kw, x=w.x, y=w.y, z=w.z)
+    vals = shifted(w, sigma) if sigma else w.values
+    sym = A.analyze(w.pat, **kw)
+    f64 = A.SupernodalLDLT(sym)
+    r64 = f64.factor(vals)
+    fmx = A.SupernodalLDLT(sym, precision=A.MIXED)
+    rmx = fmx.factor(vals)
+    assert r64["ok"] and rmx["ok"] and rmx["nNeg"] > 0
+    b = np.random.default_rng(3).uniform(-1, 1, w.n)
+    out = fmx.solveGmres(b, tol=1e-13, restart=40, maxIter=200)
+    assert out["converged"] and out["relres"] < 1e-12
+    x64 = f64.solveRefined(w.pat, vals, b, maxSteps=5, tol=1e-15)["x"]
+    assert np.linalg.norm(out["x"] - x64) / np.linalg.norm(x64) < 1e-9
+    assert relres(w.pat, vals, out["x"], b) < 1e-12
+
+
+def test_gmres_with_fp64_cholesky_converges_at_once():
+    w = W.elastic3d(8)
+    sym = A.analyze(w.pat, ordering="nd3", x=w.x, y=w.y, z=w.z)
+    num = A.NumericFactor(sym)
+    assert num.factor(w.values)
+    out = num.solve_gmres(w.rhs[0], tol=1e-13)
+    assert out["converged"] and out["iterations"] <= 2 and out["relres"] < 1e-13
