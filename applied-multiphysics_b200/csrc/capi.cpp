@@ -142,6 +142,7 @@ struct amp_plan_s {
   DevMem mem;
   amp::DevPlan dp{};
   amp::AsmTask *dAsm = nullptr;
+  amp::PotrfTask *dPotrf = nullptr;
   amp::PanelTask *dPanel = nullptr;
   amp::TileTask *dTile = nullptr, *dUTile = nullptr;
   amp::MixTask *dMixTile = nullptr, *dMixU = nullptr;
@@ -169,7 +170,6 @@ struct amp_factor_s {
   __nv_bfloat16 *dWhi = nullptr, *dWlo = nullptr;   // mixed LDL^T: BF16 split of L21 D
   CUtensorMap *dMaps = nullptr;                     // per supernode: TMA descriptors of the split A and B operands
   unsigned long long *dStatus = nullptr;
-  int *dReaders = nullptr;  // per pivot block: row chunks that have read it (reset at every factorization)
   bool ok = false, hasValues = false;
   // profiling: events around every launch while enabled
   bool profiling = false;
@@ -240,6 +240,7 @@ void upload_plan(amp_plan *pl) {
   d.invOff = m.upload(P.invOff);
   d.diagSlot = m.upload(P.diagSlot);
   pl->dAsm = m.upload(P.asmTasks);
+  pl->dPotrf = m.upload(P.potrfTasks);
   pl->dPanel = m.upload(P.panelTasks);
   pl->dTile = m.upload(P.tileTasks);
   pl->dUTile = m.upload(P.uTasks);
@@ -266,9 +267,11 @@ void ensure_solve_ws(amp_factor *f, int q) {
   f->qcap = q;
 }
 
-enum KernelKind { K_ASSEMBLE, K_PANEL, K_UPDATE, K_FORWARD, K_BACKWARD, K_PERMUTE, K_RESIDUAL, K_DIAGINV, K_NKINDS };
-const char *kKindNames[K_NKINDS] = {"assemble", "panel_potrf_trsm", "update_syrk", "solve_forward",
-                                    "solve_backward", "permute", "residual_spmv", "diag_inverse"};
+enum KernelKind {
+  K_ASSEMBLE, K_PANEL, K_UPDATE, K_FORWARD, K_BACKWARD, K_PERMUTE, K_RESIDUAL, K_POTRF, K_DIAGINV, K_NKINDS
+};
+const char *kKindNames[K_NKINDS] = {"assemble", "panel_trsm", "update_syrk", "solve_forward",
+                                    "solve_backward", "permute", "residual_spmv", "potrf", "diag_inverse"};
 
 cudaEvent_t pool_event(amp_factor *f) {
   if (f->evUsed == f->evPool.size()) {
@@ -298,7 +301,6 @@ void enqueue_factor(amp_factor *f) {
   const amp::DevPlan &dp = f->plan->dp;
   cudaStream_t st = f->stream;
   ck(cudaMemsetAsync(f->dStatus, 0xff, sizeof(unsigned long long), st), "memset status");
-  if (P.panelGroups) ck(cudaMemsetAsync(f->dReaders, 0, sizeof(int) * P.panelGroups, st), "memset readers");
   if (f->precision == AMP_MIXED) {
     amp::LdltArgs<float> ld32{};
     if (f->kind == AMP_LDLT) {
@@ -313,10 +315,15 @@ void enqueue_factor(amp_factor *f) {
       });
       for (int k = P.lvlStepPtr[L]; k < P.lvlStepPtr[L + 1]; k++) {
         const amp::StepRange &sr = P.steps[k];
-        timed(f, K_PANEL, sr.panelFlops, 0.0, [&] {
-          amp::launch_panel<float>(f->plan->dPanel + sr.panel0, sr.panel1 - sr.panel0, dp, f->dL32, f->dReaders,
-                                   f->dStatus, f->dShi, f->dSlo, ld32, st);
+        timed(f, K_POTRF, sr.potrfFlops, 0.0, [&] {
+          amp::launch_potrf<float>(f->plan->dPotrf + sr.potrf0, sr.potrf1 - sr.potrf0, dp, f->dL32, f->dStatus, ld32,
+                                   st);
         });
+        if (sr.panel1 > sr.panel0)
+          timed(f, K_PANEL, sr.panelFlops, 0.0, [&] {
+            amp::launch_trsm<float>(f->plan->dPanel + sr.panel0, sr.panel1 - sr.panel0, dp, f->dL32, f->dStatus,
+                                    f->dShi, f->dSlo, ld32, st);
+          });
         const int64_t t0 = P.mixStepPtr[k], t1 = P.mixStepPtr[k + 1];
         if (t1 > t0)
           timed(f, K_UPDATE, sr.updateFlops, 0.0, [&] {
@@ -350,10 +357,14 @@ void enqueue_factor(amp_factor *f) {
     });
     for (int k = P.lvlStepPtr[L]; k < P.lvlStepPtr[L + 1]; k++) {
       const amp::StepRange &sr = P.steps[k];
-      timed(f, K_PANEL, sr.panelFlops, 0.0, [&] {
-        amp::launch_panel<double>(f->plan->dPanel + sr.panel0, sr.panel1 - sr.panel0, dp, f->dLx, f->dReaders,
-                                  f->dStatus, nullptr, nullptr, ld, st);
+      timed(f, K_POTRF, sr.potrfFlops, 0.0, [&] {
+        amp::launch_potrf<double>(f->plan->dPotrf + sr.potrf0, sr.potrf1 - sr.potrf0, dp, f->dLx, f->dStatus, ld, st);
       });
+      if (sr.panel1 > sr.panel0)
+        timed(f, K_PANEL, sr.panelFlops, 0.0, [&] {
+          amp::launch_trsm<double>(f->plan->dPanel + sr.panel0, sr.panel1 - sr.panel0, dp, f->dLx, f->dStatus, nullptr,
+                                   nullptr, ld, st);
+        });
       if (sr.tile1 > sr.tile0)
         timed(f, K_UPDATE, sr.updateFlops, 0.0, [&] {
           amp::launch_update(f->plan->dTile + sr.tile0, sr.tile1 - sr.tile0, dp, f->dLx, f->dU, ld.W, f->dStatus,
@@ -644,7 +655,6 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
       f->dD = f->mem.alloc<double>((size_t)P.n);
       f->dValues = f->mem.alloc<double>((size_t)P.patNnz);
       f->dStatus = f->mem.alloc<unsigned long long>(1);
-      f->dReaders = f->mem.alloc<int>((size_t)P.panelGroups);
       f->dFlags = f->mem.alloc<int>((size_t)P.nflags);
       ck(cudaMemset(f->dFlags, 0, sizeof(int) * std::max(1, P.nflags)), "memset flags");
       f->dTickets = f->mem.alloc<int>(2);

@@ -6,7 +6,8 @@
 //               matrices in the reference's child order (sparse.mjs:974-985). One CTA owns a block of 32 front
 //               columns, so every entry has a single writer and the summation order is the reference's.
 //   per pivot block of 64 columns:
-//     k_panel   POTRF (or LDL^T) of the 64 x 64 diagonal block in shared memory and TRSM of 256 panel rows per CTA.
+//     k_potrf   POTRF (or LDL^T) of the 64 x 64 pivot block in registers, one CTA per block.
+//     k_trsm    the rows below the pivot block against it, one thread per row, 64 rows per CTA.
 //     k_update  FP64 trailing update F -= A B^T (A = L21, or L21 D for LDL^T; B = L21) on 128 x 64 tiles with the
 //               FP64 tensor-core MMA (mma.sync m16n8k16), covering the remaining pivot columns (in Lx) and the update
 //               block (in the U arena). The mixed-precision update is k_update_mx (update_bf16x3.cu).
@@ -29,10 +30,11 @@ __device__ __forceinline__ T *front_addr(T *Lp, T *Up, int m, int nc, int i, int
 
 // 1/d by Newton-Raphson refinement of the FP32 reciprocal (x <- x + x (1 - d x), quadratic convergence: 2^-23 ->
 // 2^-46 -> full double precision). Not correctly rounded (within a few ulp of 1/d); used only for the trailing
-// update scale of the pivot block, where the factor's own rounding dominates. Positive finite d only; other values
-// are rejected by the pivot test before the result is used.
+// update scale of the pivot block, where the factor's own rounding dominates. Finite nonzero d of either sign; other
+// values take the division.
 __device__ __forceinline__ double recip_nr(double d) {
-  if (!(d > 1e-30 && d < 1e30)) return 1.0 / d;  // outside the float range of the first approximation
+  const double a = fabs(d);
+  if (!(a > 1e-30 && a < 1e30)) return 1.0 / d;  // outside the float range of the first approximation
   double x = (double)__frcp_rn((float)d);
   double e = fma(-d, x, 1.0);
   x = fma(x, e, x);
@@ -141,113 +143,84 @@ __global__ void __launch_bounds__(256) k_assemble(const AsmTask *__restrict__ ta
 __device__ __forceinline__ double recip_t(double d) { return recip_nr(d); }
 __device__ __forceinline__ float recip_t(float d) { return __frcp_rn(d); }
 
-// T = double: the FP64 factor. T = float: the mixed-precision factor; the solved panel rows are also written as BF16
-// hi / lo pairs (hi = bf16(x), lo = bf16(x - hi)) into the split columns read by the tensor-core updates.
-// LDL^T (ld.scal != null): the same right-looking unscaled form, whose columns hold L D and whose pivots are D;
-// the pivots are perturbed as they become final, L = (L D) D^-1 with a unit diagonal is written back, D goes to
-// ld.D, and the TRSM rows are written both as L21 (Lx) and as L21 D (ld.W) for the update.
+// Pivot block: POTRF (or LDL^T) of the 64 x 64 diagonal block of a front, one CTA per pivot block, the block in
+// registers. T = double: the FP64 factor; T = float: the mixed-precision factor.
+// Thread t < 136 owns the 4 x 4 tile (ti, tj), ti >= tj, of the lower triangle. Right-looking on the unscaled
+// columns: at step k the owners of column k publish it (double-buffered in shared memory) and the owner of the
+// diagonal entry settles the pivot and publishes 1 / d_k; after one barrier every thread subtracts col_i col_j / d_k
+// from its entries with i, j > k. Cholesky tests d > 0 (sparse.mjs:1151-1156); LDL^T (ld.scal != null,
+// ldlt.mjs:450-562) perturbs |d| < tau to +-tau and counts negative and perturbed pivots. At the end the columns are scaled:
+// Cholesky L = a / sqrt(d) with sqrt(d) on the diagonal, LDL^T L = a / d with a unit diagonal (D to ld.D). The
+// factored block is written back in place for the TRSM of the rows below and the updates.
 template <class T>
-__global__ void __launch_bounds__(256, 1) k_panel(const PanelTask *__restrict__ tasks, DevPlan P,
-                                                  T *__restrict__ Lx, int *__restrict__ readers,
-                                                  unsigned long long *status, __nv_bfloat16 *__restrict__ Shi,
-                                                  __nv_bfloat16 *__restrict__ Slo, LdltArgs<T> ld) {
+__global__ void __launch_bounds__(256) k_potrf(const PotrfTask *__restrict__ tasks, DevPlan P, T *__restrict__ Lx,
+                                               unsigned long long *status, LdltArgs<T> ld) {
   if (failed(status)) return;
-  const PanelTask t = tasks[blockIdx.x];
+  const PotrfTask t = tasks[blockIdx.x];
   const int s = t.s, c0 = t.c0;
   const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
   const int w = min(kPanel, nc - c0);
-  T *Lp = Lx + P.snLxp[s];
-  __shared__ T D[kPanel][kPanel + 1];
-  __shared__ T invd[kPanel], ivsq[kPanel + 1], pd[kPanel + 1], piv[kPanel];
-  __shared__ unsigned short trail[kPanel * (kPanel - 1) / 2];  // (i, j) of the trailing entries, rightmost column first
-  extern __shared__ __align__(16) unsigned char xs_raw[];
-  T *xs = reinterpret_cast<T *>(xs_raw);  // kPanel x 256 staged solutions of the TRSM
-  __shared__ int fail, failCode, lastReader;
+  T *Lp = Lx + P.snLxp[s] + (int64_t)c0 * m + c0;  // block (i, j) at Lp[j m + i]
+  __shared__ T col[2][kPanel];
+  __shared__ T pd[kPanel], piv[2];
   __shared__ unsigned char pflag[kPanel];
+  __shared__ int fail, failCode;
   const int tid = threadIdx.x;
   const bool ldlt = ld.scal != nullptr;
   const T tau = ldlt ? (T)ld.scal[1] : T(0);
-  // the pivot block (lower part); columns w .. 63 of a short last block are padded with the identity
-  for (int e = tid; e < kPanel * kPanel; e += blockDim.x) {
-    const int i = e & (kPanel - 1), j = e >> 6;
-    if (i >= j) D[i][j] = (i < w) ? Lp[(int64_t)(c0 + j) * m + (c0 + i)] : (i == j ? T(1) : T(0));
-  }
-  // trailing-entry list: columns 63, 62, ..., 1, rows j .. 63 within each
-  for (int j = kPanel - 1 - (tid >> 6) ; j >= 1; j -= 4) {
-    const int before = (kPanel - 1 - j) * (kPanel - j) / 2;  // entries of the columns right of j
-    for (int i = j + (tid & 63); i < kPanel; i += 64) trail[before + (i - j)] = (unsigned short)(i | (j << 8));
-  }
-  __syncthreads();
-  // Every row chunk factors its own copy of the pivot block; the last chunk to have read the unfactored block writes
-  // the factored one back (no chunk waits for another).
+  // tile of this thread: row block ti, column block tj (ti >= tj), from tid by the triangular numbering
+  int ti = 0;
+  while ((ti + 1) * (ti + 2) / 2 <= tid) ti++;
+  const int tj = tid - ti * (ti + 1) / 2;
+  const bool owner = tid < 136;
+  T a[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; r++)
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const int i = 4 * ti + r, j = 4 * tj + c;
+      a[r][c] = !owner || i < j ? T(0) : (i < w ? Lp[(int64_t)j * m + i] : (i == j ? T(1) : T(0)));
+    }
   if (tid == 0) {
-    __threadfence();
-    lastReader = atomicAdd(readers + t.group, 1) == t.nchunks - 1;
     fail = -1;
     failCode = 1;
-    T d = D[0][0];
-    if (ldlt) {
-      if (!ldlt_pivot(d, tau, pflag[0])) {
-        fail = 0;
-        failCode = 2;
-      }
-    } else if (!(d > T(0))) {
-      fail = 0;
-    }
-    pd[0] = d;
-    ivsq[0] = ldlt ? T(1) / d : recip_t(d);
   }
   __syncthreads();
-  // POTRF, right-looking on the unscaled columns: step k subtracts D[i][k] D[j][k] / d_k from the trailing entries
-  // (i >= j > k), enumerated from the rightmost column so that step k's entries are the first T_k of the list. One
-  // barrier per column; the owner of the next diagonal entry publishes its value and reciprocal (the only quantities
-  // on the column-to-column critical path). The columns are scaled to L once, after the loop.
-  for (int k = 0; k < w; k++) {
-    if (fail >= 0) break;  // uniform: written before the barrier that ended the previous step
-    const T iv2 = ivsq[k];
-    const int nk = kPanel - 1 - k;     // trailing columns k+1 .. 63
-    const int Tk = nk * (nk + 1) / 2;  // trailing lower entries
-    for (int e = tid; e < Tk; e += blockDim.x) {
-      const int ij = trail[e], i = ij & 0xff, j = ij >> 8;
-      const T v = D[i][j] - (D[i][k] * D[j][k]) * iv2;
-      D[i][j] = v;
-      if (i == k + 1 && j == k + 1) {  // the next pivot is final now
-        T d = v;
-        if (ldlt) {
-          if (k + 1 < w && !ldlt_pivot(d, tau, pflag[k + 1])) {
-            fail = k + 1;
-            failCode = 2;
+  // k = 4 kb + kk with kk a compile-time constant, so the tile's registers are indexed statically
+  for (int kb = 0; kb < kPanel / 4; kb++) {
+#pragma unroll
+    for (int kk = 0; kk < 4; kk++) {
+      const int k = 4 * kb + kk, buf = kk & 1;
+      if (owner && tj == kb) {  // publish column k (rows >= 4 tj); the diagonal tile also settles the pivot
+#pragma unroll
+        for (int r = 0; r < 4; r++) col[buf][4 * ti + r] = a[r][kk];
+        if (ti == tj) {
+          T d = a[kk][kk];
+          unsigned char fl = 0;
+          const bool bad = k < w && (ldlt ? !ldlt_pivot(d, tau, fl) : !(d > T(0)));
+          if (bad && fail < 0) {
+            fail = k;
+            failCode = ldlt ? 2 : 1;
           }
-          ivsq[k + 1] = T(1) / d;
-        } else {
-          if (!(v > T(0)) && k + 1 < w) fail = k + 1;
-          ivsq[k + 1] = recip_t(v);
+          pd[k] = d;
+          pflag[k] = fl;
+          piv[buf] = recip_t(d);  // the update scale only; L is scaled with the exact 1 / d at the end
         }
-        pd[k + 1] = d;
       }
-    }
-    __syncthreads();
-  }
-  if (fail < 0 && ldlt) {
-    // LDL^T: D keeps L D (used by the TRSM below as is); pivots and their reciprocals
-    if (tid < kPanel) {
-      const T d = tid < w ? pd[tid] : T(1);
-      piv[tid] = d;
-      invd[tid] = T(1) / d;
-    }
-  } else if (fail < 0) {
-    // L = D diag(d)^-1/2: one square root and reciprocal per column, then every entry scaled once
-    if (tid < kPanel) {
-      const T d = tid < w ? pd[tid] : T(1);
-      const T lk = sqrt(d);
-      piv[tid] = lk;
-      invd[tid] = T(1) / lk;
-    }
-    __syncthreads();
-    for (int e = tid; e < kPanel * kPanel; e += blockDim.x) {
-      const int i = e & (kPanel - 1), j = e >> 6;
-      if (i > j) D[i][j] *= invd[j];
-      else if (i == j) D[i][i] = piv[i];
+      __syncthreads();
+      if (owner && ti >= kb && !(kb == kPanel / 4 - 1 && kk == 3)) {
+        const T iv = piv[buf];
+        T ci[4], cj[4];
+#pragma unroll
+        for (int r = 0; r < 4; r++) ci[r] = col[buf][4 * ti + r];
+#pragma unroll
+        for (int c = 0; c < 4; c++) cj[c] = col[buf][4 * tj + c] * iv;
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+          for (int c = 0; c < 4; c++)
+            if (4 * ti + r > k && 4 * tj + c > k) a[r][c] -= ci[r] * cj[c];
+      }
     }
   }
   __syncthreads();
@@ -255,67 +228,115 @@ __global__ void __launch_bounds__(256, 1) k_panel(const PanelTask *__restrict__ 
     if (tid == 0) atomicMin(status, status_word(f + c0 + fail, failCode, s));
     return;
   }
-  if (lastReader) {
-    if (ldlt) {
-      for (int e = tid; e < w * w; e += blockDim.x) {
-        const int i = e % w, j = e / w;
-        if (i >= j) Lp[(int64_t)(c0 + j) * m + (c0 + i)] = i == j ? T(1) : D[i][j] * invd[j];
-      }
-      if (tid < w) ld.D[f + c0 + tid] = (double)piv[tid];
-      if (tid == 0) {
-        int neg = 0, pert = 0;
-        for (int k = 0; k < w; k++) neg += pflag[k] & 1, pert += pflag[k] >> 1;
-        atomicAdd(ld.counts, neg);
-        atomicAdd(ld.counts + 1, pert);
-      }
-    } else {
-      for (int e = tid; e < w * w; e += blockDim.x) {
-        const int i = e % w, j = e / w;
-        if (i >= j) Lp[(int64_t)(c0 + j) * m + (c0 + i)] = D[i][j];
+  if (owner) {
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const int j = 4 * tj + c;
+      const T d = pd[j];
+      const T lj = ldlt ? d : sqrt(d);
+      const T inv = T(1) / lj;
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        const int i = 4 * ti + r;
+        if (i >= j && i < w && j < w) Lp[(int64_t)j * m + i] = i == j ? (ldlt ? T(1) : lj) : a[r][c] * inv;
       }
     }
   }
-  // TRSM: row r of the panel solves x L11^T = a, one thread per row, 16 columns at a time (16 doubles live in
-  // registers); solved columns are staged in shared memory (xs[c][thread]) for the later quarters' updates.
-  const int r = t.r0 + tid;
-  if (r >= t.r1) return;
+  if (ldlt) {
+    if (tid < w) ld.D[f + c0 + tid] = (double)pd[tid];
+    if (tid == 0) {
+      int neg = 0, pert = 0;
+      for (int k = 0; k < w; k++) neg += pflag[k] & 1, pert += pflag[k] >> 1;
+      atomicAdd(ld.counts, neg);
+      atomicAdd(ld.counts + 1, pert);
+    }
+  }
+}
+
+// TRSM of up to 64 rows of a front against its factored pivot block, one thread per row:
+// x_k = (a_k - sum_{c<k} x_c M(k, c)) / M(k, k), by 16-column quarters held in registers (the solved columns are
+// staged in shared memory for the later quarters). Cholesky: M = L11, x = L21. LDL^T: M(k, c) = L11(k, c) d_c,
+// M(k, k) = d_k, x = L21, and w = x D = L21 D (the update's A operand). The rows are also written as BF16 hi / lo
+// pairs (hi = bf16(x), lo = bf16(x - hi)) into the split columns of the tensor-core update (mixed precision).
+constexpr int kTrsmSmem = (kPanel * (kPanel + 1) + kPanel * kPanel) * (int)sizeof(double);
+template <class T>
+__global__ void __launch_bounds__(kPanel) k_trsm(const PanelTask *__restrict__ tasks, DevPlan P, T *__restrict__ Lx,
+                                                 const unsigned long long *status, __nv_bfloat16 *__restrict__ Shi,
+                                                 __nv_bfloat16 *__restrict__ Slo, LdltArgs<T> ld) {
+  if (failed(status)) return;
+  const PanelTask t = tasks[blockIdx.x];
+  const int s = t.s, c0 = t.c0;
+  const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
+  const int w = min(kPanel, nc - c0);
+  const bool ldlt = ld.scal != nullptr;
+  T *Lp = Lx + P.snLxp[s];
+  extern __shared__ __align__(16) unsigned char trsm_raw[];
+  T(*M)[kPanel + 1] = reinterpret_cast<T(*)[kPanel + 1]>(trsm_raw);  // M[k][c], c < k
+  T(*xs)[kPanel] = reinterpret_cast<T(*)[kPanel]>(trsm_raw + kPanel * (kPanel + 1) * sizeof(T));  // xs[c][thread]
+  __shared__ T invd[kPanel], dv[kPanel];
+  const int tid = threadIdx.x;
+  {
+    const T d = tid < w ? (ldlt ? (T)ld.D[f + c0 + tid] : Lp[(int64_t)(c0 + tid) * m + c0 + tid]) : T(1);
+    dv[tid] = d;
+    invd[tid] = T(1) / d;
+  }
+  __syncthreads();
+  {  // the pivot block, 64 loads per thread issued 16 at a time (thread tid reads row tid of every column)
+    const int k = tid;
+#pragma unroll
+    for (int c0q = 0; c0q < kPanel; c0q += 16) {
+      T v[16];
+#pragma unroll
+      for (int u = 0; u < 16; u++) {
+        const int c = c0q + u;
+        v[u] = (k < w && c < k) ? Lp[(int64_t)(c0 + c) * m + c0 + k] : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < 16; u++) M[k][c0q + u] = ldlt ? v[u] * dv[c0q + u] : v[u];
+    }
+  }
+  __syncthreads();
+  const int row = t.r0 + tid;
+  if (row >= t.r1) return;
+  const int ld8 = (m + 7) & ~7;
   constexpr int Q = 16;
-  T x[Q];
 #pragma unroll 1
   for (int q0 = 0; q0 < w; q0 += Q) {
+    T x[Q];
 #pragma unroll
-    for (int c = 0; c < Q; c++) x[c] = (q0 + c < w) ? Lp[(int64_t)(c0 + q0 + c) * m + r] : T(0);
-#pragma unroll 1
+    for (int c = 0; c < Q; c++) x[c] = q0 + c < w ? Lp[(int64_t)(c0 + q0 + c) * m + row] : T(0);
+#pragma unroll 4
     for (int k = 0; k < q0; k++) {
-      const T xk = xs[k * 256 + tid];
+      const T xk = xs[k][tid];
 #pragma unroll
-      for (int c = 0; c < Q; c++) x[c] -= xk * D[q0 + c][k];
-    }
-#pragma unroll
-    for (int k = 0; k < Q; k++) {
-      x[k] *= invd[q0 + k];
-#pragma unroll
-      for (int c = k + 1; c < Q; c++) x[c] -= x[k] * D[q0 + c][q0 + k];
+      for (int c = 0; c < Q; c++) x[c] -= xk * M[q0 + c][k];
     }
 #pragma unroll
     for (int c = 0; c < Q; c++) {
-      if (q0 + c < w) {
-        Lp[(int64_t)(c0 + q0 + c) * m + r] = x[c];
-        const T wv = ldlt ? x[c] * piv[q0 + c] : T(0);
-        if (ldlt && ld.W) ld.W[P.snLxp[s] + (int64_t)(c0 + q0 + c) * m + r] = wv;
-        if (Shi) {
-          const int64_t g = P.snSp[s] + (int64_t)(c0 + q0 + c) * ((m + 7) & ~7) + r;
-          const __nv_bfloat16 hi = __float2bfloat16_rn((float)x[c]);
-          Shi[g] = hi;
-          Slo[g] = __float2bfloat16_rn((float)x[c] - __bfloat162float(hi));
-          if (ldlt) {
-            const __nv_bfloat16 whi = __float2bfloat16_rn((float)wv);
-            ld.Whi[g] = whi;
-            ld.Wlo[g] = __float2bfloat16_rn((float)wv - __bfloat162float(whi));
-          }
+      x[c] *= invd[q0 + c];
+#pragma unroll
+      for (int c2 = c + 1; c2 < Q; c2++) x[c2] -= x[c] * M[q0 + c2][q0 + c];
+    }
+#pragma unroll
+    for (int c = 0; c < Q; c++) {
+      const int cc = q0 + c;
+      xs[cc][tid] = x[c];
+      if (cc >= w) continue;
+      const T xv = x[c];
+      Lp[(int64_t)(c0 + cc) * m + row] = xv;
+      const T wv = ldlt ? xv * dv[cc] : T(0);
+      if (ldlt && ld.W) ld.W[P.snLxp[s] + (int64_t)(c0 + cc) * m + row] = wv;
+      if (Shi) {
+        const int64_t g = P.snSp[s] + (int64_t)(c0 + cc) * ld8 + row;
+        const __nv_bfloat16 hi = __float2bfloat16_rn((float)xv);
+        Shi[g] = hi;
+        Slo[g] = __float2bfloat16_rn((float)xv - __bfloat162float(hi));
+        if (ldlt) {
+          const __nv_bfloat16 whi = __float2bfloat16_rn((float)wv);
+          ld.Whi[g] = whi;
+          ld.Wlo[g] = __float2bfloat16_rn((float)wv - __bfloat162float(whi));
         }
       }
-      xs[(q0 + c) * 256 + tid] = x[c];
     }
   }
 }
@@ -511,12 +532,12 @@ __global__ void k_permute_out(const double *__restrict__ y, double *__restrict__
 // Launchers (host side)
 // ---------------------------------------------------------------------------------------------------------------
 static int g_num_sms = 148;
-constexpr int kPanelSmem = kPanel * 256 * (int)sizeof(double);
+
 void init_mixed_attributes();
 void init_solve_attributes();
 void init_kernel_attributes() {
-  cudaFuncSetAttribute(k_panel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmem);
-  cudaFuncSetAttribute(k_panel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmem / 2);
+  cudaFuncSetAttribute(k_trsm<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsmSmem);
+  cudaFuncSetAttribute(k_trsm<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsmSmem);
   init_mixed_attributes();
   init_solve_attributes();
   cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, kUpdateSmem);
@@ -535,17 +556,23 @@ template void launch_assemble<double>(const AsmTask *, int64_t, const DevPlan &,
 template void launch_assemble<float>(const AsmTask *, int64_t, const DevPlan &, const double *, float *, float *,
                                      const unsigned long long *, cudaStream_t);
 template <class T>
-void launch_panel(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, T *Lx, int *readers,
-                  unsigned long long *status, __nv_bfloat16 *Shi, __nv_bfloat16 *Slo, const LdltArgs<T> &ld,
-                  cudaStream_t st) {
-  if (ntasks > 0)
-    k_panel<T><<<(unsigned)ntasks, 256, kPanel * 256 * (int)sizeof(T), st>>>(tasks, P, Lx, readers, status, Shi, Slo,
-                                                                            ld);
+void launch_potrf(const PotrfTask *tasks, int64_t ntasks, const DevPlan &P, T *Lx, unsigned long long *status,
+                  const LdltArgs<T> &ld, cudaStream_t st) {
+  if (ntasks > 0) k_potrf<T><<<(unsigned)ntasks, 256, 0, st>>>(tasks, P, Lx, status, ld);
 }
-template void launch_panel<double>(const PanelTask *, int64_t, const DevPlan &, double *, int *, unsigned long long *,
-                                   __nv_bfloat16 *, __nv_bfloat16 *, const LdltArgs<double> &, cudaStream_t);
-template void launch_panel<float>(const PanelTask *, int64_t, const DevPlan &, float *, int *, unsigned long long *,
-                                  __nv_bfloat16 *, __nv_bfloat16 *, const LdltArgs<float> &, cudaStream_t);
+template <class T>
+void launch_trsm(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, T *Lx, const unsigned long long *status,
+                 __nv_bfloat16 *Shi, __nv_bfloat16 *Slo, const LdltArgs<T> &ld, cudaStream_t st) {
+  if (ntasks > 0) k_trsm<T><<<(unsigned)ntasks, kPanel, kTrsmSmem, st>>>(tasks, P, Lx, status, Shi, Slo, ld);
+}
+template void launch_potrf<double>(const PotrfTask *, int64_t, const DevPlan &, double *, unsigned long long *,
+                                   const LdltArgs<double> &, cudaStream_t);
+template void launch_potrf<float>(const PotrfTask *, int64_t, const DevPlan &, float *, unsigned long long *,
+                                  const LdltArgs<float> &, cudaStream_t);
+template void launch_trsm<double>(const PanelTask *, int64_t, const DevPlan &, double *, const unsigned long long *,
+                                  __nv_bfloat16 *, __nv_bfloat16 *, const LdltArgs<double> &, cudaStream_t);
+template void launch_trsm<float>(const PanelTask *, int64_t, const DevPlan &, float *, const unsigned long long *,
+                                 __nv_bfloat16 *, __nv_bfloat16 *, const LdltArgs<float> &, cudaStream_t);
 void launch_ldlt_tau(const double *values, const DevPlan &P, double *scal, cudaStream_t st) {
   k_ldlt_tau<<<1, 1024, 0, st>>>(values, P.diagSlot, P.n, scal);
 }

@@ -32,6 +32,7 @@ void set_last_error(const std::string &msg);
 namespace {
 
 constexpr int kNoAllocMaxFront = 16384;                  // largest front m this entry point accepts
+constexpr int kNaRows = 256;                             // panel rows per CTA (one thread per row)
 constexpr int kNoAllocBlocks = kNoAllocMaxFront / kPanel; // pivot blocks of the largest front
 // [0] status word, [1 + k] readers of pivot block k: (1 + 256) x 8 bytes
 static __device__ __align__(256) unsigned long long g_front_scratch[1 + kNoAllocBlocks];
@@ -47,8 +48,8 @@ __global__ void __launch_bounds__(256) k_front_panel_na(double *__restrict__ F, 
   unsigned long long *status = scratch;
   if (na_failed(status)) return;
   const int w = min(kPanel, nc - c0), c1 = c0 + w;
-  const int nchunks = c1 < m ? (m - c1 + kTrsmRows - 1) / kTrsmRows : 1;
-  const int r0 = c1 + blockIdx.x * kTrsmRows, r1 = min(r0 + kTrsmRows, m);
+  const int nchunks = c1 < m ? (m - c1 + kNaRows - 1) / kNaRows : 1;
+  const int r0 = c1 + blockIdx.x * kNaRows, r1 = min(r0 + kNaRows, m);
   __shared__ double D[kPanel][kPanel + 1];
   __shared__ double invd[kPanel];
   __shared__ int fail, lastReader;
@@ -222,7 +223,7 @@ extern "C" AMP_API int amp_front_factor_noalloc(double *F, int32_t m, int32_t nc
   if (e == cudaSuccess) e = cudaMemsetAsync(scratch + 1, 0, sizeof(unsigned long long) * blocks, st);
   for (int k = 0; k < blocks && e == cudaSuccess; k++) {
     const int c0 = k * kPanel, c1 = std::min(c0 + kPanel, nc);
-    const int nchunks = c1 < m ? (m - c1 + kTrsmRows - 1) / kTrsmRows : 1;
+    const int nchunks = c1 < m ? (m - c1 + kNaRows - 1) / kNaRows : 1;
     k_front_panel_na<<<nchunks, 256, 0, st>>>(F, m, nc, c0, scratch);
     const int T = (m - c1 + kTile - 1) / kTile;
     if (T > 0)

@@ -17,9 +17,11 @@ template <class T>
 void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, const double *values, T *Lx, T *U,
                      const unsigned long long *status, cudaStream_t st);
 template <class T>
-void launch_panel(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, T *Lx, int *readers,
-                  unsigned long long *status, __nv_bfloat16 *Shi, __nv_bfloat16 *Slo, const LdltArgs<T> &ld,
-                  cudaStream_t st);
+void launch_potrf(const PotrfTask *tasks, int64_t ntasks, const DevPlan &P, T *Lx, unsigned long long *status,
+                  const LdltArgs<T> &ld, cudaStream_t st);
+template <class T>
+void launch_trsm(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, T *Lx, const unsigned long long *status,
+                 __nv_bfloat16 *Shi, __nv_bfloat16 *Slo, const LdltArgs<T> &ld, cudaStream_t st);
 void launch_ldlt_tau(const double *values, const DevPlan &P, double *scal, cudaStream_t st);
 void launch_update_mx(const MixTask *tasks, int64_t ntasks, const CUtensorMap *maps, float *L32, float *U32,
                       unsigned long long *status, int num_sms, cudaStream_t st);

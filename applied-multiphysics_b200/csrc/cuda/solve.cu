@@ -15,9 +15,10 @@
 // needs from a block are loaded before it waits for that block's flag, so the dependency chain through a large
 // supernode costs a flag round trip, 64 y values and a 64 x 64 product per block.
 //
-// The inverses of the diagonal blocks are computed once per factorization (k_diag_inv): column j of X = L_kk^-1 by
-// forward substitution, X(j, j) = 1 / L(j, j), X(i, j) = -(sum_{t=j}^{i-1} L(i, t) X(t, j)) X(i, i). Solving with X
-// instead of by substitution changes the result by rounding only (the FP64 path stays within 1e-12 of the oracle).
+// The inverses of the diagonal blocks are computed once per factorization, after it (k_diag_inv, all blocks in
+// parallel): column j of X = L_kk^-1 by forward substitution, X(j, j) = 1 / L(j, j),
+// X(i, j) = -(sum_{t=j}^{i-1} L(i, t) X(t, j)) X(i, i). Solving with X instead of by substitution changes the result
+// by rounding only (the FP64 path stays within 1e-12 of the oracle).
 #include <cuda_runtime.h>
 
 #include <cstdint>

@@ -198,7 +198,8 @@ void build_plan(const Symbolic &S, Plan &P) {
     P.asmLvlPtr[L + 1] = (int64_t)P.asmTasks.size();
     for (int k = 0; k < maxSteps; k++) {
       StepRange sr;
-      sr.panelFlops = sr.updateFlops = 0;
+      sr.potrfFlops = sr.panelFlops = sr.updateFlops = 0;
+      sr.potrf0 = (int64_t)P.potrfTasks.size();
       sr.panel0 = (int64_t)P.panelTasks.size();
       sr.tile0 = (int64_t)P.tileTasks.size();
       for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
@@ -206,20 +207,15 @@ void build_plan(const Symbolic &S, Plan &P) {
         const int nc = P.snNc[s], m = P.snM[s], c0 = k * kPanel;
         if (c0 >= nc) continue;
         const int c1 = std::min(c0 + kPanel, nc);
-        const int g = P.panelGroups++;
-        if (c1 >= m)
-          P.panelTasks.push_back({s, c0, m, m, g, 1});
-        else {
-          const int nch = (m - c1 + kTrsmRows - 1) / kTrsmRows;
-          for (int r0 = c1; r0 < m; r0 += kTrsmRows)
-            P.panelTasks.push_back({s, c0, r0, std::min(r0 + kTrsmRows, m), g, nch});
-        }
+        P.potrfTasks.push_back({s, c0});
+        for (int r0 = c1; r0 < m; r0 += kTrsmRows) P.panelTasks.push_back({s, c0, r0, std::min(r0 + kTrsmRows, m)});
         // Pivot blocks are grouped by kGroup: after block b of group [g0, g1) only the group's remaining columns are
         // updated (narrow, K = 64); after the group's last block the pivot columns right of the group receive the
         // whole group at once (wide, K = g1 - g0). The update block waits for the long-K pass after the level.
         const int g0 = (c0 / (kGroup * kPanel)) * (kGroup * kPanel), g1 = std::min(nc, g0 + kGroup * kPanel);
         const double w = c1 - c0, r = m - c1;
-        sr.panelFlops += w * w * w / 3.0 + r * w * w;  // POTRF + TRSM
+        sr.potrfFlops += w * w * w / 3.0;
+        sr.panelFlops += r * w * w;  // TRSM
         auto trap = [m](double a, double b) { return (b - a) * m - (a + b - 1) * (b - a) / 2; };  // lower entries
         if (c1 < g1)
           emitMix(P.mixTiles, s, c1, c1, g1, c0, c1 - c0);
@@ -237,6 +233,7 @@ void build_plan(const Symbolic &S, Plan &P) {
               P.tileTasks.push_back({(long long)P.snLxp[s], (long long)P.snUoff[s], m, nc, g0, g1 - g0, i0, j0, nc, 0});
         }
       }
+      sr.potrf1 = (int64_t)P.potrfTasks.size();
       sr.panel1 = (int64_t)P.panelTasks.size();
       sr.tile1 = (int64_t)P.tileTasks.size();
       P.steps.push_back(sr);

@@ -22,12 +22,14 @@ constexpr int kGroup = 4;      // pivot blocks whose update of the columns right
 constexpr int kTile = 64;      // trailing-update tile columns
 constexpr int kTileM = 128;    // trailing-update tile rows
 constexpr int kAsmCols = 32;   // front columns per assembly task
-constexpr int kTrsmRows = 256; // panel rows per TRSM task
+constexpr int kTrsmRows = 64;  // panel rows per TRSM task
 constexpr int kSmallFront = 0; // fronts with m <= kSmallFront use the one-CTA-per-front kernel (0 = off)
 
-struct PanelTask {  // POTRF of the pivot block [c0, c0 + w) of supernode s and TRSM of rows [r0, r1)
+struct PotrfTask {  // POTRF / LDL^T of the pivot block [c0, c0 + w) of supernode s, and its inverse
+  int s, c0;
+};
+struct PanelTask {  // TRSM of rows [r0, r1) of supernode s against the factored pivot block [c0, c0 + w)
   int s, c0, r0, r1;
-  int group, nchunks;  // all row chunks of one pivot block share a group; its last reader writes the block back
 };
 struct TileTask {  // update tile: rows [i0, i0+128) x cols [j0, min(j0+64, jend)) of a front, K = columns [c0, c0+w)
   long long lp, up;      // offsets of the front's L panel (Lx) and update block (U arena, -1 if none)
@@ -45,8 +47,8 @@ struct AsmTask {  // zero + assemble + extend-add front columns [j0, j0 + 32) of
 };
 
 struct StepRange {
-  int64_t panel0, panel1, tile0, tile1;
-  double panelFlops, updateFlops;  // algorithmic flops of the step's launches
+  int64_t potrf0, potrf1, panel0, panel1, tile0, tile1;
+  double potrfFlops, panelFlops, updateFlops;  // algorithmic flops of the step's launches
 };
 // The update block of every front receives its whole Schur update once, after the panel steps of its level:
 // U -= L21 L21^T with K = nc (tiles over the lower triangle of [nc, m)^2).
@@ -71,8 +73,8 @@ struct Plan {
   std::vector<AsmTask> asmTasks;
   std::vector<int64_t> asmLvlPtr;  // per level
   std::vector<double> asmLvlBytes;  // algorithmic bytes of each level's assembly (A entries + extend-add)
+  std::vector<PotrfTask> potrfTasks;
   std::vector<PanelTask> panelTasks;
-  int panelGroups = 0;
   std::vector<TileTask> tileTasks;
   std::vector<int> lvlStepPtr;  // per level: steps [lvlStepPtr[L], lvlStepPtr[L+1])
   std::vector<TileTask> uTasks;  // long-K update-block tiles, per level [uLvlPtr[L], uLvlPtr[L+1])

@@ -4,8 +4,11 @@ Tolerances. The update order differs from the reference's, and small indefinite 
 columns, so two correct FP64 factorizations of an indefinite matrix agree only as far as its conditioning allows (on
 the shifted elasticity case, min |d| = 1.3e-5 and max |L| = 1e4, a 1-ulp symmetric perturbation of A moves the
 oracle's own L by 2e-8 and D by 9e-8 in relative Frobenius norm). The bar is therefore relative to that sensitivity:
-L, D and the solutions within max(1e-11, 10 x the oracle's change under a 1-ulp perturbation of A), in relative
-Frobenius / 2-norm; refined residuals below 1e-12 (the strict check, independent of the order of operations).
+L, D and the solutions within max(1e-11, 100 x the oracle's change under a 1-ulp perturbation of A), in relative
+Frobenius / 2-norm: a different operation order (tiles, K = 256 groups, the pivot block's inverse in the TRSM)
+accumulates many roundings, not one (on the shifted 27-point grid a dense numpy LDL^T differs from the oracle by
+25 x the 1-ulp change in D). Refined residuals below 1e-12 are the strict check, independent of the order of
+operations.
 Inertia (nNeg) and the perturbation count are exact.
 """
 import math
@@ -20,6 +23,7 @@ import workloads as W
 pytestmark = pytest.mark.gpu
 
 FLOOR = 1e-11
+SENS = 100  # times the oracle's own change under a 1-ulp perturbation of A
 
 
 def rel(a, b):
@@ -68,8 +72,8 @@ def run_case(w, values, sym_kw, nrhs=2):
     ok_p, Lx_p, D_p, _, _ = O.factor(osym, ulp_perturbed(w.pat, values), kind="ldlt")
     assert ok_o and ok_p
     Lo = lower_parts(osym, Lx_o)
-    tol_L = max(FLOOR, 10 * rel(lower_parts(osym, Lx_p), Lo))
-    tol_D = max(FLOOR, 10 * rel(D_p, D_o))
+    tol_L = max(FLOOR, SENS * rel(lower_parts(osym, Lx_p), Lo))
+    tol_D = max(FLOOR, SENS * rel(D_p, D_o))
     f = A.SupernodalLDLT(psym)
     r = f.factor(values)
     assert r["ok"]
@@ -81,7 +85,7 @@ def run_case(w, values, sym_kw, nrhs=2):
     Xg = f.solveMany(B.reshape(-1), nrhs).reshape(nrhs, w.n)
     for k in range(nrhs):
         xo = O.solve_ldlt(osym, Lx_o, D_o, B[k])
-        tol_x = max(FLOOR, 10 * rel(O.solve_ldlt(osym, Lx_p, D_p, B[k]), xo))
+        tol_x = max(FLOOR, SENS * rel(O.solve_ldlt(osym, Lx_p, D_p, B[k]), xo))
         assert rel(Xg[k], xo) <= tol_x
         assert rel(f.solve(B[k]), Xg[k]) <= 1e-14  # one vector or several in one pass: the same arithmetic
     ref = f.solveRefined(w.pat, values, B[0], maxSteps=5, tol=1e-14)
