@@ -7,7 +7,7 @@
 //               columns, so every entry has a single writer and the summation order is the reference's.
 //   per pivot block of 64 columns:
 //     k_potrf   POTRF (or LDL^T) of the 64 x 64 pivot block in registers, one CTA per block.
-//     k_trsm    the rows below the pivot block against it, one thread per row, 64 rows per CTA.
+//     k_trsm    the rows below the pivot block against it, four threads per row, 64 rows per CTA.
 //     k_update  FP64 trailing update F -= A B^T (A = L21, or L21 D for LDL^T; B = L21) on 128 x 64 tiles with the
 //               FP64 tensor-core MMA (mma.sync m16n8k16), covering the remaining pivot columns (in Lx) and the update
 //               block (in the U arena). The mixed-precision update is k_update_mx (update_bf16x3.cu).
@@ -102,10 +102,25 @@ __global__ void __launch_bounds__(256) k_assemble(const AsmTask *__restrict__ ta
   for (int j = j0 + warp; j < jend; j += nwarps)
     for (int i = j + lane; i < m; i += 32) *front_addr(Lp, Up, m, nc, i, j) = T(0);
   __syncthreads();
-  // 2. A's entries of the owned pivot columns (each (row, col) once)
+  // 2. A's entries of the owned pivot columns (each (row, col) once); 4 entries per lane in flight
   for (int j = j0 + warp; j < min(jend, nc); j += nwarps) {
     const int p0 = P.asmColPtr[f + j], p1 = P.asmColPtr[f + j + 1];
-    for (int p = p0 + lane; p < p1; p += 32) Lp[P.asmDst[p]] += (T)values[P.asmSrc[p]];
+    for (int p = p0 + lane; p < p1; p += 128) {
+      int dst[4];
+      T v[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int pp = p + 32 * u;
+        dst[u] = pp < p1 ? P.asmDst[pp] : -1;
+        v[u] = pp < p1 ? (T)__ldg(values + P.asmSrc[pp]) : T(0);
+      }
+      T cur[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) cur[u] = dst[u] >= 0 ? Lp[dst[u]] : T(0);
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        if (dst[u] >= 0) Lp[dst[u]] = cur[u] + v[u];
+    }
   }
   __syncthreads();
   // 3. children, one after another (stack order of the reference)
@@ -131,7 +146,22 @@ __global__ void __launch_bounds__(256) k_assemble(const AsmTask *__restrict__ ta
     for (int b = b0 + warp; b < b1; b += nwarps) {
       const int jj = map[b];
       const T *col = Uc + (int64_t)b * muc;
-      for (int a = b + lane; a < muc; a += 32) *front_addr(Lp, Up, m, nc, map[a], jj) += col[a];
+      // 4 entries per lane in flight: gather the child's values and target rows, then read-modify-write the front
+      for (int a = b + lane; a < muc; a += 128) {
+        T v[4], cur[4];
+        T *dst[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int aa = a + 32 * u;
+          dst[u] = aa < muc ? front_addr(Lp, Up, m, nc, __ldg(map + aa), jj) : nullptr;
+          v[u] = aa < muc ? col[aa] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) cur[u] = dst[u] ? *dst[u] : T(0);
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          if (dst[u]) *dst[u] = cur[u] + v[u];
+      }
     }
     __syncthreads();
   }
@@ -142,6 +172,9 @@ __global__ void __launch_bounds__(256) k_assemble(const AsmTask *__restrict__ ta
 // ---------------------------------------------------------------------------------------------------------------
 __device__ __forceinline__ double recip_t(double d) { return recip_nr(d); }
 __device__ __forceinline__ float recip_t(float d) { return __frcp_rn(d); }
+// Scale factors of the pivot block's right-looking update (not stored): FP64 as recip_nr, FP32 the hardware estimate.
+__device__ __forceinline__ double fast_recip(double d) { return recip_nr(d); }
+__device__ __forceinline__ float fast_recip(float d) { return __fdividef(1.0f, d); }
 
 // Pivot block: POTRF (or LDL^T) of the 64 x 64 diagonal block of a front, one CTA per pivot block, the block in
 // registers. T = double: the FP64 factor; T = float: the mixed-precision factor.
@@ -164,7 +197,7 @@ __global__ void __launch_bounds__(256) k_potrf(const PotrfTask *__restrict__ tas
   __shared__ T col[2][kPanel];
   __shared__ T pd[kPanel], piv[2];
   __shared__ unsigned char pflag[kPanel];
-  __shared__ int fail, failCode;
+  __shared__ int fail;
   const int tid = threadIdx.x;
   const bool ldlt = ld.scal != nullptr;
   const T tau = ldlt ? (T)ld.scal[1] : T(0);
@@ -173,6 +206,7 @@ __global__ void __launch_bounds__(256) k_potrf(const PotrfTask *__restrict__ tas
   while ((ti + 1) * (ti + 2) / 2 <= tid) ti++;
   const int tj = tid - ti * (ti + 1) / 2;
   const bool owner = tid < 136;
+  int myFail = -1;  // diagonal tiles only
   T a[4][4];
 #pragma unroll
   for (int r = 0; r < 4; r++)
@@ -181,10 +215,7 @@ __global__ void __launch_bounds__(256) k_potrf(const PotrfTask *__restrict__ tas
       const int i = 4 * ti + r, j = 4 * tj + c;
       a[r][c] = !owner || i < j ? T(0) : (i < w ? Lp[(int64_t)j * m + i] : (i == j ? T(1) : T(0)));
     }
-  if (tid == 0) {
-    fail = -1;
-    failCode = 1;
-  }
+  if (tid == 0) fail = kPanel;  // none
   __syncthreads();
   // k = 4 kb + kk with kk a compile-time constant, so the tile's registers are indexed statically
   for (int kb = 0; kb < kPanel / 4; kb++) {
@@ -198,13 +229,10 @@ __global__ void __launch_bounds__(256) k_potrf(const PotrfTask *__restrict__ tas
           T d = a[kk][kk];
           unsigned char fl = 0;
           const bool bad = k < w && (ldlt ? !ldlt_pivot(d, tau, fl) : !(d > T(0)));
-          if (bad && fail < 0) {
-            fail = k;
-            failCode = ldlt ? 2 : 1;
-          }
+          if (bad && myFail < 0) myFail = k;  // first failing pivot of this diagonal tile
+          piv[buf] = fast_recip(d);  // the update scale only; L is scaled with the exact 1 / d at the end
           pd[k] = d;
           pflag[k] = fl;
-          piv[buf] = recip_t(d);  // the update scale only; L is scaled with the exact 1 / d at the end
         }
       }
       __syncthreads();
@@ -223,9 +251,10 @@ __global__ void __launch_bounds__(256) k_potrf(const PotrfTask *__restrict__ tas
       }
     }
   }
+  if (myFail >= 0) atomicMin(&fail, myFail);
   __syncthreads();
-  if (fail >= 0) {
-    if (tid == 0) atomicMin(status, status_word(f + c0 + fail, failCode, s));
+  if (fail < kPanel) {
+    if (tid == 0) atomicMin(status, status_word(f + c0 + fail, ldlt ? 2 : 1, s));
     return;
   }
   if (owner) {
@@ -253,16 +282,18 @@ __global__ void __launch_bounds__(256) k_potrf(const PotrfTask *__restrict__ tas
   }
 }
 
-// TRSM of up to 64 rows of a front against its factored pivot block, one thread per row:
-// x_k = (a_k - sum_{c<k} x_c M(k, c)) / M(k, k), by 16-column quarters held in registers (the solved columns are
-// staged in shared memory for the later quarters). Cholesky: M = L11, x = L21. LDL^T: M(k, c) = L11(k, c) d_c,
-// M(k, k) = d_k, x = L21, and w = x D = L21 D (the update's A operand). The rows are also written as BF16 hi / lo
-// pairs (hi = bf16(x), lo = bf16(x - hi)) into the split columns of the tensor-core update (mixed precision).
-constexpr int kTrsmSmem = (kPanel * (kPanel + 1) + kPanel * kPanel) * (int)sizeof(double);
+// TRSM of up to 64 rows of a front against its factored pivot block: x_k = (a_k - sum_{c<k} x_c M(k, c)) / M(k, k).
+// Four threads per row, thread (row, q) holds columns 16 q .. 16 q + 15 in registers. Phase p: the threads of quarter
+// p solve their 16 columns (the earlier quarters' contributions already applied) and publish them; after a barrier
+// the threads of the later quarters subtract quarter p's contribution (16 x 16 products) from theirs.
+// Cholesky: M = L11, x = L21. LDL^T: M(k, c) = L11(k, c) d_c, M(k, k) = d_k, x = L21, and w = x D = L21 D (the
+// update's A operand). The rows are also written as BF16 hi / lo pairs (hi = bf16(x), lo = bf16(x - hi)) into the
+// split columns of the tensor-core update (mixed precision).
+constexpr int kTrsmSmem = (kPanel * (kPanel + 1) + kPanel * (kPanel + 1)) * (int)sizeof(double);
 template <class T>
-__global__ void __launch_bounds__(kPanel) k_trsm(const PanelTask *__restrict__ tasks, DevPlan P, T *__restrict__ Lx,
-                                                 const unsigned long long *status, __nv_bfloat16 *__restrict__ Shi,
-                                                 __nv_bfloat16 *__restrict__ Slo, LdltArgs<T> ld) {
+__global__ void __launch_bounds__(256) k_trsm(const PanelTask *__restrict__ tasks, DevPlan P, T *__restrict__ Lx,
+                                              const unsigned long long *status, __nv_bfloat16 *__restrict__ Shi,
+                                              __nv_bfloat16 *__restrict__ Slo, LdltArgs<T> ld) {
   if (failed(status)) return;
   const PanelTask t = tasks[blockIdx.x];
   const int s = t.s, c0 = t.c0;
@@ -272,70 +303,76 @@ __global__ void __launch_bounds__(kPanel) k_trsm(const PanelTask *__restrict__ t
   T *Lp = Lx + P.snLxp[s];
   extern __shared__ __align__(16) unsigned char trsm_raw[];
   T(*M)[kPanel + 1] = reinterpret_cast<T(*)[kPanel + 1]>(trsm_raw);  // M[k][c], c < k
-  T(*xs)[kPanel] = reinterpret_cast<T(*)[kPanel]>(trsm_raw + kPanel * (kPanel + 1) * sizeof(T));  // xs[c][thread]
+  T(*xs)[kPanel + 1] = reinterpret_cast<T(*)[kPanel + 1]>(trsm_raw + kPanel * (kPanel + 1) * sizeof(T));  // [c][row]
   __shared__ T invd[kPanel], dv[kPanel];
-  const int tid = threadIdx.x;
-  {
+  const int tid = threadIdx.x, r = tid & (kPanel - 1), q = tid >> 6;
+  if (tid < kPanel) {
     const T d = tid < w ? (ldlt ? (T)ld.D[f + c0 + tid] : Lp[(int64_t)(c0 + tid) * m + c0 + tid]) : T(1);
     dv[tid] = d;
     invd[tid] = T(1) / d;
   }
   __syncthreads();
-  {  // the pivot block, 64 loads per thread issued 16 at a time (thread tid reads row tid of every column)
-    const int k = tid;
+  {  // the pivot block: thread (r, q) loads row r of columns 16 q .. 16 q + 15
+    T v[16];
 #pragma unroll
-    for (int c0q = 0; c0q < kPanel; c0q += 16) {
-      T v[16];
-#pragma unroll
-      for (int u = 0; u < 16; u++) {
-        const int c = c0q + u;
-        v[u] = (k < w && c < k) ? Lp[(int64_t)(c0 + c) * m + c0 + k] : T(0);
-      }
-#pragma unroll
-      for (int u = 0; u < 16; u++) M[k][c0q + u] = ldlt ? v[u] * dv[c0q + u] : v[u];
+    for (int u = 0; u < 16; u++) {
+      const int c = 16 * q + u;
+      v[u] = (r < w && c < r) ? Lp[(int64_t)(c0 + c) * m + c0 + r] : T(0);
     }
+#pragma unroll
+    for (int u = 0; u < 16; u++) M[r][16 * q + u] = ldlt ? v[u] * dv[16 * q + u] : v[u];
+  }
+  const int row = t.r0 + r;
+  const bool active = row < t.r1;
+  T x[16];
+#pragma unroll
+  for (int u = 0; u < 16; u++) {
+    const int c = 16 * q + u;
+    x[u] = active && c < w ? Lp[(int64_t)(c0 + c) * m + row] : T(0);
   }
   __syncthreads();
-  const int row = t.r0 + tid;
-  if (row >= t.r1) return;
-  const int ld8 = (m + 7) & ~7;
-  constexpr int Q = 16;
-#pragma unroll 1
-  for (int q0 = 0; q0 < w; q0 += Q) {
-    T x[Q];
+  for (int p = 0; p < 4; p++) {
+    if (q == p) {  // solve this quarter
 #pragma unroll
-    for (int c = 0; c < Q; c++) x[c] = q0 + c < w ? Lp[(int64_t)(c0 + q0 + c) * m + row] : T(0);
+      for (int u = 0; u < 16; u++) {
+        const int c = 16 * p + u;
+        x[u] *= invd[c];
+#pragma unroll
+        for (int u2 = u + 1; u2 < 16; u2++) x[u2] -= x[u] * M[16 * p + u2][c];
+      }
+#pragma unroll
+      for (int u = 0; u < 16; u++) xs[16 * p + u][r] = x[u];
+    }
+    __syncthreads();
+    if (q > p) {  // subtract quarter p's contribution
 #pragma unroll 4
-    for (int k = 0; k < q0; k++) {
-      const T xk = xs[k][tid];
+      for (int kk = 0; kk < 16; kk++) {
+        const int k = 16 * p + kk;
+        const T xk = xs[k][r];
 #pragma unroll
-      for (int c = 0; c < Q; c++) x[c] -= xk * M[q0 + c][k];
+        for (int u = 0; u < 16; u++) x[u] -= xk * M[16 * q + u][k];
+      }
     }
+  }
+  if (!active) return;
+  const int ld8 = (m + 7) & ~7;
 #pragma unroll
-    for (int c = 0; c < Q; c++) {
-      x[c] *= invd[q0 + c];
-#pragma unroll
-      for (int c2 = c + 1; c2 < Q; c2++) x[c2] -= x[c] * M[q0 + c2][q0 + c];
-    }
-#pragma unroll
-    for (int c = 0; c < Q; c++) {
-      const int cc = q0 + c;
-      xs[cc][tid] = x[c];
-      if (cc >= w) continue;
-      const T xv = x[c];
-      Lp[(int64_t)(c0 + cc) * m + row] = xv;
-      const T wv = ldlt ? xv * dv[cc] : T(0);
-      if (ldlt && ld.W) ld.W[P.snLxp[s] + (int64_t)(c0 + cc) * m + row] = wv;
-      if (Shi) {
-        const int64_t g = P.snSp[s] + (int64_t)(c0 + cc) * ld8 + row;
-        const __nv_bfloat16 hi = __float2bfloat16_rn((float)xv);
-        Shi[g] = hi;
-        Slo[g] = __float2bfloat16_rn((float)xv - __bfloat162float(hi));
-        if (ldlt) {
-          const __nv_bfloat16 whi = __float2bfloat16_rn((float)wv);
-          ld.Whi[g] = whi;
-          ld.Wlo[g] = __float2bfloat16_rn((float)wv - __bfloat162float(whi));
-        }
+  for (int u = 0; u < 16; u++) {
+    const int cc = 16 * q + u;
+    if (cc >= w) break;
+    const T xv = x[u];
+    Lp[(int64_t)(c0 + cc) * m + row] = xv;
+    const T wv = ldlt ? xv * dv[cc] : T(0);
+    if (ldlt && ld.W) ld.W[P.snLxp[s] + (int64_t)(c0 + cc) * m + row] = wv;
+    if (Shi) {
+      const int64_t g = P.snSp[s] + (int64_t)(c0 + cc) * ld8 + row;
+      const __nv_bfloat16 hi = __float2bfloat16_rn((float)xv);
+      Shi[g] = hi;
+      Slo[g] = __float2bfloat16_rn((float)xv - __bfloat162float(hi));
+      if (ldlt) {
+        const __nv_bfloat16 whi = __float2bfloat16_rn((float)wv);
+        ld.Whi[g] = whi;
+        ld.Wlo[g] = __float2bfloat16_rn((float)wv - __bfloat162float(whi));
       }
     }
   }
@@ -563,7 +600,7 @@ void launch_potrf(const PotrfTask *tasks, int64_t ntasks, const DevPlan &P, T *L
 template <class T>
 void launch_trsm(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, T *Lx, const unsigned long long *status,
                  __nv_bfloat16 *Shi, __nv_bfloat16 *Slo, const LdltArgs<T> &ld, cudaStream_t st) {
-  if (ntasks > 0) k_trsm<T><<<(unsigned)ntasks, kPanel, kTrsmSmem, st>>>(tasks, P, Lx, status, Shi, Slo, ld);
+  if (ntasks > 0) k_trsm<T><<<(unsigned)ntasks, 256, kTrsmSmem, st>>>(tasks, P, Lx, status, Shi, Slo, ld);
 }
 template void launch_potrf<double>(const PotrfTask *, int64_t, const DevPlan &, double *, unsigned long long *,
                                    const LdltArgs<double> &, cudaStream_t);
