@@ -101,6 +101,7 @@ SIGNATURES = {
     "amp_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int]),
     "amp_solve_refined": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int, C.POINTER(_RefineOpts),
                                     C.POINTER(_RefineStats)]),
+    "amp_factor_set_row_groups": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
     "amp_solve_gmres": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(_GmresOpts),
                                   C.POINTER(_GmresStats)]),
     "amp_factor_download": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -336,6 +337,16 @@ class NumericFactor:
                                        X.ctypes.data if X.size else None, 0, C.byref(ro), C.byref(st)))
         return X, st.rel_residual, st.steps
 
+    def set_row_groups(self, offsets) -> None:
+        """The factored matrix is block diagonal: rows [offsets[g], offsets[g + 1]) form independent systems.
+        Refinement then stops when ||b - A x|| / ||b|| of every system and right-hand side is below tol, as separate
+        solveRefined calls (ldlt.mjs:257-269) would. offsets=None clears."""
+        if offsets is None:
+            _check(lib().amp_factor_set_row_groups(self._h, 0, None))
+            return
+        o = np.ascontiguousarray(offsets, dtype=np.int64)
+        _check(lib().amp_factor_set_row_groups(self._h, len(o) - 1, o.ctypes.data))
+
     def solve_gmres(self, b, tol: float = 1e-10, restart: int = 40, maxIter: int = 400) -> dict:
         """gmres(A, precond = this factor's solve, b, {tol, restart, maxIter}) (gmres-real.mjs:31-105) on the device,
         from x0 = 0: GMRES-based refinement with a mixed-precision factor. Returns {x, iterations, relres,
@@ -346,6 +357,14 @@ class NumericFactor:
         _check(lib().amp_solve_gmres(self._h, bb.ctypes.data if bb.size else None, x.ctypes.data if x.size else None,
                                      0, C.byref(_GmresOpts(tol, restart, maxIter)), C.byref(st)))
         return {"x": x, "iterations": st.iterations, "relres": st.rel_residual, "converged": bool(st.converged)}
+
+    def solve_gmres_ptr(self, b_ptr: int, x_ptr: int, on_device: bool, tol: float = 1e-10, restart: int = 40,
+                        maxIter: int = 400):
+        """solve_gmres for raw buffers (device, or host pinned): returns (relres, iterations, converged)."""
+        st = _GmresStats()
+        _check(lib().amp_solve_gmres(self._h, C.c_void_p(b_ptr), C.c_void_p(x_ptr), 1 if on_device else 0,
+                                     C.byref(_GmresOpts(tol, restart, maxIter)), C.byref(st)))
+        return st.rel_residual, st.iterations, bool(st.converged)
 
     @property
     def Lx(self) -> np.ndarray:

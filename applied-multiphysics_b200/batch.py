@@ -6,8 +6,9 @@ trees, and the etree postorder visits the roots in increasing index, so every ma
 column counts and supernodes it has alone, offset by its first row. Each etree level of all the matrices goes in one
 launch, and the whole numeric factorization of the batch is one captured CUDA graph.
 
-Right-hand sides: matrix i has q_i of them; the batch solves max q_i vectors in one pass (zeros where a matrix has
-fewer) and refines them in FP64 against the block-diagonal values.
+Right-hand sides: matrix i has q_i of them; the batch solves max q_i vectors together (zeros where a matrix has
+fewer) and refines them in FP64 against the block-diagonal values until every matrix's relative residual
+||b_i - A_i x_i|| / ||b_i|| is below the tolerance for each of its right-hand sides.
 """
 from __future__ import annotations
 
@@ -59,6 +60,7 @@ class BatchedCholesky:
             if self.count else np.zeros(0, np.int64)
         self.sym = amp.analyze(self.pat, perm=perm.astype(np.int32))
         self.num = amp.NumericFactor(self.sym, amp.CHOLESKY, precision)
+        self.num.set_row_groups(self.offs)  # refinement measures each matrix's residual on its own
         self.values = None
 
     def factor(self, values: Sequence) -> bool:
@@ -67,7 +69,8 @@ class BatchedCholesky:
         return self.num.factor(self.values)
 
     def solve_refined(self, rhs: Sequence, maxSteps: int = 10, tol: float = 1e-12):
-        """rhs[i]: (q_i, n_i) array. Returns ([x_i (q_i, n_i)], worst relative residual, refinement steps)."""
+        """rhs[i]: (q_i, n_i) array. Returns ([x_i (q_i, n_i)], worst per-matrix relative residual, refinement
+        steps)."""
         q = max((np.asarray(r).reshape(-1, int(self.offs[i + 1] - self.offs[i])).shape[0] for i, r in enumerate(rhs)),
                 default=0)
         N = self.pat.n

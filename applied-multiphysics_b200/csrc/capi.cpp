@@ -196,10 +196,16 @@ struct amp_factor_s {
          *gH = nullptr;
   unsigned long long *dSolveStatus = nullptr;
   int solveEpoch = 0;
+  // refinement row groups (independent diagonal blocks): group id per row, or none
+  int ngroups = 0;
+  int *dRowGroup = nullptr;
+  double *dGroupNorms = nullptr;  // 2 x groups x multi_max_vectors()
+  DevMem groupMem;
   ~amp_factor_s() {
     if (factorGraph) cudaGraphExecDestroy(factorGraph);
     for (auto e : evPool) cudaEventDestroy(e);
     smem.release();
+    groupMem.release();
     mem.release();
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -268,10 +274,11 @@ void ensure_solve_ws(amp_factor *f, int q) {
 }
 
 enum KernelKind {
-  K_ASSEMBLE, K_PANEL, K_UPDATE, K_FORWARD, K_BACKWARD, K_PERMUTE, K_RESIDUAL, K_POTRF, K_DIAGINV, K_NKINDS
+  K_ASSEMBLE, K_PANEL, K_UPDATE, K_FORWARD, K_BACKWARD, K_PERMUTE, K_RESIDUAL, K_POTRF, K_DIAGINV, K_KRYLOV, K_NKINDS
 };
-const char *kKindNames[K_NKINDS] = {"assemble", "panel_trsm", "update_syrk", "solve_forward",
-                                    "solve_backward", "permute", "residual_spmv", "potrf", "diag_inverse"};
+const char *kKindNames[K_NKINDS] = {"assemble",      "panel_trsm", "update_syrk", "solve_forward",
+                                    "solve_backward", "permute",    "residual_spmv", "potrf",
+                                    "diag_inverse",  "krylov"};
 
 cudaEvent_t pool_event(amp_factor *f) {
   if (f->evUsed == f->evPool.size()) {
@@ -383,34 +390,33 @@ void enqueue_factor(amp_factor *f) {
 }
 
 // y (permuted order, q vectors) := A^-1 y in place
-void device_solve_permuted(amp_factor *f, int q) {
+void device_solve_permuted(amp_factor *f) {
   const amp::Plan &P = f->plan->P;
   const amp::DevPlan &dp = f->plan->dp;
   const int64_t Vs = P.nsuper ? P.Sp[P.nsuper] : 0, Ts = P.solveBufDoubles;
-  const double lbytes = (f->dL32 ? 4.0 : 8.0) * (double)P.nnzLStored * q;  // each sweep reads L once per RHS
+  const double lbytes = (f->dL32 ? 4.0 : 8.0) * (double)P.nnzLStored;  // each sweep reads L once
   cudaStream_t st = f->stream;
   ck(cudaMemsetAsync(f->dTickets, 0, sizeof(int) * 2, st), "memset tickets");
   ck(cudaMemsetAsync(f->dDone, 0, sizeof(int) * std::max(1, P.nsuper), st), "memset done");
   ck(cudaMemsetAsync(f->dSolveStatus, 0xff, sizeof(unsigned long long), st), "memset status");
   const int efwd = 2 * (++f->solveEpoch) - 1, ebwd = 2 * f->solveEpoch;
   const int nf = P.fwdLvlPtr[P.nlevels], nb = (int)(P.bwdAll.size() / 4);
-  timed(f, K_FORWARD, 0.0, lbytes, [&] {
+  const double *Dp = f->kind == AMP_LDLT ? f->dD : nullptr;
+  timed(f, K_FORWARD, 2.0 * (double)P.nnzLStored, lbytes, [&] {
     if (f->dL32)
       amp::launch_fwd_blocks<float>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->dL32, f->dInv32, f->dY, f->dV, f->dT,
-                                    f->dFlags, efwd, f->dDone, q, Vs, Ts, f->dSolveStatus, st);
+                                    f->dFlags, efwd, f->dDone, 1, Vs, Ts, f->dSolveStatus, st);
     else
       amp::launch_fwd_blocks<double>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->dLx, f->dInv, f->dY, f->dV, f->dT,
-                                     f->dFlags, efwd, f->dDone, q, Vs, Ts, f->dSolveStatus, st);
+                                     f->dFlags, efwd, f->dDone, 1, Vs, Ts, f->dSolveStatus, st);
   });
-  timed(f, K_BACKWARD, 0.0, lbytes, [&] {
+  timed(f, K_BACKWARD, 2.0 * (double)P.nnzLStored, lbytes, [&] {
     if (f->dL32)
-      amp::launch_bwd_blocks<float>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dL32, f->dInv32,
-                                    f->kind == AMP_LDLT ? f->dD : nullptr, f->dY, f->dFlags, ebwd, q,
-                                    f->dSolveStatus, st);
+      amp::launch_bwd_blocks<float>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dL32, f->dInv32, Dp, f->dY,
+                                    f->dFlags, ebwd, 1, f->dSolveStatus, st);
     else
-      amp::launch_bwd_blocks<double>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dLx, f->dInv,
-                                     f->kind == AMP_LDLT ? f->dD : nullptr, f->dY, f->dFlags, ebwd, q,
-                                     f->dSolveStatus, st);
+      amp::launch_bwd_blocks<double>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dLx, f->dInv, Dp, f->dY, f->dFlags,
+                                     ebwd, 1, f->dSolveStatus, st);
   });
 }
 
@@ -422,13 +428,128 @@ int solve_status(amp_factor *f) {
   return AMP_OK;
 }
 
-// x = A^-1 b for device vectors (original order)
-void device_solve(amp_factor *f, const double *dB, double *dX, int q) {
+// x = A^-1 b for one device vector (original order)
+void device_solve(amp_factor *f, const double *dB, double *dX) {
+  const amp::Plan &P = f->plan->P;
+  const double pb = 20.0 * P.n;
+  timed(f, K_PERMUTE, 0.0, pb, [&] { amp::launch_permute_in(dB, f->dY, f->plan->dp.perm, P.n, 1, f->stream); });
+  device_solve_permuted(f);
+  timed(f, K_PERMUTE, 0.0, pb, [&] { amp::launch_permute_out(f->dY, dX, f->plan->dp.perm, P.n, 1, f->stream); });
+}
+
+// ---- several right-hand sides: groups of up to multi_max_vectors() vectors, interleaved ([i q + k]) -------------
+// y (permuted order, interleaved) := A^-1 y in place
+void device_solve_multi_permuted(amp_factor *f, int q) {
+  const amp::Plan &P = f->plan->P;
+  const amp::DevPlan &dp = f->plan->dp;
+  const double lbytes = (f->dL32 ? 4.0 : 8.0) * (double)P.nnzLStored;  // each sweep reads L once for all q vectors
+  const double flops = 2.0 * (double)P.nnzLStored * q;
+  cudaStream_t st = f->stream;
+  ck(cudaMemsetAsync(f->dTickets, 0, sizeof(int) * 2, st), "memset tickets");
+  ck(cudaMemsetAsync(f->dDone, 0, sizeof(int) * std::max(1, P.nsuper), st), "memset done");
+  ck(cudaMemsetAsync(f->dSolveStatus, 0xff, sizeof(unsigned long long), st), "memset status");
+  const int efwd = 2 * (++f->solveEpoch) - 1, ebwd = 2 * f->solveEpoch;
+  const int nf = P.fwdLvlPtr[P.nlevels], nb = (int)(P.bwdAll.size() / 4);
+  const double *Dp = f->kind == AMP_LDLT ? f->dD : nullptr;
+  timed(f, K_FORWARD, flops, lbytes, [&] {
+    if (f->dL32)
+      amp::launch_fwd_multi<float>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->dL32, f->dInv32, f->dY, f->dV, f->dT,
+                                   f->dFlags, efwd, f->dDone, q, f->dSolveStatus, st);
+    else
+      amp::launch_fwd_multi<double>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->dLx, f->dInv, f->dY, f->dV, f->dT,
+                                    f->dFlags, efwd, f->dDone, q, f->dSolveStatus, st);
+  });
+  timed(f, K_BACKWARD, flops, lbytes, [&] {
+    if (f->dL32)
+      amp::launch_bwd_multi<float>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dL32, f->dInv32, Dp, f->dY,
+                                   f->dFlags, ebwd, q, f->dSolveStatus, st);
+    else
+      amp::launch_bwd_multi<double>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dLx, f->dInv, Dp, f->dY, f->dFlags,
+                                    ebwd, q, f->dSolveStatus, st);
+  });
+}
+
+// xil = A^-1 bil, interleaved vectors in the original order
+void device_solve_il(amp_factor *f, const double *bil, double *xil, int q) {
   const amp::Plan &P = f->plan->P;
   const double pb = 20.0 * P.n * q;
-  timed(f, K_PERMUTE, 0.0, pb, [&] { amp::launch_permute_in(dB, f->dY, f->plan->dp.perm, P.n, q, f->stream); });
-  device_solve_permuted(f, q);
-  timed(f, K_PERMUTE, 0.0, pb, [&] { amp::launch_permute_out(f->dY, dX, f->plan->dp.perm, P.n, q, f->stream); });
+  timed(f, K_PERMUTE, 0.0, pb,
+        [&] { amp::launch_rows_permute(bil, f->dY, f->plan->dp.perm, P.n, q, false, f->stream); });
+  if (q == 1)  // one vector: the interleaved layout is the plain one
+    device_solve_permuted(f);
+  else
+    device_solve_multi_permuted(f, q);
+  timed(f, K_PERMUTE, 0.0, pb,
+        [&] { amp::launch_rows_permute(f->dY, xil, f->plan->dp.perm, P.n, q, true, f->stream); });
+}
+
+// x = A^-1 b for nrhs > 1 vectors stored one after another (host or device), refined in FP64 when o is given.
+// Each group of up to multi_max_vectors() vectors is moved to the interleaved layout, solved (and refined) and moved
+// back. stt receives the worst relative residual and the largest number of refinement steps over the groups.
+int solve_many(amp_factor *f, const double *b, int nrhs, double *x, bool on_device, const amp_refine_opts *o,
+               amp_refine_stats *stt) {
+  const amp::Plan &P = f->plan->P;
+  const int n = P.n, G = amp::multi_max_vectors();
+  ensure_solve_ws(f, std::min(nrhs, G));
+  cudaStream_t st = f->stream;
+  double worst = 0;
+  int maxSteps = 0;
+  const int ng = std::max(1, f->ngroups);
+  double *dNorms = f->ngroups > 0 ? f->dGroupNorms : f->dNorms;
+  std::vector<double> norms(2 * (size_t)ng * G);
+  for (int g0 = 0; g0 < nrhs; g0 += G) {
+    const int qg = std::min(G, nrhs - g0);
+    const size_t len = (size_t)n * qg, bytes = sizeof(double) * len;
+    const double *bg = b + (size_t)g0 * n;
+    double *xg = x + (size_t)g0 * n;
+    if (!on_device) {
+      ck(cudaMemcpyAsync(f->dDX, bg, bytes, cudaMemcpyHostToDevice, st), "copy b");
+      amp::launch_to_interleaved(f->dDX, f->dB, n, qg, st);
+    } else {
+      amp::launch_to_interleaved(bg, f->dB, n, qg, st);
+    }
+    device_solve_il(f, f->dB, f->dX, qg);
+    int steps = 0;
+    double gw = 0;  // worst relative residual of this group of vectors at its last residual evaluation
+    for (; o; steps++) {
+      const size_t nn = (size_t)2 * ng * qg;
+      ck(cudaMemsetAsync(dNorms, 0, sizeof(double) * nn, st), "memset");
+      timed(f, K_RESIDUAL, 2.0 * P.patNnz * qg, 12.0 * P.patNnz + 24.0 * n * qg, [&] {
+        amp::launch_residual_multi(n, f->plan->dRowptr, f->plan->dColidx, f->dValues, f->dX, f->dB, f->dR, dNorms, qg,
+                                   f->ngroups > 0 ? f->dRowGroup : nullptr, st);
+      });
+      ck(cudaMemcpyAsync(norms.data(), dNorms, sizeof(double) * nn, cudaMemcpyDeviceToHost, st), "norms");
+      ck(cudaStreamSynchronize(st), "residual");
+      gw = 0;
+      bool any = false;
+      for (size_t e = 0; e < (size_t)ng * qg; e++) {  // (row group, vector) pairs
+        double bn = std::sqrt(norms[2 * e + 1]);
+        if (bn == 0 || std::isnan(bn)) bn = 1;
+        const double rel = std::sqrt(norms[2 * e]) / bn;
+        gw = std::max(gw, rel);
+        if (!(rel < o->tol)) any = true;
+      }
+      if (!any || steps >= o->max_steps) break;
+      device_solve_il(f, f->dR, f->dDX, qg);
+      amp::launch_axpy(f->dX, f->dDX, (int64_t)len, st);
+    }
+    worst = std::max(worst, gw);
+    maxSteps = std::max(maxSteps, steps);
+    if (!on_device) {
+      amp::launch_from_interleaved(f->dX, f->dDX, n, qg, st);
+      ck(cudaMemcpyAsync(xg, f->dDX, bytes, cudaMemcpyDeviceToHost, st), "copy x");
+    } else {
+      amp::launch_from_interleaved(f->dX, xg, n, qg, st);
+    }
+  }
+  ck(cudaGetLastError(), "kernel launch");
+  ck(cudaStreamSynchronize(st), "solve");
+  if (int rc = solve_status(f)) return rc;
+  if (stt) {
+    stt->rel_residual = worst;
+    stt->steps = maxSteps;
+  }
+  return (int)AMP_OK;
 }
 
 template <class F>
@@ -746,6 +867,7 @@ int amp_solve(amp_factor *f, const double *b, int32_t nrhs, double *x, int on_de
     const amp::Plan &P = f->plan->P;
     if (nrhs <= 0 || P.n == 0) return (int)AMP_OK;
     ck(cudaSetDevice(f->plan->device), "cudaSetDevice");
+    if (nrhs > 1) return solve_many(f, b, nrhs, x, on_device != 0, nullptr, nullptr);
     ensure_solve_ws(f, nrhs);
     size_t bytes = sizeof(double) * (size_t)P.n * nrhs;
     const double *dB = b;
@@ -755,7 +877,7 @@ int amp_solve(amp_factor *f, const double *b, int32_t nrhs, double *x, int on_de
       dB = f->dB;
       dX = f->dX;
     }
-    device_solve(f, dB, dX, nrhs);
+    device_solve(f, dB, dX);
     ck(cudaGetLastError(), "kernel launch");
     if (!on_device) ck(cudaMemcpyAsync(x, dX, bytes, cudaMemcpyDeviceToHost, f->stream), "copy x");
     ck(cudaStreamSynchronize(f->stream), "solve");
@@ -777,6 +899,11 @@ int amp_solve_refined(amp_factor *f, const double *b, int32_t nrhs, double *x, i
       return (int)AMP_OK;
     }
     ck(cudaSetDevice(f->plan->device), "cudaSetDevice");
+    if (nrhs > 1 || f->ngroups > 0) {
+      const int rc = solve_many(f, b, nrhs, x, on_device != 0, &o, &stt);
+      if (rc == AMP_OK && stats) *stats = stt;
+      return rc;
+    }
     ensure_solve_ws(f, nrhs);
     const int n = P.n;
     size_t len = (size_t)n * nrhs, bytes = sizeof(double) * len;
@@ -788,7 +915,7 @@ int amp_solve_refined(amp_factor *f, const double *b, int32_t nrhs, double *x, i
       dB = f->dB;
       dX = f->dX;
     }
-    device_solve(f, dB, dX, nrhs);
+    device_solve(f, dB, dX);
     std::vector<double> norms(2 * (size_t)nrhs);
     std::vector<char> active(nrhs, 1);
     double worst = 0;
@@ -810,7 +937,7 @@ int amp_solve_refined(amp_factor *f, const double *b, int32_t nrhs, double *x, i
         if (!(rel < o.tol)) any = true;
       }
       if (!any || steps >= o.max_steps) break;
-      device_solve(f, f->dR, f->dDX, nrhs);
+      device_solve(f, f->dR, f->dDX);
       amp::launch_axpy(dX, f->dDX, (int64_t)len, st);
     }
     ck(cudaGetLastError(), "kernel launch");
@@ -820,6 +947,30 @@ int amp_solve_refined(amp_factor *f, const double *b, int32_t nrhs, double *x, i
     stt.rel_residual = worst;
     stt.steps = steps;
     if (stats) *stats = stt;
+    return (int)AMP_OK;
+  });
+}
+
+int amp_factor_set_row_groups(amp_factor *f, int32_t ngroups, const int64_t *offsets) {
+  return guarded([&] {
+    if (!f) return fail(AMP_INVALID, "null handle");
+    const int n = f->plan->P.n;
+    if (ngroups < 0 || (ngroups > 0 && !offsets)) return fail(AMP_INVALID, "row groups: bad arguments");
+    if (ngroups == 0) {
+      f->ngroups = 0;
+      return (int)AMP_OK;
+    }
+    if (offsets[0] != 0 || offsets[ngroups] != n) return fail(AMP_INVALID, "row groups: offsets must run from 0 to n");
+    std::vector<int> gid(n);
+    for (int g = 0; g < ngroups; g++) {
+      if (offsets[g + 1] < offsets[g]) return fail(AMP_INVALID, "row groups: offsets must not decrease");
+      for (int64_t i = offsets[g]; i < offsets[g + 1]; i++) gid[i] = g;
+    }
+    ck(cudaSetDevice(f->plan->device), "cudaSetDevice");
+    f->groupMem.release();
+    f->dRowGroup = f->groupMem.upload(gid);
+    f->dGroupNorms = f->groupMem.alloc<double>((size_t)2 * ngroups * amp::multi_max_vectors());
+    f->ngroups = ngroups;
     return (int)AMP_OK;
   });
 }
@@ -862,18 +1013,20 @@ int amp_solve_gmres(amp_factor *f, const double *b, double *x, int on_device, co
     ck(cudaMemsetAsync(xb, 0, sizeof(double) * n, st), "zero x");
     std::vector<double> h(m + 1), H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
     auto dots = [&](const double *Vs, int nv, const double *v) {  // h[0..nv) = Vs[j] . v (synchronises)
-      amp::launch_dots(Vs, nv, n, v, part, dh, st);
+      timed(f, K_KRYLOV, 2.0 * n * nv, 8.0 * n * (nv + 1), [&] { amp::launch_dots(Vs, nv, n, v, part, dh, st); });
       ck(cudaMemcpyAsync(h.data(), dh, sizeof(double) * nv, cudaMemcpyDeviceToHost, st), "dots");
       ck(cudaStreamSynchronize(st), "dots");
     };
     auto residual = [&]() {  // r = b - A x, returns ||r||
-      amp::launch_matvec((int)n, f->plan->dRowptr, f->plan->dColidx, f->dValues, xb, w, 1, st);
-      amp::launch_sub_from(r, bb, w, n, st);
+      timed(f, K_RESIDUAL, 2.0 * P.patNnz, 12.0 * P.patNnz + 16.0 * n, [&] {
+        amp::launch_matvec((int)n, f->plan->dRowptr, f->plan->dColidx, f->dValues, xb, w, 1, st);
+      });
+      timed(f, K_KRYLOV, (double)n, 24.0 * n, [&] { amp::launch_sub_from(r, bb, w, n, st); });
       dots(r, 1, r);
       return std::sqrt(h[0]);
     };
     auto precond = [&](const double *v, double *z) {  // z = M^-1 v (the factor's solve)
-      device_solve(f, v, z, 1);
+      device_solve(f, v, z);
       ck(cudaGetLastError(), "kernel launch");
     };
     dots(bb, 1, bb);
@@ -884,26 +1037,31 @@ int amp_solve_gmres(amp_factor *f, const double *b, double *x, int on_device, co
     double relres = beta / bnorm;
     int iters = 0;
     while (relres > o.tol && iters < o.max_iter) {
-      amp::launch_scale_to(V, r, 1.0 / beta, n, st);
+      timed(f, K_KRYLOV, (double)n, 16.0 * n, [&] { amp::launch_scale_to(V, r, 1.0 / beta, n, st); });
       std::fill(g.begin(), g.end(), 0.0);
       g[0] = beta;
       int k = 0;
       for (; k < m && iters < o.max_iter; k++) {
         iters++;
         precond(V + (int64_t)k * n, Z + (int64_t)k * n);
-        amp::launch_matvec((int)n, f->plan->dRowptr, f->plan->dColidx, f->dValues, Z + (int64_t)k * n, w, 1, st);
+        timed(f, K_RESIDUAL, 2.0 * P.patNnz, 12.0 * P.patNnz + 16.0 * n, [&] {
+          amp::launch_matvec((int)n, f->plan->dRowptr, f->plan->dColidx, f->dValues, Z + (int64_t)k * n, w, 1, st);
+        });
         // classical Gram-Schmidt twice (as stable as modified Gram-Schmidt, two reductions per iteration)
         for (int j = 0; j <= k; j++) H[(size_t)j * m + k] = 0.0;
         for (int pass = 0; pass < 2; pass++) {
           dots(V, k + 1, w);
           ck(cudaMemcpyAsync(dh, h.data(), sizeof(double) * (k + 1), cudaMemcpyHostToDevice, st), "h");
-          amp::launch_gs_update(w, V, dh, k + 1, n, st);
+          timed(f, K_KRYLOV, 2.0 * n * (k + 1), 8.0 * n * (k + 3),
+                [&] { amp::launch_gs_update(w, V, dh, k + 1, n, st); });
           for (int j = 0; j <= k; j++) H[(size_t)j * m + k] += h[j];
         }
         dots(w, 1, w);
         const double hn = std::sqrt(h[0]);
         H[(size_t)(k + 1) * m + k] = hn;
-        if (hn > 0) amp::launch_scale_to(V + (int64_t)(k + 1) * n, w, 1.0 / hn, n, st);
+        if (hn > 0)
+          timed(f, K_KRYLOV, (double)n, 16.0 * n,
+                [&] { amp::launch_scale_to(V + (int64_t)(k + 1) * n, w, 1.0 / hn, n, st); });
         for (int j = 0; j < k; j++) {  // apply the previous Givens rotations
           const double a = H[(size_t)j * m + k], c = H[(size_t)(j + 1) * m + k];
           H[(size_t)j * m + k] = cs[j] * a + sn[j] * c;
@@ -930,7 +1088,7 @@ int amp_solve_gmres(amp_factor *f, const double *b, double *x, int on_device, co
         y[i] = s / H[(size_t)i * m + i];
       }
       ck(cudaMemcpyAsync(dh, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st), "y");
-      amp::launch_combine_add(xb, Z, dh, k, n, st);
+      timed(f, K_KRYLOV, 2.0 * n * k, 8.0 * n * (k + 2), [&] { amp::launch_combine_add(xb, Z, dh, k, n, st); });
       if (relres <= o.tol || iters >= o.max_iter) break;
       beta = residual();
       relres = beta / bnorm;

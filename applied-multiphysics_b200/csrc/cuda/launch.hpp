@@ -41,4 +41,20 @@ void launch_bwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan
                        const double *Dpiv, double *y, int *flags, int epoch, int q, unsigned long long *status,
                        cudaStream_t st);
 
+// several right-hand sides (q <= multi_max_vectors(), interleaved: entry i of vector k at [i q + k])
+int multi_max_vectors();
+template <class TL>
+void launch_fwd_multi(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
+                      double *y, double *V, double *T, int *flags, int epoch, int *done, int q,
+                      unsigned long long *status, cudaStream_t st);
+template <class TL>
+void launch_bwd_multi(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
+                      const double *Dpiv, double *y, int *flags, int epoch, int q, unsigned long long *status,
+                      cudaStream_t st);
+void launch_to_interleaved(const double *B, double *Yil, int n, int q, cudaStream_t st);
+void launch_from_interleaved(const double *Xil, double *X, int n, int q, cudaStream_t st);
+void launch_rows_permute(const double *src, double *dst, const int *perm, int n, int q, bool scatter, cudaStream_t st);
+void launch_residual_multi(int n, const int *rowptr, const int *colidx, const double *val, const double *x,
+                           const double *b, double *r, double *norms, int q, const int *rowGroup, cudaStream_t st);
+
 }  // namespace amp

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <map>
+#include <set>
 #include <stdexcept>
 
 namespace amp {
@@ -12,16 +13,17 @@ namespace {
 // Offline first-fit allocator over one arena (offsets in doubles, 256-byte aligned blocks).
 class ArenaPlanner {
  public:
+  // best fit among the free blocks (smallest that fits, lowest offset among equals), else the top
   int64_t alloc(int64_t size) {
     size = (size + 31) & ~int64_t(31);
-    for (auto it = free_.begin(); it != free_.end(); ++it) {
-      if (it->second >= size) {
-        int64_t off = it->first, rest = it->second - size;
-        free_.erase(it);
-        if (rest > 0) free_[off + size] = rest;
-        used_[off] = size;
-        return off;
-      }
+    auto b = bySize_.lower_bound({size, INT64_MIN});
+    if (b != bySize_.end()) {
+      const int64_t bsize = b->first, off = b->second, rest = bsize - size;
+      bySize_.erase(b);
+      free_.erase(off);
+      if (rest > 0) add_free(off + size, rest);
+      used_[off] = size;
+      return off;
     }
     int64_t off = top_;
     top_ += size;
@@ -33,31 +35,42 @@ class ArenaPlanner {
     if (u == used_.end()) throw std::logic_error("arena planner: double free");
     int64_t size = u->second;
     used_.erase(u);
-    auto it = free_.emplace(off, size).first;
-    auto nx = std::next(it);
-    if (nx != free_.end() && it->first + it->second == nx->first) {
-      it->second += nx->second;
-      free_.erase(nx);
+    // merge with the free neighbours
+    auto nx = free_.lower_bound(off);
+    if (nx != free_.end() && off + size == nx->first) {
+      size += nx->second;
+      remove_free(nx->first);
     }
-    if (it != free_.begin()) {
-      auto pv = std::prev(it);
-      if (pv->first + pv->second == it->first) {
-        pv->second += it->second;
-        free_.erase(it);
-        it = pv;
+    auto pv = free_.lower_bound(off);
+    if (pv != free_.begin()) {
+      --pv;
+      if (pv->first + pv->second == off) {
+        off = pv->first;
+        size += pv->second;
+        remove_free(off);
       }
     }
-    if (it->first + it->second == top_) {  // shrink the top
-      top_ = it->first;
-      free_.erase(it);
-    }
+    if (off + size == top_)  // shrink the top
+      top_ = off;
+    else
+      add_free(off, size);
     peak_ = std::max(peak_, top_);
   }
   int64_t peak() const { return std::max(peak_, top_); }
   void note() { peak_ = std::max(peak_, top_); }
 
  private:
-  std::map<int64_t, int64_t> free_, used_;
+  void add_free(int64_t off, int64_t size) {
+    free_[off] = size;
+    bySize_.insert({size, off});
+  }
+  void remove_free(int64_t off) {
+    auto it = free_.find(off);
+    bySize_.erase({it->second, off});
+    free_.erase(it);
+  }
+  std::map<int64_t, int64_t> free_, used_;      // offset -> size
+  std::set<std::pair<int64_t, int64_t>> bySize_;  // (size, offset) of the free blocks
   int64_t top_ = 0, peak_ = 0;
 };
 

@@ -218,6 +218,38 @@ def cpu_baseline_sample(w, perm, budget_s: float = 15.0, kind: str = "chol"):
             "full_factor_s_est": so.flops / (fl / dt)}
 
 
+# DRAM bytes per launch of the roofline kernel (dram__bytes_read.sum + dram__bytes_write.sum, one ncu capture of the
+# same command: the launch list of `bench.py --steps 1 --warmup 3 --no-cpu-baseline`, every launch of the kernel class
+# in the mixed phase, total / launches). Keyed by (workload, size, precision, kernel class).
+TRAFFIC = {
+    ("elastic3d", 40, "mixed", "update_syrk"): 65.085e9 / 2093,
+}
+
+
+def solution_errors(w, results):
+    """Per precision: the normwise backward error max_k ||b_k - A x_k|| / (||A||_F ||x_k|| + ||b_k||) (2-norms, FP64
+    on the host), and for the mixed path the forward error max_k ||x_k - x_k(FP64)|| / ||x_k(FP64)|| against the FP64
+    GPU solution (the FP64 path itself matches the oracle to 1e-12 in the parity tests)."""
+    import scipy.sparse as sp
+
+    A = sp.csr_matrix((w.values, w.pat.colidx, w.pat.rowptr), shape=(w.n, w.n))
+    anorm = float(np.sqrt(np.sum(w.values * w.values)))
+    B = np.ascontiguousarray(w.rhs[: next(iter(results.values()))["x"].shape[0]])
+    out = {}
+    for p, r in results.items():
+        X = r["x"]
+        be = 0.0
+        for k in range(X.shape[0]):
+            rk = B[k] - A @ X[k]
+            be = max(be, float(np.linalg.norm(rk) / (anorm * np.linalg.norm(X[k]) + np.linalg.norm(B[k]))))
+        out[p] = {"backward_error": be}
+    if "fp64" in results and "mixed" in results:
+        X, Xr = results["mixed"]["x"], results["fp64"]["x"]
+        fe = max(float(np.linalg.norm(X[k] - Xr[k]) / max(np.linalg.norm(Xr[k]), 1e-300)) for k in range(X.shape[0]))
+        out["mixed"]["forward_error_vs_fp64"] = fe
+    return out
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -264,8 +296,6 @@ def main():
     args.metric = METRIC.format(title=sysinfo["title"].format(N=args.size))
     args.desc = sysinfo["desc"].format(N=args.size)
     args.ldlt = sysinfo["kind"] == "ldlt"
-    if args.ldlt:  # LDL^T runs in FP64 only
-        args.precision = "fp64"
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -306,10 +336,24 @@ def main():
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
     for prec in precisions:
         num = amp.NumericFactor(sym, amp.LDLT if args.ldlt else amp.CHOLESKY, amp.FP64 if prec == "fp64" else amp.MIXED)
+        if isinstance(w, _Batch):
+            num.set_row_groups(w.offs)  # the residual is measured per matrix
+
+        # indefinite systems in mixed precision: GMRES-IR (the mixed LDL^T as right preconditioner, FP64 Arnoldi on the
+        # device) instead of plain refinement, which need not converge when the FP32 factor's error is large
+        gmres = args.ldlt and prec == "mixed"
+
+        def solve(bp, xp, on_device):
+            if gmres:
+                rr, its, _ = num.solve_gmres_ptr(bp, xp, on_device, tol=5e-13, restart=40, maxIter=300)
+                return rr, its
+            if on_device:
+                return num.solve_refined_device(bp, xp, nq, maxSteps=10, tol=1e-12)
+            return num.solve_refined_host_pinned(bp, xp, nq, 10, 1e-12)
 
         def step():
             ok = num.factor((vals_d.data_ptr(), vals_d.numel()), on_device=True)
-            relres, steps = num.solve_refined_device(b_d.data_ptr(), x_d.data_ptr(), nq, maxSteps=10, tol=1e-12)
+            relres, steps = solve(b_d.data_ptr(), x_d.data_ptr(), True)
             return ok, relres, steps
 
         for _ in range(args.warmup):
@@ -342,7 +386,7 @@ def main():
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record()
             num.factor(vals_h.numpy())  # H2D of the values inside the call
-            rr, ss = num.solve_refined_host_pinned(b_h.data_ptr(), x_h.data_ptr(), nq, 10, 1e-12)  # H2D b, D2H x
+            rr, ss = solve(b_h.data_ptr(), x_h.data_ptr(), False)  # H2D b, D2H x inside the call
             b.record()
             torch.cuda.synchronize()
             e2e.append(a.elapsed_time(b))
@@ -354,12 +398,13 @@ def main():
         # profile pass: per-kernel device time with CUDA events on the factor's stream
         num.profile(True)
         num.factor((vals_d.data_ptr(), vals_d.numel()), on_device=True)
-        num.solve_refined_device(b_d.data_ptr(), x_d.data_ptr(), nq, maxSteps=10, tol=1e-12)
+        solve(b_d.data_ptr(), x_d.data_ptr(), True)
         prof = num.profile_read()
         num.profile(False)
+        xsol = x_d.cpu().numpy().reshape(nq, n)
         work = flops_factor + flops_solve  # the same algorithmic work for both precisions: factor + one solve
         results[prec] = {"ok": ok, "ms": ms, "relres": relres, "ir_steps": irs, "work": work, "clk": clk.summary(),
-                         "prof": prof, "e2e_ms": e2e_ms, "factor_ms": num.ms}
+                         "prof": prof, "e2e_ms": e2e_ms, "factor_ms": num.ms, "x": xsol}
         del num
     if rank != 0:
         if world > 1:
@@ -402,14 +447,16 @@ def main():
         "gpu_launches": int(launches * args.steps),
         "clocks": R["clk"],
         "roofline": {"bound": bound, "kernel": dom["name"], "achieved": achieved, "peak": peak, "unit": punit,
-                     "frac": achieved / peak, "traffic": None, "peak_source": note},
+                     "frac": achieved / peak, "traffic": TRAFFIC.get((args.workload, args.size, head, dom["name"])),
+                     "peak_source": note},
         "kernels": R["prof"],
         "fp64_dgemm_tflops": fp64_peak,
         "fp32_sgemm_tflops": fp32_peak,
     }
+    errs = solution_errors(w, results)
     for p, r in results.items():
         line[p] = {"ms_per_step": r["ms"], "value": world * r["work"] / (r["ms"] * 1e-3) / 1e12, "relres": r["relres"],
-                   "ir_steps": r["ir_steps"], "factor_ms": r["factor_ms"], "ok": r["ok"]}
+                   "ir_steps": r["ir_steps"], "factor_ms": r["factor_ms"], "ok": r["ok"], **errs.get(p, {})}
     if world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline_sample(w, sym.perm, kind="ldlt" if args.ldlt else "chol")
         line["cpu_baseline"] = {k: v for k, v in cb.items() if k != "full_factor_s_est"}

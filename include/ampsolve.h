@@ -152,6 +152,11 @@ AMP_API int amp_solve(amp_factor *f, const double *b, int32_t nrhs, double *x, i
  * of the last amp_factor_numeric call (the unperturbed matrix). */
 AMP_API int amp_solve_refined(amp_factor *f, const double *b, int32_t nrhs, double *x, int on_device,
                       const amp_refine_opts *opts, amp_refine_stats *stats);
+/* Row groups for amp_solve_refined: the factored matrix is block diagonal with ngroups independent systems, rows
+ * [offsets[g], offsets[g + 1]) (offsets[0] = 0, offsets[ngroups] = n, non-decreasing). Refinement then measures
+ * ||b - A x|| / ||b|| per system and right-hand side, as a separate solveRefined call per system would
+ * (ldlt.mjs:257-269), and stops when every one is below tol; stats report the largest. ngroups = 0 clears. */
+AMP_API int amp_factor_set_row_groups(amp_factor *f, int32_t ngroups, const int64_t *offsets);
 /* gmres(matvec, precond, b, {tol, restart, maxIter}) (gmres-real.mjs:31-105) with matvec = the factored matrix (FP64
  * CSR on the device) and precond = this factor's solve: restarted, right-preconditioned GMRES from x0 = 0, so with a
  * mixed-precision factor it is GMRES-based iterative refinement. One right-hand side; b, x host or device memory. */
@@ -172,7 +177,8 @@ typedef struct {
 AMP_API int amp_profile_enable(amp_factor *f, int enable);
 AMP_API int amp_profile_read(amp_factor *f, amp_kernel_stat *stats, int32_t cap, int32_t *count);
 /* The individual launches behind amp_profile_read (call before it; it clears the records): kernel class index (order
- * of amp_profile_read's names: assemble, panel, update, forward, backward, permute, residual), device ms, flops. */
+ * of amp_profile_read's names: assemble, panel_trsm, update_syrk, solve_forward, solve_backward, permute,
+ * residual_spmv, potrf, diag_inverse, krylov), device ms, flops. */
 AMP_API int amp_profile_launches(amp_factor *f, int32_t *kinds, double *ms, double *flops, int32_t cap,
                                  int32_t *count);
 
