@@ -147,6 +147,7 @@ struct amp_plan_s {
   amp::TileTask *dTile = nullptr, *dUTile = nullptr;
   amp::MixTask *dMixTile = nullptr, *dMixU = nullptr;
   int4 *dFwdTasks = nullptr, *dBwdTasks = nullptr, *dBwdAll = nullptr;
+  int *dTinySn = nullptr, *dSmallSn = nullptr;  // small fronts per level (whole fronts by one warp / one CTA)
   int *dRowptr = nullptr, *dColidx = nullptr;
   std::vector<int> rowptr, colidx;  // host copy of the pattern (uploaded with the schedule)
   bool uploaded = false;
@@ -245,6 +246,7 @@ void upload_plan(amp_plan *pl) {
   d.blkOff = m.upload(P.blkOff);
   d.invOff = m.upload(P.invOff);
   d.diagSlot = m.upload(P.diagSlot);
+  d.solveSmall = m.upload(P.solveSmall);
   pl->dAsm = m.upload(P.asmTasks);
   pl->dPotrf = m.upload(P.potrfTasks);
   pl->dPanel = m.upload(P.panelTasks);
@@ -255,6 +257,8 @@ void upload_plan(amp_plan *pl) {
   pl->dFwdTasks = (int4 *)m.upload(P.fwdTasks);
   pl->dBwdTasks = (int4 *)m.upload(P.bwdTasks);
   pl->dBwdAll = (int4 *)m.upload(P.bwdAll);
+  pl->dTinySn = m.upload(P.tinySn);
+  pl->dSmallSn = m.upload(P.smallSn);
 }
 
 void ensure_solve_ws(amp_factor *f, int q) {
@@ -274,11 +278,12 @@ void ensure_solve_ws(amp_factor *f, int q) {
 }
 
 enum KernelKind {
-  K_ASSEMBLE, K_PANEL, K_UPDATE, K_FORWARD, K_BACKWARD, K_PERMUTE, K_RESIDUAL, K_POTRF, K_DIAGINV, K_KRYLOV, K_NKINDS
+  K_ASSEMBLE, K_PANEL, K_UPDATE, K_FORWARD, K_BACKWARD, K_PERMUTE, K_RESIDUAL, K_POTRF, K_DIAGINV, K_KRYLOV,
+  K_FRONTS, K_NKINDS
 };
 const char *kKindNames[K_NKINDS] = {"assemble",      "panel_trsm", "update_syrk", "solve_forward",
                                     "solve_backward", "permute",    "residual_spmv", "potrf",
-                                    "diag_inverse",  "krylov"};
+                                    "diag_inverse",  "krylov",     "small_fronts"};
 
 cudaEvent_t pool_event(amp_factor *f) {
   if (f->evUsed == f->evPool.size()) {
@@ -303,6 +308,19 @@ void timed(amp_factor *f, int kind, double flops, double bytes, L &&launch) {
   f->recs.push_back(r);
 }
 
+// the small fronts of level L (whole fronts, one warp or one CTA each)
+template <class T>
+void enqueue_small_fronts(amp_factor *f, int L, T *Lx, T *U, const amp::LdltArgs<T> &la) {
+  const amp::Plan &P = f->plan->P;
+  const int64_t t0 = P.tinyPtr[L], t1 = P.tinyPtr[L + 1], s0 = P.smallPtr[L], s1 = P.smallPtr[L + 1];
+  if (t1 == t0 && s1 == s0) return;
+  const double scale = sizeof(T) / 8.0;
+  timed(f, K_FRONTS, 2.0 * P.frontLvlFlops[L], P.frontLvlBytes[L] * scale, [&] {
+    amp::launch_fronts_small<T>(f->plan->dTinySn + t0, (int)(t1 - t0), f->plan->dSmallSn + s0, (int)(s1 - s0),
+                                P.smallMaxM[L], f->plan->dp, f->dValues, Lx, U, f->dStatus, la, f->stream);
+  });
+}
+
 void enqueue_factor(amp_factor *f) {
   const amp::Plan &P = f->plan->P;
   const amp::DevPlan &dp = f->plan->dp;
@@ -316,10 +334,12 @@ void enqueue_factor(amp_factor *f) {
       amp::launch_ldlt_tau(f->dValues, dp, f->dScal, st);
     }
     for (int L = 0; L < P.nlevels; L++) {
-      timed(f, K_ASSEMBLE, 0.0, P.asmLvlBytes[L] / 2, [&] {
-        amp::launch_assemble<float>(f->plan->dAsm + P.asmLvlPtr[L], P.asmLvlPtr[L + 1] - P.asmLvlPtr[L], dp,
-                                    f->dValues, f->dL32, f->dU32, f->dStatus, st);
-      });
+      enqueue_small_fronts<float>(f, L, f->dL32, f->dU32, ld32);
+      if (P.asmLvlPtr[L + 1] > P.asmLvlPtr[L])
+        timed(f, K_ASSEMBLE, 0.0, P.asmLvlBytes[L] / 2, [&] {
+          amp::launch_assemble<float>(f->plan->dAsm + P.asmLvlPtr[L], P.asmLvlPtr[L + 1] - P.asmLvlPtr[L], dp,
+                                      f->dValues, f->dL32, f->dU32, f->dStatus, st);
+        });
       for (int k = P.lvlStepPtr[L]; k < P.lvlStepPtr[L + 1]; k++) {
         const amp::StepRange &sr = P.steps[k];
         timed(f, K_POTRF, sr.potrfFlops, 0.0, [&] {
@@ -358,10 +378,12 @@ void enqueue_factor(amp_factor *f) {
     amp::launch_ldlt_tau(f->dValues, dp, f->dScal, st);
   }
   for (int L = 0; L < P.nlevels; L++) {
-    timed(f, K_ASSEMBLE, 0.0, P.asmLvlBytes[L], [&] {
-      amp::launch_assemble<double>(f->plan->dAsm + P.asmLvlPtr[L], P.asmLvlPtr[L + 1] - P.asmLvlPtr[L], dp,
-                                   f->dValues, f->dLx, f->dU, f->dStatus, st);
-    });
+    enqueue_small_fronts<double>(f, L, f->dLx, f->dU, ld);
+    if (P.asmLvlPtr[L + 1] > P.asmLvlPtr[L])
+      timed(f, K_ASSEMBLE, 0.0, P.asmLvlBytes[L], [&] {
+        amp::launch_assemble<double>(f->plan->dAsm + P.asmLvlPtr[L], P.asmLvlPtr[L + 1] - P.asmLvlPtr[L], dp,
+                                     f->dValues, f->dLx, f->dU, f->dStatus, st);
+      });
     for (int k = P.lvlStepPtr[L]; k < P.lvlStepPtr[L + 1]; k++) {
       const amp::StepRange &sr = P.steps[k];
       timed(f, K_POTRF, sr.potrfFlops, 0.0, [&] {

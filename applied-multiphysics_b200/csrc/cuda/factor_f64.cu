@@ -573,12 +573,14 @@ static int g_num_sms = 148;
 void init_mixed_attributes();
 void init_solve_attributes();
 void init_solve_multi_attributes();
+void init_front_small_attributes();
 void init_kernel_attributes() {
   cudaFuncSetAttribute(k_trsm<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsmSmem);
   cudaFuncSetAttribute(k_trsm<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsmSmem);
   init_mixed_attributes();
   init_solve_attributes();
   init_solve_multi_attributes();
+  init_front_small_attributes();
   cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, kUpdateSmem);
   int dev = 0;
   cudaGetDevice(&dev);

@@ -25,6 +25,7 @@
 
 #include "../host/plan.hpp"
 #include "devplan.cuh"
+#include "solve_small.cuh"
 
 namespace amp {
 
@@ -124,6 +125,15 @@ __global__ void __launch_bounds__(256, 3) k_fwd_blocks(const int4 *__restrict__ 
   // persistent: take tickets until the list is exhausted (a task only waits for earlier tickets)
   auto run = [&](const int tkv) -> bool {
     const int4 t = tasks[tkv];
+    if (t.z == 2) {  // up to kSolveGroup supernodes with m <= 32, one warp each
+      const int warp = threadIdx.x >> 5;
+      if (threadIdx.x == 0) waitOk = 1;
+      __syncthreads();
+      if (warp < t.y && !small_fwd_warp<TL>(P.solveSmall[t.x + warp], P, Lx, y, T, done, status, &red[0][0] + 32 * warp))
+        waitOk = 0;
+      __syncthreads();
+      return waitOk != 0;
+    }
     const int s = t.x, blk = t.y, below = t.z;
     const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s], mu = m - nc;
     const TL *Lp = Lx + P.snLxp[s];
@@ -267,6 +277,15 @@ __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ 
   // persistent: take tickets until the list is exhausted (a task only waits for earlier tickets)
   auto run = [&](const int tkv) -> bool {
     const int4 t = tasks[tkv];
+    if (t.z == 2) {  // up to kSolveGroup supernodes with m <= 32, one warp each
+      const int warp = threadIdx.x >> 5;
+      if (threadIdx.x == 0) waitOk = 1;
+      __syncthreads();
+      if (warp < t.y && !small_bwd_warp<TL>(P.solveSmall[t.x + warp], P, Lx, Dpiv, y, flags, epoch, status))
+        waitOk = 0;
+      __syncthreads();
+      return waitOk != 0;
+    }
     const int s = t.x, blk = t.y;
     const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
     const TL *Lp = Lx + P.snLxp[s];

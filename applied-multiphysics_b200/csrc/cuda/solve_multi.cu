@@ -17,6 +17,7 @@
 
 #include "../host/plan.hpp"
 #include "devplan.cuh"
+#include "solve_small.cuh"
 
 namespace amp {
 
@@ -26,6 +27,7 @@ constexpr int kMQ = 64;              // vectors per pass (the host splits larger
 constexpr int kLdt = 66;             // shared tile row stride in doubles (even: 16-byte aligned double2 reads)
 constexpr int kMultiThreads = 256;
 constexpr int kMultiSmem = (2 * kKC + kMB) * kLdt * (int)sizeof(double);
+static_assert(kSolveGroup * 32 * kMQ * (int)sizeof(double) <= kMultiSmem, "small-supernode tasks: front vectors");
 constexpr long long kMSpinLimit = 1ll << 24;
 
 __device__ __forceinline__ int mld_acquire(const int *p) {
@@ -110,6 +112,16 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_fwd_multi(const int4 *__re
   const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
   auto run = [&](const int tkv) -> bool {
     const int4 t = tasks[tkv];
+    if (t.z == 2) {  // up to kSolveGroup supernodes with m <= 32, one warp each (32 x 64 doubles of msm per warp)
+      const int warp = tid >> 5;
+      if (tid == 0) waitOk = 1;
+      __syncthreads();
+      if (warp < t.y &&
+          !small_fwd_warp_multi<TL>(P.solveSmall[t.x + warp], P, Lx, y, T, done, q, status, msm + 32 * kMQ * warp))
+        waitOk = 0;
+      __syncthreads();
+      return waitOk != 0;
+    }
     const int s = t.x, blk = t.y, below = t.z;
     const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s], mu = m - nc;
     const TL *Lp = Lx + P.snLxp[s];
@@ -254,6 +266,16 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_bwd_multi(const int4 *__re
   const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
   auto run = [&](const int tkv) -> bool {
     const int4 t = tasks[tkv];
+    if (t.z == 2) {  // up to kSolveGroup supernodes with m <= 32, one warp each (32 x 64 doubles of msm per warp)
+      const int warp = tid >> 5;
+      if (tid == 0) waitOk = 1;
+      __syncthreads();
+      if (warp < t.y && !small_bwd_warp_multi<TL>(P.solveSmall[t.x + warp], P, Lx, Dpiv, y, flags, epoch, q, status,
+                                                  msm + 32 * kMQ * warp))
+        waitOk = 0;
+      __syncthreads();
+      return waitOk != 0;
+    }
     const int s = t.x, blk = t.y;
     const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
     const TL *Lp = Lx + P.snLxp[s];

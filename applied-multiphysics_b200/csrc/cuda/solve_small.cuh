@@ -1,0 +1,221 @@
+// Solves of supernodes with m <= 32 by one warp each (solve tasks of kind 2), one right-hand side (lane = front row)
+// or several interleaved ones (lane = vector, the front vectors in shared memory). Forward: gather the front vector
+// (y rows of the pivot columns, the children's pass-up vectors in the reference's child order), eliminate column by
+// column (y_k = v_k / L(k, k), v_i -= L(i, k) y_k), write y and the pass-up vector and count the supernode done.
+// Backward: gather the rows below from the ancestors' final values, then x_k = (r_k - sum_{i > k} L(i, k) x_i) /
+// L(k, k) from the last column down (r = y, divided by D for LDL^T, whose stored L(k, k) is 1), and release the
+// supernode's block flag. Waits are bounded (status set on time-out).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "devplan.cuh"
+
+namespace amp {
+
+constexpr long long kSmallSpinLimit = 1ll << 24;
+
+__device__ __forceinline__ int sm_ld_acquire(const int *p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void sm_st_release(int *p, int v) {
+  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void sm_red_release_add(int *p, int v) {
+  asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// lane 0 waits (bounded) until *p == v (eq) or *p >= v; the result is broadcast to the warp
+__device__ __forceinline__ bool warp_wait(const int *p, int v, bool eq, unsigned long long *status, int s) {
+  int ok = 1;
+  if ((threadIdx.x & 31) == 0) {
+    long long spins = 0;
+    for (;;) {
+      const int cur = sm_ld_acquire(p);
+      if (eq ? cur == v : cur >= v) break;
+      if (++spins > kSmallSpinLimit) {
+        atomicMin(status, status_word(0x7fffffff, 3, s));
+        ok = 0;
+        break;
+      }
+      __nanosleep(32);
+    }
+  }
+  return __shfl_sync(0xffffffffu, ok, 0) != 0;
+}
+
+// children of s complete in the forward sweep (their pass-up vectors written)
+__device__ __forceinline__ bool warp_wait_children(const DevPlan &P, int s, const int *done,
+                                                   unsigned long long *status) {
+  for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
+    const int c = P.chList[qq];
+    const int need = (P.snM[c] - P.snNc[c] + 63) / 64;
+    if (!warp_wait(done + c, need, false, status, s)) return false;
+  }
+  return true;
+}
+
+// ---- one right-hand side --------------------------------------------------------------------------------------------
+// vs: the warp's 32 doubles of shared memory
+template <class TL>
+__device__ bool small_fwd_warp(int s, const DevPlan &P, const TL *__restrict__ Lx, double *__restrict__ y,
+                               double *__restrict__ T, int *done, unsigned long long *status, double *vs) {
+  const int lane = threadIdx.x & 31;
+  const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
+  if (!warp_wait_children(P, s, done, status)) return false;
+  vs[lane] = lane < nc ? y[f + lane] : 0.0;
+  __syncwarp();
+  for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
+    const int c = P.chList[qq];
+    const int muc = P.snM[c] - P.snNc[c];
+    const int *map = P.eaMap + P.eaPtr[c];
+    const double *tc = T + P.snTOff[c];
+    for (int a = lane; a < muc; a += 32) vs[map[a]] += __ldcg(tc + a);
+    __syncwarp();
+  }
+  double v = vs[lane];
+  const TL *Lp = Lx + P.snLxp[s];
+  double lk = lane < m ? (double)Lp[lane] : 0.0;  // column 0
+  for (int k = 0; k < nc; k++) {
+    const double ln = (k + 1 < nc && lane < m) ? (double)Lp[(int64_t)(k + 1) * m + lane] : 0.0;
+    const double yk = __shfl_sync(0xffffffffu, lane == k ? v / lk : 0.0, k);
+    if (lane == k)
+      v = yk;
+    else if (lane > k)
+      v -= lk * yk;
+    lk = ln;
+  }
+  if (lane < nc)
+    y[f + lane] = v;
+  else if (lane < m)
+    T[P.snTOff[s] + lane - nc] = v;
+  __syncwarp();  // orders the warp's stores before the counted arrival
+  if (lane == 0) sm_red_release_add(done + s, 1);
+  return true;
+}
+
+template <class TL>
+__device__ bool small_bwd_warp(int s, const DevPlan &P, const TL *__restrict__ Lx, const double *__restrict__ Dpiv,
+                               double *__restrict__ y, int *flags, int epoch, unsigned long long *status) {
+  const int lane = threadIdx.x & 31;
+  const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
+  const int par = P.snParent[s];
+  if (par >= 0 && m > nc && !warp_wait(flags + P.blkOff[par], epoch, true, status, s)) return false;
+  double x = 0.0;
+  if (lane >= nc && lane < m) {
+    x = __ldcg(y + P.Si[P.Sp[s] + lane]);
+  } else if (lane < nc) {
+    x = y[f + lane];
+    if (Dpiv) x = x / Dpiv[f + lane];  // LDL^T: y /= D before the backward sweep (ldlt.mjs:629)
+  }
+  const TL *Lp = Lx + P.snLxp[s];
+  for (int k = nc - 1; k >= 0; k--) {
+    const double lk = (lane >= k && lane < m) ? (double)Lp[(int64_t)k * m + lane] : 0.0;
+    double p = lane > k ? lk * x : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
+    if (lane == k) x = (x - p) / lk;
+  }
+  if (lane < nc) y[f + lane] = x;
+  __syncwarp();  // orders the warp's stores before the release
+  if (lane == 0) sm_st_release(flags + P.blkOff[s], epoch);
+  return true;
+}
+
+// ---- q interleaved right-hand sides (q <= 64; lane l holds vectors l and l + 32) -------------------------------------
+// Vs: the warp's 32 x 64 doubles of shared memory, row r of the front vectors at Vs[64 r + k]
+template <class TL>
+__device__ bool small_fwd_warp_multi(int s, const DevPlan &P, const TL *__restrict__ Lx, double *__restrict__ y,
+                                     double *__restrict__ T, int *done, int q, unsigned long long *status, double *Vs) {
+  const int lane = threadIdx.x & 31;
+  const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
+  const int k0 = lane, k1 = lane + 32;
+  const bool v0 = k0 < q, v1 = k1 < q;
+  if (!warp_wait_children(P, s, done, status)) return false;
+  for (int r = 0; r < m; r++) {
+    if (v0) Vs[64 * r + k0] = r < nc ? y[(int64_t)(f + r) * q + k0] : 0.0;
+    if (v1) Vs[64 * r + k1] = r < nc ? y[(int64_t)(f + r) * q + k1] : 0.0;
+  }
+  for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {  // each lane touches only its own vectors: no barrier
+    const int c = P.chList[qq];
+    const int muc = P.snM[c] - P.snNc[c];
+    const int *map = P.eaMap + P.eaPtr[c];
+    const double *tc = T + P.snTOff[c] * q;
+    for (int a = 0; a < muc; a++) {
+      const int r = map[a];
+      if (v0) Vs[64 * r + k0] += __ldcg(tc + (int64_t)a * q + k0);
+      if (v1) Vs[64 * r + k1] += __ldcg(tc + (int64_t)a * q + k1);
+    }
+  }
+  const TL *Lp = Lx + P.snLxp[s];
+  for (int k = 0; k < nc; k++) {
+    const TL *Lk = Lp + (int64_t)k * m;
+    const double lkk = (double)Lk[k];
+    const double y0 = v0 ? Vs[64 * k + k0] / lkk : 0.0, y1 = v1 ? Vs[64 * k + k1] / lkk : 0.0;
+    if (v0) Vs[64 * k + k0] = y0;
+    if (v1) Vs[64 * k + k1] = y1;
+    for (int r = k + 1; r < m; r++) {
+      const double l = (double)Lk[r];
+      if (v0) Vs[64 * r + k0] -= l * y0;
+      if (v1) Vs[64 * r + k1] -= l * y1;
+    }
+  }
+  for (int r = 0; r < m; r++) {
+    double *dst = r < nc ? y + (int64_t)(f + r) * q : T + (P.snTOff[s] + r - nc) * q;
+    if (v0) dst[k0] = Vs[64 * r + k0];
+    if (v1) dst[k1] = Vs[64 * r + k1];
+  }
+  __syncwarp();
+  if (lane == 0) sm_red_release_add(done + s, 1);
+  return true;
+}
+
+template <class TL>
+__device__ bool small_bwd_warp_multi(int s, const DevPlan &P, const TL *__restrict__ Lx,
+                                     const double *__restrict__ Dpiv, double *__restrict__ y, int *flags, int epoch,
+                                     int q, unsigned long long *status, double *Vs) {
+  const int lane = threadIdx.x & 31;
+  const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
+  const int k0 = lane, k1 = lane + 32;
+  const bool v0 = k0 < q, v1 = k1 < q;
+  const int par = P.snParent[s];
+  if (par >= 0 && m > nc && !warp_wait(flags + P.blkOff[par], epoch, true, status, s)) return false;
+  const int *rowsOf = P.Si + P.Sp[s];
+  for (int r = 0; r < m; r++) {
+    const int64_t gi = r < nc ? f + r : rowsOf[r];
+    const double d = (r < nc && Dpiv) ? Dpiv[f + r] : 1.0;
+    if (v0) {
+      const double xv = r < nc ? y[gi * q + k0] : __ldcg(y + gi * q + k0);
+      Vs[64 * r + k0] = (r < nc && Dpiv) ? xv / d : xv;
+    }
+    if (v1) {
+      const double xv = r < nc ? y[gi * q + k1] : __ldcg(y + gi * q + k1);
+      Vs[64 * r + k1] = (r < nc && Dpiv) ? xv / d : xv;
+    }
+  }
+  const TL *Lp = Lx + P.snLxp[s];
+  for (int k = nc - 1; k >= 0; k--) {
+    const TL *Lk = Lp + (int64_t)k * m;
+    double s0 = 0.0, s1 = 0.0;
+    for (int r = k + 1; r < m; r++) {
+      const double l = (double)Lk[r];
+      if (v0) s0 += l * Vs[64 * r + k0];
+      if (v1) s1 += l * Vs[64 * r + k1];
+    }
+    const double lkk = (double)Lk[k];
+    if (v0) Vs[64 * k + k0] = (Vs[64 * k + k0] - s0) / lkk;
+    if (v1) Vs[64 * k + k1] = (Vs[64 * k + k1] - s1) / lkk;
+  }
+  for (int r = 0; r < nc; r++) {
+    if (v0) y[(int64_t)(f + r) * q + k0] = Vs[64 * r + k0];
+    if (v1) y[(int64_t)(f + r) * q + k1] = Vs[64 * r + k1];
+  }
+  __syncwarp();
+  if (lane == 0) sm_st_release(flags + P.blkOff[s], epoch);
+  return true;
+}
+
+}  // namespace amp

@@ -194,10 +194,39 @@ void build_plan(const Symbolic &S, Plan &P) {
   P.asmLvlBytes.assign(P.nlevels, 0.0);
   P.uLvlPtr.assign(1, 0);
   P.lvlStepPtr.assign(P.nlevels + 1, 0);
+  P.tinyPtr.assign(1, 0);
+  P.smallPtr.assign(1, 0);
+  auto isSmall = [&](int s) { return P.snM[s] <= kSmallFront; };
   for (int L = 0; L < P.nlevels; L++) {
+    // small fronts: the whole front in one kernel; the rest go through the steps below
+    int maxM = 0;
+    double ff = 0, fb = 0;
+    for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
+      const int s = P.lvlSn[q];
+      if (!isSmall(s)) continue;
+      const double m = P.snM[s], nc = P.snNc[s], mu = m - nc;
+      ff += nc * nc * nc / 3.0 + nc * nc * mu + nc * mu * mu;
+      fb += 16.0 * (S.lowerP[P.snF[s] + P.snNc[s]] - S.lowerP[P.snF[s]]) + 8.0 * (m * nc + mu * (mu + 1) / 2);
+      for (int k = P.chPtr[s]; k < P.chPtr[s + 1]; k++) {
+        const double muc = P.snM[P.chList[k]] - P.snNc[P.chList[k]];
+        fb += 8.0 * muc * (muc + 1) / 2;
+      }
+      if (P.snM[s] <= kTinyFront) {
+        P.tinySn.push_back(s);
+      } else {
+        P.smallSn.push_back(s);
+        maxM = std::max(maxM, P.snM[s]);
+      }
+    }
+    P.tinyPtr.push_back((int64_t)P.tinySn.size());
+    P.smallPtr.push_back((int64_t)P.smallSn.size());
+    P.smallMaxM.push_back(maxM);
+    P.frontLvlFlops.push_back(ff);
+    P.frontLvlBytes.push_back(fb);
     int maxSteps = 0;
     for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
       int s = P.lvlSn[q];
+      if (isSmall(s)) continue;
       for (int j0 = 0; j0 < P.snM[s]; j0 += kAsmCols) P.asmTasks.push_back({s, j0});
       maxSteps = std::max(maxSteps, (P.snNc[s] + kPanel - 1) / kPanel);
       // bytes: value + lowerI + lowerSrc per A entry (16); read U + read/write the parent entry per child entry (24)
@@ -218,7 +247,7 @@ void build_plan(const Symbolic &S, Plan &P) {
       for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
         int s = P.lvlSn[q];
         const int nc = P.snNc[s], m = P.snM[s], c0 = k * kPanel;
-        if (c0 >= nc) continue;
+        if (c0 >= nc || isSmall(s)) continue;
         const int c1 = std::min(c0 + kPanel, nc);
         P.potrfTasks.push_back({s, c0});
         for (int r0 = c1; r0 < m; r0 += kTrsmRows) P.panelTasks.push_back({s, c0, r0, std::min(r0 + kTrsmRows, m)});
@@ -258,7 +287,7 @@ void build_plan(const Symbolic &S, Plan &P) {
     for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
       int s = P.lvlSn[q];
       const int nc = P.snNc[s], m = P.snM[s];
-      if (m <= nc) continue;
+      if (m <= nc || isSmall(s)) continue;
       const double mu = m - nc;
       uf += (double)nc * mu * (mu + 1);
       for (int j0 = nc; j0 < m; j0 += kTile)
@@ -297,23 +326,36 @@ void build_plan(const Symbolic &S, Plan &P) {
     v.push_back(c);
     v.push_back(0);
   };
+  // Supernodes with m <= kTinyFront are solved whole by one warp: tasks {first, count, 2} over solveSmall, up to
+  // kSolveGroup supernodes of one level per task, listed before the level's block tasks.
+  auto solveSmall = [&](int s) { return P.snM[s] <= kTinyFront; };
   for (int L = 0; L < P.nlevels; L++) {
+    const int64_t g0 = (int64_t)P.solveSmall.size();
+    for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++)
+      if (solveSmall(P.lvlSn[q])) P.solveSmall.push_back(P.lvlSn[q]);
+    const int64_t g1 = (int64_t)P.solveSmall.size();
+    for (int64_t g = g0; g < g1; g += kSolveGroup) {
+      push(P.fwdTasks, (int)g, (int)std::min<int64_t>(kSolveGroup, g1 - g), 2);
+      push(P.bwdTasks, (int)g, (int)std::min<int64_t>(kSolveGroup, g1 - g), 2);
+    }
     int maxNb = 0;
-    for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) maxNb = std::max(maxNb, (P.snNc[P.lvlSn[q]] + B - 1) / B);
+    for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++)
+      if (!solveSmall(P.lvlSn[q])) maxNb = std::max(maxNb, (P.snNc[P.lvlSn[q]] + B - 1) / B);
     for (int blk = 0; blk < maxNb; blk++)
       for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
         int s = P.lvlSn[q];
-        if (blk < (P.snNc[s] + B - 1) / B) push(P.fwdTasks, s, blk, 0);
+        if (!solveSmall(s) && blk < (P.snNc[s] + B - 1) / B) push(P.fwdTasks, s, blk, 0);
       }
     for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
       int s = P.lvlSn[q], mu = P.snM[s] - P.snNc[s];
+      if (solveSmall(s)) continue;
       for (int j = 0; j * B < mu; j++) push(P.fwdTasks, s, j, 1);
     }
     P.fwdLvlPtr[L + 1] = (int)(P.fwdTasks.size() / 4);
     for (int d = 0; d < maxNb; d++)
       for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
         int s = P.lvlSn[q], nb = (P.snNc[s] + B - 1) / B;
-        if (d < nb) push(P.bwdTasks, s, nb - 1 - d, 0);
+        if (!solveSmall(s) && d < nb) push(P.bwdTasks, s, nb - 1 - d, 0);
       }
     P.bwdLvlPtr[L + 1] = (int)(P.bwdTasks.size() / 4);
   }

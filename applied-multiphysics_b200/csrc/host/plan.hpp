@@ -23,7 +23,9 @@ constexpr int kTile = 64;      // trailing-update tile columns
 constexpr int kTileM = 128;    // trailing-update tile rows
 constexpr int kAsmCols = 32;   // front columns per assembly task
 constexpr int kTrsmRows = 64;  // panel rows per TRSM task
-constexpr int kSmallFront = 0; // fronts with m <= kSmallFront use the one-CTA-per-front kernel (0 = off)
+constexpr int kTinyFront = 32;    // fronts with m <= 32: one warp per front does the whole front (front_small.cu)
+constexpr int kSmallFront = 128;  // fronts with 32 < m <= 128: one CTA per front does the whole front
+constexpr int kSolveGroup = 4;    // supernodes with m <= kTinyFront per solve task (one warp each)
 
 struct PotrfTask {  // POTRF / LDL^T of the pivot block [c0, c0 + w) of supernode s, and its inverse
   int s, c0;
@@ -86,6 +88,11 @@ struct Plan {
   std::vector<int64_t> uLvlPtr;
   std::vector<double> uLvlFlops;
   std::vector<StepRange> steps;
+  // small fronts of each level, done whole by one warp (tiny) or one CTA (small) per front: tiny fronts of level L
+  // are tinySn[tinyPtr[L] .. tinyPtr[L + 1]), small ones smallSn[smallPtr[L] ..], the largest m of those smallMaxM[L]
+  std::vector<int> tinySn, smallSn, smallMaxM;
+  std::vector<int64_t> tinyPtr, smallPtr;
+  std::vector<double> frontLvlFlops, frontLvlBytes;  // algorithmic work of each level's small fronts
   // solve: rows below of each supernode (Si[Sp[s] + nc ..]) and the perm
   std::vector<int> perm, Sp, Si;
   int64_t solveBufDoubles = 0;      // sum of mu (per RHS) for the forward update vectors
@@ -96,6 +103,7 @@ struct Plan {
   std::vector<int64_t> invOff;      // per diagonal block (flag index): offset of its w x w inverse; [nflags] = total
   std::vector<int> diagSlot;        // CSR slot of each diagonal entry of A (LDL^T pivot scale)
   std::vector<int> fwdTasks, bwdTasks;  // int4 records, flattened
+  std::vector<int> solveSmall;          // supernodes solved whole by one warp, grouped by level (tasks of kind 2)
   std::vector<int> fwdLvlPtr, bwdLvlPtr;
   std::vector<int> bwdAll;  // backward tasks of all levels, top-down (one launch)
   double flops = 0;
