@@ -158,7 +158,9 @@ struct amp_factor_s {
   amp_plan *plan = nullptr;
   int kind = AMP_CHOLESKY, precision = AMP_FP64;
   cudaStream_t stream = nullptr;
+  cudaStream_t side = nullptr;                      // look-ahead: part B of the panel steps' updates
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t evPanel = nullptr, evSide = nullptr;  // look-ahead ordering between the two streams
   DevMem mem;
   double *dLx = nullptr, *dU = nullptr, *dD = nullptr, *dValues = nullptr;
   float *dL32 = nullptr, *dU32 = nullptr;           // mixed precision: FP32 factor and update arena
@@ -210,6 +212,9 @@ struct amp_factor_s {
     mem.release();
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    if (evPanel) cudaEventDestroy(evPanel);
+    if (evSide) cudaEventDestroy(evSide);
+    if (side) cudaStreamDestroy(side);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -296,17 +301,45 @@ cudaEvent_t pool_event(amp_factor *f) {
 
 // Run one launch; while profiling, bracket it with events and record its algorithmic work.
 template <class L>
-void timed(amp_factor *f, int kind, double flops, double bytes, L &&launch) {
+void timed_on(amp_factor *f, cudaStream_t st, int kind, double flops, double bytes, L &&launch) {
   if (!f->profiling) {
     launch();
     return;
   }
   amp_factor_s::Rec r{kind, pool_event(f), pool_event(f), flops, bytes};
-  ck(cudaEventRecord(r.a, f->stream), "event");
+  ck(cudaEventRecord(r.a, st), "event");
   launch();
-  ck(cudaEventRecord(r.b, f->stream), "event");
+  ck(cudaEventRecord(r.b, st), "event");
   f->recs.push_back(r);
 }
+template <class L>
+void timed(amp_factor *f, int kind, double flops, double bytes, L &&launch) {
+  timed_on(f, f->stream, kind, flops, bytes, launch);
+}
+
+// Look-ahead of the panel steps: part B of a step's update (the columns right of the next pivot block) runs on the
+// side stream while the factor's stream factors the next pivot block (part A of the update, POTRF, TRSM). Part A of
+// step k + 1 writes columns part B of step k also writes, so it waits for it; the level's update-block pass and
+// the next level wait for all of it. Inside the captured graph these waits are the graph's edges.
+struct LookAhead {
+  amp_factor *f;
+  bool pending = false;  // a part B was issued since the last join
+  void trsm_done() { ck(cudaEventRecord(f->evPanel, f->stream), "event"); }
+  void before_part_a() {
+    if (pending) ck(cudaStreamWaitEvent(f->stream, f->evSide, 0), "wait");
+  }
+  template <class L>
+  void part_b(int kind, double flops, L &&launch) {
+    ck(cudaStreamWaitEvent(f->side, f->evPanel, 0), "wait");
+    timed_on(f, f->side, kind, flops, 0.0, launch);
+    ck(cudaEventRecord(f->evSide, f->side), "event");
+    pending = true;
+  }
+  void join() {
+    if (pending) ck(cudaStreamWaitEvent(f->stream, f->evSide, 0), "wait");
+    pending = false;
+  }
+};
 
 // the small fronts of level L (whole fronts, one warp or one CTA each)
 template <class T>
@@ -340,6 +373,7 @@ void enqueue_factor(amp_factor *f) {
           amp::launch_assemble<float>(f->plan->dAsm + P.asmLvlPtr[L], P.asmLvlPtr[L + 1] - P.asmLvlPtr[L], dp,
                                       f->dValues, f->dL32, f->dU32, f->dStatus, st);
         });
+      LookAhead la{f};
       for (int k = P.lvlStepPtr[L]; k < P.lvlStepPtr[L + 1]; k++) {
         const amp::StepRange &sr = P.steps[k];
         timed(f, K_POTRF, sr.potrfFlops, 0.0, [&] {
@@ -351,13 +385,20 @@ void enqueue_factor(amp_factor *f) {
             amp::launch_trsm<float>(f->plan->dPanel + sr.panel0, sr.panel1 - sr.panel0, dp, f->dL32, f->dStatus,
                                     f->dShi, f->dSlo, ld32, st);
           });
-        const int64_t t0 = P.mixStepPtr[k], t1 = P.mixStepPtr[k + 1];
-        if (t1 > t0)
-          timed(f, K_UPDATE, sr.updateFlops, 0.0, [&] {
-            amp::launch_update_mx(f->plan->dMixTile + t0, t1 - t0, f->dMaps, f->dL32, f->dU32, f->dStatus,
-                                  amp::num_sms(), st);
+        la.trsm_done();
+        la.before_part_a();
+        if (sr.mixMid > sr.mix0)
+          timed(f, K_UPDATE, sr.updateFlopsA, 0.0, [&] {
+            amp::launch_update_mx(f->plan->dMixTile + sr.mix0, sr.mixMid - sr.mix0, f->dMaps, f->dL32, f->dU32,
+                                  f->dStatus, amp::num_sms(), st);
+          });
+        if (sr.mix1 > sr.mixMid)
+          la.part_b(K_UPDATE, sr.updateFlopsB, [&] {
+            amp::launch_update_mx(f->plan->dMixTile + sr.mixMid, sr.mix1 - sr.mixMid, f->dMaps, f->dL32, f->dU32,
+                                  f->dStatus, amp::num_sms(), f->side);
           });
       }
+      la.join();
       const int64_t u0 = P.mixULvlPtr[L], u1 = P.mixULvlPtr[L + 1];
       if (u1 > u0)
         timed(f, K_UPDATE, P.uLvlFlops[L], 0.0, [&] {
@@ -384,6 +425,7 @@ void enqueue_factor(amp_factor *f) {
         amp::launch_assemble<double>(f->plan->dAsm + P.asmLvlPtr[L], P.asmLvlPtr[L + 1] - P.asmLvlPtr[L], dp,
                                      f->dValues, f->dLx, f->dU, f->dStatus, st);
       });
+    LookAhead la{f};
     for (int k = P.lvlStepPtr[L]; k < P.lvlStepPtr[L + 1]; k++) {
       const amp::StepRange &sr = P.steps[k];
       timed(f, K_POTRF, sr.potrfFlops, 0.0, [&] {
@@ -394,12 +436,20 @@ void enqueue_factor(amp_factor *f) {
           amp::launch_trsm<double>(f->plan->dPanel + sr.panel0, sr.panel1 - sr.panel0, dp, f->dLx, f->dStatus, nullptr,
                                    nullptr, ld, st);
         });
-      if (sr.tile1 > sr.tile0)
-        timed(f, K_UPDATE, sr.updateFlops, 0.0, [&] {
-          amp::launch_update(f->plan->dTile + sr.tile0, sr.tile1 - sr.tile0, dp, f->dLx, f->dU, ld.W, f->dStatus,
+      la.trsm_done();
+      la.before_part_a();
+      if (sr.tileMid > sr.tile0)
+        timed(f, K_UPDATE, sr.updateFlopsA, 0.0, [&] {
+          amp::launch_update(f->plan->dTile + sr.tile0, sr.tileMid - sr.tile0, dp, f->dLx, f->dU, ld.W, f->dStatus,
                              st);
         });
+      if (sr.tile1 > sr.tileMid)
+        la.part_b(K_UPDATE, sr.updateFlopsB, [&] {
+          amp::launch_update(f->plan->dTile + sr.tileMid, sr.tile1 - sr.tileMid, dp, f->dLx, f->dU, ld.W, f->dStatus,
+                             f->side);
+        });
     }
+    la.join();
     if (P.uLvlPtr[L + 1] > P.uLvlPtr[L])
       timed(f, K_UPDATE, P.uLvlFlops[L], 0.0, [&] {
         amp::launch_update(f->plan->dUTile + P.uLvlPtr[L], P.uLvlPtr[L + 1] - P.uLvlPtr[L], dp, f->dLx, f->dU, ld.W,
@@ -767,6 +817,9 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
     f->precision = o.precision;
     try {
       ck(cudaStreamCreateWithFlags(&f->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+      ck(cudaStreamCreateWithFlags(&f->side, cudaStreamNonBlocking), "cudaStreamCreate");
+      ck(cudaEventCreateWithFlags(&f->evPanel, cudaEventDisableTiming), "cudaEventCreate");
+      ck(cudaEventCreateWithFlags(&f->evSide, cudaEventDisableTiming), "cudaEventCreate");
       ck(cudaEventCreate(&f->ev0), "cudaEventCreate");
       ck(cudaEventCreate(&f->ev1), "cudaEventCreate");
       const amp::Plan &P = pl->P;

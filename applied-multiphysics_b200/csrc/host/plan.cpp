@@ -187,7 +187,6 @@ void build_plan(const Symbolic &S, Plan &P) {
         out.push_back({(long long)P.snLxp[s], (long long)P.snUoff[s], (long long)P.snSp[s], m, nc, (m + 7) & ~7, kc0,
                        kw, i0, j0, rlo, clo, chi, s});
   };
-  P.mixStepPtr.assign(1, 0);
   P.mixULvlPtr.assign(1, 0);
   // task lists per level
   P.asmLvlPtr.assign(P.nlevels + 1, 0);
@@ -240,10 +239,18 @@ void build_plan(const Symbolic &S, Plan &P) {
     P.asmLvlPtr[L + 1] = (int64_t)P.asmTasks.size();
     for (int k = 0; k < maxSteps; k++) {
       StepRange sr;
-      sr.potrfFlops = sr.panelFlops = sr.updateFlops = 0;
+      sr.potrfFlops = sr.panelFlops = sr.updateFlopsA = sr.updateFlopsB = 0;
       sr.potrf0 = (int64_t)P.potrfTasks.size();
       sr.panel0 = (int64_t)P.panelTasks.size();
-      sr.tile0 = (int64_t)P.tileTasks.size();
+      // Pivot blocks are grouped by kGroup: after block b of group [g0, g1) only the group's remaining columns are
+      // updated (narrow, K = 64); after the group's last block the pivot columns right of the group receive the whole
+      // group at once (wide, K = g1 - g0). The update block waits for the long-K pass after the level. Each step's
+      // update region [lo, hi) is split into its first 64 columns (the next pivot block: part A, which the next step's
+      // POTRF waits for) and the rest (part B, which may run while the next pivot block is factored).
+      struct Region {
+        int s, lo, hi, kc0, kw;
+      };
+      std::vector<Region> regions;
       for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
         int s = P.lvlSn[q];
         const int nc = P.snNc[s], m = P.snM[s], c0 = k * kPanel;
@@ -251,35 +258,37 @@ void build_plan(const Symbolic &S, Plan &P) {
         const int c1 = std::min(c0 + kPanel, nc);
         P.potrfTasks.push_back({s, c0});
         for (int r0 = c1; r0 < m; r0 += kTrsmRows) P.panelTasks.push_back({s, c0, r0, std::min(r0 + kTrsmRows, m)});
-        // Pivot blocks are grouped by kGroup: after block b of group [g0, g1) only the group's remaining columns are
-        // updated (narrow, K = 64); after the group's last block the pivot columns right of the group receive the
-        // whole group at once (wide, K = g1 - g0). The update block waits for the long-K pass after the level.
         const int g0 = (c0 / (kGroup * kPanel)) * (kGroup * kPanel), g1 = std::min(nc, g0 + kGroup * kPanel);
         const double w = c1 - c0, r = m - c1;
         sr.potrfFlops += w * w * w / 3.0;
         sr.panelFlops += r * w * w;  // TRSM
-        auto trap = [m](double a, double b) { return (b - a) * m - (a + b - 1) * (b - a) / 2; };  // lower entries
         if (c1 < g1)
-          emitMix(P.mixTiles, s, c1, c1, g1, c0, c1 - c0);
+          regions.push_back({s, c1, g1, c0, c1 - c0});
         else if (g1 < nc)
-          emitMix(P.mixTiles, s, g1, g1, nc, g0, g1 - g0);
-        if (c1 < g1) {
-          sr.updateFlops += 2 * w * trap(c1, g1);
-          for (int j0 = c1; j0 < g1; j0 += kTile)
-            for (int i0 = c1 + ((j0 - c1) / kTileM) * kTileM; i0 < m; i0 += kTileM)
-              P.tileTasks.push_back({(long long)P.snLxp[s], (long long)P.snUoff[s], m, nc, c0, c1 - c0, i0, j0, g1, 0});
-        } else if (g1 < nc) {
-          sr.updateFlops += 2.0 * (g1 - g0) * trap(g1, nc);
-          for (int j0 = g1; j0 < nc; j0 += kTile)
-            for (int i0 = g1 + ((j0 - g1) / kTileM) * kTileM; i0 < m; i0 += kTileM)
-              P.tileTasks.push_back({(long long)P.snLxp[s], (long long)P.snUoff[s], m, nc, g0, g1 - g0, i0, j0, nc, 0});
-        }
+          regions.push_back({s, g1, nc, g0, g1 - g0});
       }
+      // lower entries of columns [a, b) of an m-row front
+      auto trap = [](double m, double a, double b) { return (b - a) * m - (a + b - 1) * (b - a) / 2; };
+      auto emit = [&](const Region &g, int lo, int hi, double &flops) {
+        if (lo >= hi) return;
+        const int m = P.snM[g.s], nc = P.snNc[g.s];
+        flops += 2.0 * g.kw * trap(m, lo, hi);
+        emitMix(P.mixTiles, g.s, lo, lo, hi, g.kc0, g.kw);
+        for (int j0 = lo; j0 < hi; j0 += kTile)
+          for (int i0 = lo + ((j0 - lo) / kTileM) * kTileM; i0 < m; i0 += kTileM)
+            P.tileTasks.push_back({(long long)P.snLxp[g.s], (long long)P.snUoff[g.s], m, nc, g.kc0, g.kw, i0, j0, hi, 0});
+      };
+      sr.tile0 = (int64_t)P.tileTasks.size();
+      sr.mix0 = (int64_t)P.mixTiles.size();
+      for (const Region &g : regions) emit(g, g.lo, std::min(g.lo + kPanel, g.hi), sr.updateFlopsA);
+      sr.tileMid = (int64_t)P.tileTasks.size();
+      sr.mixMid = (int64_t)P.mixTiles.size();
+      for (const Region &g : regions) emit(g, g.lo + kPanel, g.hi, sr.updateFlopsB);
       sr.potrf1 = (int64_t)P.potrfTasks.size();
       sr.panel1 = (int64_t)P.panelTasks.size();
       sr.tile1 = (int64_t)P.tileTasks.size();
+      sr.mix1 = (int64_t)P.mixTiles.size();
       P.steps.push_back(sr);
-      P.mixStepPtr.push_back((int64_t)P.mixTiles.size());
     }
     P.lvlStepPtr[L + 1] = (int)P.steps.size();
     // update blocks of the level's fronts: one long-K pass each

@@ -21,7 +21,7 @@ constexpr int kPanel = 64;     // pivot block width of the dense partial factori
 constexpr int kGroup = 4;      // pivot blocks whose update of the columns right of them is applied together
 constexpr int kTile = 64;      // trailing-update tile columns
 constexpr int kTileM = 128;    // trailing-update tile rows
-constexpr int kAsmCols = 32;   // front columns per assembly task
+constexpr int kAsmCols = 8;    // front columns per assembly task (one per warp)
 constexpr int kTrsmRows = 64;  // panel rows per TRSM task
 constexpr int kTinyFront = 32;    // fronts with m <= 32: one warp per front does the whole front (front_small.cu)
 constexpr int kSmallFront = 128;  // fronts with 32 < m <= 128: one CTA per front does the whole front
@@ -49,8 +49,10 @@ struct AsmTask {  // zero + assemble + extend-add front columns [j0, j0 + 32) of
 };
 
 struct StepRange {
-  int64_t potrf0, potrf1, panel0, panel1, tile0, tile1;
-  double potrfFlops, panelFlops, updateFlops;  // algorithmic flops of the step's launches
+  int64_t potrf0, potrf1, panel0, panel1;
+  int64_t tile0, tileMid, tile1;  // FP64 update tiles: part A [tile0, tileMid), part B [tileMid, tile1)
+  int64_t mix0, mixMid, mix1;     // the same for the mixed-precision tiles
+  double potrfFlops, panelFlops, updateFlopsA, updateFlopsB;  // algorithmic flops of the step's launches
 };
 // The update block of every front receives its whole Schur update once, after the panel steps of its level:
 // U -= L21 L21^T with K = nc (tiles over the lower triangle of [nc, m)^2).
@@ -82,7 +84,7 @@ struct Plan {
   std::vector<TileTask> uTasks;  // long-K update-block tiles, per level [uLvlPtr[L], uLvlPtr[L+1])
   // mixed precision: the same steps with 128 x 256 tiles; BF16 split storage of the pivot columns
   std::vector<MixTask> mixTiles, mixUTasks;
-  std::vector<int64_t> mixStepPtr, mixULvlPtr;  // per step / per level
+  std::vector<int64_t> mixULvlPtr;  // per level
   std::vector<int64_t> snSp;  // split-column offset of supernode s (ld = round_up(m, 8) per front)
   int64_t splitElems = 0;
   std::vector<int64_t> uLvlPtr;
