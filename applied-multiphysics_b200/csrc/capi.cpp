@@ -88,6 +88,9 @@ void set_last_error(const std::string &msg) { g_err = msg; }
 
 namespace {
 // elements of the diagonal-block inverses (none for an empty pattern, whose plan has no per-block arrays)
+// chain-matrix slots: nb - 1 per supernode with nb diagonal blocks, 64 x 64 each
+size_t chain_elems(const amp::Plan &P) { return (size_t)std::max(0, P.nflags - P.nsuper) * 64 * 64; }
+
 int64_t inv_elems(const amp::Plan &P) { return P.invOff.empty() ? 0 : P.invOff[P.nflags]; }
 
 // TMA descriptors of the BF16 split columns, two per supernode that has mixed-precision update tiles (hi, lo): the
@@ -148,6 +151,7 @@ struct amp_plan_s {
   amp::MixTask *dMixTile = nullptr, *dMixU = nullptr;
   int4 *dFwdTasks = nullptr, *dBwdTasks = nullptr, *dBwdAll = nullptr;
   int *dTinySn = nullptr, *dSmallSn = nullptr;  // small fronts per level (whole fronts by one warp / one CTA)
+  int2 *dChain = nullptr;                        // chain-matrix tasks {s, b}
   int *dRowptr = nullptr, *dColidx = nullptr;
   std::vector<int> rowptr, colidx;  // host copy of the pattern (uploaded with the schedule)
   bool uploaded = false;
@@ -169,6 +173,8 @@ struct amp_factor_s {
   int *dCounts = nullptr;                           // LDL^T: nNeg, nPerturbed
   double *dInv = nullptr;                           // inverses of the 64-column diagonal blocks (FP64 factor)
   float *dInv32 = nullptr;                          // the same for the FP32 factor
+  double *dMch = nullptr, *dGch = nullptr;          // chain matrices of consecutive diagonal blocks (FP64 factor)
+  float *dMch32 = nullptr, *dGch32 = nullptr;       // the same for the FP32 factor
   __nv_bfloat16 *dShi = nullptr, *dSlo = nullptr;   // BF16 split columns of the factored pivot blocks
   __nv_bfloat16 *dWhi = nullptr, *dWlo = nullptr;   // mixed LDL^T: BF16 split of L21 D
   CUtensorMap *dMaps = nullptr;                     // per supernode: TMA descriptors of the split A and B operands
@@ -264,6 +270,7 @@ void upload_plan(amp_plan *pl) {
   pl->dBwdAll = (int4 *)m.upload(P.bwdAll);
   pl->dTinySn = m.upload(P.tinySn);
   pl->dSmallSn = m.upload(P.smallSn);
+  pl->dChain = (int2 *)m.upload(P.chainTasks);
 }
 
 void ensure_solve_ws(amp_factor *f, int q) {
@@ -284,11 +291,11 @@ void ensure_solve_ws(amp_factor *f, int q) {
 
 enum KernelKind {
   K_ASSEMBLE, K_PANEL, K_UPDATE, K_FORWARD, K_BACKWARD, K_PERMUTE, K_RESIDUAL, K_POTRF, K_DIAGINV, K_KRYLOV,
-  K_FRONTS, K_NKINDS
+  K_FRONTS, K_CHAIN, K_NKINDS
 };
 const char *kKindNames[K_NKINDS] = {"assemble",      "panel_trsm", "update_syrk", "solve_forward",
                                     "solve_backward", "permute",    "residual_spmv", "potrf",
-                                    "diag_inverse",  "krylov",     "small_fronts"};
+                                    "diag_inverse",  "krylov",     "small_fronts", "chain_mats"};
 
 cudaEvent_t pool_event(amp_factor *f) {
   if (f->evUsed == f->evPool.size()) {
@@ -354,6 +361,17 @@ void enqueue_small_fronts(amp_factor *f, int L, T *Lx, T *U, const amp::LdltArgs
   });
 }
 
+// chain matrices of consecutive diagonal blocks for the one-vector sweeps (after the inverses)
+template <class T>
+void enqueue_chain_mats(amp_factor *f, const T *Lx, const T *Inv, T *Mch, T *Gch) {
+  const amp::Plan &P = f->plan->P;
+  const int nt = (int)(P.chainTasks.size() / 2);
+  if (nt == 0 || f->kind == AMP_LDLT) return;  // LDL^T sweeps apply the inverse blocks last
+  timed(f, K_CHAIN, 2.0 * 2.0 * 64.0 * 64.0 * 64.0 / 2.0 * nt, 3.0 * 64.0 * 64.0 * sizeof(T) * nt, [&] {
+    amp::launch_chain_mats<T>(f->plan->dChain, nt, f->plan->dp, Lx, Inv, Mch, Gch, f->stream);
+  });
+}
+
 void enqueue_factor(amp_factor *f) {
   const amp::Plan &P = f->plan->P;
   const amp::DevPlan &dp = f->plan->dp;
@@ -409,6 +427,7 @@ void enqueue_factor(amp_factor *f) {
     if (P.nflags)
       timed(f, K_DIAGINV, 0.0, 8.0 * (double)inv_elems(P),
             [&] { amp::launch_diag_inv<float>(dp, P.nflags, f->dL32, f->dInv32, st); });
+    enqueue_chain_mats<float>(f, f->dL32, f->dInv32, f->dMch32, f->dGch32);
     return;
   }
   const bool ldlt = f->kind == AMP_LDLT;
@@ -459,13 +478,13 @@ void enqueue_factor(amp_factor *f) {
   if (P.nflags)
     timed(f, K_DIAGINV, 0.0, 16.0 * (double)inv_elems(P),
           [&] { amp::launch_diag_inv<double>(dp, P.nflags, f->dLx, f->dInv, st); });
+  enqueue_chain_mats<double>(f, f->dLx, f->dInv, f->dMch, f->dGch);
 }
 
 // y (permuted order, q vectors) := A^-1 y in place
 void device_solve_permuted(amp_factor *f) {
   const amp::Plan &P = f->plan->P;
   const amp::DevPlan &dp = f->plan->dp;
-  const int64_t Vs = P.nsuper ? P.Sp[P.nsuper] : 0, Ts = P.solveBufDoubles;
   const double lbytes = (f->dL32 ? 4.0 : 8.0) * (double)P.nnzLStored;  // each sweep reads L once
   cudaStream_t st = f->stream;
   ck(cudaMemsetAsync(f->dTickets, 0, sizeof(int) * 2, st), "memset tickets");
@@ -473,22 +492,24 @@ void device_solve_permuted(amp_factor *f) {
   ck(cudaMemsetAsync(f->dSolveStatus, 0xff, sizeof(unsigned long long), st), "memset status");
   const int efwd = 2 * (++f->solveEpoch) - 1, ebwd = 2 * f->solveEpoch;
   const int nf = P.fwdLvlPtr[P.nlevels], nb = (int)(P.bwdAll.size() / 4);
-  const double *Dp = f->kind == AMP_LDLT ? f->dD : nullptr;
+  const bool ldlt = f->kind == AMP_LDLT;
+  const double *Dp = ldlt ? f->dD : nullptr;
   timed(f, K_FORWARD, 2.0 * (double)P.nnzLStored, lbytes, [&] {
     if (f->dL32)
-      amp::launch_fwd_blocks<float>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->dL32, f->dInv32, f->dY, f->dV, f->dT,
-                                    f->dFlags, efwd, f->dDone, 1, Vs, Ts, f->dSolveStatus, st);
+      amp::launch_fwd_blocks<float>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->dL32, f->dInv32,
+                                    ldlt ? nullptr : f->dMch32, f->dY, f->dT, f->dFlags, efwd, f->dDone,
+                                    f->dSolveStatus, st);
     else
-      amp::launch_fwd_blocks<double>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->dLx, f->dInv, f->dY, f->dV, f->dT,
-                                     f->dFlags, efwd, f->dDone, 1, Vs, Ts, f->dSolveStatus, st);
+      amp::launch_fwd_blocks<double>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->dLx, f->dInv, ldlt ? nullptr : f->dMch,
+                                     f->dY, f->dT, f->dFlags, efwd, f->dDone, f->dSolveStatus, st);
   });
   timed(f, K_BACKWARD, 2.0 * (double)P.nnzLStored, lbytes, [&] {
     if (f->dL32)
-      amp::launch_bwd_blocks<float>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dL32, f->dInv32, Dp, f->dY,
-                                    f->dFlags, ebwd, 1, f->dSolveStatus, st);
+      amp::launch_bwd_blocks<float>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dL32, f->dInv32,
+                                    ldlt ? nullptr : f->dGch32, Dp, f->dY, f->dFlags, ebwd, f->dSolveStatus, st);
     else
-      amp::launch_bwd_blocks<double>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dLx, f->dInv, Dp, f->dY, f->dFlags,
-                                     ebwd, 1, f->dSolveStatus, st);
+      amp::launch_bwd_blocks<double>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dLx, f->dInv,
+                                     ldlt ? nullptr : f->dGch, Dp, f->dY, f->dFlags, ebwd, f->dSolveStatus, st);
   });
 }
 
@@ -827,6 +848,8 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
         f->dLx = f->mem.alloc<double>((size_t)P.nnzLStored);
         f->dU = f->mem.alloc<double>((size_t)P.arenaDoubles);
         f->dInv = f->mem.alloc<double>((size_t)inv_elems(P));
+        f->dMch = f->mem.alloc<double>(chain_elems(P));
+        f->dGch = f->mem.alloc<double>(chain_elems(P));
         if (o.kind == AMP_LDLT) {
           f->dW = f->mem.alloc<double>((size_t)P.nnzLStored);
           f->dScal = f->mem.alloc<double>(2);
@@ -836,6 +859,8 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
         f->dL32 = f->mem.alloc<float>((size_t)P.nnzLStored);
         f->dU32 = f->mem.alloc<float>((size_t)P.arenaDoubles);
         f->dInv32 = f->mem.alloc<float>((size_t)inv_elems(P));
+        f->dMch32 = f->mem.alloc<float>(chain_elems(P));
+        f->dGch32 = f->mem.alloc<float>(chain_elems(P));
         f->dShi = f->mem.alloc<__nv_bfloat16>((size_t)P.splitElems);
         f->dSlo = f->mem.alloc<__nv_bfloat16>((size_t)P.splitElems);
         if (o.kind == AMP_LDLT) {

@@ -40,11 +40,15 @@ template <class TL>
 void launch_diag_inv(const DevPlan &P, int nblocks, const TL *Lx, TL *Inv, cudaStream_t st);
 template <class TL>
 void launch_fwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
-                       double *y, double *V, double *T, int *flags, int epoch, int *done, int q, int64_t Vstride,
-                       int64_t Tstride, unsigned long long *status, cudaStream_t st);
+                       const TL *Mch, double *y, double *T, int *flags, int epoch, int *done,
+                       unsigned long long *status, cudaStream_t st);
 template <class TL>
 void launch_bwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
-                       const double *Dpiv, double *y, int *flags, int epoch, int q, unsigned long long *status,
+                       const TL *Gch, const double *Dpiv, double *y, int *flags, int epoch, unsigned long long *status,
+                       cudaStream_t st);
+// M_b = X_b L[b, b-1] and G_b = L[b+1, b] X_b of consecutive diagonal blocks (tasks {s, b}), after launch_diag_inv
+template <class TL>
+void launch_chain_mats(const int2 *tasks, int ntasks, const DevPlan &P, const TL *Lx, const TL *Inv, TL *Mch, TL *Gch,
                        cudaStream_t st);
 
 // several right-hand sides (q <= multi_max_vectors(), interleaved: entry i of vector k at [i q + k])

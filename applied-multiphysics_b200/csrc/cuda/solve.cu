@@ -105,24 +105,83 @@ __global__ void __launch_bounds__(kSB) k_diag_inv(DevPlan P, const TL *__restric
   }
 }
 
+// ---- chain matrices ----------------------------------------------------------------------------------------------
+// For consecutive 64-column diagonal blocks b - 1, b of a supernode (after the factorization, after k_diag_inv):
+//   M_b = X_b L[b, b-1]   (w_b x 64): forward  y_b = X_b (v_b - P_b) - M_b y_{b-1}
+//   G_b = L[b+1, b] X_b   (w_{b+1} x w_b): backward x_b = X_b^T (r_b - Q_b) - G_b^T x_{b+1}
+// with P_b / Q_b the contributions of all other blocks, so that only one 64 x 64 product waits for the neighbouring
+// block. Slots: supernode s's block b uses M slot blkOff[s] - s + b - 1 and G slot blkOff[s] - s + b (64 x 64,
+// column-major), since a supernode with nb blocks has nb - 1 of each.
+constexpr int kChainSmem = 2 * kSB * (kSB + 1) * (int)sizeof(double);
+template <class TL>
+__global__ void __launch_bounds__(256) k_chain_mats(const int2 *__restrict__ tasks, DevPlan P, const TL *__restrict__ Lx,
+                                                    const TL *__restrict__ Inv, TL *__restrict__ Mch,
+                                                    TL *__restrict__ Gch) {
+  extern __shared__ double ch_dyn[];
+  double(*Xs)[kSB + 1] = reinterpret_cast<double(*)[kSB + 1]>(ch_dyn);
+  double(*Lt)[kSB + 1] = reinterpret_cast<double(*)[kSB + 1]>(ch_dyn + kSB * (kSB + 1));
+  const int2 t = tasks[blockIdx.x];
+  const int s = t.x, b = t.y;
+  const int nc = P.snNc[s], m = P.snM[s], nb = (nc + kSB - 1) / kSB;
+  const int c0 = b * kSB, w = min(kSB, nc - c0);
+  const TL *Lp = Lx + P.snLxp[s];
+  const TL *X = Inv + P.invOff[P.blkOff[s] + b];
+  const int tid = threadIdx.x, i = tid & (kSB - 1), cg = tid >> 6;
+  for (int e = tid; e < kSB * kSB; e += blockDim.x) {
+    const int r = e & (kSB - 1), c = e >> 6;
+    Xs[r][c] = (r < w && c < w) ? (double)X[c * w + r] : 0.0;  // X(r, c), lower
+  }
+  const int slotBase = P.blkOff[s] - s;
+  if (b >= 1) {  // M(i, c) = sum_{j <= i} X(i, j) L(c0 + j, c0 - 64 + c)
+    for (int e = tid; e < kSB * kSB; e += blockDim.x) {
+      const int j = e & (kSB - 1), c = e >> 6;
+      Lt[j][c] = j < w ? (double)Lp[(int64_t)(c0 - kSB + c) * m + c0 + j] : 0.0;
+    }
+    __syncthreads();
+    TL *M = Mch + (int64_t)(slotBase + b - 1) * kSB * kSB;
+    for (int u = 0; u < 16; u++) {
+      const int c = cg * 16 + u;
+      double a = 0.0;
+      for (int j = 0; j <= i && j < w; j++) a += Xs[i][j] * Lt[j][c];
+      M[c * kSB + i] = (TL)a;
+    }
+    __syncthreads();
+  }
+  if (b + 1 < nb) {  // G(r, c) = sum_{j >= c} L(c0 + 64 + r, c0 + j) X(j, c)
+    const int wn = min(kSB, nc - c0 - kSB);
+    for (int e = tid; e < kSB * kSB; e += blockDim.x) {
+      const int r = e & (kSB - 1), j = e >> 6;
+      Lt[r][j] = (r < wn && j < w) ? (double)Lp[(int64_t)(c0 + j) * m + c0 + kSB + r] : 0.0;
+    }
+    __syncthreads();
+    TL *G = Gch + (int64_t)(slotBase + b) * kSB * kSB;
+    for (int u = 0; u < 16; u++) {
+      const int c = cg * 16 + u;
+      double a = 0.0;
+      for (int j = c; j < w; j++) a += Lt[i][j] * Xs[j][c];
+      G[c * kSB + i] = (TL)a;
+    }
+  }
+}
+
 // ---- forward block tasks -----------------------------------------------------------------------------------------
-// task: .x supernode, .y block, .z kind (0 diagonal, 1 below)
-// One launch for the whole sweep: tasks are listed level by level (leaves first), so every wait below is on a task
-// with an earlier ticket. The first diagonal task of a supernode waits for its children's pass-up vectors (their
-// below tasks count themselves in done[]) and gathers its front vector; every below task counts itself when its
-// part of the pass-up vector is written.
+// task: .x supernode, .y block, .z kind (0 diagonal, 1 below, 2 small supernodes)
+// One launch for the whole sweep: tasks are listed level by level (leaves first), so every wait is on a task with an
+// earlier ticket. Every task first waits for the supernode's children and gathers its own rows of the front vector
+// v_s = [y(f .. f + nc); 0] + the children's pass-up vectors (in the reference's child order). A below task forms its
+// part of the pass-up vector u_j = v_j - L[j, 0:nc] y and counts itself in done[s]; diagonal task b forms
+// w_b = X_b (v_b - L[b, 0:(b-1) 64] y) while the earlier blocks finish, then waits for block b - 1 alone:
+// y_b = w_b - M_b y_{b-1}.
 template <class TL>
 __global__ void __launch_bounds__(256, 3) k_fwd_blocks(const int4 *__restrict__ tasks, int ntasks, int *__restrict__ ticket,
                                                     DevPlan P, const TL *__restrict__ Lx, const TL *__restrict__ Inv,
-                                                    double *__restrict__ y, double *__restrict__ V,
+                                                    const TL *__restrict__ Mch, double *__restrict__ y,
                                                     double *__restrict__ T, int *__restrict__ flags, int epoch,
-                                                    int *__restrict__ done, int q, int64_t Vstride, int64_t Tstride,
-                                                    unsigned long long *status) {
+                                                    int *__restrict__ done, unsigned long long *status) {
   __shared__ int tk, waitOk;
   __shared__ double red[4][kSB];
   __shared__ double rk[kSB];
   __shared__ double Xs[kSB][kSB + 1];
-  // persistent: take tickets until the list is exhausted (a task only waits for earlier tickets)
   auto run = [&](const int tkv) -> bool {
     const int4 t = tasks[tkv];
     if (t.z == 2) {  // up to kSolveGroup supernodes with m <= 32, one warp each
@@ -139,55 +198,56 @@ __global__ void __launch_bounds__(256, 3) k_fwd_blocks(const int4 *__restrict__ 
     const TL *Lp = Lx + P.snLxp[s];
     const int r0 = below ? nc + blk * kSB : blk * kSB;
     const int rows = below ? min(kSB, mu - blk * kSB) : min(kSB, nc - blk * kSB);
-    const int ncols = below ? nc : blk * kSB;  // columns of L to the left of the diagonal block / all pivot columns
+    // with chain matrices (Cholesky) the diagonal task sums blocks 0 .. b - 2 before its last wait and applies M_b to
+    // block b - 1; without them (LDL^T, whose inverse blocks can be large) it sums all blocks before b and applies X_b
+    // last, as the reference's substitution does
+    const bool chain = Mch != nullptr;
+    const int ncols = below ? nc : max(0, chain ? blk - 1 : blk) * kSB;  // columns summed before the last product
     const int tid = threadIdx.x, row = tid & (kSB - 1), part = tid >> 6;
     const bool rowok = row < rows;
     int *myflags = flags + P.blkOff[s];
-    if (!below) {  // inverse of the diagonal block, needed at the end
+    if (!below) {
       const TL *X = Inv + P.invOff[P.blkOff[s] + blk];
       for (int e = tid; e < rows * rows; e += blockDim.x) Xs[e % rows][e / rows] = (double)X[e];
     }
-    if (!below && blk == 0) {
-      // children's pass-up vectors complete?
-      for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
-        const int c = P.chList[qq];
-        const int need = (P.snM[c] - P.snNc[c] + kSB - 1) / kSB;
-        if (tid == 0) waitOk = wait_count(done + c, need, status, s);
-        __syncthreads();
-        if (!waitOk) return false;
-      }
-      // gather v_s = [y(f .. f + nc); 0] + children's pass-up vectors (the reference's child order)
-      for (int k = 0; k < q; k++) {
-        double *v = V + (int64_t)k * Vstride + P.Sp[s];
-        const double *yk = y + (int64_t)k * P.n;
-        for (int r = tid; r < m; r += blockDim.x) v[r] = r < nc ? yk[f + r] : 0.0;
-      }
+    // children complete?
+    for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
+      const int c = P.chList[qq];
+      const int need = (P.snM[c] - P.snNc[c] + kSB - 1) / kSB;
+      if (tid == 0) waitOk = wait_count(done + c, need, status, s);
       __syncthreads();
-      for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
-        const int c = P.chList[qq];
-        const int muc = P.snM[c] - P.snNc[c];
-        const int *map = P.eaMap + P.eaPtr[c];
-        for (int k = 0; k < q; k++) {
-          double *v = V + (int64_t)k * Vstride + P.Sp[s];
-          const double *tc = T + (int64_t)k * Tstride + P.snTOff[c];
-          for (int a = tid; a < muc; a += blockDim.x) v[map[a]] += __ldcg(tc + a);
-        }
-        __syncthreads();
-      }
+      if (!waitOk) return false;
     }
-    const int ncb = (ncols + kSB - 1) / kSB;
-    for (int k = 0; k < q; k++) {
-      const double *yk = y + (int64_t)k * P.n + f;
-      double acc = 0.0, vreg = 0.0;
-      // v rows of this block: final once the supernode's first diagonal block is (it gathers them)
-      auto loadV = [&] {
-        if (tid < rows) vreg = __ldcg(V + (int64_t)k * Vstride + P.Sp[s] + r0 + tid);
-      };
-      if (ncb == 0 || k > 0) loadV();
-      // row-block dot products over the columns of the blocks this one depends on; the L values of a block are loaded
-      // before waiting for its flag (thread: row `row`, columns part, part + 4, ... of the block)
+    // this task's rows of v: pivot rows start from y; the children's entries mapping to rows [r0, r0 + rows) added in
+    // child order (the map is increasing, so they form one range per child)
+    if (tid < kSB) rk[tid] = (tid < rows && r0 + tid < nc) ? y[f + r0 + tid] : 0.0;
+    __syncthreads();
+    for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
+      const int c = P.chList[qq];
+      const int muc = P.snM[c] - P.snNc[c];
+      const int *map = P.eaMap + P.eaPtr[c];
+      int lo = 0, hi = muc;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (map[mid] < r0) lo = mid + 1; else hi = mid;
+      }
+      const int a0 = lo;
+      hi = muc;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (map[mid] < r0 + rows) lo = mid + 1; else hi = mid;
+      }
+      const double *tc = T + P.snTOff[c];
+      for (int a = a0 + tid; a < lo; a += blockDim.x) rk[map[a] - r0] += __ldcg(tc + a);
+      __syncthreads();
+    }
+    const double vreg = tid < kSB ? rk[tid] : 0.0;
+    // sums over the columns of the finished blocks; a block's L values are loaded before waiting for its flag
+    double acc = 0.0;
+    {
+      const int ncb = (ncols + kSB - 1) / kSB;
       TL lv[16];
-  #pragma unroll
+#pragma unroll
       for (int u = 0; u < 16; u++) {
         const int c = part + 4 * u;
         lv[u] = (rowok && c < ncols) ? Lp[(int64_t)c * m + r0 + row] : (TL)0;
@@ -195,53 +255,67 @@ __global__ void __launch_bounds__(256, 3) k_fwd_blocks(const int4 *__restrict__ 
       for (int cb = 0; cb < ncb; cb++) {
         TL ln[16];
         const int cn = (cb + 1) * kSB;
-  #pragma unroll
+#pragma unroll
         for (int u = 0; u < 16; u++) {
           const int c = cn + part + 4 * u;
           ln[u] = (rowok && c < ncols) ? Lp[(int64_t)c * m + r0 + row] : (TL)0;
         }
-        if (k == 0) {
-          if (tid == 0) waitOk = wait_flag(myflags + cb, epoch, status, s);
-          __syncthreads();
-          if (!waitOk) return false;  // block-uniform
-          if (cb == 0) loadV();
-        }
+        if (tid == 0) waitOk = wait_flag(myflags + cb, epoch, status, s);
+        __syncthreads();
+        if (!waitOk) return false;  // block-uniform
         const int cbase = cb * kSB;
-  #pragma unroll
+#pragma unroll
         for (int u = 0; u < 16; u++) {
           const int c = cbase + part + 4 * u;
-          if (c < ncols) acc += (double)lv[u] * __ldcg(yk + c);
+          if (c < ncols) acc += (double)lv[u] * __ldcg(y + f + c);
         }
-  #pragma unroll
+#pragma unroll
         for (int u = 0; u < 16; u++) lv[u] = ln[u];
       }
-      red[part][row] = acc;
-      __syncthreads();
-      if (tid < kSB) {
-        const double sum = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
-        rk[tid] = tid < rows ? vreg - sum : 0.0;
-      }
-      __syncthreads();
-      if (below) {
-        double *tk_out = T + (int64_t)k * Tstride + P.snTOff[s];
-        if (tid < rows) tk_out[blk * kSB + tid] = rk[tid];
-      } else {
-        // y_k = X r_k, X = L_kk^-1 lower triangular: thread (row, part) sums columns part, part + 4, ... <= row
-        double a2 = 0.0;
-        if (rowok)
-          for (int c = part; c <= row; c += 4) a2 += Xs[row][c] * rk[c];
-        red[part][row] = a2;
-        __syncthreads();
-        if (tid < rows) y[(int64_t)k * P.n + f + r0 + tid] = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
-      }
-      __syncthreads();
     }
-    if (tid == 0) {  // after the barrier: the CTA's stores are ordered before the release / the counted arrival
-      if (below)
-        red_release_add(done + s, 1);
-      else
-        st_release(myflags + blk, epoch);
+    // diagonal b >= 1: M_b(row, part + 4 u), loaded now (the tiles above are dead) and used after the last wait
+    TL mv[16];
+    if (!below && chain && blk > 0) {
+      const TL *M = Mch + (int64_t)(P.blkOff[s] - s + blk - 1) * kSB * kSB;
+#pragma unroll
+      for (int u = 0; u < 16; u++) mv[u] = rowok ? M[(part + 4 * u) * kSB + row] : (TL)0;
     }
+    red[part][row] = acc;
+    __syncthreads();
+    if (below) {
+      if (tid < rows)
+        T[P.snTOff[s] + blk * kSB + tid] = vreg - ((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]));
+      __syncthreads();
+      if (tid == 0) red_release_add(done + s, 1);
+      return true;
+    }
+    if (tid < kSB) rk[tid] = tid < rows ? vreg - ((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid])) : 0.0;
+    __syncthreads();
+    // w_b = X_b (v_b - the sums so far), X_b lower triangular: thread (row, part) sums columns part, part + 4, ... <= row
+    {
+      double a2 = 0.0;
+      if (rowok)
+        for (int c = part; c <= row; c += 4) a2 += Xs[row][c] * rk[c];
+      red[part][row] = a2;
+    }
+    __syncthreads();
+    const double wv = tid < rows ? (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]) : 0.0;
+    double yv = wv;
+    if (chain && blk > 0) {  // the chain step: wait for block b - 1, then y_b = w_b - M_b y_{b-1}
+      if (tid == 0) waitOk = wait_flag(myflags + blk - 1, epoch, status, s);
+      __syncthreads();
+      if (!waitOk) return false;
+      const double *yp = y + f + r0 - kSB;
+      double a3 = 0.0;
+#pragma unroll
+      for (int u = 0; u < 16; u++) a3 += (double)mv[u] * __ldcg(yp + part + 4 * u);
+      red[part][row] = a3;
+      __syncthreads();
+      if (tid < rows) yv = wv - ((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]));
+    }
+    if (tid < rows) y[f + r0 + tid] = yv;
+    __syncthreads();
+    if (tid == 0) st_release(myflags + blk, epoch);  // after the barrier: the CTA's stores are ordered before it
     return true;
   };
   for (;;) {
@@ -254,17 +328,17 @@ __global__ void __launch_bounds__(256, 3) k_fwd_blocks(const int4 *__restrict__ 
 }
 
 // ---- backward block tasks ----------------------------------------------------------------------------------------
-// task: .x supernode, .y column block (tasks of a supernode listed from the last block down)
-// r_k = y_k - L[rows below the block, k]^T x(rows): the rows below the supernode (ancestors, final once the parent's
-// first pivot block is) and the later pivot blocks except the next one accumulate in registers (warps own columns,
-// lanes walk rows) and are reduced before the last wait; the next block's L tile is staged in shared memory and
-// read column-wise after its flag, so the chain step is a 64 x 64 product, a reduction and the inverse product.
+// task: .x supernode, .y column block (tasks of a supernode listed from the last block down), .z 0 or 2 (small)
+// r_b = y_b - L[rows below the block, b]^T x(rows): the rows below the supernode (ancestors, final once the parent's
+// first pivot block is) and the pivot blocks b + 2 and later accumulate in registers (warps own columns, lanes walk
+// rows) and give w_b = X_b^T (r_b without block b + 1); then, after block b + 1's flag, x_b = w_b - G_b^T x_{b+1} with
+// G_b staged in shared memory beforehand.
 constexpr int kBwdSmem = 2 * kSB * (kSB + 1) * (int)sizeof(double);
 template <class TL>
 __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ tasks, int ntasks, int *__restrict__ ticket,
                                                     DevPlan P, const TL *__restrict__ Lx, const TL *__restrict__ Inv,
-                                                    const double *__restrict__ Dpiv, double *__restrict__ y,
-                                                    int *__restrict__ flags, int epoch, int q,
+                                                    const TL *__restrict__ Gch, const double *__restrict__ Dpiv,
+                                                    double *__restrict__ y, int *__restrict__ flags, int epoch,
                                                     unsigned long long *status) {
   __shared__ int tk, waitOk;
   __shared__ double red[4][kSB];
@@ -272,9 +346,8 @@ __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ 
   __shared__ double xs[kSB];
   __shared__ double rk[kSB];
   extern __shared__ double bwd_dyn[];
-  double(*Xs)[kSB + 1] = reinterpret_cast<double(*)[kSB + 1]>(bwd_dyn);            // L_kk^-1
-  double(*Lf)[kSB + 1] = reinterpret_cast<double(*)[kSB + 1]>(bwd_dyn + kSB * (kSB + 1));  // next block, [row][col]
-  // persistent: take tickets until the list is exhausted (a task only waits for earlier tickets)
+  double(*Xs)[kSB + 1] = reinterpret_cast<double(*)[kSB + 1]>(bwd_dyn);                    // X_b
+  double(*Gt)[kSB + 1] = reinterpret_cast<double(*)[kSB + 1]>(bwd_dyn + kSB * (kSB + 1));  // G_b, [r][c]
   auto run = [&](const int tkv) -> bool {
     const int4 t = tasks[tkv];
     if (t.z == 2) {  // up to kSolveGroup supernodes with m <= 32, one warp each
@@ -292,16 +365,22 @@ __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ 
     const int *rowsOf = P.Si + P.Sp[s];
     const int c0 = blk * kSB, w = min(kSB, nc - c0), nb = (nc + kSB - 1) / kSB;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const bool hasNext = blk + 1 < nb;
+    // with chain matrices (Cholesky) block b + 1 is applied last through G_b; without them (LDL^T) it is summed with
+    // the other blocks before X_b^T is applied
+    const bool chain = Gch != nullptr;
+    const bool hasNext = chain && blk + 1 < nb;
     const int rn = (blk + 1) * kSB, wn = hasNext ? min(kSB, nc - rn) : 0;  // the next pivot block: rows [rn, rn + wn)
+    const int rbLast = chain ? blk + 1 : blk;  // pivot blocks above rbLast are summed in registers
     int *myflags = flags + P.blkOff[s];
     {
       const TL *X = Inv + P.invOff[P.blkOff[s] + blk];
       for (int e = tid; e < w * w; e += blockDim.x) Xs[e % w][e / w] = (double)X[e];
-      // next block's tile: Lf[r][c] = L(rn + r, c0 + c); coalesced along r
-      for (int e = tid; e < kSB * kSB; e += blockDim.x) {
-        const int r = e & (kSB - 1), c = e >> 6;
-        Lf[r][c] = (r < wn && c < w) ? (double)Lp[(int64_t)(c0 + c) * m + rn + r] : 0.0;
+      if (hasNext) {
+        const TL *G = Gch + (int64_t)(P.blkOff[s] - s + blk) * kSB * kSB;
+        for (int e = tid; e < kSB * kSB; e += blockDim.x) {
+          const int r = e & (kSB - 1), c = e >> 6;
+          Gt[r][c] = (r < wn && c < w) ? (double)G[c * kSB + r] : 0.0;
+        }
       }
     }
     // one launch for the whole sweep (levels top-down): the rows below this supernode are final once its parent's
@@ -312,95 +391,92 @@ __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ 
       __syncthreads();
       if (!waitOk) return false;
     }
-    for (int k = 0; k < q; k++) {
-      double *yk = y + (int64_t)k * P.n;
-      double acc[8];
-  #pragma unroll
-      for (int u = 0; u < 8; u++) acc[u] = 0.0;
-      // rows of the supernode below its pivot columns: ancestors, final
-      for (int r = nc + lane; r < m; r += 32) {
-        const double xr = __ldcg(yk + rowsOf[r]);
-  #pragma unroll
+    double acc[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) acc[u] = 0.0;
+    // rows of the supernode below its pivot columns: ancestors, final
+    for (int r = nc + lane; r < m; r += 32) {
+      const double xr = __ldcg(y + rowsOf[r]);
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int c = warp + 8 * u;
+        if (c < w) acc[u] += (double)Lp[(int64_t)(c0 + c) * m + r] * xr;
+      }
+    }
+    // pivot blocks after the next one, as they become final; a block's L values are loaded before its wait
+    TL lv[2][8];
+    auto load_block = [&](int rb, TL (&dst)[2][8]) {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int r = rb * kSB + lane + 32 * h;
+#pragma unroll
         for (int u = 0; u < 8; u++) {
           const int c = warp + 8 * u;
-          if (c < w) acc[u] += (double)Lp[(int64_t)(c0 + c) * m + r] * xr;
+          dst[h][u] = (rb > rbLast && r < nc && c < w) ? Lp[(int64_t)(c0 + c) * m + r] : (TL)0;
         }
       }
-      // pivot blocks after the next one, as they become final; a block's L values are loaded before its wait
-      TL lv[2][8];
-      auto load_block = [&](int rb, TL (&dst)[2][8]) {
-  #pragma unroll
-        for (int h = 0; h < 2; h++) {
-          const int r = rb * kSB + lane + 32 * h;
-  #pragma unroll
-          for (int u = 0; u < 8; u++) {
-            const int c = warp + 8 * u;
-            dst[h][u] = (rb > blk + 1 && r < nc && c < w) ? Lp[(int64_t)(c0 + c) * m + r] : (TL)0;
-          }
-        }
-      };
-      load_block(nb - 1, lv);
-      for (int rb = nb - 1; rb > blk + 1; rb--) {
-        TL ln[2][8];
-        load_block(rb - 1, ln);
-        if (k == 0) {
-          if (tid == 0) waitOk = wait_flag(myflags + rb, epoch, status, s);
-          __syncthreads();
-          if (!waitOk) return false;  // block-uniform
-        }
-  #pragma unroll
-        for (int h = 0; h < 2; h++) {
-          const int r = rb * kSB + lane + 32 * h;
-          const double xr = r < nc ? __ldcg(yk + f + r) : 0.0;
-  #pragma unroll
-          for (int u = 0; u < 8; u++) acc[u] += (double)lv[h][u] * xr;
-        }
-  #pragma unroll
-        for (int h = 0; h < 2; h++)
-  #pragma unroll
-          for (int u = 0; u < 8; u++) lv[h][u] = ln[h][u];
-      }
-  #pragma unroll
-      for (int u = 0; u < 8; u++) {
-        double v = acc[u];
-  #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        if (lane == 0) red0[warp + 8 * u] = v;
-      }
-      double yv = 0.0;  // LDL^T: y /= D before the backward sweep (ldlt.mjs:629)
-      if (tid < w) yv = Dpiv ? yk[f + c0 + tid] / Dpiv[f + c0 + tid] : yk[f + c0 + tid];
-      // the chain step: wait for the next block, then its contribution from the staged tile
-      if (hasNext && k == 0) {
-        if (tid == 0) waitOk = wait_flag(myflags + blk + 1, epoch, status, s);
-        __syncthreads();
-        if (!waitOk) return false;  // block-uniform
-      }
-      if (tid < kSB) xs[tid] = tid < wn ? __ldcg(yk + f + rn + tid) : 0.0;
+    };
+    load_block(nb - 1, lv);
+    for (int rb = nb - 1; rb > rbLast; rb--) {
+      TL ln[2][8];
+      load_block(rb - 1, ln);
+      if (tid == 0) waitOk = wait_flag(myflags + rb, epoch, status, s);
       __syncthreads();
-      {
-        const int c = tid & (kSB - 1), part = tid >> 6;
-        double a2 = 0.0;
-  #pragma unroll 4
-        for (int r = part; r < wn; r += 4) a2 += Lf[r][c] * xs[r];
-        red[part][c] = a2;
+      if (!waitOk) return false;  // block-uniform
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int r = rb * kSB + lane + 32 * h;
+        const double xr = r < nc ? __ldcg(y + f + r) : 0.0;
+#pragma unroll
+        for (int u = 0; u < 8; u++) acc[u] += (double)lv[h][u] * xr;
       }
-      __syncthreads();
-      if (tid < kSB)
-        rk[tid] = tid < w ? yv - red0[tid] - ((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid])) : 0.0;
-      __syncthreads();
-      // x_k = X^T r_k, X = L_kk^-1 lower triangular: thread (row i, part) sums X(j, i) r(j) over j = i + part, +4 ...
-      {
-        const int i = tid & (kSB - 1), part = tid >> 6;
-        double a2 = 0.0;
-        if (i < w)
-          for (int j = i + part; j < w; j += 4) a2 += Xs[j][i] * rk[j];
-        red[part][i] = a2;
-      }
-      __syncthreads();
-      if (tid < w) yk[f + c0 + tid] = (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]);
-      __syncthreads();
+#pragma unroll
+      for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int u = 0; u < 8; u++) lv[h][u] = ln[h][u];
     }
-    if (tid == 0) st_release(myflags + blk, epoch);  // after the barrier: the CTA's stores of x_k are ordered before
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      double v = acc[u];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lane == 0) red0[warp + 8 * u] = v;
+    }
+    __syncthreads();
+    if (tid < kSB) {
+      double yv = 0.0;  // LDL^T: y /= D before the backward sweep (ldlt.mjs:629)
+      if (tid < w) yv = Dpiv ? y[f + c0 + tid] / Dpiv[f + c0 + tid] : y[f + c0 + tid];
+      rk[tid] = tid < w ? yv - red0[tid] : 0.0;
+    }
+    __syncthreads();
+    // w_b = X_b^T r: thread (i, part) sums X(j, i) r(j) over j = i + part, i + part + 4, ... < w
+    {
+      const int i = tid & (kSB - 1), part = tid >> 6;
+      double a2 = 0.0;
+      if (i < w)
+        for (int j = i + part; j < w; j += 4) a2 += Xs[j][i] * rk[j];
+      red[part][i] = a2;
+    }
+    __syncthreads();
+    const double wv = tid < w ? (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]) : 0.0;
+    double xv = wv;
+    if (hasNext) {  // the chain step: wait for block b + 1, then x_b = w_b - G_b^T x_{b+1}
+      if (tid == 0) waitOk = wait_flag(myflags + blk + 1, epoch, status, s);
+      __syncthreads();
+      if (!waitOk) return false;  // block-uniform
+      if (tid < kSB) xs[tid] = tid < wn ? __ldcg(y + f + rn + tid) : 0.0;
+      __syncthreads();
+      const int c = tid & (kSB - 1), part = tid >> 6;
+      double a3 = 0.0;
+#pragma unroll 4
+      for (int r = part; r < wn; r += 4) a3 += Gt[r][c] * xs[r];
+      red[part][c] = a3;
+      __syncthreads();
+      if (tid < w) xv = wv - ((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]));
+    }
+    if (tid < w) y[f + c0 + tid] = xv;
+    __syncthreads();
+    if (tid == 0) st_release(myflags + blk, epoch);  // after the barrier: the CTA's stores of x_b are ordered before
     return true;
   };
   for (;;) {
@@ -415,6 +491,8 @@ __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ 
 void init_solve_attributes() {
   cudaFuncSetAttribute(k_bwd_blocks<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBwdSmem);
   cudaFuncSetAttribute(k_bwd_blocks<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBwdSmem);
+  cudaFuncSetAttribute(k_chain_mats<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kChainSmem);
+  cudaFuncSetAttribute(k_chain_mats<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kChainSmem);
 }
 
 int num_sms();
@@ -426,32 +504,43 @@ void launch_diag_inv(const DevPlan &P, int nblocks, const TL *Lx, TL *Inv, cudaS
   if (nblocks > 0) k_diag_inv<TL><<<nblocks, kSB, 0, st>>>(P, Lx, Inv);
 }
 template <class TL>
+void launch_chain_mats(const int2 *tasks, int ntasks, const DevPlan &P, const TL *Lx, const TL *Inv, TL *Mch, TL *Gch,
+                       cudaStream_t st) {
+  if (ntasks > 0) k_chain_mats<TL><<<ntasks, 256, kChainSmem, st>>>(tasks, P, Lx, Inv, Mch, Gch);
+}
+template <class TL>
 void launch_fwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
-                       double *y, double *V, double *T, int *flags, int epoch, int *done, int q, int64_t Vstride,
-                       int64_t Tstride, unsigned long long *status, cudaStream_t st) {
+                       const TL *Mch, double *y, double *T, int *flags, int epoch, int *done,
+                       unsigned long long *status, cudaStream_t st) {
   if (ntasks > 0)
-    k_fwd_blocks<TL><<<solve_grid(ntasks), 256, 0, st>>>(tasks, ntasks, ticket, P, Lx, Inv, y, V, T, flags, epoch, done, q,
-                                             Vstride, Tstride, status);
+    k_fwd_blocks<TL><<<solve_grid(ntasks), 256, 0, st>>>(tasks, ntasks, ticket, P, Lx, Inv, Mch, y, T, flags, epoch,
+                                                         done, status);
 }
 template <class TL>
 void launch_bwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
-                       const double *Dpiv, double *y, int *flags, int epoch, int q, unsigned long long *status,
+                       const TL *Gch, const double *Dpiv, double *y, int *flags, int epoch, unsigned long long *status,
                        cudaStream_t st) {
   if (ntasks > 0)
-    k_bwd_blocks<TL><<<solve_grid(ntasks), 256, kBwdSmem, st>>>(tasks, ntasks, ticket, P, Lx, Inv, Dpiv, y, flags,
-                                                                 epoch, q, status);
+    k_bwd_blocks<TL><<<solve_grid(ntasks), 256, kBwdSmem, st>>>(tasks, ntasks, ticket, P, Lx, Inv, Gch, Dpiv, y, flags,
+                                                                 epoch, status);
 }
 template void launch_diag_inv<double>(const DevPlan &, int, const double *, double *, cudaStream_t);
 template void launch_diag_inv<float>(const DevPlan &, int, const float *, float *, cudaStream_t);
+template void launch_chain_mats<double>(const int2 *, int, const DevPlan &, const double *, const double *, double *,
+                                        double *, cudaStream_t);
+template void launch_chain_mats<float>(const int2 *, int, const DevPlan &, const float *, const float *, float *,
+                                       float *, cudaStream_t);
 template void launch_fwd_blocks<double>(const int4 *, int, int *, const DevPlan &, const double *, const double *,
-                                        double *, double *, double *, int *, int, int *, int, int64_t, int64_t,
-                                        unsigned long long *, cudaStream_t);
+                                        const double *, double *, double *, int *, int, int *, unsigned long long *,
+                                        cudaStream_t);
 template void launch_fwd_blocks<float>(const int4 *, int, int *, const DevPlan &, const float *, const float *,
-                                       double *, double *, double *, int *, int, int *, int, int64_t, int64_t,
-                                       unsigned long long *, cudaStream_t);
+                                       const float *, double *, double *, int *, int, int *, unsigned long long *,
+                                       cudaStream_t);
 template void launch_bwd_blocks<double>(const int4 *, int, int *, const DevPlan &, const double *, const double *,
-                                        const double *, double *, int *, int, int, unsigned long long *, cudaStream_t);
+                                        const double *, const double *, double *, int *, int, unsigned long long *,
+                                        cudaStream_t);
 template void launch_bwd_blocks<float>(const int4 *, int, int *, const DevPlan &, const float *, const float *,
-                                       const double *, double *, int *, int, int, unsigned long long *, cudaStream_t);
+                                       const float *, const double *, double *, int *, int, unsigned long long *,
+                                       cudaStream_t);
 
 }  // namespace amp

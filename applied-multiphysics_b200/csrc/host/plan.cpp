@@ -335,6 +335,11 @@ void build_plan(const Symbolic &S, Plan &P) {
     v.push_back(c);
     v.push_back(0);
   };
+  for (int s = 0; s < ns; s++)
+    for (int b = 0; P.snNc[s] > B && b * B < P.snNc[s]; b++) {
+      P.chainTasks.push_back(s);
+      P.chainTasks.push_back(b);
+    }
   // Supernodes with m <= kTinyFront are solved whole by one warp: tasks {first, count, 2} over solveSmall, up to
   // kSolveGroup supernodes of one level per task, listed before the level's block tasks.
   auto solveSmall = [&](int s) { return P.snM[s] <= kTinyFront; };

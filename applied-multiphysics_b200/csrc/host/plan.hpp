@@ -106,6 +106,7 @@ struct Plan {
   std::vector<int> diagSlot;        // CSR slot of each diagonal entry of A (LDL^T pivot scale)
   std::vector<int> fwdTasks, bwdTasks;  // int4 records, flattened
   std::vector<int> solveSmall;          // supernodes solved whole by one warp, grouped by level (tasks of kind 2)
+  std::vector<int> chainTasks;          // {s, b} pairs: every diagonal block of a supernode with two or more
   std::vector<int> fwdLvlPtr, bwdLvlPtr;
   std::vector<int> bwdAll;  // backward tasks of all levels, top-down (one launch)
   double flops = 0;
