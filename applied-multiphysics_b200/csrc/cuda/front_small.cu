@@ -42,22 +42,23 @@ __device__ __forceinline__ bool small_ldlt_pivot(T &d, T tau, int &neg, int &per
   return true;
 }
 
-// The whole front of supernode s by a group of G threads (thread t) over the shared m x m column-major tile F.
-// pv / flag: the group's shared scalars.
-template <class T, int G>
+// The whole front of supernode s by a group of G threads (thread t) over the shared m x m column-major tile F, in the
+// compute type TC (the storage type T of L and U, or FP64: an FP32 LDL^T factor's small fronts are computed in FP64
+// and rounded once when stored, since the indefinite factor's pivots cancel). pv / flag: the group's shared scalars.
+template <class T, class TC, int G>
 __device__ void factor_front(int s, const DevPlan &P, const double *__restrict__ values, T *__restrict__ Lx,
-                             T *__restrict__ U, T *F, unsigned long long *status, const LdltArgs<T> &la, int t,
-                             T *pv, int *flag) {
+                             T *__restrict__ U, TC *F, unsigned long long *status, const LdltArgs<T> &la, int t,
+                             TC *pv, int *flag) {
   const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s], mu = m - nc;
   const bool ldlt = la.scal != nullptr;
-  const T tau = ldlt ? (T)la.scal[1] : T(0);
-  for (int e = t; e < m * m; e += G) F[e] = T(0);
+  const TC tau = ldlt ? (TC)(T)la.scal[1] : TC(0);
+  for (int e = t; e < m * m; e += G) F[e] = TC(0);
   if (t == 0) *flag = 0;
   group_sync<G>();
   // A's entries of the pivot columns: slot dst = j m + i of the L panel, each (i, j) once
   for (int j = 0; j < nc; j++) {
     const int p0 = P.asmColPtr[f + j], p1 = P.asmColPtr[f + j + 1];
-    for (int p = p0 + t; p < p1; p += G) F[P.asmDst[p]] += (T)__ldg(values + P.asmSrc[p]);
+    for (int p = p0 + t; p < p1; p += G) F[P.asmDst[p]] += (TC)(T)__ldg(values + P.asmSrc[p]);
   }
   group_sync<G>();
   // children's update matrices, one after another (the map is injective within a child)
@@ -69,7 +70,7 @@ __device__ void factor_front(int s, const DevPlan &P, const double *__restrict__
     const T *Uc = U + P.snUoff[c];
     for (int e = t; e < muc * muc; e += G) {
       const int b = e / muc, a = e - b * muc;
-      if (a >= b) F[map[b] * m + map[a]] += Uc[e];
+      if (a >= b) F[map[b] * m + map[a]] += (TC)Uc[e];
     }
     group_sync<G>();
   }
@@ -77,19 +78,19 @@ __device__ void factor_front(int s, const DevPlan &P, const double *__restrict__
   int neg = 0, pert = 0;  // thread 0
   for (int k = 0; k < nc; k++) {
     if (t == 0) {
-      T d = F[k * m + k];
+      TC d = F[k * m + k];
       int bad = 0;
       if (ldlt) {
         if (!small_ldlt_pivot(d, tau, neg, pert)) bad = 2;
-        la.D[f + k] = (double)d;
+        la.D[f + k] = (double)(T)d;
         pv[0] = d;
-        pv[1] = T(1) / d;
-        F[k * m + k] = T(1);
+        pv[1] = TC(1) / d;
+        F[k * m + k] = TC(1);
       } else {
-        if (!(d > T(0))) bad = 1;
-        const T r = sqrt(d);
-        pv[0] = T(1);
-        pv[1] = T(1) / r;
+        if (!(d > TC(0))) bad = 1;
+        const TC r = sqrt(d);
+        pv[0] = TC(1);
+        pv[1] = TC(1) / r;
         F[k * m + k] = r;
       }
       if (bad) {
@@ -99,8 +100,8 @@ __device__ void factor_front(int s, const DevPlan &P, const double *__restrict__
     }
     group_sync<G>();
     if (*flag) return;  // group-uniform
-    const T inv = pv[1], dk = pv[0];
-    T *Fk = F + k * m;
+    const TC inv = pv[1], dk = pv[0];
+    TC *Fk = F + k * m;
     for (int i = k + 1 + t; i < m; i += G) Fk[i] *= inv;
     group_sync<G>();
     const int w = m - k - 1;
@@ -120,62 +121,74 @@ __device__ void factor_front(int s, const DevPlan &P, const double *__restrict__
   T *Lp = Lx + P.snLxp[s];
   for (int e = t; e < nc * m; e += G) {
     const int j = e / m, i = e - j * m;
-    if (i >= j) Lp[e] = F[e];
+    if (i >= j) Lp[e] = (T)F[e];
   }
   if (mu > 0) {
     T *Up = U + P.snUoff[s];
     for (int e = t; e < mu * mu; e += G) {
       const int jj = e / mu, ii = e - jj * mu;
-      if (ii >= jj) Up[e] = F[(nc + jj) * m + nc + ii];
+      if (ii >= jj) Up[e] = (T)F[(nc + jj) * m + nc + ii];
     }
   }
 }
 
 // m <= 32: one warp per front, kTinyWarps fronts per CTA
-template <class T>
+template <class T, class TC>
 __global__ void __launch_bounds__(32 * kTinyWarps) k_front_tiny(const int *__restrict__ fronts, int count, DevPlan P,
                                                                 const double *__restrict__ values, T *__restrict__ Lx,
                                                                 T *__restrict__ U, unsigned long long *status,
                                                                 LdltArgs<T> la) {
-  __shared__ T F[kTinyWarps][kTinyFront * kTinyFront];
-  __shared__ T pv[kTinyWarps][2];
+  __shared__ TC F[kTinyWarps][kTinyFront * kTinyFront];
+  __shared__ TC pv[kTinyWarps][2];
   __shared__ int flag[kTinyWarps];
   if (status_failed(status)) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int idx = blockIdx.x * kTinyWarps + warp;
   if (idx >= count) return;  // warp-uniform; no CTA-wide barrier follows
-  factor_front<T, 32>(fronts[idx], P, values, Lx, U, F[warp], status, la, lane, pv[warp], &flag[warp]);
+  factor_front<T, TC, 32>(fronts[idx], P, values, Lx, U, F[warp], status, la, lane, pv[warp], &flag[warp]);
 }
 
 // 32 < m <= 128: one CTA per front; dynamic shared memory = the launch's largest m squared
-template <class T>
+template <class T, class TC>
 __global__ void __launch_bounds__(256) k_front_small(const int *__restrict__ fronts, int count, DevPlan P,
                                                      const double *__restrict__ values, T *__restrict__ Lx,
                                                      T *__restrict__ U, unsigned long long *status, LdltArgs<T> la) {
   extern __shared__ __align__(16) unsigned char fs_dyn[];
-  __shared__ T pv[2];
+  __shared__ TC pv[2];
   __shared__ int flag;
   if (status_failed(status)) return;
-  factor_front<T, 256>(fronts[blockIdx.x], P, values, Lx, U, reinterpret_cast<T *>(fs_dyn), status, la, threadIdx.x,
-                       pv, &flag);
+  factor_front<T, TC, 256>(fronts[blockIdx.x], P, values, Lx, U, reinterpret_cast<TC *>(fs_dyn), status, la,
+                           threadIdx.x, pv, &flag);
 }
 
 void init_front_small_attributes() {
-  cudaFuncSetAttribute(k_front_small<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(k_front_small<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        kSmallFront * kSmallFront * (int)sizeof(double));
-  cudaFuncSetAttribute(k_front_small<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(k_front_small<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        kSmallFront * kSmallFront * (int)sizeof(float));
+  cudaFuncSetAttribute(k_front_small<float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       kSmallFront * kSmallFront * (int)sizeof(double));
 }
 
+template <class T, class TC>
+static void launch_fronts_tc(const int *tiny, int ntiny, const int *small, int nsmall, int maxM, const DevPlan &P,
+                             const double *values, T *Lx, T *U, unsigned long long *status, const LdltArgs<T> &la,
+                             cudaStream_t st) {
+  if (ntiny > 0)
+    k_front_tiny<T, TC><<<(ntiny + kTinyWarps - 1) / kTinyWarps, 32 * kTinyWarps, 0, st>>>(tiny, ntiny, P, values, Lx,
+                                                                                           U, status, la);
+  if (nsmall > 0)
+    k_front_small<T, TC><<<nsmall, 256, (size_t)maxM * maxM * sizeof(TC), st>>>(small, nsmall, P, values, Lx, U,
+                                                                                status, la);
+}
 template <class T>
 void launch_fronts_small(const int *tiny, int ntiny, const int *small, int nsmall, int maxM, const DevPlan &P,
                          const double *values, T *Lx, T *U, unsigned long long *status, const LdltArgs<T> &la,
                          cudaStream_t st) {
-  if (ntiny > 0)
-    k_front_tiny<T><<<(ntiny + kTinyWarps - 1) / kTinyWarps, 32 * kTinyWarps, 0, st>>>(tiny, ntiny, P, values, Lx, U,
-                                                                                       status, la);
-  if (nsmall > 0)
-    k_front_small<T><<<nsmall, 256, (size_t)maxM * maxM * sizeof(T), st>>>(small, nsmall, P, values, Lx, U, status, la);
+  if (la.scal != nullptr)  // LDL^T: FP64 arithmetic whatever the storage
+    launch_fronts_tc<T, double>(tiny, ntiny, small, nsmall, maxM, P, values, Lx, U, status, la, st);
+  else
+    launch_fronts_tc<T, T>(tiny, ntiny, small, nsmall, maxM, P, values, Lx, U, status, la, st);
 }
 template void launch_fronts_small<double>(const int *, int, const int *, int, int, const DevPlan &, const double *,
                                           double *, double *, unsigned long long *, const LdltArgs<double> &,
