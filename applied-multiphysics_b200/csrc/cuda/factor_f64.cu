@@ -194,8 +194,8 @@ __global__ void __launch_bounds__(256) k_potrf(const PotrfTask *__restrict__ tas
   const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
   const int w = min(kPanel, nc - c0);
   T *Lp = Lx + P.snLxp[s] + (int64_t)c0 * m + c0;  // block (i, j) at Lp[j m + i]
-  __shared__ T col[2][kPanel];
-  __shared__ T pd[kPanel], piv[2];
+  __shared__ T col[2][4][kPanel];  // per 4-column block (double-buffered): the block's unscaled columns, by row
+  __shared__ T pd[kPanel], piv[2][4];
   __shared__ unsigned char pflag[kPanel];
   __shared__ int fail;
   const int tid = threadIdx.x;
@@ -216,38 +216,65 @@ __global__ void __launch_bounds__(256) k_potrf(const PotrfTask *__restrict__ tas
       a[r][c] = !owner || i < j ? T(0) : (i < w ? Lp[(int64_t)j * m + i] : (i == j ? T(1) : T(0)));
     }
   if (tid == 0) fail = kPanel;  // none
-  __syncthreads();
-  // k = 4 kb + kk with kk a compile-time constant, so the tile's registers are indexed statically
+  // Four columns per step kb, two barriers: (1) the diagonal tile eliminates its four columns (settling the pivots)
+  // and publishes them; (2) the tiles below it in column block kb eliminate the same four columns against it and
+  // publish theirs; then every tile right of the block applies the rank-4 update S(i, j) -= sum S(i, k) S(j, k) / d_k.
   for (int kb = 0; kb < kPanel / 4; kb++) {
+    const int buf = kb & 1;
+    if (owner && ti == kb && tj == kb) {
 #pragma unroll
-    for (int kk = 0; kk < 4; kk++) {
-      const int k = 4 * kb + kk, buf = kk & 1;
-      if (owner && tj == kb) {  // publish column k (rows >= 4 tj); the diagonal tile also settles the pivot
+      for (int kk = 0; kk < 4; kk++) {
+        const int k = 4 * kb + kk;
+        T d = a[kk][kk];
+        unsigned char fl = 0;
+        const bool bad = k < w && (ldlt ? !ldlt_pivot(d, tau, fl) : !(d > T(0)));
+        if (bad && myFail < 0) myFail = k;  // first failing pivot of this diagonal tile
+        const T iv = fast_recip(d);           // the update scale only; L is scaled with the exact 1 / d at the end
+        pd[k] = d;
+        pflag[k] = fl;
+        piv[buf][kk] = iv;
 #pragma unroll
-        for (int r = 0; r < 4; r++) col[buf][4 * ti + r] = a[r][kk];
-        if (ti == tj) {
-          T d = a[kk][kk];
-          unsigned char fl = 0;
-          const bool bad = k < w && (ldlt ? !ldlt_pivot(d, tau, fl) : !(d > T(0)));
-          if (bad && myFail < 0) myFail = k;  // first failing pivot of this diagonal tile
-          piv[buf] = fast_recip(d);  // the update scale only; L is scaled with the exact 1 / d at the end
-          pd[k] = d;
-          pflag[k] = fl;
+        for (int r = kk + 1; r < 4; r++)
+#pragma unroll
+          for (int c = kk + 1; c <= r; c++) a[r][c] -= a[r][kk] * (a[c][kk] * iv);
+      }
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++)
+#pragma unroll
+        for (int r = 0; r < 4; r++) col[buf][kk][4 * kb + r] = a[r][kk];
+    }
+    __syncthreads();
+    if (owner && tj == kb && ti > kb) {
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) {
+        const T iv = piv[buf][kk];
+#pragma unroll
+        for (int c = kk + 1; c < 4; c++) {
+          const T cj = col[buf][kk][4 * kb + c] * iv;
+#pragma unroll
+          for (int r = 0; r < 4; r++) a[r][c] -= a[r][kk] * cj;
         }
       }
-      __syncthreads();
-      if (owner && ti >= kb && !(kb == kPanel / 4 - 1 && kk == 3)) {
-        const T iv = piv[buf];
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++)
+#pragma unroll
+        for (int r = 0; r < 4; r++) col[buf][kk][4 * ti + r] = a[r][kk];
+    }
+    __syncthreads();
+    if (owner && tj > kb) {
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) {
+        const T iv = piv[buf][kk];
         T ci[4], cj[4];
 #pragma unroll
-        for (int r = 0; r < 4; r++) ci[r] = col[buf][4 * ti + r];
+        for (int r = 0; r < 4; r++) ci[r] = col[buf][kk][4 * ti + r];
 #pragma unroll
-        for (int c = 0; c < 4; c++) cj[c] = col[buf][4 * tj + c] * iv;
+        for (int c = 0; c < 4; c++) cj[c] = col[buf][kk][4 * tj + c] * iv;
 #pragma unroll
         for (int r = 0; r < 4; r++)
 #pragma unroll
           for (int c = 0; c < 4; c++)
-            if (4 * ti + r > k && 4 * tj + c > k) a[r][c] -= ci[r] * cj[c];
+            if (ti > tj || c <= r) a[r][c] -= ci[r] * cj[c];
       }
     }
   }

@@ -218,11 +218,11 @@ def cpu_baseline_sample(w, perm, budget_s: float = 15.0, kind: str = "chol"):
             "full_factor_s_est": so.flops / (fl / dt)}
 
 
-# DRAM bytes per launch of the roofline kernel (dram__bytes_read.sum + dram__bytes_write.sum, one ncu capture of the
-# same command: the launch list of `bench.py --steps 1 --warmup 3 --no-cpu-baseline`, every launch of the kernel class
-# in the mixed phase, total / launches). Keyed by (workload, size, precision, kernel class).
+# DRAM bytes per launch of the roofline kernel (dram__bytes_read.sum + dram__bytes_write.sum, one ncu capture: the
+# launch list of `bench.py --precision mixed --steps 1 --warmup 1 --no-cpu-baseline`, every launch of the kernel class,
+# total / launches). Keyed by (workload, size, precision, kernel class).
 TRAFFIC = {
-    ("elastic3d", 40, "mixed", "update_syrk"): 65.085e9 / 2093,
+    ("elastic3d", 40, "mixed", "update_syrk"): 50.229e9 / 2485,
 }
 
 
