@@ -408,7 +408,7 @@ void enqueue_factor(amp_factor *f) {
         if (sr.mixMid > sr.mix0)
           timed(f, K_UPDATE, sr.updateFlopsA, 0.0, [&] {
             amp::launch_update_mx(f->plan->dMixTile + sr.mix0, sr.mixMid - sr.mix0, f->dMaps, f->dL32, f->dU32,
-                                  f->dStatus, amp::num_sms(), st);
+                                  f->dStatus, amp::num_sms(), st, true);
           });
         if (sr.mix1 > sr.mixMid)
           la.part_b(K_UPDATE, sr.updateFlopsB, [&] {

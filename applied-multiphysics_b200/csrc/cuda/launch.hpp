@@ -29,8 +29,9 @@ template <class T>
 void launch_fronts_small(const int *tiny, int ntiny, const int *small, int nsmall, int maxM, const DevPlan &P,
                          const double *values, T *Lx, T *U, unsigned long long *status, const LdltArgs<T> &la,
                          cudaStream_t st);
+// narrow: 128 x 64 tiles (tasks whose columns are one 64-column pivot block), else 128 x 256
 void launch_update_mx(const MixTask *tasks, int64_t ntasks, const CUtensorMap *maps, float *L32, float *U32,
-                      unsigned long long *status, int num_sms, cudaStream_t st);
+                      unsigned long long *status, int num_sms, cudaStream_t st, bool narrow = false);
 int num_sms();
 void launch_update(const TileTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, double *U, const double *W,
                    const unsigned long long *status, cudaStream_t st);

@@ -1,4 +1,5 @@
-// Mixed-precision trailing / update-block tiles on the 5th-generation tensor cores (tcgen05, sm_100a).
+// Mixed-precision trailing / update-block tiles on the 5th-generation tensor cores (tcgen05, sm_100a), 128 x 256, or
+// 128 x 64 for the look-ahead's next pivot block (one 64-column block wide).
 //
 // C[i0:i0+128, j0:j0+256] -= A B^T in FP32, where A and B are rows of the factored pivot columns of a front (for
 // LDL^T, A holds those rows times the pivots, L21 D) and the product runs as BF16x3: every FP32 value x is carried
@@ -30,12 +31,14 @@
 namespace amp {
 
 namespace {
-constexpr int kM = 128, kN = 256, kK = 64;
+constexpr int kM = 128, kK = 64;
 constexpr int kBox = 64;                                  // rows per TMA box (128 bytes of BF16)
 constexpr uint32_t kBoxBytes = kBox * kK * 2;             // 8 KB
 constexpr uint32_t kABytes = kM * kK * 2;                 // 16 KB (hi or lo)
-constexpr uint32_t kBBytes = kN * kK * 2;                 // 32 KB
-constexpr uint32_t kStageBytes = 2 * kABytes + 2 * kBBytes;  // 96 KB
+template <int N>
+constexpr uint32_t b_bytes() { return N * kK * 2; }  // 32 KB for N = 256 (hi or lo)
+template <int N>
+constexpr uint32_t stage_bytes() { return 2 * kABytes + 2 * b_bytes<N>(); }  // 96 KB for N = 256
 constexpr int kStages = 2;
 constexpr uint32_t kLbo = kBoxBytes;                      // between 64-row MN blocks
 constexpr uint32_t kSbo = 8 * 128;                        // between groups of 8 K rows
@@ -43,12 +46,11 @@ constexpr uint32_t kKStep = 16 * 128;                     // one K16 step (2 gro
 constexpr int kEpiPerQuad = 2;                           // epilogue warps per TMEM lane quadrant
 constexpr int kEpiWarps = 4 * kEpiPerQuad;
 constexpr int kThreads = 32 * (2 + kEpiWarps);
-constexpr uint32_t kTmemCols = 2 * kN;
-constexpr uint32_t kIdesc = umma::idesc_bf16_f32_mn(kM, kN);
 constexpr long long kSpin = 1ll << 22;                    // ~0.5 s with back-off
 }  // namespace
 
-constexpr int kMixedSmem = kStages * kStageBytes + 1024;
+template <int N>
+constexpr int mixed_smem() { return kStages * stage_bytes<N>() + 1024; }
 
 struct MxShared {
   uint64_t full[kStages], empty[kStages], accFull[2], accEmpty[2], drain;
@@ -68,10 +70,15 @@ __device__ __forceinline__ bool mx_wait(uint64_t *bar, uint32_t parity, MxShared
   return false;
 }
 
+// N: tile columns, 256 (the general tiles) or 64 (the next pivot block of the look-ahead, which is 64 columns wide)
+template <int N>
 __global__ void __launch_bounds__(kThreads, 1) k_update_mx(const MixTask *__restrict__ tasks, int ntasks,
                                                            const CUtensorMap *__restrict__ maps,
                                                            float *__restrict__ L32, float *__restrict__ U32,
                                                            unsigned long long *status) {
+  constexpr uint32_t kBBytes = b_bytes<N>(), kStageBytes = stage_bytes<N>(), kTmemCols = 2 * N;
+  constexpr uint32_t kIdesc = umma::idesc_bf16_f32_mn(kM, N);
+  constexpr int kN = N;
   extern __shared__ __align__(1024) uint8_t smem_mx[];
   __shared__ MxShared sh;
   if (*(volatile unsigned long long *)status != kStatusOk) return;
@@ -223,14 +230,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_update_mx(const MixTask *__rest
 }
 
 void init_mixed_attributes() {
-  cudaFuncSetAttribute(k_update_mx, cudaFuncAttributeMaxDynamicSharedMemorySize, kMixedSmem);
+  cudaFuncSetAttribute(k_update_mx<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, mixed_smem<256>());
+  cudaFuncSetAttribute(k_update_mx<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, mixed_smem<64>());
 }
 
 void launch_update_mx(const MixTask *tasks, int64_t ntasks, const CUtensorMap *maps, float *L32, float *U32,
-                      unsigned long long *status, int num_sms, cudaStream_t st) {
+                      unsigned long long *status, int num_sms, cudaStream_t st, bool narrow) {
   if (ntasks <= 0) return;
   const int grid = (int)(ntasks < num_sms ? ntasks : num_sms);
-  k_update_mx<<<grid, kThreads, kMixedSmem, st>>>(tasks, (int)ntasks, maps, L32, U32, status);
+  if (narrow)
+    k_update_mx<64><<<grid, kThreads, mixed_smem<64>(), st>>>(tasks, (int)ntasks, maps, L32, U32, status);
+  else
+    k_update_mx<256><<<grid, kThreads, mixed_smem<256>(), st>>>(tasks, (int)ntasks, maps, L32, U32, status);
 }
 
 }  // namespace amp
