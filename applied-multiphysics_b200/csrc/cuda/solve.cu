@@ -26,49 +26,11 @@
 #include "../host/plan.hpp"
 #include "devplan.cuh"
 #include "solve_small.cuh"
+#include "sync.cuh"
 
 namespace amp {
 
-constexpr int kSB = 64;                      // solve block rows
-constexpr long long kSpinLimit = 1ll << 24;  // ~ seconds with the back-off below
-
-__device__ __forceinline__ int ld_acquire(const int *p) {
-  int v;
-  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release(int *p, int v) {
-  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ void red_release_add(int *p, int v) {
-  asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-// Wait until flag == epoch; false on time-out (status set).
-__device__ bool wait_flag(const int *flag, int epoch, unsigned long long *status, int s) {
-  long long spins = 0;
-  while (ld_acquire(flag) != epoch) {
-    if (++spins > kSpinLimit) {
-      atomicMin(status, status_word(0x7fffffff, 3, s));
-      return false;
-    }
-    __nanosleep(32);
-  }
-  return true;
-}
-
-// Wait until *cnt == need; false on time-out (status set).
-__device__ bool wait_count(const int *cnt, int need, unsigned long long *status, int s) {
-  long long spins = 0;
-  while (ld_acquire(cnt) < need) {
-    if (++spins > kSpinLimit) {
-      atomicMin(status, status_word(0x7fffffff, 3, s));
-      return false;
-    }
-    __nanosleep(32);
-  }
-  return true;
-}
+constexpr int kSB = 64;  // solve block rows
 
 // ---- inverses of the diagonal blocks -----------------------------------------------------------------------------
 // One CTA per 64-column block b of the pivot columns (all supernodes): X = L_kk^-1, w x w column-major, lower part.

@@ -18,6 +18,7 @@
 #include "../host/plan.hpp"
 #include "devplan.cuh"
 #include "solve_small.cuh"
+#include "sync.cuh"
 
 namespace amp {
 
@@ -28,43 +29,6 @@ constexpr int kLdt = 66;             // shared tile row stride in doubles (even:
 constexpr int kMultiThreads = 256;
 constexpr int kMultiSmem = (2 * kKC + kMB) * kLdt * (int)sizeof(double);
 static_assert(kSolveGroup * 32 * kMQ * (int)sizeof(double) <= kMultiSmem, "small-supernode tasks: front vectors");
-constexpr long long kMSpinLimit = 1ll << 24;
-
-__device__ __forceinline__ int mld_acquire(const int *p) {
-  int v;
-  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void mst_release(int *p, int v) {
-  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ void mred_release_add(int *p, int v) {
-  asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-// bounded waits (status set to a device time-out on expiry)
-__device__ bool mwait_eq(const int *flag, int epoch, unsigned long long *status, int s) {
-  long long spins = 0;
-  while (mld_acquire(flag) != epoch) {
-    if (++spins > kMSpinLimit) {
-      atomicMin(status, status_word(0x7fffffff, 3, s));
-      return false;
-    }
-    __nanosleep(32);
-  }
-  return true;
-}
-__device__ bool mwait_ge(const int *cnt, int need, unsigned long long *status, int s) {
-  long long spins = 0;
-  while (mld_acquire(cnt) < need) {
-    if (++spins > kMSpinLimit) {
-      atomicMin(status, status_word(0x7fffffff, 3, s));
-      return false;
-    }
-    __nanosleep(32);
-  }
-  return true;
-}
-
 // acc[i][j] += sum over kk < kc of A[kk][4 ty + i] B[kk][4 tx + j]
 __device__ __forceinline__ void mm_tile(const double *__restrict__ A, const double *__restrict__ B, int kc, int ty,
                                         int tx, double (&acc)[4][4]) {
@@ -134,7 +98,7 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_fwd_multi(const int4 *__re
       for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
         const int c = P.chList[qq];
         const int need = (P.snM[c] - P.snNc[c] + kMB - 1) / kMB;
-        if (tid == 0) waitOk = mwait_ge(done + c, need, status, s);
+        if (tid == 0) waitOk = wait_count(done + c, need, status, s);
         __syncthreads();
         if (!waitOk) return false;
       }
@@ -175,7 +139,7 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_fwd_multi(const int4 *__re
     for (int ch = 0; ch < nch; ch++) {
       const int cb = ch * kKC, cw = min(kKC, ncols - cb);
       if ((cb & (kMB - 1)) == 0) {  // first chunk of a pivot block: its y values final?
-        if (tid == 0) waitOk = mwait_eq(myflags + cb / kMB, epoch, status, s);
+        if (tid == 0) waitOk = wait_flag(myflags + cb / kMB, epoch, status, s);
         __syncthreads();
         if (!waitOk) return false;
       }
@@ -207,7 +171,7 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_fwd_multi(const int4 *__re
         }
       }
       __syncthreads();
-      if (tid == 0) mred_release_add(done + s, 1);
+      if (tid == 0) red_release_add(done + s, 1);
       return true;
     }
 #pragma unroll
@@ -243,7 +207,7 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_fwd_multi(const int4 *__re
       }
     }
     __syncthreads();
-    if (tid == 0) mst_release(myflags + blk, epoch);
+    if (tid == 0) st_release(myflags + blk, epoch);
     return true;
   };
   ticket_loop(ticket, ntasks, run);
@@ -284,7 +248,7 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_bwd_multi(const int4 *__re
     int *myflags = flags + P.blkOff[s];
     const int par = P.snParent[s];
     if (par >= 0) {
-      if (tid == 0) waitOk = mwait_eq(flags + P.blkOff[par], epoch, status, s);
+      if (tid == 0) waitOk = wait_flag(flags + P.blkOff[par], epoch, status, s);
       __syncthreads();
       if (!waitOk) return false;
     }
@@ -325,7 +289,7 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_bwd_multi(const int4 *__re
     for (int ch = 0; ch < nch; ch++) {
       const bool anc = ch < nanc;
       if (!anc && ((ch - nanc) & 1) == 0) {  // first chunk of a pivot block: its x values final?
-        if (tid == 0) waitOk = mwait_eq(myflags + rb / kMB, epoch, status, s);
+        if (tid == 0) waitOk = wait_flag(myflags + rb / kMB, epoch, status, s);
         __syncthreads();
         if (!waitOk) return false;
       }
@@ -392,7 +356,7 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_bwd_multi(const int4 *__re
       }
     }
     __syncthreads();
-    if (tid == 0) mst_release(myflags + blk, epoch);
+    if (tid == 0) st_release(myflags + blk, epoch);
     return true;
   };
   ticket_loop(ticket, ntasks, run);

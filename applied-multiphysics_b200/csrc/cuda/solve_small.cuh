@@ -11,39 +11,14 @@
 #include <cstdint>
 
 #include "devplan.cuh"
+#include "sync.cuh"
 
 namespace amp {
-
-constexpr long long kSmallSpinLimit = 1ll << 24;
-
-__device__ __forceinline__ int sm_ld_acquire(const int *p) {
-  int v;
-  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void sm_st_release(int *p, int v) {
-  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ void sm_red_release_add(int *p, int v) {
-  asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
 
 // lane 0 waits (bounded) until *p == v (eq) or *p >= v; the result is broadcast to the warp
 __device__ __forceinline__ bool warp_wait(const int *p, int v, bool eq, unsigned long long *status, int s) {
   int ok = 1;
-  if ((threadIdx.x & 31) == 0) {
-    long long spins = 0;
-    for (;;) {
-      const int cur = sm_ld_acquire(p);
-      if (eq ? cur == v : cur >= v) break;
-      if (++spins > kSmallSpinLimit) {
-        atomicMin(status, status_word(0x7fffffff, 3, s));
-        ok = 0;
-        break;
-      }
-      __nanosleep(32);
-    }
-  }
+  if ((threadIdx.x & 31) == 0) ok = eq ? wait_flag(p, v, status, s) : wait_count(p, v, status, s);
   return __shfl_sync(0xffffffffu, ok, 0) != 0;
 }
 
@@ -93,7 +68,7 @@ __device__ bool small_fwd_warp(int s, const DevPlan &P, const TL *__restrict__ L
   else if (lane < m)
     T[P.snTOff[s] + lane - nc] = v;
   __syncwarp();  // orders the warp's stores before the counted arrival
-  if (lane == 0) sm_red_release_add(done + s, 1);
+  if (lane == 0) red_release_add(done + s, 1);
   return true;
 }
 
@@ -121,7 +96,7 @@ __device__ bool small_bwd_warp(int s, const DevPlan &P, const TL *__restrict__ L
   }
   if (lane < nc) y[f + lane] = x;
   __syncwarp();  // orders the warp's stores before the release
-  if (lane == 0) sm_st_release(flags + P.blkOff[s], epoch);
+  if (lane == 0) st_release(flags + P.blkOff[s], epoch);
   return true;
 }
 
@@ -169,7 +144,7 @@ __device__ bool small_fwd_warp_multi(int s, const DevPlan &P, const TL *__restri
     if (v1) dst[k1] = Vs[64 * r + k1];
   }
   __syncwarp();
-  if (lane == 0) sm_red_release_add(done + s, 1);
+  if (lane == 0) red_release_add(done + s, 1);
   return true;
 }
 
@@ -214,7 +189,7 @@ __device__ bool small_bwd_warp_multi(int s, const DevPlan &P, const TL *__restri
     if (v1) y[(int64_t)(f + r) * q + k1] = Vs[64 * r + k1];
   }
   __syncwarp();
-  if (lane == 0) sm_st_release(flags + P.blkOff[s], epoch);
+  if (lane == 0) st_release(flags + P.blkOff[s], epoch);
   return true;
 }
 
