@@ -152,6 +152,7 @@ struct amp_plan_s {
   int4 *dFwdTasks = nullptr, *dBwdTasks = nullptr, *dBwdAll = nullptr;
   int *dTinySn = nullptr, *dSmallSn = nullptr;  // small fronts per level (whole fronts by one warp / one CTA)
   int2 *dChain = nullptr;                        // chain-matrix tasks {s, b}
+  int *dInvBlocks = nullptr;                     // diagonal blocks whose inverses the solves use
   int *dRowptr = nullptr, *dColidx = nullptr;
   std::vector<int> rowptr, colidx;  // host copy of the pattern (uploaded with the schedule)
   bool uploaded = false;
@@ -271,6 +272,7 @@ void upload_plan(amp_plan *pl) {
   pl->dTinySn = m.upload(P.tinySn);
   pl->dSmallSn = m.upload(P.smallSn);
   pl->dChain = (int2 *)m.upload(P.chainTasks);
+  pl->dInvBlocks = m.upload(P.invBlocks);
 }
 
 void ensure_solve_ws(amp_factor *f, int q) {
@@ -356,8 +358,9 @@ void enqueue_small_fronts(amp_factor *f, int L, T *Lx, T *U, const amp::LdltArgs
   if (t1 == t0 && s1 == s0) return;
   const double scale = sizeof(T) / 8.0;
   timed(f, K_FRONTS, 2.0 * P.frontLvlFlops[L], P.frontLvlBytes[L] * scale, [&] {
-    amp::launch_fronts_small<T>(f->plan->dTinySn + t0, (int)(t1 - t0), f->plan->dSmallSn + s0, (int)(s1 - s0),
-                                P.smallMaxM[L], f->plan->dp, f->dValues, Lx, U, f->dStatus, la, f->stream);
+    amp::launch_fronts_small<T>(f->plan->dTinySn + t0, (int)(t1 - t0), (int)(P.tinyMid[L] - t0),
+                                f->plan->dSmallSn + s0, (int)(s1 - s0), P.smallMaxM[L], f->plan->dp, f->dValues, Lx,
+                                U, f->dStatus, la, f->stream);
   });
 }
 
@@ -426,7 +429,9 @@ void enqueue_factor(amp_factor *f) {
     }
     if (P.nflags)
       timed(f, K_DIAGINV, 0.0, 8.0 * (double)inv_elems(P),
-            [&] { amp::launch_diag_inv<float>(dp, P.nflags, f->dL32, f->dInv32, st); });
+            [&] {
+              amp::launch_diag_inv<float>(f->plan->dInvBlocks, (int)P.invBlocks.size(), dp, f->dL32, f->dInv32, st);
+            });
     enqueue_chain_mats<float>(f, f->dL32, f->dInv32, f->dMch32, f->dGch32);
     return;
   }
@@ -477,7 +482,9 @@ void enqueue_factor(amp_factor *f) {
   }
   if (P.nflags)
     timed(f, K_DIAGINV, 0.0, 16.0 * (double)inv_elems(P),
-          [&] { amp::launch_diag_inv<double>(dp, P.nflags, f->dLx, f->dInv, st); });
+          [&] {
+            amp::launch_diag_inv<double>(f->plan->dInvBlocks, (int)P.invBlocks.size(), dp, f->dLx, f->dInv, st);
+          });
   enqueue_chain_mats<double>(f, f->dLx, f->dInv, f->dMch, f->dGch);
 }
 

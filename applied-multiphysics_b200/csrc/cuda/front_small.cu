@@ -1,5 +1,5 @@
-// Small fronts: one warp (m <= 32, four fronts per CTA) or one CTA (32 < m <= 128) per front does all of the front's
-// work for its level in shared memory, in one launch per level and size class:
+// Small fronts: one warp (m <= 32, four or eight fronts per CTA) or one CTA (32 < m <= 128) per front does all of the
+// front's work for its level in shared memory, in one launch per level and size class:
 //   zero the front, add A's entries of the pivot columns (sparse.mjs:965-973), extend-add the children's update
 //   matrices in the reference's child order (sparse.mjs:974-985), factor the nc pivot columns right-looking over the
 //   whole trailing triangle (Cholesky sparse.mjs:995-1098; LDL^T with static pivot perturbation ldlt.mjs:450-562), and
@@ -16,7 +16,13 @@
 
 namespace amp {
 
-constexpr int kTinyWarps = 4;  // tiny fronts per CTA
+// Tiny fronts come in two size classes (sorted by m within each level by the plan): m <= kTinyMid with 8 warps per
+// CTA and 16 x 16 tiles, and kTinyMid < m <= 32 with 4 warps per CTA and 32 x 32 tiles, so that the many smallest fronts
+// are not held to the shared memory of the largest.
+template <int MAXM>
+constexpr int tiny_warps() {
+  return MAXM <= kTinyMid ? 8 : 4;
+}
 
 template <int G>
 __device__ __forceinline__ void group_sync() {
@@ -42,86 +48,130 @@ __device__ __forceinline__ bool small_ldlt_pivot(T &d, T tau, int &neg, int &per
   return true;
 }
 
+// Children of one front whose metadata a group holds at a time (fetched in parallel, applied in the reference's order)
+constexpr int kChildChunk = 32;
+struct ChildMeta {
+  int muc[kChildChunk];
+  int64_t ea[kChildChunk], uo[kChildChunk];
+};
+
 // The whole front of supernode s by a group of G threads (thread t) over the shared m x m column-major tile F, in the
 // compute type TC (the storage type T of L and U, or FP64: an FP32 LDL^T factor's small fronts are computed in FP64
-// and rounded once when stored, since the indefinite factor's pivots cancel). pv / flag: the group's shared scalars.
+// and rounded once when stored, since the indefinite factor's pivots cancel). cm: the group's child metadata (G > 32;
+// a warp passes its child metadata by shuffles).
+//
+// Column k of the elimination is one phase with one barrier: every thread reads the pivot F(k, k) (final since the
+// previous barrier), computes the same pivot decision and scale, writes its share of L's column k straight to Lx and
+// updates its share of the trailing triangle from the unscaled column k, which nobody writes in the phase. The
+// arithmetic is the column-scaled form's: l_i = F(i, k) / r (Cholesky, r = sqrt F(k, k)) or F(i, k) / d (LDL^T), and
+// F(i, j) -= l_i (l_j d) with d = 1 for Cholesky.
 template <class T, class TC, int G>
 __device__ void factor_front(int s, const DevPlan &P, const double *__restrict__ values, T *__restrict__ Lx,
                              T *__restrict__ U, TC *F, unsigned long long *status, const LdltArgs<T> &la, int t,
-                             TC *pv, int *flag) {
+                             ChildMeta *cm) {
+  constexpr int NW = G / 32;
+  const int warp = t >> 5, lane = t & 31;
   const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s], mu = m - nc;
   const bool ldlt = la.scal != nullptr;
   const TC tau = ldlt ? (TC)(T)la.scal[1] : TC(0);
   for (int e = t; e < m * m; e += G) F[e] = TC(0);
-  if (t == 0) *flag = 0;
   group_sync<G>();
-  // A's entries of the pivot columns: slot dst = j m + i of the L panel, each (i, j) once
-  for (int j = 0; j < nc; j++) {
-    const int p0 = P.asmColPtr[f + j], p1 = P.asmColPtr[f + j + 1];
+  // A's entries of all nc pivot columns (one contiguous CSR range): slot dst = j m + i of the L panel, each (i, j) once
+  {
+    const int p0 = P.asmColPtr[f], p1 = P.asmColPtr[f + nc];
     for (int p = p0 + t; p < p1; p += G) F[P.asmDst[p]] += (TC)(T)__ldg(values + P.asmSrc[p]);
   }
   group_sync<G>();
-  // children's update matrices, one after another (the map is injective within a child)
-  for (int q = P.chPtr[s]; q < P.chPtr[s + 1]; q++) {
-    const int c = P.chList[q];
-    const int muc = P.snM[c] - P.snNc[c];
-    if (muc <= 0) continue;
-    const int *map = P.eaMap + P.eaPtr[c];
-    const T *Uc = U + P.snUoff[c];
-    for (int e = t; e < muc * muc; e += G) {
-      const int b = e / muc, a = e - b * muc;
-      if (a >= b) F[map[b] * m + map[a]] += (TC)Uc[e];
+  // children's update matrices, one after another (the map is injective within a child); the metadata of up to
+  // kChildChunk children is fetched at once, one child per thread
+  const int q0 = P.chPtr[s], q1 = P.chPtr[s + 1];
+  for (int qb = q0; qb < q1; qb += kChildChunk) {
+    const int nq = min(kChildChunk, q1 - qb);
+    int muc = 0;
+    int64_t ea = 0, uo = 0;
+    if (warp == 0 && lane < nq) {
+      const int c = P.chList[qb + lane];
+      muc = P.snM[c] - P.snNc[c];
+      ea = P.eaPtr[c];
+      uo = P.snUoff[c];
     }
-    group_sync<G>();
-  }
-  // partial factorization of the nc pivot columns; the trailing triangle (pivot columns and U) updated per column
-  int neg = 0, pert = 0;  // thread 0
-  for (int k = 0; k < nc; k++) {
-    if (t == 0) {
-      TC d = F[k * m + k];
-      int bad = 0;
-      if (ldlt) {
-        if (!small_ldlt_pivot(d, tau, neg, pert)) bad = 2;
-        la.D[f + k] = (double)(T)d;
-        pv[0] = d;
-        pv[1] = TC(1) / d;
-        F[k * m + k] = TC(1);
+    if constexpr (G > 32) {
+      if (qb > q0) __syncthreads();  // the previous chunk's metadata is read by all warps before it is replaced
+      if (warp == 0 && lane < nq) {
+        cm->muc[lane] = muc;
+        cm->ea[lane] = ea;
+        cm->uo[lane] = uo;
+      }
+      __syncthreads();
+    }
+    for (int q = 0; q < nq; q++) {
+      int mq;
+      int64_t eq, uq;
+      if constexpr (G == 32) {
+        mq = __shfl_sync(0xffffffffu, muc, q);
+        eq = __shfl_sync(0xffffffffu, ea, q);
+        uq = __shfl_sync(0xffffffffu, uo, q);
       } else {
-        if (!(d > TC(0))) bad = 1;
-        const TC r = sqrt(d);
-        pv[0] = TC(1);
-        pv[1] = TC(1) / r;
-        F[k * m + k] = r;
+        mq = cm->muc[q];
+        eq = cm->ea[q];
+        uq = cm->uo[q];
       }
-      if (bad) {
-        atomicMin(status, status_word(f + k, bad, s));
-        *flag = 1;
+      if (mq <= 0) continue;  // group-uniform
+      const int *map = P.eaMap + eq;
+      const T *Uc = U + uq;
+      for (int e = t; e < mq * mq; e += G) {
+        const int b = e / mq, a = e - b * mq;
+        if (a >= b) F[map[b] * m + map[a]] += (TC)Uc[e];
       }
+      group_sync<G>();
     }
-    group_sync<G>();
-    if (*flag) return;  // group-uniform
-    const TC inv = pv[1], dk = pv[0];
-    TC *Fk = F + k * m;
-    for (int i = k + 1 + t; i < m; i += G) Fk[i] *= inv;
-    group_sync<G>();
-    const int w = m - k - 1;
-    for (int e = t; e < w * w; e += G) {
-      const int jj = e / w, ii = e - jj * w;
-      if (ii >= jj) {
-        const int i = k + 1 + ii, j = k + 1 + jj;
-        F[j * m + i] -= Fk[i] * (Fk[j] * dk);
+  }
+  // partial factorization of the nc pivot columns, one barrier per column; warps over the trailing columns j, lanes
+  // over the rows i >= j
+  int neg = 0, pert = 0;  // thread 0
+  T *Lp = Lx + P.snLxp[s];
+  for (int k = 0; k < nc; k++) {
+    TC d = F[k * m + k], inv, dk, diag;
+    if (ldlt) {
+      int n1 = 0, p1 = 0;
+      const bool ok = small_ldlt_pivot(d, tau, n1, p1);
+      if (!ok) {
+        if (t == 0) atomicMin(status, status_word(f + k, 2, s));
+        return;  // group-uniform: every thread saw the same pivot
       }
+      if (t == 0) {
+        neg += n1;
+        pert += p1;
+        la.D[f + k] = (double)(T)d;
+      }
+      dk = d;
+      inv = TC(1) / d;
+      diag = TC(1);
+    } else {
+      if (!(d > TC(0))) {
+        if (t == 0) atomicMin(status, status_word(f + k, 1, s));
+        return;  // group-uniform
+      }
+      const TC r = sqrt(d);
+      dk = TC(1);
+      inv = TC(1) / r;
+      diag = r;
+    }
+    const TC *Fk = F + k * m;
+    T *Lk = Lp + (int64_t)k * m;
+    for (int i = k + t; i < m; i += G) Lk[i] = (T)(i == k ? diag : Fk[i] * inv);
+    const int w = m - k - 1;
+    for (int jj = warp; jj < w; jj += NW) {
+      const int j = k + 1 + jj;
+      const TC lj = (Fk[j] * inv) * dk;
+      TC *Fj = F + j * m;
+      for (int i = j + lane; i < m; i += 32) Fj[i] -= (Fk[i] * inv) * lj;
     }
     group_sync<G>();
   }
   if (ldlt && t == 0 && (neg | pert)) {
     atomicAdd(la.counts, neg);
     atomicAdd(la.counts + 1, pert);
-  }
-  T *Lp = Lx + P.snLxp[s];
-  for (int e = t; e < nc * m; e += G) {
-    const int j = e / m, i = e - j * m;
-    if (i >= j) Lp[e] = (T)F[e];
   }
   if (mu > 0) {
     T *Up = U + P.snUoff[s];
@@ -132,20 +182,19 @@ __device__ void factor_front(int s, const DevPlan &P, const double *__restrict__
   }
 }
 
-// m <= 32: one warp per front, kTinyWarps fronts per CTA
-template <class T, class TC>
-__global__ void __launch_bounds__(32 * kTinyWarps) k_front_tiny(const int *__restrict__ fronts, int count, DevPlan P,
-                                                                const double *__restrict__ values, T *__restrict__ Lx,
-                                                                T *__restrict__ U, unsigned long long *status,
-                                                                LdltArgs<T> la) {
-  __shared__ TC F[kTinyWarps][kTinyFront * kTinyFront];
-  __shared__ TC pv[kTinyWarps][2];
-  __shared__ int flag[kTinyWarps];
+// m <= MAXM (16 or 32): one warp per front, tiny_warps<MAXM>() fronts per CTA
+template <class T, class TC, int MAXM>
+__global__ void __launch_bounds__(32 * tiny_warps<MAXM>()) k_front_tiny(const int *__restrict__ fronts, int count,
+                                                                         DevPlan P, const double *__restrict__ values,
+                                                                         T *__restrict__ Lx, T *__restrict__ U,
+                                                                         unsigned long long *status, LdltArgs<T> la) {
+  constexpr int W = tiny_warps<MAXM>();
+  __shared__ TC F[W][MAXM * MAXM];
   if (status_failed(status)) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int idx = blockIdx.x * kTinyWarps + warp;
+  const int idx = blockIdx.x * W + warp;
   if (idx >= count) return;  // warp-uniform; no CTA-wide barrier follows
-  factor_front<T, TC, 32>(fronts[idx], P, values, Lx, U, F[warp], status, la, lane, pv[warp], &flag[warp]);
+  factor_front<T, TC, 32>(fronts[idx], P, values, Lx, U, F[warp], status, la, lane, nullptr);
 }
 
 // 32 < m <= 128: one CTA per front; dynamic shared memory = the launch's largest m squared
@@ -154,11 +203,10 @@ __global__ void __launch_bounds__(256) k_front_small(const int *__restrict__ fro
                                                      const double *__restrict__ values, T *__restrict__ Lx,
                                                      T *__restrict__ U, unsigned long long *status, LdltArgs<T> la) {
   extern __shared__ __align__(16) unsigned char fs_dyn[];
-  __shared__ TC pv[2];
-  __shared__ int flag;
+  __shared__ ChildMeta cm;
   if (status_failed(status)) return;
   factor_front<T, TC, 256>(fronts[blockIdx.x], P, values, Lx, U, reinterpret_cast<TC *>(fs_dyn), status, la,
-                           threadIdx.x, pv, &flag);
+                           threadIdx.x, &cm);
 }
 
 void init_front_small_attributes() {
@@ -170,30 +218,38 @@ void init_front_small_attributes() {
                        kSmallFront * kSmallFront * (int)sizeof(double));
 }
 
+template <class T, class TC, int MAXM>
+static void launch_tiny(const int *fronts, int count, const DevPlan &P, const double *values, T *Lx, T *U,
+                        unsigned long long *status, const LdltArgs<T> &la, cudaStream_t st) {
+  constexpr int W = tiny_warps<MAXM>();
+  if (count > 0)
+    k_front_tiny<T, TC, MAXM><<<(count + W - 1) / W, 32 * W, 0, st>>>(fronts, count, P, values, Lx, U, status, la);
+}
+
 template <class T, class TC>
-static void launch_fronts_tc(const int *tiny, int ntiny, const int *small, int nsmall, int maxM, const DevPlan &P,
-                             const double *values, T *Lx, T *U, unsigned long long *status, const LdltArgs<T> &la,
-                             cudaStream_t st) {
-  if (ntiny > 0)
-    k_front_tiny<T, TC><<<(ntiny + kTinyWarps - 1) / kTinyWarps, 32 * kTinyWarps, 0, st>>>(tiny, ntiny, P, values, Lx,
-                                                                                           U, status, la);
+static void launch_fronts_tc(const int *tiny, int ntiny, int ntinyMid, const int *small, int nsmall, int maxM,
+                             const DevPlan &P, const double *values, T *Lx, T *U, unsigned long long *status,
+                             const LdltArgs<T> &la, cudaStream_t st) {
+  launch_tiny<T, TC, kTinyMid>(tiny, ntinyMid, P, values, Lx, U, status, la, st);
+  launch_tiny<T, TC, kTinyFront>(tiny + ntinyMid, ntiny - ntinyMid, P, values, Lx, U, status, la, st);
   if (nsmall > 0)
     k_front_small<T, TC><<<nsmall, 256, (size_t)maxM * maxM * sizeof(TC), st>>>(small, nsmall, P, values, Lx, U,
                                                                                 status, la);
 }
 template <class T>
-void launch_fronts_small(const int *tiny, int ntiny, const int *small, int nsmall, int maxM, const DevPlan &P,
-                         const double *values, T *Lx, T *U, unsigned long long *status, const LdltArgs<T> &la,
-                         cudaStream_t st) {
+void launch_fronts_small(const int *tiny, int ntiny, int ntinyMid, const int *small, int nsmall, int maxM,
+                         const DevPlan &P, const double *values, T *Lx, T *U, unsigned long long *status,
+                         const LdltArgs<T> &la, cudaStream_t st) {
   if (la.scal != nullptr)  // LDL^T: FP64 arithmetic whatever the storage
-    launch_fronts_tc<T, double>(tiny, ntiny, small, nsmall, maxM, P, values, Lx, U, status, la, st);
+    launch_fronts_tc<T, double>(tiny, ntiny, ntinyMid, small, nsmall, maxM, P, values, Lx, U, status, la, st);
   else
-    launch_fronts_tc<T, T>(tiny, ntiny, small, nsmall, maxM, P, values, Lx, U, status, la, st);
+    launch_fronts_tc<T, T>(tiny, ntiny, ntinyMid, small, nsmall, maxM, P, values, Lx, U, status, la, st);
 }
-template void launch_fronts_small<double>(const int *, int, const int *, int, int, const DevPlan &, const double *,
-                                          double *, double *, unsigned long long *, const LdltArgs<double> &,
-                                          cudaStream_t);
-template void launch_fronts_small<float>(const int *, int, const int *, int, int, const DevPlan &, const double *,
-                                         float *, float *, unsigned long long *, const LdltArgs<float> &, cudaStream_t);
+template void launch_fronts_small<double>(const int *, int, int, const int *, int, int, const DevPlan &,
+                                          const double *, double *, double *, unsigned long long *,
+                                          const LdltArgs<double> &, cudaStream_t);
+template void launch_fronts_small<float>(const int *, int, int, const int *, int, int, const DevPlan &,
+                                         const double *, float *, float *, unsigned long long *,
+                                         const LdltArgs<float> &, cudaStream_t);
 
 }  // namespace amp

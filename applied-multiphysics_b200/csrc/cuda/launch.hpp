@@ -23,12 +23,12 @@ template <class T>
 void launch_trsm(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, T *Lx, const unsigned long long *status,
                  __nv_bfloat16 *Shi, __nv_bfloat16 *Slo, const LdltArgs<T> &ld, cudaStream_t st);
 void launch_ldlt_tau(const double *values, const DevPlan &P, double *scal, cudaStream_t st);
-// whole small fronts of one level: tiny (m <= 32, warp per front) and small (m <= 128, CTA per front; maxM = their
-// largest m)
+// whole small fronts of one level: tiny (m <= 32, warp per front; sorted by m, the first ntinyMid with m <= 16) and
+// small (m <= 128, CTA per front; maxM = their largest m)
 template <class T>
-void launch_fronts_small(const int *tiny, int ntiny, const int *small, int nsmall, int maxM, const DevPlan &P,
-                         const double *values, T *Lx, T *U, unsigned long long *status, const LdltArgs<T> &la,
-                         cudaStream_t st);
+void launch_fronts_small(const int *tiny, int ntiny, int ntinyMid, const int *small, int nsmall, int maxM,
+                         const DevPlan &P, const double *values, T *Lx, T *U, unsigned long long *status,
+                         const LdltArgs<T> &la, cudaStream_t st);
 // narrow: 128 x 64 tiles (tasks whose columns are one 64-column pivot block), else 128 x 256
 void launch_update_mx(const MixTask *tasks, int64_t ntasks, const CUtensorMap *maps, float *L32, float *U32,
                       unsigned long long *status, int num_sms, cudaStream_t st, bool narrow = false);
@@ -38,7 +38,7 @@ void launch_update(const TileTask *tasks, int64_t ntasks, const DevPlan &P, doub
 void launch_permute_in(const double *b, double *y, const int *perm, int n, int q, cudaStream_t st);
 void launch_permute_out(const double *y, double *x, const int *perm, int n, int q, cudaStream_t st);
 template <class TL>
-void launch_diag_inv(const DevPlan &P, int nblocks, const TL *Lx, TL *Inv, cudaStream_t st);
+void launch_diag_inv(const int *blocks, int nblocks, const DevPlan &P, const TL *Lx, TL *Inv, cudaStream_t st);
 template <class TL>
 void launch_fwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
                        const TL *Mch, double *y, double *T, int *flags, int epoch, int *done,

@@ -15,7 +15,8 @@
 // needs from a block are loaded before it waits for that block's flag, so the dependency chain through a large
 // supernode costs a flag round trip, 64 y values and a 64 x 64 product per block.
 //
-// The inverses of the diagonal blocks are computed once per factorization, after it (k_diag_inv, all blocks in
+// The inverses of the diagonal blocks are computed once per factorization, after it (k_diag_inv, all blocks of the
+// supernodes solved by block tasks (m > 32; the smaller ones are solved by one warp each, by substitution) in
 // parallel): column j of X = L_kk^-1 by forward substitution, X(j, j) = 1 / L(j, j),
 // X(i, j) = -(sum_{t=j}^{i-1} L(i, t) X(t, j)) X(i, i). Solving with X instead of by substitution changes the result
 // by rounding only (the FP64 path stays within 1e-12 of the oracle).
@@ -36,10 +37,11 @@ constexpr int kSB = 64;  // solve block rows
 // One CTA per 64-column block b of the pivot columns (all supernodes): X = L_kk^-1, w x w column-major, lower part.
 // Thread j computes column j; L is read through the read-only cache.
 template <class TL>
-__global__ void __launch_bounds__(kSB) k_diag_inv(DevPlan P, const TL *__restrict__ Lx, TL *__restrict__ Inv) {
+__global__ void __launch_bounds__(kSB) k_diag_inv(const int *__restrict__ blocks, DevPlan P, const TL *__restrict__ Lx,
+                                                  TL *__restrict__ Inv) {
   __shared__ double Xs[kSB][kSB + 1];
   __shared__ double dinv[kSB];
-  const int b = blockIdx.x;
+  const int b = blocks[blockIdx.x];
   int lo = 0, hi = P.nsuper;  // supernode s with blkOff[s] <= b < blkOff[s + 1]
   while (hi - lo > 1) {
     const int mid = (lo + hi) >> 1;
@@ -462,8 +464,8 @@ int num_sms();
 static int solve_grid(int ntasks) { return ntasks < 3 * num_sms() ? ntasks : 3 * num_sms(); }
 
 template <class TL>
-void launch_diag_inv(const DevPlan &P, int nblocks, const TL *Lx, TL *Inv, cudaStream_t st) {
-  if (nblocks > 0) k_diag_inv<TL><<<nblocks, kSB, 0, st>>>(P, Lx, Inv);
+void launch_diag_inv(const int *blocks, int nblocks, const DevPlan &P, const TL *Lx, TL *Inv, cudaStream_t st) {
+  if (nblocks > 0) k_diag_inv<TL><<<nblocks, kSB, 0, st>>>(blocks, P, Lx, Inv);
 }
 template <class TL>
 void launch_chain_mats(const int2 *tasks, int ntasks, const DevPlan &P, const TL *Lx, const TL *Inv, TL *Mch, TL *Gch,
@@ -486,8 +488,8 @@ void launch_bwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan
     k_bwd_blocks<TL><<<solve_grid(ntasks), 256, kBwdSmem, st>>>(tasks, ntasks, ticket, P, Lx, Inv, Gch, Dpiv, y, flags,
                                                                  epoch, status);
 }
-template void launch_diag_inv<double>(const DevPlan &, int, const double *, double *, cudaStream_t);
-template void launch_diag_inv<float>(const DevPlan &, int, const float *, float *, cudaStream_t);
+template void launch_diag_inv<double>(const int *, int, const DevPlan &, const double *, double *, cudaStream_t);
+template void launch_diag_inv<float>(const int *, int, const DevPlan &, const float *, float *, cudaStream_t);
 template void launch_chain_mats<double>(const int2 *, int, const DevPlan &, const double *, const double *, double *,
                                         double *, cudaStream_t);
 template void launch_chain_mats<float>(const int2 *, int, const DevPlan &, const float *, const float *, float *,

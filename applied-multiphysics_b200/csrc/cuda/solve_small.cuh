@@ -125,18 +125,21 @@ __device__ bool small_fwd_warp_multi(int s, const DevPlan &P, const TL *__restri
       if (v1) Vs[64 * r + k1] += __ldcg(tc + (int64_t)a * q + k1);
     }
   }
+  // column k of L is held one row per lane (loaded one column ahead) and broadcast by shuffles
   const TL *Lp = Lx + P.snLxp[s];
+  double lcol = lane < m ? (double)Lp[lane] : 0.0;
   for (int k = 0; k < nc; k++) {
-    const TL *Lk = Lp + (int64_t)k * m;
-    const double lkk = (double)Lk[k];
+    const double lnext = (k + 1 < nc && lane < m) ? (double)Lp[(int64_t)(k + 1) * m + lane] : 0.0;
+    const double lkk = __shfl_sync(0xffffffffu, lcol, k);
     const double y0 = v0 ? Vs[64 * k + k0] / lkk : 0.0, y1 = v1 ? Vs[64 * k + k1] / lkk : 0.0;
     if (v0) Vs[64 * k + k0] = y0;
     if (v1) Vs[64 * k + k1] = y1;
     for (int r = k + 1; r < m; r++) {
-      const double l = (double)Lk[r];
+      const double l = __shfl_sync(0xffffffffu, lcol, r);
       if (v0) Vs[64 * r + k0] -= l * y0;
       if (v1) Vs[64 * r + k1] -= l * y1;
     }
+    lcol = lnext;
   }
   for (int r = 0; r < m; r++) {
     double *dst = r < nc ? y + (int64_t)(f + r) * q : T + (P.snTOff[s] + r - nc) * q;
@@ -171,16 +174,19 @@ __device__ bool small_bwd_warp_multi(int s, const DevPlan &P, const TL *__restri
       Vs[64 * r + k1] = (r < nc && Dpiv) ? xv / d : xv;
     }
   }
+  // column k of L one row per lane (loaded one column ahead), broadcast by shuffles
   const TL *Lp = Lx + P.snLxp[s];
+  double lcol = (nc > 0 && lane < m) ? (double)Lp[(int64_t)(nc - 1) * m + lane] : 0.0;
   for (int k = nc - 1; k >= 0; k--) {
-    const TL *Lk = Lp + (int64_t)k * m;
+    const double lnext = (k > 0 && lane < m) ? (double)Lp[(int64_t)(k - 1) * m + lane] : 0.0;
     double s0 = 0.0, s1 = 0.0;
     for (int r = k + 1; r < m; r++) {
-      const double l = (double)Lk[r];
+      const double l = __shfl_sync(0xffffffffu, lcol, r);
       if (v0) s0 += l * Vs[64 * r + k0];
       if (v1) s1 += l * Vs[64 * r + k1];
     }
-    const double lkk = (double)Lk[k];
+    const double lkk = __shfl_sync(0xffffffffu, lcol, k);
+    lcol = lnext;
     if (v0) Vs[64 * k + k0] = (Vs[64 * k + k0] - s0) / lkk;
     if (v1) Vs[64 * k + k1] = (Vs[64 * k + k1] - s1) / lkk;
   }

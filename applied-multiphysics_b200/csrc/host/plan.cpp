@@ -194,6 +194,7 @@ void build_plan(const Symbolic &S, Plan &P) {
   P.uLvlPtr.assign(1, 0);
   P.lvlStepPtr.assign(P.nlevels + 1, 0);
   P.tinyPtr.assign(1, 0);
+  P.tinyMid.clear();
   P.smallPtr.assign(1, 0);
   auto isSmall = [&](int s) { return P.snM[s] <= kSmallFront; };
   for (int L = 0; L < P.nlevels; L++) {
@@ -216,6 +217,12 @@ void build_plan(const Symbolic &S, Plan &P) {
         P.smallSn.push_back(s);
         maxM = std::max(maxM, P.snM[s]);
       }
+    }
+    {
+      auto t0 = P.tinySn.begin() + P.tinyPtr.back();
+      std::stable_sort(t0, P.tinySn.end(), [&](int a, int b) { return P.snM[a] < P.snM[b]; });
+      P.tinyMid.push_back(std::partition_point(t0, P.tinySn.end(), [&](int a) { return P.snM[a] <= kTinyMid; }) -
+                          P.tinySn.begin());
     }
     P.tinyPtr.push_back((int64_t)P.tinySn.size());
     P.smallPtr.push_back((int64_t)P.smallSn.size());
@@ -343,6 +350,9 @@ void build_plan(const Symbolic &S, Plan &P) {
   // Supernodes with m <= kTinyFront are solved whole by one warp: tasks {first, count, 2} over solveSmall, up to
   // kSolveGroup supernodes of one level per task, listed before the level's block tasks.
   auto solveSmall = [&](int s) { return P.snM[s] <= kTinyFront; };
+  for (int s = 0; s < ns; s++)
+    if (!solveSmall(s))
+      for (int b = P.blkOff[s]; b < P.blkOff[s + 1]; b++) P.invBlocks.push_back(b);
   for (int L = 0; L < P.nlevels; L++) {
     const int64_t g0 = (int64_t)P.solveSmall.size();
     for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++)

@@ -24,6 +24,7 @@ constexpr int kTileM = 128;    // trailing-update tile rows
 constexpr int kAsmCols = 8;    // front columns per assembly task (one per warp)
 constexpr int kTrsmRows = 64;  // panel rows per TRSM task
 constexpr int kTinyFront = 32;    // fronts with m <= 32: one warp per front does the whole front (front_small.cu)
+constexpr int kTinyMid = 16;      // the smaller tiny class (m <= 16: 16 x 16 tiles, eight fronts per CTA)
 constexpr int kSmallFront = 128;  // fronts with 32 < m <= 128: one CTA per front does the whole front
 constexpr int kSolveGroup = 4;    // supernodes with m <= kTinyFront per solve task (one warp each)
 
@@ -94,6 +95,7 @@ struct Plan {
   // are tinySn[tinyPtr[L] .. tinyPtr[L + 1]), small ones smallSn[smallPtr[L] ..], the largest m of those smallMaxM[L]
   std::vector<int> tinySn, smallSn, smallMaxM;
   std::vector<int64_t> tinyPtr, smallPtr;
+  std::vector<int64_t> tinyMid;  // each level's tiny fronts are sorted by m; those from tinyMid[L] on have m > kTinyMid
   std::vector<double> frontLvlFlops, frontLvlBytes;  // algorithmic work of each level's small fronts
   // solve: rows below of each supernode (Si[Sp[s] + nc ..]) and the perm
   std::vector<int> perm, Sp, Si;
@@ -106,6 +108,7 @@ struct Plan {
   std::vector<int> diagSlot;        // CSR slot of each diagonal entry of A (LDL^T pivot scale)
   std::vector<int> fwdTasks, bwdTasks;  // int4 records, flattened
   std::vector<int> solveSmall;          // supernodes solved whole by one warp, grouped by level (tasks of kind 2)
+  std::vector<int> invBlocks;           // diagonal blocks (flag index) whose inverse the block-task solves use
   std::vector<int> chainTasks;          // {s, b} pairs: every diagonal block of a supernode with two or more
   std::vector<int> fwdLvlPtr, bwdLvlPtr;
   std::vector<int> bwdAll;  // backward tasks of all levels, top-down (one launch)
