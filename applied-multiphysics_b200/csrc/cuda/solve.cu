@@ -129,6 +129,7 @@ __global__ void __launch_bounds__(256) k_chain_mats(const int2 *__restrict__ tas
 }
 
 // ---- forward block tasks -----------------------------------------------------------------------------------------
+constexpr int kChPre = 64;  // children located and waited for at once by a forward block task
 // task: .x supernode, .y block, .z kind (0 diagonal, 1 below, 2 small supernodes)
 // One launch for the whole sweep: tasks are listed level by level (leaves first), so every wait is on a task with an
 // earlier ticket. Every task first waits for the supernode's children and gathers its own rows of the front vector
@@ -146,6 +147,8 @@ __global__ void __launch_bounds__(256, 3) k_fwd_blocks(const int4 *__restrict__ 
   __shared__ double red[4][kSB];
   __shared__ double rk[kSB];
   __shared__ double Xs[kSB][kSB + 1];
+  __shared__ int2 chA[kChPre];
+  __shared__ int64_t chMap[kChPre], chT[kChPre];
   auto run = [&](const int tkv) -> bool {
     const int4 t = tasks[tkv];
     if (t.z == 2) {  // up to kSolveGroup supernodes with m <= 32, one warp each
@@ -174,37 +177,45 @@ __global__ void __launch_bounds__(256, 3) k_fwd_blocks(const int4 *__restrict__ 
       const TL *X = Inv + P.invOff[P.blkOff[s] + blk];
       for (int e = tid; e < rows * rows; e += blockDim.x) Xs[e % rows][e / rows] = (double)X[e];
     }
-    // children complete?
-    for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
-      const int c = P.chList[qq];
-      const int need = (P.snM[c] - P.snNc[c] + kSB - 1) / kSB;
-      if (tid == 0) waitOk = wait_count(done + c, need, status, s);
-      __syncthreads();
-      if (!waitOk) return false;
-    }
-    // this task's rows of v: pivot rows start from y; the children's entries mapping to rows [r0, r0 + rows) added in
-    // child order (the map is increasing, so they form one range per child)
+    // this task's rows of v: pivot rows start from y; the children's entries mapping to rows [r0, r0 + rows) are added
+    // in child order (the map is increasing, so they form one range per child). Up to kChPre children at a time, one
+    // per thread: the thread locates the child's range (static) and then waits for the child, so that the searches
+    // and the waits of all children overlap.
     if (tid < kSB) rk[tid] = (tid < rows && r0 + tid < nc) ? y[f + r0 + tid] : 0.0;
-    __syncthreads();
-    for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
-      const int c = P.chList[qq];
-      const int muc = P.snM[c] - P.snNc[c];
-      const int *map = P.eaMap + P.eaPtr[c];
-      int lo = 0, hi = muc;
-      while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (map[mid] < r0) lo = mid + 1; else hi = mid;
+    const int q0 = P.chPtr[s], q1 = P.chPtr[s + 1];
+    for (int qb = q0; qb < q1; qb += kChPre) {
+      const int nq = min(kChPre, q1 - qb);
+      if (qb > q0) __syncthreads();  // the previous chunk's ranges are consumed
+      int ok = 1;
+      if (tid < nq) {
+        const int c = P.chList[qb + tid];
+        const int muc = P.snM[c] - P.snNc[c];
+        const int *map = P.eaMap + P.eaPtr[c];
+        int lo = 0, hi = muc;
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (map[mid] < r0) lo = mid + 1; else hi = mid;
+        }
+        const int a0 = lo;
+        hi = muc;
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (map[mid] < r0 + rows) lo = mid + 1; else hi = mid;
+        }
+        chA[tid] = make_int2(a0, lo);
+        chMap[tid] = P.eaPtr[c];
+        chT[tid] = P.snTOff[c];
+        ok = wait_count(done + c, (muc + kSB - 1) / kSB, status, s);
       }
-      const int a0 = lo;
-      hi = muc;
-      while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (map[mid] < r0 + rows) lo = mid + 1; else hi = mid;
+      if (!__syncthreads_and(ok)) return false;  // block-uniform
+      for (int q = 0; q < nq; q++) {
+        const int *map = P.eaMap + chMap[q];
+        const double *tc = T + chT[q];
+        for (int a = chA[q].x + tid; a < chA[q].y; a += blockDim.x) rk[map[a] - r0] += __ldcg(tc + a);
+        __syncthreads();
       }
-      const double *tc = T + P.snTOff[c];
-      for (int a = a0 + tid; a < lo; a += blockDim.x) rk[map[a] - r0] += __ldcg(tc + a);
-      __syncthreads();
     }
+    if (q0 == q1) __syncthreads();
     const double vreg = tid < kSB ? rk[tid] : 0.0;
     // sums over the columns of the finished blocks; a block's L values are loaded before waiting for its flag
     double acc = 0.0;
