@@ -358,26 +358,41 @@ __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ 
         }
       }
     }
-    // one launch for the whole sweep (levels top-down): the rows below this supernode are final once its parent's
-    // first pivot block (the parent's last backward task) is
-    const int par = P.snParent[s];
-    if (par >= 0) {
-      if (tid == 0) waitOk = wait_flag(flags + P.blkOff[par], epoch, status, s);
-      __syncthreads();
-      if (!waitOk) return false;
-    }
     double acc[8];
 #pragma unroll
     for (int u = 0; u < 8; u++) acc[u] = 0.0;
-    // rows of the supernode below its pivot columns: ancestors, final
-    for (int r = nc + lane; r < m; r += 32) {
-      const double xr = __ldcg(y + rowsOf[r]);
+    // Rows of the supernode below its pivot columns (ancestors' rows, ascending), from the last down in chunks of 32
+    // (lane = row; warps over the columns). One launch covers the whole sweep (levels top-down), and the parent's
+    // pivot blocks become final from its last block down, each block's flag set only after the next one's (rows
+    // above the parent's pivot columns are final before its last block is). So a chunk waits only for the parent's
+    // block that holds its first row, and the chunks of rows in the parent's later blocks are summed while the
+    // parent's earlier blocks are still being solved. Each warp waits on its own (lane 0, bounded).
+    bool wok = true;
+    const int mu = m - nc;
+    if (mu > 0) {
+      const int par = P.snParent[s];
+      const int fp = P.snF[par], ncp = P.snNc[par], nbp = (ncp + kSB - 1) / kSB;
+      const int *pflags = flags + P.blkOff[par];
+      int ready = nbp;  // the parent's blocks >= ready are known final (warp-uniform)
+      for (int rb = nc + ((mu - 1) / 32) * 32; rb >= nc; rb -= 32) {
+        const int g0 = rowsOf[rb];  // the chunk's first row (>= fp: every row below is a row of the parent's front)
+        const int k = g0 < fp + ncp ? max(0, g0 - fp) / kSB : nbp - 1;
+        if (k < ready && wok) {
+          wok = warp_wait(pflags + k, epoch, true, status, s);
+          ready = k;
+        }
+        const int r = rb + lane;
+        if (r < m && wok) {
+          const double xr = __ldcg(y + rowsOf[r]);
 #pragma unroll
-      for (int u = 0; u < 8; u++) {
-        const int c = warp + 8 * u;
-        if (c < w) acc[u] += (double)Lp[(int64_t)(c0 + c) * m + r] * xr;
+          for (int u = 0; u < 8; u++) {
+            const int c = warp + 8 * u;
+            if (c < w) acc[u] += (double)Lp[(int64_t)(c0 + c) * m + r] * xr;
+          }
+        }
       }
     }
+    if (!__syncthreads_and(wok)) return false;  // block-uniform
     // pivot blocks after the next one, as they become final; a block's L values are loaded before its wait
     TL lv[2][8];
     auto load_block = [&](int rb, TL (&dst)[2][8]) {

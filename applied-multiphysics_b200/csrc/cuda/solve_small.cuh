@@ -15,11 +15,14 @@
 
 namespace amp {
 
-// lane 0 waits (bounded) until *p == v (eq) or *p >= v; the result is broadcast to the warp
+// lane 0 waits (bounded) until *p == v (eq) or *p >= v; the result is broadcast to the warp, and the warp barrier
+// orders the other lanes' later loads after lane 0's acquire
 __device__ __forceinline__ bool warp_wait(const int *p, int v, bool eq, unsigned long long *status, int s) {
   int ok = 1;
   if ((threadIdx.x & 31) == 0) ok = eq ? wait_flag(p, v, status, s) : wait_count(p, v, status, s);
-  return __shfl_sync(0xffffffffu, ok, 0) != 0;
+  ok = __shfl_sync(0xffffffffu, ok, 0);
+  __syncwarp();
+  return ok != 0;
 }
 
 // children of s complete in the forward sweep (their pass-up vectors written)
