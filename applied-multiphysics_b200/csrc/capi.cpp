@@ -199,6 +199,7 @@ struct amp_factor_s {
   double *dY = nullptr, *dV = nullptr, *dT = nullptr, *dB = nullptr, *dX = nullptr, *dR = nullptr, *dDX = nullptr,
          *dNorms = nullptr;
   int *dFlags = nullptr, *dTickets = nullptr;  // solve block ready flags (epoch-stamped) and per-launch tickets
+  unsigned long long *dHand = nullptr;          // chain hand-off of consecutive diagonal blocks (epoch-tagged words)
   int *dDone = nullptr;                         // forward: finished below tasks per supernode
   DevMem gmem;                                  // GMRES workspace (Krylov and preconditioned bases), grown on demand
   int gmresCap = 0;
@@ -504,19 +505,21 @@ void device_solve_permuted(amp_factor *f) {
   timed(f, K_FORWARD, 2.0 * (double)P.nnzLStored, lbytes, [&] {
     if (f->dL32)
       amp::launch_fwd_blocks<float>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->dL32, f->dInv32,
-                                    ldlt ? nullptr : f->dMch32, f->dY, f->dT, f->dFlags, efwd, f->dDone,
+                                    ldlt ? nullptr : f->dMch32, f->dY, f->dT, f->dFlags, f->dHand, efwd, f->dDone,
                                     f->dSolveStatus, st);
     else
       amp::launch_fwd_blocks<double>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->dLx, f->dInv, ldlt ? nullptr : f->dMch,
-                                     f->dY, f->dT, f->dFlags, efwd, f->dDone, f->dSolveStatus, st);
+                                     f->dY, f->dT, f->dFlags, f->dHand, efwd, f->dDone, f->dSolveStatus, st);
   });
   timed(f, K_BACKWARD, 2.0 * (double)P.nnzLStored, lbytes, [&] {
     if (f->dL32)
       amp::launch_bwd_blocks<float>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dL32, f->dInv32,
-                                    ldlt ? nullptr : f->dGch32, Dp, f->dY, f->dFlags, ebwd, f->dSolveStatus, st);
+                                    ldlt ? nullptr : f->dGch32, Dp, f->dY, f->dFlags, f->dHand, ebwd, f->dSolveStatus,
+                                    st);
     else
       amp::launch_bwd_blocks<double>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dLx, f->dInv,
-                                     ldlt ? nullptr : f->dGch, Dp, f->dY, f->dFlags, ebwd, f->dSolveStatus, st);
+                                     ldlt ? nullptr : f->dGch, Dp, f->dY, f->dFlags, f->dHand, ebwd, f->dSolveStatus,
+                                     st);
   });
 }
 
@@ -885,6 +888,11 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
       f->dStatus = f->mem.alloc<unsigned long long>(1);
       f->dFlags = f->mem.alloc<int>((size_t)P.nflags);
       ck(cudaMemset(f->dFlags, 0, sizeof(int) * std::max(1, P.nflags)), "memset flags");
+      {  // two tagged words per value of a 64-row block, one slot per pair of consecutive diagonal blocks
+        const size_t hw = std::max<size_t>(1, (size_t)std::max(0, P.nflags - P.nsuper) * 128);
+        f->dHand = f->mem.alloc<unsigned long long>(hw);
+        ck(cudaMemset(f->dHand, 0, sizeof(unsigned long long) * hw), "memset hand-off");
+      }
       f->dTickets = f->mem.alloc<int>(2);
       f->dDone = f->mem.alloc<int>((size_t)std::max(1, P.nsuper));
       f->dSolveStatus = f->mem.alloc<unsigned long long>(1);

@@ -41,12 +41,12 @@ template <class TL>
 void launch_diag_inv(const int *blocks, int nblocks, const DevPlan &P, const TL *Lx, TL *Inv, cudaStream_t st);
 template <class TL>
 void launch_fwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
-                       const TL *Mch, double *y, double *T, int *flags, int epoch, int *done,
+                       const TL *Mch, double *y, double *T, int *flags, unsigned long long *hand, int epoch, int *done,
                        unsigned long long *status, cudaStream_t st);
 template <class TL>
 void launch_bwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
-                       const TL *Gch, const double *Dpiv, double *y, int *flags, int epoch, unsigned long long *status,
-                       cudaStream_t st);
+                       const TL *Gch, const double *Dpiv, double *y, int *flags, unsigned long long *hand, int epoch,
+                       unsigned long long *status, cudaStream_t st);
 // M_b = X_b L[b, b-1] and G_b = L[b+1, b] X_b of consecutive diagonal blocks (tasks {s, b}), after launch_diag_inv
 template <class TL>
 void launch_chain_mats(const int2 *tasks, int ntasks, const DevPlan &P, const TL *Lx, const TL *Inv, TL *Mch, TL *Gch,

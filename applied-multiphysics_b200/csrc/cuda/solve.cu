@@ -141,9 +141,11 @@ template <class TL>
 __global__ void __launch_bounds__(256, 3) k_fwd_blocks(const int4 *__restrict__ tasks, int ntasks, int *__restrict__ ticket,
                                                     DevPlan P, const TL *__restrict__ Lx, const TL *__restrict__ Inv,
                                                     const TL *__restrict__ Mch, double *__restrict__ y,
-                                                    double *__restrict__ T, int *__restrict__ flags, int epoch,
+                                                    double *__restrict__ T, int *__restrict__ flags,
+                                                    unsigned long long *__restrict__ hand, int epoch,
                                                     int *__restrict__ done, unsigned long long *status) {
   __shared__ int tk, waitOk;
+  __shared__ unsigned hw[2 * kSB];
   __shared__ double red[4][kSB];
   __shared__ double rk[kSB];
   __shared__ double Xs[kSB][kSB + 1];
@@ -276,19 +278,34 @@ __global__ void __launch_bounds__(256, 3) k_fwd_blocks(const int4 *__restrict__ 
     __syncthreads();
     const double wv = tid < rows ? (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]) : 0.0;
     double yv = wv;
-    if (chain && blk > 0) {  // the chain step: wait for block b - 1, then y_b = w_b - M_b y_{b-1}
-      if (tid == 0) waitOk = wait_flag(myflags + blk - 1, epoch, status, s);
-      __syncthreads();
-      if (!waitOk) return false;
-      const double *yp = y + f + r0 - kSB;
+    // the chain step: y_b = w_b - M_b y_{b-1}, with y_{b-1} taken from block b - 1's tagged words (hand, two per
+    // value, slot of M_b) as soon as they carry this sweep's epoch, without waiting for its flag
+    const int nb = (nc + kSB - 1) / kSB;
+    const int64_t slot0 = P.blkOff[s] - s;  // this supernode's chain slots: slot0 + b for the pair (b, b + 1)
+    if (chain && blk > 0) {
+      int ok = 1;
+      if (tid < 2 * kSB) {
+        unsigned lo = 0;
+        ok = wait_tagged(hand + (slot0 + blk - 1) * 2 * kSB + tid, epoch, status, s, lo);
+        hw[tid] = lo;
+      }
+      if (!__syncthreads_and(ok)) return false;  // block-uniform
       double a3 = 0.0;
 #pragma unroll
-      for (int u = 0; u < 16; u++) a3 += (double)mv[u] * __ldcg(yp + part + 4 * u);
+      for (int u = 0; u < 16; u++) {
+        const int k = part + 4 * u;
+        a3 += (double)mv[u] * untag(hw[2 * k], hw[2 * k + 1]);
+      }
       red[part][row] = a3;
       __syncthreads();
       if (tid < rows) yv = wv - ((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]));
     }
-    if (tid < rows) y[f + r0 + tid] = yv;
+    if (tid < rows) {
+      if (chain && blk + 1 < nb) st_tagged(hand + (slot0 + blk) * 2 * kSB + 2 * tid, epoch, yv);
+      y[f + r0 + tid] = yv;
+    }
+    // every reader of a forward flag acquires each block's flag it needs on its own (the chain step, which takes
+    // y_{b-1} from the tagged words, is the one reader that does not), so block b's flag need not stand for b - 1
     __syncthreads();
     if (tid == 0) st_release(myflags + blk, epoch);  // after the barrier: the CTA's stores are ordered before it
     return true;
@@ -313,9 +330,11 @@ template <class TL>
 __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ tasks, int ntasks, int *__restrict__ ticket,
                                                     DevPlan P, const TL *__restrict__ Lx, const TL *__restrict__ Inv,
                                                     const TL *__restrict__ Gch, const double *__restrict__ Dpiv,
-                                                    double *__restrict__ y, int *__restrict__ flags, int epoch,
+                                                    double *__restrict__ y, int *__restrict__ flags,
+                                                    unsigned long long *__restrict__ hand, int epoch,
                                                     unsigned long long *status) {
   __shared__ int tk, waitOk;
+  __shared__ unsigned hw[2 * kSB];
   __shared__ double red[4][kSB];
   __shared__ double red0[kSB];
   __shared__ double xs[kSB];
@@ -450,11 +469,16 @@ __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ 
     __syncthreads();
     const double wv = tid < w ? (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]) : 0.0;
     double xv = wv;
-    if (hasNext) {  // the chain step: wait for block b + 1, then x_b = w_b - G_b^T x_{b+1}
-      if (tid == 0) waitOk = wait_flag(myflags + blk + 1, epoch, status, s);
-      __syncthreads();
-      if (!waitOk) return false;  // block-uniform
-      if (tid < kSB) xs[tid] = tid < wn ? __ldcg(y + f + rn + tid) : 0.0;
+    const int64_t slot0 = P.blkOff[s] - s;  // this supernode's chain slots: slot0 + b for the pair (b, b + 1)
+    if (hasNext) {  // the chain step: x_b = w_b - G_b^T x_{b+1}, x_{b+1} from block b + 1's tagged words
+      int ok = 1;
+      if (tid < 2 * wn) {
+        unsigned lo = 0;
+        ok = wait_tagged(hand + (slot0 + blk) * 2 * kSB + tid, epoch, status, s, lo);
+        hw[tid] = lo;
+      }
+      if (!__syncthreads_and(ok)) return false;  // block-uniform
+      if (tid < kSB) xs[tid] = tid < wn ? untag(hw[2 * tid], hw[2 * tid + 1]) : 0.0;
       __syncthreads();
       const int c = tid & (kSB - 1), part = tid >> 6;
       double a3 = 0.0;
@@ -464,9 +488,16 @@ __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ 
       __syncthreads();
       if (tid < w) xv = wv - ((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]));
     }
-    if (tid < w) y[f + c0 + tid] = xv;
-    __syncthreads();
-    if (tid == 0) st_release(myflags + blk, epoch);  // after the barrier: the CTA's stores of x_b are ordered before
+    if (tid < w) {
+      if (chain && blk > 0) st_tagged(hand + (slot0 + blk - 1) * 2 * kSB + 2 * tid, epoch, xv);
+      y[f + c0 + tid] = xv;
+    }
+    // block b's flag stands for every later block (the children's rows-below waits rely on it): acquire block
+    // b + 1's flag, taken above without an acquire, before releasing ours after the barrier
+    int fok = 1;
+    if (tid == 0 && hasNext) fok = wait_flag(myflags + blk + 1, epoch, status, s);
+    if (!__syncthreads_and(fok)) return false;  // block-uniform
+    if (tid == 0) st_release(myflags + blk, epoch);
     return true;
   };
   for (;;) {
@@ -500,19 +531,19 @@ void launch_chain_mats(const int2 *tasks, int ntasks, const DevPlan &P, const TL
 }
 template <class TL>
 void launch_fwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
-                       const TL *Mch, double *y, double *T, int *flags, int epoch, int *done,
+                       const TL *Mch, double *y, double *T, int *flags, unsigned long long *hand, int epoch, int *done,
                        unsigned long long *status, cudaStream_t st) {
   if (ntasks > 0)
-    k_fwd_blocks<TL><<<solve_grid(ntasks), 256, 0, st>>>(tasks, ntasks, ticket, P, Lx, Inv, Mch, y, T, flags, epoch,
-                                                         done, status);
+    k_fwd_blocks<TL><<<solve_grid(ntasks), 256, 0, st>>>(tasks, ntasks, ticket, P, Lx, Inv, Mch, y, T, flags, hand,
+                                                         epoch, done, status);
 }
 template <class TL>
 void launch_bwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
-                       const TL *Gch, const double *Dpiv, double *y, int *flags, int epoch, unsigned long long *status,
-                       cudaStream_t st) {
+                       const TL *Gch, const double *Dpiv, double *y, int *flags, unsigned long long *hand, int epoch,
+                       unsigned long long *status, cudaStream_t st) {
   if (ntasks > 0)
     k_bwd_blocks<TL><<<solve_grid(ntasks), 256, kBwdSmem, st>>>(tasks, ntasks, ticket, P, Lx, Inv, Gch, Dpiv, y, flags,
-                                                                 epoch, status);
+                                                                 hand, epoch, status);
 }
 template void launch_diag_inv<double>(const int *, int, const DevPlan &, const double *, double *, cudaStream_t);
 template void launch_diag_inv<float>(const int *, int, const DevPlan &, const float *, float *, cudaStream_t);
@@ -521,16 +552,16 @@ template void launch_chain_mats<double>(const int2 *, int, const DevPlan &, cons
 template void launch_chain_mats<float>(const int2 *, int, const DevPlan &, const float *, const float *, float *,
                                        float *, cudaStream_t);
 template void launch_fwd_blocks<double>(const int4 *, int, int *, const DevPlan &, const double *, const double *,
-                                        const double *, double *, double *, int *, int, int *, unsigned long long *,
-                                        cudaStream_t);
+                                        const double *, double *, double *, int *, unsigned long long *, int, int *,
+                                        unsigned long long *, cudaStream_t);
 template void launch_fwd_blocks<float>(const int4 *, int, int *, const DevPlan &, const float *, const float *,
-                                       const float *, double *, double *, int *, int, int *, unsigned long long *,
-                                       cudaStream_t);
+                                       const float *, double *, double *, int *, unsigned long long *, int, int *,
+                                       unsigned long long *, cudaStream_t);
 template void launch_bwd_blocks<double>(const int4 *, int, int *, const DevPlan &, const double *, const double *,
-                                        const double *, const double *, double *, int *, int, unsigned long long *,
-                                        cudaStream_t);
+                                        const double *, const double *, double *, int *, unsigned long long *, int,
+                                        unsigned long long *, cudaStream_t);
 template void launch_bwd_blocks<float>(const int4 *, int, int *, const DevPlan &, const float *, const float *,
-                                       const float *, const double *, double *, int *, int, unsigned long long *,
-                                       cudaStream_t);
+                                       const float *, const double *, double *, int *, unsigned long long *, int,
+                                       unsigned long long *, cudaStream_t);
 
 }  // namespace amp
