@@ -393,22 +393,40 @@ __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ 
       const int fp = P.snF[par], ncp = P.snNc[par], nbp = (ncp + kSB - 1) / kSB;
       const int *pflags = flags + P.blkOff[par];
       int ready = nbp;  // the parent's blocks >= ready are known final (warp-uniform)
-      for (int rb = nc + ((mu - 1) / 32) * 32; rb >= nc; rb -= 32) {
-        const int g0 = rowsOf[rb];  // the chunk's first row (>= fp: every row below is a row of the parent's front)
+      // the chunk's row indices and L values (static) are loaded one chunk ahead, so that a chunk waits for one load
+      // round trip (its x values) after its flag
+      int rb = nc + ((mu - 1) / 32) * 32;
+      int idx = rb + lane < m ? rowsOf[rb + lane] : -1;
+      TL lc[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int c = warp + 8 * u;
+        lc[u] = (idx >= 0 && c < w) ? Lp[(int64_t)(c0 + c) * m + rb + lane] : (TL)0;
+      }
+      for (; rb >= nc; rb -= 32) {
+        const int rbn = rb - 32;  // the next chunk (rows below rb, all < m)
+        const int idxn = rbn >= nc ? rowsOf[rbn + lane] : -1;
+        TL ln[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const int c = warp + 8 * u;
+          ln[u] = (idxn >= 0 && c < w) ? Lp[(int64_t)(c0 + c) * m + rbn + lane] : (TL)0;
+        }
+        // the chunk's first row, lane 0's (>= fp: every row below is a row of the parent's front)
+        const int g0 = __shfl_sync(0xffffffffu, idx, 0);
         const int k = g0 < fp + ncp ? max(0, g0 - fp) / kSB : nbp - 1;
         if (k < ready && wok) {
           wok = warp_wait(pflags + k, epoch, true, status, s);
           ready = k;
         }
-        const int r = rb + lane;
-        if (r < m && wok) {
-          const double xr = __ldcg(y + rowsOf[r]);
+        if (idx >= 0 && wok) {
+          const double xr = __ldcg(y + idx);
 #pragma unroll
-          for (int u = 0; u < 8; u++) {
-            const int c = warp + 8 * u;
-            if (c < w) acc[u] += (double)Lp[(int64_t)(c0 + c) * m + r] * xr;
-          }
+          for (int u = 0; u < 8; u++) acc[u] += (double)lc[u] * xr;
         }
+        idx = idxn;
+#pragma unroll
+        for (int u = 0; u < 8; u++) lc[u] = ln[u];
       }
     }
     if (!__syncthreads_and(wok)) return false;  // block-uniform
