@@ -150,6 +150,7 @@ struct amp_plan_s {
   amp::TileTask *dTile = nullptr, *dUTile = nullptr;
   amp::MixTask *dMixTile = nullptr, *dMixU = nullptr;
   int4 *dFwdTasks = nullptr, *dBwdTasks = nullptr, *dBwdAll = nullptr;
+  int4 *dFwdTasks1 = nullptr;  // the one-vector forward's list (with whole-supernode tasks)
   int *dTinySn = nullptr, *dSmallSn = nullptr;  // small fronts per level (whole fronts by one warp / one CTA)
   int2 *dChain = nullptr;                        // chain-matrix tasks {s, b}
   int *dInvBlocks = nullptr;                     // diagonal blocks whose inverses the solves use
@@ -268,6 +269,7 @@ void upload_plan(amp_plan *pl) {
   pl->dMixTile = m.upload(P.mixTiles);
   pl->dMixU = m.upload(P.mixUTasks);
   pl->dFwdTasks = (int4 *)m.upload(P.fwdTasks);
+  pl->dFwdTasks1 = (int4 *)m.upload(P.fwdTasks1);
   pl->dBwdTasks = (int4 *)m.upload(P.bwdTasks);
   pl->dBwdAll = (int4 *)m.upload(P.bwdAll);
   pl->dTinySn = m.upload(P.tinySn);
@@ -499,16 +501,16 @@ void device_solve_permuted(amp_factor *f) {
   ck(cudaMemsetAsync(f->dDone, 0, sizeof(int) * std::max(1, P.nsuper), st), "memset done");
   ck(cudaMemsetAsync(f->dSolveStatus, 0xff, sizeof(unsigned long long), st), "memset status");
   const int efwd = 2 * (++f->solveEpoch) - 1, ebwd = 2 * f->solveEpoch;
-  const int nf = P.fwdLvlPtr[P.nlevels], nb = (int)(P.bwdAll.size() / 4);
+  const int nf = (int)(P.fwdTasks1.size() / 4), nb = (int)(P.bwdAll.size() / 4);
   const bool ldlt = f->kind == AMP_LDLT;
   const double *Dp = ldlt ? f->dD : nullptr;
   timed(f, K_FORWARD, 2.0 * (double)P.nnzLStored, lbytes, [&] {
     if (f->dL32)
-      amp::launch_fwd_blocks<float>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->dL32, f->dInv32,
+      amp::launch_fwd_blocks<float>(f->plan->dFwdTasks1, nf, f->dTickets, dp, f->dL32, f->dInv32,
                                     ldlt ? nullptr : f->dMch32, f->dY, f->dT, f->dFlags, f->dHand, efwd, f->dDone,
                                     f->dSolveStatus, st);
     else
-      amp::launch_fwd_blocks<double>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->dLx, f->dInv, ldlt ? nullptr : f->dMch,
+      amp::launch_fwd_blocks<double>(f->plan->dFwdTasks1, nf, f->dTickets, dp, f->dLx, f->dInv, ldlt ? nullptr : f->dMch,
                                      f->dY, f->dT, f->dFlags, f->dHand, efwd, f->dDone, f->dSolveStatus, st);
   });
   timed(f, K_BACKWARD, 2.0 * (double)P.nnzLStored, lbytes, [&] {

@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(256) k_chain_mats(const int2 *__restrict__ tas
 
 // ---- forward block tasks -----------------------------------------------------------------------------------------
 constexpr int kChPre = 64;  // children located and waited for at once by a forward block task
-// task: .x supernode, .y block, .z kind (0 diagonal, 1 below, 2 small supernodes)
+// task: .x supernode, .y block, .z kind (0 diagonal, 1 below, 2 small supernodes, 3 whole supernode: one-vector list)
 // One launch for the whole sweep: tasks are listed level by level (leaves first), so every wait is on a task with an
 // earlier ticket. Every task first waits for the supernode's children and gathers its own rows of the front vector
 // v_s = [y(f .. f + nc); 0] + the children's pass-up vectors (in the reference's child order). A below task forms its
@@ -151,8 +151,93 @@ __global__ void __launch_bounds__(256, 3) k_fwd_blocks(const int4 *__restrict__ 
   __shared__ double Xs[kSB][kSB + 1];
   __shared__ int2 chA[kChPre];
   __shared__ int64_t chMap[kChPre], chT[kChPre];
+  __shared__ double vs[kWholeFront];
+  // kind 3: the whole supernode s (nc <= 64, m <= kWholeFront): gather its front vector v (all m rows) in shared
+  // memory, y = X v[0:nc), then u = v - L[rows below, :] y in 64-row chunks (L values loaded a chunk ahead, the first
+  // chunk before the waits); the same arithmetic, term by term, as a diagonal task and its below tasks
+  auto whole = [&](const int s) -> bool {
+    const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s], mu = m - nc;
+    const TL *Lp = Lx + P.snLxp[s];
+    const int tid = threadIdx.x, row = tid & (kSB - 1), part = tid >> 6;
+    {
+      const TL *X = Inv + P.invOff[P.blkOff[s]];
+      for (int e = tid; e < nc * nc; e += blockDim.x) Xs[e % nc][e / nc] = (double)X[e];
+    }
+    TL lv[16];
+    auto loadChunk = [&](int j, TL (&dst)[16]) {
+      const int r = nc + j * kSB + row;
+#pragma unroll
+      for (int u = 0; u < 16; u++) {
+        const int c = part + 4 * u;
+        dst[u] = (r < m && c < nc) ? Lp[(int64_t)c * m + r] : (TL)0;
+      }
+    };
+    loadChunk(0, lv);
+    for (int r = tid; r < m; r += blockDim.x) vs[r] = r < nc ? y[f + r] : 0.0;
+    // children: metadata and waits in parallel, kChPre at a time; whole pass-up vectors added in child order
+    const int q0 = P.chPtr[s], q1 = P.chPtr[s + 1];
+    for (int qb = q0; qb < q1; qb += kChPre) {
+      const int nq = min(kChPre, q1 - qb);
+      if (qb > q0) __syncthreads();  // the previous chunk's metadata is consumed
+      int ok = 1;
+      if (tid < nq) {
+        const int c = P.chList[qb + tid];
+        const int muc = P.snM[c] - P.snNc[c];
+        chA[tid] = make_int2(0, muc);
+        chMap[tid] = P.eaPtr[c];
+        chT[tid] = P.snTOff[c];
+        ok = wait_count(done + c, (muc + kSB - 1) / kSB, status, s);
+      }
+      if (!__syncthreads_and(ok)) return false;  // block-uniform
+      for (int q = 0; q < nq; q++) {
+        const int *map = P.eaMap + chMap[q];
+        const double *tc = T + chT[q];
+        for (int a = tid; a < chA[q].y; a += blockDim.x) vs[map[a]] += __ldcg(tc + a);
+        __syncthreads();
+      }
+    }
+    if (q0 == q1) __syncthreads();
+    {  // y = X v[0:nc): thread (row, part) sums columns part, part + 4, ... <= row
+      double a2 = 0.0;
+      if (row < nc)
+        for (int c = part; c <= row; c += 4) a2 += Xs[row][c] * vs[c];
+      red[part][row] = a2;
+    }
+    __syncthreads();
+    if (tid < kSB) {
+      const double yv = tid < nc ? (red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]) : 0.0;
+      rk[tid] = yv;
+      if (tid < nc) y[f + tid] = yv;
+    }
+    __syncthreads();
+    const int nch = (mu + kSB - 1) / kSB;
+    for (int j = 0; j < nch; j++) {
+      TL ln[16];
+      loadChunk(j + 1, ln);
+      double acc = 0.0;
+#pragma unroll
+      for (int u = 0; u < 16; u++) {
+        const int c = part + 4 * u;
+        if (c < nc) acc += (double)lv[u] * rk[c];
+      }
+      red[part][row] = acc;
+      __syncthreads();
+      const int r0 = nc + j * kSB;
+      if (tid < min(kSB, m - r0))
+        T[P.snTOff[s] + j * kSB + tid] = vs[r0 + tid] - ((red[0][tid] + red[1][tid]) + (red[2][tid] + red[3][tid]));
+      __syncthreads();  // red is reused by the next chunk
+#pragma unroll
+      for (int u = 0; u < 16; u++) lv[u] = ln[u];
+    }
+    if (tid == 0) {  // after the barrier: the CTA's stores of y and T are ordered before both
+      st_release(flags + P.blkOff[s], epoch);
+      if (nch > 0) red_release_add(done + s, nch);
+    }
+    return true;
+  };
   auto run = [&](const int tkv) -> bool {
     const int4 t = tasks[tkv];
+    if (t.z == 3) return whole(t.x);
     if (t.z == 2) {  // up to kSolveGroup supernodes with m <= 32, one warp each
       const int warp = threadIdx.x >> 5;
       if (threadIdx.x == 0) waitOk = 1;

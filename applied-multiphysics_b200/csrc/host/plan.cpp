@@ -350,6 +350,8 @@ void build_plan(const Symbolic &S, Plan &P) {
   // Supernodes with m <= kTinyFront are solved whole by one warp: tasks {first, count, 2} over solveSmall, up to
   // kSolveGroup supernodes of one level per task, listed before the level's block tasks.
   auto solveSmall = [&](int s) { return P.snM[s] <= kTinyFront; };
+  auto whole = [&](int s) { return !solveSmall(s) && P.snNc[s] <= B && P.snM[s] <= kWholeFront; };
+  P.fwdTasks1.clear();
   for (int s = 0; s < ns; s++)
     if (!solveSmall(s))
       for (int b = P.blkOff[s]; b < P.blkOff[s + 1]; b++) P.invBlocks.push_back(b);
@@ -360,20 +362,31 @@ void build_plan(const Symbolic &S, Plan &P) {
     const int64_t g1 = (int64_t)P.solveSmall.size();
     for (int64_t g = g0; g < g1; g += kSolveGroup) {
       push(P.fwdTasks, (int)g, (int)std::min<int64_t>(kSolveGroup, g1 - g), 2);
+      push(P.fwdTasks1, (int)g, (int)std::min<int64_t>(kSolveGroup, g1 - g), 2);
       push(P.bwdTasks, (int)g, (int)std::min<int64_t>(kSolveGroup, g1 - g), 2);
     }
+    // one-vector forward: a supernode with one pivot block and m <= kWholeFront is one task (kind 3) doing its
+    // diagonal block and all of its rows below
+    for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++)
+      if (whole(P.lvlSn[q])) push(P.fwdTasks1, P.lvlSn[q], 0, 3);
     int maxNb = 0;
     for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++)
       if (!solveSmall(P.lvlSn[q])) maxNb = std::max(maxNb, (P.snNc[P.lvlSn[q]] + B - 1) / B);
     for (int blk = 0; blk < maxNb; blk++)
       for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
         int s = P.lvlSn[q];
-        if (!solveSmall(s) && blk < (P.snNc[s] + B - 1) / B) push(P.fwdTasks, s, blk, 0);
+        if (!solveSmall(s) && blk < (P.snNc[s] + B - 1) / B) {
+          push(P.fwdTasks, s, blk, 0);
+          if (!whole(s)) push(P.fwdTasks1, s, blk, 0);
+        }
       }
     for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
       int s = P.lvlSn[q], mu = P.snM[s] - P.snNc[s];
       if (solveSmall(s)) continue;
-      for (int j = 0; j * B < mu; j++) push(P.fwdTasks, s, j, 1);
+      for (int j = 0; j * B < mu; j++) {
+        push(P.fwdTasks, s, j, 1);
+        if (!whole(s)) push(P.fwdTasks1, s, j, 1);
+      }
     }
     P.fwdLvlPtr[L + 1] = (int)(P.fwdTasks.size() / 4);
     for (int d = 0; d < maxNb; d++)

@@ -27,6 +27,7 @@ constexpr int kTinyFront = 32;    // fronts with m <= 32: one warp per front doe
 constexpr int kTinyMid = 16;      // the smaller tiny class (m <= 16: 16 x 16 tiles, eight fronts per CTA)
 constexpr int kSmallFront = 128;  // fronts with 32 < m <= 128: one CTA per front does the whole front
 constexpr int kSolveGroup = 4;    // supernodes with m <= kTinyFront per solve task (one warp each)
+constexpr int kWholeFront = 512;  // one-vector forward: supernodes with nc <= 64 and m <= 512 are one task each
 
 struct PotrfTask {  // POTRF / LDL^T of the pivot block [c0, c0 + w) of supernode s, and its inverse
   int s, c0;
@@ -107,6 +108,7 @@ struct Plan {
   std::vector<int64_t> invOff;      // per diagonal block (flag index): offset of its w x w inverse; [nflags] = total
   std::vector<int> diagSlot;        // CSR slot of each diagonal entry of A (LDL^T pivot scale)
   std::vector<int> fwdTasks, bwdTasks;  // int4 records, flattened
+  std::vector<int> fwdTasks1;           // the one-vector forward's list: fwdTasks with kind 3 (whole supernode) tasks
   std::vector<int> solveSmall;          // supernodes solved whole by one warp, grouped by level (tasks of kind 2)
   std::vector<int> invBlocks;           // diagonal blocks (flag index) whose inverse the block-task solves use
   std::vector<int> chainTasks;          // {s, b} pairs: every diagonal block of a supernode with two or more
