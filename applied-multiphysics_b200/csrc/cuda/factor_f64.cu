@@ -86,6 +86,27 @@ __device__ __forceinline__ bool failed(const unsigned long long *st) {
 // ---------------------------------------------------------------------------------------------------------------
 // Assembly + extend-add
 // ---------------------------------------------------------------------------------------------------------------
+constexpr int kAsmChildren = 64;  // children whose column ranges an assembly CTA locates up front
+constexpr int kAsmInFlight = 4;   // extend-add entries per lane in flight
+
+// the columns [b0, b1) of child c's update matrix that map into front columns [j0, j1) (its map is increasing)
+__device__ __forceinline__ int2 child_cols(const DevPlan &P, int c, int j0, int j1) {
+  const int muc = P.snM[c] - P.snNc[c];
+  const int *map = P.eaMap + P.eaPtr[c];
+  int lo = 0, hi = max(muc, 0);
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (map[mid] < j0) lo = mid + 1; else hi = mid;
+  }
+  const int b0 = lo;
+  hi = max(muc, 0);
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (map[mid] < j1) lo = mid + 1; else hi = mid;
+  }
+  return make_int2(b0, lo);
+}
+
 template <class T>
 __global__ void __launch_bounds__(256) k_assemble(const AsmTask *__restrict__ tasks, DevPlan P,
                                                   const double *__restrict__ values, T *__restrict__ Lx,
@@ -98,6 +119,11 @@ __global__ void __launch_bounds__(256) k_assemble(const AsmTask *__restrict__ ta
   T *Lp = Lx + P.snLxp[s];
   T *Up = (m > nc) ? U + P.snUoff[s] : nullptr;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  // 0. the child columns mapping into [j0, jend), one child per thread (the first kAsmChildren children; the map of
+  // a child is increasing, so they form one range per child): located while the columns are zeroed
+  __shared__ int2 chRange[kAsmChildren];
+  const int q0 = P.chPtr[s], nch = P.chPtr[s + 1] - q0;
+  if ((int)threadIdx.x < min(nch, kAsmChildren)) chRange[threadIdx.x] = child_cols(P, P.chList[q0 + threadIdx.x], j0, jend);
   // 1. zero the lower part of the owned columns
   for (int j = j0 + warp; j < jend; j += nwarps)
     for (int i = j + lane; i < m; i += 32) *front_addr(Lp, Up, m, nc, i, j) = T(0);
@@ -124,42 +150,30 @@ __global__ void __launch_bounds__(256) k_assemble(const AsmTask *__restrict__ ta
   }
   __syncthreads();
   // 3. children, one after another (stack order of the reference)
-  for (int q = P.chPtr[s]; q < P.chPtr[s + 1]; q++) {
-    const int c = P.chList[q];
+  for (int q = 0; q < nch; q++) {
+    const int c = P.chList[q0 + q];
     const int muc = P.snM[c] - P.snNc[c];
-    if (muc <= 0) continue;
+    if (muc <= 0) continue;  // block-uniform
     const int *map = P.eaMap + P.eaPtr[c];
     const T *Uc = U + P.snUoff[c];
-    // child columns b mapping into [j0, jend): map is increasing
-    int lo = 0, hi = muc;
-    while (lo < hi) {
-      int mid = (lo + hi) >> 1;
-      if (map[mid] < j0) lo = mid + 1; else hi = mid;
-    }
-    const int b0 = lo;
-    hi = muc;
-    while (lo < hi) {
-      int mid = (lo + hi) >> 1;
-      if (map[mid] < jend) lo = mid + 1; else hi = mid;
-    }
-    const int b1 = lo;
-    for (int b = b0 + warp; b < b1; b += nwarps) {
+    const int2 br = q < kAsmChildren ? chRange[q] : child_cols(P, c, j0, jend);
+    for (int b = br.x + warp; b < br.y; b += nwarps) {
       const int jj = map[b];
       const T *col = Uc + (int64_t)b * muc;
-      // 4 entries per lane in flight: gather the child's values and target rows, then read-modify-write the front
-      for (int a = b + lane; a < muc; a += 128) {
-        T v[4], cur[4];
-        T *dst[4];
+      // kAsmInFlight entries per lane in flight: gather the child's values and target rows, then read-modify-write
+      for (int a = b + lane; a < muc; a += 32 * kAsmInFlight) {
+        T v[kAsmInFlight], cur[kAsmInFlight];
+        T *dst[kAsmInFlight];
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
+        for (int u = 0; u < kAsmInFlight; u++) {
           const int aa = a + 32 * u;
           dst[u] = aa < muc ? front_addr(Lp, Up, m, nc, __ldg(map + aa), jj) : nullptr;
           v[u] = aa < muc ? col[aa] : T(0);
         }
 #pragma unroll
-        for (int u = 0; u < 4; u++) cur[u] = dst[u] ? *dst[u] : T(0);
+        for (int u = 0; u < kAsmInFlight; u++) cur[u] = dst[u] ? *dst[u] : T(0);
 #pragma unroll
-        for (int u = 0; u < 4; u++)
+        for (int u = 0; u < kAsmInFlight; u++)
           if (dst[u]) *dst[u] = cur[u] + v[u];
       }
     }
