@@ -27,7 +27,11 @@ CHOLESKY, LDLT = 0, 1
 FP64, MIXED = 0, 1
 
 FIELDS = ["perm", "pinv", "parent", "colCount", "lowerP", "lowerI", "lowerSrc", "superStart", "colSuper",
-          "superParent", "childHead", "childNext", "Sp", "Si", "Lxp"]
+          "superParent", "childHead", "childNext", "Sp", "Si", "Lxp",
+          # the device schedule (amp_field after AMP_F_LXP): read-only introspection
+          "levelPtr", "levelSupernodes", "fwdTasks", "fwdTasksMulti", "bwdTasks", "solveSmall", "tinyFronts",
+          "tinyPtr", "tinyMid"]
+_INT64_FIELDS = ("Lxp", "tinyPtr", "tinyMid")
 
 
 class AmpError(Exception):
@@ -213,7 +217,7 @@ class SymbolicAnalysis:
                 k = FIELDS.index(name)
                 ln = C.c_int64(0)
                 _check(lib().amp_plan_array(self._h, k, None, 0, C.byref(ln)))
-                arr = np.zeros(max(ln.value, 1), np.int64 if name == "Lxp" else np.int32)
+                arr = np.zeros(max(ln.value, 1), np.int64 if name in _INT64_FIELDS else np.int32)
                 _check(lib().amp_plan_array(self._h, k, arr.ctypes.data, ln.value, C.byref(ln)))
                 self._arrays[name] = arr[: ln.value]
             return self._arrays[name]

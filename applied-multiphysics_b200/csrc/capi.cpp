@@ -802,9 +802,20 @@ int amp_plan_array(const amp_plan *pl, int field, void *dst, int64_t len, int64_
     case AMP_F_CHILDNEXT: v = &S.childNext; break;
     case AMP_F_SP: v = &S.Sp; break;
     case AMP_F_SI: v = &S.Si; break;
-    case AMP_F_LXP: {
-      if (out_len) *out_len = (int64_t)S.Lxp.size();
-      if (dst) std::memcpy(dst, S.Lxp.data(), sizeof(int64_t) * std::min<int64_t>(len, S.Lxp.size()));
+    case AMP_F_LEVEL_PTR: v = &pl->P.lvlPtr; break;
+    case AMP_F_LEVEL_SUPERNODES: v = &pl->P.lvlSn; break;
+    case AMP_F_FWD_TASKS: v = &pl->P.fwdTasks1; break;
+    case AMP_F_FWD_TASKS_MULTI: v = &pl->P.fwdTasks; break;
+    case AMP_F_BWD_TASKS: v = &pl->P.bwdAll; break;
+    case AMP_F_SOLVE_SMALL: v = &pl->P.solveSmall; break;
+    case AMP_F_TINY_FRONTS: v = &pl->P.tinySn; break;
+    case AMP_F_LXP:
+    case AMP_F_TINY_PTR:
+    case AMP_F_TINY_MID: {
+      const std::vector<int64_t> &w =
+          field == AMP_F_LXP ? S.Lxp : field == AMP_F_TINY_PTR ? pl->P.tinyPtr : pl->P.tinyMid;
+      if (out_len) *out_len = (int64_t)w.size();
+      if (dst) std::memcpy(dst, w.data(), sizeof(int64_t) * std::min<int64_t>(len, w.size()));
       return AMP_OK;
     }
     default: return fail(AMP_INVALID, "unknown field");

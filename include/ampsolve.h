@@ -68,11 +68,24 @@ typedef struct {
   int64_t device_bytes; /* device memory of one factor of this plan (L, update arena, schedule) */
 } amp_plan_info;
 
-/* Array fields of a symbolic analysis for amp_plan_array (int32 unless noted). */
+/* Array fields of a symbolic analysis for amp_plan_array (int32 unless noted). The fields after AMP_F_LXP expose
+   the device schedule built with the analysis (read-only introspection; no reference counterpart):
+   - AMP_F_LEVEL_PTR / AMP_F_LEVEL_SUPERNODES: the supernodes of etree level L (leaves first) are
+     LEVEL_SUPERNODES[LEVEL_PTR[L] .. LEVEL_PTR[L + 1]);
+   - AMP_F_FWD_TASKS: the one-vector forward sweep's tasks, records {x, y, kind, 0} in launch order: kind 0 diagonal
+     block y of supernode x, kind 1 the 64-row chunk y of supernode x's rows below, kind 2 the supernodes
+     SOLVE_SMALL[x .. x + y) (one warp each), kind 3 the whole supernode x;
+   - AMP_F_FWD_TASKS_MULTI: the multi-vector forward sweep's tasks (kinds 0-2);
+   - AMP_F_BWD_TASKS: the backward sweep's tasks, levels top-down (kinds 0 and 2);
+   - AMP_F_SOLVE_SMALL: supernodes solved whole by one warp (m <= 32), grouped by level;
+   - AMP_F_TINY_FRONTS, AMP_F_TINY_PTR (int64), AMP_F_TINY_MID (int64): fronts factored whole by one warp (m <= 32):
+     level L's are TINY_FRONTS[TINY_PTR[L] .. TINY_PTR[L + 1]), sorted by m, those from TINY_MID[L] on with m > 16. */
 typedef enum {
   AMP_F_PERM = 0, AMP_F_PINV, AMP_F_PARENT, AMP_F_COLCOUNT, AMP_F_LOWERP, AMP_F_LOWERI, AMP_F_LOWERSRC,
   AMP_F_SUPERSTART, AMP_F_COLSUPER, AMP_F_SUPERPARENT, AMP_F_CHILDHEAD, AMP_F_CHILDNEXT, AMP_F_SP, AMP_F_SI,
-  AMP_F_LXP /* int64 */
+  AMP_F_LXP /* int64 */,
+  AMP_F_LEVEL_PTR, AMP_F_LEVEL_SUPERNODES, AMP_F_FWD_TASKS, AMP_F_FWD_TASKS_MULTI, AMP_F_BWD_TASKS,
+  AMP_F_SOLVE_SMALL, AMP_F_TINY_FRONTS, AMP_F_TINY_PTR /* int64 */, AMP_F_TINY_MID /* int64 */
 } amp_field;
 
 typedef struct {
