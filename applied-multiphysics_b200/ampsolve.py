@@ -10,6 +10,7 @@ a GPU for the numeric calls) every call raises.
 from __future__ import annotations
 
 import ctypes as C
+from decimal import ROUND_HALF_UP, Decimal
 import os
 import time
 from typing import Sequence
@@ -619,3 +620,64 @@ class SupernodalLDLT:
         an indefinite matrix, gmres-real.mjs:31-105)."""
         self._need()
         return self.num.solve_gmres(b, tol=tol, restart=restart, maxIter=maxIter)
+
+
+# ---- 'auto' choice between the direct solver and the iterative one ----------------------------------------------------
+# The reference's study setting 'auto' (physics/src/common/scalar.ts:264-283) picks AMG-PCG over the direct factor when
+# the factor's symbolic flops per DOF reach a break-even measured for its single-threaded CPU factor (3e5 flop/DOF: a
+# 15.6k-node tet10 heat pattern at 2.7e5 had both within 10%), or when 8 nnzL bytes exceed a 1 GiB memory budget.
+AUTO_FLOPS_PER_DOF_CPU = 3e5
+AUTO_MAX_FACTOR_BYTES_CPU = 2 ** 30
+# The same rule for this GPU factor. AMG-PCG (on the host, as in the reference) costs about 3e5 flop/DOF at the CPU
+# factor's 23 GFlop/s, i.e. about 13 us per DOF. The GPU factor + solve runs at 13 TFLOP/s end to end on the 3D
+# elasticity system in FP64 (0.79 TFLOP in 60 ms, its slowest measured rate; 26 in mixed precision, 63 on the 3D P2
+# heat system), so the break-even is 13e-6 s x 13e12 flop/s = 1.7e8 flop/DOF; the memory bound is the factor's
+# device memory (L, update arena and schedule) against a budget of 128 GiB of the B200's 180 GB.
+AUTO_FLOPS_PER_DOF_GPU = 1.7e8
+AUTO_MAX_FACTOR_BYTES_GPU = 128 * 2 ** 30
+
+
+def autoSolverChoice(n: int, flops: float, nnzL: int, factorBytes: int | None = None,
+                     flopsPerDof: float = AUTO_FLOPS_PER_DOF_GPU, maxFactorBytes: int = AUTO_MAX_FACTOR_BYTES_GPU) -> dict:
+    """{'kind': 'cholesky' | 'amg-pcg', 'reason': str} for a pattern with n rows and an analysis giving flops and nnzL
+    (autoSolverChoice, scalar.ts:271-276: the memory test first, then flop/DOF against the break-even). factorBytes:
+    the factor's memory (the plan's deviceBytes); 8 nnzL when None, as the reference counts it. With
+    flopsPerDof=AUTO_FLOPS_PER_DOF_CPU and maxFactorBytes=AUTO_MAX_FACTOR_BYTES_CPU the choice and the message are the
+    reference's."""
+    fpd = flops / max(n, 1)
+    nbytes = 8 * nnzL if factorBytes is None else factorBytes
+    if nbytes > maxFactorBytes:
+        return {"kind": "amg-pcg",
+                "reason": f"direct factor {_js_fixed0(nbytes / 2 ** 20)} MiB > {_js_num(maxFactorBytes / 2 ** 20)} MiB"}
+    if fpd >= flopsPerDof:
+        return {"kind": "amg-pcg", "reason": f"direct factor {_js_exp(fpd, 2)} flop/DOF >= {_js_exp(flopsPerDof, 0)}"}
+    return {"kind": "cholesky", "reason": f"direct factor {_js_exp(fpd, 2)} flop/DOF < {_js_exp(flopsPerDof, 0)}"}
+
+
+def _js_exp(x: float, digits: int) -> str:
+    """Number.prototype.toExponential(digits) of x >= 0: the exact value rounded half up, '2.70e+5'."""
+    if x == 0:
+        return f"{0:.{digits}f}e+0"
+    d = Decimal(x)
+    e = d.adjusted()
+    q = Decimal(1).scaleb(-digits)
+    m = d.scaleb(-e).quantize(q, rounding=ROUND_HALF_UP)
+    if m >= 10:
+        e += 1
+        m = d.scaleb(-e).quantize(q, rounding=ROUND_HALF_UP)
+    return f"{m}e{'+' if e >= 0 else '-'}{abs(e)}"
+
+
+def _js_fixed0(x: float) -> str:
+    """Number.prototype.toFixed(0) of x >= 0 (half up)."""
+    return str(Decimal(x).quantize(Decimal(1), rounding=ROUND_HALF_UP))
+
+
+def _js_num(x: float) -> str:
+    """String(x) for the whole numbers used here."""
+    return str(int(x)) if x == int(x) else repr(x)
+
+
+def autoSolverChoiceFor(sym: SymbolicAnalysis, **kw) -> dict:
+    """autoSolverChoice from an analysis, with the factor's device memory as its size."""
+    return autoSolverChoice(sym.n, sym.flops, sym.nnzL, factorBytes=kw.pop("factorBytes", sym.deviceBytes), **kw)
