@@ -9,6 +9,7 @@
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/ampsolve.h"
@@ -22,7 +23,7 @@ void launch_matvec(int n, const int *rowptr, const int *colidx, const double *va
 void launch_residual(int n, const int *rowptr, const int *colidx, const double *val, const double *x, const double *b,
                      double *r, double *norms, int q, cudaStream_t st);
 void launch_axpy(double *x, const double *dx, int64_t len, cudaStream_t st);
-void launch_dots(const double *V, int nv, int64_t n, const double *w, double *partial, double *out, cudaStream_t st);
+int launch_dots(const double *V, int nv, int64_t n, const double *w, double *partial, double *out, cudaStream_t st);
 void launch_gs_update(double *w, const double *V, const double *h, int nv, int64_t n, cudaStream_t st);
 void launch_combine_add(double *x, const double *Z, const double *y, int nv, int64_t n, cudaStream_t st);
 void launch_scale_to(double *v, const double *w, double a, int64_t n, cudaStream_t st);
@@ -188,6 +189,7 @@ struct amp_factor_s {
     int kind;
     cudaEvent_t a, b;
     double flops, bytes;
+    int kernels;  // kernel launches between a and b
   };
   std::vector<Rec> recs;
   std::vector<cudaEvent_t> evPool;
@@ -311,16 +313,20 @@ cudaEvent_t pool_event(amp_factor *f) {
   return f->evPool[f->evUsed++];
 }
 
-// Run one launch; while profiling, bracket it with events and record its algorithmic work.
+// Run one launch; while profiling, bracket it with events and record its algorithmic work. launch() issues one
+// kernel, or returns how many it issued.
 template <class L>
 void timed_on(amp_factor *f, cudaStream_t st, int kind, double flops, double bytes, L &&launch) {
   if (!f->profiling) {
     launch();
     return;
   }
-  amp_factor_s::Rec r{kind, pool_event(f), pool_event(f), flops, bytes};
+  amp_factor_s::Rec r{kind, pool_event(f), pool_event(f), flops, bytes, 1};
   ck(cudaEventRecord(r.a, st), "event");
-  launch();
+  if constexpr (std::is_void_v<decltype(launch())>)
+    launch();
+  else
+    r.kernels = (int)launch();
   ck(cudaEventRecord(r.b, st), "event");
   f->recs.push_back(r);
 }
@@ -361,9 +367,9 @@ void enqueue_small_fronts(amp_factor *f, int L, T *Lx, T *U, const amp::LdltArgs
   if (t1 == t0 && s1 == s0) return;
   const double scale = sizeof(T) / 8.0;
   timed(f, K_FRONTS, 2.0 * P.frontLvlFlops[L], P.frontLvlBytes[L] * scale, [&] {
-    amp::launch_fronts_small<T>(f->plan->dTinySn + t0, (int)(t1 - t0), (int)(P.tinyMid[L] - t0),
-                                f->plan->dSmallSn + s0, (int)(s1 - s0), P.smallMaxM[L], f->plan->dp, f->dValues, Lx,
-                                U, f->dStatus, la, f->stream);
+    return amp::launch_fronts_small<T>(f->plan->dTinySn + t0, (int)(t1 - t0), (int)(P.tinyMid[L] - t0),
+                                       f->plan->dSmallSn + s0, (int)(s1 - s0), P.smallMaxM[L], f->plan->dp,
+                                       f->dValues, Lx, U, f->dStatus, la, f->stream);
   });
 }
 
@@ -1141,7 +1147,8 @@ int amp_solve_gmres(amp_factor *f, const double *b, double *x, int on_device, co
     ck(cudaMemsetAsync(xb, 0, sizeof(double) * n, st), "zero x");
     std::vector<double> h(m + 1), H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
     auto dots = [&](const double *Vs, int nv, const double *v) {  // h[0..nv) = Vs[j] . v (synchronises)
-      timed(f, K_KRYLOV, 2.0 * n * nv, 8.0 * n * (nv + 1), [&] { amp::launch_dots(Vs, nv, n, v, part, dh, st); });
+      timed(f, K_KRYLOV, 2.0 * n * nv, 8.0 * n * (nv + 1),
+            [&] { return amp::launch_dots(Vs, nv, n, v, part, dh, st); });
       ck(cudaMemcpyAsync(h.data(), dh, sizeof(double) * nv, cudaMemcpyDeviceToHost, st), "dots");
       ck(cudaStreamSynchronize(st), "dots");
     };
@@ -1291,7 +1298,7 @@ int amp_profile_read(amp_factor *f, amp_kernel_stat *stats, int32_t cap, int32_t
     for (auto &r : f->recs) {
       float ms = 0;
       ck(cudaEventElapsedTime(&ms, r.a, r.b), "elapsed");
-      acc[r.kind].launches++;
+      acc[r.kind].launches += r.kernels;
       acc[r.kind].ms += ms;
       acc[r.kind].flops += r.flops;
       acc[r.kind].bytes += r.bytes;

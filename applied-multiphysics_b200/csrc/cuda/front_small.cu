@@ -219,37 +219,38 @@ void init_front_small_attributes() {
 }
 
 template <class T, class TC, int MAXM>
-static void launch_tiny(const int *fronts, int count, const DevPlan &P, const double *values, T *Lx, T *U,
-                        unsigned long long *status, const LdltArgs<T> &la, cudaStream_t st) {
+static int launch_tiny(const int *fronts, int count, const DevPlan &P, const double *values, T *Lx, T *U,
+                       unsigned long long *status, const LdltArgs<T> &la, cudaStream_t st) {
   constexpr int W = tiny_warps<MAXM>();
-  if (count > 0)
-    k_front_tiny<T, TC, MAXM><<<(count + W - 1) / W, 32 * W, 0, st>>>(fronts, count, P, values, Lx, U, status, la);
+  if (count <= 0) return 0;
+  k_front_tiny<T, TC, MAXM><<<(count + W - 1) / W, 32 * W, 0, st>>>(fronts, count, P, values, Lx, U, status, la);
+  return 1;
 }
 
 template <class T, class TC>
-static void launch_fronts_tc(const int *tiny, int ntiny, int ntinyMid, const int *small, int nsmall, int maxM,
-                             const DevPlan &P, const double *values, T *Lx, T *U, unsigned long long *status,
-                             const LdltArgs<T> &la, cudaStream_t st) {
-  launch_tiny<T, TC, kTinyMid>(tiny, ntinyMid, P, values, Lx, U, status, la, st);
-  launch_tiny<T, TC, kTinyFront>(tiny + ntinyMid, ntiny - ntinyMid, P, values, Lx, U, status, la, st);
+static int launch_fronts_tc(const int *tiny, int ntiny, int ntinyMid, const int *small, int nsmall, int maxM,
+                            const DevPlan &P, const double *values, T *Lx, T *U, unsigned long long *status,
+                            const LdltArgs<T> &la, cudaStream_t st) {
+  int k = launch_tiny<T, TC, kTinyMid>(tiny, ntinyMid, P, values, Lx, U, status, la, st);
+  k += launch_tiny<T, TC, kTinyFront>(tiny + ntinyMid, ntiny - ntinyMid, P, values, Lx, U, status, la, st);
   if (nsmall > 0)
     k_front_small<T, TC><<<nsmall, 256, (size_t)maxM * maxM * sizeof(TC), st>>>(small, nsmall, P, values, Lx, U,
                                                                                 status, la);
+  return k + (nsmall > 0 ? 1 : 0);
 }
 template <class T>
-void launch_fronts_small(const int *tiny, int ntiny, int ntinyMid, const int *small, int nsmall, int maxM,
-                         const DevPlan &P, const double *values, T *Lx, T *U, unsigned long long *status,
-                         const LdltArgs<T> &la, cudaStream_t st) {
+int launch_fronts_small(const int *tiny, int ntiny, int ntinyMid, const int *small, int nsmall, int maxM,
+                        const DevPlan &P, const double *values, T *Lx, T *U, unsigned long long *status,
+                        const LdltArgs<T> &la, cudaStream_t st) {
   if (la.scal != nullptr)  // LDL^T: FP64 arithmetic whatever the storage
-    launch_fronts_tc<T, double>(tiny, ntiny, ntinyMid, small, nsmall, maxM, P, values, Lx, U, status, la, st);
-  else
-    launch_fronts_tc<T, T>(tiny, ntiny, ntinyMid, small, nsmall, maxM, P, values, Lx, U, status, la, st);
+    return launch_fronts_tc<T, double>(tiny, ntiny, ntinyMid, small, nsmall, maxM, P, values, Lx, U, status, la, st);
+  return launch_fronts_tc<T, T>(tiny, ntiny, ntinyMid, small, nsmall, maxM, P, values, Lx, U, status, la, st);
 }
-template void launch_fronts_small<double>(const int *, int, int, const int *, int, int, const DevPlan &,
-                                          const double *, double *, double *, unsigned long long *,
-                                          const LdltArgs<double> &, cudaStream_t);
-template void launch_fronts_small<float>(const int *, int, int, const int *, int, int, const DevPlan &,
-                                         const double *, float *, float *, unsigned long long *,
-                                         const LdltArgs<float> &, cudaStream_t);
+template int launch_fronts_small<double>(const int *, int, int, const int *, int, int, const DevPlan &,
+                                         const double *, double *, double *, unsigned long long *,
+                                         const LdltArgs<double> &, cudaStream_t);
+template int launch_fronts_small<float>(const int *, int, int, const int *, int, int, const DevPlan &,
+                                        const double *, float *, float *, unsigned long long *,
+                                        const LdltArgs<float> &, cudaStream_t);
 
 }  // namespace amp

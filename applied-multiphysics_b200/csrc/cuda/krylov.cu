@@ -74,10 +74,11 @@ __global__ void k_sub_from(double *__restrict__ r, const double *__restrict__ b,
 
 static unsigned blocks_for(int64_t n) { return (unsigned)((n + 255) / 256); }
 
-void launch_dots(const double *V, int nv, int64_t n, const double *w, double *partial, double *out, cudaStream_t st) {
-  if (nv <= 0) return;
+int launch_dots(const double *V, int nv, int64_t n, const double *w, double *partial, double *out, cudaStream_t st) {
+  if (nv <= 0) return 0;
   k_dots_partial<<<kDotBlocks, kDotThreads, 0, st>>>(V, nv, n, w, partial);
   k_dots_final<<<(nv + 63) / 64, 64, 0, st>>>(partial, nv, kDotBlocks, out);
+  return 2;
 }
 void launch_gs_update(double *w, const double *V, const double *h, int nv, int64_t n, cudaStream_t st) {
   if (n > 0 && nv > 0) k_gs_update<<<blocks_for(n), 256, 0, st>>>(w, V, h, nv, n);

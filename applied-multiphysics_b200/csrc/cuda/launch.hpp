@@ -24,11 +24,11 @@ void launch_trsm(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, T *Lx
                  __nv_bfloat16 *Shi, __nv_bfloat16 *Slo, const LdltArgs<T> &ld, cudaStream_t st);
 void launch_ldlt_tau(const double *values, const DevPlan &P, double *scal, cudaStream_t st);
 // whole small fronts of one level: tiny (m <= 32, warp per front; sorted by m, the first ntinyMid with m <= 16) and
-// small (m <= 128, CTA per front; maxM = their largest m)
+// small (m <= 128, CTA per front; maxM = their largest m); returns the kernels launched
 template <class T>
-void launch_fronts_small(const int *tiny, int ntiny, int ntinyMid, const int *small, int nsmall, int maxM,
-                         const DevPlan &P, const double *values, T *Lx, T *U, unsigned long long *status,
-                         const LdltArgs<T> &la, cudaStream_t st);
+int launch_fronts_small(const int *tiny, int ntiny, int ntinyMid, const int *small, int nsmall, int maxM,
+                        const DevPlan &P, const double *values, T *Lx, T *U, unsigned long long *status,
+                        const LdltArgs<T> &la, cudaStream_t st);
 // narrow: 128 x 64 tiles (tasks whose columns are one 64-column pivot block), else 128 x 256
 void launch_update_mx(const MixTask *tasks, int64_t ntasks, const CUtensorMap *maps, float *L32, float *U32,
                       unsigned long long *status, int num_sms, cudaStream_t st, bool narrow = false);
