@@ -112,6 +112,8 @@ SIGNATURES = {
     "amp_factor_download": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "amp_factor_destroy": (None, [C.c_void_p]),
     "amp_matvec": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    "amp_factor_set_wait_limit": (C.c_int, [C.c_void_p, C.c_int64]),
+    "amp_matvec_csr": (C.c_int, [C.c_int32, _i32p, _i32p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int]),
     "amp_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
     "amp_profile_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
     "amp_profile_launches": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
@@ -422,6 +424,11 @@ class NumericFactor:
         _check(lib().amp_solve_refined(self._h, C.c_void_p(b_ptr), q, C.c_void_p(x_ptr), 0, C.byref(ro), C.byref(st)))
         return st.rel_residual, st.steps
 
+    def set_wait_limit(self, polls: int) -> None:
+        """Bound of this factor's device waits in polls (0 = the defaults, about a second). A wait that runs out
+        makes the call raise AmpError with code AMP_DEVICE_TIMEOUT; the device stays usable."""
+        _check(lib().amp_factor_set_wait_limit(self._h, int(polls)))
+
     def matVec(self, x) -> np.ndarray:
         xa = _f64(x)
         y = np.empty_like(xa)
@@ -482,12 +489,17 @@ def solveNumericMulti(num: NumericFactor, bs: Sequence, outs=None) -> list:
     return res
 
 
-def matVec(pat, val, x, out=None) -> np.ndarray:
-    """y = A x on full CSR storage (sparse.mjs:219-228), host arithmetic for the caller's convenience."""
-    import scipy.sparse as sp
-    n = int(pat.n)
-    A = sp.csr_matrix((_f64(val), np.asarray(pat.colidx), np.asarray(pat.rowptr)), shape=(n, n))
-    y = A @ _f64(x)
+def matVec(pat, val, x, out=None, device: int = 0) -> np.ndarray:
+    """y = A x on full CSR storage (sparse.mjs:219-228), computed on the GPU (amp_matvec_csr)."""
+    n, rp, ci = _pat(pat)
+    v = _f64(val)
+    xa = _f64(x)
+    y = np.empty_like(xa)
+    q = xa.shape[0] if xa.ndim == 2 else 1
+    if len(v) != int(rp[-1] if n else 0):
+        raise ValueError(f"matVec: {len(v)} values for a pattern with {int(rp[-1]) if n else 0} entries")
+    _check(lib().amp_matvec_csr(n, rp, ci, v.ctypes.data if v.size else None, xa.ctypes.data if xa.size else None, q,
+                                y.ctypes.data if y.size else None, device))
     if out is not None:
         out[:] = y
         return out

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -182,6 +183,7 @@ struct amp_factor_s {
   __nv_bfloat16 *dWhi = nullptr, *dWlo = nullptr;   // mixed LDL^T: BF16 split of L21 D
   CUtensorMap *dMaps = nullptr;                     // per supernode: TMA descriptors of the split A and B operands
   unsigned long long *dStatus = nullptr;
+  long long waitSpins = 0;  // bound of the device waits in polls (0 = the kernels' defaults)
   bool ok = false, hasValues = false;
   // profiling: events around every launch while enabled
   bool profiling = false;
@@ -237,6 +239,7 @@ void upload_plan(amp_plan *pl) {
   DevMem &m = pl->mem;
   amp::DevPlan &d = pl->dp;
   d.n = P.n;
+  d.spin = amp::kSpinLimit;
   d.nsuper = P.nsuper;
   d.maxFront = P.maxFront;
   if (P.nsuper == 0) return;
@@ -420,12 +423,12 @@ void enqueue_factor(amp_factor *f) {
         if (sr.mixMid > sr.mix0)
           timed(f, K_UPDATE, sr.updateFlopsA, 0.0, [&] {
             amp::launch_update_mx(f->plan->dMixTile + sr.mix0, sr.mixMid - sr.mix0, f->dMaps, f->dL32, f->dU32,
-                                  f->dStatus, amp::num_sms(), st, true);
+                                  f->dStatus, amp::num_sms(), st, true, f->waitSpins);
           });
         if (sr.mix1 > sr.mixMid)
           la.part_b(K_UPDATE, sr.updateFlopsB, [&] {
             amp::launch_update_mx(f->plan->dMixTile + sr.mixMid, sr.mix1 - sr.mixMid, f->dMaps, f->dL32, f->dU32,
-                                  f->dStatus, amp::num_sms(), f->side);
+                                  f->dStatus, amp::num_sms(), f->side, false, f->waitSpins);
           });
       }
       la.join();
@@ -433,7 +436,7 @@ void enqueue_factor(amp_factor *f) {
       if (u1 > u0)
         timed(f, K_UPDATE, P.uLvlFlops[L], 0.0, [&] {
           amp::launch_update_mx(f->plan->dMixU + u0, u1 - u0, f->dMaps, f->dL32, f->dU32, f->dStatus,
-                                amp::num_sms(), st);
+                                amp::num_sms(), st, false, f->waitSpins);
         });
     }
     if (P.nflags)
@@ -498,9 +501,16 @@ void enqueue_factor(amp_factor *f) {
 }
 
 // y (permuted order, q vectors) := A^-1 y in place
+// the plan's device view with this factor's wait bound
+amp::DevPlan solve_view(const amp_factor *f) {
+  amp::DevPlan dp = f->plan->dp;
+  if (f->waitSpins > 0) dp.spin = f->waitSpins;
+  return dp;
+}
+
 void device_solve_permuted(amp_factor *f) {
   const amp::Plan &P = f->plan->P;
-  const amp::DevPlan &dp = f->plan->dp;
+  const amp::DevPlan dp = solve_view(f);
   const double lbytes = (f->dL32 ? 4.0 : 8.0) * (double)P.nnzLStored;  // each sweep reads L once
   cudaStream_t st = f->stream;
   ck(cudaMemsetAsync(f->dTickets, 0, sizeof(int) * 2, st), "memset tickets");
@@ -552,7 +562,7 @@ void device_solve(amp_factor *f, const double *dB, double *dX) {
 // y (permuted order, interleaved) := A^-1 y in place
 void device_solve_multi_permuted(amp_factor *f, int q) {
   const amp::Plan &P = f->plan->P;
-  const amp::DevPlan &dp = f->plan->dp;
+  const amp::DevPlan dp = solve_view(f);
   const double lbytes = (f->dL32 ? 4.0 : 8.0) * (double)P.nnzLStored;  // each sweep reads L once for all q vectors
   const double flops = 2.0 * (double)P.nnzLStored * q;
   cudaStream_t st = f->stream;
@@ -661,6 +671,20 @@ int solve_many(amp_factor *f, const double *b, int nrhs, double *x, bool on_devi
     stt->steps = maxSteps;
   }
   return (int)AMP_OK;
+}
+
+// Kernel attributes (large dynamic shared memory) belong to each device's context: set them once per device, with
+// that device current, the first time a factor is created on it. Host threads creating factors on the same device
+// take turns.
+void init_device_once(int dev) {
+  static std::mutex mu;
+  static std::vector<char> done;
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev < 0) throw std::runtime_error("invalid device ordinal");
+  if ((size_t)dev >= done.size()) done.resize(dev + 1, 0);
+  if (done[dev]) return;
+  ck(amp::init_kernel_attributes(), "cudaFuncSetAttribute");
+  done[dev] = 1;
 }
 
 template <class F>
@@ -915,11 +939,7 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
       f->dTickets = f->mem.alloc<int>(2);
       f->dDone = f->mem.alloc<int>((size_t)std::max(1, P.nsuper));
       f->dSolveStatus = f->mem.alloc<unsigned long long>(1);
-      static bool attrs = false;
-      if (!attrs) {
-        amp::init_kernel_attributes();
-        attrs = true;
-      }
+      init_device_once(pl->device);
     } catch (...) {
       delete f;
       throw;
@@ -985,6 +1005,9 @@ int amp_factor_numeric(amp_factor *f, const double *values, int64_t nvalues, int
     if (status == amp::kStatusOk) {
       r.ok = 1;
       f->ok = true;
+    } else if (((status >> 24) & 0xff) == 3) {  // a bounded device wait gave up: not a numerical result
+      if (res) *res = r;
+      return fail(AMP_DEVICE_TIMEOUT, "factorNumeric: a device wait timed out");
     } else {
       r.ok = 0;
       r.fail_column = (int32_t)(status >> 32);
@@ -1259,6 +1282,20 @@ int amp_factor_download(const amp_factor *f, double *Lx, double *D) {
 
 void amp_factor_destroy(amp_factor *f) { delete f; }
 
+int amp_factor_set_wait_limit(amp_factor *f, int64_t polls) {
+  return guarded([&] {
+    if (!f || polls < 0) return fail(AMP_INVALID, "set_wait_limit: null handle or negative bound");
+    if (polls != f->waitSpins && f->factorGraph) {  // the captured factorization holds the old bound
+      ck(cudaSetDevice(f->plan->device), "cudaSetDevice");
+      ck(cudaStreamSynchronize(f->stream), "sync");
+      ck(cudaGraphExecDestroy(f->factorGraph), "graph destroy");
+      f->factorGraph = nullptr;
+    }
+    f->waitSpins = polls;
+    return (int)AMP_OK;
+  });
+}
+
 int amp_profile_enable(amp_factor *f, int enable) {
   if (!f) return fail(AMP_INVALID, "null handle");
   f->profiling = enable != 0;
@@ -1309,6 +1346,29 @@ int amp_profile_read(amp_factor *f, amp_kernel_stat *stats, int32_t cap, int32_t
     if (count) *count = c;
     f->recs.clear();
     f->evUsed = 0;
+    return (int)AMP_OK;
+  });
+}
+
+int amp_matvec_csr(int32_t n, const int32_t *rowptr, const int32_t *colidx, const double *values, const double *x,
+                   int32_t nrhs, double *y, int device) {
+  return guarded([&] {
+    if (n < 0 || nrhs < 0 || (n > 0 && (!rowptr || !colidx || !values || !x || !y)))
+      return fail(AMP_INVALID, "matVec: invalid arguments");
+    if (n == 0 || nrhs == 0) return (int)AMP_OK;
+    ck(cudaSetDevice(device), "cudaSetDevice");
+    const int64_t nnz = rowptr[n];
+    DevMem m;
+    int *dRp = m.alloc<int>((size_t)n + 1), *dCi = m.alloc<int>((size_t)nnz);
+    double *dV = m.alloc<double>((size_t)nnz), *dX = m.alloc<double>((size_t)n * nrhs),
+           *dY = m.alloc<double>((size_t)n * nrhs);
+    ck(cudaMemcpy(dRp, rowptr, sizeof(int) * ((size_t)n + 1), cudaMemcpyHostToDevice), "copy rowptr");
+    ck(cudaMemcpy(dCi, colidx, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice), "copy colidx");
+    ck(cudaMemcpy(dV, values, sizeof(double) * (size_t)nnz, cudaMemcpyHostToDevice), "copy values");
+    ck(cudaMemcpy(dX, x, sizeof(double) * (size_t)n * nrhs, cudaMemcpyHostToDevice), "copy x");
+    amp::launch_matvec(n, dRp, dCi, dV, dX, dY, nrhs, nullptr);
+    ck(cudaGetLastError(), "kernel launch");
+    ck(cudaMemcpy(y, dY, sizeof(double) * (size_t)n * nrhs, cudaMemcpyDeviceToHost), "copy y");
     return (int)AMP_OK;
   });
 }

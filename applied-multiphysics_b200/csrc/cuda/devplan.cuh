@@ -20,6 +20,7 @@ struct DevPlan {
   const int64_t *invOff;   // offset of the inverse of each diagonal block (w x w, column-major)
   const int *diagSlot;     // CSR slot of A(i, i), original row i (the LDL^T pivot scale)
   const int *solveSmall;   // supernodes solved whole by one warp (solve tasks of kind 2 index this list)
+  long long spin;          // bound of every inter-CTA wait of the solve sweeps, in polls (kSpinLimit by default)
 };
 
 // LDL^T variant of the panel and update kernels (ldlt.mjs:450-562); all null for Cholesky.
@@ -31,6 +32,9 @@ struct LdltArgs {
   double *D;           // the pivots, permuted order
   __nv_bfloat16 *Whi, *Wlo;  // mixed precision: BF16 split of L21 D (the A operand of the tensor-core update)
 };
+
+// Default bound of an inter-CTA wait of the solve sweeps, in polls (about a second with their back-off).
+constexpr long long kSpinLimit = 1ll << 24;
 
 // Failure record: the lowest failing global column wins (atomicMin), code in the low bits.
 // kStatusOk means no failure. code 1: Cholesky pivot not > 0; code 2: non-finite LDL^T pivot; code 3: device timeout.

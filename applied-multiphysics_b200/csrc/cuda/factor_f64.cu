@@ -611,21 +611,23 @@ __global__ void k_permute_out(const double *__restrict__ y, double *__restrict__
 // ---------------------------------------------------------------------------------------------------------------
 static int g_num_sms = 148;
 
-void init_mixed_attributes();
-void init_solve_attributes();
-void init_solve_multi_attributes();
-void init_front_small_attributes();
-void init_kernel_attributes() {
-  cudaFuncSetAttribute(k_trsm<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsmSmem);
-  cudaFuncSetAttribute(k_trsm<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsmSmem);
-  init_mixed_attributes();
-  init_solve_attributes();
-  init_solve_multi_attributes();
-  init_front_small_attributes();
-  cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, kUpdateSmem);
+cudaError_t init_mixed_attributes();
+cudaError_t init_solve_attributes();
+cudaError_t init_solve_multi_attributes();
+cudaError_t init_front_small_attributes();
+cudaError_t init_kernel_attributes() {
+  // function attributes belong to the current device's context: the caller runs this once per device
+  cudaError_t e = cudaFuncSetAttribute(k_trsm<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsmSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_trsm<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsmSmem);
+  if (e == cudaSuccess) e = init_mixed_attributes();
+  if (e == cudaSuccess) e = init_solve_attributes();
+  if (e == cudaSuccess) e = init_solve_multi_attributes();
+  if (e == cudaSuccess) e = init_front_small_attributes();
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, kUpdateSmem);
   int dev = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+  return e;
 }
 
 template <class T>

@@ -14,12 +14,17 @@
 // streams) race on the array; callers must serialise them. The first call on a device looks up the array's device
 // address (cudaGetSymbolAddress) with that device current and caches it; make that first call before relying on
 // anything else about the call sequence on that device.
+//
+// After a pivot failure (*fail_column >= 0) F holds a partial result, as the reference's factorization leaves its
+// front after ok = false: the pivot blocks before the failing one are factored, their trailing updates applied, and
+// the failing block and everything right of it are left as the last completed update wrote them.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <string>
 
 #include "../../../include/ampsolve.h"
@@ -32,6 +37,7 @@ void set_last_error(const std::string &msg);
 namespace {
 
 constexpr int kNoAllocMaxFront = 16384;                  // largest front m this entry point accepts
+constexpr int kNoAllocMaxDevices = 64;                   // device ordinals 0 .. 63
 constexpr int kNaRows = 256;                             // panel rows per CTA (one thread per row)
 constexpr int kNoAllocBlocks = kNoAllocMaxFront / kPanel; // pivot blocks of the largest front
 // [0] status word, [1 + k] readers of pivot block k: (1 + 256) x 8 bytes
@@ -194,28 +200,39 @@ extern "C" AMP_API int amp_front_factor_noalloc(double *F, int32_t m, int32_t nc
   }
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= 64) {
+  if (e != cudaSuccess) {
     set_last_error(std::string("amp_front_factor_noalloc: cudaGetDevice: ") + cudaGetErrorString(e));
     return AMP_CUDA_ERROR;
   }
-  // device address of the scratch array, looked up once per device with that device current
-  static unsigned long long *s_addr[64] = {nullptr};
-  if (!s_addr[dev]) {
-    unsigned long long *ptr = nullptr;
-    e = cudaGetSymbolAddress((void **)&ptr, g_front_scratch);
-    if (e != cudaSuccess || !ptr) {
-      set_last_error(std::string("amp_front_factor_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-      return AMP_CUDA_ERROR;
-    }
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(k_front_update_na, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           2 * kPanel * kNaLd * (int)sizeof(double));
-      attr = true;
-    }
-    s_addr[dev] = ptr;
+  if (dev < 0 || dev >= kNoAllocMaxDevices) {
+    set_last_error("amp_front_factor_noalloc: device ordinal " + std::to_string(dev) + " is outside the supported 0.." +
+                   std::to_string(kNoAllocMaxDevices - 1));
+    return AMP_INVALID;
   }
-  unsigned long long *scratch = s_addr[dev];
+  // Set-up once per device, with that device current: the device address of the scratch array and the kernel's
+  // dynamic shared memory limit (a per-device attribute). Host threads making first calls take turns.
+  static std::mutex s_mu;
+  static unsigned long long *s_addr[kNoAllocMaxDevices] = {nullptr};
+  unsigned long long *scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(s_mu);
+    if (!s_addr[dev]) {
+      unsigned long long *ptr = nullptr;
+      e = cudaGetSymbolAddress((void **)&ptr, g_front_scratch);
+      if (e != cudaSuccess || !ptr) {
+        set_last_error(std::string("amp_front_factor_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        return AMP_CUDA_ERROR;
+      }
+      e = cudaFuncSetAttribute(k_front_update_na, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               2 * kPanel * kNaLd * (int)sizeof(double));
+      if (e != cudaSuccess) {
+        set_last_error(std::string("amp_front_factor_noalloc: cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+        return AMP_CUDA_ERROR;
+      }
+      s_addr[dev] = ptr;
+    }
+    scratch = s_addr[dev];
+  }
   cudaStream_t st = (cudaStream_t)stream;
   const int blocks = (nc + kPanel - 1) / kPanel;
   // the array keeps the last call's contents: reset the status word (all ones = no failure) and the counters

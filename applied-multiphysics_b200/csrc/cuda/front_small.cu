@@ -209,13 +209,16 @@ __global__ void __launch_bounds__(256) k_front_small(const int *__restrict__ fro
                            threadIdx.x, &cm);
 }
 
-void init_front_small_attributes() {
-  cudaFuncSetAttribute(k_front_small<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       kSmallFront * kSmallFront * (int)sizeof(double));
-  cudaFuncSetAttribute(k_front_small<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       kSmallFront * kSmallFront * (int)sizeof(float));
-  cudaFuncSetAttribute(k_front_small<float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       kSmallFront * kSmallFront * (int)sizeof(double));
+cudaError_t init_front_small_attributes() {
+  cudaError_t e = cudaFuncSetAttribute(k_front_small<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kSmallFront * kSmallFront * (int)sizeof(double));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_front_small<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kSmallFront * kSmallFront * (int)sizeof(float));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_front_small<float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kSmallFront * kSmallFront * (int)sizeof(double));
+  return e;
 }
 
 template <class T, class TC, int MAXM>

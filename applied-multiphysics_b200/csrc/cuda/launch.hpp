@@ -11,7 +11,7 @@
 
 namespace amp {
 
-void init_kernel_attributes();  // once per process and device, before the first launch
+cudaError_t init_kernel_attributes();  // once per device (with that device current), before its first launch
 
 template <class T>
 void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, const double *values, T *Lx, T *U,
@@ -30,8 +30,10 @@ int launch_fronts_small(const int *tiny, int ntiny, int ntinyMid, const int *sma
                         const DevPlan &P, const double *values, T *Lx, T *U, unsigned long long *status,
                         const LdltArgs<T> &la, cudaStream_t st);
 // narrow: 128 x 64 tiles (tasks whose columns are one 64-column pivot block), else 128 x 256
+// spin: bound of each role's wait in polls (0 = the default, about 0.5 s)
 void launch_update_mx(const MixTask *tasks, int64_t ntasks, const CUtensorMap *maps, float *L32, float *U32,
-                      unsigned long long *status, int num_sms, cudaStream_t st, bool narrow = false);
+                      unsigned long long *status, int num_sms, cudaStream_t st, bool narrow = false,
+                      long long spin = 0);
 int num_sms();
 void launch_update(const TileTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, double *U, const double *W,
                    const unsigned long long *status, cudaStream_t st);

@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(256, 3) k_fwd_blocks(const int4 *__restrict__ 
         chA[tid] = make_int2(0, muc);
         chMap[tid] = P.eaPtr[c];
         chT[tid] = P.snTOff[c];
-        ok = wait_count(done + c, (muc + kSB - 1) / kSB, status, s);
+        ok = wait_count(done + c, (muc + kSB - 1) / kSB, status, s, P.spin);
       }
       if (!__syncthreads_and(ok)) return false;  // block-uniform
       for (int q = 0; q < nq; q++) {
@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(256, 3) k_fwd_blocks(const int4 *__restrict__ 
         chA[tid] = make_int2(a0, lo);
         chMap[tid] = P.eaPtr[c];
         chT[tid] = P.snTOff[c];
-        ok = wait_count(done + c, (muc + kSB - 1) / kSB, status, s);
+        ok = wait_count(done + c, (muc + kSB - 1) / kSB, status, s, P.spin);
       }
       if (!__syncthreads_and(ok)) return false;  // block-uniform
       for (int q = 0; q < nq; q++) {
@@ -322,7 +322,7 @@ __global__ void __launch_bounds__(256, 3) k_fwd_blocks(const int4 *__restrict__ 
           const int c = cn + part + 4 * u;
           ln[u] = (rowok && c < ncols) ? Lp[(int64_t)c * m + r0 + row] : (TL)0;
         }
-        if (tid == 0) waitOk = wait_flag(myflags + cb, epoch, status, s);
+        if (tid == 0) waitOk = wait_flag(myflags + cb, epoch, status, s, P.spin);
         __syncthreads();
         if (!waitOk) return false;  // block-uniform
         const int cbase = cb * kSB;
@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(256, 3) k_fwd_blocks(const int4 *__restrict__ 
       int ok = 1;
       if (tid < 2 * kSB) {
         unsigned lo = 0;
-        ok = wait_tagged(hand + (slot0 + blk - 1) * 2 * kSB + tid, epoch, status, s, lo);
+        ok = wait_tagged(hand + (slot0 + blk - 1) * 2 * kSB + tid, epoch, status, s, lo, P.spin);
         hw[tid] = lo;
       }
       if (!__syncthreads_and(ok)) return false;  // block-uniform
@@ -501,7 +501,7 @@ __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ 
         const int g0 = __shfl_sync(0xffffffffu, idx, 0);
         const int k = g0 < fp + ncp ? max(0, g0 - fp) / kSB : nbp - 1;
         if (k < ready && wok) {
-          wok = warp_wait(pflags + k, epoch, true, status, s);
+          wok = warp_wait(pflags + k, epoch, true, status, s, P.spin);
           ready = k;
         }
         if (idx >= 0 && wok) {
@@ -532,7 +532,7 @@ __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ 
     for (int rb = nb - 1; rb > rbLast; rb--) {
       TL ln[2][8];
       load_block(rb - 1, ln);
-      if (tid == 0) waitOk = wait_flag(myflags + rb, epoch, status, s);
+      if (tid == 0) waitOk = wait_flag(myflags + rb, epoch, status, s, P.spin);
       __syncthreads();
       if (!waitOk) return false;  // block-uniform
 #pragma unroll
@@ -577,7 +577,7 @@ __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ 
       int ok = 1;
       if (tid < 2 * wn) {
         unsigned lo = 0;
-        ok = wait_tagged(hand + (slot0 + blk) * 2 * kSB + tid, epoch, status, s, lo);
+        ok = wait_tagged(hand + (slot0 + blk) * 2 * kSB + tid, epoch, status, s, lo, P.spin);
         hw[tid] = lo;
       }
       if (!__syncthreads_and(ok)) return false;  // block-uniform
@@ -598,7 +598,7 @@ __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ 
     // block b's flag stands for every later block (the children's rows-below waits rely on it): acquire block
     // b + 1's flag, taken above without an acquire, before releasing ours after the barrier
     int fok = 1;
-    if (tid == 0 && hasNext) fok = wait_flag(myflags + blk + 1, epoch, status, s);
+    if (tid == 0 && hasNext) fok = wait_flag(myflags + blk + 1, epoch, status, s, P.spin);
     if (!__syncthreads_and(fok)) return false;  // block-uniform
     if (tid == 0) st_release(myflags + blk, epoch);
     return true;
@@ -612,11 +612,14 @@ __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ 
   }
 }
 
-void init_solve_attributes() {
-  cudaFuncSetAttribute(k_bwd_blocks<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBwdSmem);
-  cudaFuncSetAttribute(k_bwd_blocks<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBwdSmem);
-  cudaFuncSetAttribute(k_chain_mats<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kChainSmem);
-  cudaFuncSetAttribute(k_chain_mats<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kChainSmem);
+cudaError_t init_solve_attributes() {
+  cudaError_t e = cudaFuncSetAttribute(k_bwd_blocks<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBwdSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_bwd_blocks<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBwdSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_chain_mats<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kChainSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_chain_mats<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kChainSmem);
+  return e;
 }
 
 int num_sms();

@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_fwd_multi(const int4 *__re
       for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
         const int c = P.chList[qq];
         const int need = (P.snM[c] - P.snNc[c] + kMB - 1) / kMB;
-        if (tid == 0) waitOk = wait_count(done + c, need, status, s);
+        if (tid == 0) waitOk = wait_count(done + c, need, status, s, P.spin);
         __syncthreads();
         if (!waitOk) return false;
       }
@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_fwd_multi(const int4 *__re
     for (int ch = 0; ch < nch; ch++) {
       const int cb = ch * kKC, cw = min(kKC, ncols - cb);
       if ((cb & (kMB - 1)) == 0) {  // first chunk of a pivot block: its y values final?
-        if (tid == 0) waitOk = wait_flag(myflags + cb / kMB, epoch, status, s);
+        if (tid == 0) waitOk = wait_flag(myflags + cb / kMB, epoch, status, s, P.spin);
         __syncthreads();
         if (!waitOk) return false;
       }
@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_bwd_multi(const int4 *__re
     int *myflags = flags + P.blkOff[s];
     const int par = P.snParent[s];
     if (par >= 0) {
-      if (tid == 0) waitOk = wait_flag(flags + P.blkOff[par], epoch, status, s);
+      if (tid == 0) waitOk = wait_flag(flags + P.blkOff[par], epoch, status, s, P.spin);
       __syncthreads();
       if (!waitOk) return false;
     }
@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_bwd_multi(const int4 *__re
     for (int ch = 0; ch < nch; ch++) {
       const bool anc = ch < nanc;
       if (!anc && ((ch - nanc) & 1) == 0) {  // first chunk of a pivot block: its x values final?
-        if (tid == 0) waitOk = wait_flag(myflags + rb / kMB, epoch, status, s);
+        if (tid == 0) waitOk = wait_flag(myflags + rb / kMB, epoch, status, s, P.spin);
         __syncthreads();
         if (!waitOk) return false;
       }
@@ -483,11 +483,12 @@ __global__ void __launch_bounds__(256) k_residual_multi(int n, const int *__rest
   }
 }
 
-void init_solve_multi_attributes() {
-  cudaFuncSetAttribute(k_fwd_multi<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMultiSmem);
-  cudaFuncSetAttribute(k_fwd_multi<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMultiSmem);
-  cudaFuncSetAttribute(k_bwd_multi<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMultiSmem);
-  cudaFuncSetAttribute(k_bwd_multi<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMultiSmem);
+cudaError_t init_solve_multi_attributes() {
+  cudaError_t e = cudaFuncSetAttribute(k_fwd_multi<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMultiSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fwd_multi<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMultiSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_bwd_multi<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMultiSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_bwd_multi<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMultiSmem);
+  return e;
 }
 
 int num_sms();

@@ -17,9 +17,10 @@ namespace amp {
 
 // lane 0 waits (bounded) until *p == v (eq) or *p >= v; the result is broadcast to the warp, and the warp barrier
 // orders the other lanes' later loads after lane 0's acquire
-__device__ __forceinline__ bool warp_wait(const int *p, int v, bool eq, unsigned long long *status, int s) {
+__device__ __forceinline__ bool warp_wait(const int *p, int v, bool eq, unsigned long long *status, int s,
+                                          long long limit) {
   int ok = 1;
-  if ((threadIdx.x & 31) == 0) ok = eq ? wait_flag(p, v, status, s) : wait_count(p, v, status, s);
+  if ((threadIdx.x & 31) == 0) ok = eq ? wait_flag(p, v, status, s, limit) : wait_count(p, v, status, s, limit);
   ok = __shfl_sync(0xffffffffu, ok, 0);
   __syncwarp();
   return ok != 0;
@@ -31,7 +32,7 @@ __device__ __forceinline__ bool warp_wait_children(const DevPlan &P, int s, cons
   for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
     const int c = P.chList[qq];
     const int need = (P.snM[c] - P.snNc[c] + 63) / 64;
-    if (!warp_wait(done + c, need, false, status, s)) return false;
+    if (!warp_wait(done + c, need, false, status, s, P.spin)) return false;
   }
   return true;
 }
@@ -81,7 +82,7 @@ __device__ bool small_bwd_warp(int s, const DevPlan &P, const TL *__restrict__ L
   const int lane = threadIdx.x & 31;
   const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
   const int par = P.snParent[s];
-  if (par >= 0 && m > nc && !warp_wait(flags + P.blkOff[par], epoch, true, status, s)) return false;
+  if (par >= 0 && m > nc && !warp_wait(flags + P.blkOff[par], epoch, true, status, s, P.spin)) return false;
   double x = 0.0;
   if (lane >= nc && lane < m) {
     x = __ldcg(y + P.Si[P.Sp[s] + lane]);
@@ -163,7 +164,7 @@ __device__ bool small_bwd_warp_multi(int s, const DevPlan &P, const TL *__restri
   const int k0 = lane, k1 = lane + 32;
   const bool v0 = k0 < q, v1 = k1 < q;
   const int par = P.snParent[s];
-  if (par >= 0 && m > nc && !warp_wait(flags + P.blkOff[par], epoch, true, status, s)) return false;
+  if (par >= 0 && m > nc && !warp_wait(flags + P.blkOff[par], epoch, true, status, s, P.spin)) return false;
   const int *rowsOf = P.Si + P.Sp[s];
   for (int r = 0; r < m; r++) {
     const int64_t gi = r < nc ? f + r : rowsOf[r];

@@ -9,7 +9,6 @@
 
 namespace amp {
 
-constexpr long long kSpinLimit = 1ll << 24;  // ~ seconds with the back-off below
 
 __device__ __forceinline__ int ld_acquire(const int *p) {
   int v;
@@ -44,13 +43,15 @@ __device__ __forceinline__ double untag(unsigned lo, unsigned hi) {
   return __longlong_as_double((long long)(((unsigned long long)hi << 32) | lo));
 }
 
+// The waits below poll at most `limit` times (DevPlan::spin: kSpinLimit unless the caller set a bound).
+
 // Wait until the tag of *w is epoch and return its low 32 bits in lo; false on time-out (status set for s).
 __device__ __forceinline__ bool wait_tagged(const unsigned long long *w, int epoch, unsigned long long *status, int s,
-                                            unsigned &lo) {
+                                            unsigned &lo, long long limit) {
   long long spins = 0;
   unsigned long long v;
   while (((v = ld_relaxed_u64(w)) >> 32) != (unsigned long long)(unsigned)epoch) {
-    if (++spins > kSpinLimit) {
+    if (++spins > limit) {
       atomicMin(status, status_word(0x7fffffff, 3, s));
       return false;
     }
@@ -61,10 +62,11 @@ __device__ __forceinline__ bool wait_tagged(const unsigned long long *w, int epo
 }
 
 // Wait until *flag == epoch; false on time-out (status set for supernode s).
-__device__ __forceinline__ bool wait_flag(const int *flag, int epoch, unsigned long long *status, int s) {
+__device__ __forceinline__ bool wait_flag(const int *flag, int epoch, unsigned long long *status, int s,
+                                          long long limit) {
   long long spins = 0;
   while (ld_acquire(flag) != epoch) {
-    if (++spins > kSpinLimit) {
+    if (++spins > limit) {
       atomicMin(status, status_word(0x7fffffff, 3, s));
       return false;
     }
@@ -74,10 +76,11 @@ __device__ __forceinline__ bool wait_flag(const int *flag, int epoch, unsigned l
 }
 
 // Wait until *cnt >= need; false on time-out (status set for supernode s).
-__device__ __forceinline__ bool wait_count(const int *cnt, int need, unsigned long long *status, int s) {
+__device__ __forceinline__ bool wait_count(const int *cnt, int need, unsigned long long *status, int s,
+                                           long long limit) {
   long long spins = 0;
   while (ld_acquire(cnt) < need) {
-    if (++spins > kSpinLimit) {
+    if (++spins > limit) {
       atomicMin(status, status_word(0x7fffffff, 3, s));
       return false;
     }

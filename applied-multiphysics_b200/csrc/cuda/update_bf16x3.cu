@@ -46,7 +46,7 @@ constexpr uint32_t kKStep = 16 * 128;                     // one K16 step (2 gro
 constexpr int kEpiPerQuad = 2;                           // epilogue warps per TMEM lane quadrant
 constexpr int kEpiWarps = 4 * kEpiPerQuad;
 constexpr int kThreads = 32 * (2 + kEpiWarps);
-constexpr long long kSpin = 1ll << 22;                    // ~0.5 s with back-off
+constexpr long long kMxSpin = 1ll << 22;                  // default bound of a role's wait: ~0.5 s with back-off
 }  // namespace
 
 template <int N>
@@ -58,9 +58,11 @@ struct MxShared {
   int abort;
 };
 
-// Bounded wait that also gives up when another role raised the abort flag. false: aborted or timed out.
-__device__ __forceinline__ bool mx_wait(uint64_t *bar, uint32_t parity, MxShared &sh, unsigned long long *status) {
-  for (long long i = 0; i < kSpin; i++) {
+// Bounded wait (at most `limit` polls) that also gives up when another role raised the abort flag. false: aborted
+// or timed out. The drains before the tensor memory is freed keep their own bound (umma::mbar_wait), whatever limit.
+__device__ __forceinline__ bool mx_wait(uint64_t *bar, uint32_t parity, MxShared &sh, unsigned long long *status,
+                                        long long limit) {
+  for (long long i = 0; i < limit; i++) {
     if (umma::mbar_try_wait(bar, parity)) return true;
     if (*(volatile int *)&sh.abort) return false;
     if (i > 64) __nanosleep(128);
@@ -75,7 +77,7 @@ template <int N>
 __global__ void __launch_bounds__(kThreads, 1) k_update_mx(const MixTask *__restrict__ tasks, int ntasks,
                                                            const CUtensorMap *__restrict__ maps,
                                                            float *__restrict__ L32, float *__restrict__ U32,
-                                                           unsigned long long *status) {
+                                                           unsigned long long *status, long long spin) {
   constexpr uint32_t kBBytes = b_bytes<N>(), kStageBytes = stage_bytes<N>(), kTmemCols = 2 * N;
   constexpr uint32_t kIdesc = umma::idesc_bf16_f32_mn(kM, N);
   constexpr int kN = N;
@@ -115,7 +117,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_update_mx(const MixTask *__rest
         for (int c = 0; c < nch; c++, it++) {
           const int s = it % kStages;
           const uint32_t n = it / kStages;
-          if (!mx_wait(&sh.empty[s], (n & 1) ^ 1, sh, status)) {
+          if (!mx_wait(&sh.empty[s], (n & 1) ^ 1, sh, status, spin)) {
             ok = false;
             break;
           }
@@ -147,13 +149,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_update_mx(const MixTask *__rest
         const MixTask tk = tasks[t];
         const int nch = (tk.w + kK - 1) / kK;
         const int a = tl & 1;
-        if (!mx_wait(&sh.accEmpty[a], ((tl >> 1) & 1) ^ 1, sh, status)) break;
+        if (!mx_wait(&sh.accEmpty[a], ((tl >> 1) & 1) ^ 1, sh, status, spin)) break;
         umma::tc_fence_after();
         const uint32_t d = tmem + a * kN;
         bool ok = true;
         for (int c = 0; c < nch; c++, it++) {
           const int s = it % kStages;
-          if (!mx_wait(&sh.full[s], (it / kStages) & 1, sh, status)) {
+          if (!mx_wait(&sh.full[s], (it / kStages) & 1, sh, status, spin)) {
             ok = false;
             break;
           }
@@ -185,7 +187,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_update_mx(const MixTask *__rest
       const MixTask tk = tasks[t];
       const int a = tl & 1;
       bool ok = true;
-      if (lane == 0) ok = mx_wait(&sh.accFull[a], (tl >> 1) & 1, sh, status);
+      if (lane == 0) ok = mx_wait(&sh.accFull[a], (tl >> 1) & 1, sh, status, spin);
       if (!__shfl_sync(0xffffffffu, ok ? 1 : 0, 0)) break;
       umma::tc_fence_after();
       const int i = tk.i0 + 32 * q + lane, m = tk.m, nc = tk.nc, mu = m - nc;
@@ -229,19 +231,22 @@ __global__ void __launch_bounds__(kThreads, 1) k_update_mx(const MixTask *__rest
   }
 }
 
-void init_mixed_attributes() {
-  cudaFuncSetAttribute(k_update_mx<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, mixed_smem<256>());
-  cudaFuncSetAttribute(k_update_mx<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, mixed_smem<64>());
+cudaError_t init_mixed_attributes() {
+  cudaError_t e = cudaFuncSetAttribute(k_update_mx<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, mixed_smem<256>());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_update_mx<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, mixed_smem<64>());
+  return e;
 }
 
 void launch_update_mx(const MixTask *tasks, int64_t ntasks, const CUtensorMap *maps, float *L32, float *U32,
-                      unsigned long long *status, int num_sms, cudaStream_t st, bool narrow) {
+                      unsigned long long *status, int num_sms, cudaStream_t st, bool narrow, long long spin) {
   if (ntasks <= 0) return;
   const int grid = (int)(ntasks < num_sms ? ntasks : num_sms);
+  if (spin <= 0) spin = kMxSpin;
   if (narrow)
-    k_update_mx<64><<<grid, kThreads, mixed_smem<64>(), st>>>(tasks, (int)ntasks, maps, L32, U32, status);
+    k_update_mx<64><<<grid, kThreads, mixed_smem<64>(), st>>>(tasks, (int)ntasks, maps, L32, U32, status, spin);
   else
-    k_update_mx<256><<<grid, kThreads, mixed_smem<256>(), st>>>(tasks, (int)ntasks, maps, L32, U32, status);
+    k_update_mx<256><<<grid, kThreads, mixed_smem<256>(), st>>>(tasks, (int)ntasks, maps, L32, U32, status, spin);
 }
 
 }  // namespace amp

@@ -112,7 +112,7 @@ def heat3d_p2(N: int = 48, nsph: int = 64, radius: float = 0.05, seed: int = 4, 
 
 
 # k^2 of the 32^3 driven Maxwell system: midway between its 10th (34.3115) and 11th (36.2170) nonzero eigenvalues,
-# found by inertia bisection with the GPU LDL^T (maxwell_k2.py 32, on a B200).
+# found by inertia bisection with the GPU LDL^T (tests/golden/maxwell_k2.py 32, on a B200).
 MAXWELL_K2_32 = 35.2642118891234
 
 

@@ -89,7 +89,7 @@ typedef enum {
 } amp_field;
 
 typedef struct {
-  int kind;         /* amp_factor_kind; AMP_LDLT requires AMP_FP64 */
+  int kind;         /* amp_factor_kind; either kind in either precision (mixed LDL^T: FP32 fronts, BF16x3 updates) */
   int precision;    /* amp_precision */
 } amp_factor_opts;
 
@@ -178,6 +178,12 @@ AMP_API int amp_solve_gmres(amp_factor *f, const double *b, double *x, int on_de
 /* num.Lx (the m x nc column-major blocks at Lxp) and D (LDL^T) copied to host; either pointer may be null. */
 AMP_API int amp_factor_download(const amp_factor *f, double *Lx, double *D);
 AMP_API void amp_factor_destroy(amp_factor *f);
+/* Bound of this factor's device waits, in polls (0 = the defaults: about a second for the solve sweeps' inter-CTA
+ * waits, half a second for the tensor-core update's pipeline waits). A wait that runs out ends its kernel early and
+ * the call returns AMP_DEVICE_TIMEOUT; the device stays usable. No counterpart in the reference (its solver runs on
+ * one CPU thread and never waits); for callers that want a stuck device reported sooner, and for tests of that path.
+ * Changing the bound discards the factor's captured factorization graph (it is captured again on the next call). */
+AMP_API int amp_factor_set_wait_limit(amp_factor *f, int64_t polls);
 
 /* Per-kernel-class device time of the calls made while profiling is on (CUDA events around every launch on the
  * factor's stream; graphs are not used meanwhile). Algorithmic flops / bytes are the counts the work requires.
@@ -198,6 +204,10 @@ AMP_API int amp_profile_launches(amp_factor *f, int32_t *kinds, double *ms, doub
 
 /* matVec(pat, val, x) (sparse.mjs:219-228) on the device: y = A x for nrhs vectors (host pointers). */
 AMP_API int amp_matvec(amp_factor *f, const double *x, int32_t nrhs, double *y);
+/* matVec(pat, val, x) (sparse.mjs:219-228) without a factor: y = A x for nrhs vectors on device `device` (host
+ * pointers; the call allocates its device buffers and waits for the result). */
+AMP_API int amp_matvec_csr(int32_t n, const int32_t *rowptr, const int32_t *colidx, const double *values,
+                           const double *x, int32_t nrhs, double *y, int device);
 
 /* Partial Cholesky of ONE dense front in place, allocating nothing. No counterpart in the reference's API.
  * For callers that cannot call cudaMalloc: applications that give all device memory to their own pool at start-up,
@@ -206,8 +216,10 @@ AMP_API int amp_matvec(amp_factor *f, const double *x, int32_t nrhs, double *y);
  * (m - nc) block receives the Schur update. Limit: m <= 16384; larger fronts are rejected with AMP_INVALID.
  * Scratch: a static device array of 2 KB per GPU that loads the library, kept until exit and shared by every call
  * (each call resets it); calls that overlap on the GPU race on it. The first call on a device looks up the array's
- * address with that device current. stream: a cudaStream_t (null = default stream); the call waits for its work.
- * *fail_column: -1, or the first pivot column that was not positive. */
+ * address with that device current (devices 0..63); the look-up is serialised across host threads. stream: a
+ * cudaStream_t (null = default stream); the call waits for its work.
+ * *fail_column: -1, or the first pivot column that was not positive. After a failure F holds a partial result: the
+ * pivot blocks before the failing one are factored and their updates applied; the rest is as those updates left it. */
 AMP_API int amp_front_factor_noalloc(double *F, int32_t m, int32_t nc, void *stream, int32_t *fail_column);
 
 /* Message of the last failing call on this thread ("" when none). */

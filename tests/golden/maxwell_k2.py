@@ -8,14 +8,19 @@ for sigma > 0
 
 Bisection on that count with the GPU LDL^T gives lambda_10 and lambda_11; k2 is their midpoint. Run on a GPU:
 
-    python applied-multiphysics_b200/maxwell_k2.py 32
+    python tests/golden/maxwell_k2.py 32
+
+This is the recipe of the stored constant workloads.MAXWELL_K2_32; nothing imports it.
 """
 from __future__ import annotations
 
+import os
 import sys
 
-import ampsolve as amp
-import workloads as wl
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "..", "applied-multiphysics_b200"))
+
+import ampsolve as amp  # noqa: E402
+import workloads as wl  # noqa: E402
 
 
 def inertia_counter(N: int, nbox: int = 8, eps_in: float = 12.0, seed: int = 5):

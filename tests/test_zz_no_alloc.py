@@ -26,12 +26,12 @@ def _dense_spd(n, seed):
     return M @ M.T + n * np.eye(n)
 
 
-def _noalloc(F_dev_ptr, m, nc):
+def _noalloc(F_dev_ptr, m, nc, stream=None):
     fn = amp.lib().amp_front_factor_noalloc
     fn.restype = C.c_int
     fn.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.POINTER(C.c_int32)]
     fail = C.c_int32(-2)
-    code = fn(C.c_void_p(F_dev_ptr), m, nc, None, C.byref(fail))
+    code = fn(C.c_void_p(F_dev_ptr), m, nc, None if stream is None else C.c_void_p(stream), C.byref(fail))
     return code, fail.value
 
 
@@ -81,6 +81,29 @@ def test_noalloc_partial_front_schur_and_failure():
     Fb = torch.from_numpy(B.copy().reshape(-1)).cuda()
     code, fail = _noalloc(Fb.data_ptr(), 64, 64)
     assert code == amp.AMP_OK and fail == 0
+
+
+@pytest.mark.parametrize("m,nc", [(1024, 512), (1100, 640)])
+def test_noalloc_on_a_stream_multi_chunk(m, nc):
+    """A caller's own stream, several 256-row panel chunks per pivot block (the last-reader counter with more than
+    two readers), nc a multiple of 64 and not, two calls in a row against numpy's Cholesky and Schur complement."""
+    torch = pytest.importorskip("torch")
+    st = torch.cuda.Stream()
+    for seed in (21, 22):
+        A = _dense_spd(m, seed)
+        with torch.cuda.stream(st):
+            F = torch.from_numpy(A.T.copy().reshape(-1)).to("cuda", non_blocking=False)
+        st.synchronize()
+        code, fail = _noalloc(F.data_ptr(), m, nc, stream=st.cuda_stream)
+        assert code == amp.AMP_OK and fail == -1, amp.lib().amp_last_error()
+        R = F.cpu().numpy().reshape(m, m).T
+        L11 = np.linalg.cholesky(A[:nc, :nc])
+        L21 = np.linalg.solve(L11, A[:nc, nc:]).T
+        S = A[nc:, nc:] - L21 @ L21.T
+        low = np.tril(np.ones((m - nc, m - nc), bool))
+        assert np.max(np.abs(np.tril(R[:nc, :nc]) - L11)) <= TOL * np.max(np.abs(L11))
+        assert np.max(np.abs(R[nc:, :nc] - L21)) <= TOL * np.max(np.abs(L21))
+        assert np.max(np.abs(R[nc:, nc:][low] - S[low])) <= TOL * np.max(np.abs(S))
 
 
 def test_noalloc_rejects_oversized_front():
