@@ -23,7 +23,8 @@ def test_reference_arm_line():
     for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
               "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
         assert k in d, k
-    assert d["steps"] == 2 and d["warmup"] == 1 and d["n_gpus"] == 1
+    assert 1 <= d["steps"] <= 2 and d["steps_requested"] == 2 and d["warmup"] == 1 and d["n_gpus"] == 1
+    assert d["ms_per_step"] > 0 and "complete factor + solve" in d["cpu_baseline"]["sample"]
     assert d["value"] > 0 and d["higher_is_better"] is True
     assert d["config"]["workload"].startswith("elastic3d-8")
     cb = d["cpu_baseline"]
