@@ -85,6 +85,16 @@ class _RefineStats(C.Structure):
     _fields_ = [("rel_residual", C.c_double), ("steps", C.c_int32)]
 
 
+class _EigenOpts(C.Structure):
+    _fields_ = [("n_want", C.c_int32), ("block_size", C.c_int32), ("max_basis", C.c_int32),
+                ("max_restarts", C.c_int32), ("tol", C.c_double), ("seed", C.c_uint32)]
+
+
+class _EigenStats(C.Structure):
+    _fields_ = [("converged", C.c_int32), ("restarts", C.c_int32), ("op_vectors", C.c_int32), ("basis", C.c_int32),
+                ("max_residual", C.c_double), ("ms", C.c_double)]
+
+
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 
@@ -114,6 +124,10 @@ SIGNATURES = {
     "amp_matvec": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "amp_factor_set_wait_limit": (C.c_int, [C.c_void_p, C.c_int64]),
     "amp_matvec_csr": (C.c_int, [C.c_int32, _i32p, _i32p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int]),
+    "amp_factor_set_mass": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int]),
+    "amp_shift_invert_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int]),
+    "amp_eigen_block_arnoldi": (C.c_int, [C.c_void_p, C.POINTER(_EigenOpts), C.c_void_p, C.c_void_p, C.c_int,
+                                          C.POINTER(_EigenStats)]),
     "amp_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
     "amp_profile_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
     "amp_profile_launches": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
@@ -423,6 +437,33 @@ class NumericFactor:
         ro = _RefineOpts(maxSteps, tol)
         _check(lib().amp_solve_refined(self._h, C.c_void_p(b_ptr), q, C.c_void_p(x_ptr), 0, C.byref(ro), C.byref(st)))
         return st.rel_residual, st.steps
+
+    def set_mass(self, mvalues) -> None:
+        """M's values on the factored pattern (the shift-invert operator op(X) = A^-1 M X, eigen.ts:150-160)."""
+        m = _f64(mvalues)
+        _check(lib().amp_factor_set_mass(self._h, m.ctypes.data if m.size else None, m.size, 0))
+
+    def shift_invert_apply(self, X: np.ndarray) -> np.ndarray:
+        """A^-1 (M X) for X (m, n) or (n,) on the device."""
+        Xa = _f64(X)
+        m = Xa.shape[0] if Xa.ndim == 2 else 1
+        Y = np.empty_like(Xa)
+        _check(lib().amp_shift_invert_apply(self._h, Xa.ctypes.data, m, Y.ctypes.data, 0))
+        return Y
+
+    def block_arnoldi(self, nWant: int, blockSize: int = 1, maxBasis: int = 0, tol: float = 1e-10,
+                      maxRestarts: int = 60, seed: int = 20261014):
+        """blockArnoldi with op = shift_invert_apply on the device (la/arnoldi.mjs:36-200): (mu (nWant,), Ritz
+        vectors (nWant, n), stats dict); mu by decreasing modulus."""
+        n = self.sym.n
+        mu = np.zeros(max(nWant, 1))
+        vecs = np.zeros((max(nWant, 1), n))
+        st = _EigenStats()
+        o = _EigenOpts(nWant, blockSize, maxBasis, maxRestarts, tol, seed & 0xFFFFFFFF)
+        _check(lib().amp_eigen_block_arnoldi(self._h, C.byref(o), mu.ctypes.data, vecs.ctypes.data, 0, C.byref(st)))
+        stats = {"converged": bool(st.converged), "restarts": st.restarts, "opVectors": st.op_vectors,
+                 "basis": st.basis, "maxResidual": st.max_residual, "ms": st.ms}
+        return mu[:nWant], vecs[:nWant], stats
 
     def set_wait_limit(self, polls: int) -> None:
         """Bound of this factor's device waits in polls (0 = the defaults, about a second). A wait that runs out

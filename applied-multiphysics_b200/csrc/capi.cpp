@@ -4,6 +4,8 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -217,7 +219,13 @@ struct amp_factor_s {
   int *dRowGroup = nullptr;
   double *dGroupNorms = nullptr;  // 2 x groups x multi_max_vectors()
   DevMem groupMem;
+  // shift-invert eigen operator: M's values on the pattern; Krylov workspace (grown on demand)
+  double *dMass = nullptr;
+  DevMem massMem, eigMem;
+  int64_t eigCap = 0;
   ~amp_factor_s() {
+    eigMem.release();
+    massMem.release();
     if (factorGraph) cudaGraphExecDestroy(factorGraph);
     for (auto e : evPool) cudaEventDestroy(e);
     smem.release();
@@ -700,6 +708,91 @@ int guarded(F &&fn) {
     return fail(AMP_INVALID, e.what());
   }
 }
+
+}  // namespace
+
+
+// ---- shift-invert eigen operator and the device block Lanczos / Arnoldi (eigen.ts:116-175, arnoldi.mjs:36-200) ----
+namespace {
+
+// Y = A^-1 (M X) for m device vectors (one after another); T: n m scratch. Synchronises; returns an amp_status.
+int device_shift_invert(amp_factor *f, const double *dX, int m, double *dY, double *dT) {
+  const amp::Plan &P = f->plan->P;
+  cudaStream_t st = f->stream;
+  amp::launch_matvec(P.n, f->plan->dRowptr, f->plan->dColidx, f->dMass, dX, dT, m, st);
+  if (m > 1) return solve_many(f, dT, m, dY, true, nullptr, nullptr);
+  ensure_solve_ws(f, 1);
+  device_solve(f, dT, dY);
+  ck(cudaGetLastError(), "kernel launch");
+  ck(cudaStreamSynchronize(st), "shift-invert");
+  return solve_status(f);
+}
+
+// Eigen-decomposition of a symmetric p x p matrix S (row-major) by cyclic Jacobi rotations: S = Q diag(w) Q^T,
+// Q row-major (column c of Q is the eigenvector of w[c]).
+void jacobi_eigen(int p, std::vector<double> S, std::vector<double> &w, std::vector<double> &Q) {
+  Q.assign((size_t)p * p, 0.0);
+  for (int i = 0; i < p; i++) Q[(size_t)i * p + i] = 1.0;
+  for (int sweep = 0; sweep < 100; sweep++) {
+    double off = 0.0, tot = 0.0;
+    for (int i = 0; i < p; i++)
+      for (int j = 0; j < p; j++) {
+        const double v = S[(size_t)i * p + j] * S[(size_t)i * p + j];
+        tot += v;
+        if (i != j) off += v;
+      }
+    if (off <= 1e-30 * tot || off == 0.0) break;
+    for (int a = 0; a < p - 1; a++)
+      for (int c = a + 1; c < p; c++) {
+        const double sac = S[(size_t)a * p + c];
+        if (sac == 0.0) continue;
+        const double theta = (S[(size_t)c * p + c] - S[(size_t)a * p + a]) / (2.0 * sac);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double cs = 1.0 / std::sqrt(t * t + 1.0), sn = t * cs;
+        for (int k = 0; k < p; k++) {  // S <- S J (columns a, c)
+          const double ska = S[(size_t)k * p + a], skc = S[(size_t)k * p + c];
+          S[(size_t)k * p + a] = cs * ska - sn * skc;
+          S[(size_t)k * p + c] = sn * ska + cs * skc;
+        }
+        for (int k = 0; k < p; k++) {  // S <- J^T S (rows a, c)
+          const double sak = S[(size_t)a * p + k], sck = S[(size_t)c * p + k];
+          S[(size_t)a * p + k] = cs * sak - sn * sck;
+          S[(size_t)c * p + k] = sn * sak + cs * sck;
+        }
+        for (int k = 0; k < p; k++) {  // Q <- Q J
+          const double qka = Q[(size_t)k * p + a], qkc = Q[(size_t)k * p + c];
+          Q[(size_t)k * p + a] = cs * qka - sn * qkc;
+          Q[(size_t)k * p + c] = sn * qka + cs * qkc;
+        }
+      }
+  }
+  w.resize(p);
+  for (int i = 0; i < p; i++) w[i] = S[(size_t)i * p + i];
+}
+
+struct EigenWork {
+  amp_factor *f;
+  int64_t n;
+  double *part, *dh;
+  std::vector<double> h;
+  // h[j] = A_j . w for the nv device vectors A (n each), synchronised
+  const std::vector<double> &dots(const double *A, int nv, const double *w) {
+    cudaStream_t st = f->stream;
+    h.resize(std::max(nv, 1));
+    amp::launch_dots(A, nv, n, w, part, dh, st);
+    ck(cudaMemcpyAsync(h.data(), dh, sizeof(double) * nv, cudaMemcpyDeviceToHost, st), "dots");
+    ck(cudaStreamSynchronize(st), "dots");
+    return h;
+  }
+  // out = sum_j c[j] A_j (nv device vectors A); out is overwritten
+  void combine(double *out, const double *A, const std::vector<double> &c, int nv) {
+    cudaStream_t st = f->stream;
+    ck(cudaMemsetAsync(out, 0, sizeof(double) * n, st), "zero");
+    ck(cudaMemcpyAsync(dh, c.data(), sizeof(double) * nv, cudaMemcpyHostToDevice, st), "coefficients");
+    amp::launch_combine_add(out, A, dh, nv, n, st);
+    ck(cudaStreamSynchronize(st), "combine");  // dh is reused by the next call
+  }
+};
 
 }  // namespace
 
@@ -1346,6 +1439,246 @@ int amp_profile_read(amp_factor *f, amp_kernel_stat *stats, int32_t cap, int32_t
     if (count) *count = c;
     f->recs.clear();
     f->evUsed = 0;
+    return (int)AMP_OK;
+  });
+}
+
+
+int amp_factor_set_mass(amp_factor *f, const double *mvalues, int64_t nvalues, int on_device) {
+  return guarded([&] {
+    if (!f || (nvalues > 0 && !mvalues)) return fail(AMP_INVALID, "set_mass: null handle or values");
+    const amp::Plan &P = f->plan->P;
+    if (nvalues != P.patNnz)
+      return fail(AMP_BAD_LENGTH, "setMass: " + std::to_string(nvalues) + " values for a pattern with " +
+                                      std::to_string(P.patNnz) + " entries");
+    ck(cudaSetDevice(f->plan->device), "cudaSetDevice");
+    if (!f->dMass) f->dMass = f->massMem.alloc<double>((size_t)P.patNnz);
+    if (nvalues)
+      ck(cudaMemcpy(f->dMass, mvalues, sizeof(double) * nvalues,
+                    on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice), "copy mass");
+    return (int)AMP_OK;
+  });
+}
+
+int amp_shift_invert_apply(amp_factor *f, const double *X, int32_t m, double *Y, int on_device) {
+  return guarded([&] {
+    if (!f) return fail(AMP_INVALID, "null handle");
+    if (!f->ok) return fail(AMP_NO_FACTOR, "solveNumeric: no successful numeric factorization");
+    if (!f->dMass) return fail(AMP_INVALID, "shift-invert: no mass values (amp_factor_set_mass)");
+    const amp::Plan &P = f->plan->P;
+    if (m <= 0 || P.n == 0) return (int)AMP_OK;
+    ck(cudaSetDevice(f->plan->device), "cudaSetDevice");
+    const size_t len = (size_t)P.n * m;
+    DevMem tmp;
+    double *dT = tmp.alloc<double>(len);
+    const double *dX = X;
+    double *dY = Y;
+    if (!on_device) {
+      double *a = tmp.alloc<double>(len), *b = tmp.alloc<double>(len);
+      ck(cudaMemcpy(a, X, sizeof(double) * len, cudaMemcpyHostToDevice), "copy X");
+      dX = a;
+      dY = b;
+    }
+    if (int rc = device_shift_invert(f, dX, m, dY, dT)) return rc;
+    if (!on_device) ck(cudaMemcpy(Y, dY, sizeof(double) * len, cudaMemcpyDeviceToHost), "copy Y");
+    return (int)AMP_OK;
+  });
+}
+
+int amp_eigen_block_arnoldi(amp_factor *f, const amp_eigen_opts *opts, double *mu, double *vecs, int on_device,
+                            amp_eigen_stats *stats) {
+  return guarded([&] {
+    if (!f || !opts || !mu) return fail(AMP_INVALID, "eigen: null argument");
+    if (!f->ok) return fail(AMP_NO_FACTOR, "solveNumeric: no successful numeric factorization");
+    if (!f->dMass) return fail(AMP_INVALID, "eigen: no mass values (amp_factor_set_mass)");
+    const amp::Plan &P = f->plan->P;
+    const int64_t n = P.n;
+    const amp_eigen_opts o = *opts;
+    const int b = std::max(1, o.block_size), nw = o.n_want;
+    if (nw < 1 || n < 2) return fail(AMP_INVALID, "eigen: need n_want >= 1 and n >= 2");
+    // basis per cycle p (a multiple of b) as the reference sizes it (arnoldi.mjs:37-41), capped by n
+    int p = std::max(o.max_basis > 0 ? o.max_basis : std::max(30, 2 * nw + 12), nw + 3 * b);
+    p = (p + b - 1) / b * b;
+    if (p + b > n) p = (int)((n - b) / b * b);
+    if (p < nw + b) return fail(AMP_INVALID, "eigen: the system is too small for n_want Ritz pairs");
+    const int nKeep = std::max(nw, std::min(nw + std::max(2, nw), p - 2 * b));
+    const double tol = o.tol > 0 ? o.tol : 1e-10;
+    const int maxRestarts = o.max_restarts > 0 ? o.max_restarts : 60;
+    ck(cudaSetDevice(f->plan->device), "cudaSetDevice");
+    cudaStream_t st = f->stream;
+    const auto t0 = std::chrono::steady_clock::now();
+    // workspace: V, MV ((p + b) n each), W, MW, T (b n each), U (nKeep n), dot partials
+    const int64_t need = (int64_t)(2 * (p + b) + 3 * b + nKeep) * n + (int64_t)(p + b) * (amp::dot_partials() + 1);
+    if (need > f->eigCap) {
+      f->eigMem.release();
+      f->eigMem.alloc<double>((size_t)need);
+      f->eigCap = need;
+    }
+    double *base = (double *)f->eigMem.ptrs[0];
+    double *V = base, *MV = V + (p + b) * n, *W = MV + (p + b) * n, *MW = W + b * n, *T = MW + b * n,
+           *U = T + b * n, *part = U + (int64_t)nKeep * n, *dh = part + (int64_t)(p + b) * amp::dot_partials();
+    EigenWork ew{f, n, part, dh, {}};
+    // start block: the reference's LCG (arnoldi.mjs seededRandom), vector after vector
+    {
+      uint32_t s = o.seed ? o.seed : 20261014u;
+      std::vector<double> x0((size_t)b * n);
+      for (auto &v : x0) {
+        s = s * 1664525u + 1013904223u;
+        v = (double)s / 4294967296.0 - 0.5;
+      }
+      ck(cudaMemcpy(V, x0.data(), sizeof(double) * x0.size(), cudaMemcpyHostToDevice), "start block");
+    }
+    int opVectors = 0;
+    // M-orthonormalise the b vectors at X (M X at MX): X <- X R^-1 with R^T R = X^T M X; R to Rout (b x b,
+    // row-major) when given. false when the block is (numerically) dependent.
+    auto orthonormalise = [&](double *X, double *MX, std::vector<double> *Rout) -> bool {
+      amp::launch_matvec((int)n, f->plan->dRowptr, f->plan->dColidx, f->dMass, X, MX, b, st);
+      std::vector<double> G((size_t)b * b), R((size_t)b * b, 0.0);
+      for (int j = 0; j < b; j++) {
+        const auto &h = ew.dots(X, b, MX + (int64_t)j * n);
+        for (int i = 0; i < b; i++) G[(size_t)i * b + j] = h[i];
+      }
+      for (int j = 0; j < b; j++) {  // Cholesky G = R^T R (R upper)
+        double d = G[(size_t)j * b + j];
+        for (int k = 0; k < j; k++) d -= R[(size_t)k * b + j] * R[(size_t)k * b + j];
+        if (!(d > 1e-28 * std::max(1.0, G[0]))) return false;
+        R[(size_t)j * b + j] = std::sqrt(d);
+        for (int i = j + 1; i < b; i++) {
+          double s2 = G[(size_t)j * b + i];
+          for (int k = 0; k < j; k++) s2 -= R[(size_t)k * b + j] * R[(size_t)k * b + i];
+          R[(size_t)j * b + i] = s2 / R[(size_t)j * b + j];
+        }
+      }
+      std::vector<double> Ri((size_t)b * b, 0.0);  // R^-1 (upper)
+      for (int c = 0; c < b; c++) {
+        Ri[(size_t)c * b + c] = 1.0 / R[(size_t)c * b + c];
+        for (int i = c - 1; i >= 0; i--) {
+          double s2 = 0.0;
+          for (int k = i + 1; k <= c; k++) s2 += R[(size_t)i * b + k] * Ri[(size_t)k * b + c];
+          Ri[(size_t)i * b + c] = -s2 / R[(size_t)i * b + i];
+        }
+      }
+      for (double *Z : {X, MX}) {
+        for (int c = 0; c < b; c++) {
+          std::vector<double> coef(b);
+          for (int j = 0; j < b; j++) coef[j] = Ri[(size_t)j * b + c];
+          ew.combine(T + (int64_t)c * n, Z, coef, b);
+        }
+        ck(cudaMemcpyAsync(Z, T, sizeof(double) * b * n, cudaMemcpyDeviceToDevice, st), "copy block");
+      }
+      if (Rout) *Rout = R;
+      return true;
+    };
+    if (!orthonormalise(V, MV, nullptr)) return fail(AMP_INVALID, "eigen: degenerate start block");
+    // H: projected matrix, (p + b) x p row-major; ncur basis vectors, the last block the one to expand
+    std::vector<double> H((size_t)(p + b) * p, 0.0);
+    int ncur = b, restarts = 0;
+    bool converged = false, exhausted = false;
+    std::vector<double> w, Q, res;
+    std::vector<int> order;
+    int pc = 0;  // projected size of the last Rayleigh-Ritz
+    for (;;) {
+      // expand the last block until the basis holds p + b vectors (or the Krylov space is exhausted)
+      while (ncur < p + b) {
+        const int c0 = ncur - b;
+        if (int rc = device_shift_invert(f, V + (int64_t)c0 * n, b, W, T)) return rc;
+        opVectors += b;
+        for (int c = 0; c < b; c++) {  // two passes of block Gram-Schmidt in the M inner product (DGKS)
+          double *wc = W + (int64_t)c * n;
+          for (int pass = 0; pass < 2; pass++) {
+            const auto &h = ew.dots(MV, ncur, wc);
+            std::vector<double> hv(h.begin(), h.begin() + ncur);
+            ck(cudaMemcpyAsync(dh, hv.data(), sizeof(double) * ncur, cudaMemcpyHostToDevice, st), "h");
+            amp::launch_gs_update(wc, V, dh, ncur, n, st);
+            ck(cudaStreamSynchronize(st), "gs");
+            for (int i = 0; i < ncur; i++) H[(size_t)i * p + c0 + c] += hv[i];
+          }
+        }
+        std::vector<double> R;
+        if (!orthonormalise(W, MW, &R)) {  // an invariant subspace: the Ritz values of the basis are exact
+          exhausted = true;
+          break;
+        }
+        for (int i = 0; i < b; i++)
+          for (int c = 0; c < b; c++) H[(size_t)(ncur + i) * p + c0 + c] = R[(size_t)i * b + c];
+        ck(cudaMemcpyAsync(V + (int64_t)ncur * n, W, sizeof(double) * b * n, cudaMemcpyDeviceToDevice, st), "append");
+        ck(cudaMemcpyAsync(MV + (int64_t)ncur * n, MW, sizeof(double) * b * n, cudaMemcpyDeviceToDevice, st),
+           "append");
+        ncur += b;
+      }
+      // Rayleigh-Ritz on the symmetrised projected matrix of the expanded columns
+      pc = exhausted ? ncur : ncur - b;
+      std::vector<double> S((size_t)pc * pc);
+      for (int i = 0; i < pc; i++)
+        for (int j = 0; j < pc; j++) S[(size_t)i * pc + j] = 0.5 * (H[(size_t)i * p + j] + H[(size_t)j * p + i]);
+      jacobi_eigen(pc, S, w, Q);
+      order.resize(pc);
+      for (int i = 0; i < pc; i++) order[i] = i;
+      std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return std::fabs(w[a]) > std::fabs(w[c]); });
+      // residual of Ritz pair i: || R_last y_i(last block) ||_M (the appended block is M-orthonormal)
+      res.assign(pc, 0.0);
+      if (!exhausted)
+        for (int i = 0; i < pc; i++) {
+          double s2 = 0.0;
+          for (int r = 0; r < b; r++) {
+            double t = 0.0;
+            for (int c = 0; c < b; c++) t += H[(size_t)(pc + r) * p + pc - b + c] * Q[(size_t)(pc - b + c) * pc + i];
+            s2 += t * t;
+          }
+          res[i] = std::sqrt(s2);
+        }
+      converged = true;
+      for (int k = 0; k < std::min(nw, pc); k++)
+        if (!(res[order[k]] <= tol * std::fabs(w[order[k]]))) converged = false;
+      if (converged || exhausted || restarts >= maxRestarts || pc < nw) break;
+      // thick restart: keep the nKeep Ritz vectors of largest |mu| and the residual block
+      const int k = nKeep;
+      for (double *Z : {V, MV}) {
+        for (int c = 0; c < k; c++) {
+          std::vector<double> coef(pc);
+          for (int j = 0; j < pc; j++) coef[j] = Q[(size_t)j * pc + order[c]];
+          ew.combine(U + (int64_t)c * n, Z, coef, pc);
+        }
+        ck(cudaMemcpyAsync(Z + (int64_t)k * n, Z + (int64_t)pc * n, sizeof(double) * b * n, cudaMemcpyDeviceToDevice,
+                           st), "residual block");
+        ck(cudaMemcpyAsync(Z, U, sizeof(double) * k * n, cudaMemcpyDeviceToDevice, st), "kept vectors");
+      }
+      std::vector<double> Hn((size_t)(p + b) * p, 0.0);
+      for (int c = 0; c < k; c++) {
+        Hn[(size_t)c * p + c] = w[order[c]];
+        for (int r = 0; r < b; r++) {  // coupling of the residual block: R_last y_c(last block)
+          double t = 0.0;
+          for (int cc = 0; cc < b; cc++) t += H[(size_t)(pc + r) * p + pc - b + cc] * Q[(size_t)(pc - b + cc) * pc + order[c]];
+          Hn[(size_t)(k + r) * p + c] = t;
+        }
+      }
+      H.swap(Hn);
+      ncur = k + b;
+      restarts++;
+    }
+    const int nout = std::min(nw, pc);
+    double worst = 0.0;
+    for (int k = 0; k < nout; k++) {
+      mu[k] = w[order[k]];
+      worst = std::max(worst, res[order[k]] / std::max(std::fabs(w[order[k]]), 1e-300));
+    }
+    if (vecs) {  // Ritz vectors V y (M-orthonormal)
+      for (int k = 0; k < nout; k++) {
+        std::vector<double> coef(pc);
+        for (int j = 0; j < pc; j++) coef[j] = Q[(size_t)j * pc + order[k]];
+        ew.combine(U, V, coef, pc);
+        ck(cudaMemcpy(vecs + (int64_t)k * n, U, sizeof(double) * n,
+                      on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost), "copy Ritz vector");
+      }
+    }
+    if (stats) {
+      stats->converged = converged || exhausted;
+      stats->restarts = restarts;
+      stats->op_vectors = opVectors;
+      stats->basis = p;
+      stats->max_residual = worst;
+      stats->ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
     return (int)AMP_OK;
   });
 }

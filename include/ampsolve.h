@@ -209,6 +209,42 @@ AMP_API int amp_matvec(amp_factor *f, const double *x, int32_t nrhs, double *y);
 AMP_API int amp_matvec_csr(int32_t n, const int32_t *rowptr, const int32_t *colidx, const double *values,
                            const double *x, int32_t nrhs, double *y, int device);
 
+/* ---- shift-invert eigen operator (physics/src/common/eigen.ts:116-175 shiftInvertEigen; la/arnoldi.mjs) ---- */
+/* The factor holds A = K - sigma M (Cholesky or LDL^T). amp_factor_set_mass gives M's values on the same pattern
+ * (nvalues CSR slots, host or device memory; copied to the device once). */
+AMP_API int amp_factor_set_mass(amp_factor *f, const double *mvalues, int64_t nvalues, int on_device);
+/* op(X) = A^-1 (M X) for m vectors of length n one after another (eigen.ts:150-160): M X by the device SpMV, then one
+ * multi-vector solve; host (on_device 0) or device (1) pointers. */
+AMP_API int amp_shift_invert_apply(amp_factor *f, const double *X, int32_t m, double *Y, int on_device);
+
+typedef struct {
+  int32_t n_want;       /* Ritz values wanted: those of largest modulus (eigenvalues nearest the shift) */
+  int32_t block_size;   /* vectors per block (reference default 1) */
+  int32_t max_basis;    /* basis size per cycle (reference default max(30, 2 nWant + 12)) */
+  int32_t max_restarts; /* thick restarts (reference default 60) */
+  double tol;           /* converged when the Ritz residual <= tol |mu| (reference default 1e-10) */
+  uint32_t seed;        /* start block: the reference's LCG (arnoldi.mjs seededRandom) */
+} amp_eigen_opts;
+
+typedef struct {
+  int32_t converged;    /* all n_want Ritz pairs below the tolerance */
+  int32_t restarts;
+  int32_t op_vectors;   /* operator applications (vectors) */
+  int32_t basis;        /* basis size used per cycle */
+  double max_residual;  /* largest Ritz residual / |mu| of the returned pairs */
+  double ms;            /* wall time of the Krylov iteration */
+} amp_eigen_stats;
+
+/* blockArnoldi(n, op, {nWant, blockSize, maxBasis, tol, maxRestarts, seed}) (la/arnoldi.mjs:36-200) with op =
+ * amp_shift_invert_apply, run on the device: the Krylov basis, its M-products and the orthogonalisation live in device
+ * memory and only the small projected matrix is on the host (one round trip per block, none per vector). The basis
+ * is M-orthonormal (op is self-adjoint in the M inner product for symmetric K and M, M positive definite), so the
+ * projected matrix is symmetric; block Lanczos with full reorthogonalisation and thick restart. mu: the n_want Ritz
+ * values of largest modulus, by decreasing |mu| (eigenvalue lambda = sigma + 1 / mu); vecs: the matching M-orthonormal
+ * Ritz vectors, n each one after another, host (on_device 0) or device (1). */
+AMP_API int amp_eigen_block_arnoldi(amp_factor *f, const amp_eigen_opts *opts, double *mu, double *vecs, int on_device,
+                                    amp_eigen_stats *stats);
+
 /* Partial Cholesky of ONE dense front in place, allocating nothing. No counterpart in the reference's API.
  * For callers that cannot call cudaMalloc: applications that give all device memory to their own pool at start-up,
  * or that must not let an allocation stall their other streams. F: device pointer to an m x m column-major front
