@@ -25,6 +25,7 @@ AMP_OK, AMP_NOT_SPD, AMP_NONFINITE_PIVOT, AMP_PATTERN_MISMATCH, AMP_BAD_LENGTH, 
     AMP_DEVICE_TIMEOUT, AMP_CUDA_ERROR, AMP_OOM, AMP_INVALID = range(11)
 ORDER_AMD, ORDER_ND, ORDER_ND3, ORDER_GIVEN = range(4)
 CHOLESKY, LDLT = 0, 1
+AMP_ELEM_P1_TRI_SCALAR, AMP_ELEM_P1_TET_ELASTIC = 0, 1
 FP64, MIXED = 0, 1
 
 FIELDS = ["perm", "pinv", "parent", "colCount", "lowerP", "lowerI", "lowerSrc", "superStart", "colSuper",
@@ -125,6 +126,10 @@ SIGNATURES = {
     "amp_factor_set_wait_limit": (C.c_int, [C.c_void_p, C.c_int64]),
     "amp_matvec_csr": (C.c_int, [C.c_int32, _i32p, _i32p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int]),
     "amp_factor_set_mass": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int]),
+    "amp_assembly_create": (C.c_int, [C.c_int, C.c_int32, _i32p, _i32p, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p,
+                                      C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "amp_assemble": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
+    "amp_assembly_destroy": (None, [C.c_void_p]),
     "amp_shift_invert_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int]),
     "amp_eigen_block_arnoldi": (C.c_int, [C.c_void_p, C.POINTER(_EigenOpts), C.c_void_p, C.c_void_p, C.c_int,
                                           C.POINTER(_EigenStats)]),
@@ -481,6 +486,41 @@ class NumericFactor:
         h = self.__dict__.get("_h")
         if h and _lib is not None:
             _lib.amp_factor_destroy(h)
+            self._h = None
+
+
+class Assembly:
+    """On-device assembly of a system's CSR values from its mesh (assembleCells, physics/src/common/scalar.ts:96-146,
+    with the element slots of la/sparse.mjs:113-185 computed once): kind AMP_ELEM_P1_TRI_SCALAR (coefficient per
+    triangle) or AMP_ELEM_P1_TET_ELASTIC ((E, nu) per tet)."""
+
+    def __init__(self, kind: int, pat, coords, conn, dofs, device: int = 0):
+        n, rp, ci = _pat(pat)
+        self.kind, self.nnz = kind, int(rp[-1]) if n else 0
+        self._keep = [np.ascontiguousarray(coords, np.float64), np.ascontiguousarray(conn, np.int32),
+                      np.ascontiguousarray(dofs, np.int32)]
+        xy, cn, dm = self._keep
+        h = C.c_void_p()
+        _check(lib().amp_assembly_create(kind, n, rp, ci, xy.shape[0], xy.ctypes.data, cn.shape[0], cn.ctypes.data,
+                                         dm.ctypes.data, device, C.byref(h)))
+        self._h = h.value
+
+    def assemble(self, coef) -> np.ndarray:
+        """The assembled values (host copy) for per-element coefficients."""
+        c = _f64(coef)
+        v = np.empty(self.nnz)
+        _check(lib().amp_assemble(self._h, c.ctypes.data, 0, v.ctypes.data, 0, None))
+        return v
+
+    def assemble_device(self, coef_ptr: int, coef_on_device: bool, values_ptr: int, stream: int = 0) -> None:
+        """Assemble into a device buffer of nnz doubles (coefficients from host or device memory)."""
+        _check(lib().amp_assemble(self._h, C.c_void_p(coef_ptr), 1 if coef_on_device else 0, C.c_void_p(values_ptr),
+                                  1, C.c_void_p(stream) if stream else None))
+
+    def __del__(self):
+        h = self.__dict__.get("_h")
+        if h and _lib is not None:
+            _lib.amp_assembly_destroy(h)
             self._h = None
 
 

@@ -28,6 +28,10 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-Wall", "-I" + os.path.join(CUDA_HOME, "include"),
              "-I" + os.path.join(ROOT, "include")]
 
+# per-source flags: the assembly kernels round every product and sum on its own (no FMA contraction), as the host
+# assembly they reproduce bit for bit
+FILE_FLAGS = {"assemble.cu": ["-fmad=false"]}
+
 SOLVER_LIB = os.path.join(HERE, "libampsolve.so")
 WORK_LIB = os.path.join(HERE, "libampwork.so")
 
@@ -66,7 +70,8 @@ def build(verbose: bool = False, extra_nvcc: list[str] | None = None) -> None:
     for src in cu:
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")
         if _stale(obj, [src]) or os.path.getmtime(obj) < hdr:
-            _run([NVCC] + NVCC_FLAGS + (extra_nvcc or []) + ["-c", src, "-o", obj], verbose)
+            _run([NVCC] + NVCC_FLAGS + FILE_FLAGS.get(os.path.basename(src), []) + (extra_nvcc or []) +
+                 ["-c", src, "-o", obj], verbose)
         objs.append(obj)
     for src in cpp:
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")

@@ -21,6 +21,8 @@
 #include "host/symbolic.hpp"
 
 namespace amp {
+int launch_assemble_values(int kind, int64_t ne, const int *conn, const double *coords, const double *coef, double *Ke,
+                           int64_t nnz, const int64_t *gptr, const uint32_t *gidx, double *values, cudaStream_t st);
 void launch_matvec(int n, const int *rowptr, const int *colidx, const double *val, const double *x, double *y, int q,
                    cudaStream_t st);
 void launch_residual(int n, const int *rowptr, const int *colidx, const double *val, const double *x, const double *b,
@@ -162,6 +164,17 @@ struct amp_plan_s {
   std::vector<int> rowptr, colidx;  // host copy of the pattern (uploaded with the schedule)
   bool uploaded = false;
   ~amp_plan_s() { mem.release(); }
+};
+
+// mesh and element-slot gather map of the on-device assembly
+struct amp_assembly_s {
+  int kind = 0, device = 0, ncoef = 1, nd = 3;
+  int64_t nelem = 0, nnz = 0;
+  DevMem mem;
+  int *dConn = nullptr;
+  double *dCoords = nullptr, *dKe = nullptr, *dCoef = nullptr, *dValues = nullptr;
+  int64_t *dGptr = nullptr;
+  uint32_t *dGidx = nullptr;
 };
 
 struct amp_factor_s {
@@ -1443,6 +1456,106 @@ int amp_profile_read(amp_factor *f, amp_kernel_stat *stats, int32_t cap, int32_t
   });
 }
 
+
+int amp_assembly_create(int kind, int32_t n, const int32_t *rowptr, const int32_t *colidx, int32_t nnodes,
+                        const double *coords, int64_t nelem, const int32_t *conn, const int32_t *dofs, int device,
+                        amp_assembly **out) {
+  return guarded([&] {
+    if (!out || n < 0 || nnodes < 0 || nelem < 0 || !rowptr || (nelem > 0 && (!conn || !coords || !dofs)))
+      return fail(AMP_INVALID, "assembly: invalid arguments");
+    if (kind != AMP_ELEM_P1_TRI_SCALAR && kind != AMP_ELEM_P1_TET_ELASTIC)
+      return fail(AMP_INVALID, "assembly: unknown element kind");
+    *out = nullptr;
+    const int k = kind == AMP_ELEM_P1_TRI_SCALAR ? 3 : 4, bs = kind == AMP_ELEM_P1_TRI_SCALAR ? 1 : 3;
+    const int dim = kind == AMP_ELEM_P1_TRI_SCALAR ? 2 : 3, nd = k * bs;
+    const int64_t nnz = n ? rowptr[n] : 0;
+    if ((uint64_t)nelem * nd * nd >= (1ull << 32)) return fail(AMP_INVALID, "assembly: mesh too large");
+    // element slots (elementSlots / blockElementSlots): slot of local entry (r, c) of element e, or -1
+    std::vector<int64_t> cnt(nnz + 1, 0);
+    std::vector<int> slot((size_t)nelem * nd * nd);
+    for (int64_t e = 0; e < nelem; e++)
+      for (int r = 0; r < nd; r++) {
+        const int vr = conn[k * e + r / bs];
+        if (vr < 0 || vr >= nnodes) return fail(AMP_INVALID, "assembly: connectivity out of range");
+        const int row = dofs[(int64_t)vr * bs + r % bs];
+        for (int c = 0; c < nd; c++) {
+          const int vc = conn[k * e + c / bs];
+          if (vc < 0 || vc >= nnodes) return fail(AMP_INVALID, "assembly: connectivity out of range");
+          const int col = dofs[(int64_t)vc * bs + c % bs];
+          int s = -1;
+          if (row >= 0 && col >= 0) {
+            if (row >= n || col >= n) return fail(AMP_INVALID, "assembly: DOF map out of range");
+            const int32_t *b0 = colidx + rowptr[row], *b1 = colidx + rowptr[row + 1];
+            const int32_t *it = std::lower_bound(b0, b1, col);
+            if (it == b1 || *it != col)
+              return fail(AMP_PATTERN_MISMATCH, "assembly: element " + std::to_string(e) + " couples rows " +
+                                                    std::to_string(row) + " and " + std::to_string(col) +
+                                                    " outside the pattern");
+            s = rowptr[row] + (int)(it - b0);
+            cnt[s + 1]++;
+          }
+          slot[((size_t)e * nd + r) * nd + c] = s;
+        }
+      }
+    for (int64_t s = 0; s < nnz; s++) cnt[s + 1] += cnt[s];
+    std::vector<uint32_t> gidx(cnt[nnz]);
+    {  // contributions of every slot in increasing element order
+      std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
+      for (int64_t e = 0; e < nelem; e++)
+        for (int q = 0; q < nd * nd; q++) {
+          const int s = slot[(size_t)e * nd * nd + q];
+          if (s >= 0) gidx[fill[s]++] = (uint32_t)(e * nd * nd + q);
+        }
+    }
+    auto *a = new amp_assembly_s();
+    try {
+      a->kind = kind;
+      a->device = device;
+      a->nd = nd;
+      a->ncoef = kind == AMP_ELEM_P1_TRI_SCALAR ? 1 : 2;
+      a->nelem = nelem;
+      a->nnz = nnz;
+      ck(cudaSetDevice(device), "cudaSetDevice");
+      a->dConn = a->mem.upload(std::vector<int>(conn, conn + (size_t)nelem * k));
+      a->dCoords = a->mem.upload(std::vector<double>(coords, coords + (size_t)nnodes * dim));
+      a->dGptr = a->mem.upload(cnt);
+      a->dGidx = a->mem.upload(gidx);
+      a->dKe = a->mem.alloc<double>((size_t)nelem * nd * nd);
+      a->dCoef = a->mem.alloc<double>((size_t)nelem * a->ncoef);
+      a->dValues = a->mem.alloc<double>((size_t)nnz);
+    } catch (...) {
+      delete a;
+      throw;
+    }
+    *out = a;
+    return (int)AMP_OK;
+  });
+}
+
+int amp_assemble(amp_assembly *a, const double *coef, int coef_on_device, double *values, int values_on_device,
+                 void *stream) {
+  return guarded([&] {
+    if (!a || (a->nelem > 0 && !coef) || (a->nnz > 0 && !values)) return fail(AMP_INVALID, "assemble: null argument");
+    ck(cudaSetDevice(a->device), "cudaSetDevice");
+    cudaStream_t st = (cudaStream_t)stream;
+    const double *dCoef = coef;
+    if (!coef_on_device && a->nelem > 0) {
+      ck(cudaMemcpyAsync(a->dCoef, coef, sizeof(double) * a->nelem * a->ncoef, cudaMemcpyHostToDevice, st),
+         "copy coefficients");
+      dCoef = a->dCoef;
+    }
+    double *dV = values_on_device ? values : a->dValues;
+    amp::launch_assemble_values(a->kind, a->nelem, a->dConn, a->dCoords, dCoef, a->dKe, a->nnz, a->dGptr, a->dGidx,
+                                dV, st);
+    ck(cudaGetLastError(), "kernel launch");
+    if (!values_on_device && a->nnz > 0)
+      ck(cudaMemcpyAsync(values, dV, sizeof(double) * a->nnz, cudaMemcpyDeviceToHost, st), "copy values");
+    ck(cudaStreamSynchronize(st), "assemble");
+    return (int)AMP_OK;
+  });
+}
+
+void amp_assembly_destroy(amp_assembly *a) { delete a; }
 
 int amp_factor_set_mass(amp_factor *f, const double *mvalues, int64_t nvalues, int on_device) {
   return guarded([&] {

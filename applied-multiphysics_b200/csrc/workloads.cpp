@@ -729,6 +729,82 @@ WL_API amp_workload *amp_wl_chain(int n, double diag, double off) {
   return W;
 }
 
+// The mesh behind a workload, for on-device assembly (the inputs of assembleCells, physics/src/common/scalar.ts:96-146):
+// node coordinates (dim per node), element connectivity (k nodes per element), the DOF map (system row of node v's
+// component c at dofs[v bs + c], -1 for a Dirichlet DOF; the map of restrict_to) and the per-element coefficients.
+//   kind 0: heat2d_lognormal(N, seed) P1 triangles, bs 1, coef = conductivity per triangle (seed 0: all 1, the
+//           Poisson system);
+//   kind 1: elastic3d(N, E, nu) P1 tets, bs 3, x = 0 clamped, coef = (E, nu) per tet.
+// Outputs are malloc'd (free with amp_wl_free_array).
+WL_API int amp_wl_mesh(int kind, int N, uint32_t seed, double E, double nu, int *nnodes, int *dim, double **coords,
+                       int64_t *nelem, int *k, int **conn, int *bs, int **dofs, double **coef, int *ncoef) {
+  std::vector<double> X, Y, Z;
+  std::vector<int> elem;
+  std::vector<char> isFree;
+  std::vector<double> cf;
+  int B = 1, D = 2, K = 3, nn = 0;
+  if (kind == 0) {
+    tri_grid(N, X, Y, elem);
+    nn = (N + 1) * (N + 1);
+    isFree.assign(nn, 0);
+    for (int j = 1; j < N; j++)
+      for (int i = 1; i < N; i++) isFree[i + (N + 1) * j] = 1;
+    cf.assign(elem.size() / 3, 1.0);
+    if (seed) {
+      Lcg r(seed);
+      for (auto &c : cf) c = std::exp(r.normal());
+    }
+  } else if (kind == 1) {
+    const int NX = N + 1;
+    nn = NX * NX * NX;
+    kuhn_tets(N, N, N, elem);
+    X.resize(nn);
+    Y.resize(nn);
+    Z.resize(nn);
+    for (int kk = 0; kk < NX; kk++)
+      for (int j = 0; j < NX; j++)
+        for (int i = 0; i < NX; i++) {
+          const int v = i + NX * (j + NX * kk);
+          X[v] = (double)i / N;
+          Y[v] = (double)j / N;
+          Z[v] = (double)kk / N;
+        }
+    B = 3;
+    D = 3;
+    K = 4;
+    isFree.assign((size_t)nn * 3, 1);
+    for (int v = 0; v < nn; v++)
+      if (v % NX == 0) isFree[3 * v] = isFree[3 * v + 1] = isFree[3 * v + 2] = 0;
+    for (size_t e = 0; e < elem.size() / 4; e++) {
+      cf.push_back(E);
+      cf.push_back(nu);
+    }
+  } else {
+    return 1;
+  }
+  std::vector<double> xyz((size_t)nn * D);
+  for (int v = 0; v < nn; v++) {
+    xyz[(size_t)D * v] = X[v];
+    xyz[(size_t)D * v + 1] = Y[v];
+    if (D == 3) xyz[(size_t)D * v + 2] = Z[v];
+  }
+  std::vector<int> map(isFree.size(), -1);
+  int nf = 0;
+  for (size_t i = 0; i < isFree.size(); i++)
+    if (isFree[i]) map[i] = nf++;
+  *nnodes = nn;
+  *dim = D;
+  *coords = dup(xyz);
+  *nelem = (int64_t)elem.size() / K;
+  *k = K;
+  *conn = dup(elem);
+  *bs = B;
+  *dofs = dup(map);
+  *coef = dup(cf);
+  *ncoef = (int)cf.size();
+  return 0;
+}
+
 // Pattern utilities of the reference (sparse.mjs buildPattern :37-78 for triangles is buildElementPattern with k = 3
 // up to the in-row sort, which gives the same sorted unique rows). Outputs malloc'd arrays.
 WL_API int amp_wl_element_pattern(int n, const int *elem, int64_t ne, int k, int **rowptr, int **colidx) {

@@ -157,3 +157,45 @@ def heat2d_batch_sizes(count: int = 256, seed: int = 3) -> list[tuple[int, int]]
 def heat2d_batch(count: int = 256, seed: int = 3) -> list[Workload]:
     """The batched 2D heat set: `count` lognormal-conductivity P1 problems of uneven size with q_i seeded RHS each."""
     return [heat2d_lognormal(N, seed * 1000 + i, q) for i, (N, q) in enumerate(heat2d_batch_sizes(count, seed))]
+
+
+@dataclass
+class Mesh:
+    """The mesh behind a workload (inputs of on-device assembly): node coordinates (nnodes, dim), connectivity
+    (nelem, k), DOF map (nnodes * bs, -1 for Dirichlet DOFs) and per-element coefficients."""
+    kind: int
+    coords: np.ndarray
+    conn: np.ndarray
+    dofs: np.ndarray
+    coef: np.ndarray
+
+
+def mesh(kind: int, N: int, seed: int = 0, E: float = 1.0, nu: float = 0.3) -> Mesh:
+    """kind 0: the triangles of heat2d_lognormal(N, seed) (seed 0: conductivity 1, the Poisson system); kind 1: the
+    tets of elastic3d(N, E, nu) (3 DOFs per node, x = 0 clamped, (E, nu) per tet)."""
+    L = lib()
+    f = L.amp_wl_mesh
+    f.restype = C.c_int
+    f.argtypes = [C.c_int, C.c_int, C.c_uint32, C.c_double, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                  C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.c_int64), C.POINTER(C.c_int),
+                  C.POINTER(C.POINTER(C.c_int)), C.POINTER(C.c_int), C.POINTER(C.POINTER(C.c_int)),
+                  C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.c_int)]
+    L.amp_wl_free_array.argtypes = [C.c_void_p]
+    nn, dim, k, bs, nco = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    ne = C.c_int64()
+    xy, cf = C.POINTER(C.c_double)(), C.POINTER(C.c_double)()
+    cn, dm = C.POINTER(C.c_int)(), C.POINTER(C.c_int)()
+    if f(kind, N, seed, E, nu, C.byref(nn), C.byref(dim), C.byref(xy), C.byref(ne), C.byref(k), C.byref(cn),
+         C.byref(bs), C.byref(dm), C.byref(cf), C.byref(nco)) != 0:
+        raise ValueError(f"unknown mesh kind {kind}")
+
+    def take(p, ln, dt):
+        a = np.ctypeslib.as_array(p, shape=(ln,)).astype(dt, copy=True)
+        L.amp_wl_free_array(C.cast(p, C.c_void_p))
+        return a
+
+    coords = take(xy, nn.value * dim.value, np.float64).reshape(nn.value, dim.value)
+    conn = take(cn, ne.value * k.value, np.int32).reshape(ne.value, k.value)
+    dofs = take(dm, nn.value * bs.value, np.int32)
+    coef = take(cf, nco.value, np.float64)
+    return Mesh(kind, coords, conn, dofs, coef)

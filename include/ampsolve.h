@@ -209,6 +209,29 @@ AMP_API int amp_matvec(amp_factor *f, const double *x, int32_t nrhs, double *y);
 AMP_API int amp_matvec_csr(int32_t n, const int32_t *rowptr, const int32_t *colidx, const double *values,
                            const double *x, int32_t nrhs, double *y, int device);
 
+/* ---- on-device assembly of the values (physics/src/common/scalar.ts:96-146 assembleCells; la/sparse.mjs:113-185
+ * elementSlots / blockElementSlots; fem/tri.mjs:192-225 restrictMatrix) ---- */
+typedef struct amp_assembly_s amp_assembly;
+typedef enum {
+  AMP_ELEM_P1_TRI_SCALAR = 0,  /* P1 triangles, 2D, one coefficient per element (conductivity), fem/tri.mjs:45-80 */
+  AMP_ELEM_P1_TET_ELASTIC = 1  /* P1 tets, 3D, 3 DOFs per node, (E, nu) per element, physics/src/elastic/index.ts */
+} amp_element_kind;
+/* The element slots of a mesh in the system's CSR pattern (n rows, full symmetric storage), computed on the host and
+ * kept on the device with the mesh: coords (dim per node: 2 for triangles, 3 for tets), conn (nelem x nodes per
+ * element), dofs (nnodes x DOFs per node: the system row of node v's component c at dofs[v bs + c], or -1 for a DOF
+ * removed by the Dirichlet restriction, whose element rows and columns are dropped). AMP_PATTERN_MISMATCH when an
+ * element couples two rows the pattern does not connect. */
+AMP_API int amp_assembly_create(int kind, int32_t n, const int32_t *rowptr, const int32_t *colidx, int32_t nnodes,
+                                const double *coords, int64_t nelem, const int32_t *conn, const int32_t *dofs,
+                                int device, amp_assembly **out);
+/* values = the assembled system (the pattern's nnz CSR values) for per-element coefficients coef (kind 0: one per
+ * element; kind 1: E and nu per element), summed per CSR slot in element order as the reference's element loop adds
+ * them. coef host (coef_on_device 0) or device (1); values host (0) or device (1); stream: a cudaStream_t (null =
+ * default); the call waits for its work. */
+AMP_API int amp_assemble(amp_assembly *a, const double *coef, int coef_on_device, double *values,
+                         int values_on_device, void *stream);
+AMP_API void amp_assembly_destroy(amp_assembly *a);
+
 /* ---- shift-invert eigen operator (physics/src/common/eigen.ts:116-175 shiftInvertEigen; la/arnoldi.mjs) ---- */
 /* The factor holds A = K - sigma M (Cholesky or LDL^T). amp_factor_set_mass gives M's values on the same pattern
  * (nvalues CSR slots, host or device memory; copied to the device once). */
