@@ -151,8 +151,8 @@ struct amp_plan_s {
   DevMem mem;
   amp::DevPlan dp{};
   amp::AsmTask *dAsm = nullptr;
-  amp::PotrfTask *dPotrf = nullptr;
-  amp::PanelTask *dPanel = nullptr;
+  amp::GroupItem *dGroupItems = nullptr;
+  amp::StripTask *dStrips = nullptr;
   amp::TileTask *dTile = nullptr, *dUTile = nullptr;
   amp::MixTask *dMixTile = nullptr, *dMixU = nullptr;
   int4 *dFwdTasks = nullptr, *dBwdTasks = nullptr, *dBwdAll = nullptr;
@@ -198,6 +198,7 @@ struct amp_factor_s {
   __nv_bfloat16 *dWhi = nullptr, *dWlo = nullptr;   // mixed LDL^T: BF16 split of L21 D
   CUtensorMap *dMaps = nullptr;                     // per supernode: TMA descriptors of the split A and B operands
   unsigned long long *dStatus = nullptr;
+  int *dGroupFlags = nullptr;  // group panels: flags of every item, then the ticket counter of every group step
   long long waitSpins = 0;  // bound of the device waits in polls (0 = the kernels' defaults)
   bool ok = false, hasValues = false;
   // profiling: events around every launch while enabled
@@ -288,8 +289,8 @@ void upload_plan(amp_plan *pl) {
   d.diagSlot = m.upload(P.diagSlot);
   d.solveSmall = m.upload(P.solveSmall);
   pl->dAsm = m.upload(P.asmTasks);
-  pl->dPotrf = m.upload(P.potrfTasks);
-  pl->dPanel = m.upload(P.panelTasks);
+  pl->dGroupItems = m.upload(P.groupItems);
+  pl->dStrips = m.upload(P.strips);
   pl->dTile = m.upload(P.tileTasks);
   pl->dUTile = m.upload(P.uTasks);
   pl->dMixTile = m.upload(P.mixTiles);
@@ -324,7 +325,7 @@ enum KernelKind {
   K_ASSEMBLE, K_PANEL, K_UPDATE, K_FORWARD, K_BACKWARD, K_PERMUTE, K_RESIDUAL, K_POTRF, K_DIAGINV, K_KRYLOV,
   K_FRONTS, K_CHAIN, K_NKINDS
 };
-const char *kKindNames[K_NKINDS] = {"assemble",      "panel_trsm", "update_syrk", "solve_forward",
+const char *kKindNames[K_NKINDS] = {"assemble",      "group_panel", "update_syrk", "solve_forward",
                                     "solve_backward", "permute",    "residual_spmv", "potrf",
                                     "diag_inverse",  "krylov",     "small_fronts", "chain_mats"};
 
@@ -410,9 +411,13 @@ void enqueue_chain_mats(amp_factor *f, const T *Lx, const T *Inv, T *Mch, T *Gch
 
 void enqueue_factor(amp_factor *f) {
   const amp::Plan &P = f->plan->P;
-  const amp::DevPlan &dp = f->plan->dp;
+  amp::DevPlan dp = f->plan->dp;
+  if (f->waitSpins > 0) dp.spin = f->waitSpins;
   cudaStream_t st = f->stream;
   ck(cudaMemsetAsync(f->dStatus, 0xff, sizeof(unsigned long long), st), "memset status");
+  if (P.nGroupFlags + P.nGroupTickets > 0)
+    ck(cudaMemsetAsync(f->dGroupFlags, 0, sizeof(int) * (P.nGroupFlags + P.nGroupTickets), st), "memset flags");
+  int *tickets = f->dGroupFlags + P.nGroupFlags;
   if (f->precision == AMP_MIXED) {
     amp::LdltArgs<float> ld32{};
     if (f->kind == AMP_LDLT) {
@@ -430,21 +435,17 @@ void enqueue_factor(amp_factor *f) {
       LookAhead la{f};
       for (int k = P.lvlStepPtr[L]; k < P.lvlStepPtr[L + 1]; k++) {
         const amp::StepRange &sr = P.steps[k];
-        timed(f, K_POTRF, sr.potrfFlops, 0.0, [&] {
-          amp::launch_potrf<float>(f->plan->dPotrf + sr.potrf0, sr.potrf1 - sr.potrf0, dp, f->dL32, f->dStatus, ld32,
-                                   st);
+        timed(f, K_PANEL, sr.panelFlops, 0.0, [&] {
+          amp::launch_group_panel<float>(f->plan->dGroupItems, f->plan->dStrips + sr.strip0,
+                                         (int)(sr.strip1 - sr.strip0), tickets + sr.ticket, f->dGroupFlags, dp,
+                                         f->dL32, f->dStatus, f->dShi, f->dSlo, ld32, st);
         });
-        if (sr.panel1 > sr.panel0)
-          timed(f, K_PANEL, sr.panelFlops, 0.0, [&] {
-            amp::launch_trsm<float>(f->plan->dPanel + sr.panel0, sr.panel1 - sr.panel0, dp, f->dL32, f->dStatus,
-                                    f->dShi, f->dSlo, ld32, st);
-          });
         la.trsm_done();
         la.before_part_a();
         if (sr.mixMid > sr.mix0)
           timed(f, K_UPDATE, sr.updateFlopsA, 0.0, [&] {
             amp::launch_update_mx(f->plan->dMixTile + sr.mix0, sr.mixMid - sr.mix0, f->dMaps, f->dL32, f->dU32,
-                                  f->dStatus, amp::num_sms(), st, true, f->waitSpins);
+                                  f->dStatus, amp::num_sms(), st, false, f->waitSpins);
           });
         if (sr.mix1 > sr.mixMid)
           la.part_b(K_UPDATE, sr.updateFlopsB, [&] {
@@ -485,14 +486,11 @@ void enqueue_factor(amp_factor *f) {
     LookAhead la{f};
     for (int k = P.lvlStepPtr[L]; k < P.lvlStepPtr[L + 1]; k++) {
       const amp::StepRange &sr = P.steps[k];
-      timed(f, K_POTRF, sr.potrfFlops, 0.0, [&] {
-        amp::launch_potrf<double>(f->plan->dPotrf + sr.potrf0, sr.potrf1 - sr.potrf0, dp, f->dLx, f->dStatus, ld, st);
+      timed(f, K_PANEL, sr.panelFlops, 0.0, [&] {
+        amp::launch_group_panel<double>(f->plan->dGroupItems, f->plan->dStrips + sr.strip0,
+                                        (int)(sr.strip1 - sr.strip0), tickets + sr.ticket, f->dGroupFlags, dp, f->dLx,
+                                        f->dStatus, nullptr, nullptr, ld, st);
       });
-      if (sr.panel1 > sr.panel0)
-        timed(f, K_PANEL, sr.panelFlops, 0.0, [&] {
-          amp::launch_trsm<double>(f->plan->dPanel + sr.panel0, sr.panel1 - sr.panel0, dp, f->dLx, f->dStatus, nullptr,
-                                   nullptr, ld, st);
-        });
       la.trsm_done();
       la.before_part_a();
       if (sr.tileMid > sr.tile0)
@@ -915,7 +913,7 @@ int amp_plan_get_info(const amp_plan *pl, amp_plan_info *info) {
   info->symbolic_ms = S.symbolic_ms;
   info->device_bytes = 8 * (pl->P.nnzLStored + pl->P.arenaDoubles + pl->P.patNnz + S.n) + 4 * (int64_t)(
       pl->P.asmDst.size() * 2 + pl->P.eaMap.size() + pl->P.Si.size() + pl->rowptr.size() + pl->colidx.size()) +
-      (int64_t)(sizeof(amp::TileTask) * pl->P.tileTasks.size() + sizeof(amp::PanelTask) * pl->P.panelTasks.size());
+      (int64_t)(sizeof(amp::TileTask) * pl->P.tileTasks.size() + sizeof(amp::StripTask) * pl->P.strips.size());
   return AMP_OK;
 }
 
@@ -1043,6 +1041,7 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
         ck(cudaMemset(f->dHand, 0, sizeof(unsigned long long) * hw), "memset hand-off");
       }
       f->dTickets = f->mem.alloc<int>(2);
+      f->dGroupFlags = f->mem.alloc<int>((size_t)std::max(1, P.nGroupFlags + P.nGroupTickets));
       f->dDone = f->mem.alloc<int>((size_t)std::max(1, P.nsuper));
       f->dSolveStatus = f->mem.alloc<unsigned long long>(1);
       init_device_once(pl->device);

@@ -5,12 +5,14 @@
 //   k_assemble  zero the front, scatter A's entries (sparse.mjs:965-973) and extend-add the children's update
 //               matrices in the reference's child order (sparse.mjs:974-985). One CTA owns a block of 32 front
 //               columns, so every entry has a single writer and the summation order is the reference's.
-//   per pivot block of 64 columns:
-//     k_potrf   POTRF (or LDL^T) of the 64 x 64 pivot block in registers, one CTA per block.
-//     k_trsm    the rows below the pivot block against it, four threads per row, 64 rows per CTA.
-//     k_update  FP64 trailing update F -= A B^T (A = L21, or L21 D for LDL^T; B = L21) on 128 x 64 tiles with the
-//               FP64 tensor-core MMA (mma.sync m16n8k16), covering the remaining pivot columns (in Lx) and the update
-//               block (in the U arena). The mixed-precision update is k_update_mx (update_bf16x3.cu).
+//   per group of up to kGroup pivot blocks of 64 columns:
+//     k_group_panel  one dataflow launch: POTRF (or LDL^T) of each 64 x 64 pivot block in registers, the rows below
+//                    it against it (TRSM, 64-row strips, one CTA each) and the update of the group's remaining
+//                    columns, ordered by flags between the strips of the launch.
+//     k_update       FP64 update F -= A B^T of the columns right of the group (A = L21, or L21 D for LDL^T; B = L21;
+//                    K = the group) on 128 x 64 tiles with the FP64 tensor-core MMA (mma.sync m16n8k16), covering
+//                    the remaining pivot columns (in Lx) and the update block (in the U arena). The mixed-precision
+//                    update is k_update_mx (update_bf16x3.cu).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -18,6 +20,7 @@
 #include <cstdint>
 
 #include "devplan.cuh"
+#include "sync.cuh"
 #include "../host/plan.hpp"
 
 namespace amp {
@@ -181,33 +184,29 @@ __global__ void __launch_bounds__(256) k_assemble(const AsmTask *__restrict__ ta
   }
 }
 
-// ---------------------------------------------------------------------------------------------------------------
-// Panel: POTRF of the pivot block + TRSM of a chunk of rows below it
-// ---------------------------------------------------------------------------------------------------------------
-__device__ __forceinline__ double recip_t(double d) { return recip_nr(d); }
-__device__ __forceinline__ float recip_t(float d) { return __frcp_rn(d); }
 // Scale factors of the pivot block's right-looking update (not stored): FP64 as recip_nr, FP32 the hardware estimate.
 __device__ __forceinline__ double fast_recip(double d) { return recip_nr(d); }
 __device__ __forceinline__ float fast_recip(float d) { return __fdividef(1.0f, d); }
 
-// Pivot block: POTRF (or LDL^T) of the 64 x 64 diagonal block of a front, one CTA per pivot block, the block in
-// registers. T = double: the FP64 factor; T = float: the mixed-precision factor.
-// Thread t < 136 owns the 4 x 4 tile (ti, tj), ti >= tj, of the lower triangle. Right-looking on the unscaled
-// columns: at step k the owners of column k publish it (double-buffered in shared memory) and the owner of the
-// diagonal entry settles the pivot and publishes 1 / d_k; after one barrier every thread subtracts col_i col_j / d_k
-// from its entries with i, j > k. Cholesky tests d > 0 (sparse.mjs:1151-1156); LDL^T (ld.scal != null,
-// ldlt.mjs:450-562) perturbs |d| < tau to +-tau and counts negative and perturbed pivots. At the end the columns are scaled:
-// Cholesky L = a / sqrt(d) with sqrt(d) on the diagonal, LDL^T L = a / d with a unit diagonal (D to ld.D). The
-// factored block is written back in place for the TRSM of the rows below and the updates.
+// ---------------------------------------------------------------------------------------------------------------
+// Group panel: the pivot blocks of a group of up to kGroup 64-column blocks of a front, factored in one dataflow
+// launch (POTRF of each pivot block, TRSM of the rows below it, and the update of the group's remaining columns).
+// ---------------------------------------------------------------------------------------------------------------
+
+// Pivot block: POTRF (or LDL^T) of the 64 x 64 diagonal block of a front, called by all 256 threads of a CTA, the
+// block in registers. T = double: the FP64 factor; T = float: the mixed-precision factor. Lp: the block's (0, 0)
+// entry (ld m), w <= 64 its columns. Thread t < 136 owns the 4 x 4 tile (ti, tj), ti >= tj, of the lower triangle.
+// Right-looking on the unscaled columns, four columns per step kb with two barriers: (1) the diagonal tile eliminates
+// its four columns (settling the pivots) and publishes them; (2) the tiles below it in column block kb eliminate the
+// same four columns against it and publish theirs; then every tile right of the block applies the rank-4 update
+// S(i, j) -= sum S(i, k) S(j, k) / d_k. Cholesky tests d > 0 (sparse.mjs:1151-1156); LDL^T (ld.scal != null,
+// ldlt.mjs:450-562) perturbs |d| < tau to +-tau and counts negative and perturbed pivots. At the end the columns are
+// scaled: Cholesky L = a / sqrt(d) with sqrt(d) on the diagonal, LDL^T L = a / d with a unit diagonal (D to ld.D).
+// Returns false (status set for the first failing column f + c0 + k) when a pivot failed; the block is then not
+// written back.
 template <class T>
-__global__ void __launch_bounds__(256) k_potrf(const PotrfTask *__restrict__ tasks, DevPlan P, T *__restrict__ Lx,
-                                               unsigned long long *status, LdltArgs<T> ld) {
-  if (failed(status)) return;
-  const PotrfTask t = tasks[blockIdx.x];
-  const int s = t.s, c0 = t.c0;
-  const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
-  const int w = min(kPanel, nc - c0);
-  T *Lp = Lx + P.snLxp[s] + (int64_t)c0 * m + c0;  // block (i, j) at Lp[j m + i]
+__device__ bool potrf_block(T *Lp, int m, int w, int f, int c0, int s, unsigned long long *status,
+                            const LdltArgs<T> &ld) {
   __shared__ T col[2][4][kPanel];  // per 4-column block (double-buffered): the block's unscaled columns, by row
   __shared__ T pd[kPanel], piv[2][4];
   __shared__ unsigned char pflag[kPanel];
@@ -230,9 +229,6 @@ __global__ void __launch_bounds__(256) k_potrf(const PotrfTask *__restrict__ tas
       a[r][c] = !owner || i < j ? T(0) : (i < w ? Lp[(int64_t)j * m + i] : (i == j ? T(1) : T(0)));
     }
   if (tid == 0) fail = kPanel;  // none
-  // Four columns per step kb, two barriers: (1) the diagonal tile eliminates its four columns (settling the pivots)
-  // and publishes them; (2) the tiles below it in column block kb eliminate the same four columns against it and
-  // publish theirs; then every tile right of the block applies the rank-4 update S(i, j) -= sum S(i, k) S(j, k) / d_k.
   for (int kb = 0; kb < kPanel / 4; kb++) {
     const int buf = kb & 1;
     if (owner && ti == kb && tj == kb) {
@@ -296,7 +292,7 @@ __global__ void __launch_bounds__(256) k_potrf(const PotrfTask *__restrict__ tas
   __syncthreads();
   if (fail < kPanel) {
     if (tid == 0) atomicMin(status, status_word(f + c0 + fail, ldlt ? 2 : 1, s));
-    return;
+    return false;
   }
   if (owner) {
 #pragma unroll
@@ -321,34 +317,27 @@ __global__ void __launch_bounds__(256) k_potrf(const PotrfTask *__restrict__ tas
       atomicAdd(ld.counts + 1, pert);
     }
   }
+  return true;
 }
 
-// TRSM of up to 64 rows of a front against its factored pivot block: x_k = (a_k - sum_{c<k} x_c M(k, c)) / M(k, k).
-// Four threads per row, thread (row, q) holds columns 16 q .. 16 q + 15 in registers. Phase p: the threads of quarter
-// p solve their 16 columns (the earlier quarters' contributions already applied) and publish them; after a barrier
-// the threads of the later quarters subtract quarter p's contribution (16 x 16 products) from theirs.
-// Cholesky: M = L11, x = L21. LDL^T: M(k, c) = L11(k, c) d_c, M(k, k) = d_k, x = L21, and w = x D = L21 D (the
-// update's A operand). The rows are also written as BF16 hi / lo pairs (hi = bf16(x), lo = bf16(x - hi)) into the
-// split columns of the tensor-core update (mixed precision).
-constexpr int kTrsmSmem = (kPanel * (kPanel + 1) + kPanel * (kPanel + 1)) * (int)sizeof(double);
+// TRSM of up to 64 rows [r0, r1) of a front (L: its column-major block, ld m) against its factored pivot block
+// [c0, c0 + w): x_k = (a_k - sum_{c<k} x_c M(k, c)) / M(k, k). Four threads per row, thread (row, q) holds columns
+// 16 q .. 16 q + 15 in registers. Phase p: the threads of quarter p solve their 16 columns (the earlier quarters'
+// contributions already applied) and publish them; after a barrier the threads of the later quarters subtract
+// quarter p's contribution (16 x 16 products) from theirs. Cholesky: M = L11, x = L21. LDL^T: M(k, c) = L11(k, c) d_c,
+// M(k, k) = d_k, x = L21, and w = x D = L21 D (the update's A operand, written to ld.W for the FP64 factor). The rows
+// are also written as BF16 hi / lo pairs (hi = bf16(x), lo = bf16(x - hi)) into the split columns of the tensor-core
+// update (mixed precision). The pivot block and D come from another CTA of the launch: read through L2 (__ldcg).
+// On return Ws[c][r] holds this strip's update operand (x, or x D for LDL^T), c < w, r < r1 - r0.
 template <class T>
-__global__ void __launch_bounds__(256) k_trsm(const PanelTask *__restrict__ tasks, DevPlan P, T *__restrict__ Lx,
-                                              const unsigned long long *status, __nv_bfloat16 *__restrict__ Shi,
-                                              __nv_bfloat16 *__restrict__ Slo, LdltArgs<T> ld) {
-  if (failed(status)) return;
-  const PanelTask t = tasks[blockIdx.x];
-  const int s = t.s, c0 = t.c0;
-  const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
-  const int w = min(kPanel, nc - c0);
+__device__ void trsm_strip(T *L, int m, int f, int c0, int w, int r0, int r1, int64_t lxp, int64_t sp,
+                           __nv_bfloat16 *Shi, __nv_bfloat16 *Slo, const LdltArgs<T> &ld, T (*M)[kPanel + 1],
+                           T (*Ws)[kPanel + 1], T *invd, T *dv) {
   const bool ldlt = ld.scal != nullptr;
-  T *Lp = Lx + P.snLxp[s];
-  extern __shared__ __align__(16) unsigned char trsm_raw[];
-  T(*M)[kPanel + 1] = reinterpret_cast<T(*)[kPanel + 1]>(trsm_raw);  // M[k][c], c < k
-  T(*xs)[kPanel + 1] = reinterpret_cast<T(*)[kPanel + 1]>(trsm_raw + kPanel * (kPanel + 1) * sizeof(T));  // [c][row]
-  __shared__ T invd[kPanel], dv[kPanel];
   const int tid = threadIdx.x, r = tid & (kPanel - 1), q = tid >> 6;
   if (tid < kPanel) {
-    const T d = tid < w ? (ldlt ? (T)ld.D[f + c0 + tid] : Lp[(int64_t)(c0 + tid) * m + c0 + tid]) : T(1);
+    const T d = tid < w ? (ldlt ? (T)__ldcg(ld.D + f + c0 + tid) : __ldcg(L + (int64_t)(c0 + tid) * m + c0 + tid))
+                        : T(1);
     dv[tid] = d;
     invd[tid] = T(1) / d;
   }
@@ -358,18 +347,18 @@ __global__ void __launch_bounds__(256) k_trsm(const PanelTask *__restrict__ task
 #pragma unroll
     for (int u = 0; u < 16; u++) {
       const int c = 16 * q + u;
-      v[u] = (r < w && c < r) ? Lp[(int64_t)(c0 + c) * m + c0 + r] : T(0);
+      v[u] = (r < w && c < r) ? __ldcg(L + (int64_t)(c0 + c) * m + c0 + r) : T(0);
     }
 #pragma unroll
     for (int u = 0; u < 16; u++) M[r][16 * q + u] = ldlt ? v[u] * dv[16 * q + u] : v[u];
   }
-  const int row = t.r0 + r;
-  const bool active = row < t.r1;
+  const int row = r0 + r;
+  const bool active = row < r1;
   T x[16];
 #pragma unroll
   for (int u = 0; u < 16; u++) {
     const int c = 16 * q + u;
-    x[u] = active && c < w ? Lp[(int64_t)(c0 + c) * m + row] : T(0);
+    x[u] = active && c < w ? L[(int64_t)(c0 + c) * m + row] : T(0);
   }
   __syncthreads();
   for (int p = 0; p < 4; p++) {
@@ -382,31 +371,32 @@ __global__ void __launch_bounds__(256) k_trsm(const PanelTask *__restrict__ task
         for (int u2 = u + 1; u2 < 16; u2++) x[u2] -= x[u] * M[16 * p + u2][c];
       }
 #pragma unroll
-      for (int u = 0; u < 16; u++) xs[16 * p + u][r] = x[u];
+      for (int u = 0; u < 16; u++) Ws[16 * p + u][r] = x[u];
     }
     __syncthreads();
     if (q > p) {  // subtract quarter p's contribution
 #pragma unroll 4
       for (int kk = 0; kk < 16; kk++) {
         const int k = 16 * p + kk;
-        const T xk = xs[k][r];
+        const T xk = Ws[k][r];
 #pragma unroll
         for (int u = 0; u < 16; u++) x[u] -= xk * M[16 * q + u][k];
       }
     }
   }
-  if (!active) return;
+  __syncthreads();  // every quarter read Ws: overwrite it with the update operand
   const int ld8 = (m + 7) & ~7;
 #pragma unroll
   for (int u = 0; u < 16; u++) {
     const int cc = 16 * q + u;
-    if (cc >= w) break;
     const T xv = x[u];
-    Lp[(int64_t)(c0 + cc) * m + row] = xv;
-    const T wv = ldlt ? xv * dv[cc] : T(0);
-    if (ldlt && ld.W) ld.W[P.snLxp[s] + (int64_t)(c0 + cc) * m + row] = wv;
+    const T wv = ldlt ? xv * dv[cc] : xv;
+    Ws[cc][r] = active && cc < w ? wv : T(0);
+    if (!active || cc >= w) continue;
+    L[(int64_t)(c0 + cc) * m + row] = xv;
+    if (ldlt && ld.W) ld.W[lxp + (int64_t)(c0 + cc) * m + row] = wv;
     if (Shi) {
-      const int64_t g = P.snSp[s] + (int64_t)(c0 + cc) * ld8 + row;
+      const int64_t g = sp + (int64_t)(c0 + cc) * ld8 + row;
       const __nv_bfloat16 hi = __float2bfloat16_rn((float)xv);
       Shi[g] = hi;
       Slo[g] = __float2bfloat16_rn((float)xv - __bfloat162float(hi));
@@ -416,6 +406,130 @@ __global__ void __launch_bounds__(256) k_trsm(const PanelTask *__restrict__ task
         ld.Wlo[g] = __float2bfloat16_rn((float)wv - __bfloat162float(whi));
       }
     }
+  }
+  __syncthreads();
+}
+
+// Wait (thread 0, bounded) until *p >= need; false when the factorization has failed (a pivot, or a wait that ran
+// out: status set). Thread 0 decides and the CTA follows it after the barrier, so every thread returns the same.
+__device__ __forceinline__ bool panel_wait(const int *p, int need, unsigned long long *status, long long limit) {
+  __shared__ int ok;
+  if (threadIdx.x == 0) {
+    long long spins = 0;
+    int v = 1;
+    while (ld_acquire(p) < need) {
+      if (failed(status)) {
+        v = 0;
+        break;
+      }
+      if (++spins > limit) {
+        atomicMin(status, status_word(0x7fffffff, 3, 0));
+        v = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    if (failed(status)) v = 0;  // a failed pivot also releases its flag
+    ok = v;
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// Publish *p = v after this CTA's global writes (all threads pass the barrier first).
+__device__ __forceinline__ void panel_release(int *p, int v) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    st_release(p, v);
+  }
+}
+
+// One group of pivot blocks [g0, g1) of a front, a strip of up to 64 rows per CTA, CTAs ordered by an atomic ticket
+// (the diagonal strips of every item first, then the strips below the group). Per pivot block b of the group:
+//   the diagonal strip of block b (rows [c0, c0 + w)) factors it once its own updates are done and publishes P[b];
+//   every strip with rows below block b waits for P[b], solves its rows against the block (TRSM) and, when it is a
+//   diagonal strip, publishes D[j] = b + 1; then it updates its rows of the group's remaining columns [c0 + w, g1)
+//   with block b (C -= W_r X_c^T, K = w; X_c: the rows of those columns, from the diagonal strips' TRSM, waited for
+//   by D[j] >= b + 1; a diagonal strip updates only the lower part, columns up to its own rows).
+// Every wait is on a strip with a smaller ticket, which runs to completion without waiting on a larger one, so the
+// launch cannot deadlock whatever the number of resident CTAs. The columns right of the group receive the group's
+// update afterwards (k_update / k_update_mx, K = the group). Failure (a pivot, a bounded wait) sets the status and
+// releases P[b], so every waiter leaves.
+constexpr int kGroupSmem = 2 * kPanel * (kPanel + 1) * (int)sizeof(double);
+template <class T>
+__global__ void __launch_bounds__(256) k_group_panel(const GroupItem *__restrict__ items,
+                                                     const StripTask *__restrict__ strips, int nstrips, int *ticket,
+                                                     int *flags, DevPlan P, T *__restrict__ Lx,
+                                                     unsigned long long *status, __nv_bfloat16 *__restrict__ Shi,
+                                                     __nv_bfloat16 *__restrict__ Slo, LdltArgs<T> ld) {
+  extern __shared__ __align__(16) unsigned char gp_raw[];
+  T(*M)[kPanel + 1] = reinterpret_cast<T(*)[kPanel + 1]>(gp_raw);  // pivot block (TRSM), then the X_c chunk
+  T(*Ws)[kPanel + 1] = reinterpret_cast<T(*)[kPanel + 1]>(gp_raw + kPanel * (kPanel + 1) * sizeof(T));
+  __shared__ T invd[kPanel], dv[kPanel];
+  __shared__ int sTicket;
+  if (threadIdx.x == 0) sTicket = failed(status) ? nstrips : atomicAdd(ticket, 1);
+  __syncthreads();
+  const int t = sTicket;
+  if (t >= nstrips) return;
+  const StripTask st = strips[t];
+  const GroupItem it = items[st.item];
+  const int s = it.s, g0 = it.g0, g1 = it.g1;
+  const int f = P.snF[s], m = P.snM[s];
+  const int nb = (g1 - g0 + kPanel - 1) / kPanel;
+  const int r0 = st.r0, r1 = st.r1, jd = st.diag;
+  const int bmax = jd >= 0 ? jd : nb;  // pivot blocks whose rows below include this strip
+  T *L = Lx + P.snLxp[s];
+  int *Pf = flags + it.flag0, *Df = Pf + nb;
+  const int tid = threadIdx.x, tr = tid & 15, tc = tid >> 4;
+  for (int b = 0; b < bmax; b++) {
+    const int c0 = g0 + b * kPanel, w = min(kPanel, g1 - c0), c1 = c0 + w;
+    if (!panel_wait(Pf + b, 1, status, P.spin)) return;
+    trsm_strip<T>(L, m, f, c0, w, r0, r1, P.snLxp[s], P.snSp[s], Shi, Slo, ld, M, Ws, invd, dv);
+    if (jd >= 0) panel_release(Df + jd, b + 1);
+    // the group's remaining columns [c1, hi): a diagonal strip only its lower part (columns < r1)
+    const int hi = jd >= 0 ? min(g1, r1) : g1;
+    for (int cb = c1; cb < hi; cb += kPanel) {
+      const int j = (cb - g0) / kPanel, ncol = min(kPanel, hi - cb);
+      if (j != jd && !panel_wait(Df + j, b + 1, status, P.spin)) return;
+      for (int e = tid; e < kPanel * kPanel; e += blockDim.x) {  // X_c[k][jj] = L(cb + jj, c0 + k)
+        const int k = e >> 6, jj = e & 63;
+        M[k][jj] = (k < w && jj < ncol) ? __ldcg(L + (int64_t)(c0 + k) * m + cb + jj) : T(0);
+      }
+      __syncthreads();
+      T acc[4][4];
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int bb = 0; bb < 4; bb++) acc[a][bb] = T(0);
+      for (int k = 0; k < w; k++) {
+        T wv[4], xv[4];
+#pragma unroll
+        for (int a = 0; a < 4; a++) wv[a] = Ws[k][tr + 16 * a];
+#pragma unroll
+        for (int bb = 0; bb < 4; bb++) xv[bb] = M[k][tc + 16 * bb];
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+          for (int bb = 0; bb < 4; bb++) acc[a][bb] += wv[a] * xv[bb];
+      }
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int bb = 0; bb < 4; bb++) {
+          const int row = r0 + tr + 16 * a, colj = cb + tc + 16 * bb;
+          if (row < r1 && colj < cb + ncol && (jd < 0 || row >= colj)) {
+            T *cptr = L + (int64_t)colj * m + row;
+            *cptr = *cptr - acc[a][bb];
+          }
+        }
+      __syncthreads();  // M is reloaded by the next chunk
+    }
+  }
+  if (jd >= 0) {  // this strip's own pivot block, fully updated: factor it and publish it (also after a failure)
+    const int c0 = g0 + jd * kPanel, w = min(kPanel, g1 - c0);
+    potrf_block<T>(L + (int64_t)c0 * m + c0, m, w, f, c0, s, status, ld);
+    panel_release(Pf + jd, 1);
   }
 }
 
@@ -617,8 +731,9 @@ cudaError_t init_solve_multi_attributes();
 cudaError_t init_front_small_attributes();
 cudaError_t init_kernel_attributes() {
   // function attributes belong to the current device's context: the caller runs this once per device
-  cudaError_t e = cudaFuncSetAttribute(k_trsm<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsmSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_trsm<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsmSmem);
+  cudaError_t e = cudaFuncSetAttribute(k_group_panel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGroupSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_group_panel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGroupSmem / 2);
   if (e == cudaSuccess) e = init_mixed_attributes();
   if (e == cudaSuccess) e = init_solve_attributes();
   if (e == cudaSuccess) e = init_solve_multi_attributes();
@@ -640,23 +755,19 @@ template void launch_assemble<double>(const AsmTask *, int64_t, const DevPlan &,
 template void launch_assemble<float>(const AsmTask *, int64_t, const DevPlan &, const double *, float *, float *,
                                      const unsigned long long *, cudaStream_t);
 template <class T>
-void launch_potrf(const PotrfTask *tasks, int64_t ntasks, const DevPlan &P, T *Lx, unsigned long long *status,
-                  const LdltArgs<T> &ld, cudaStream_t st) {
-  if (ntasks > 0) k_potrf<T><<<(unsigned)ntasks, 256, 0, st>>>(tasks, P, Lx, status, ld);
+void launch_group_panel(const GroupItem *items, const StripTask *strips, int nstrips, int *ticket, int *flags,
+                        const DevPlan &P, T *Lx, unsigned long long *status, __nv_bfloat16 *Shi, __nv_bfloat16 *Slo,
+                        const LdltArgs<T> &ld, cudaStream_t st) {
+  if (nstrips > 0)
+    k_group_panel<T><<<(unsigned)nstrips, 256, 2 * kPanel * (kPanel + 1) * sizeof(T), st>>>(
+        items, strips, nstrips, ticket, flags, P, Lx, status, Shi, Slo, ld);
 }
-template <class T>
-void launch_trsm(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, T *Lx, const unsigned long long *status,
-                 __nv_bfloat16 *Shi, __nv_bfloat16 *Slo, const LdltArgs<T> &ld, cudaStream_t st) {
-  if (ntasks > 0) k_trsm<T><<<(unsigned)ntasks, 256, kTrsmSmem, st>>>(tasks, P, Lx, status, Shi, Slo, ld);
-}
-template void launch_potrf<double>(const PotrfTask *, int64_t, const DevPlan &, double *, unsigned long long *,
-                                   const LdltArgs<double> &, cudaStream_t);
-template void launch_potrf<float>(const PotrfTask *, int64_t, const DevPlan &, float *, unsigned long long *,
-                                  const LdltArgs<float> &, cudaStream_t);
-template void launch_trsm<double>(const PanelTask *, int64_t, const DevPlan &, double *, const unsigned long long *,
-                                  __nv_bfloat16 *, __nv_bfloat16 *, const LdltArgs<double> &, cudaStream_t);
-template void launch_trsm<float>(const PanelTask *, int64_t, const DevPlan &, float *, const unsigned long long *,
-                                 __nv_bfloat16 *, __nv_bfloat16 *, const LdltArgs<float> &, cudaStream_t);
+template void launch_group_panel<double>(const GroupItem *, const StripTask *, int, int *, int *, const DevPlan &,
+                                         double *, unsigned long long *, __nv_bfloat16 *, __nv_bfloat16 *,
+                                         const LdltArgs<double> &, cudaStream_t);
+template void launch_group_panel<float>(const GroupItem *, const StripTask *, int, int *, int *, const DevPlan &,
+                                        float *, unsigned long long *, __nv_bfloat16 *, __nv_bfloat16 *,
+                                        const LdltArgs<float> &, cudaStream_t);
 void launch_ldlt_tau(const double *values, const DevPlan &P, double *scal, cudaStream_t st) {
   k_ldlt_tau<<<1, 1024, 0, st>>>(values, P.diagSlot, P.n, scal);
 }

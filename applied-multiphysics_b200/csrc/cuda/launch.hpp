@@ -16,12 +16,11 @@ cudaError_t init_kernel_attributes();  // once per device (with that device curr
 template <class T>
 void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, const double *values, T *Lx, T *U,
                      const unsigned long long *status, cudaStream_t st);
+// one group of pivot blocks per item: nstrips strip tasks, ticket and flags zeroed before the factorization
 template <class T>
-void launch_potrf(const PotrfTask *tasks, int64_t ntasks, const DevPlan &P, T *Lx, unsigned long long *status,
-                  const LdltArgs<T> &ld, cudaStream_t st);
-template <class T>
-void launch_trsm(const PanelTask *tasks, int64_t ntasks, const DevPlan &P, T *Lx, const unsigned long long *status,
-                 __nv_bfloat16 *Shi, __nv_bfloat16 *Slo, const LdltArgs<T> &ld, cudaStream_t st);
+void launch_group_panel(const GroupItem *items, const StripTask *strips, int nstrips, int *ticket, int *flags,
+                        const DevPlan &P, T *Lx, unsigned long long *status, __nv_bfloat16 *Shi, __nv_bfloat16 *Slo,
+                        const LdltArgs<T> &ld, cudaStream_t st);
 void launch_ldlt_tau(const double *values, const DevPlan &P, double *scal, cudaStream_t st);
 // whole small fronts of one level: tiny (m <= 32, warp per front; sorted by m, the first ntinyMid with m <= 16) and
 // small (m <= 128, CTA per front; maxM = their largest m); returns the kernels launched

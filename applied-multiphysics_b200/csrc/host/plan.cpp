@@ -234,7 +234,7 @@ void build_plan(const Symbolic &S, Plan &P) {
       int s = P.lvlSn[q];
       if (isSmall(s)) continue;
       for (int j0 = 0; j0 < P.snM[s]; j0 += kAsmCols) P.asmTasks.push_back({s, j0});
-      maxSteps = std::max(maxSteps, (P.snNc[s] + kPanel - 1) / kPanel);
+      maxSteps = std::max(maxSteps, (P.snNc[s] + kGroup * kPanel - 1) / (kGroup * kPanel));
       // bytes: value + lowerI + lowerSrc per A entry (16); read U + read/write the parent entry per child entry (24)
       double b = 16.0 * (S.lowerP[P.snF[s] + P.snNc[s]] - S.lowerP[P.snF[s]]);
       for (int k = P.chPtr[s]; k < P.chPtr[s + 1]; k++) {
@@ -246,36 +246,45 @@ void build_plan(const Symbolic &S, Plan &P) {
     P.asmLvlPtr[L + 1] = (int64_t)P.asmTasks.size();
     for (int k = 0; k < maxSteps; k++) {
       StepRange sr;
-      sr.potrfFlops = sr.panelFlops = sr.updateFlopsA = sr.updateFlopsB = 0;
-      sr.potrf0 = (int64_t)P.potrfTasks.size();
-      sr.panel0 = (int64_t)P.panelTasks.size();
-      // Pivot blocks are grouped by kGroup: after block b of group [g0, g1) only the group's remaining columns are
-      // updated (narrow, K = 64); after the group's last block the pivot columns right of the group receive the whole
-      // group at once (wide, K = g1 - g0). The update block waits for the long-K pass after the level. Each step's
-      // update region [lo, hi) is split into its first 64 columns (the next pivot block: part A, which the next step's
-      // POTRF waits for) and the rest (part B, which may run while the next pivot block is factored).
+      sr.panelFlops = sr.updateFlopsA = sr.updateFlopsB = 0;
+      sr.item0 = (int64_t)P.groupItems.size();
+      sr.strip0 = (int64_t)P.strips.size();
+      sr.ticket = P.nGroupTickets++;
+      // Group k of every front of the level (pivot columns [g0, g1), up to kGroup pivot blocks) in one group-panel
+      // launch; then the columns right of the group receive its update (K = g1 - g0): part A the next group's
+      // columns, part B the rest.
       struct Region {
         int s, lo, hi, kc0, kw;
       };
       std::vector<Region> regions;
-      for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
-        int s = P.lvlSn[q];
-        const int nc = P.snNc[s], m = P.snM[s], c0 = k * kPanel;
-        if (c0 >= nc || isSmall(s)) continue;
-        const int c1 = std::min(c0 + kPanel, nc);
-        P.potrfTasks.push_back({s, c0});
-        for (int r0 = c1; r0 < m; r0 += kTrsmRows) P.panelTasks.push_back({s, c0, r0, std::min(r0 + kTrsmRows, m)});
-        const int g0 = (c0 / (kGroup * kPanel)) * (kGroup * kPanel), g1 = std::min(nc, g0 + kGroup * kPanel);
-        const double w = c1 - c0, r = m - c1;
-        sr.potrfFlops += w * w * w / 3.0;
-        sr.panelFlops += r * w * w;  // TRSM
-        if (c1 < g1)
-          regions.push_back({s, c1, g1, c0, c1 - c0});
-        else if (g1 < nc)
-          regions.push_back({s, g1, nc, g0, g1 - g0});
-      }
       // lower entries of columns [a, b) of an m-row front
       auto trap = [](double m, double a, double b) { return (b - a) * m - (a + b - 1) * (b - a) / 2; };
+      for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
+        int s = P.lvlSn[q];
+        const int nc = P.snNc[s], m = P.snM[s], g0 = k * kGroup * kPanel;
+        if (g0 >= nc || isSmall(s)) continue;
+        const int g1 = std::min(g0 + kGroup * kPanel, nc), nb = (g1 - g0 + kPanel - 1) / kPanel;
+        P.groupItems.push_back({s, g0, g1, P.nGroupFlags});
+        P.nGroupFlags += 2 * nb;
+        for (int c0 = g0; c0 < g1; c0 += kPanel) {
+          const double w = std::min(kPanel, g1 - c0), c1 = c0 + w;
+          sr.panelFlops += w * w * w / 3.0 + (m - c1) * w * w + 2.0 * w * trap(m, c1, g1);
+        }
+        if (g1 < nc) regions.push_back({s, g1, nc, g0, g1 - g0});
+      }
+      const int64_t i0 = sr.item0, i1 = (int64_t)P.groupItems.size();
+      for (int64_t it = i0; it < i1; it++) {  // the diagonal strips of every item first (they take the first tickets)
+        const GroupItem &gi = P.groupItems[it];
+        for (int c0 = gi.g0, j = 0; c0 < gi.g1; c0 += kPanel, j++)
+          P.strips.push_back({(int)it, c0, std::min(c0 + kPanel, gi.g1), j});
+      }
+      for (int64_t it = i0; it < i1; it++) {  // then the strips below the groups
+        const GroupItem &gi = P.groupItems[it];
+        const int m = P.snM[gi.s];
+        for (int r0 = gi.g1; r0 < m; r0 += kPanel) P.strips.push_back({(int)it, r0, std::min(r0 + kPanel, m), -1});
+      }
+      sr.item1 = i1;
+      sr.strip1 = (int64_t)P.strips.size();
       auto emit = [&](const Region &g, int lo, int hi, double &flops) {
         if (lo >= hi) return;
         const int m = P.snM[g.s], nc = P.snNc[g.s];
@@ -287,12 +296,10 @@ void build_plan(const Symbolic &S, Plan &P) {
       };
       sr.tile0 = (int64_t)P.tileTasks.size();
       sr.mix0 = (int64_t)P.mixTiles.size();
-      for (const Region &g : regions) emit(g, g.lo, std::min(g.lo + kPanel, g.hi), sr.updateFlopsA);
+      for (const Region &g : regions) emit(g, g.lo, std::min(g.lo + kGroup * kPanel, g.hi), sr.updateFlopsA);
       sr.tileMid = (int64_t)P.tileTasks.size();
       sr.mixMid = (int64_t)P.mixTiles.size();
-      for (const Region &g : regions) emit(g, g.lo + kPanel, g.hi, sr.updateFlopsB);
-      sr.potrf1 = (int64_t)P.potrfTasks.size();
-      sr.panel1 = (int64_t)P.panelTasks.size();
+      for (const Region &g : regions) emit(g, g.lo + kGroup * kPanel, g.hi, sr.updateFlopsB);
       sr.tile1 = (int64_t)P.tileTasks.size();
       sr.mix1 = (int64_t)P.mixTiles.size();
       P.steps.push_back(sr);

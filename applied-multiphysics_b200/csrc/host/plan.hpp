@@ -29,11 +29,13 @@ constexpr int kSmallFront = 128;  // fronts with 32 < m <= 128: one CTA per fron
 constexpr int kSolveGroup = 4;    // supernodes with m <= kTinyFront per solve task (one warp each)
 constexpr int kWholeFront = 512;  // one-vector forward: supernodes with nc <= 64 and m <= 512 are one task each
 
-struct PotrfTask {  // POTRF / LDL^T of the pivot block [c0, c0 + w) of supernode s, and its inverse
-  int s, c0;
+struct GroupItem {  // pivot columns [g0, g1) (up to kGroup pivot blocks) of supernode s, factored by one group-panel
+                    // launch; its flags start at flag0: one POTRF flag per pivot block, then one TRSM counter per
+                    // diagonal strip
+  int s, g0, g1, flag0;
 };
-struct PanelTask {  // TRSM of rows [r0, r1) of supernode s against the factored pivot block [c0, c0 + w)
-  int s, c0, r0, r1;
+struct StripTask {  // rows [r0, r1) of the item's front; diag >= 0: the rows of the item's pivot block `diag`
+  int item, r0, r1, diag;
 };
 struct TileTask {  // update tile: rows [i0, i0+128) x cols [j0, min(j0+64, jend)) of a front, K = columns [c0, c0+w)
   long long lp, up;      // offsets of the front's L panel (Lx) and update block (U arena, -1 if none)
@@ -50,13 +52,17 @@ struct AsmTask {  // zero + assemble + extend-add front columns [j0, j0 + 32) of
   int s, j0;
 };
 
+// One group step of a level: the group-panel launch over its items (the level's fronts with a group at this index),
+// then the update of the columns right of each group with K = the group: part A = the next group's columns (on the
+// factor's stream: the next group panel reads them), part B = the rest (side stream, overlapping the next panel).
 struct StepRange {
-  int64_t potrf0, potrf1, panel0, panel1;
+  int64_t item0, item1, strip0, strip1;  // group items and strip tasks of the panel launch
+  int ticket;                            // the launch's ticket counter (index into the group tickets)
   int64_t tile0, tileMid, tile1;  // FP64 update tiles: part A [tile0, tileMid), part B [tileMid, tile1)
   int64_t mix0, mixMid, mix1;     // the same for the mixed-precision tiles
-  double potrfFlops, panelFlops, updateFlopsA, updateFlopsB;  // algorithmic flops of the step's launches
+  double panelFlops, updateFlopsA, updateFlopsB;  // algorithmic flops of the step's launches
 };
-// The update block of every front receives its whole Schur update once, after the panel steps of its level:
+// The update block of every front receives its whole Schur update once, after the group steps of its level:
 // U -= L21 L21^T with K = nc (tiles over the lower triangle of [nc, m)^2).
 
 struct Plan {
@@ -79,8 +85,9 @@ struct Plan {
   std::vector<AsmTask> asmTasks;
   std::vector<int64_t> asmLvlPtr;  // per level
   std::vector<double> asmLvlBytes;  // algorithmic bytes of each level's assembly (A entries + extend-add)
-  std::vector<PotrfTask> potrfTasks;
-  std::vector<PanelTask> panelTasks;
+  std::vector<GroupItem> groupItems;
+  std::vector<StripTask> strips;
+  int nGroupFlags = 0, nGroupTickets = 0;  // flags of all items, ticket counters of all group steps
   std::vector<TileTask> tileTasks;
   std::vector<int> lvlStepPtr;  // per level: steps [lvlStepPtr[L], lvlStepPtr[L+1])
   std::vector<TileTask> uTasks;  // long-K update-block tiles, per level [uLvlPtr[L], uLvlPtr[L+1])

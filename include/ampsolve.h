@@ -197,8 +197,9 @@ AMP_API int amp_profile_enable(amp_factor *f, int enable);
 AMP_API int amp_profile_read(amp_factor *f, amp_kernel_stat *stats, int32_t cap, int32_t *count);
 /* The individual timed regions behind amp_profile_read (call before it; it clears the records; a region is one
  * kernel, or the few of one class launched together: a level's small-front classes, a dot product's two passes):
- * kernel class index (order of amp_profile_read's names: assemble, panel_trsm, update_syrk, solve_forward,
- * solve_backward, permute, residual_spmv, potrf, diag_inverse, krylov, small_fronts, chain_mats), device ms, flops. */
+ * kernel class index (order of amp_profile_read's names: assemble, group_panel, update_syrk, solve_forward,
+ * solve_backward, permute, residual_spmv, potrf (unused: POTRF runs inside group_panel), diag_inverse, krylov,
+ * small_fronts, chain_mats), device ms, flops. */
 AMP_API int amp_profile_launches(amp_factor *f, int32_t *kinds, double *ms, double *flops, int32_t cap,
                                  int32_t *count);
 
