@@ -41,6 +41,14 @@ static void *xmalloc(size_t n) {
   }
   return p;
 }
+static void *xrealloc(void *q, size_t n) {
+  void *p = realloc(q, n ? n : 1);
+  if (!p) {
+    fprintf(stderr, "oracle: out of memory (%zu bytes)\n", n);
+    abort();
+  }
+  return p;
+}
 static void *xcalloc(size_t n, size_t s) {
   void *p = calloc(n ? n : 1, s ? s : 1);
   if (!p) {
@@ -1735,6 +1743,201 @@ ORC_API int orc_solve_refined(const orc_sym *S, const int *rowptr, const int *co
   free(r);
   free(dx);
   return steps;
+}
+
+
+/* ---- complex-symmetric supernodal LDL^T: ldlt.mjs:648-864 (ComplexSupernodalLDLT) ---------------------------------
+ * A = A^T complex (no conjugation), values as two arrays (re, im) on the CSR slots. Multifrontal over the supernodal
+ * tree with dense column-major complex fronts (planar: Fr, Fi), left-looking within the front: column k is updated by
+ * the earlier pivot columns (update(k, k)), its pivot settled (|d| < tau -> d scaled to magnitude tau, or tau when
+ * d = 0; non-finite -> failure), L(:, k) = F(:, k) / d with a unit diagonal; the update block's columns take all
+ * pivot columns (update(j, j)); the update block goes on the stack. tau = pivotTol * max_i hypot(A(i, i)) (diagScale,
+ * ldlt.mjs:419-424; C hypot stands for Math.hypot). Returns 1 (ok) or 0; stats[0] = nPerturbed. */
+ORC_API int orc_cfactor(const orc_sym *S, const double *re, const double *im, double pivotTol, double *Lr, double *Li,
+                        double *Dr, double *Di, int *stats) {
+  int n = S->n, nsuper = S->nsuper, maxFront = S->maxFront;
+  stats[0] = 0;
+  if (n == 0) return 1;
+  double amax = 0;
+  for (int j = 0; j < n; j++)
+    for (int p = S->lowerP[j]; p < S->lowerP[j + 1]; p++)
+      if (S->lowerI[p] == j) amax = js_max(amax, hypot(re[S->lowerSrc[p]], im[S->lowerSrc[p]]));
+  const double tau = pivotTol * (amax > 0 ? amax : 1);
+  double *Fr = xmalloc(sizeof(double) * (size_t)maxFront * maxFront + 8);
+  double *Fi = xmalloc(sizeof(double) * (size_t)maxFront * maxFront + 8);
+  int *rel = xcalloc(n, sizeof(int));
+  size_t cap = 1024, top = 0;
+  double *sr = xmalloc(sizeof(double) * cap), *si = xmalloc(sizeof(double) * cap);
+  int *stackDim = xcalloc(nsuper, sizeof(int));
+  size_t *stackPos = xmalloc(sizeof(size_t) * (nsuper + 1));
+  int nsp = 0, nPert = 0, ok = 1;
+  for (int s = 0; s < nsuper && ok; s++) {
+    const int f = S->superStart[s], nc = S->superStart[s + 1] - f, r0 = S->Sp[s], m = S->Sp[s + 1] - r0;
+    for (int r = 0; r < m; r++) rel[S->Si[r0 + r]] = r;
+    for (int b = 0; b < m; b++)
+      for (int a = b; a < m; a++) Fr[(size_t)b * m + a] = Fi[(size_t)b * m + a] = 0.0;
+    for (int c = 0; c < nc; c++) {
+      const int j = f + c;
+      const size_t cb = (size_t)c * m;
+      for (int p = S->lowerP[j]; p < S->lowerP[j + 1]; p++) {
+        const size_t at = rel[S->lowerI[p]] + cb;
+        Fr[at] += re[S->lowerSrc[p]];
+        Fi[at] += im[S->lowerSrc[p]];
+      }
+    }
+    for (int ch = S->childHead[s]; ch != -1; ch = S->childNext[ch]) {
+      const size_t off = stackPos[--nsp];
+      const int mu = stackDim[ch];
+      const int cr0 = S->Sp[ch] + (S->superStart[ch + 1] - S->superStart[ch]);
+      for (int b = 0; b < mu; b++) {
+        const size_t cbb = (size_t)rel[S->Si[cr0 + b]] * m, ub = off + (size_t)b * mu;
+        for (int a = b; a < mu; a++) {
+          const size_t at = rel[S->Si[cr0 + a]] + cbb;
+          Fr[at] += sr[ub + a];
+          Fi[at] += si[ub + a];
+        }
+      }
+      top = off;
+    }
+    /* update(k, lim): column k (rows i >= lim) -= sum_{c < min(k, nc)} L[:, c] D[c] L[k, c] */
+#define CUPDATE(K, LIM)                                              \
+    do {                                                             \
+      const int k_ = (K), lim_ = (LIM);                              \
+      const size_t kb_ = (size_t)k_ * m;                             \
+      const int cmax_ = k_ < nc ? k_ : nc;                           \
+      for (int c = 0; c < cmax_; c++) {                              \
+        const size_t b0 = (size_t)c * m;                             \
+        const double lr = Fr[k_ + b0], li = Fi[k_ + b0];             \
+        const double dr = Dr[f + c], di = Di[f + c];                 \
+        const double wr = lr * dr - li * di, wi = lr * di + li * dr; \
+        if (wr == 0 && wi == 0) continue;                            \
+        for (int i = lim_; i < m; i++) {                             \
+          const double ar = Fr[i + b0], ai = Fi[i + b0];             \
+          Fr[i + kb_] -= ar * wr - ai * wi;                          \
+          Fi[i + kb_] -= ar * wi + ai * wr;                          \
+        }                                                            \
+      }                                                              \
+    } while (0)
+    for (int k = 0; k < nc && ok; k++) {
+      CUPDATE(k, k);
+      const size_t kb = (size_t)k * m;
+      double dr = Fr[k + kb], di = Fi[k + kb];
+      const double mag = hypot(dr, di);
+      if (!(mag >= tau)) {
+        if (!isfinite(mag)) {
+          ok = 0;
+          break;
+        }
+        if (mag == 0) {
+          dr = tau;
+        } else {
+          dr *= tau / mag;
+          di *= tau / mag;
+        }
+        nPert++;
+      }
+      Dr[f + k] = dr;
+      Di[f + k] = di;
+      Fr[k + kb] = 1;
+      Fi[k + kb] = 0;
+      const double den = dr * dr + di * di, ir = dr / den, ii = -di / den;
+      for (int i = k + 1; i < m; i++) {
+        const double ar = Fr[i + kb], ai = Fi[i + kb];
+        Fr[i + kb] = ar * ir - ai * ii;
+        Fi[i + kb] = ar * ii + ai * ir;
+      }
+    }
+    if (!ok) break;
+    for (int j = nc; j < m; j++) CUPDATE(j, j);
+#undef CUPDATE
+    memcpy(Lr + S->Lxp[s], Fr, sizeof(double) * (size_t)m * nc);
+    memcpy(Li + S->Lxp[s], Fi, sizeof(double) * (size_t)m * nc);
+    const int mu = m - nc;
+    stackDim[s] = mu;
+    if (mu > 0) {
+      const size_t need = top + (size_t)mu * mu;
+      if (need > cap) {
+        size_t len = need > 2 * cap ? need : 2 * cap;
+        sr = xrealloc(sr, sizeof(double) * len);
+        si = xrealloc(si, sizeof(double) * len);
+        cap = len;
+      }
+      for (int b = 0; b < mu; b++) {
+        const size_t src = (size_t)(nc + b) * m + nc, dst = top + (size_t)b * mu;
+        for (int a = b; a < mu; a++) {
+          sr[dst + a] = Fr[src + a];
+          si[dst + a] = Fi[src + a];
+        }
+      }
+      stackPos[nsp++] = top;
+      top = need;
+    } else {
+      stackPos[nsp++] = top;
+    }
+  }
+  free(Fr);
+  free(Fi);
+  free(rel);
+  free(sr);
+  free(si);
+  free(stackDim);
+  free(stackPos);
+  stats[0] = nPert;
+  return ok;
+}
+
+/* ComplexSupernodalLDLT.solve (ldlt.mjs:802-862, the JS path): y = P b; forward with the unit lower L column by column
+ * (zero columns skipped); y /= D; backward; x = P^T y. */
+ORC_API void orc_csolve(const orc_sym *S, const double *Lr, const double *Li, const double *Dr, const double *Di,
+                        const double *br, const double *bi, double *xr, double *xi) {
+  const int n = S->n;
+  double *yr = xmalloc(sizeof(double) * (n + 1)), *yi = xmalloc(sizeof(double) * (n + 1));
+  for (int i = 0; i < n; i++) {
+    yr[i] = br[S->perm[i]];
+    yi[i] = bi[S->perm[i]];
+  }
+  for (int s = 0; s < S->nsuper; s++) {
+    const int f = S->superStart[s], nc = S->superStart[s + 1] - f, r0 = S->Sp[s], m = S->Sp[s + 1] - r0;
+    const int64_t lo = S->Lxp[s];
+    for (int c = 0; c < nc; c++) {
+      const int64_t cb = lo + (int64_t)c * m;
+      const double a = yr[f + c], b = yi[f + c];
+      if (a == 0 && b == 0) continue;
+      for (int r = c + 1; r < m; r++) {
+        const double lr = Lr[cb + r], li = Li[cb + r];
+        const int t = S->Si[r0 + r];
+        yr[t] -= lr * a - li * b;
+        yi[t] -= lr * b + li * a;
+      }
+    }
+  }
+  for (int j = 0; j < n; j++) {
+    const double ar = Dr[j], ai = Di[j], den = ar * ar + ai * ai, a = yr[j], b = yi[j];
+    yr[j] = (a * ar + b * ai) / den;
+    yi[j] = (b * ar - a * ai) / den;
+  }
+  for (int s = S->nsuper - 1; s >= 0; s--) {
+    const int f = S->superStart[s], nc = S->superStart[s + 1] - f, r0 = S->Sp[s], m = S->Sp[s + 1] - r0;
+    const int64_t lo = S->Lxp[s];
+    for (int c = nc - 1; c >= 0; c--) {
+      const int64_t cb = lo + (int64_t)c * m;
+      double a = yr[f + c], b = yi[f + c];
+      for (int r = c + 1; r < m; r++) {
+        const double lr = Lr[cb + r], li = Li[cb + r];
+        const int t = S->Si[r0 + r];
+        a -= lr * yr[t] - li * yi[t];
+        b -= lr * yi[t] + li * yr[t];
+      }
+      yr[f + c] = a;
+      yi[f + c] = b;
+    }
+  }
+  for (int i = 0; i < n; i++) {
+    xr[S->perm[i]] = yr[i];
+    xi[S->perm[i]] = yi[i];
+  }
+  free(yr);
+  free(yi);
 }
 
 /* ---- up-looking Cholesky (the reference's own test oracle): sparse.mjs:1379-1544 ------------------------------- */

@@ -60,6 +60,9 @@ def lib():
         L.orc_solve_refined.restype = C.c_int
         L.orc_solve_refined.argtypes = [C.c_void_p, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_int, _f64p, C.c_int,
                                         C.c_double, _f64p, C.POINTER(C.c_double)]
+        L.orc_cfactor.restype = C.c_int
+        L.orc_cfactor.argtypes = [C.c_void_p, _f64p, _f64p, C.c_double, _f64p, _f64p, _f64p, _f64p, _i32p]
+        L.orc_csolve.argtypes = [C.c_void_p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p]
         L.orc_up_create.restype = C.c_void_p
         L.orc_up_create.argtypes = [C.c_int, _i32p, _i32p, _i32p]
         L.orc_up_Lp.restype = C.POINTER(C.c_int)
@@ -254,6 +257,33 @@ def solve_refined(sym: Symbolic, pat, values, Lx, D, b, kind: str = "ldlt", max_
                                     np.ascontiguousarray(Lx, np.float64), Dv, 0 if kind == "chol" else 1,
                                     np.ascontiguousarray(b, np.float64), max_steps, tol, x, C.byref(rel))
     return x[:n], rel.value, steps
+
+
+def cfactor(sym: Symbolic, re, im, pivot_tol: float = 1e-13):
+    """ComplexSupernodalLDLT.factor(re, im, {pivotTol}) (ldlt.mjs:667-800): (ok, Lr, Li, Dr, Di, nPerturbed)."""
+    n, nl = max(sym.n, 1), max(int(sym.nnzLStored), 1)
+    Lr, Li, Dr, Di = np.zeros(nl), np.zeros(nl), np.zeros(n), np.zeros(n)
+    st = np.zeros(2, np.int32)
+    ok = lib().orc_cfactor(sym.handle, np.ascontiguousarray(re, np.float64), np.ascontiguousarray(im, np.float64),
+                           pivot_tol, Lr, Li, Dr, Di, st)
+    k = int(sym.nnzLStored)
+    return bool(ok), Lr[:k], Li[:k], Dr[: sym.n], Di[: sym.n], int(st[0])
+
+
+def csolve(sym: Symbolic, Lr, Li, Dr, Di, br, bi):
+    """ComplexSupernodalLDLT.solve(br, bi) (ldlt.mjs:802-862): (xr, xi)."""
+    n = max(sym.n, 1)
+    xr, xi = np.zeros(n), np.zeros(n)
+    f = lambda a: np.ascontiguousarray(a if len(a) else np.zeros(1), np.float64)  # noqa: E731
+    lib().orc_csolve(sym.handle, f(Lr), f(Li), f(Dr), f(Di), f(br), f(bi), xr, xi)
+    return xr[: sym.n], xi[: sym.n]
+
+
+def cmatvec(pat, re, im, xr, xi):
+    """y = A x for complex A = re + i im on the pattern and complex x (the residual of complexSolveRefined)."""
+    yr = matvec(pat, re, xr) - matvec(pat, im, xi)
+    yi = matvec(pat, re, xi) + matvec(pat, im, xr)
+    return yr, yi
 
 
 class UpLookingCholesky:

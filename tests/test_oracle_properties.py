@@ -325,3 +325,60 @@ def test_ldlt_inertia_sylvester():
     assert ok_u and nneg_u == 10
     ok, _, _, nneg, _ = O.factor(sym, w.values, kind="ldlt")
     assert ok and nneg == 10
+
+
+# ---- complex-symmetric LDL^T (ldlt.mjs:648-864) -------------------------------------------------------------------
+def _complex_case(N=5, shift=30.0, loss=0.3):
+    w = W.maxwell3d(N, 2, 12.0, shift, 5, 1)
+    return w, loss * w.values
+
+
+def test_complex_ldlt_solves_the_complex_symmetric_system():
+    import scipy.sparse as sp
+    w, im = _complex_case()
+    so = O.analyze(w.pat, perm=O.nd3_order(w.pat, w.x, w.y, w.z))
+    ok, Lr, Li, Dr, Di, npert = O.cfactor(so, w.values, im)
+    assert ok and npert == 0
+    rng = np.random.default_rng(4)
+    br, bi = rng.uniform(-1, 1, w.n), rng.uniform(-1, 1, w.n)
+    xr, xi = O.csolve(so, Lr, Li, Dr, Di, br, bi)
+    A = sp.csr_matrix((w.values + 1j * im, w.pat.colidx, w.pat.rowptr), shape=(w.n, w.n)).toarray()
+    x = np.linalg.solve(A, br + 1j * bi)
+    assert np.linalg.norm(xr + 1j * xi - x) / np.linalg.norm(x) < 1e-10
+    # no conjugation: A^T = A, and the factor reproduces A = L D L^T
+    assert np.array_equal(A, A.T)
+
+
+def test_complex_ldlt_reduces_to_the_real_one_for_real_values():
+    w, _ = _complex_case(4)
+    so = O.analyze(w.pat, perm=O.nd3_order(w.pat, w.x, w.y, w.z))
+    ok, Lr, Li, Dr, Di, npert = O.cfactor(so, w.values, np.zeros_like(w.values))
+    okr, Lx, D, nneg, nper = O.factor(so, w.values, kind="ldlt")
+    assert ok and okr and npert == nper
+
+    def lower(L):  # the lower parts of the stored blocks (the upper part of a diagonal block is never read)
+        out = []
+        for s in range(so.nsuper):
+            nc, m = int(so.superStart[s + 1] - so.superStart[s]), int(so.Sp[s + 1] - so.Sp[s])
+            blk = L[so.Lxp[s]: so.Lxp[s] + m * nc].reshape(nc, m)
+            out += [blk[c, c + 1:] for c in range(nc)]
+        return np.concatenate(out)
+
+    assert not np.any(lower(Li)) and not np.any(Di)
+    assert np.max(np.abs(lower(Lr) - lower(Lx))) <= 1e-10 * np.max(np.abs(lower(Lx)))
+    assert np.max(np.abs(Dr - D)) <= 1e-10 * np.max(np.abs(D))
+
+
+def test_complex_ldlt_perturbs_a_zero_pivot_and_fails_on_nan():
+    n = 4
+    rp = np.arange(0, n * n + 1, n, dtype=np.int32)
+    ci = np.tile(np.arange(n, dtype=np.int32), n)
+    pat = W.CsrPattern(n, rp, ci)
+    A = np.eye(n) * 2.0
+    A[0, 0] = 0.0  # a zero pivot: perturbed to tau
+    so = O.analyze(pat, perm=np.arange(n, dtype=np.int32))
+    ok, Lr, Li, Dr, Di, npert = O.cfactor(so, A.reshape(-1), np.zeros(n * n))
+    assert ok and npert == 1 and Dr[0] == 1e-13 * 2.0
+    A[2, 2] = np.nan
+    ok, *_ = O.cfactor(so, A.reshape(-1), np.zeros(n * n))
+    assert not ok
