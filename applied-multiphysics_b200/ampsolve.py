@@ -24,7 +24,7 @@ _lib = None
 AMP_OK, AMP_NOT_SPD, AMP_NONFINITE_PIVOT, AMP_PATTERN_MISMATCH, AMP_BAD_LENGTH, AMP_NO_FACTOR, AMP_NEED_COORDS, \
     AMP_DEVICE_TIMEOUT, AMP_CUDA_ERROR, AMP_OOM, AMP_INVALID = range(11)
 ORDER_AMD, ORDER_ND, ORDER_ND3, ORDER_GIVEN = range(4)
-CHOLESKY, LDLT = 0, 1
+CHOLESKY, LDLT, LDLT_COMPLEX = 0, 1, 2
 AMP_ELEM_P1_TRI_SCALAR, AMP_ELEM_P1_TET_ELASTIC = 0, 1
 FP64, MIXED = 0, 1
 
@@ -126,6 +126,13 @@ SIGNATURES = {
     "amp_factor_set_wait_limit": (C.c_int, [C.c_void_p, C.c_int64]),
     "amp_matvec_csr": (C.c_int, [C.c_int32, _i32p, _i32p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int]),
     "amp_factor_set_mass": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int]),
+    "amp_cfactor_create": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "amp_cfactor_numeric": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_double,
+                                      C.POINTER(_FactorResult)]),
+    "amp_csolve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int]),
+    "amp_csolve_refined": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int,
+                                     C.POINTER(_RefineOpts), C.POINTER(_RefineStats)]),
+    "amp_cfactor_download": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "amp_assembly_create": (C.c_int, [C.c_int, C.c_int32, _i32p, _i32p, C.c_int32, C.c_void_p, C.c_int64, C.c_void_p,
                                       C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "amp_assemble": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
@@ -713,6 +720,70 @@ class SupernodalLDLT:
         an indefinite matrix, gmres-real.mjs:31-105)."""
         self._need()
         return self.num.solve_gmres(b, tol=tol, restart=restart, maxIter=maxIter)
+
+
+class ComplexSupernodalLDLT:
+    """Complex-symmetric multifrontal LDL^T (A = A^T, no conjugation) over a supernodal analysis, on the GPU: the
+    reference's ComplexSupernodalLDLT (ldlt.mjs:648-864) with its solveRefined (:870-900). Values and right-hand sides
+    are (re, im) pairs of FP64 arrays on the CSR slots / rows, as the reference takes them."""
+
+    def __init__(self, sym: SymbolicAnalysis):
+        self.sym = sym
+        self.kernel = "cuda-sm100a"
+        self.ok = False
+        self.nPerturbed = 0
+        h = C.c_void_p()
+        _check(lib().amp_cfactor_create(sym.handle, C.byref(h)))
+        self._h = h.value
+
+    def factor(self, re, im, pivotTol: float = 1e-13) -> dict:
+        r, i = _f64(re), _f64(im)
+        if len(r) != _nnz_of(self.sym) or len(i) != len(r):
+            raise AmpError(AMP_BAD_LENGTH, f"factorNumeric: {len(r)} values for a pattern with "
+                                           f"{_nnz_of(self.sym)} entries")
+        res = _FactorResult()
+        _check(lib().amp_cfactor_numeric(self._h, r.ctypes.data if r.size else None,
+                                         i.ctypes.data if i.size else None, r.size, 0, pivotTol, C.byref(res)))
+        self.ok, self.nPerturbed = bool(res.ok), res.n_perturbed
+        return {"ok": self.ok, "nPerturbed": self.nPerturbed, "ms": res.ms}
+
+    def _need(self):
+        if not self.ok:
+            raise AmpError(AMP_NO_FACTOR, "solveNumeric: no successful numeric factorization")
+
+    def solve(self, br, bi) -> dict:
+        self._need()
+        r, i = _f64(br), _f64(bi)
+        xr, xi = np.empty_like(r), np.empty_like(i)
+        _check(lib().amp_csolve(self._h, r.ctypes.data, i.ctypes.data, 1, xr.ctypes.data, xi.ctypes.data, 0))
+        return {"re": xr, "im": xi}
+
+    def solveRefined(self, pat, re, im, br, bi, maxSteps: int = 3, tol: float = 1e-14) -> dict:
+        """Refinement against the factored (unperturbed) values; `pat`, `re`, `im` must be what was factored."""
+        self._need()
+        checkSymbolic(self.sym, pat)
+        if len(re) != _nnz_of(self.sym):
+            raise AmpError(AMP_BAD_LENGTH, f"solveRefined: {len(re)} values for a pattern with "
+                                           f"{_nnz_of(self.sym)} entries")
+        r, i = _f64(br), _f64(bi)
+        xr, xi = np.empty_like(r), np.empty_like(i)
+        st = _RefineStats()
+        _check(lib().amp_csolve_refined(self._h, r.ctypes.data, i.ctypes.data, 1, xr.ctypes.data, xi.ctypes.data, 0,
+                                        C.byref(_RefineOpts(maxSteps, tol)), C.byref(st)))
+        return {"re": xr, "im": xi, "relResidual": st.rel_residual, "steps": st.steps}
+
+    def factors(self):
+        """(Lr, Li, Dr, Di) host copies."""
+        nl, n = max(self.sym.nnzLStored, 1), max(self.sym.n, 1)
+        Lr, Li, Dr, Di = np.zeros(nl), np.zeros(nl), np.zeros(n), np.zeros(n)
+        _check(lib().amp_cfactor_download(self._h, Lr.ctypes.data, Li.ctypes.data, Dr.ctypes.data, Di.ctypes.data))
+        return Lr[: self.sym.nnzLStored], Li[: self.sym.nnzLStored], Dr[: self.sym.n], Di[: self.sym.n]
+
+    def __del__(self):
+        h = self.__dict__.get("_h")
+        if h and _lib is not None:
+            _lib.amp_factor_destroy(h)
+            self._h = None
 
 
 # ---- 'auto' choice between the direct solver and the iterative one ----------------------------------------------------

@@ -163,6 +163,13 @@ struct amp_plan_s {
   int *dRowptr = nullptr, *dColidx = nullptr;
   std::vector<int> rowptr, colidx;  // host copy of the pattern (uploaded with the schedule)
   bool uploaded = false;
+  // the dense schedule of every front, for complex-symmetric factors (built and uploaded by the first of them)
+  amp::DenseSched cx;
+  bool cxUploaded = false;
+  amp::AsmTask *dCxAsm = nullptr;
+  amp::GroupItem *dCxItems = nullptr;
+  amp::StripTask *dCxStrips = nullptr;
+  amp::TileTask *dCxTiles = nullptr, *dCxU = nullptr;
   ~amp_plan_s() { mem.release(); }
 };
 
@@ -233,6 +240,11 @@ struct amp_factor_s {
   int *dRowGroup = nullptr;
   double *dGroupNorms = nullptr;  // 2 x groups x multi_max_vectors()
   DevMem groupMem;
+  // complex-symmetric LDL^T (kind AMP_LDLT_COMPLEX): factor, update arena, L21 D, pivots, values, solve vectors
+  amp::cplx *dLc = nullptr, *dUc = nullptr, *dWc = nullptr, *dDc = nullptr, *dValC = nullptr;
+  amp::cplx *dYc = nullptr, *dBc = nullptr, *dXc = nullptr, *dRc = nullptr, *dDXc = nullptr;
+  double *dBr = nullptr, *dBi = nullptr, *dXr = nullptr, *dXi = nullptr, *dNormsC = nullptr;
+  int *dCxFlags = nullptr;
   // shift-invert eigen operator: M's values on the pattern; Krylov workspace (grown on demand)
   double *dMass = nullptr;
   DevMem massMem, eigMem;
@@ -807,6 +819,79 @@ struct EigenWork {
 
 }  // namespace
 
+// ---- complex-symmetric LDL^T (ldlt.mjs:648-900) --------------------------------------------------------------------
+namespace {
+
+void upload_cx(amp_plan *pl) {
+  if (pl->cxUploaded) return;
+  amp::build_dense_all(pl->P, pl->cx);
+  DevMem &m = pl->mem;
+  pl->dCxAsm = m.upload(pl->cx.asmTasks);
+  pl->dCxItems = m.upload(pl->cx.groupItems);
+  pl->dCxStrips = m.upload(pl->cx.strips);
+  pl->dCxTiles = m.upload(pl->cx.tileTasks);
+  pl->dCxU = m.upload(pl->cx.uTasks);
+  pl->cxUploaded = true;
+}
+
+// the complex factorization: per level, assembly, the group steps (group panel, then the group's update of the
+// columns right of it: the next group's columns, then the rest), the update blocks
+void enqueue_cfactor(amp_factor *f) {
+  const amp::Plan &P = f->plan->P;
+  const amp::DenseSched &D = f->plan->cx;
+  amp::DevPlan dp = f->plan->dp;
+  if (f->waitSpins > 0) dp.spin = f->waitSpins;
+  cudaStream_t st = f->stream;
+  ck(cudaMemsetAsync(f->dStatus, 0xff, sizeof(unsigned long long), st), "memset status");
+  ck(cudaMemsetAsync(f->dCounts, 0, 2 * sizeof(int), st), "memset counts");
+  if (D.nGroupFlags + D.nGroupTickets > 0)
+    ck(cudaMemsetAsync(f->dCxFlags, 0, sizeof(int) * (D.nGroupFlags + D.nGroupTickets), st), "memset flags");
+  int *tickets = f->dCxFlags + D.nGroupFlags;
+  amp::launch_ctau(f->dValC, dp, f->dScal, st);
+  const amp::LdltArgs<amp::cplx> ld{f->dScal, f->dCounts, f->dWc, f->dDc, nullptr, nullptr};
+  for (int L = 0; L < P.nlevels; L++) {
+    if (D.asmLvlPtr[L + 1] > D.asmLvlPtr[L])
+      timed(f, K_ASSEMBLE, 0.0, 0.0, [&] {
+        amp::launch_assemble<amp::cplx>(f->plan->dCxAsm + D.asmLvlPtr[L], D.asmLvlPtr[L + 1] - D.asmLvlPtr[L], dp,
+                                        f->dValC, f->dLc, f->dUc, f->dStatus, st);
+      });
+    for (int k = D.lvlStepPtr[L]; k < D.lvlStepPtr[L + 1]; k++) {
+      const amp::StepRange &sr = D.steps[k];
+      timed(f, K_PANEL, 4.0 * sr.panelFlops, 0.0, [&] {
+        amp::launch_group_panel<amp::cplx>(f->plan->dCxItems, f->plan->dCxStrips + sr.strip0,
+                                           (int)(sr.strip1 - sr.strip0), tickets + sr.ticket, f->dCxFlags, dp,
+                                           f->dLc, f->dStatus, nullptr, nullptr, ld, st);
+      });
+      if (sr.tile1 > sr.tile0)
+        timed(f, K_UPDATE, 4.0 * (sr.updateFlopsA + sr.updateFlopsB), 0.0, [&] {
+          amp::launch_update_c(f->plan->dCxTiles + sr.tile0, sr.tile1 - sr.tile0, f->dLc, f->dUc, f->dWc, f->dStatus,
+                               st);
+        });
+    }
+    if (D.uLvlPtr[L + 1] > D.uLvlPtr[L])
+      timed(f, K_UPDATE, 0.0, 0.0, [&] {
+        amp::launch_update_c(f->plan->dCxU + D.uLvlPtr[L], D.uLvlPtr[L + 1] - D.uLvlPtr[L], f->dLc, f->dUc, f->dWc,
+                             f->dStatus, st);
+      });
+  }
+}
+
+// y (permuted order) := A^-1 y
+void csolve_permuted(amp_factor *f, amp::cplx *y) {
+  const amp::Plan &P = f->plan->P;
+  timed(f, K_FORWARD, 8.0 * (double)P.nnzLStored, 16.0 * (double)P.nnzLStored, [&] {
+    return amp::launch_csolve_permuted(f->plan->dp, P.lvlPtr.data(), P.nlevels, f->dLc, f->dDc, y, f->stream);
+  });
+}
+
+int require_complex(const amp_factor *f) {
+  if (!f) return fail(AMP_INVALID, "null handle");
+  if (f->kind != AMP_LDLT_COMPLEX) return fail(AMP_INVALID, "a real factor: use the real-valued entry points");
+  return AMP_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 const char *amp_last_error(void) { return g_err.c_str(); }
@@ -1058,6 +1143,7 @@ int amp_factor_numeric(amp_factor *f, const double *values, int64_t nvalues, int
                        amp_factor_result *res) {
   return guarded([&] {
     if (!f) return fail(AMP_INVALID, "null handle");
+    if (f->kind == AMP_LDLT_COMPLEX) return fail(AMP_INVALID, "a complex-symmetric factor: use the amp_c* entry points");
     const amp::Plan &P = f->plan->P;
     if (nvalues != P.patNnz)
       return fail(AMP_BAD_LENGTH, "factorNumeric: " + std::to_string(nvalues) + " values for a pattern with " +
@@ -1125,6 +1211,7 @@ int amp_factor_numeric(amp_factor *f, const double *values, int64_t nvalues, int
 int amp_solve(amp_factor *f, const double *b, int32_t nrhs, double *x, int on_device) {
   return guarded([&] {
     if (!f) return fail(AMP_INVALID, "null handle");
+    if (f->kind == AMP_LDLT_COMPLEX) return fail(AMP_INVALID, "a complex-symmetric factor: use the amp_c* entry points");
     if (!f->ok) return fail(AMP_NO_FACTOR, "solveNumeric: no successful numeric factorization");
     const amp::Plan &P = f->plan->P;
     if (nrhs <= 0 || P.n == 0) return (int)AMP_OK;
@@ -1151,6 +1238,7 @@ int amp_solve_refined(amp_factor *f, const double *b, int32_t nrhs, double *x, i
                       const amp_refine_opts *opts, amp_refine_stats *stats) {
   return guarded([&] {
     if (!f) return fail(AMP_INVALID, "null handle");
+    if (f->kind == AMP_LDLT_COMPLEX) return fail(AMP_INVALID, "a complex-symmetric factor: use the amp_c* entry points");
     if (!f->ok) return fail(AMP_NO_FACTOR, "solveNumeric: no successful numeric factorization");
     const amp::Plan &P = f->plan->P;
     amp_refine_opts o{3, 1e-14};
@@ -1216,6 +1304,7 @@ int amp_solve_refined(amp_factor *f, const double *b, int32_t nrhs, double *x, i
 int amp_factor_set_row_groups(amp_factor *f, int32_t ngroups, const int64_t *offsets) {
   return guarded([&] {
     if (!f) return fail(AMP_INVALID, "null handle");
+    if (f->kind == AMP_LDLT_COMPLEX) return fail(AMP_INVALID, "a complex-symmetric factor: use the amp_c* entry points");
     const int n = f->plan->P.n;
     if (ngroups < 0 || (ngroups > 0 && !offsets)) return fail(AMP_INVALID, "row groups: bad arguments");
     if (ngroups == 0) {
@@ -1241,6 +1330,7 @@ int amp_solve_gmres(amp_factor *f, const double *b, double *x, int on_device, co
                     amp_gmres_stats *stats) {
   return guarded([&] {
     if (!f) return fail(AMP_INVALID, "null handle");
+    if (f->kind == AMP_LDLT_COMPLEX) return fail(AMP_INVALID, "a complex-symmetric factor: use the amp_c* entry points");
     if (!f->ok) return fail(AMP_NO_FACTOR, "solveNumeric: no successful numeric factorization");
     amp_gmres_opts o{1e-10, 40, 400};
     if (opts) o = *opts;
@@ -1371,6 +1461,7 @@ int amp_solve_gmres(amp_factor *f, const double *b, double *x, int on_device, co
 int amp_factor_download(const amp_factor *f, double *Lx, double *D) {
   return guarded([&] {
     if (!f) return fail(AMP_INVALID, "null handle");
+    if (f->kind == AMP_LDLT_COMPLEX) return fail(AMP_INVALID, "a complex-symmetric factor: use the amp_c* entry points");
     const amp::Plan &P = f->plan->P;
     ck(cudaSetDevice(f->plan->device), "cudaSetDevice");
     if (Lx && P.nnzLStored && f->dLx)
@@ -1455,6 +1546,199 @@ int amp_profile_read(amp_factor *f, amp_kernel_stat *stats, int32_t cap, int32_t
   });
 }
 
+
+int amp_cfactor_create(amp_plan *pl, amp_factor **out) {
+  return guarded([&] {
+    if (!pl || !out) return fail(AMP_INVALID, "null handle");
+    *out = nullptr;
+    ck(cudaSetDevice(pl->device), "cudaSetDevice");
+    if (!pl->uploaded) {
+      upload_plan(pl);
+      pl->dRowptr = pl->mem.upload(pl->rowptr);
+      pl->dColidx = pl->mem.upload(pl->colidx);
+      pl->uploaded = true;
+    }
+    upload_cx(pl);
+    auto *f = new amp_factor_s();
+    f->plan = pl;
+    f->kind = AMP_LDLT_COMPLEX;
+    f->precision = AMP_FP64;
+    try {
+      ck(cudaStreamCreateWithFlags(&f->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+      ck(cudaEventCreate(&f->ev0), "cudaEventCreate");
+      ck(cudaEventCreate(&f->ev1), "cudaEventCreate");
+      const amp::Plan &P = pl->P;
+      const size_t n = (size_t)std::max(1, P.n);
+      f->dLc = f->mem.alloc<amp::cplx>((size_t)P.nnzLStored);
+      f->dUc = f->mem.alloc<amp::cplx>((size_t)P.arenaDoubles);
+      f->dWc = f->mem.alloc<amp::cplx>((size_t)P.nnzLStored);
+      f->dDc = f->mem.alloc<amp::cplx>(n);
+      f->dValC = f->mem.alloc<amp::cplx>((size_t)P.patNnz);
+      for (amp::cplx **v : {&f->dYc, &f->dBc, &f->dXc, &f->dRc, &f->dDXc}) *v = f->mem.alloc<amp::cplx>(n);
+      for (double **v : {&f->dBr, &f->dBi, &f->dXr, &f->dXi}) *v = f->mem.alloc<double>(n);
+      f->dNormsC = f->mem.alloc<double>(2);
+      f->dScal = f->mem.alloc<double>(2);
+      f->dCounts = f->mem.alloc<int>(2);
+      f->dStatus = f->mem.alloc<unsigned long long>(1);
+      f->dCxFlags = f->mem.alloc<int>((size_t)std::max(1, pl->cx.nGroupFlags + pl->cx.nGroupTickets));
+      init_device_once(pl->device);
+    } catch (...) {
+      delete f;
+      throw;
+    }
+    *out = f;
+    return (int)AMP_OK;
+  });
+}
+
+int amp_cfactor_numeric(amp_factor *f, const double *re, const double *im, int64_t nvalues, int values_on_device,
+                        double pivot_tol, amp_factor_result *res) {
+  return guarded([&] {
+    if (int rc = require_complex(f)) return rc;
+    const amp::Plan &P = f->plan->P;
+    if (nvalues != P.patNnz)
+      return fail(AMP_BAD_LENGTH, "factorNumeric: " + std::to_string(nvalues) + " values for a pattern with " +
+                                      std::to_string(P.patNnz) + " entries");
+    if (nvalues > 0 && (!re || !im)) return fail(AMP_INVALID, "factor: null values");
+    ck(cudaSetDevice(f->plan->device), "cudaSetDevice");
+    f->ok = false;
+    amp_factor_result r{};
+    r.fail_column = -1;
+    if (P.n == 0) {
+      f->ok = true;
+      r.ok = 1;
+      if (res) *res = r;
+      return (int)AMP_OK;
+    }
+    cudaStream_t st = f->stream;
+    const double *dre = re, *dim = im;
+    DevMem tmp;
+    if (!values_on_device) {
+      double *a = tmp.alloc<double>((size_t)nvalues), *b = tmp.alloc<double>((size_t)nvalues);
+      ck(cudaMemcpyAsync(a, re, sizeof(double) * nvalues, cudaMemcpyHostToDevice, st), "copy re");
+      ck(cudaMemcpyAsync(b, im, sizeof(double) * nvalues, cudaMemcpyHostToDevice, st), "copy im");
+      dre = a;
+      dim = b;
+    }
+    amp::launch_cpack(nvalues, dre, dim, f->dValC, st);
+    f->hasValues = true;
+    ck(cudaMemcpyAsync(f->dScal, &pivot_tol, sizeof(double), cudaMemcpyHostToDevice, st), "copy pivotTol");
+    ck(cudaEventRecord(f->ev0, st), "event");
+    enqueue_cfactor(f);
+    ck(cudaGetLastError(), "kernel launch");
+    ck(cudaEventRecord(f->ev1, st), "event");
+    unsigned long long status = 0;
+    int counts[2] = {0, 0};
+    ck(cudaMemcpyAsync(&status, f->dStatus, sizeof status, cudaMemcpyDeviceToHost, st), "copy status");
+    ck(cudaMemcpyAsync(counts, f->dCounts, sizeof counts, cudaMemcpyDeviceToHost, st), "copy counts");
+    ck(cudaStreamSynchronize(st), "factor");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, f->ev0, f->ev1);
+    r.ms = ms;
+    r.n_perturbed = counts[1];
+    if (status == amp::kStatusOk) {
+      r.ok = 1;
+      f->ok = true;
+    } else if (((status >> 24) & 0xff) == 3) {
+      if (res) *res = r;
+      return fail(AMP_DEVICE_TIMEOUT, "factorNumeric: a device wait timed out");
+    } else {
+      r.ok = 0;
+      r.fail_column = (int32_t)(status >> 32);
+    }
+    if (res) *res = r;
+    return (int)AMP_OK;
+  });
+}
+
+int amp_csolve_refined(amp_factor *f, const double *br, const double *bi, int32_t nrhs, double *xr, double *xi,
+                       int on_device, const amp_refine_opts *opts, amp_refine_stats *stats) {
+  return guarded([&] {
+    if (int rc = require_complex(f)) return rc;
+    if (!f->ok) return fail(AMP_NO_FACTOR, "solveNumeric: no successful numeric factorization");
+    const amp::Plan &P = f->plan->P;
+    const int n = P.n;
+    amp_refine_stats stt{0.0, 0};
+    if (nrhs <= 0 || n == 0) {
+      if (stats) *stats = stt;
+      return (int)AMP_OK;
+    }
+    ck(cudaSetDevice(f->plan->device), "cudaSetDevice");
+    cudaStream_t st = f->stream;
+    const int *perm = f->plan->dp.perm;
+    const size_t vb = sizeof(double) * (size_t)n;
+    for (int k = 0; k < nrhs; k++) {
+      const double *kr = br + (size_t)k * n, *ki = bi + (size_t)k * n;
+      if (!on_device) {
+        ck(cudaMemcpyAsync(f->dBr, kr, vb, cudaMemcpyHostToDevice, st), "copy b");
+        ck(cudaMemcpyAsync(f->dBi, ki, vb, cudaMemcpyHostToDevice, st), "copy b");
+        kr = f->dBr;
+        ki = f->dBi;
+      }
+      amp::launch_cpack(n, kr, ki, f->dBc, st);
+      amp::launch_cpermute_vec(n, f->dBc, perm, f->dYc, true, st);
+      csolve_permuted(f, f->dYc);
+      amp::launch_cpermute_vec(n, f->dYc, perm, f->dXc, false, st);
+      int steps = 0;
+      double rel = 0.0;
+      for (; opts; steps++) {  // complexSolveRefined: residual against the unperturbed values, up to maxSteps
+        ck(cudaMemsetAsync(f->dNormsC, 0, 2 * sizeof(double), st), "memset");
+        timed(f, K_RESIDUAL, 8.0 * P.patNnz, 32.0 * P.patNnz, [&] {
+          amp::launch_cresidual(n, f->plan->dRowptr, f->plan->dColidx, f->dValC, f->dXc, f->dBc, f->dRc, f->dNormsC,
+                                st);
+        });
+        double nr[2];
+        ck(cudaMemcpyAsync(nr, f->dNormsC, sizeof nr, cudaMemcpyDeviceToHost, st), "norms");
+        ck(cudaStreamSynchronize(st), "residual");
+        double bn = std::sqrt(nr[1]);
+        if (bn == 0 || std::isnan(bn)) bn = 1;
+        rel = std::sqrt(nr[0]) / bn;
+        if (rel < opts->tol || steps >= opts->max_steps) break;
+        amp::launch_cpermute_vec(n, f->dRc, perm, f->dYc, true, st);
+        csolve_permuted(f, f->dYc);
+        amp::launch_cpermute_vec(n, f->dYc, perm, f->dDXc, false, st);
+        amp::launch_caxpy(n, f->dXc, f->dDXc, st);
+      }
+      double *ox = xr + (size_t)k * n, *oi = xi + (size_t)k * n;
+      amp::launch_cunpack(n, f->dXc, on_device ? ox : f->dXr, on_device ? oi : f->dXi, st);
+      if (!on_device) {
+        ck(cudaMemcpyAsync(ox, f->dXr, vb, cudaMemcpyDeviceToHost, st), "copy x");
+        ck(cudaMemcpyAsync(oi, f->dXi, vb, cudaMemcpyDeviceToHost, st), "copy x");
+      }
+      ck(cudaGetLastError(), "kernel launch");
+      ck(cudaStreamSynchronize(st), "solve");
+      stt.rel_residual = std::max(stt.rel_residual, rel);
+      stt.steps = std::max(stt.steps, steps);
+    }
+    if (stats) *stats = stt;
+    return (int)AMP_OK;
+  });
+}
+
+int amp_csolve(amp_factor *f, const double *br, const double *bi, int32_t nrhs, double *xr, double *xi,
+               int on_device) {
+  return amp_csolve_refined(f, br, bi, nrhs, xr, xi, on_device, nullptr, nullptr);
+}
+
+int amp_cfactor_download(const amp_factor *f, double *Lr, double *Li, double *Dr, double *Di) {
+  return guarded([&] {
+    if (int rc = require_complex(f)) return rc;
+    const amp::Plan &P = f->plan->P;
+    ck(cudaSetDevice(f->plan->device), "cudaSetDevice");
+    auto split = [&](const amp::cplx *src, int64_t len, double *re, double *im) {
+      if ((!re && !im) || len == 0) return;
+      std::vector<amp::cplx> h((size_t)len);
+      ck(cudaMemcpy(h.data(), src, sizeof(amp::cplx) * len, cudaMemcpyDeviceToHost), "copy factor");
+      for (int64_t i = 0; i < len; i++) {
+        if (re) re[i] = h[i].re;
+        if (im) im[i] = h[i].im;
+      }
+    };
+    split(f->dLc, P.nnzLStored, Lr, Li);
+    split(f->dDc, P.n, Dr, Di);
+    return (int)AMP_OK;
+  });
+}
 
 int amp_assembly_create(int kind, int32_t n, const int32_t *rowptr, const int32_t *colidx, int32_t nnodes,
                         const double *coords, int64_t nelem, const int32_t *conn, const int32_t *dofs, int device,
@@ -1559,6 +1843,7 @@ void amp_assembly_destroy(amp_assembly *a) { delete a; }
 int amp_factor_set_mass(amp_factor *f, const double *mvalues, int64_t nvalues, int on_device) {
   return guarded([&] {
     if (!f || (nvalues > 0 && !mvalues)) return fail(AMP_INVALID, "set_mass: null handle or values");
+    if (f->kind == AMP_LDLT_COMPLEX) return fail(AMP_INVALID, "a complex-symmetric factor: use the amp_c* entry points");
     const amp::Plan &P = f->plan->P;
     if (nvalues != P.patNnz)
       return fail(AMP_BAD_LENGTH, "setMass: " + std::to_string(nvalues) + " values for a pattern with " +
@@ -1575,6 +1860,7 @@ int amp_factor_set_mass(amp_factor *f, const double *mvalues, int64_t nvalues, i
 int amp_shift_invert_apply(amp_factor *f, const double *X, int32_t m, double *Y, int on_device) {
   return guarded([&] {
     if (!f) return fail(AMP_INVALID, "null handle");
+    if (f->kind == AMP_LDLT_COMPLEX) return fail(AMP_INVALID, "a complex-symmetric factor: use the amp_c* entry points");
     if (!f->ok) return fail(AMP_NO_FACTOR, "solveNumeric: no successful numeric factorization");
     if (!f->dMass) return fail(AMP_INVALID, "shift-invert: no mass values (amp_factor_set_mass)");
     const amp::Plan &P = f->plan->P;
@@ -1601,6 +1887,7 @@ int amp_eigen_block_arnoldi(amp_factor *f, const amp_eigen_opts *opts, double *m
                             amp_eigen_stats *stats) {
   return guarded([&] {
     if (!f || !opts || !mu) return fail(AMP_INVALID, "eigen: null argument");
+    if (f->kind == AMP_LDLT_COMPLEX) return fail(AMP_INVALID, "a complex-symmetric factor: use the amp_c* entry points");
     if (!f->ok) return fail(AMP_NO_FACTOR, "solveNumeric: no successful numeric factorization");
     if (!f->dMass) return fail(AMP_INVALID, "eigen: no mass values (amp_factor_set_mass)");
     const amp::Plan &P = f->plan->P;
@@ -1821,6 +2108,7 @@ int amp_matvec_csr(int32_t n, const int32_t *rowptr, const int32_t *colidx, cons
 int amp_matvec(amp_factor *f, const double *x, int32_t nrhs, double *y) {
   return guarded([&] {
     if (!f) return fail(AMP_INVALID, "null handle");
+    if (f->kind == AMP_LDLT_COMPLEX) return fail(AMP_INVALID, "a complex-symmetric factor: use the amp_c* entry points");
     if (!f->hasValues) return fail(AMP_NO_FACTOR, "matVec: no values on the device (call amp_factor_numeric first)");
     const amp::Plan &P = f->plan->P;
     if (nrhs <= 0 || P.n == 0) return (int)AMP_OK;

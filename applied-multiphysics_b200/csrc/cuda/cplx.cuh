@@ -11,7 +11,7 @@ namespace amp {
 
 struct __align__(16) cplx {
   double re, im;
-  __host__ __device__ cplx() : re(0.0), im(0.0) {}
+  cplx() = default;  // trivial, so that shared-memory arrays of it need no initialisation
   __host__ __device__ constexpr cplx(double r, double i = 0.0) : re(r), im(i) {}
 };
 
@@ -43,5 +43,8 @@ template <>
 struct real_of<cplx> {
   using type = double;
 };
+// type of the CSR values a factor of scalar type T assembles from (FP64 real, or complex)
+template <class T>
+using value_of = typename std::conditional<is_cplx<T>::value, cplx, double>::type;
 
 }  // namespace amp

@@ -4,6 +4,8 @@
 
 #include <cstdint>
 
+#include "cplx.cuh"
+
 namespace amp {
 
 struct DevPlan {
@@ -26,10 +28,11 @@ struct DevPlan {
 // LDL^T variant of the panel and update kernels (ldlt.mjs:450-562); all null for Cholesky.
 template <class T>
 struct LdltArgs {
+  using DT = value_of<T>;  // type of the stored pivots: FP64 (real factors, FP32 ones too) or complex
   const double *scal;  // [0] pivotTol (copied per factorization), [1] tau = pivotTol * max |A(i, i)| (device)
   int *counts;         // [0] nNeg, [1] nPerturbed
   T *W;                // L21 D (rows of the solved panel times the pivots): the A operand of the FP64 update
-  double *D;           // the pivots, permuted order
+  DT *D;               // the pivots, permuted order
   __nv_bfloat16 *Whi, *Wlo;  // mixed precision: BF16 split of L21 D (the A operand of the tensor-core update)
 };
 

@@ -61,6 +61,42 @@ __device__ __forceinline__ bool ldlt_pivot(T &d, T tau, unsigned char &flags) {
   return true;
 }
 
+// Complex pivot of the complex-symmetric LDL^T (ldlt.mjs:715-730): a magnitude below tau (or not a number) becomes
+// tau, keeping the pivot's phase (tau itself when d = 0); a non-finite small magnitude fails the factorization.
+// flags: bit 1 perturbed (a complex factor has no inertia).
+__device__ __forceinline__ bool ldlt_pivot(cplx &d, double tau, unsigned char &flags) {
+  flags = 0;
+  const double mag = hypot(d.re, d.im);
+  if (!(mag >= tau)) {
+    if (!isfinite(mag)) return false;
+    if (mag == 0)
+      d.re = tau;
+    else
+      d = cplx(d.re * (tau / mag), d.im * (tau / mag));
+    flags = 2;
+  }
+  return true;
+}
+// Cholesky's pivot test and diagonal (real factors only; a complex factor is always LDL^T)
+template <class T>
+__device__ __forceinline__ bool chol_pivot_ok(T d) { return d > T(0); }
+__device__ __forceinline__ bool chol_pivot_ok(cplx) { return false; }
+template <class T>
+__device__ __forceinline__ T chol_sqrt(T d) { return sqrt(d); }
+__device__ __forceinline__ cplx chol_sqrt(cplx d) { return d; }
+// loads through L2 (data another CTA of the running launch wrote) and read-only loads, for every scalar type
+__device__ __forceinline__ double ldcg_v(const double *p) { return __ldcg(p); }
+__device__ __forceinline__ float ldcg_v(const float *p) { return __ldcg(p); }
+__device__ __forceinline__ cplx ldcg_v(const cplx *p) {
+  const double2 v = __ldcg(reinterpret_cast<const double2 *>(p));
+  return cplx(v.x, v.y);
+}
+__device__ __forceinline__ double ldg_v(const double *p) { return __ldg(p); }
+__device__ __forceinline__ cplx ldg_v(const cplx *p) {
+  const double2 v = __ldg(reinterpret_cast<const double2 *>(p));
+  return cplx(v.x, v.y);
+}
+
 // tau = pivotTol * max |A(i, i)| (1 when that maximum is 0 or not a number, ldlt.mjs:419-424). One CTA.
 __global__ void __launch_bounds__(1024) k_ldlt_tau(const double *__restrict__ values, const int *__restrict__ diagSlot,
                                                     int n, double *scal) {
@@ -112,7 +148,7 @@ __device__ __forceinline__ int2 child_cols(const DevPlan &P, int c, int j0, int 
 
 template <class T>
 __global__ void __launch_bounds__(256) k_assemble(const AsmTask *__restrict__ tasks, DevPlan P,
-                                                  const double *__restrict__ values, T *__restrict__ Lx,
+                                                  const value_of<T> *__restrict__ values, T *__restrict__ Lx,
                                                   T *__restrict__ U, const unsigned long long *status) {
   if (failed(status)) return;
   const AsmTask t = tasks[blockIdx.x];
@@ -141,7 +177,7 @@ __global__ void __launch_bounds__(256) k_assemble(const AsmTask *__restrict__ ta
       for (int u = 0; u < 4; u++) {
         const int pp = p + 32 * u;
         dst[u] = pp < p1 ? P.asmDst[pp] : -1;
-        v[u] = pp < p1 ? (T)__ldg(values + P.asmSrc[pp]) : T(0);
+        v[u] = pp < p1 ? (T)ldg_v(values + P.asmSrc[pp]) : T(0);
       }
       T cur[4];
 #pragma unroll
@@ -187,6 +223,7 @@ __global__ void __launch_bounds__(256) k_assemble(const AsmTask *__restrict__ ta
 // Scale factors of the pivot block's right-looking update (not stored): FP64 as recip_nr, FP32 the hardware estimate.
 __device__ __forceinline__ double fast_recip(double d) { return recip_nr(d); }
 __device__ __forceinline__ float fast_recip(float d) { return __fdividef(1.0f, d); }
+__device__ __forceinline__ cplx fast_recip(cplx d) { return cplx(1.0) / d; }
 
 // ---------------------------------------------------------------------------------------------------------------
 // Group panel: the pivot blocks of a group of up to kGroup 64-column blocks of a front, factored in one dataflow
@@ -213,7 +250,8 @@ __device__ bool potrf_block(T *Lp, int m, int w, int f, int c0, int s, unsigned 
   __shared__ int fail;
   const int tid = threadIdx.x;
   const bool ldlt = ld.scal != nullptr;
-  const T tau = ldlt ? (T)ld.scal[1] : T(0);
+  using RT = typename real_of<T>::type;
+  const RT tau = ldlt ? (RT)ld.scal[1] : RT(0);
   // tile of this thread: row block ti, column block tj (ti >= tj), from tid by the triangular numbering
   int ti = 0;
   while ((ti + 1) * (ti + 2) / 2 <= tid) ti++;
@@ -237,7 +275,7 @@ __device__ bool potrf_block(T *Lp, int m, int w, int f, int c0, int s, unsigned 
         const int k = 4 * kb + kk;
         T d = a[kk][kk];
         unsigned char fl = 0;
-        const bool bad = k < w && (ldlt ? !ldlt_pivot(d, tau, fl) : !(d > T(0)));
+        const bool bad = k < w && (ldlt ? !ldlt_pivot(d, tau, fl) : !chol_pivot_ok(d));
         if (bad && myFail < 0) myFail = k;  // first failing pivot of this diagonal tile
         const T iv = fast_recip(d);           // the update scale only; L is scaled with the exact 1 / d at the end
         pd[k] = d;
@@ -299,7 +337,7 @@ __device__ bool potrf_block(T *Lp, int m, int w, int f, int c0, int s, unsigned 
     for (int c = 0; c < 4; c++) {
       const int j = 4 * tj + c;
       const T d = pd[j];
-      const T lj = ldlt ? d : sqrt(d);
+      const T lj = ldlt ? d : chol_sqrt(d);
       const T inv = T(1) / lj;
 #pragma unroll
       for (int r = 0; r < 4; r++) {
@@ -309,7 +347,7 @@ __device__ bool potrf_block(T *Lp, int m, int w, int f, int c0, int s, unsigned 
     }
   }
   if (ldlt) {
-    if (tid < w) ld.D[f + c0 + tid] = (double)pd[tid];
+    if (tid < w) ld.D[f + c0 + tid] = (typename LdltArgs<T>::DT)pd[tid];
     if (tid == 0) {
       int neg = 0, pert = 0;
       for (int k = 0; k < w; k++) neg += pflag[k] & 1, pert += pflag[k] >> 1;
@@ -336,7 +374,7 @@ __device__ void trsm_strip(T *L, int m, int f, int c0, int w, int r0, int r1, in
   const bool ldlt = ld.scal != nullptr;
   const int tid = threadIdx.x, r = tid & (kPanel - 1), q = tid >> 6;
   if (tid < kPanel) {
-    const T d = tid < w ? (ldlt ? (T)__ldcg(ld.D + f + c0 + tid) : __ldcg(L + (int64_t)(c0 + tid) * m + c0 + tid))
+    const T d = tid < w ? (ldlt ? (T)ldcg_v(ld.D + f + c0 + tid) : ldcg_v(L + (int64_t)(c0 + tid) * m + c0 + tid))
                         : T(1);
     dv[tid] = d;
     invd[tid] = T(1) / d;
@@ -347,7 +385,7 @@ __device__ void trsm_strip(T *L, int m, int f, int c0, int w, int r0, int r1, in
 #pragma unroll
     for (int u = 0; u < 16; u++) {
       const int c = 16 * q + u;
-      v[u] = (r < w && c < r) ? __ldcg(L + (int64_t)(c0 + c) * m + c0 + r) : T(0);
+      v[u] = (r < w && c < r) ? ldcg_v(L + (int64_t)(c0 + c) * m + c0 + r) : T(0);
     }
 #pragma unroll
     for (int u = 0; u < 16; u++) M[r][16 * q + u] = ldlt ? v[u] * dv[16 * q + u] : v[u];
@@ -395,6 +433,7 @@ __device__ void trsm_strip(T *L, int m, int f, int c0, int w, int r0, int r1, in
     if (!active || cc >= w) continue;
     L[(int64_t)(c0 + cc) * m + row] = xv;
     if (ldlt && ld.W) ld.W[lxp + (int64_t)(c0 + cc) * m + row] = wv;
+    if constexpr (!is_cplx<T>::value)
     if (Shi) {
       const int64_t g = sp + (int64_t)(c0 + cc) * ld8 + row;
       const __nv_bfloat16 hi = __float2bfloat16_rn((float)xv);
@@ -494,7 +533,7 @@ __global__ void __launch_bounds__(256) k_group_panel(const GroupItem *__restrict
       if (j != jd && !panel_wait(Df + j, b + 1, status, P.spin)) return;
       for (int e = tid; e < kPanel * kPanel; e += blockDim.x) {  // X_c[k][jj] = L(cb + jj, c0 + k)
         const int k = e >> 6, jj = e & 63;
-        M[k][jj] = (k < w && jj < ncol) ? __ldcg(L + (int64_t)(c0 + k) * m + cb + jj) : T(0);
+        M[k][jj] = (k < w && jj < ncol) ? ldcg_v(L + (int64_t)(c0 + k) * m + cb + jj) : T(0);
       }
       __syncthreads();
       T acc[4][4];
@@ -701,6 +740,67 @@ __global__ void __launch_bounds__(256, 1) k_update(const TileTask *__restrict__ 
   }
 }
 
+
+// Complex-symmetric update tiles (no conjugation): F[i0:i0+128, j0:j0+64] -= W B^T with W = L21 D (the A operand of
+// the LDL^T update) and B = L21, K = the task's pivot columns, on the CUDA cores (four FP64 products per complex
+// product). One CTA per tile: 256 threads as 32 (rows) x 8 (columns), 4 x 8 outputs each; K in chunks of 8 staged
+// in shared memory. Same tiles and masks as k_update.
+__global__ void __launch_bounds__(256) k_update_c(const TileTask *__restrict__ tasks, cplx *__restrict__ Lx,
+                                                  cplx *__restrict__ U, const cplx *__restrict__ W,
+                                                  const unsigned long long *status) {
+  __shared__ int sOk;
+  if (threadIdx.x == 0) sOk = !failed(status);
+  __syncthreads();
+  if (!sOk) return;
+  const TileTask t = tasks[blockIdx.x];
+  constexpr int KC = 8;
+  __shared__ cplx As[KC][kTileM], Bs[KC][kTile];
+  const int tid = threadIdx.x, tr = tid & 31, tc = tid >> 5;
+  const int m = t.m, nc = t.nc, mu = m - nc;
+  const cplx *Ap = W + t.lp, *Bp = Lx + t.lp;
+  cplx acc[4][8];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 8; b++) acc[a][b] = cplx(0.0);
+  for (int k0 = 0; k0 < t.w; k0 += KC) {
+    for (int e = tid; e < KC * kTileM; e += 256) {
+      const int k = e / kTileM, i = e % kTileM, r = t.i0 + i;
+      As[k][i] = (k0 + k < t.w && r < m) ? Ap[(int64_t)(t.c0 + k0 + k) * m + r] : cplx(0.0);
+    }
+    for (int e = tid; e < KC * kTile; e += 256) {
+      const int k = e / kTile, j = e % kTile, r = t.j0 + j;
+      Bs[k][j] = (k0 + k < t.w && r < m) ? Bp[(int64_t)(t.c0 + k0 + k) * m + r] : cplx(0.0);
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int k = 0; k < KC; k++) {
+      cplx av[4], bv[8];
+#pragma unroll
+      for (int a = 0; a < 4; a++) av[a] = As[k][tr + 32 * a];
+#pragma unroll
+      for (int b = 0; b < 8; b++) bv[b] = Bs[k][tc + 8 * b];
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 8; b++) acc[a][b] += av[a] * bv[b];
+    }
+    __syncthreads();
+  }
+  cplx *Lp = Lx + t.lp;
+  cplx *Up = t.up >= 0 ? U + t.up : Lp;
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 8; b++) {
+      const int i = t.i0 + tr + 32 * a, j = t.j0 + tc + 8 * b;
+      if (i < m && j < t.jend && i >= j) {
+        cplx *c = j < nc ? Lp + (int64_t)j * m + i : Up + (int64_t)(j - nc) * mu + (i - nc);
+        *c = *c - acc[a][b];
+      }
+    }
+}
+
 // ---------------------------------------------------------------------------------------------------------------
 // Solves. Vectors: q right-hand sides stored one after another (y[k n + i]) in the permuted order.
 // ---------------------------------------------------------------------------------------------------------------
@@ -734,6 +834,8 @@ cudaError_t init_kernel_attributes() {
   cudaError_t e = cudaFuncSetAttribute(k_group_panel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGroupSmem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_group_panel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGroupSmem / 2);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_group_panel<cplx>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGroupSmem * 2);
   if (e == cudaSuccess) e = init_mixed_attributes();
   if (e == cudaSuccess) e = init_solve_attributes();
   if (e == cudaSuccess) e = init_solve_multi_attributes();
@@ -746,7 +848,7 @@ cudaError_t init_kernel_attributes() {
 }
 
 template <class T>
-void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, const double *values, T *Lx, T *U,
+void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, const value_of<T> *values, T *Lx, T *U,
                      const unsigned long long *status, cudaStream_t st) {
   if (ntasks > 0) k_assemble<T><<<(unsigned)ntasks, 256, 0, st>>>(tasks, P, values, Lx, U, status);
 }
@@ -754,6 +856,8 @@ template void launch_assemble<double>(const AsmTask *, int64_t, const DevPlan &,
                                       const unsigned long long *, cudaStream_t);
 template void launch_assemble<float>(const AsmTask *, int64_t, const DevPlan &, const double *, float *, float *,
                                      const unsigned long long *, cudaStream_t);
+template void launch_assemble<cplx>(const AsmTask *, int64_t, const DevPlan &, const cplx *, cplx *, cplx *,
+                                    const unsigned long long *, cudaStream_t);
 template <class T>
 void launch_group_panel(const GroupItem *items, const StripTask *strips, int nstrips, int *ticket, int *flags,
                         const DevPlan &P, T *Lx, unsigned long long *status, __nv_bfloat16 *Shi, __nv_bfloat16 *Slo,
@@ -768,6 +872,13 @@ template void launch_group_panel<double>(const GroupItem *, const StripTask *, i
 template void launch_group_panel<float>(const GroupItem *, const StripTask *, int, int *, int *, const DevPlan &,
                                         float *, unsigned long long *, __nv_bfloat16 *, __nv_bfloat16 *,
                                         const LdltArgs<float> &, cudaStream_t);
+template void launch_group_panel<cplx>(const GroupItem *, const StripTask *, int, int *, int *, const DevPlan &,
+                                       cplx *, unsigned long long *, __nv_bfloat16 *, __nv_bfloat16 *,
+                                       const LdltArgs<cplx> &, cudaStream_t);
+void launch_update_c(const TileTask *tasks, int64_t ntasks, cplx *Lx, cplx *U, const cplx *W,
+                     const unsigned long long *status, cudaStream_t st) {
+  if (ntasks > 0) k_update_c<<<(unsigned)ntasks, 256, 0, st>>>(tasks, Lx, U, W, status);
+}
 void launch_ldlt_tau(const double *values, const DevPlan &P, double *scal, cudaStream_t st) {
   k_ldlt_tau<<<1, 1024, 0, st>>>(values, P.diagSlot, P.n, scal);
 }

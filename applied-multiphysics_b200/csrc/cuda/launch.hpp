@@ -14,7 +14,7 @@ namespace amp {
 cudaError_t init_kernel_attributes();  // once per device (with that device current), before its first launch
 
 template <class T>
-void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, const double *values, T *Lx, T *U,
+void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, const value_of<T> *values, T *Lx, T *U,
                      const unsigned long long *status, cudaStream_t st);
 // one group of pivot blocks per item: nstrips strip tasks, ticket and flags zeroed before the factorization
 template <class T>
@@ -22,6 +22,9 @@ void launch_group_panel(const GroupItem *items, const StripTask *strips, int nst
                         const DevPlan &P, T *Lx, unsigned long long *status, __nv_bfloat16 *Shi, __nv_bfloat16 *Slo,
                         const LdltArgs<T> &ld, cudaStream_t st);
 void launch_ldlt_tau(const double *values, const DevPlan &P, double *scal, cudaStream_t st);
+// complex-symmetric update tiles (FP64 complex, CUDA cores), one CTA per tile
+void launch_update_c(const TileTask *tasks, int64_t ntasks, cplx *Lx, cplx *U, const cplx *W,
+                     const unsigned long long *status, cudaStream_t st);
 // whole small fronts of one level: tiny (m <= 32, warp per front; sorted by m, the first ntinyMid with m <= 16) and
 // small (m <= 128, CTA per front; maxM = their largest m); returns the kernels launched
 template <class T>
@@ -68,5 +71,18 @@ void launch_from_interleaved(const double *Xil, double *X, int n, int q, cudaStr
 void launch_rows_permute(const double *src, double *dst, const int *perm, int n, int q, bool scatter, cudaStream_t st);
 void launch_residual_multi(int n, const int *rowptr, const int *colidx, const double *val, const double *x,
                            const double *b, double *r, double *norms, int q, const int *rowGroup, cudaStream_t st);
+
+// complex-symmetric LDL^T: packing, permutation, the level sweeps, the residual (csolve.cu)
+void launch_cpack(int64_t nnz, const double *re, const double *im, cplx *out, cudaStream_t st);
+void launch_cunpack(int n, const cplx *x, double *xr, double *xi, cudaStream_t st);
+void launch_ctau(const cplx *values, const DevPlan &P, double *scal, cudaStream_t st);
+void launch_cpermute_in(int n, const double *br, const double *bi, const int *perm, cplx *y, cudaStream_t st);
+void launch_cpermute_out(int n, const cplx *y, const int *perm, double *xr, double *xi, cudaStream_t st);
+void launch_cpermute_vec(int n, const cplx *src, const int *perm, cplx *dst, bool gather, cudaStream_t st);
+void launch_caxpy(int n, cplx *x, const cplx *dx, cudaStream_t st);
+int launch_csolve_permuted(const DevPlan &P, const int *lvlPtr, int nlevels, const cplx *L, const cplx *D, cplx *y,
+                           cudaStream_t st);
+void launch_cresidual(int n, const int *rowptr, const int *colidx, const cplx *val, const cplx *x, const cplx *b,
+                      cplx *r, double *norms, cudaStream_t st);
 
 }  // namespace amp

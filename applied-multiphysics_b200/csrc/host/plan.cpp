@@ -410,4 +410,79 @@ void build_plan(const Symbolic &S, Plan &P) {
                     P.bwdTasks.begin() + 4 * (size_t)P.bwdLvlPtr[L + 1]);
 }
 
+void build_dense_all(const Plan &P, DenseSched &D) {
+  D = DenseSched();
+  D.asmLvlPtr.assign(P.nlevels + 1, 0);
+  D.lvlStepPtr.assign(P.nlevels + 1, 0);
+  D.uLvlPtr.assign(1, 0);
+  auto trap = [](double m, double a, double b) { return (b - a) * m - (a + b - 1) * (b - a) / 2; };
+  for (int L = 0; L < P.nlevels; L++) {
+    int maxSteps = 0;
+    for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
+      const int s = P.lvlSn[q];
+      for (int j0 = 0; j0 < P.snM[s]; j0 += kAsmCols) D.asmTasks.push_back({s, j0});
+      maxSteps = std::max(maxSteps, (P.snNc[s] + kGroup * kPanel - 1) / (kGroup * kPanel));
+    }
+    D.asmLvlPtr[L + 1] = (int64_t)D.asmTasks.size();
+    for (int k = 0; k < maxSteps; k++) {
+      StepRange sr{};
+      sr.item0 = (int64_t)D.groupItems.size();
+      sr.strip0 = (int64_t)D.strips.size();
+      sr.ticket = D.nGroupTickets++;
+      struct Region {
+        int s, lo, hi, kc0, kw;
+      };
+      std::vector<Region> regions;
+      for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
+        const int s = P.lvlSn[q], nc = P.snNc[s], m = P.snM[s], g0 = k * kGroup * kPanel;
+        if (g0 >= nc) continue;
+        const int g1 = std::min(g0 + kGroup * kPanel, nc), nb = (g1 - g0 + kPanel - 1) / kPanel;
+        D.groupItems.push_back({s, g0, g1, D.nGroupFlags});
+        D.nGroupFlags += 2 * nb;
+        for (int c0 = g0; c0 < g1; c0 += kPanel) {
+          const double w = std::min(kPanel, g1 - c0), c1 = c0 + w;
+          sr.panelFlops += w * w * w / 3.0 + (m - c1) * w * w + 2.0 * w * trap(m, c1, g1);
+        }
+        if (g1 < nc) regions.push_back({s, g1, nc, g0, g1 - g0});
+      }
+      const int64_t i0 = sr.item0, i1 = (int64_t)D.groupItems.size();
+      for (int64_t it = i0; it < i1; it++) {  // the diagonal strips of every item take the first tickets
+        const GroupItem &gi = D.groupItems[it];
+        for (int c0 = gi.g0, j = 0; c0 < gi.g1; c0 += kPanel, j++)
+          D.strips.push_back({(int)it, c0, std::min(c0 + kPanel, gi.g1), j});
+      }
+      for (int64_t it = i0; it < i1; it++) {
+        const GroupItem &gi = D.groupItems[it];
+        const int m = P.snM[gi.s];
+        for (int r0 = gi.g1; r0 < m; r0 += kPanel) D.strips.push_back({(int)it, r0, std::min(r0 + kPanel, m), -1});
+      }
+      sr.item1 = i1;
+      sr.strip1 = (int64_t)D.strips.size();
+      auto emit = [&](const Region &g, int lo, int hi, double &flops) {
+        if (lo >= hi) return;
+        const int m = P.snM[g.s], nc = P.snNc[g.s];
+        flops += 2.0 * g.kw * trap(m, lo, hi);
+        for (int j0 = lo; j0 < hi; j0 += kTile)
+          for (int i0 = lo + ((j0 - lo) / kTileM) * kTileM; i0 < m; i0 += kTileM)
+            D.tileTasks.push_back({(long long)P.snLxp[g.s], (long long)P.snUoff[g.s], m, nc, g.kc0, g.kw, i0, j0, hi, 0});
+      };
+      sr.tile0 = (int64_t)D.tileTasks.size();
+      for (const Region &g : regions) emit(g, g.lo, std::min(g.lo + kGroup * kPanel, g.hi), sr.updateFlopsA);
+      sr.tileMid = (int64_t)D.tileTasks.size();
+      for (const Region &g : regions) emit(g, g.lo + kGroup * kPanel, g.hi, sr.updateFlopsB);
+      sr.tile1 = (int64_t)D.tileTasks.size();
+      D.steps.push_back(sr);
+    }
+    D.lvlStepPtr[L + 1] = (int)D.steps.size();
+    for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
+      const int s = P.lvlSn[q], nc = P.snNc[s], m = P.snM[s];
+      if (m <= nc) continue;
+      for (int j0 = nc; j0 < m; j0 += kTile)
+        for (int i0 = nc + ((j0 - nc) / kTileM) * kTileM; i0 < m; i0 += kTileM)
+          D.uTasks.push_back({(long long)P.snLxp[s], (long long)P.snUoff[s], m, nc, 0, nc, i0, j0, m, 0});
+    }
+    D.uLvlPtr.push_back((int64_t)D.uTasks.size());
+  }
+}
+
 }  // namespace amp

@@ -65,6 +65,21 @@ struct StepRange {
 // The update block of every front receives its whole Schur update once, after the group steps of its level:
 // U -= L21 L21^T with K = nc (tiles over the lower triangle of [nc, m)^2).
 
+// The dense path for every front, small ones included (the complex-symmetric factor, which has no whole-front
+// kernels): assembly tasks, group steps and FP64-layout update tiles per level, with the same meaning as the main
+// schedule's fields of Plan.
+struct DenseSched {
+  std::vector<AsmTask> asmTasks;
+  std::vector<int64_t> asmLvlPtr;
+  std::vector<GroupItem> groupItems;
+  std::vector<StripTask> strips;
+  int nGroupFlags = 0, nGroupTickets = 0;
+  std::vector<StepRange> steps;
+  std::vector<int> lvlStepPtr;
+  std::vector<TileTask> tileTasks, uTasks;
+  std::vector<int64_t> uLvlPtr;
+};
+
 struct Plan {
   int n = 0, nsuper = 0, nlevels = 0, maxFront = 0;
   int64_t nnzLStored = 0, arenaDoubles = 0, nnzA = 0, patNnz = 0;
@@ -125,5 +140,7 @@ struct Plan {
 };
 
 void build_plan(const Symbolic &S, Plan &P);
+// the dense schedule of every front (built on demand, by the first complex factor of a plan)
+void build_dense_all(const Plan &P, DenseSched &D);
 
 }  // namespace amp

@@ -43,7 +43,7 @@ typedef enum {
 } amp_status;
 
 typedef enum { AMP_ORDER_AMD = 0, AMP_ORDER_ND = 1, AMP_ORDER_ND3 = 2, AMP_ORDER_GIVEN = 3 } amp_ordering;
-typedef enum { AMP_CHOLESKY = 0, AMP_LDLT = 1 } amp_factor_kind;
+typedef enum { AMP_CHOLESKY = 0, AMP_LDLT = 1, AMP_LDLT_COMPLEX = 2 } amp_factor_kind;
 typedef enum { AMP_FP64 = 0, AMP_MIXED = 1 } amp_precision;
 
 typedef struct amp_plan_s amp_plan;     /* symbolic analysis + device schedule of one pattern (reference: sym) */
@@ -209,6 +209,28 @@ AMP_API int amp_matvec(amp_factor *f, const double *x, int32_t nrhs, double *y);
  * pointers; the call allocates its device buffers and waits for the result). */
 AMP_API int amp_matvec_csr(int32_t n, const int32_t *rowptr, const int32_t *colidx, const double *values,
                            const double *x, int32_t nrhs, double *y, int device);
+
+/* ---- complex-symmetric LDL^T (ldlt.mjs:648-900 ComplexSupernodalLDLT, complexSolveRefined) ----
+ * A = A^T complex (no conjugation) on the plan's pattern, values as two FP64 arrays (re, im) aligned with the CSR
+ * slots, as the reference takes them. FP64 complex factor on the device: every front through the group-panel
+ * kernels (1 x 1 pivots with the reference's static perturbation: a pivot of magnitude below tau = pivotTol *
+ * max_i |A(i, i)| is scaled to magnitude tau; a non-finite one fails), complex update tiles on the CUDA cores and
+ * level-scheduled complex solves. The factor is destroyed with amp_factor_destroy; the real-valued entry points
+ * reject it, and these reject real factors. */
+/* new ComplexSupernodalLDLT(sym) (ldlt.mjs:649-666) */
+AMP_API int amp_cfactor_create(amp_plan *plan, amp_factor **out);
+/* factor(re, im, {pivotTol}) (ldlt.mjs:667-800): result.ok, n_perturbed, fail_column (n_neg is 0: no inertia). */
+AMP_API int amp_cfactor_numeric(amp_factor *f, const double *re, const double *im, int64_t nvalues,
+                                int values_on_device, double pivot_tol, amp_factor_result *result);
+/* solve(br, bi) (ldlt.mjs:802-862) for nrhs right-hand sides one after another; host (0) or device (1) pointers. */
+AMP_API int amp_csolve(amp_factor *f, const double *br, const double *bi, int32_t nrhs, double *xr, double *xi,
+                       int on_device);
+/* solveRefined(pat, re, im, br, bi, {maxSteps, tol}) (complexSolveRefined, ldlt.mjs:870-900) against the values of
+ * the last amp_cfactor_numeric (unperturbed): stats report the worst relative residual and the most steps. */
+AMP_API int amp_csolve_refined(amp_factor *f, const double *br, const double *bi, int32_t nrhs, double *xr,
+                               double *xi, int on_device, const amp_refine_opts *opts, amp_refine_stats *stats);
+/* Lr, Li (the m x nc column-major blocks at Lxp) and Dr, Di copied to host; any pointer may be null. */
+AMP_API int amp_cfactor_download(const amp_factor *f, double *Lr, double *Li, double *Dr, double *Di);
 
 /* ---- on-device assembly of the values (physics/src/common/scalar.ts:96-146 assembleCells; la/sparse.mjs:113-185
  * elementSlots / blockElementSlots; fem/tri.mjs:192-225 restrictMatrix) ---- */
