@@ -46,7 +46,8 @@ class AmpError(Exception):
 
 class _AnalyzeOpts(C.Structure):
     _fields_ = [("ordering", C.c_int), ("relax", C.c_int), ("perm", C.c_void_p), ("x", C.c_void_p),
-                ("y", C.c_void_p), ("z", C.c_void_p), ("leaf", C.c_int), ("device", C.c_int)]
+                ("y", C.c_void_p), ("z", C.c_void_p), ("leaf", C.c_int), ("device", C.c_int),
+                ("group_blocks", C.c_int), ("small_front", C.c_int)]
 
 
 class _PlanInfo(C.Structure):
@@ -86,6 +87,11 @@ class _RefineStats(C.Structure):
     _fields_ = [("rel_residual", C.c_double), ("steps", C.c_int32)]
 
 
+class _TuneResult(C.Structure):
+    _fields_ = [("group_blocks", C.c_int32), ("small_front", C.c_int32), ("cached", C.c_int32),
+                ("candidates", C.c_int32), ("ms_best", C.c_double), ("ms_default", C.c_double)]
+
+
 class _EigenOpts(C.Structure):
     _fields_ = [("n_want", C.c_int32), ("block_size", C.c_int32), ("max_basis", C.c_int32),
                 ("max_restarts", C.c_int32), ("tol", C.c_double), ("seed", C.c_uint32)]
@@ -111,6 +117,8 @@ SIGNATURES = {
     "amp_plan_fingerprint": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32]),
     "amp_plan_check_pattern": (C.c_int, [C.c_void_p, C.c_int32, _i32p, _i32p]),
     "amp_plan_destroy": (None, [C.c_void_p]),
+    "amp_plan_autotune": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int,
+                                    C.POINTER(_TuneResult)]),
     "amp_factor_create": (C.c_int, [C.c_void_p, C.POINTER(_FactorOpts), C.POINTER(C.c_void_p)]),
     "amp_factor_numeric": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_double,
                                      C.POINTER(_FactorResult)]),
@@ -272,6 +280,8 @@ def analyze(pat, opts: dict | None = None, **kw) -> SymbolicAnalysis:
     ao.relax = 1 if o.get("relax", True) else 0
     ao.leaf = int(o.get("leaf", 0) or 0)
     ao.device = int(o.get("device", 0))
+    ao.group_blocks = int(o.get("groupBlocks", 0) or 0)
+    ao.small_front = int(o.get("smallFront", 0) or 0)
     keep = []
     perm = o.get("perm")
     if perm is not None:
@@ -303,6 +313,17 @@ def analyze(pat, opts: dict | None = None, **kw) -> SymbolicAnalysis:
     h = C.c_void_p()
     _check(lib().amp_analyze(n, rp, ci, C.byref(ao), C.byref(h)))
     return SymbolicAnalysis(h.value)
+
+
+def autotune(sym: SymbolicAnalysis, values, kind: int = CHOLESKY, precision: int = FP64) -> dict:
+    """Pick the device schedule (pivot blocks per group panel, whole-front cut-off) of `sym` by timing the
+    factorization of `values` for each candidate (amp_plan_autotune); call before the first factor of `sym`."""
+    v = _f64(values)
+    r = _TuneResult()
+    _check(lib().amp_plan_autotune(sym.handle, v.ctypes.data if v.size else None, v.size, 0, kind, precision,
+                                   C.byref(r)))
+    return {"groupBlocks": r.group_blocks, "smallFront": r.small_front, "cached": bool(r.cached),
+            "candidates": r.candidates, "msBest": r.ms_best, "msDefault": r.ms_default}
 
 
 def checkSymbolic(sym: SymbolicAnalysis, pat) -> None:

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -968,7 +969,10 @@ int amp_analyze(int32_t n, const int32_t *rowptr, const int32_t *colidx, const a
         perm = permBuf.data();
       }
       amp::analyze(A, perm, perm ? 3 : ordering, o.x, o.y, o.z, o.relax != 0, pl->S);
-      amp::build_plan(pl->S, pl->P);
+      amp::Tuning tune;
+      if (o.group_blocks > 0) tune.groupBlocks = o.group_blocks;
+      if (o.small_front > 0) tune.smallCut = o.small_front;
+      amp::build_plan(pl->S, pl->P, tune);
       pl->key = amp::pattern_key(A);
       pl->rowptr.assign(rowptr, rowptr + n + 1);
       pl->colidx.assign(colidx, colidx + (n ? rowptr[n] : 0));
@@ -1042,6 +1046,75 @@ int amp_plan_array(const amp_plan *pl, int field, void *dst, int64_t len, int64_
   if (out_len) *out_len = (int64_t)v->size();
   if (dst) std::memcpy(dst, v->data(), sizeof(int) * std::min<int64_t>(len, v->size()));
   return AMP_OK;
+}
+
+int amp_plan_autotune(amp_plan *pl, const double *values, int64_t nvalues, int values_on_device, int kind,
+                      int precision, amp_tune_result *res) {
+  return guarded([&] {
+    if (!pl || !res) return fail(AMP_INVALID, "null handle");
+    if (pl->uploaded) return fail(AMP_INVALID, "autotune: the plan already has a factor (tune before the first one)");
+    if (nvalues != pl->P.patNnz)
+      return fail(AMP_BAD_LENGTH, "factorNumeric: " + std::to_string(nvalues) + " values for a pattern with " +
+                                      std::to_string(pl->P.patNnz) + " entries");
+    static std::mutex mu;
+    static std::map<std::string, amp::Tuning> cache;
+    const std::string key = pl->key + ":" + std::to_string(kind) + ":" + std::to_string(precision);
+    amp_tune_result r{};
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      auto it = cache.find(key);
+      if (it != cache.end()) {
+        amp::build_plan(pl->S, pl->P, it->second);
+        r.group_blocks = it->second.groupBlocks;
+        r.small_front = it->second.smallCut;
+        r.cached = 1;
+        *res = r;
+        return (int)AMP_OK;
+      }
+    }
+    const int groups[3] = {4, 2, 8}, smalls[2] = {128, 64};  // the default first
+    amp_factor_opts fo{kind, precision};
+    double best = 0.0;
+    amp::Tuning bestT;
+    for (int g : groups)
+      for (int sc : smalls) {
+        amp::Tuning t;
+        t.groupBlocks = g;
+        t.smallCut = sc;
+        amp::build_plan(pl->S, pl->P, t);
+        amp_factor *f = nullptr;
+        int rc = amp_factor_create(pl, &fo, &f);
+        double ms = 0.0;
+        if (rc == AMP_OK) {
+          amp_factor_result fr{};
+          for (int rep = 0; rep < 3 && rc == AMP_OK; rep++) {  // the first run captures the graph; time the third
+            rc = amp_factor_numeric(f, values, nvalues, values_on_device, 1e-13, &fr);
+            ms = fr.ms;
+          }
+          amp_factor_destroy(f);
+        }
+        pl->mem.release();  // the next candidate uploads its own schedule
+        pl->uploaded = false;
+        pl->cxUploaded = false;
+        if (rc != AMP_OK) return rc;
+        r.candidates++;
+        if (g == 4 && sc == 128) r.ms_default = ms;
+        if (r.candidates == 1 || ms < best) {
+          best = ms;
+          bestT = t;
+        }
+      }
+    amp::build_plan(pl->S, pl->P, bestT);
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      cache[key] = bestT;
+    }
+    r.group_blocks = bestT.groupBlocks;
+    r.small_front = bestT.smallCut;
+    r.ms_best = best;
+    *res = r;
+    return (int)AMP_OK;
+  });
 }
 
 int amp_plan_fingerprint(const amp_plan *pl, char *buf, int32_t buflen) {

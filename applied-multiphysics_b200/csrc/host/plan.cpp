@@ -76,8 +76,12 @@ class ArenaPlanner {
 
 }  // namespace
 
-void build_plan(const Symbolic &S, Plan &P) {
+void build_plan(const Symbolic &S, Plan &P, const Tuning &tune) {
   P = Plan();
+  if (tune.groupBlocks < 1 || tune.groupBlocks > 16 || tune.smallCut < kTinyFront || tune.smallCut > kSmallFront)
+    throw std::invalid_argument("schedule parameters out of range (group blocks 1..16, small fronts 32..128)");
+  P.tune = tune;
+  const int GW = tune.groupBlocks * kPanel;  // group width
   const int n = S.n, ns = S.nsuper;
   P.n = n;
   P.nsuper = ns;
@@ -196,7 +200,7 @@ void build_plan(const Symbolic &S, Plan &P) {
   P.tinyPtr.assign(1, 0);
   P.tinyMid.clear();
   P.smallPtr.assign(1, 0);
-  auto isSmall = [&](int s) { return P.snM[s] <= kSmallFront; };
+  auto isSmall = [&](int s) { return P.snM[s] <= tune.smallCut; };
   for (int L = 0; L < P.nlevels; L++) {
     // small fronts: the whole front in one kernel; the rest go through the steps below
     int maxM = 0;
@@ -234,7 +238,7 @@ void build_plan(const Symbolic &S, Plan &P) {
       int s = P.lvlSn[q];
       if (isSmall(s)) continue;
       for (int j0 = 0; j0 < P.snM[s]; j0 += kAsmCols) P.asmTasks.push_back({s, j0});
-      maxSteps = std::max(maxSteps, (P.snNc[s] + kGroup * kPanel - 1) / (kGroup * kPanel));
+      maxSteps = std::max(maxSteps, (P.snNc[s] + GW - 1) / (GW));
       // bytes: value + lowerI + lowerSrc per A entry (16); read U + read/write the parent entry per child entry (24)
       double b = 16.0 * (S.lowerP[P.snF[s] + P.snNc[s]] - S.lowerP[P.snF[s]]);
       for (int k = P.chPtr[s]; k < P.chPtr[s + 1]; k++) {
@@ -261,9 +265,9 @@ void build_plan(const Symbolic &S, Plan &P) {
       auto trap = [](double m, double a, double b) { return (b - a) * m - (a + b - 1) * (b - a) / 2; };
       for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
         int s = P.lvlSn[q];
-        const int nc = P.snNc[s], m = P.snM[s], g0 = k * kGroup * kPanel;
+        const int nc = P.snNc[s], m = P.snM[s], g0 = k * GW;
         if (g0 >= nc || isSmall(s)) continue;
-        const int g1 = std::min(g0 + kGroup * kPanel, nc), nb = (g1 - g0 + kPanel - 1) / kPanel;
+        const int g1 = std::min(g0 + GW, nc), nb = (g1 - g0 + kPanel - 1) / kPanel;
         P.groupItems.push_back({s, g0, g1, P.nGroupFlags});
         P.nGroupFlags += 2 * nb;
         for (int c0 = g0; c0 < g1; c0 += kPanel) {
@@ -296,10 +300,10 @@ void build_plan(const Symbolic &S, Plan &P) {
       };
       sr.tile0 = (int64_t)P.tileTasks.size();
       sr.mix0 = (int64_t)P.mixTiles.size();
-      for (const Region &g : regions) emit(g, g.lo, std::min(g.lo + kGroup * kPanel, g.hi), sr.updateFlopsA);
+      for (const Region &g : regions) emit(g, g.lo, std::min(g.lo + GW, g.hi), sr.updateFlopsA);
       sr.tileMid = (int64_t)P.tileTasks.size();
       sr.mixMid = (int64_t)P.mixTiles.size();
-      for (const Region &g : regions) emit(g, g.lo + kGroup * kPanel, g.hi, sr.updateFlopsB);
+      for (const Region &g : regions) emit(g, g.lo + GW, g.hi, sr.updateFlopsB);
       sr.tile1 = (int64_t)P.tileTasks.size();
       sr.mix1 = (int64_t)P.mixTiles.size();
       P.steps.push_back(sr);
@@ -412,6 +416,7 @@ void build_plan(const Symbolic &S, Plan &P) {
 
 void build_dense_all(const Plan &P, DenseSched &D) {
   D = DenseSched();
+  const int GW = P.tune.groupBlocks * kPanel;  // group width
   D.asmLvlPtr.assign(P.nlevels + 1, 0);
   D.lvlStepPtr.assign(P.nlevels + 1, 0);
   D.uLvlPtr.assign(1, 0);
@@ -421,7 +426,7 @@ void build_dense_all(const Plan &P, DenseSched &D) {
     for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
       const int s = P.lvlSn[q];
       for (int j0 = 0; j0 < P.snM[s]; j0 += kAsmCols) D.asmTasks.push_back({s, j0});
-      maxSteps = std::max(maxSteps, (P.snNc[s] + kGroup * kPanel - 1) / (kGroup * kPanel));
+      maxSteps = std::max(maxSteps, (P.snNc[s] + GW - 1) / (GW));
     }
     D.asmLvlPtr[L + 1] = (int64_t)D.asmTasks.size();
     for (int k = 0; k < maxSteps; k++) {
@@ -434,9 +439,9 @@ void build_dense_all(const Plan &P, DenseSched &D) {
       };
       std::vector<Region> regions;
       for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
-        const int s = P.lvlSn[q], nc = P.snNc[s], m = P.snM[s], g0 = k * kGroup * kPanel;
+        const int s = P.lvlSn[q], nc = P.snNc[s], m = P.snM[s], g0 = k * GW;
         if (g0 >= nc) continue;
-        const int g1 = std::min(g0 + kGroup * kPanel, nc), nb = (g1 - g0 + kPanel - 1) / kPanel;
+        const int g1 = std::min(g0 + GW, nc), nb = (g1 - g0 + kPanel - 1) / kPanel;
         D.groupItems.push_back({s, g0, g1, D.nGroupFlags});
         D.nGroupFlags += 2 * nb;
         for (int c0 = g0; c0 < g1; c0 += kPanel) {
@@ -467,9 +472,9 @@ void build_dense_all(const Plan &P, DenseSched &D) {
             D.tileTasks.push_back({(long long)P.snLxp[g.s], (long long)P.snUoff[g.s], m, nc, g.kc0, g.kw, i0, j0, hi, 0});
       };
       sr.tile0 = (int64_t)D.tileTasks.size();
-      for (const Region &g : regions) emit(g, g.lo, std::min(g.lo + kGroup * kPanel, g.hi), sr.updateFlopsA);
+      for (const Region &g : regions) emit(g, g.lo, std::min(g.lo + GW, g.hi), sr.updateFlopsA);
       sr.tileMid = (int64_t)D.tileTasks.size();
-      for (const Region &g : regions) emit(g, g.lo + kGroup * kPanel, g.hi, sr.updateFlopsB);
+      for (const Region &g : regions) emit(g, g.lo + GW, g.hi, sr.updateFlopsB);
       sr.tile1 = (int64_t)D.tileTasks.size();
       D.steps.push_back(sr);
     }

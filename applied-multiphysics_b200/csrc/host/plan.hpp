@@ -80,7 +80,16 @@ struct DenseSched {
   std::vector<int64_t> uLvlPtr;
 };
 
+// Tunable schedule parameters (the autotuner's search space, amp_plan_autotune): pivot blocks per group (the width
+// of a group panel and the K of the group's update: 64 x groupBlocks columns) and the largest front factored whole
+// by one CTA (the small-front kernel; larger fronts take the group path).
+struct Tuning {
+  int groupBlocks = kGroup;
+  int smallCut = kSmallFront;
+};
+
 struct Plan {
+  Tuning tune;
   int n = 0, nsuper = 0, nlevels = 0, maxFront = 0;
   int64_t nnzLStored = 0, arenaDoubles = 0, nnzA = 0, patNnz = 0;
   // per supernode
@@ -139,7 +148,7 @@ struct Plan {
   double flops = 0;
 };
 
-void build_plan(const Symbolic &S, Plan &P);
+void build_plan(const Symbolic &S, Plan &P, const Tuning &tune = Tuning());
 // the dense schedule of every front (built on demand, by the first complex factor of a plan)
 void build_dense_all(const Plan &P, DenseSched &D);
 

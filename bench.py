@@ -321,6 +321,7 @@ def main():
     ap.add_argument("--workload", default="elastic3d", choices=sorted(SYSTEMS))
     ap.add_argument("--size", type=int, default=0, help="hexes per side, or problems of the batch (0 = benchmark size)")
     ap.add_argument("--ref-budget", type=float, default=240.0, help="wall seconds of the reference arm's steps")
+    ap.add_argument("--no-autotune", action="store_true", help="the default schedule instead of the autotuned one")
     args = ap.parse_args()
     sysinfo = SYSTEMS[args.workload]
     args.size = args.size or sysinfo["size"]
@@ -361,8 +362,17 @@ def main():
     b_d = torch.from_numpy(np.ascontiguousarray(w.rhs).reshape(-1)).to(dev)
     x_d = torch.empty_like(b_d)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+    tuning = {}
     for prec in precisions:
-        num = amp.NumericFactor(sym, amp.LDLT if args.ldlt else amp.CHOLESKY, amp.FP64 if prec == "fp64" else amp.MIXED)
+        kind, precision = amp.LDLT if args.ldlt else amp.CHOLESKY, amp.FP64 if prec == "fp64" else amp.MIXED
+        psym = sym
+        if not args.no_autotune:  # the schedule per precision, chosen by timing candidates (per pattern, not timed)
+            if isinstance(w, _Batch):
+                psym = amp.analyze(w.pat, perm=w.perm, device=local)
+            else:
+                psym = amp.analyze(w.pat, ordering="nd3", x=w.x, y=w.y, z=w.z, device=local)
+            tuning[prec] = amp.autotune(psym, w.values, kind, precision)
+        num = amp.NumericFactor(psym, kind, precision)
         if isinstance(w, _Batch):
             num.set_row_groups(w.offs)  # the residual is measured per matrix
 
@@ -435,7 +445,7 @@ def main():
                          "converged": bool(ok and relres <= RESIDUAL),
                          "refinement": "gmres-ir (iterations)" if gmres else "ir (steps)",
                          "prof": prof, "e2e_ms": e2e_ms, "factor_ms": num.ms, "x": xsol}
-        del num
+        del num, psym
     # units processed by all ranks: a replica each, or each rank's share of the batch
     total_work = work
     if world > 1:
@@ -479,7 +489,10 @@ def main():
                    "l2": "flushed between timed steps (256 MB write)",
                    "parallelism": ("batch split over ranks" if isinstance(w, _Batch) else "replicas")
                    if world > 1 else "1 gpu",
-                   "symbolic_ms": symbolic_ms},
+                   "symbolic_ms": symbolic_ms,
+                   "schedule": {p: {"group_blocks": t["groupBlocks"], "small_front": t["smallFront"],
+                                    "factor_ms_tuned": t["msBest"], "factor_ms_default": t["msDefault"]}
+                                for p, t in tuning.items()} or "default (group 4 x 64 columns, whole fronts <= 128)"},
         "relres": R["relres"], "ir_steps": R["ir_steps"], "factor_ms": R["factor_ms"],
         "e2e": {"value": total_work / (R["e2e_ms"] * 1e-3) / 1e12, "unit": UNIT,
                 "h2d_bytes_per_step": int(8 * w.pat.nnz + 8 * n * nq), "d2h_bytes_per_step": int(8 * n * nq),

@@ -58,6 +58,8 @@ typedef struct {
   const double *x, *y, *z;
   int leaf;              /* ND leaf size; 0 = the reference default (48 for 2D, 2000 for 3D) */
   int device;            /* CUDA device ordinal */
+  int group_blocks;      /* schedule: 64-column pivot blocks per group panel (1..16; 0 = the default, 4) */
+  int small_front;       /* schedule: largest front factored whole by one CTA (32..128; 0 = the default, 128) */
 } amp_analyze_opts;
 
 /* Scalars of a symbolic analysis (SymbolicAnalysis fields, types.d.mts:13-20). */
@@ -142,6 +144,20 @@ AMP_API int amp_analyze(int32_t n, const int32_t *rowptr, const int32_t *colidx,
 AMP_API int amp_plan_get_info(const amp_plan *plan, amp_plan_info *info);
 /* Copies one SymbolicAnalysis array (amp_field) into dst (capacity len elements); *out_len = its length. */
 AMP_API int amp_plan_array(const amp_plan *plan, int field, void *dst, int64_t len, int64_t *out_len);
+/* Autotuner of the device schedule (no reference counterpart: the reference's fixed crossovers, e.g. WASM_MIN_FRONT
+ * and QCAP in la/wasm/*.mjs, are constants). Times the numeric factorization of `values` (kind, precision as in
+ * amp_factor_opts) on this plan's device for each candidate schedule -- pivot blocks per group panel {2, 4, 8} x
+ * largest whole-front CTA front {64, 128} -- and keeps the fastest; ties go to the earlier candidate. The choice is
+ * cached per (pattern fingerprint, kind, precision) for the process, so another plan of the same pattern takes it
+ * without timing (cached = 1). Call before the plan's first amp_factor_create (AMP_INVALID otherwise). */
+typedef struct {
+  int32_t group_blocks, small_front;  /* the chosen schedule */
+  int32_t cached;                     /* 1 when taken from the cache, without timing */
+  int32_t candidates;                 /* schedules timed */
+  double ms_best, ms_default;         /* factorization time of the choice and of the default schedule */
+} amp_tune_result;
+AMP_API int amp_plan_autotune(amp_plan *plan, const double *values, int64_t nvalues, int values_on_device, int kind,
+                              int precision, amp_tune_result *result);
 /* sym.patternKey */
 AMP_API int amp_plan_fingerprint(const amp_plan *plan, char *buf, int32_t buflen);
 /* checkSymbolic(sym, pat) (sparse.mjs:928-930): AMP_PATTERN_MISMATCH when pat is not the analysed pattern. */

@@ -200,3 +200,22 @@ def test_tiny_front_classes(plan):
         k = tm[L] - tp[L]
         assert 0 <= k <= len(sl)
         assert np.all(ms[:k] <= TINY_MID) and np.all(ms[k:] > TINY_MID)
+
+
+# ---- schedule parameters (the autotuner's search space) -------------------------------------------------------------
+@pytest.mark.parametrize("gb,sf", [(1, 32), (2, 64), (8, 128), (16, 96)])
+def test_schedule_parameters_leave_the_symbolic_analysis_unchanged(gb, sf):
+    w = wl.elastic3d(8)
+    base = amp.analyze(w.pat, ordering="nd3", x=w.x, y=w.y, z=w.z)
+    tuned = amp.analyze(w.pat, ordering="nd3", x=w.x, y=w.y, z=w.z, groupBlocks=gb, smallFront=sf)
+    for f in ("perm", "parent", "superStart", "Sp", "Si", "Lxp", "fwdTasks", "bwdTasks"):
+        assert np.array_equal(getattr(base, f), getattr(tuned, f)), f
+    # fronts factored whole by one warp (m <= 32) do not depend on the whole-front CTA cut-off either
+    assert np.array_equal(base.tinyFronts, tuned.tinyFronts)
+
+
+@pytest.mark.parametrize("gb,sf", [(17, 128), (4, 129), (4, 20)])
+def test_schedule_parameters_out_of_range_are_rejected(gb, sf):
+    w = wl.poisson2d(8)
+    with pytest.raises(amp.AmpError, match="schedule parameters out of range"):
+        amp.analyze(w.pat, groupBlocks=gb, smallFront=sf)
