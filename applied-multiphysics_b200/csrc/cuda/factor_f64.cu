@@ -17,6 +17,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cfloat>
+#include <type_traits>
 #include <cstdint>
 
 #include "devplan.cuh"
@@ -77,6 +79,10 @@ __device__ __forceinline__ bool ldlt_pivot(cplx &d, double tau, unsigned char &f
   }
   return true;
 }
+// magnitude of a pivot
+__device__ __forceinline__ double pivot_mag(double d) { return fabs(d); }
+__device__ __forceinline__ double pivot_mag(float d) { return fabs((double)d); }
+__device__ __forceinline__ double pivot_mag(cplx d) { return hypot(d.re, d.im); }
 // Cholesky's pivot test and diagonal (real factors only; a complex factor is always LDL^T)
 template <class T>
 __device__ __forceinline__ bool chol_pivot_ok(T d) { return d > T(0); }
@@ -241,16 +247,16 @@ __device__ __forceinline__ cplx fast_recip(cplx d) { return cplx(1.0) / d; }
 // scaled: Cholesky L = a / sqrt(d) with sqrt(d) on the diagonal, LDL^T L = a / d with a unit diagonal (D to ld.D).
 // Returns false (status set for the first failing column f + c0 + k) when a pivot failed; the block is then not
 // written back.
-template <class T>
-__device__ bool potrf_block(T *Lp, int m, int w, int f, int c0, int s, unsigned long long *status,
-                            const LdltArgs<T> &ld) {
-  __shared__ T col[2][4][kPanel];  // per 4-column block (double-buffered): the block's unscaled columns, by row
-  __shared__ T pd[kPanel], piv[2][4];
+template <class T, class TC>
+__device__ int potrf_core(T *Lp, int m, int w, int f, int c0, int s, unsigned long long *status,
+                          const LdltArgs<T> &ld, double promoteBelow) {
+  __shared__ TC col[2][4][kPanel];  // per 4-column block (double-buffered): the block's unscaled columns, by row
+  __shared__ TC pd[kPanel], piv[2][4];
   __shared__ unsigned char pflag[kPanel];
-  __shared__ int fail;
+  __shared__ int fail, promote;
   const int tid = threadIdx.x;
   const bool ldlt = ld.scal != nullptr;
-  using RT = typename real_of<T>::type;
+  using RT = typename real_of<TC>::type;
   const RT tau = ldlt ? (RT)ld.scal[1] : RT(0);
   // tile of this thread: row block ti, column block tj (ti >= tj), from tid by the triangular numbering
   int ti = 0;
@@ -258,26 +264,29 @@ __device__ bool potrf_block(T *Lp, int m, int w, int f, int c0, int s, unsigned 
   const int tj = tid - ti * (ti + 1) / 2;
   const bool owner = tid < 136;
   int myFail = -1;  // diagonal tiles only
-  T a[4][4];
+  TC a[4][4];
 #pragma unroll
   for (int r = 0; r < 4; r++)
 #pragma unroll
     for (int c = 0; c < 4; c++) {
       const int i = 4 * ti + r, j = 4 * tj + c;
-      a[r][c] = !owner || i < j ? T(0) : (i < w ? Lp[(int64_t)j * m + i] : (i == j ? T(1) : T(0)));
+      a[r][c] = !owner || i < j ? TC(0) : (i < w ? (TC)Lp[(int64_t)j * m + i] : (i == j ? TC(1) : TC(0)));
     }
-  if (tid == 0) fail = kPanel;  // none
+  if (tid == 0) {
+    fail = kPanel;  // none
+    promote = 0;
+  }
   for (int kb = 0; kb < kPanel / 4; kb++) {
     const int buf = kb & 1;
     if (owner && ti == kb && tj == kb) {
 #pragma unroll
       for (int kk = 0; kk < 4; kk++) {
         const int k = 4 * kb + kk;
-        T d = a[kk][kk];
+        TC d = a[kk][kk];
         unsigned char fl = 0;
         const bool bad = k < w && (ldlt ? !ldlt_pivot(d, tau, fl) : !chol_pivot_ok(d));
         if (bad && myFail < 0) myFail = k;  // first failing pivot of this diagonal tile
-        const T iv = fast_recip(d);           // the update scale only; L is scaled with the exact 1 / d at the end
+        const TC iv = fast_recip(d);          // the update scale only; L is scaled with the exact 1 / d at the end
         pd[k] = d;
         pflag[k] = fl;
         piv[buf][kk] = iv;
@@ -295,10 +304,10 @@ __device__ bool potrf_block(T *Lp, int m, int w, int f, int c0, int s, unsigned 
     if (owner && tj == kb && ti > kb) {
 #pragma unroll
       for (int kk = 0; kk < 4; kk++) {
-        const T iv = piv[buf][kk];
+        const TC iv = piv[buf][kk];
 #pragma unroll
         for (int c = kk + 1; c < 4; c++) {
-          const T cj = col[buf][kk][4 * kb + c] * iv;
+          const TC cj = col[buf][kk][4 * kb + c] * iv;
 #pragma unroll
           for (int r = 0; r < 4; r++) a[r][c] -= a[r][kk] * cj;
         }
@@ -312,8 +321,8 @@ __device__ bool potrf_block(T *Lp, int m, int w, int f, int c0, int s, unsigned 
     if (owner && tj > kb) {
 #pragma unroll
       for (int kk = 0; kk < 4; kk++) {
-        const T iv = piv[buf][kk];
-        T ci[4], cj[4];
+        const TC iv = piv[buf][kk];
+        TC ci[4], cj[4];
 #pragma unroll
         for (int r = 0; r < 4; r++) ci[r] = col[buf][kk][4 * ti + r];
 #pragma unroll
@@ -327,22 +336,24 @@ __device__ bool potrf_block(T *Lp, int m, int w, int f, int c0, int s, unsigned 
     }
   }
   if (myFail >= 0) atomicMin(&fail, myFail);
+  if (promoteBelow > 0.0 && tid < w && !(pivot_mag(pd[tid]) >= promoteBelow)) promote = 1;
   __syncthreads();
+  if (promote) return 2;  // the caller redoes the block in higher precision (nothing written)
   if (fail < kPanel) {
     if (tid == 0) atomicMin(status, status_word(f + c0 + fail, ldlt ? 2 : 1, s));
-    return false;
+    return 1;
   }
   if (owner) {
 #pragma unroll
     for (int c = 0; c < 4; c++) {
       const int j = 4 * tj + c;
-      const T d = pd[j];
-      const T lj = ldlt ? d : chol_sqrt(d);
-      const T inv = T(1) / lj;
+      const TC d = pd[j];
+      const TC lj = ldlt ? d : chol_sqrt(d);
+      const TC inv = TC(1) / lj;
 #pragma unroll
       for (int r = 0; r < 4; r++) {
         const int i = 4 * ti + r;
-        if (i >= j && i < w && j < w) Lp[(int64_t)j * m + i] = i == j ? (ldlt ? T(1) : lj) : a[r][c] * inv;
+        if (i >= j && i < w && j < w) Lp[(int64_t)j * m + i] = (T)(i == j ? (ldlt ? TC(1) : lj) : a[r][c] * inv);
       }
     }
   }
@@ -355,7 +366,25 @@ __device__ bool potrf_block(T *Lp, int m, int w, int f, int c0, int s, unsigned 
       atomicAdd(ld.counts + 1, pert);
     }
   }
-  return true;
+  return 0;
+}
+
+// POTRF / LDL^T of a pivot block (potrf_core in the factor's precision). An FP32 LDL^T block with a pivot of
+// magnitude below FLT_EPSILON x max_i |A(i, i)| (a pivot with no correct FP32 digit left) is factored again from its
+// stored entries in FP64 arithmetic (stored FP32): the small-pivot blocks of the mixed-precision indefinite factor get
+// FP64 pivots. Returns false when a pivot failed (status set).
+template <class T>
+__device__ bool potrf_block(T *Lp, int m, int w, int f, int c0, int s, unsigned long long *status,
+                            const LdltArgs<T> &ld) {
+  if constexpr (std::is_same<T, float>::value) {
+    if (ld.scal != nullptr) {
+      const double amax = ld.scal[0] > 0.0 ? ld.scal[1] / ld.scal[0] : 0.0;
+      const int r = potrf_core<float, float>(Lp, m, w, f, c0, s, status, ld, amax * (double)FLT_EPSILON);
+      if (r != 2) return r == 0;
+      return potrf_core<float, double>(Lp, m, w, f, c0, s, status, ld, -1.0) == 0;
+    }
+  }
+  return potrf_core<T, T>(Lp, m, w, f, c0, s, status, ld, -1.0) == 0;
 }
 
 // TRSM of up to 64 rows [r0, r1) of a front (L: its column-major block, ld m) against its factored pivot block
