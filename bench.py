@@ -310,6 +310,26 @@ TRAFFIC = {
 }
 
 
+def one_factor(args, w, amp, local):
+    if isinstance(w, _Batch):
+        sym = amp.analyze(w.pat, perm=w.perm, device=local)
+    else:
+        sym = amp.analyze(w.pat, ordering="nd3", x=w.x, y=w.y, z=w.z, device=local)
+    prec = amp.FP64 if args.precision == "fp64" else amp.MIXED
+    num = amp.NumericFactor(sym, amp.LDLT if args.ldlt else amp.CHOLESKY, prec)
+    num.profile(True)  # direct launches, each bracketed by events, in stream order
+    ok = num.factor(w.values)
+    k, ms, fl = num.profile_launches()
+    out = {"workload": args.desc, "ok": ok}
+    for name, kind in (("group_panel", 1), ("update", 2), ("assemble", 0)):
+        idx = np.where(k == kind)[0]
+        if idx.size:
+            j = int(np.argmax(ms[idx]))
+            out[name] = {"launches": int(idx.size), "longest_index": j, "longest_ms": float(ms[idx][j]),
+                         "longest_tflops": float(fl[idx][j] / ms[idx][j] / 1e9), "total_ms": float(ms[idx].sum())}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -322,6 +342,10 @@ def main():
     ap.add_argument("--size", type=int, default=0, help="hexes per side, or problems of the batch (0 = benchmark size)")
     ap.add_argument("--ref-budget", type=float, default=240.0, help="wall seconds of the reference arm's steps")
     ap.add_argument("--no-autotune", action="store_true", help="the default schedule instead of the autotuned one")
+    ap.add_argument("--one-factor", action="store_true",
+                    help="profiling case: one factorization of the workload (first precision of --precision) with "
+                         "direct launches in stream order; prints the per-class launch index of the longest group "
+                         "panel and update (the -s of an ncu capture)")
     args = ap.parse_args()
     sysinfo = SYSTEMS[args.workload]
     args.size = args.size or sysinfo["size"]
@@ -344,6 +368,9 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     w = make_system(args.workload, args.size, rank, world)
+    if args.one_factor:
+        one_factor(args, w, amp, local)
+        return
     n = w.n
     nq = w.rhs.shape[0]
     t0 = time.perf_counter()
