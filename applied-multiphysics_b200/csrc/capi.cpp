@@ -96,6 +96,7 @@ void set_last_error(const std::string &msg) { g_err = msg; }
 namespace {
 // elements of the diagonal-block inverses (none for an empty pattern, whose plan has no per-block arrays)
 // chain-matrix slots: nb - 1 per supernode with nb diagonal blocks, 64 x 64 each
+constexpr int kSlices = 4;  // vector slices of the multi-vector sweeps: multi_max_vectors() / 16
 size_t chain_elems(const amp::Plan &P) { return (size_t)std::max(0, P.nflags - P.nsuper) * 64 * 64; }
 
 int64_t inv_elems(const amp::Plan &P) { return P.invOff.empty() ? 0 : P.invOff[P.nflags]; }
@@ -298,6 +299,7 @@ void upload_plan(amp_plan *pl) {
   d.Sp = m.upload(P.Sp);
   d.Si = m.upload(P.Si);
   d.blkOff = m.upload(P.blkOff);
+  d.rowBlk = m.upload(P.rowBlk);
   d.invOff = m.upload(P.invOff);
   d.diagSlot = m.upload(P.diagSlot);
   d.solveSmall = m.upload(P.solveSmall);
@@ -599,7 +601,8 @@ void device_solve_multi_permuted(amp_factor *f, int q) {
   const double flops = 2.0 * (double)P.nnzLStored * q;
   cudaStream_t st = f->stream;
   ck(cudaMemsetAsync(f->dTickets, 0, sizeof(int) * 2, st), "memset tickets");
-  ck(cudaMemsetAsync(f->dDone, 0, sizeof(int) * std::max(1, P.nsuper), st), "memset done");
+  const int nfl = std::max(1, P.nflags);
+  ck(cudaMemsetAsync(f->dDone, 0, sizeof(int) * kSlices * std::max(1, P.nsuper), st), "memset done");
   ck(cudaMemsetAsync(f->dSolveStatus, 0xff, sizeof(unsigned long long), st), "memset status");
   const int efwd = 2 * (++f->solveEpoch) - 1, ebwd = 2 * f->solveEpoch;
   const int nf = P.fwdLvlPtr[P.nlevels], nb = (int)(P.bwdAll.size() / 4);
@@ -607,18 +610,18 @@ void device_solve_multi_permuted(amp_factor *f, int q) {
   timed(f, K_FORWARD, flops, lbytes, [&] {
     if (f->dL32)
       amp::launch_fwd_multi<float>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->dL32, f->dInv32, f->dY, f->dV, f->dT,
-                                   f->dFlags, efwd, f->dDone, q, f->dSolveStatus, st);
+                                   f->dFlags, nfl, efwd, f->dDone, q, f->dSolveStatus, st);
     else
       amp::launch_fwd_multi<double>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->dLx, f->dInv, f->dY, f->dV, f->dT,
-                                    f->dFlags, efwd, f->dDone, q, f->dSolveStatus, st);
+                                    f->dFlags, nfl, efwd, f->dDone, q, f->dSolveStatus, st);
   });
   timed(f, K_BACKWARD, flops, lbytes, [&] {
     if (f->dL32)
       amp::launch_bwd_multi<float>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dL32, f->dInv32, Dp, f->dY,
-                                   f->dFlags, ebwd, q, f->dSolveStatus, st);
+                                   f->dFlags, nfl, ebwd, q, f->dSolveStatus, st);
     else
       amp::launch_bwd_multi<double>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dLx, f->dInv, Dp, f->dY, f->dFlags,
-                                    ebwd, q, f->dSolveStatus, st);
+                                    nfl, ebwd, q, f->dSolveStatus, st);
   });
 }
 
@@ -1191,8 +1194,8 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
       f->dD = f->mem.alloc<double>((size_t)P.n);
       f->dValues = f->mem.alloc<double>((size_t)P.patNnz);
       f->dStatus = f->mem.alloc<unsigned long long>(1);
-      f->dFlags = f->mem.alloc<int>((size_t)P.nflags);
-      ck(cudaMemset(f->dFlags, 0, sizeof(int) * std::max(1, P.nflags)), "memset flags");
+      f->dFlags = f->mem.alloc<int>((size_t)kSlices * std::max(1, P.nflags));  // one set per vector slice
+      ck(cudaMemset(f->dFlags, 0, sizeof(int) * kSlices * std::max(1, P.nflags)), "memset flags");
       {  // two tagged words per value of a 64-row block, one slot per pair of consecutive diagonal blocks
         const size_t hw = std::max<size_t>(1, (size_t)std::max(0, P.nflags - P.nsuper) * 128);
         f->dHand = f->mem.alloc<unsigned long long>(hw);
@@ -1200,7 +1203,7 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
       }
       f->dTickets = f->mem.alloc<int>(2);
       f->dGroupFlags = f->mem.alloc<int>((size_t)std::max(1, P.nGroupFlags + P.nGroupTickets));
-      f->dDone = f->mem.alloc<int>((size_t)std::max(1, P.nsuper));
+      f->dDone = f->mem.alloc<int>((size_t)kSlices * std::max(1, P.nsuper));
       f->dSolveStatus = f->mem.alloc<unsigned long long>(1);
       init_device_once(pl->device);
     } catch (...) {

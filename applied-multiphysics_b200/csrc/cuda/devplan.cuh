@@ -19,6 +19,7 @@ struct DevPlan {
   const int *lvlSn;
   const int *perm, *Sp, *Si;
   const int *blkOff;       // first 64-column diagonal block of supernode s (nsuper + 1)
+  const int *rowBlk;       // 64-column diagonal block holding column i (n; the flag a backward reader of row i waits for)
   const int64_t *invOff;   // offset of the inverse of each diagonal block (w x w, column-major)
   const int *diagSlot;     // CSR slot of A(i, i), original row i (the LDL^T pivot scale)
   const int *solveSmall;   // supernodes solved whole by one warp (solve tasks of kind 2 index this list)

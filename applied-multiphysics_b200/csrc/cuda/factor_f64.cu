@@ -237,8 +237,9 @@ __device__ __forceinline__ cplx fast_recip(cplx d) { return cplx(1.0) / d; }
 // ---------------------------------------------------------------------------------------------------------------
 
 // Pivot block: POTRF (or LDL^T) of the 64 x 64 diagonal block of a front, called by all 256 threads of a CTA, the
-// block in registers. T = double: the FP64 factor; T = float: the mixed-precision factor. Lp: the block's (0, 0)
-// entry (ld m), w <= 64 its columns. Thread t < 136 owns the 4 x 4 tile (ti, tj), ti >= tj, of the lower triangle.
+// block in registers. T = double: the FP64 factor; T = float: the mixed-precision factor. src: the updated block in
+// shared memory, entry (i, j) at src[j lds + i]; Lp: the block's (0, 0) entry in the front (ld m), where the factor is
+// written; w <= 64 its columns. Thread t < 136 owns the 4 x 4 tile (ti, tj), ti >= tj, of the lower triangle.
 // Right-looking on the unscaled columns, four columns per step kb with two barriers: (1) the diagonal tile eliminates
 // its four columns (settling the pivots) and publishes them; (2) the tiles below it in column block kb eliminate the
 // same four columns against it and publish theirs; then every tile right of the block applies the rank-4 update
@@ -248,8 +249,8 @@ __device__ __forceinline__ cplx fast_recip(cplx d) { return cplx(1.0) / d; }
 // Returns false (status set for the first failing column f + c0 + k) when a pivot failed; the block is then not
 // written back.
 template <class T, class TC>
-__device__ int potrf_core(T *Lp, int m, int w, int f, int c0, int s, unsigned long long *status,
-                          const LdltArgs<T> &ld, double promoteBelow) {
+__device__ int potrf_core(const T *src, int lds, T *Lp, int m, int w, int f, int c0, int s,
+                          unsigned long long *status, const LdltArgs<T> &ld, double promoteBelow) {
   __shared__ TC col[2][4][kPanel];  // per 4-column block (double-buffered): the block's unscaled columns, by row
   __shared__ TC pd[kPanel], piv[2][4];
   __shared__ unsigned char pflag[kPanel];
@@ -270,7 +271,7 @@ __device__ int potrf_core(T *Lp, int m, int w, int f, int c0, int s, unsigned lo
 #pragma unroll
     for (int c = 0; c < 4; c++) {
       const int i = 4 * ti + r, j = 4 * tj + c;
-      a[r][c] = !owner || i < j ? TC(0) : (i < w ? (TC)Lp[(int64_t)j * m + i] : (i == j ? TC(1) : TC(0)));
+      a[r][c] = !owner || i < j ? TC(0) : (i < w ? (TC)src[j * lds + i] : (i == j ? TC(1) : TC(0)));
     }
   if (tid == 0) {
     fail = kPanel;  // none
@@ -370,21 +371,21 @@ __device__ int potrf_core(T *Lp, int m, int w, int f, int c0, int s, unsigned lo
 }
 
 // POTRF / LDL^T of a pivot block (potrf_core in the factor's precision). An FP32 LDL^T block with a pivot of
-// magnitude below FLT_EPSILON x max_i |A(i, i)| (a pivot with no correct FP32 digit left) is factored again from its
-// stored entries in FP64 arithmetic (stored FP32): the small-pivot blocks of the mixed-precision indefinite factor get
-// FP64 pivots. Returns false when a pivot failed (status set).
+// magnitude below FLT_EPSILON x max_i |A(i, i)| (a pivot with no correct FP32 digit left) is factored again from the
+// same entries (src is left unchanged) in FP64 arithmetic (stored FP32): the small-pivot blocks of the mixed-precision
+// indefinite factor get FP64 pivots. Returns false when a pivot failed (status set).
 template <class T>
-__device__ bool potrf_block(T *Lp, int m, int w, int f, int c0, int s, unsigned long long *status,
-                            const LdltArgs<T> &ld) {
+__device__ bool potrf_block(const T *src, int lds, T *Lp, int m, int w, int f, int c0, int s,
+                            unsigned long long *status, const LdltArgs<T> &ld) {
   if constexpr (std::is_same<T, float>::value) {
     if (ld.scal != nullptr) {
       const double amax = ld.scal[0] > 0.0 ? ld.scal[1] / ld.scal[0] : 0.0;
-      const int r = potrf_core<float, float>(Lp, m, w, f, c0, s, status, ld, amax * (double)FLT_EPSILON);
+      const int r = potrf_core<float, float>(src, lds, Lp, m, w, f, c0, s, status, ld, amax * (double)FLT_EPSILON);
       if (r != 2) return r == 0;
-      return potrf_core<float, double>(Lp, m, w, f, c0, s, status, ld, -1.0) == 0;
+      return potrf_core<float, double>(src, lds, Lp, m, w, f, c0, s, status, ld, -1.0) == 0;
     }
   }
-  return potrf_core<T, T>(Lp, m, w, f, c0, s, status, ld, -1.0) == 0;
+  return potrf_core<T, T>(src, lds, Lp, m, w, f, c0, s, status, ld, -1.0) == 0;
 }
 
 // TRSM of up to 64 rows [r0, r1) of a front (L: its column-major block, ld m) against its factored pivot block
@@ -395,7 +396,8 @@ __device__ bool potrf_block(T *Lp, int m, int w, int f, int c0, int s, unsigned 
 // M(k, k) = d_k, x = L21, and w = x D = L21 D (the update's A operand, written to ld.W for the FP64 factor). The rows
 // are also written as BF16 hi / lo pairs (hi = bf16(x), lo = bf16(x - hi)) into the split columns of the tensor-core
 // update (mixed precision). The pivot block and D come from another CTA of the launch: read through L2 (__ldcg).
-// On return Ws[c][r] holds this strip's update operand (x, or x D for LDL^T), c < w, r < r1 - r0.
+// On return Ws[c][r] holds this strip's update operand (x, or x D for LDL^T) and M[c][r] the solved rows x
+// (c < w, r < r1 - r0; zero elsewhere): a diagonal strip's X_c for its own column block.
 template <class T>
 __device__ void trsm_strip(T *L, int m, int f, int c0, int w, int r0, int r1, int64_t lxp, int64_t sp,
                            __nv_bfloat16 *Shi, __nv_bfloat16 *Slo, const LdltArgs<T> &ld, T (*M)[kPanel + 1],
@@ -459,6 +461,7 @@ __device__ void trsm_strip(T *L, int m, int f, int c0, int w, int r0, int r1, in
     const T xv = x[u];
     const T wv = ldlt ? xv * dv[cc] : xv;
     Ws[cc][r] = active && cc < w ? wv : T(0);
+    M[cc][r] = active && cc < w ? xv : T(0);  // the pivot block in M is no longer read
     if (!active || cc >= w) continue;
     L[(int64_t)(c0 + cc) * m + row] = xv;
     if (ldlt && ld.W) ld.W[lxp + (int64_t)(c0 + cc) * m + row] = wv;
@@ -504,13 +507,11 @@ __device__ __forceinline__ bool panel_wait(const int *p, int need, unsigned long
   return ok != 0;
 }
 
-// Publish *p = v after this CTA's global writes (all threads pass the barrier first).
+// Publish *p = v after this CTA's global writes: all threads pass the barrier first, and thread 0's release store
+// orders every write made before the barrier (by any thread of the CTA) before the flag, for a reader that acquires it.
 __device__ __forceinline__ void panel_release(int *p, int v) {
   __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    st_release(p, v);
-  }
+  if (threadIdx.x == 0) st_release(p, v);
 }
 
 // One group of pivot blocks [g0, g1) of a front, a strip of up to 64 rows per CTA, CTAs ordered by an atomic ticket
@@ -524,9 +525,12 @@ __device__ __forceinline__ void panel_release(int *p, int v) {
 // launch cannot deadlock whatever the number of resident CTAs. The columns right of the group receive the group's
 // update afterwards (k_update / k_update_mx, K = the group). Failure (a pivot, a bounded wait) sets the status and
 // releases P[b], so every waiter leaves.
-constexpr int kGroupSmem = 2 * kPanel * (kPanel + 1) * (int)sizeof(double);
+constexpr int kGroupSmem = 3 * kPanel * (kPanel + 1) * (int)sizeof(double);
+// two CTAs per SM for the real factors (registers capped at 128); the complex one is held to one by its shared memory
 template <class T>
-__global__ void __launch_bounds__(256) k_group_panel(const GroupItem *__restrict__ items,
+constexpr int group_min_blocks() { return is_cplx<T>::value ? 1 : 2; }
+template <class T>
+__global__ void __launch_bounds__(256, group_min_blocks<T>()) k_group_panel(const GroupItem *__restrict__ items,
                                                      const StripTask *__restrict__ strips, int nstrips, int *ticket,
                                                      int *flags, DevPlan P, T *__restrict__ Lx,
                                                      unsigned long long *status, __nv_bfloat16 *__restrict__ Shi,
@@ -534,6 +538,7 @@ __global__ void __launch_bounds__(256) k_group_panel(const GroupItem *__restrict
   extern __shared__ __align__(16) unsigned char gp_raw[];
   T(*M)[kPanel + 1] = reinterpret_cast<T(*)[kPanel + 1]>(gp_raw);  // pivot block (TRSM), then the X_c chunk
   T(*Ws)[kPanel + 1] = reinterpret_cast<T(*)[kPanel + 1]>(gp_raw + kPanel * (kPanel + 1) * sizeof(T));
+  T(*Ds)[kPanel + 1] = reinterpret_cast<T(*)[kPanel + 1]>(gp_raw + 2 * kPanel * (kPanel + 1) * sizeof(T));
   __shared__ T invd[kPanel], dv[kPanel];
   __shared__ int sTicket;
   if (threadIdx.x == 0) sTicket = failed(status) ? nstrips : atomicAdd(ticket, 1);
@@ -550,21 +555,35 @@ __global__ void __launch_bounds__(256) k_group_panel(const GroupItem *__restrict
   T *L = Lx + P.snLxp[s];
   int *Pf = flags + it.flag0, *Df = Pf + nb;
   const int tid = threadIdx.x, tr = tid & 15, tc = tid >> 4;
+  // A diagonal strip keeps its own pivot block (columns [r0, r1), lower part) in shared memory while it updates it
+  // (Ds[j][i] = block (i, j)), and its POTRF reads it from there: no round trip through the front.
+  if (jd >= 0) {
+    for (int e = tid; e < kPanel * kPanel; e += blockDim.x) {
+      const int i = e & 63, j = e >> 6;
+      Ds[j][i] = (r0 + i < r1 && j <= i) ? L[(int64_t)(r0 + j) * m + r0 + i] : T(0);
+    }
+  }
   for (int b = 0; b < bmax; b++) {
     const int c0 = g0 + b * kPanel, w = min(kPanel, g1 - c0), c1 = c0 + w;
     if (!panel_wait(Pf + b, 1, status, P.spin)) return;
     trsm_strip<T>(L, m, f, c0, w, r0, r1, P.snLxp[s], P.snSp[s], Shi, Slo, ld, M, Ws, invd, dv);
     if (jd >= 0) panel_release(Df + jd, b + 1);
-    // the group's remaining columns [c1, hi): a diagonal strip only its lower part (columns < r1)
-    const int hi = jd >= 0 ? min(g1, r1) : g1;
-    for (int cb = c1; cb < hi; cb += kPanel) {
-      const int j = (cb - g0) / kPanel, ncol = min(kPanel, hi - cb);
-      if (j != jd && !panel_wait(Df + j, b + 1, status, P.spin)) return;
-      for (int e = tid; e < kPanel * kPanel; e += blockDim.x) {  // X_c[k][jj] = L(cb + jj, c0 + k)
-        const int k = e >> 6, jj = e & 63;
-        M[k][jj] = (k < w && jj < ncol) ? ldcg_v(L + (int64_t)(c0 + k) * m + cb + jj) : T(0);
+    // Update with block b (C -= W_r X_c^T, K = w): a diagonal strip first its own pivot block (X_c = its solved rows,
+    // left in M by the TRSM; into Ds), then the blocks between block b and its own; a strip below every remaining
+    // column block of the group.
+    const int hi = jd >= 0 ? r0 : g1, nown = jd >= 0 ? 1 : 0;
+    const int nchunk = nown + (hi > c1 ? (hi - c1 + kPanel - 1) / kPanel : 0);
+    for (int ch = 0; ch < nchunk; ch++) {
+      const bool own = ch < nown;
+      const int cb = own ? r0 : c1 + (ch - nown) * kPanel, ncol = own ? r1 - r0 : min(kPanel, hi - cb);
+      if (!own) {
+        if (!panel_wait(Df + (cb - g0) / kPanel, b + 1, status, P.spin)) return;
+        for (int e = tid; e < kPanel * kPanel; e += blockDim.x) {  // X_c[k][jj] = L(cb + jj, c0 + k)
+          const int k = e >> 6, jj = e & 63;
+          M[k][jj] = (k < w && jj < ncol) ? ldcg_v(L + (int64_t)(c0 + k) * m + cb + jj) : T(0);
+        }
+        __syncthreads();
       }
-      __syncthreads();
       T acc[4][4];
 #pragma unroll
       for (int a = 0; a < 4; a++)
@@ -585,18 +604,21 @@ __global__ void __launch_bounds__(256) k_group_panel(const GroupItem *__restrict
       for (int a = 0; a < 4; a++)
 #pragma unroll
         for (int bb = 0; bb < 4; bb++) {
-          const int row = r0 + tr + 16 * a, colj = cb + tc + 16 * bb;
-          if (row < r1 && colj < cb + ncol && (jd < 0 || row >= colj)) {
-            T *cptr = L + (int64_t)colj * m + row;
+          const int i = tr + 16 * a, jj = tc + 16 * bb;
+          if (own) {
+            if (jj <= i) Ds[jj][i] -= acc[a][bb];
+          } else if (r0 + i < r1 && jj < ncol) {
+            T *cptr = L + (int64_t)(cb + jj) * m + r0 + i;
             *cptr = *cptr - acc[a][bb];
           }
         }
-      __syncthreads();  // M is reloaded by the next chunk
+      __syncthreads();  // M is reloaded by the next chunk, or by the next TRSM
     }
   }
   if (jd >= 0) {  // this strip's own pivot block, fully updated: factor it and publish it (also after a failure)
     const int c0 = g0 + jd * kPanel, w = min(kPanel, g1 - c0);
-    potrf_block<T>(L + (int64_t)c0 * m + c0, m, w, f, c0, s, status, ld);
+    __syncthreads();  // Ds complete (also when the strip had no earlier pivot block)
+    potrf_block<T>(&Ds[0][0], kPanel + 1, L + (int64_t)c0 * m + c0, m, w, f, c0, s, status, ld);
     panel_release(Pf + jd, 1);
   }
 }
@@ -892,7 +914,7 @@ void launch_group_panel(const GroupItem *items, const StripTask *strips, int nst
                         const DevPlan &P, T *Lx, unsigned long long *status, __nv_bfloat16 *Shi, __nv_bfloat16 *Slo,
                         const LdltArgs<T> &ld, cudaStream_t st) {
   if (nstrips > 0)
-    k_group_panel<T><<<(unsigned)nstrips, 256, 2 * kPanel * (kPanel + 1) * sizeof(T), st>>>(
+    k_group_panel<T><<<(unsigned)nstrips, 256, 3 * kPanel * (kPanel + 1) * sizeof(T), st>>>(
         items, strips, nstrips, ticket, flags, P, Lx, status, Shi, Slo, ld);
 }
 template void launch_group_panel<double>(const GroupItem *, const StripTask *, int, int *, int *, const DevPlan &,

@@ -1,16 +1,28 @@
 // Supernodal triangular solves with several right-hand sides at once (sparse.mjs solveNumericMulti :1261-1310,
-// ldlt.mjs solveMany :595-643): the same task lists, flags and ticket order as the one-vector sweeps (solve.cu), but
-// every task moves all q <= 64 vectors together, so each L element is read once per sweep instead of once per vector.
+// ldlt.mjs solveMany :595-643): the same task lists and ticket order as the one-vector sweeps (solve.cu), every task
+// moving a slice of up to 16 of the q <= 64 vectors.
 //
 // Vectors are interleaved: entry i of vector k sits at y[i q + k] (and likewise the front vectors V and the pass-up
 // buffers T), so a row of the solution is q contiguous doubles and the gathers through the extend-add maps and the
 // row lists move whole rows.
 //
-// A task is a small GEMM: out (64 rows x q) = sum over a reduction index of A (64 x KC tile) times B (KC x q tile),
-// both tiles staged in shared memory (FP64; FP32 factors are widened on load), each thread accumulating a 4 x 4
-// register tile. Forward: A = L[block rows, pivot columns so far], B = y[those columns]. Backward: A = the block's
-// columns of L over the rows below the block (transposed on load), B = x[those rows]. Then the 64 x 64 inverse of the
-// diagonal block is applied the same way.
+// Vector slices: task t of the launch is list entry t / ns for vector slice t % ns (ns = ceil(q / 16)), with its own
+// ready flags (flags[slice * nflags + block]) and done counters (done[slice * nsuper + s]), so the slices of a
+// supernode run as independent dependency chains on different CTAs and a task never computes on absent vectors. The
+// expanded order keeps every wait on a task with a smaller ticket. The small supernodes (kind 2, one warp each) solve
+// all q vectors in the task of slice 0 and count/release every slice.
+//
+// A task is a small GEMM on the FP64 tensor cores (mma.sync m16n8k16): out (64 rows x 16 vectors) = sum over a
+// reduction index of A (64 x 32 chunk, FP32 factors widened on the shared-memory store) times B (32 x 16), 8 warps
+// as 4 (16-row blocks) x 2 (16-wide halves of the chunk), the halves summed through shared memory at the end.
+// Forward: A = L[block rows, pivot columns so far], B = y[those columns]. Backward: A = the block's columns of L over
+// the rows below the block (transposed on load), B = x[those rows]. Then the 64 x 64 inverse of the diagonal block,
+// prefetched into shared memory by cp.async when the task starts, is applied the same way.
+//
+// Backward order: the rows below the supernode are summed from the last chunk down, each chunk after the flags of the
+// ancestor blocks that hold its rows (rowBlk), so a task works while its ancestors are still being solved (the
+// highest ancestors, which hold the last rows, finish first); then the supernode's own later blocks, each after its
+// flag.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -24,26 +36,88 @@ namespace amp {
 
 constexpr int kMB = 64;              // rows of a block task
 constexpr int kKC = 32;              // reduction chunk
+constexpr int kQS = 16;              // vectors per slice (one slice per task)
 constexpr int kMQ = 64;              // vectors per pass (the host splits larger sets)
-constexpr int kLdt = 66;             // shared tile row stride in doubles (even: 16-byte aligned double2 reads)
+constexpr int kLdKM = kMB + 4;       // A stored [k][m] (m contiguous): 68 doubles, == 4 mod 16 (conflict-free fragments)
+constexpr int kLdMK = kKC + 4;       // A chunk stored [m][k]: 36
+constexpr int kLdX = kMB + 4;        // inverse block stored [k][m] or [m][k], 64 x 64: 68
+constexpr int kLdB = kQS + 4;        // B stored [k][n]: 20
 constexpr int kMultiThreads = 256;
-constexpr int kMultiSmem = (2 * kKC + kMB) * kLdt * (int)sizeof(double);
-static_assert(kSolveGroup * 32 * kMQ * (int)sizeof(double) <= kMultiSmem, "small-supernode tasks: front vectors");
-// acc[i][j] += sum over kk < kc of A[kk][4 ty + i] B[kk][4 tx + j]
-__device__ __forceinline__ void mm_tile(const double *__restrict__ A, const double *__restrict__ B, int kc, int ty,
-                                        int tx, double (&acc)[4][4]) {
-#pragma unroll 4
-  for (int kk = 0; kk < kc; kk++) {
-    const double2 a0 = *reinterpret_cast<const double2 *>(A + kk * kLdt + 4 * ty);
-    const double2 a1 = *reinterpret_cast<const double2 *>(A + kk * kLdt + 4 * ty + 2);
-    const double2 b0 = *reinterpret_cast<const double2 *>(B + kk * kLdt + 4 * tx);
-    const double2 b1 = *reinterpret_cast<const double2 *>(B + kk * kLdt + 4 * tx + 2);
-    const double a[4] = {a0.x, a0.y, a1.x, a1.y}, b[4] = {b0.x, b0.y, b1.x, b1.y};
+constexpr int kAElems = kMB * kLdMK;  // >= kKC * kLdKM; also the halves' reduction buffer (64 x 17)
+static_assert(kAElems >= kKC * kLdKM && kAElems >= kMB * (kQS + 1), "A tile buffer");
+template <class TL>
+constexpr int multi_smem() {
+  const int own = (kAElems + kKC * kLdB + kMB * kLdB) * (int)sizeof(double) + kMB * kLdX * (int)sizeof(TL);
+  const int small = kSolveGroup * 32 * kMQ * (int)sizeof(double);  // kind 2 tasks: 32 x 64 front vectors per warp
+  return own > small ? own : small;
+}
+
+__device__ __forceinline__ void dmma16816(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]), "d"(b[1]),
+        "d"(b[2]), "d"(b[3]));
+}
+
+// Fragment layouts of the m16n8k16 FP64 MMA (g = lane / 4, t = lane % 4): A (m = g + 8 (v & 1), k = t + 4 (v >> 1)),
+// B (n = g, k = t + 4 v), C (m = g + 8 (v >> 1), n = 2 t + (v & 1)).
+// c[nb] += A[16 mw .. +16, k0 .. k0 + 16) B[k0 .. k0 + 16, 8 nb .. 8 nb + 8) for both n halves; A element (m, k) at
+// A[k * lda + m] (KM) or A[m * lda + k] (MK), B element (k, n) at B[k * kLdB + n].
+template <bool KM, class TA>
+__device__ __forceinline__ void mma_k16(const TA *__restrict__ A, int lda, const double *__restrict__ B, int k0,
+                                        int mw, int lane, double (&c)[2][4]) {
+  const int g = lane >> 2, t = lane & 3;
+  double a[8];
 #pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-      for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+  for (int v = 0; v < 8; v++) {
+    const int m = 16 * mw + g + 8 * (v & 1), k = k0 + t + 4 * (v >> 1);
+    a[v] = (double)(KM ? A[k * lda + m] : A[m * lda + k]);
   }
+#pragma unroll
+  for (int nb = 0; nb < 2; nb++) {
+    double b[4];
+#pragma unroll
+    for (int v = 0; v < 4; v++) b[v] = B[(k0 + t + 4 * v) * kLdB + 8 * nb + g];
+    dmma16816(c[nb], a, b);
+  }
+}
+
+// The two halves of the reduction index: warps 4-7 add their partial tile into warps 0-3's (red: 64 x 17 doubles).
+// On return warps 0-3 hold the sum; red is free after the caller's next barrier.
+__device__ __forceinline__ void halves_sum(double (&c)[2][4], double *red, int warp, int lane) {
+  const int mw = warp & 3, g = lane >> 2, t = lane & 3;
+  if (warp >= 4) {
+#pragma unroll
+    for (int nb = 0; nb < 2; nb++)
+#pragma unroll
+      for (int v = 0; v < 4; v++) red[(16 * mw + g + 8 * (v >> 1)) * (kQS + 1) + 8 * nb + 2 * t + (v & 1)] = c[nb][v];
+  }
+  __syncthreads();
+  if (warp < 4) {
+#pragma unroll
+    for (int nb = 0; nb < 2; nb++)
+#pragma unroll
+      for (int v = 0; v < 4; v++) c[nb][v] += red[(16 * mw + g + 8 * (v >> 1)) * (kQS + 1) + 8 * nb + 2 * t + (v & 1)];
+  }
+}
+
+// row / vector of accumulator element (nb, v) of this lane (warps 0-3)
+__device__ __forceinline__ int acc_row(int warp, int lane, int v) { return 16 * (warp & 3) + (lane >> 2) + 8 * (v >> 1); }
+__device__ __forceinline__ int acc_vec(int lane, int nb, int v) { return 8 * nb + 2 * (lane & 3) + (v & 1); }
+
+__device__ __forceinline__ void cp_async_el(void *smem, const void *gmem, int bytes, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = valid ? bytes : 0;  // zero-fill when out of range
+  if (bytes == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(n) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(gmem), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_all() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 // persistent ticket loop shared by both sweeps
@@ -60,52 +134,69 @@ __device__ __forceinline__ void ticket_loop(int *ticket, int ntasks, Run &&run) 
 }
 
 // ---- forward ------------------------------------------------------------------------------------------------------
-// task (s, blk, below): as k_fwd_blocks. Diagonal: y[block] = X (V[block] - L[block, 0:blk 64] y[0:blk 64]);
+// task (s, blk, below) of slice sl: as k_fwd_blocks. Diagonal: y[block] = X (V[block] - L[block, 0:blk 64] y[0:blk 64]);
 // below: T[block] = V[block] - L[block, 0:nc] y[0:nc].
 template <class TL>
-__global__ void __launch_bounds__(kMultiThreads, 3) k_fwd_multi(const int4 *__restrict__ tasks, int ntasks,
+__global__ void __launch_bounds__(kMultiThreads, 3) k_fwd_multi(const int4 *__restrict__ tasks, int ntasks, int ns,
                                                                 int *__restrict__ ticket, DevPlan P,
                                                                 const TL *__restrict__ Lx, const TL *__restrict__ Inv,
                                                                 double *__restrict__ y, double *__restrict__ V,
                                                                 double *__restrict__ T, int *__restrict__ flags,
-                                                                int epoch, int *__restrict__ done, int q,
+                                                                int nflags, int epoch, int *__restrict__ done, int q,
                                                                 unsigned long long *status) {
   extern __shared__ double msm[];
-  double *As = msm, *Bs = msm + kKC * kLdt, *Rs = msm + 2 * kKC * kLdt;
+  double *As = msm, *Bs = As + kAElems, *Rs = Bs + kKC * kLdB;
+  TL *Xs = reinterpret_cast<TL *>(Rs + kMB * kLdB);
   __shared__ int waitOk;
-  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, mw = warp & 3, kh = warp >> 2;
+  auto bail = [] {  // a wait gave up: drain this thread's copies into shared memory before the CTA leaves
+    cp_async_all();
+    return false;
+  };
   auto run = [&](const int tkv) -> bool {
-    const int4 t = tasks[tkv];
-    if (t.z == 2) {  // up to kSolveGroup supernodes with m <= 32, one warp each (32 x 64 doubles of msm per warp)
-      const int warp = tid >> 5;
+    const int base = tkv / ns, sl = tkv - base * ns;
+    const int4 t = tasks[base];
+    if (t.z == 2) {  // up to kSolveGroup supernodes with m <= 32, one warp each, all q vectors (slice 0's task)
+      if (sl != 0) return true;
       if (tid == 0) waitOk = 1;
       __syncthreads();
-      if (warp < t.y &&
-          !small_fwd_warp_multi<TL>(P.solveSmall[t.x + warp], P, Lx, y, T, done, q, status, msm + 32 * kMQ * warp))
+      if (warp < t.y && !small_fwd_warp_multi<TL>(P.solveSmall[t.x + warp], P, Lx, y, T, done, q, ns, status,
+                                                  msm + 32 * kMQ * warp))
         waitOk = 0;
       __syncthreads();
       return waitOk != 0;
     }
     const int s = t.x, blk = t.y, below = t.z;
     const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s], mu = m - nc;
+    const int vb = sl * kQS, qs = min(kQS, q - vb);
     const TL *Lp = Lx + P.snLxp[s];
     const int r0 = below ? nc + blk * kMB : blk * kMB;
     const int rows = below ? min(kMB, mu - blk * kMB) : min(kMB, nc - blk * kMB);
     const int ncols = below ? nc : blk * kMB;
-    int *myflags = flags + P.blkOff[s];
+    int *myflags = flags + (int64_t)sl * nflags + P.blkOff[s];
+    int *mydone = done + (int64_t)sl * P.nsuper;
     const int64_t vbase = (int64_t)P.Sp[s];
+    if (!below) {  // the inverse of the diagonal block, [k][m], arrives while the task sums
+      const TL *X = Inv + P.invOff[P.blkOff[s] + blk];
+      for (int e = tid; e < kMB * kMB; e += kMultiThreads) {
+        const int i = e & (kMB - 1), k = e >> 6;
+        const bool ok = i < rows && k < rows;
+        cp_async_el(Xs + k * kLdX + i, ok ? X + (int64_t)k * rows + i : X, (int)sizeof(TL), ok);
+      }
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
     if (!below && blk == 0) {
       for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
         const int c = P.chList[qq];
         const int need = (P.snM[c] - P.snNc[c] + kMB - 1) / kMB;
-        if (tid == 0) waitOk = wait_count(done + c, need, status, s, P.spin);
+        if (tid == 0) waitOk = wait_count(mydone + c, need, status, s, P.spin);
         __syncthreads();
-        if (!waitOk) return false;
+        if (!waitOk) return bail();
       }
-      // v_s = [y(f .. f + nc); 0] + the children's pass-up vectors in the reference's child order
-      for (int64_t e = tid; e < (int64_t)m * q; e += kMultiThreads) {
-        const int r = (int)(e / q), k = (int)(e - (int64_t)r * q);
-        V[(vbase + r) * q + k] = r < nc ? y[(int64_t)(f + r) * q + k] : 0.0;
+      // v_s = [y(f .. f + nc); 0] + the children's pass-up vectors in the reference's child order (this slice)
+      for (int e = tid; e < m * kQS; e += kMultiThreads) {
+        const int r = e >> 4, k = e & (kQS - 1);
+        if (k < qs) V[(vbase + r) * q + vb + k] = r < nc ? y[(int64_t)(f + r) * q + vb + k] : 0.0;
       }
       __syncthreads();
       for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
@@ -113,25 +204,25 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_fwd_multi(const int4 *__re
         const int muc = P.snM[c] - P.snNc[c];
         const int *map = P.eaMap + P.eaPtr[c];
         const double *tc = T + P.snTOff[c] * q;
-        for (int64_t e = tid; e < (int64_t)muc * q; e += kMultiThreads) {
-          const int a = (int)(e / q), k = (int)(e - (int64_t)a * q);
-          V[(vbase + map[a]) * q + k] += __ldcg(tc + e);
+        for (int e = tid; e < muc * kQS; e += kMultiThreads) {
+          const int a = e >> 4, k = e & (kQS - 1);
+          if (k < qs) V[(vbase + map[a]) * q + vb + k] += __ldcg(tc + (int64_t)a * q + vb + k);
         }
         __syncthreads();
       }
     }
-    double acc[4][4];
+    double c[2][4];
 #pragma unroll
-    for (int i = 0; i < 4; i++)
+    for (int nb = 0; nb < 2; nb++)
 #pragma unroll
-      for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
-    // L tile of a chunk: As[c][row] = L(r0 + row, cb + c); thread elements e = tid + 256 u: row = e & 63, c = e >> 6
+      for (int v = 0; v < 4; v++) c[nb][v] = 0.0;
+    // L chunk, [k][m]: As[cc][row] = L(r0 + row, cb + cc); thread elements e = tid + 256 u: row = e & 63, cc = e >> 6
     TL lr[8];
     auto loadL = [&](int cb) {
 #pragma unroll
       for (int u = 0; u < 8; u++) {
-        const int e = tid + kMultiThreads * u, row = e & (kMB - 1), c = e >> 6;
-        lr[u] = (row < rows && cb + c < ncols) ? Lp[(int64_t)(cb + c) * m + r0 + row] : (TL)0;
+        const int e = tid + kMultiThreads * u, row = e & (kMB - 1), cc = e >> 6;
+        lr[u] = (row < rows && cb + cc < ncols) ? Lp[(int64_t)(cb + cc) * m + r0 + row] : (TL)0;
       }
     };
     const int nch = (ncols + kKC - 1) / kKC;
@@ -141,70 +232,69 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_fwd_multi(const int4 *__re
       if ((cb & (kMB - 1)) == 0) {  // first chunk of a pivot block: its y values final?
         if (tid == 0) waitOk = wait_flag(myflags + cb / kMB, epoch, status, s, P.spin);
         __syncthreads();
-        if (!waitOk) return false;
+        if (!waitOk) return bail();
       }
-      for (int e = tid; e < kKC * kMQ; e += kMultiThreads) {
-        const int c = e >> 6, k = e & (kMQ - 1);
-        Bs[c * kLdt + k] = (c < cw && k < q) ? __ldcg(y + (int64_t)(f + cb + c) * q + k) : 0.0;
+      for (int e = tid; e < kKC * kQS; e += kMultiThreads) {
+        const int k = e >> 4, n = e & (kQS - 1);
+        Bs[k * kLdB + n] = (k < cw && n < qs) ? __ldcg(y + (int64_t)(f + cb + k) * q + vb + n) : 0.0;
       }
 #pragma unroll
       for (int u = 0; u < 8; u++) {
         const int e = tid + kMultiThreads * u;
-        As[(e >> 6) * kLdt + (e & (kMB - 1))] = (double)lr[u];
+        As[(e >> 6) * kLdKM + (e & (kMB - 1))] = (double)lr[u];
       }
       __syncthreads();
       if (ch + 1 < nch) loadL(cb + kKC);
-      mm_tile(As, Bs, cw, ty, tx, acc);
+      if (16 * kh < cw) mma_k16<true>(As, kLdKM, Bs, 16 * kh, mw, lane, c);
       __syncthreads();
     }
+    halves_sum(c, As, warp, lane);
     // R = V[block] - acc (V final once the supernode's first diagonal block is: waited above, or gathered here)
     if (below) {
-      double *to = T + (P.snTOff[s] + (int64_t)blk * kMB) * q;
+      if (warp < 4) {
+        double *to = T + (P.snTOff[s] + (int64_t)blk * kMB) * q + vb;
 #pragma unroll
-      for (int i = 0; i < 4; i++) {
-        const int row = 4 * ty + i;
-        if (row >= rows) continue;
+        for (int nb = 0; nb < 2; nb++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-          const int k = 4 * tx + j;
-          if (k < q) to[(int64_t)row * q + k] = __ldcg(V + (vbase + r0 + row) * q + k) - acc[i][j];
-        }
+          for (int v = 0; v < 4; v++) {
+            const int row = acc_row(warp, lane, v), n = acc_vec(lane, nb, v);
+            if (row < rows && n < qs) to[(int64_t)row * q + n] = __ldcg(V + (vbase + r0 + row) * q + vb + n) - c[nb][v];
+          }
       }
       __syncthreads();
-      if (tid == 0) red_release_add(done + s, 1);
+      if (tid == 0) red_release_add(mydone + s, 1);
       return true;
     }
+    if (warp < 4) {
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-      const int row = 4 * ty + i;
+      for (int nb = 0; nb < 2; nb++)
 #pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const int k = 4 * tx + j;
-        Rs[row * kLdt + k] = (row < rows && k < q) ? __ldcg(V + (vbase + r0 + row) * q + k) - acc[i][j] : 0.0;
-        acc[i][j] = 0.0;
-      }
-    }
-    // y[block] = X R, X = L_kk^-1 (rows x rows, column-major): As[jj][i] = X(i, jb + jj)
-    const TL *X = Inv + P.invOff[P.blkOff[s] + blk];
-    for (int jb = 0; jb < rows; jb += kKC) {
-      const int jw = min(kKC, rows - jb);
-      __syncthreads();
-      for (int e = tid; e < kKC * kMB; e += kMultiThreads) {
-        const int i = e & (kMB - 1), jj = e >> 6;
-        As[jj * kLdt + i] = (i < rows && jj < jw) ? (double)X[(int64_t)(jb + jj) * rows + i] : 0.0;
-      }
-      __syncthreads();
-      mm_tile(As, Rs + jb * kLdt, jw, ty, tx, acc);
+        for (int v = 0; v < 4; v++) {
+          const int row = acc_row(warp, lane, v), n = acc_vec(lane, nb, v);
+          Rs[row * kLdB + n] = (row < rows && n < qs) ? __ldcg(V + (vbase + r0 + row) * q + vb + n) - c[nb][v] : 0.0;
+        }
     }
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-      const int row = 4 * ty + i;
-      if (row >= rows) continue;
+    for (int nb = 0; nb < 2; nb++)
 #pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const int k = 4 * tx + j;
-        if (k < q) y[(int64_t)(f + r0 + row) * q + k] = acc[i][j];
-      }
+      for (int v = 0; v < 4; v++) c[nb][v] = 0.0;
+    cp_async_all();
+    __syncthreads();
+    // y[block] = X R: k = 0 .. 63 of X as four k16 steps, two per warp half
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int k0 = 32 * h + 16 * kh;
+      if (k0 < rows) mma_k16<true>(Xs, kLdX, Rs, k0, mw, lane, c);
+    }
+    halves_sum(c, As, warp, lane);
+    if (warp < 4) {
+#pragma unroll
+      for (int nb = 0; nb < 2; nb++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+          const int row = acc_row(warp, lane, v), n = acc_vec(lane, nb, v);
+          if (row < rows && n < qs) y[(int64_t)(f + r0 + row) * q + vb + n] = c[nb][v];
+        }
     }
     __syncthreads();
     if (tid == 0) st_release(myflags + blk, epoch);
@@ -214,57 +304,68 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_fwd_multi(const int4 *__re
 }
 
 // ---- backward -----------------------------------------------------------------------------------------------------
-// task (s, blk): x[block] = X^T (y[block] (/ D for LDL^T) - L[rows below the block, block columns]^T x[those rows]).
-// The rows below the supernode (ancestors, final once the parent's first pivot block is) go first, then the later
-// pivot blocks of the supernode from the last one down, each after its flag.
+// task (s, blk) of slice sl: x[block] = X^T (y[block] (/ D for LDL^T) - L[rows below the block, block columns]^T
+// x[those rows]).
 template <class TL>
-__global__ void __launch_bounds__(kMultiThreads, 3) k_bwd_multi(const int4 *__restrict__ tasks, int ntasks,
+__global__ void __launch_bounds__(kMultiThreads, 3) k_bwd_multi(const int4 *__restrict__ tasks, int ntasks, int ns,
                                                                 int *__restrict__ ticket, DevPlan P,
                                                                 const TL *__restrict__ Lx, const TL *__restrict__ Inv,
                                                                 const double *__restrict__ Dpiv,
                                                                 double *__restrict__ y, int *__restrict__ flags,
-                                                                int epoch, int q, unsigned long long *status) {
+                                                                int nflags, int epoch, int q,
+                                                                unsigned long long *status) {
   extern __shared__ double msm[];
-  double *As = msm, *Bs = msm + kKC * kLdt, *Rs = msm + 2 * kKC * kLdt;
+  double *As = msm, *Bs = As + kAElems, *Rs = Bs + kKC * kLdB;
+  TL *Xs = reinterpret_cast<TL *>(Rs + kMB * kLdB);
   __shared__ int waitOk;
-  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, mw = warp & 3, kh = warp >> 2;
+  auto bail = [] {  // a wait gave up: drain this thread's copies into shared memory before the CTA leaves
+    cp_async_all();
+    return false;
+  };
   auto run = [&](const int tkv) -> bool {
-    const int4 t = tasks[tkv];
-    if (t.z == 2) {  // up to kSolveGroup supernodes with m <= 32, one warp each (32 x 64 doubles of msm per warp)
-      const int warp = tid >> 5;
+    const int base = tkv / ns, sl = tkv - base * ns;
+    const int4 t = tasks[base];
+    if (t.z == 2) {  // up to kSolveGroup supernodes with m <= 32, one warp each, all q vectors (slice 0's task)
+      if (sl != 0) return true;
       if (tid == 0) waitOk = 1;
       __syncthreads();
-      if (warp < t.y && !small_bwd_warp_multi<TL>(P.solveSmall[t.x + warp], P, Lx, Dpiv, y, flags, epoch, q, status,
-                                                  msm + 32 * kMQ * warp))
+      if (warp < t.y && !small_bwd_warp_multi<TL>(P.solveSmall[t.x + warp], P, Lx, Dpiv, y, flags, nflags, epoch, q,
+                                                  ns, status, msm + 32 * kMQ * warp))
         waitOk = 0;
       __syncthreads();
       return waitOk != 0;
     }
     const int s = t.x, blk = t.y;
     const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
+    const int vb = sl * kQS, qs = min(kQS, q - vb);
     const TL *Lp = Lx + P.snLxp[s];
     const int *rowsOf = P.Si + P.Sp[s];
     const int c0 = blk * kMB, w = min(kMB, nc - c0), nb = (nc + kMB - 1) / kMB;
-    int *myflags = flags + P.blkOff[s];
-    const int par = P.snParent[s];
-    if (par >= 0) {
-      if (tid == 0) waitOk = wait_flag(flags + P.blkOff[par], epoch, status, s, P.spin);
-      __syncthreads();
-      if (!waitOk) return false;
+    int *sflags = flags + (int64_t)sl * nflags;
+    int *myflags = sflags + P.blkOff[s];
+    {  // X^T: Xs[i][j] = X(j, i) = X[i w + j] ([m][k] with m = i), arriving while the task sums
+      const TL *X = Inv + P.invOff[P.blkOff[s] + blk];
+      for (int e = tid; e < kMB * kMB; e += kMultiThreads) {
+        const int j = e & (kMB - 1), i = e >> 6;
+        const bool ok = i < w && j < w;
+        cp_async_el(Xs + i * kLdX + j, ok ? X + (int64_t)i * w + j : X, (int)sizeof(TL), ok);
+      }
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
     }
-    double acc[4][4];
+    double c[2][4];
 #pragma unroll
-    for (int i = 0; i < 4; i++)
+    for (int nb2 = 0; nb2 < 2; nb2++)
 #pragma unroll
-      for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
-    // chunks: ancestors rows [nc, m) in kKC steps, then pivot blocks nb - 1 .. blk + 1 (two chunks each)
+      for (int v = 0; v < 4; v++) c[nb2][v] = 0.0;
+    // chunks: the rows below the supernode [nc, m) in kKC steps from the last down, then pivot blocks nb - 1 .. blk + 1
+    // (two chunks each)
     const int nanc = (m - nc + kKC - 1) / kKC;
     const int npiv = (nb - 1 - blk) * (kMB / kKC);
     const int nch = nanc + npiv;
-    // chunk ch -> first row and row count
     auto chunk = [&](int ch, int &rb, int &rw) {
       if (ch < nanc) {
-        rb = nc + ch * kKC;
+        rb = nc + (nanc - 1 - ch) * kKC;
         rw = min(kKC, m - rb);
       } else {
         const int p = ch - nanc, pb = nb - 1 - p / 2;  // pivot block, from the last down
@@ -272,13 +373,13 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_bwd_multi(const int4 *__re
         rw = max(0, min(kKC, nc - rb));
       }
     };
-    // L tile: As[rr][c] = L(rb + rr, c0 + c); elements e = tid + 256 u: rr = e & 31, c = e >> 5
+    // L chunk, [m][k]: As[cc][rr] = L(rb + rr, c0 + cc); elements e = tid + 256 u: rr = e & 31, cc = e >> 5
     TL lr[8];
     auto loadL = [&](int rb, int rw) {
 #pragma unroll
       for (int u = 0; u < 8; u++) {
-        const int e = tid + kMultiThreads * u, rr = e & (kKC - 1), c = e >> 5;
-        lr[u] = (rr < rw && c < w) ? Lp[(int64_t)(c0 + c) * m + rb + rr] : (TL)0;
+        const int e = tid + kMultiThreads * u, rr = e & (kKC - 1), cc = e >> 5;
+        lr[u] = (rr < rw && cc < w) ? Lp[(int64_t)(c0 + cc) * m + rb + rr] : (TL)0;
       }
     };
     int rb = 0, rw = 0;
@@ -288,24 +389,35 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_bwd_multi(const int4 *__re
     }
     for (int ch = 0; ch < nch; ch++) {
       const bool anc = ch < nanc;
-      if (!anc && ((ch - nanc) & 1) == 0) {  // first chunk of a pivot block: its x values final?
+      if (anc) {  // the ancestor blocks holding this chunk's rows final? (one lane per row, each distinct block once)
+        if (warp == 0) {
+          const int fb = lane < rw ? P.rowBlk[rowsOf[rb + lane]] : -1;
+          const int prev = __shfl_up_sync(0xffffffffu, fb, 1);
+          int ok = 1;
+          if (fb >= 0 && (lane == 0 || fb != prev)) ok = wait_flag(sflags + fb, epoch, status, s, P.spin);
+          ok = __all_sync(0xffffffffu, ok);
+          if (lane == 0) waitOk = ok;
+        }
+        __syncthreads();
+        if (!waitOk) return bail();
+      } else if (((ch - nanc) & 1) == 0) {  // first chunk of a pivot block: its x values final?
         if (tid == 0) waitOk = wait_flag(myflags + rb / kMB, epoch, status, s, P.spin);
         __syncthreads();
-        if (!waitOk) return false;
+        if (!waitOk) return bail();
       }
-      for (int e = tid; e < kKC * kMQ; e += kMultiThreads) {
-        const int rr = e >> 6, k = e & (kMQ - 1);
+      for (int e = tid; e < kKC * kQS; e += kMultiThreads) {
+        const int rr = e >> 4, n = e & (kQS - 1);
         double v = 0.0;
-        if (rr < rw && k < q) {
+        if (rr < rw && n < qs) {
           const int gi = anc ? rowsOf[rb + rr] : f + rb + rr;
-          v = __ldcg(y + (int64_t)gi * q + k);
+          v = __ldcg(y + (int64_t)gi * q + vb + n);
         }
-        Bs[rr * kLdt + k] = v;
+        Bs[rr * kLdB + n] = v;
       }
 #pragma unroll
       for (int u = 0; u < 8; u++) {
         const int e = tid + kMultiThreads * u;
-        As[(e & (kKC - 1)) * kLdt + (e >> 5)] = (double)lr[u];
+        As[(e >> 5) * kLdMK + (e & (kKC - 1))] = (double)lr[u];
       }
       __syncthreads();
       const int cw = rw;
@@ -313,47 +425,49 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_bwd_multi(const int4 *__re
         chunk(ch + 1, rb, rw);
         loadL(rb, rw);
       }
-      mm_tile(As, Bs, cw, ty, tx, acc);
+      if (16 * kh < cw) mma_k16<false>(As, kLdMK, Bs, 16 * kh, mw, lane, c);
       __syncthreads();
     }
+    halves_sum(c, As, warp, lane);
     // R = y[block] (/ D) - acc
+    if (warp < 4) {
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-      const int c = 4 * ty + i;
-      const double d = (Dpiv && c < w) ? Dpiv[f + c0 + c] : 1.0;
+      for (int nb2 = 0; nb2 < 2; nb2++)
 #pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const int k = 4 * tx + j;
-        double v = 0.0;
-        if (c < w && k < q) {
-          const double yv = y[(int64_t)(f + c0 + c) * q + k];
-          v = (Dpiv ? yv / d : yv) - acc[i][j];  // LDL^T: y /= D before the backward sweep (ldlt.mjs:629)
+        for (int v = 0; v < 4; v++) {
+          const int cc = acc_row(warp, lane, v), n = acc_vec(lane, nb2, v);
+          double r = 0.0;
+          if (cc < w && n < qs) {
+            const double yv = y[(int64_t)(f + c0 + cc) * q + vb + n];
+            r = (Dpiv ? yv / Dpiv[f + c0 + cc] : yv) - c[nb2][v];  // LDL^T: y /= D before the backward sweep (ldlt.mjs:629)
+          }
+          Rs[cc * kLdB + n] = r;
+          c[nb2][v] = 0.0;
         }
-        Rs[c * kLdt + k] = v;
-        acc[i][j] = 0.0;
-      }
     }
-    // x[block] = X^T R: As[jj][i] = X(jb + jj, i) = Inv[i w + jb + jj]
-    const TL *X = Inv + P.invOff[P.blkOff[s] + blk];
-    for (int jb = 0; jb < w; jb += kKC) {
-      const int jw = min(kKC, w - jb);
-      __syncthreads();
-      for (int e = tid; e < kKC * kMB; e += kMultiThreads) {
-        const int jj = e & (kKC - 1), i = e >> 5;
-        As[jj * kLdt + i] = (i < w && jj < jw) ? (double)X[(int64_t)i * w + jb + jj] : 0.0;
-      }
-      __syncthreads();
-      mm_tile(As, Rs + jb * kLdt, jw, ty, tx, acc);
+    if (warp >= 4) {
+#pragma unroll
+      for (int nb2 = 0; nb2 < 2; nb2++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) c[nb2][v] = 0.0;
     }
+    cp_async_all();
+    __syncthreads();
+    // x[block] = X^T R
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-      const int c = 4 * ty + i;
-      if (c >= w) continue;
+    for (int h = 0; h < 2; h++) {
+      const int k0 = 32 * h + 16 * kh;
+      if (k0 < w) mma_k16<false>(Xs, kLdX, Rs, k0, mw, lane, c);
+    }
+    halves_sum(c, As, warp, lane);
+    if (warp < 4) {
 #pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const int k = 4 * tx + j;
-        if (k < q) y[(int64_t)(f + c0 + c) * q + k] = acc[i][j];
-      }
+      for (int nb2 = 0; nb2 < 2; nb2++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+          const int cc = acc_row(warp, lane, v), n = acc_vec(lane, nb2, v);
+          if (cc < w && n < qs) y[(int64_t)(f + c0 + cc) * q + vb + n] = c[nb2][v];
+        }
     }
     __syncthreads();
     if (tid == 0) st_release(myflags + blk, epoch);
@@ -483,33 +597,40 @@ __global__ void __launch_bounds__(256) k_residual_multi(int n, const int *__rest
   }
 }
 
-cudaError_t init_solve_multi_attributes() {
-  cudaError_t e = cudaFuncSetAttribute(k_fwd_multi<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMultiSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fwd_multi<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMultiSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_bwd_multi<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMultiSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_bwd_multi<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMultiSmem);
+template <class TL>
+static cudaError_t set_multi_smem() {
+  cudaError_t e = cudaFuncSetAttribute(k_fwd_multi<TL>, cudaFuncAttributeMaxDynamicSharedMemorySize, multi_smem<TL>());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_bwd_multi<TL>, cudaFuncAttributeMaxDynamicSharedMemorySize, multi_smem<TL>());
   return e;
+}
+cudaError_t init_solve_multi_attributes() {
+  cudaError_t e = set_multi_smem<double>();
+  return e == cudaSuccess ? set_multi_smem<float>() : e;
 }
 
 int num_sms();
 int multi_max_vectors() { return kMQ; }
-static int multi_grid(int ntasks) { return ntasks < 3 * num_sms() ? ntasks : 3 * num_sms(); }
+int multi_slices(int q) { return (q + kQS - 1) / kQS; }
+static int multi_grid(int64_t ntasks) { return ntasks < 3 * num_sms() ? (int)ntasks : 3 * num_sms(); }
 
 template <class TL>
 void launch_fwd_multi(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
-                      double *y, double *V, double *T, int *flags, int epoch, int *done, int q,
+                      double *y, double *V, double *T, int *flags, int nflags, int epoch, int *done, int q,
                       unsigned long long *status, cudaStream_t st) {
+  const int ns = multi_slices(q);
   if (ntasks > 0)
-    k_fwd_multi<TL><<<multi_grid(ntasks), kMultiThreads, kMultiSmem, st>>>(tasks, ntasks, ticket, P, Lx, Inv, y, V, T,
-                                                                          flags, epoch, done, q, status);
+    k_fwd_multi<TL><<<multi_grid((int64_t)ntasks * ns), kMultiThreads, multi_smem<TL>(), st>>>(
+        tasks, ntasks * ns, ns, ticket, P, Lx, Inv, y, V, T, flags, nflags, epoch, done, q, status);
 }
 template <class TL>
 void launch_bwd_multi(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
-                      const double *Dpiv, double *y, int *flags, int epoch, int q, unsigned long long *status,
-                      cudaStream_t st) {
+                      const double *Dpiv, double *y, int *flags, int nflags, int epoch, int q,
+                      unsigned long long *status, cudaStream_t st) {
+  const int ns = multi_slices(q);
   if (ntasks > 0)
-    k_bwd_multi<TL><<<multi_grid(ntasks), kMultiThreads, kMultiSmem, st>>>(tasks, ntasks, ticket, P, Lx, Inv, Dpiv, y,
-                                                                          flags, epoch, q, status);
+    k_bwd_multi<TL><<<multi_grid((int64_t)ntasks * ns), kMultiThreads, multi_smem<TL>(), st>>>(
+        tasks, ntasks * ns, ns, ticket, P, Lx, Inv, Dpiv, y, flags, nflags, epoch, q, status);
 }
 void launch_to_interleaved(const double *B, double *Yil, int n, int q, cudaStream_t st) {
   if (n > 0 && q > 0) k_to_interleaved<<<dim3((n + 31) / 32, (q + 31) / 32), dim3(32, 8), 0, st>>>(B, Yil, n, q);
@@ -529,14 +650,16 @@ void launch_residual_multi(int n, const int *rowptr, const int *colidx, const do
   k_residual_multi<<<grid, 256, 0, st>>>(n, rowptr, colidx, val, x, b, r, norms, q, rowGroup);
 }
 template void launch_fwd_multi<double>(const int4 *, int, int *, const DevPlan &, const double *, const double *,
-                                       double *, double *, double *, int *, int, int *, int, unsigned long long *,
+                                       double *, double *, double *, int *, int, int, int *, int, unsigned long long *,
                                        cudaStream_t);
 template void launch_fwd_multi<float>(const int4 *, int, int *, const DevPlan &, const float *, const float *,
-                                      double *, double *, double *, int *, int, int *, int, unsigned long long *,
+                                      double *, double *, double *, int *, int, int, int *, int, unsigned long long *,
                                       cudaStream_t);
 template void launch_bwd_multi<double>(const int4 *, int, int *, const DevPlan &, const double *, const double *,
-                                       const double *, double *, int *, int, int, unsigned long long *, cudaStream_t);
+                                       const double *, double *, int *, int, int, int, unsigned long long *,
+                                       cudaStream_t);
 template void launch_bwd_multi<float>(const int4 *, int, int *, const DevPlan &, const float *, const float *,
-                                      const double *, double *, int *, int, int, unsigned long long *, cudaStream_t);
+                                      const double *, double *, int *, int, int, int, unsigned long long *,
+                                      cudaStream_t);
 
 }  // namespace amp

@@ -108,12 +108,14 @@ __device__ bool small_bwd_warp(int s, const DevPlan &P, const TL *__restrict__ L
 // Vs: the warp's 32 x 64 doubles of shared memory, row r of the front vectors at Vs[64 r + k]
 template <class TL>
 __device__ bool small_fwd_warp_multi(int s, const DevPlan &P, const TL *__restrict__ Lx, double *__restrict__ y,
-                                     double *__restrict__ T, int *done, int q, unsigned long long *status, double *Vs) {
+                                     double *__restrict__ T, int *done, int q, int ns, unsigned long long *status,
+                                     double *Vs) {
   const int lane = threadIdx.x & 31;
   const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
   const int k0 = lane, k1 = lane + 32;
   const bool v0 = k0 < q, v1 = k1 < q;
-  if (!warp_wait_children(P, s, done, status)) return false;
+  for (int sl = 0; sl < ns; sl++)  // every vector slice of the children done
+    if (!warp_wait_children(P, s, done + (int64_t)sl * P.nsuper, status)) return false;
   for (int r = 0; r < m; r++) {
     if (v0) Vs[64 * r + k0] = r < nc ? y[(int64_t)(f + r) * q + k0] : 0.0;
     if (v1) Vs[64 * r + k1] = r < nc ? y[(int64_t)(f + r) * q + k1] : 0.0;
@@ -151,20 +153,22 @@ __device__ bool small_fwd_warp_multi(int s, const DevPlan &P, const TL *__restri
     if (v1) dst[k1] = Vs[64 * r + k1];
   }
   __syncwarp();
-  if (lane == 0) red_release_add(done + s, 1);
+  if (lane < ns) red_release_add(done + (int64_t)lane * P.nsuper + s, 1);  // one count per vector slice
   return true;
 }
 
 template <class TL>
 __device__ bool small_bwd_warp_multi(int s, const DevPlan &P, const TL *__restrict__ Lx,
-                                     const double *__restrict__ Dpiv, double *__restrict__ y, int *flags, int epoch,
-                                     int q, unsigned long long *status, double *Vs) {
+                                     const double *__restrict__ Dpiv, double *__restrict__ y, int *flags, int nflags,
+                                     int epoch, int q, int ns, unsigned long long *status, double *Vs) {
   const int lane = threadIdx.x & 31;
   const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
   const int k0 = lane, k1 = lane + 32;
   const bool v0 = k0 < q, v1 = k1 < q;
   const int par = P.snParent[s];
-  if (par >= 0 && m > nc && !warp_wait(flags + P.blkOff[par], epoch, true, status, s, P.spin)) return false;
+  if (par >= 0 && m > nc)
+    for (int sl = 0; sl < ns; sl++)  // the parent's every vector slice final
+      if (!warp_wait(flags + (int64_t)sl * nflags + P.blkOff[par], epoch, true, status, s, P.spin)) return false;
   const int *rowsOf = P.Si + P.Sp[s];
   for (int r = 0; r < m; r++) {
     const int64_t gi = r < nc ? f + r : rowsOf[r];
@@ -199,7 +203,7 @@ __device__ bool small_bwd_warp_multi(int s, const DevPlan &P, const TL *__restri
     if (v1) y[(int64_t)(f + r) * q + k1] = Vs[64 * r + k1];
   }
   __syncwarp();
-  if (lane == 0) st_release(flags + P.blkOff[s], epoch);
+  if (lane < ns) st_release(flags + (int64_t)lane * nflags + P.blkOff[s], epoch);  // one flag per vector slice
   return true;
 }
 

@@ -335,6 +335,9 @@ void build_plan(const Symbolic &S, Plan &P, const Tuning &tune) {
   P.blkOff.assign(ns + 1, 0);
   for (int s = 0; s < ns; s++) P.blkOff[s + 1] = P.blkOff[s] + (P.snNc[s] + B - 1) / B;
   P.nflags = P.blkOff[ns];
+  P.rowBlk.assign(S.n, 0);
+  for (int s = 0; s < ns; s++)
+    for (int c = 0; c < P.snNc[s]; c++) P.rowBlk[P.snF[s] + c] = P.blkOff[s] + c / B;
   P.diagSlot.clear();
   for (int j = 0; j < S.n; j++)
     for (int p = S.lowerP[j]; p < S.lowerP[j + 1]; p++)

@@ -135,6 +135,7 @@ struct Plan {
   std::vector<int64_t> snTOff;      // offset of supernode s's forward update vector (per RHS)
   // block tasks of the solves ({supernode, block, kind, 0}); ready flags per 64-row pivot block
   std::vector<int> blkOff;          // first flag of supernode s
+  std::vector<int> rowBlk;          // flag (64-column diagonal block) holding each column, permuted order (n)
   int nflags = 0;
   std::vector<int64_t> invOff;      // per diagonal block (flag index): offset of its w x w inverse; [nflags] = total
   std::vector<int> diagSlot;        // CSR slot of each diagonal entry of A (LDL^T pivot scale)
