@@ -96,7 +96,6 @@ void set_last_error(const std::string &msg) { g_err = msg; }
 namespace {
 // elements of the diagonal-block inverses (none for an empty pattern, whose plan has no per-block arrays)
 // chain-matrix slots: nb - 1 per supernode with nb diagonal blocks, 64 x 64 each
-constexpr int kSlices = 4;  // vector slices of the multi-vector sweeps: multi_max_vectors() / 16
 size_t chain_elems(const amp::Plan &P) { return (size_t)std::max(0, P.nflags - P.nsuper) * 64 * 64; }
 
 int64_t inv_elems(const amp::Plan &P) { return P.invOff.empty() ? 0 : P.invOff[P.nflags]; }
@@ -145,6 +144,8 @@ std::vector<CUtensorMap> split_tensor_maps(const amp::Plan &P, const __nv_bfloat
 }
 }  // namespace
 
+constexpr int kSlices = 4;  // vector slices of the multi-vector sweeps: multi_max_vectors() / 16
+
 struct amp_plan_s {
   amp::Symbolic S;
   amp::Plan P;
@@ -159,6 +160,11 @@ struct amp_plan_s {
   amp::MixTask *dMixTile = nullptr, *dMixU = nullptr;
   int4 *dFwdTasks = nullptr, *dBwdTasks = nullptr, *dBwdAll = nullptr;
   int4 *dFwdTasks1 = nullptr;  // the one-vector forward's list (with whole-supernode tasks)
+  // the multi-vector lists with every block task expanded into ns vector slices, built on first use (index ns - 1)
+  int4 *dFwdSl[kSlices] = {}, *dBwdSl[kSlices] = {};
+  int nFwdSl[kSlices] = {}, nBwdSl[kSlices] = {};
+  bool wideSl[kSlices] = {};  // the list holds all-vector tasks (.w = -1)
+  std::mutex slMu;
   int *dTinySn = nullptr, *dSmallSn = nullptr;  // small fronts per level (whole fronts by one warp / one CTA)
   int2 *dChain = nullptr;                        // chain-matrix tasks {s, b}
   int *dInvBlocks = nullptr;                     // diagonal blocks whose inverses the solves use
@@ -593,6 +599,47 @@ void device_solve(amp_factor *f, const double *dB, double *dX) {
 }
 
 // ---- several right-hand sides: groups of up to multi_max_vectors() vectors, interleaved ([i q + k]) -------------
+// The multi-vector task lists for ns vector slices: a block task (kind 0 / 1) is expanded into ns consecutive entries
+// with .w = the slice (the slices' chains run on different CTAs); the small-supernode tasks (kind 2) stay single.
+// When supernodes with at most kWideBlocks pivot blocks hold at least half of L (a plan of many small systems, like
+// the batch) and there are two or more slices, those supernodes' tasks stay single with .w = -1
+// and move all vectors at once (no chain to split, one pass over the L tile, a quarter of the tasks). Built and
+// uploaded once per plan and ns.
+constexpr int kWideBlocks = 2;
+static std::vector<int> expand_slices(const amp::Plan &P, const std::vector<int> &tasks, size_t ntasks, int ns,
+                                      bool wide) {
+  std::vector<int> out;
+  out.reserve(4 * ntasks * (size_t)ns);
+  for (size_t i = 0; i < ntasks; i++) {
+    const int *t = &tasks[4 * i];
+    if (t[2] == 2 || (wide && (P.snNc[t[0]] + 63) / 64 <= kWideBlocks)) {
+      out.insert(out.end(), {t[0], t[1], t[2], t[2] == 2 ? 0 : -1});
+      continue;
+    }
+    for (int sl = 0; sl < ns; sl++) out.insert(out.end(), {t[0], t[1], t[2], sl});
+  }
+  return out;
+}
+static void slice_lists(amp_plan *pl, int ns) {
+  std::lock_guard<std::mutex> lock(pl->slMu);
+  if (pl->dFwdSl[ns - 1]) return;
+  const amp::Plan &P = pl->P;
+  const size_t nf = (size_t)P.fwdLvlPtr[P.nlevels];
+  double lAll = 0, lSmall = 0;  // L entries (nc m per supernode): all, and in supernodes of few pivot blocks
+  for (int sn = 0; sn < P.nsuper; sn++) {
+    const double e = (double)P.snNc[sn] * P.snM[sn];
+    lAll += e;
+    if ((P.snNc[sn] + 63) / 64 <= kWideBlocks) lSmall += e;
+  }
+  const bool wide = ns > 1 && lAll > 0 && 2 * lSmall >= lAll;
+  const std::vector<int> fw = expand_slices(P, P.fwdTasks, nf, ns, wide);
+  const std::vector<int> bw = expand_slices(P, P.bwdAll, P.bwdAll.size() / 4, ns, wide);
+  pl->wideSl[ns - 1] = wide;
+  pl->dBwdSl[ns - 1] = (int4 *)pl->mem.upload(bw);
+  pl->nBwdSl[ns - 1] = (int)(bw.size() / 4);
+  pl->nFwdSl[ns - 1] = (int)(fw.size() / 4);
+  pl->dFwdSl[ns - 1] = (int4 *)pl->mem.upload(fw);
+}
 // y (permuted order, interleaved) := A^-1 y in place
 void device_solve_multi_permuted(amp_factor *f, int q) {
   const amp::Plan &P = f->plan->P;
@@ -605,23 +652,27 @@ void device_solve_multi_permuted(amp_factor *f, int q) {
   ck(cudaMemsetAsync(f->dDone, 0, sizeof(int) * kSlices * std::max(1, P.nsuper), st), "memset done");
   ck(cudaMemsetAsync(f->dSolveStatus, 0xff, sizeof(unsigned long long), st), "memset status");
   const int efwd = 2 * (++f->solveEpoch) - 1, ebwd = 2 * f->solveEpoch;
-  const int nf = P.fwdLvlPtr[P.nlevels], nb = (int)(P.bwdAll.size() / 4);
+  const int ns = amp::multi_slices(q);
+  slice_lists(f->plan, ns);
+  const int nf = f->plan->nFwdSl[ns - 1], nb = f->plan->nBwdSl[ns - 1];
+  int4 *fwdTasks = f->plan->dFwdSl[ns - 1], *bwdTasks = f->plan->dBwdSl[ns - 1];
+  const bool wide = f->plan->wideSl[ns - 1];
   const double *Dp = f->kind == AMP_LDLT ? f->dD : nullptr;
   timed(f, K_FORWARD, flops, lbytes, [&] {
     if (f->dL32)
-      amp::launch_fwd_multi<float>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->dL32, f->dInv32, f->dY, f->dV, f->dT,
-                                   f->dFlags, nfl, efwd, f->dDone, q, f->dSolveStatus, st);
+      amp::launch_fwd_multi<float>(fwdTasks, nf, wide, f->dTickets, dp, f->dL32, f->dInv32, f->dY, f->dV, f->dT, f->dFlags,
+                                   nfl, efwd, f->dDone, q, f->dSolveStatus, st);
     else
-      amp::launch_fwd_multi<double>(f->plan->dFwdTasks, nf, f->dTickets, dp, f->dLx, f->dInv, f->dY, f->dV, f->dT,
-                                    f->dFlags, nfl, efwd, f->dDone, q, f->dSolveStatus, st);
+      amp::launch_fwd_multi<double>(fwdTasks, nf, wide, f->dTickets, dp, f->dLx, f->dInv, f->dY, f->dV, f->dT, f->dFlags,
+                                    nfl, efwd, f->dDone, q, f->dSolveStatus, st);
   });
   timed(f, K_BACKWARD, flops, lbytes, [&] {
     if (f->dL32)
-      amp::launch_bwd_multi<float>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dL32, f->dInv32, Dp, f->dY,
-                                   f->dFlags, nfl, ebwd, q, f->dSolveStatus, st);
+      amp::launch_bwd_multi<float>(bwdTasks, nb, wide, f->dTickets + 1, dp, f->dL32, f->dInv32, Dp, f->dY, f->dFlags, nfl,
+                                   ebwd, q, f->dSolveStatus, st);
     else
-      amp::launch_bwd_multi<double>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dLx, f->dInv, Dp, f->dY, f->dFlags,
-                                    nfl, ebwd, q, f->dSolveStatus, st);
+      amp::launch_bwd_multi<double>(bwdTasks, nb, wide, f->dTickets + 1, dp, f->dLx, f->dInv, Dp, f->dY, f->dFlags, nfl,
+                                    ebwd, q, f->dSolveStatus, st);
   });
 }
 

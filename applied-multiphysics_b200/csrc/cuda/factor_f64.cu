@@ -396,39 +396,42 @@ __device__ bool potrf_block(const T *src, int lds, T *Lp, int m, int w, int f, i
 // M(k, k) = d_k, x = L21, and w = x D = L21 D (the update's A operand, written to ld.W for the FP64 factor). The rows
 // are also written as BF16 hi / lo pairs (hi = bf16(x), lo = bf16(x - hi)) into the split columns of the tensor-core
 // update (mixed precision). The pivot block and D come from another CTA of the launch: read through L2 (__ldcg).
+// x: this thread's 16 entries of its row (row r0 + tid % 64, columns c0 + 16 (tid / 64) + u), loaded by the caller
+// before it waited for the pivot block (the strip's own rows are final by then).
 // On return Ws[c][r] holds this strip's update operand (x, or x D for LDL^T) and M[c][r] the solved rows x
 // (c < w, r < r1 - r0; zero elsewhere): a diagonal strip's X_c for its own column block.
 template <class T>
 __device__ void trsm_strip(T *L, int m, int f, int c0, int w, int r0, int r1, int64_t lxp, int64_t sp,
                            __nv_bfloat16 *Shi, __nv_bfloat16 *Slo, const LdltArgs<T> &ld, T (*M)[kPanel + 1],
-                           T (*Ws)[kPanel + 1], T *invd, T *dv) {
+                           T (*Ws)[kPanel + 1], T *invd, T *dv, T (&x)[16]) {
   const bool ldlt = ld.scal != nullptr;
   const int tid = threadIdx.x, r = tid & (kPanel - 1), q = tid >> 6;
-  if (tid < kPanel) {
-    const T d = tid < w ? (ldlt ? (T)ldcg_v(ld.D + f + c0 + tid) : ldcg_v(L + (int64_t)(c0 + tid) * m + c0 + tid))
-                        : T(1);
-    dv[tid] = d;
-    invd[tid] = T(1) / d;
-  }
-  __syncthreads();
-  {  // the pivot block: thread (r, q) loads row r of columns 16 q .. 16 q + 15
+  {  // the pivot block: thread (r, q) loads row r of columns 16 q .. 16 q + 15 (times their pivots for LDL^T), and
+     // thread r < 64 the pivot of column r, in one round trip
     T v[16];
 #pragma unroll
     for (int u = 0; u < 16; u++) {
       const int c = 16 * q + u;
       v[u] = (r < w && c < r) ? ldcg_v(L + (int64_t)(c0 + c) * m + c0 + r) : T(0);
     }
+    if (ldlt) {
 #pragma unroll
-    for (int u = 0; u < 16; u++) M[r][16 * q + u] = ldlt ? v[u] * dv[16 * q + u] : v[u];
+      for (int u = 0; u < 16; u++) {
+        const int c = 16 * q + u;
+        v[u] = v[u] * (c < w ? (T)ldcg_v(ld.D + f + c0 + c) : T(1));
+      }
+    }
+    if (tid < kPanel) {
+      const T d = tid < w ? (ldlt ? (T)ldcg_v(ld.D + f + c0 + tid) : ldcg_v(L + (int64_t)(c0 + tid) * m + c0 + tid))
+                          : T(1);
+      dv[tid] = d;
+      invd[tid] = T(1) / d;
+    }
+#pragma unroll
+    for (int u = 0; u < 16; u++) M[r][16 * q + u] = v[u];
   }
   const int row = r0 + r;
   const bool active = row < r1;
-  T x[16];
-#pragma unroll
-  for (int u = 0; u < 16; u++) {
-    const int c = 16 * q + u;
-    x[u] = active && c < w ? L[(int64_t)(c0 + c) * m + row] : T(0);
-  }
   __syncthreads();
   for (int p = 0; p < 4; p++) {
     if (q == p) {  // solve this quarter
@@ -565,8 +568,17 @@ __global__ void __launch_bounds__(256, group_min_blocks<T>()) k_group_panel(cons
   }
   for (int b = 0; b < bmax; b++) {
     const int c0 = g0 + b * kPanel, w = min(kPanel, g1 - c0), c1 = c0 + w;
+    T x[16];  // this thread's part of the strip's rows of block b, loaded while the pivot block is not yet ready
+    {
+      const int xr = r0 + (tid & (kPanel - 1)), xq = tid >> 6;
+#pragma unroll
+      for (int u = 0; u < 16; u++) {
+        const int c = 16 * xq + u;
+        x[u] = xr < r1 && c < w ? L[(int64_t)(c0 + c) * m + xr] : T(0);
+      }
+    }
     if (!panel_wait(Pf + b, 1, status, P.spin)) return;
-    trsm_strip<T>(L, m, f, c0, w, r0, r1, P.snLxp[s], P.snSp[s], Shi, Slo, ld, M, Ws, invd, dv);
+    trsm_strip<T>(L, m, f, c0, w, r0, r1, P.snLxp[s], P.snSp[s], Shi, Slo, ld, M, Ws, invd, dv, x);
     if (jd >= 0) panel_release(Df + jd, b + 1);
     // Update with block b (C -= W_r X_c^T, K = w): a diagonal strip first its own pivot block (X_c = its solved rows,
     // left in M by the TRSM; into Ds), then the blocks between block b and its own; a strip below every remaining

@@ -59,15 +59,18 @@ void launch_chain_mats(const int2 *tasks, int ntasks, const DevPlan &P, const TL
 // several right-hand sides (q <= multi_max_vectors(), interleaved: entry i of vector k at [i q + k])
 // Vectors move in slices of 16, each with its own ready flags (flags[slice * nflags + block], nflags >= the plan's
 // flag count) and done counters (done[slice * nsuper + s]): the flag and done arrays hold multi_max_vectors() / 16
-// sets.
+// sets. tasks: the plan's list with block tasks expanded into multi_slices(q) consecutive entries (.w = the slice), or
+// left single with .w = -1 (the task moves every vector at once).
 int multi_max_vectors();
+int multi_slices(int q);
+// wide: the list holds .w = -1 tasks (the kernels with the all-vector path)
 template <class TL>
-void launch_fwd_multi(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
-                      double *y, double *V, double *T, int *flags, int nflags, int epoch, int *done, int q,
-                      unsigned long long *status, cudaStream_t st);
+void launch_fwd_multi(const int4 *tasks, int ntasks, bool wide, int *ticket, const DevPlan &P, const TL *Lx,
+                      const TL *Inv, double *y, double *V, double *T, int *flags, int nflags, int epoch, int *done,
+                      int q, unsigned long long *status, cudaStream_t st);
 template <class TL>
-void launch_bwd_multi(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
-                      const double *Dpiv, double *y, int *flags, int nflags, int epoch, int q,
+void launch_bwd_multi(const int4 *tasks, int ntasks, bool wide, int *ticket, const DevPlan &P, const TL *Lx,
+                      const TL *Inv, const double *Dpiv, double *y, int *flags, int nflags, int epoch, int q,
                       unsigned long long *status, cudaStream_t st);
 void launch_to_interleaved(const double *B, double *Yil, int n, int q, cudaStream_t st);
 void launch_from_interleaved(const double *Xil, double *X, int n, int q, cudaStream_t st);

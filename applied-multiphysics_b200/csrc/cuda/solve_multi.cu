@@ -6,11 +6,14 @@
 // buffers T), so a row of the solution is q contiguous doubles and the gathers through the extend-add maps and the
 // row lists move whole rows.
 //
-// Vector slices: task t of the launch is list entry t / ns for vector slice t % ns (ns = ceil(q / 16)), with its own
-// ready flags (flags[slice * nflags + block]) and done counters (done[slice * nsuper + s]), so the slices of a
-// supernode run as independent dependency chains on different CTAs and a task never computes on absent vectors. The
-// expanded order keeps every wait on a task with a smaller ticket. The small supernodes (kind 2, one warp each) solve
-// all q vectors in the task of slice 0 and count/release every slice.
+// Vector slices of 16 (ns = ceil(q / 16)), each with its own ready flags (flags[slice * nflags + block]) and done
+// counters (done[slice * nsuper + s]): the host expands the block tasks of supernodes with several pivot blocks into
+// ns consecutive tasks, one per slice (int4 .w = the slice), so the slices' dependency chains run on different CTAs;
+// a task with .w = -1 (a supernode of few pivot blocks) moves all vectors at once (below; compiled into the sweeps of
+// the WIDE instantiation only, which the host launches for plans made mostly of such supernodes: the all-vector path
+// holds more registers, and in the same kernel the sliced tasks would spill). The expanded order keeps every wait on a
+// task with a smaller ticket, and a task never computes on absent vectors. The small supernodes (kind 2, one warp
+// each, not expanded) solve all q vectors and count/release every slice.
 //
 // A task is a small GEMM on the FP64 tensor cores (mma.sync m16n8k16): out (64 rows x 16 vectors) = sum over a
 // reduction index of A (64 x 32 chunk, FP32 factors widened on the shared-memory store) times B (32 x 16), 8 warps
@@ -43,13 +46,16 @@ constexpr int kLdMK = kKC + 4;       // A chunk stored [m][k]: 36
 constexpr int kLdX = kMB + 4;        // inverse block stored [k][m] or [m][k], 64 x 64: 68
 constexpr int kLdB = kQS + 4;        // B stored [k][n]: 20
 constexpr int kMultiThreads = 256;
+constexpr int kMultiCtas = 3;      // resident CTAs per SM of the persistent sweeps (registers capped at 80)
 constexpr int kAElems = kMB * kLdMK;  // >= kKC * kLdKM; also the halves' reduction buffer (64 x 17)
 static_assert(kAElems >= kKC * kLdKM && kAElems >= kMB * (kQS + 1), "A tile buffer");
 template <class TL>
 constexpr int multi_smem() {
-  const int own = (kAElems + kKC * kLdB + kMB * kLdB) * (int)sizeof(double) + kMB * kLdX * (int)sizeof(TL);
+  const int own = (kAElems + 2 * kMB * kLdB) * (int)sizeof(double) + kMB * kLdX * (int)sizeof(TL);
   const int small = kSolveGroup * 32 * kMQ * (int)sizeof(double);  // kind 2 tasks: 32 x 64 front vectors per warp
-  return own > small ? own : small;
+  const int wide = (2 * 32 + kMB) * 66 * (int)sizeof(double);        // all-vector tasks (kWideSmem)
+  const int m1 = own > small ? own : small;
+  return m1 > wide ? m1 : wide;
 }
 
 __device__ __forceinline__ void dmma16816(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
@@ -133,11 +139,306 @@ __device__ __forceinline__ void ticket_loop(int *ticket, int ntasks, Run &&run) 
   }
 }
 
+// ---- tasks of supernodes with few pivot blocks: all q vectors at once on the CUDA cores ----------------------------
+// A task of a supernode with at most two pivot blocks (list entry .w = -1) moves all q <= 64 vectors together: out
+// (64 rows x 64 vectors) = sum of A (64 x 32 L chunk) times B (32 x 64 vector chunk), both in shared memory, each
+// thread accumulating a 4 x 4 register tile in FP64. Such a task has no chain worth splitting, and one pass over
+// its L tile serves every vector. It waits for every slice of what another supernode provides (children's counts,
+// the parent's flag) and releases every slice of its own flags and counts.
+constexpr int kWKC = 32;  // reduction chunk
+constexpr int kWLd = 66;  // shared tile row stride in doubles (even: 16-byte aligned double2 reads)
+constexpr int kWideSmem = (2 * kWKC + kMB) * kWLd * (int)sizeof(double);
+// acc[i][j] += sum over kk < kc of A[kk][4 ty + i] B[kk][4 tx + j]
+__device__ __forceinline__ void mm_tile_w(const double *__restrict__ A, const double *__restrict__ B, int kc, int ty,
+                                          int tx, double (&acc)[4][4]) {
+#pragma unroll 4
+  for (int kk = 0; kk < kc; kk++) {
+    const double2 a0 = *reinterpret_cast<const double2 *>(A + kk * kWLd + 4 * ty);
+    const double2 a1 = *reinterpret_cast<const double2 *>(A + kk * kWLd + 4 * ty + 2);
+    const double2 b0 = *reinterpret_cast<const double2 *>(B + kk * kWLd + 4 * tx);
+    const double2 b1 = *reinterpret_cast<const double2 *>(B + kk * kWLd + 4 * tx + 2);
+    const double a[4] = {a0.x, a0.y, a1.x, a1.y}, b[4] = {b0.x, b0.y, b1.x, b1.y};
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+  }
+}
+
+// forward: as the sliced task (diagonal y[block] = X (V[block] - L[block, 0:blk 64] y), below T[block] = V[block] -
+// L[block, 0:nc] y), every vector
+template <class TL>
+__device__ __forceinline__ bool fwd_wide_task(const int4 t, const DevPlan &P, const TL *__restrict__ Lx, const TL *__restrict__ Inv,
+                              double *__restrict__ y, double *__restrict__ V, double *__restrict__ T, int *flags,
+                              int nflags, int epoch, int *done, int q, int ns, unsigned long long *status,
+                              double *msm, int &waitOk) {
+  double *As = msm, *Bs = msm + kWKC * kWLd, *Rs = msm + 2 * kWKC * kWLd;
+  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  const int s = t.x, blk = t.y, below = t.z;
+  const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s], mu = m - nc;
+  const TL *Lp = Lx + P.snLxp[s];
+  const int r0 = below ? nc + blk * kMB : blk * kMB;
+  const int rows = below ? min(kMB, mu - blk * kMB) : min(kMB, nc - blk * kMB);
+  const int ncols = below ? nc : blk * kMB;
+  int *myflags = flags + P.blkOff[s];  // the slice-0 set: this supernode releases every slice at once
+  const int64_t vbase = (int64_t)P.Sp[s];
+  if (!below && blk == 0) {
+    for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
+      const int c = P.chList[qq];
+      const int need = (P.snM[c] - P.snNc[c] + kMB - 1) / kMB;
+      if (tid == 0) {  // every vector slice of the child done
+        waitOk = 1;
+        for (int sl = 0; sl < ns && waitOk; sl++)
+          waitOk = wait_count(done + (int64_t)sl * P.nsuper + c, need, status, s, P.spin);
+      }
+      __syncthreads();
+      if (!waitOk) return false;
+    }
+    // v_s = [y(f .. f + nc); 0] + the children's pass-up vectors in the reference's child order
+    for (int64_t e = tid; e < (int64_t)m * q; e += kMultiThreads) {
+      const int r = (int)(e / q), k = (int)(e - (int64_t)r * q);
+      V[(vbase + r) * q + k] = r < nc ? y[(int64_t)(f + r) * q + k] : 0.0;
+    }
+    __syncthreads();
+    for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
+      const int c = P.chList[qq];
+      const int muc = P.snM[c] - P.snNc[c];
+      const int *map = P.eaMap + P.eaPtr[c];
+      const double *tc = T + P.snTOff[c] * q;
+      for (int64_t e = tid; e < (int64_t)muc * q; e += kMultiThreads) {
+        const int a = (int)(e / q), k = (int)(e - (int64_t)a * q);
+        V[(vbase + map[a]) * q + k] += __ldcg(tc + e);
+      }
+      __syncthreads();
+    }
+  }
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
+  // L tile of a chunk: As[c][row] = L(r0 + row, cb + c); thread elements e = tid + 256 u: row = e & 63, c = e >> 6
+  TL lr[8];
+  auto loadL = [&](int cb) {
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int e = tid + kMultiThreads * u, row = e & (kMB - 1), c = e >> 6;
+      lr[u] = (row < rows && cb + c < ncols) ? Lp[(int64_t)(cb + c) * m + r0 + row] : (TL)0;
+    }
+  };
+  const int nch = (ncols + kWKC - 1) / kWKC;
+  if (nch > 0) loadL(0);
+  for (int ch = 0; ch < nch; ch++) {
+    const int cb = ch * kWKC, cw = min(kWKC, ncols - cb);
+    if ((cb & (kMB - 1)) == 0) {  // first chunk of a pivot block: its y values final?
+      if (tid == 0) waitOk = wait_flag(myflags + cb / kMB, epoch, status, s, P.spin);
+      __syncthreads();
+      if (!waitOk) return false;
+    }
+    for (int e = tid; e < kWKC * kMQ; e += kMultiThreads) {
+      const int c = e >> 6, k = e & (kMQ - 1);
+      Bs[c * kWLd + k] = (c < cw && k < q) ? __ldcg(y + (int64_t)(f + cb + c) * q + k) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int e = tid + kMultiThreads * u;
+      As[(e >> 6) * kWLd + (e & (kMB - 1))] = (double)lr[u];
+    }
+    __syncthreads();
+    if (ch + 1 < nch) loadL(cb + kWKC);
+    mm_tile_w(As, Bs, cw, ty, tx, acc);
+    __syncthreads();
+  }
+  // R = V[block] - acc (V final once the supernode's first diagonal block is: waited above, or gathered here)
+  if (below) {
+    double *to = T + (P.snTOff[s] + (int64_t)blk * kMB) * q;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int row = 4 * ty + i;
+      if (row >= rows) continue;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int k = 4 * tx + j;
+        if (k < q) to[(int64_t)row * q + k] = __ldcg(V + (vbase + r0 + row) * q + k) - acc[i][j];
+      }
+    }
+    __syncthreads();
+    if (tid < ns) red_release_add(done + (int64_t)tid * P.nsuper + s, 1);  // one count per vector slice
+    return true;
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int row = 4 * ty + i;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int k = 4 * tx + j;
+      Rs[row * kWLd + k] = (row < rows && k < q) ? __ldcg(V + (vbase + r0 + row) * q + k) - acc[i][j] : 0.0;
+      acc[i][j] = 0.0;
+    }
+  }
+  // y[block] = X R, X = L_kk^-1 (rows x rows, column-major): As[jj][i] = X(i, jb + jj)
+  const TL *X = Inv + P.invOff[P.blkOff[s] + blk];
+  for (int jb = 0; jb < rows; jb += kWKC) {
+    const int jw = min(kWKC, rows - jb);
+    __syncthreads();
+    for (int e = tid; e < kWKC * kMB; e += kMultiThreads) {
+      const int i = e & (kMB - 1), jj = e >> 6;
+      As[jj * kWLd + i] = (i < rows && jj < jw) ? (double)X[(int64_t)(jb + jj) * rows + i] : 0.0;
+    }
+    __syncthreads();
+    mm_tile_w(As, Rs + jb * kWLd, jw, ty, tx, acc);
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int row = 4 * ty + i;
+    if (row >= rows) continue;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int k = 4 * tx + j;
+      if (k < q) y[(int64_t)(f + r0 + row) * q + k] = acc[i][j];
+    }
+  }
+  __syncthreads();
+  if (tid < ns) st_release(flags + (int64_t)tid * nflags + P.blkOff[s] + blk, epoch);  // every vector slice
+  return true;
+}
+
+// backward: as the sliced task, every vector (the rows below after the parent's every slice is final)
+template <class TL>
+__device__ __forceinline__ bool bwd_wide_task(const int4 t, const DevPlan &P, const TL *__restrict__ Lx, const TL *__restrict__ Inv,
+                              const double *__restrict__ Dpiv, double *__restrict__ y, int *flags, int nflags,
+                              int epoch, int q, int ns, unsigned long long *status, double *msm, int &waitOk) {
+  double *As = msm, *Bs = msm + kWKC * kWLd, *Rs = msm + 2 * kWKC * kWLd;
+  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  const int s = t.x, blk = t.y;
+  const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
+  const TL *Lp = Lx + P.snLxp[s];
+  const int *rowsOf = P.Si + P.Sp[s];
+  const int c0 = blk * kMB, w = min(kMB, nc - c0), nb = (nc + kMB - 1) / kMB;
+  int *myflags = flags + P.blkOff[s];  // the slice-0 set: this supernode releases every slice at once
+  const int par = P.snParent[s];
+  if (par >= 0) {  // the parent's every vector slice final
+    if (tid == 0) {
+      waitOk = 1;
+      for (int sl = 0; sl < ns && waitOk; sl++)
+        waitOk = wait_flag(flags + (int64_t)sl * nflags + P.blkOff[par], epoch, status, s, P.spin);
+    }
+    __syncthreads();
+    if (!waitOk) return false;
+  }
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
+  // chunks: ancestors rows [nc, m) in kWKC steps, then pivot blocks nb - 1 .. blk + 1 (two chunks each)
+  const int nanc = (m - nc + kWKC - 1) / kWKC;
+  const int npiv = (nb - 1 - blk) * (kMB / kWKC);
+  const int nch = nanc + npiv;
+  // chunk ch -> first row and row count
+  auto chunk = [&](int ch, int &rb, int &rw) {
+    if (ch < nanc) {
+      rb = nc + ch * kWKC;
+      rw = min(kWKC, m - rb);
+    } else {
+      const int p = ch - nanc, pb = nb - 1 - p / 2;  // pivot block, from the last down
+      rb = pb * kMB + (p & 1) * kWKC;
+      rw = max(0, min(kWKC, nc - rb));
+    }
+  };
+  // L tile: As[rr][c] = L(rb + rr, c0 + c); elements e = tid + 256 u: rr = e & 31, c = e >> 5
+  TL lr[8];
+  auto loadL = [&](int rb, int rw) {
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int e = tid + kMultiThreads * u, rr = e & (kWKC - 1), c = e >> 5;
+      lr[u] = (rr < rw && c < w) ? Lp[(int64_t)(c0 + c) * m + rb + rr] : (TL)0;
+    }
+  };
+  int rb = 0, rw = 0;
+  if (nch > 0) {
+    chunk(0, rb, rw);
+    loadL(rb, rw);
+  }
+  for (int ch = 0; ch < nch; ch++) {
+    const bool anc = ch < nanc;
+    if (!anc && ((ch - nanc) & 1) == 0) {  // first chunk of a pivot block: its x values final?
+      if (tid == 0) waitOk = wait_flag(myflags + rb / kMB, epoch, status, s, P.spin);
+      __syncthreads();
+      if (!waitOk) return false;
+    }
+    for (int e = tid; e < kWKC * kMQ; e += kMultiThreads) {
+      const int rr = e >> 6, k = e & (kMQ - 1);
+      double v = 0.0;
+      if (rr < rw && k < q) {
+        const int gi = anc ? rowsOf[rb + rr] : f + rb + rr;
+        v = __ldcg(y + (int64_t)gi * q + k);
+      }
+      Bs[rr * kWLd + k] = v;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int e = tid + kMultiThreads * u;
+      As[(e & (kWKC - 1)) * kWLd + (e >> 5)] = (double)lr[u];
+    }
+    __syncthreads();
+    const int cw = rw;
+    if (ch + 1 < nch) {
+      chunk(ch + 1, rb, rw);
+      loadL(rb, rw);
+    }
+    mm_tile_w(As, Bs, cw, ty, tx, acc);
+    __syncthreads();
+  }
+  // R = y[block] (/ D) - acc
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int c = 4 * ty + i;
+    const double d = (Dpiv && c < w) ? Dpiv[f + c0 + c] : 1.0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int k = 4 * tx + j;
+      double v = 0.0;
+      if (c < w && k < q) {
+        const double yv = y[(int64_t)(f + c0 + c) * q + k];
+        v = (Dpiv ? yv / d : yv) - acc[i][j];  // LDL^T: y /= D before the backward sweep (ldlt.mjs:629)
+      }
+      Rs[c * kWLd + k] = v;
+      acc[i][j] = 0.0;
+    }
+  }
+  // x[block] = X^T R: As[jj][i] = X(jb + jj, i) = Inv[i w + jb + jj]
+  const TL *X = Inv + P.invOff[P.blkOff[s] + blk];
+  for (int jb = 0; jb < w; jb += kWKC) {
+    const int jw = min(kWKC, w - jb);
+    __syncthreads();
+    for (int e = tid; e < kWKC * kMB; e += kMultiThreads) {
+      const int jj = e & (kWKC - 1), i = e >> 5;
+      As[jj * kWLd + i] = (i < w && jj < jw) ? (double)X[(int64_t)i * w + jb + jj] : 0.0;
+    }
+    __syncthreads();
+    mm_tile_w(As, Rs + jb * kWLd, jw, ty, tx, acc);
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int c = 4 * ty + i;
+    if (c >= w) continue;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int k = 4 * tx + j;
+      if (k < q) y[(int64_t)(f + c0 + c) * q + k] = acc[i][j];
+    }
+  }
+  __syncthreads();
+  if (tid < ns) st_release(flags + (int64_t)tid * nflags + P.blkOff[s] + blk, epoch);  // every vector slice
+  return true;
+}
+
 // ---- forward ------------------------------------------------------------------------------------------------------
 // task (s, blk, below) of slice sl: as k_fwd_blocks. Diagonal: y[block] = X (V[block] - L[block, 0:blk 64] y[0:blk 64]);
 // below: T[block] = V[block] - L[block, 0:nc] y[0:nc].
-template <class TL>
-__global__ void __launch_bounds__(kMultiThreads, 3) k_fwd_multi(const int4 *__restrict__ tasks, int ntasks, int ns,
+template <class TL, bool WIDE>
+__global__ void __launch_bounds__(kMultiThreads, kMultiCtas) k_fwd_multi(const int4 *__restrict__ tasks, int ntasks, int ns,
                                                                 int *__restrict__ ticket, DevPlan P,
                                                                 const TL *__restrict__ Lx, const TL *__restrict__ Inv,
                                                                 double *__restrict__ y, double *__restrict__ V,
@@ -145,7 +446,7 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_fwd_multi(const int4 *__re
                                                                 int nflags, int epoch, int *__restrict__ done, int q,
                                                                 unsigned long long *status) {
   extern __shared__ double msm[];
-  double *As = msm, *Bs = As + kAElems, *Rs = Bs + kKC * kLdB;
+  double *As = msm, *Bs = As + kAElems, *Rs = Bs + kMB * kLdB;
   TL *Xs = reinterpret_cast<TL *>(Rs + kMB * kLdB);
   __shared__ int waitOk;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, mw = warp & 3, kh = warp >> 2;
@@ -153,19 +454,8 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_fwd_multi(const int4 *__re
     cp_async_all();
     return false;
   };
-  auto run = [&](const int tkv) -> bool {
-    const int base = tkv / ns, sl = tkv - base * ns;
-    const int4 t = tasks[base];
-    if (t.z == 2) {  // up to kSolveGroup supernodes with m <= 32, one warp each, all q vectors (slice 0's task)
-      if (sl != 0) return true;
-      if (tid == 0) waitOk = 1;
-      __syncthreads();
-      if (warp < t.y && !small_fwd_warp_multi<TL>(P.solveSmall[t.x + warp], P, Lx, y, T, done, q, ns, status,
-                                                  msm + 32 * kMQ * warp))
-        waitOk = 0;
-      __syncthreads();
-      return waitOk != 0;
-    }
+  // one block task for vector slice sl
+  auto run_slice = [&](const int4 t, const int sl) -> bool {
     const int s = t.x, blk = t.y, below = t.z;
     const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s], mu = m - nc;
     const int vb = sl * kQS, qs = min(kQS, q - vb);
@@ -229,14 +519,15 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_fwd_multi(const int4 *__re
     if (nch > 0) loadL(0);
     for (int ch = 0; ch < nch; ch++) {
       const int cb = ch * kKC, cw = min(kKC, ncols - cb);
-      if ((cb & (kMB - 1)) == 0) {  // first chunk of a pivot block: its y values final?
+      const double *Bc = Bs + (cb & (kMB - 1)) * kLdB;  // this chunk's rows of the block's y values
+      if ((cb & (kMB - 1)) == 0) {  // first chunk of a pivot block: its y values final? Then all 64 rows at once
         if (tid == 0) waitOk = wait_flag(myflags + cb / kMB, epoch, status, s, P.spin);
         __syncthreads();
         if (!waitOk) return bail();
-      }
-      for (int e = tid; e < kKC * kQS; e += kMultiThreads) {
-        const int k = e >> 4, n = e & (kQS - 1);
-        Bs[k * kLdB + n] = (k < cw && n < qs) ? __ldcg(y + (int64_t)(f + cb + k) * q + vb + n) : 0.0;
+        for (int e = tid; e < kMB * kQS; e += kMultiThreads) {
+          const int k = e >> 4, n = e & (kQS - 1);
+          Bs[k * kLdB + n] = (cb + k < ncols && n < qs) ? __ldcg(y + (int64_t)(f + cb + k) * q + vb + n) : 0.0;
+        }
       }
 #pragma unroll
       for (int u = 0; u < 8; u++) {
@@ -245,7 +536,7 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_fwd_multi(const int4 *__re
       }
       __syncthreads();
       if (ch + 1 < nch) loadL(cb + kKC);
-      if (16 * kh < cw) mma_k16<true>(As, kLdKM, Bs, 16 * kh, mw, lane, c);
+      if (16 * kh < cw) mma_k16<true>(As, kLdKM, Bc, 16 * kh, mw, lane, c);
       __syncthreads();
     }
     halves_sum(c, As, warp, lane);
@@ -300,14 +591,30 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_fwd_multi(const int4 *__re
     if (tid == 0) st_release(myflags + blk, epoch);
     return true;
   };
+  auto run = [&](const int tkv) -> bool {
+    const int4 t = tasks[tkv];
+    if (t.z == 2) {  // up to kSolveGroup supernodes with m <= 32, one warp each, all q vectors
+      if (tid == 0) waitOk = 1;
+      __syncthreads();
+      if (warp < t.y && !small_fwd_warp_multi<TL>(P.solveSmall[t.x + warp], P, Lx, y, T, done, q, ns, status,
+                                                  msm + 32 * kMQ * warp))
+        waitOk = 0;
+      __syncthreads();
+      return waitOk != 0;
+    }
+    if constexpr (WIDE) {
+      if (t.w < 0) return fwd_wide_task<TL>(t, P, Lx, Inv, y, V, T, flags, nflags, epoch, done, q, ns, status, msm, waitOk);
+    }
+    return run_slice(t, t.w);
+  };
   ticket_loop(ticket, ntasks, run);
 }
 
 // ---- backward -----------------------------------------------------------------------------------------------------
 // task (s, blk) of slice sl: x[block] = X^T (y[block] (/ D for LDL^T) - L[rows below the block, block columns]^T
 // x[those rows]).
-template <class TL>
-__global__ void __launch_bounds__(kMultiThreads, 3) k_bwd_multi(const int4 *__restrict__ tasks, int ntasks, int ns,
+template <class TL, bool WIDE>
+__global__ void __launch_bounds__(kMultiThreads, kMultiCtas) k_bwd_multi(const int4 *__restrict__ tasks, int ntasks, int ns,
                                                                 int *__restrict__ ticket, DevPlan P,
                                                                 const TL *__restrict__ Lx, const TL *__restrict__ Inv,
                                                                 const double *__restrict__ Dpiv,
@@ -315,7 +622,7 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_bwd_multi(const int4 *__re
                                                                 int nflags, int epoch, int q,
                                                                 unsigned long long *status) {
   extern __shared__ double msm[];
-  double *As = msm, *Bs = As + kAElems, *Rs = Bs + kKC * kLdB;
+  double *As = msm, *Bs = As + kAElems, *Rs = Bs + kMB * kLdB;
   TL *Xs = reinterpret_cast<TL *>(Rs + kMB * kLdB);
   __shared__ int waitOk;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, mw = warp & 3, kh = warp >> 2;
@@ -323,19 +630,8 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_bwd_multi(const int4 *__re
     cp_async_all();
     return false;
   };
-  auto run = [&](const int tkv) -> bool {
-    const int base = tkv / ns, sl = tkv - base * ns;
-    const int4 t = tasks[base];
-    if (t.z == 2) {  // up to kSolveGroup supernodes with m <= 32, one warp each, all q vectors (slice 0's task)
-      if (sl != 0) return true;
-      if (tid == 0) waitOk = 1;
-      __syncthreads();
-      if (warp < t.y && !small_bwd_warp_multi<TL>(P.solveSmall[t.x + warp], P, Lx, Dpiv, y, flags, nflags, epoch, q,
-                                                  ns, status, msm + 32 * kMQ * warp))
-        waitOk = 0;
-      __syncthreads();
-      return waitOk != 0;
-    }
+  // one block task for vector slice sl
+  auto run_slice = [&](const int4 t, const int sl) -> bool {
     const int s = t.x, blk = t.y;
     const int f = P.snF[s], nc = P.snNc[s], m = P.snM[s];
     const int vb = sl * kQS, qs = min(kQS, q - vb);
@@ -473,6 +769,22 @@ __global__ void __launch_bounds__(kMultiThreads, 3) k_bwd_multi(const int4 *__re
     if (tid == 0) st_release(myflags + blk, epoch);
     return true;
   };
+  auto run = [&](const int tkv) -> bool {
+    const int4 t = tasks[tkv];
+    if (t.z == 2) {  // up to kSolveGroup supernodes with m <= 32, one warp each, all q vectors
+      if (tid == 0) waitOk = 1;
+      __syncthreads();
+      if (warp < t.y && !small_bwd_warp_multi<TL>(P.solveSmall[t.x + warp], P, Lx, Dpiv, y, flags, nflags, epoch, q,
+                                                  ns, status, msm + 32 * kMQ * warp))
+        waitOk = 0;
+      __syncthreads();
+      return waitOk != 0;
+    }
+    if constexpr (WIDE) {
+      if (t.w < 0) return bwd_wide_task<TL>(t, P, Lx, Inv, Dpiv, y, flags, nflags, epoch, q, ns, status, msm, waitOk);
+    }
+    return run_slice(t, t.w);
+  };
   ticket_loop(ticket, ntasks, run);
 }
 
@@ -597,40 +909,47 @@ __global__ void __launch_bounds__(256) k_residual_multi(int n, const int *__rest
   }
 }
 
-template <class TL>
+template <class TL, bool WIDE>
 static cudaError_t set_multi_smem() {
-  cudaError_t e = cudaFuncSetAttribute(k_fwd_multi<TL>, cudaFuncAttributeMaxDynamicSharedMemorySize, multi_smem<TL>());
+  cudaError_t e =
+      cudaFuncSetAttribute(k_fwd_multi<TL, WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize, multi_smem<TL>());
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_bwd_multi<TL>, cudaFuncAttributeMaxDynamicSharedMemorySize, multi_smem<TL>());
+    e = cudaFuncSetAttribute(k_bwd_multi<TL, WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize, multi_smem<TL>());
   return e;
 }
 cudaError_t init_solve_multi_attributes() {
-  cudaError_t e = set_multi_smem<double>();
-  return e == cudaSuccess ? set_multi_smem<float>() : e;
+  cudaError_t e = set_multi_smem<double, false>();
+  if (e == cudaSuccess) e = set_multi_smem<double, true>();
+  if (e == cudaSuccess) e = set_multi_smem<float, false>();
+  return e == cudaSuccess ? set_multi_smem<float, true>() : e;
 }
 
 int num_sms();
 int multi_max_vectors() { return kMQ; }
 int multi_slices(int q) { return (q + kQS - 1) / kQS; }
-static int multi_grid(int64_t ntasks) { return ntasks < 3 * num_sms() ? (int)ntasks : 3 * num_sms(); }
+static int multi_grid(int64_t ntasks) {
+  return ntasks < kMultiCtas * num_sms() ? (int)ntasks : kMultiCtas * num_sms();
+}
 
 template <class TL>
-void launch_fwd_multi(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
-                      double *y, double *V, double *T, int *flags, int nflags, int epoch, int *done, int q,
-                      unsigned long long *status, cudaStream_t st) {
+void launch_fwd_multi(const int4 *tasks, int ntasks, bool wide, int *ticket, const DevPlan &P, const TL *Lx,
+                      const TL *Inv, double *y, double *V, double *T, int *flags, int nflags, int epoch, int *done,
+                      int q, unsigned long long *status, cudaStream_t st) {
   const int ns = multi_slices(q);
-  if (ntasks > 0)
-    k_fwd_multi<TL><<<multi_grid((int64_t)ntasks * ns), kMultiThreads, multi_smem<TL>(), st>>>(
-        tasks, ntasks * ns, ns, ticket, P, Lx, Inv, y, V, T, flags, nflags, epoch, done, q, status);
+  if (ntasks <= 0) return;
+  auto k = wide ? k_fwd_multi<TL, true> : k_fwd_multi<TL, false>;
+  k<<<multi_grid(ntasks), kMultiThreads, multi_smem<TL>(), st>>>(tasks, ntasks, ns, ticket, P, Lx, Inv, y, V, T,
+                                                                  flags, nflags, epoch, done, q, status);
 }
 template <class TL>
-void launch_bwd_multi(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
-                      const double *Dpiv, double *y, int *flags, int nflags, int epoch, int q,
+void launch_bwd_multi(const int4 *tasks, int ntasks, bool wide, int *ticket, const DevPlan &P, const TL *Lx,
+                      const TL *Inv, const double *Dpiv, double *y, int *flags, int nflags, int epoch, int q,
                       unsigned long long *status, cudaStream_t st) {
   const int ns = multi_slices(q);
-  if (ntasks > 0)
-    k_bwd_multi<TL><<<multi_grid((int64_t)ntasks * ns), kMultiThreads, multi_smem<TL>(), st>>>(
-        tasks, ntasks * ns, ns, ticket, P, Lx, Inv, Dpiv, y, flags, nflags, epoch, q, status);
+  if (ntasks <= 0) return;
+  auto k = wide ? k_bwd_multi<TL, true> : k_bwd_multi<TL, false>;
+  k<<<multi_grid(ntasks), kMultiThreads, multi_smem<TL>(), st>>>(tasks, ntasks, ns, ticket, P, Lx, Inv, Dpiv, y,
+                                                                  flags, nflags, epoch, q, status);
 }
 void launch_to_interleaved(const double *B, double *Yil, int n, int q, cudaStream_t st) {
   if (n > 0 && q > 0) k_to_interleaved<<<dim3((n + 31) / 32, (q + 31) / 32), dim3(32, 8), 0, st>>>(B, Yil, n, q);
@@ -649,16 +968,16 @@ void launch_residual_multi(int n, const int *rowptr, const int *colidx, const do
   const int grid = (int)(want < 8 * num_sms() ? want : 8 * num_sms());
   k_residual_multi<<<grid, 256, 0, st>>>(n, rowptr, colidx, val, x, b, r, norms, q, rowGroup);
 }
-template void launch_fwd_multi<double>(const int4 *, int, int *, const DevPlan &, const double *, const double *,
-                                       double *, double *, double *, int *, int, int, int *, int, unsigned long long *,
-                                       cudaStream_t);
-template void launch_fwd_multi<float>(const int4 *, int, int *, const DevPlan &, const float *, const float *,
+template void launch_fwd_multi<double>(const int4 *, int, bool, int *, const DevPlan &, const double *,
+                                       const double *, double *, double *, double *, int *, int, int, int *, int,
+                                       unsigned long long *, cudaStream_t);
+template void launch_fwd_multi<float>(const int4 *, int, bool, int *, const DevPlan &, const float *, const float *,
                                       double *, double *, double *, int *, int, int, int *, int, unsigned long long *,
                                       cudaStream_t);
-template void launch_bwd_multi<double>(const int4 *, int, int *, const DevPlan &, const double *, const double *,
-                                       const double *, double *, int *, int, int, int, unsigned long long *,
-                                       cudaStream_t);
-template void launch_bwd_multi<float>(const int4 *, int, int *, const DevPlan &, const float *, const float *,
+template void launch_bwd_multi<double>(const int4 *, int, bool, int *, const DevPlan &, const double *,
+                                       const double *, const double *, double *, int *, int, int, int,
+                                       unsigned long long *, cudaStream_t);
+template void launch_bwd_multi<float>(const int4 *, int, bool, int *, const DevPlan &, const float *, const float *,
                                       const double *, double *, int *, int, int, int, unsigned long long *,
                                       cudaStream_t);
 

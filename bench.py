@@ -297,7 +297,9 @@ def run_reference(args, rank):
             "data": "synthetic",
             "config": {"workload": args.desc, "n": w.n, "nnz": w.pat.nnz, "flops_factor": so.flops,
                        "rhs": int(w.rhs.shape[0]), "sample": sample,
-                       "warmup": "factorizations of a small subtree", "budget_s": args.ref_budget},
+                       "warmup": "factorizations of a small subtree", "budget_s": args.ref_budget,
+                       # every timed step is a complete factor + solve of the whole system, all inside this run
+                       "fits_in_driver_run": bool(times)},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

@@ -112,3 +112,25 @@ def test_noalloc_rejects_oversized_front():
     code, _ = _noalloc(F.data_ptr(), 16385, 16)
     assert code == amp.AMP_INVALID
     assert "exceeds the maximum" in amp.lib().amp_last_error().decode()
+
+
+def test_noalloc_on_every_device():
+    # the per-device set-up (scratch address, kernel attributes): a front factored on each visible GPU in turn, the
+    # calling thread's current device being the front's; skipped with one GPU
+    torch = pytest.importorskip("torch")
+    ndev = torch.cuda.device_count()
+    if ndev < 2:
+        pytest.skip("one GPU: the second device's set-up is not reachable")
+    m = nc = 200
+    A = _dense_spd(m, 5)
+    L = np.linalg.cholesky(A)
+    low = np.tril(np.ones((m, m), bool))
+    for dev in range(ndev):
+        with torch.cuda.device(dev):
+            F = torch.from_numpy(np.asfortranarray(A).T.copy().reshape(-1)).to(f"cuda:{dev}")
+            torch.cuda.synchronize()
+            code, fail = _noalloc(F.data_ptr(), m, nc)
+            assert code == amp.AMP_OK, (dev, amp.lib().amp_last_error())
+            assert fail == -1
+            R = F.cpu().numpy().reshape(m, m).T
+        assert np.max(np.abs(R[low] - L[low])) <= TOL * np.max(np.abs(L)), dev
