@@ -24,7 +24,7 @@ _lib = None
 AMP_OK, AMP_NOT_SPD, AMP_NONFINITE_PIVOT, AMP_PATTERN_MISMATCH, AMP_BAD_LENGTH, AMP_NO_FACTOR, AMP_NEED_COORDS, \
     AMP_DEVICE_TIMEOUT, AMP_CUDA_ERROR, AMP_OOM, AMP_INVALID = range(11)
 ORDER_AMD, ORDER_ND, ORDER_ND3, ORDER_GIVEN = range(4)
-CHOLESKY, LDLT, LDLT_COMPLEX = 0, 1, 2
+CHOLESKY, LDLT, LDLT_COMPLEX, LDLT_BK = 0, 1, 2, 3  # LDLT_BK: Bunch-Kaufman pivots in each pivot block
 AMP_ELEM_P1_TRI_SCALAR, AMP_ELEM_P1_TET_ELASTIC = 0, 1
 FP64, MIXED = 0, 1
 
@@ -129,6 +129,7 @@ SIGNATURES = {
     "amp_solve_gmres": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(_GmresOpts),
                                   C.POINTER(_GmresStats)]),
     "amp_factor_download": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "amp_factor_download_pivots": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "amp_factor_destroy": (None, [C.c_void_p]),
     "amp_matvec": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "amp_factor_set_wait_limit": (C.c_int, [C.c_void_p, C.c_int64]),
@@ -432,6 +433,14 @@ class NumericFactor:
         _check(lib().amp_factor_download(self._h, None, out.ctypes.data))
         return out[: self.sym.n]
 
+    def pivots(self):
+        """(Doff, piv) of a Bunch-Kaufman factor: Doff[j] = D(j + 1, j) of a 2 x 2 pivot (j, j + 1), else 0; piv[f + c0
+        + i] = the column of the pivot block at c0 of the supernode at f that became its i-th pivot."""
+        n = max(self.sym.n, 1)
+        doff, piv = np.zeros(n), np.zeros(n, np.int32)
+        _check(lib().amp_factor_download_pivots(self._h, doff.ctypes.data, piv.ctypes.data))
+        return doff[: self.sym.n], piv[: self.sym.n]
+
     def profile(self, enable: bool = True) -> None:
         """Time every kernel launch of the following calls with CUDA events (see profile_read)."""
         _check(lib().amp_profile_enable(self._h, 1 if enable else 0))
@@ -675,13 +684,20 @@ class SparseCholesky:
 
 class SupernodalLDLT:
     """Real symmetric LDL^T over a supernodal analysis: 1x1 pivots with static perturbation (|d| < tau -> +-tau,
-    tau = pivotTol * max |A(i, i)|), inertia and refinement (ldlt.mjs:431-645). Factor and solves run on the GPU."""
+    tau = pivotTol * max |A(i, i)|), inertia and refinement (ldlt.mjs:431-645). Factor and solves run on the GPU.
 
-    def __init__(self, sym: SymbolicAnalysis, factor=None, precision: int = FP64):
+    pivoting="bunch-kaufman" (no reference counterpart; FP64) chooses 1 x 1 and 2 x 2 pivots by the Bunch-Kaufman rule
+    inside each 64-column pivot block of every supernode (the symbolic structure is unchanged); a column with no entry
+    at or above tau still takes the static perturbation. nNeg counts the negative eigenvalues of D's blocks."""
+
+    def __init__(self, sym: SymbolicAnalysis, factor=None, precision: int = FP64, pivoting: str = "static"):
+        if pivoting not in ("static", "bunch-kaufman"):
+            raise AmpError(AMP_INVALID, f"SupernodalLDLT: unknown pivoting {pivoting!r}")
         self.sym = sym
         self.factorKind = factor
+        self.pivoting = pivoting
         self.kernel = "cuda-sm100a"
-        self.num = NumericFactor(sym, LDLT, precision)
+        self.num = NumericFactor(sym, LDLT_BK if pivoting == "bunch-kaufman" else LDLT, precision)
         self.nnzL = sym.nnzL
         self.nNeg = 0
         self.nPerturbed = 0

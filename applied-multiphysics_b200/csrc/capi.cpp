@@ -195,6 +195,7 @@ struct amp_assembly_s {
 struct amp_factor_s {
   amp_plan *plan = nullptr;
   int kind = AMP_CHOLESKY, precision = AMP_FP64;
+  bool bk = false;  // LDL^T with Bunch-Kaufman pivots inside each pivot block (amp_factor_opts kind AMP_LDLT_BK)
   cudaStream_t stream = nullptr;
   cudaStream_t side = nullptr;                      // look-ahead: part B of the panel steps' updates
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -205,6 +206,8 @@ struct amp_factor_s {
   double *dW = nullptr;                             // LDL^T: L21 D of every front (the update's A operand)
   double *dScal = nullptr;                          // LDL^T: pivotTol, tau
   int *dCounts = nullptr;                           // LDL^T: nNeg, nPerturbed
+  double *dDoff = nullptr;                          // Bunch-Kaufman: D(j + 1, j) of each 2 x 2 pivot (else 0)
+  int *dPiv = nullptr;                              // Bunch-Kaufman: pivot order inside each 64-column block
   double *dInv = nullptr;                           // inverses of the 64-column diagonal blocks (FP64 factor)
   float *dInv32 = nullptr;                          // the same for the FP32 factor
   double *dMch = nullptr, *dGch = nullptr;          // chain matrices of consecutive diagonal blocks (FP64 factor)
@@ -430,7 +433,13 @@ void enqueue_chain_mats(amp_factor *f, const T *Lx, const T *Inv, T *Mch, T *Gch
   });
 }
 
+void enqueue_bkfactor(amp_factor *f);
+
 void enqueue_factor(amp_factor *f) {
+  if (f->bk) {
+    enqueue_bkfactor(f);
+    return;
+  }
   const amp::Plan &P = f->plan->P;
   amp::DevPlan dp = f->plan->dp;
   if (f->waitSpins > 0) dp.spin = f->waitSpins;
@@ -545,6 +554,7 @@ void enqueue_factor(amp_factor *f) {
 amp::DevPlan solve_view(const amp_factor *f) {
   amp::DevPlan dp = f->plan->dp;
   if (f->waitSpins > 0) dp.spin = f->waitSpins;
+  if (f->bk) dp.lpiv = f->dPiv;
   return dp;
 }
 
@@ -559,7 +569,7 @@ void device_solve_permuted(amp_factor *f) {
   const int efwd = 2 * (++f->solveEpoch) - 1, ebwd = 2 * f->solveEpoch;
   const int nf = (int)(P.fwdTasks1.size() / 4), nb = (int)(P.bwdAll.size() / 4);
   const bool ldlt = f->kind == AMP_LDLT;
-  const double *Dp = ldlt ? f->dD : nullptr;
+  const double *Dp = ldlt && !f->bk ? f->dD : nullptr;  // a Bunch-Kaufman factor's D solve runs between the sweeps
   timed(f, K_FORWARD, 2.0 * (double)P.nnzLStored, lbytes, [&] {
     if (f->dL32)
       amp::launch_fwd_blocks<float>(f->plan->dFwdTasks1, nf, f->dTickets, dp, f->dL32, f->dInv32,
@@ -569,6 +579,8 @@ void device_solve_permuted(amp_factor *f) {
       amp::launch_fwd_blocks<double>(f->plan->dFwdTasks1, nf, f->dTickets, dp, f->dLx, f->dInv, ldlt ? nullptr : f->dMch,
                                      f->dY, f->dT, f->dFlags, f->dHand, efwd, f->dDone, f->dSolveStatus, st);
   });
+  if (f->bk)
+    timed(f, K_PERMUTE, (double)P.n, 24.0 * P.n, [&] { amp::launch_dsolve_bk(P.n, 1, f->dD, f->dDoff, f->dY, st); });
   timed(f, K_BACKWARD, 2.0 * (double)P.nnzLStored, lbytes, [&] {
     if (f->dL32)
       amp::launch_bwd_blocks<float>(f->plan->dBwdAll, nb, f->dTickets + 1, dp, f->dL32, f->dInv32,
@@ -657,7 +669,7 @@ void device_solve_multi_permuted(amp_factor *f, int q) {
   const int nf = f->plan->nFwdSl[ns - 1], nb = f->plan->nBwdSl[ns - 1];
   int4 *fwdTasks = f->plan->dFwdSl[ns - 1], *bwdTasks = f->plan->dBwdSl[ns - 1];
   const bool wide = f->plan->wideSl[ns - 1];
-  const double *Dp = f->kind == AMP_LDLT ? f->dD : nullptr;
+  const double *Dp = f->kind == AMP_LDLT && !f->bk ? f->dD : nullptr;  // Bunch-Kaufman: D solve between the sweeps
   timed(f, K_FORWARD, flops, lbytes, [&] {
     if (f->dL32)
       amp::launch_fwd_multi<float>(fwdTasks, nf, wide, f->dTickets, dp, f->dL32, f->dInv32, f->dY, f->dV, f->dT, f->dFlags,
@@ -666,6 +678,9 @@ void device_solve_multi_permuted(amp_factor *f, int q) {
       amp::launch_fwd_multi<double>(fwdTasks, nf, wide, f->dTickets, dp, f->dLx, f->dInv, f->dY, f->dV, f->dT, f->dFlags,
                                     nfl, efwd, f->dDone, q, f->dSolveStatus, st);
   });
+  if (f->bk)
+    timed(f, K_PERMUTE, (double)P.n * q, 24.0 * P.n * q,
+          [&] { amp::launch_dsolve_bk(P.n, q, f->dD, f->dDoff, f->dY, st); });
   timed(f, K_BACKWARD, flops, lbytes, [&] {
     if (f->dL32)
       amp::launch_bwd_multi<float>(bwdTasks, nb, wide, f->dTickets + 1, dp, f->dL32, f->dInv32, Dp, f->dY, f->dFlags, nfl,
@@ -931,6 +946,57 @@ void enqueue_cfactor(amp_factor *f) {
   }
 }
 
+// The FP64 LDL^T with Bunch-Kaufman pivots inside each pivot block: every front through the dense schedule (the
+// complex factor's: assembly, group steps with the Bunch-Kaufman pivot blocks, FP64 update tiles with A = L21 D), then
+// the inverses of the diagonal blocks with each block's pivot order folded in.
+void enqueue_bkfactor(amp_factor *f) {
+  const amp::Plan &P = f->plan->P;
+  const amp::DenseSched &D = f->plan->cx;
+  amp::DevPlan dp = f->plan->dp;
+  if (f->waitSpins > 0) dp.spin = f->waitSpins;
+  cudaStream_t st = f->stream;
+  ck(cudaMemsetAsync(f->dStatus, 0xff, sizeof(unsigned long long), st), "memset status");
+  ck(cudaMemsetAsync(f->dCounts, 0, 2 * sizeof(int), st), "memset counts");
+  if (D.nGroupFlags + D.nGroupTickets > 0)
+    ck(cudaMemsetAsync(f->dCxFlags, 0, sizeof(int) * (D.nGroupFlags + D.nGroupTickets), st), "memset flags");
+  int *tickets = f->dCxFlags + D.nGroupFlags;
+  amp::launch_ldlt_tau(f->dValues, dp, f->dScal, st);
+  amp::LdltArgs<double> ld{f->dScal, f->dCounts, f->dW, f->dD, nullptr, nullptr};
+  ld.piv = f->dPiv;
+  ld.Doff = f->dDoff;
+  for (int L = 0; L < P.nlevels; L++) {
+    if (D.asmLvlPtr[L + 1] > D.asmLvlPtr[L])
+      timed(f, K_ASSEMBLE, 0.0, 0.0, [&] {
+        amp::launch_assemble<double>(f->plan->dCxAsm + D.asmLvlPtr[L], D.asmLvlPtr[L + 1] - D.asmLvlPtr[L], dp,
+                                     f->dValues, f->dLx, f->dU, f->dStatus, st);
+      });
+    for (int k = D.lvlStepPtr[L]; k < D.lvlStepPtr[L + 1]; k++) {
+      const amp::StepRange &sr = D.steps[k];
+      timed(f, K_PANEL, sr.panelFlops, 0.0, [&] {
+        amp::launch_group_panel<double>(f->plan->dCxItems, f->plan->dCxStrips + sr.strip0,
+                                        (int)(sr.strip1 - sr.strip0), tickets + sr.ticket, f->dCxFlags, dp, f->dLx,
+                                        f->dStatus, nullptr, nullptr, ld, st);
+      });
+      if (sr.tile1 > sr.tile0)
+        timed(f, K_UPDATE, sr.updateFlopsA + sr.updateFlopsB, 0.0, [&] {
+          amp::launch_update(f->plan->dCxTiles + sr.tile0, sr.tile1 - sr.tile0, dp, f->dLx, f->dU, f->dW, f->dStatus,
+                             st);
+        });
+    }
+    if (D.uLvlPtr[L + 1] > D.uLvlPtr[L])
+      timed(f, K_UPDATE, 0.0, 0.0, [&] {
+        amp::launch_update(f->plan->dCxU + D.uLvlPtr[L], D.uLvlPtr[L + 1] - D.uLvlPtr[L], dp, f->dLx, f->dU, f->dW,
+                           f->dStatus, st);
+      });
+  }
+  dp.lpiv = f->dPiv;  // the inverse blocks with the pivot order folded in
+  if (P.nflags)
+    timed(f, K_DIAGINV, 0.0, 16.0 * (double)inv_elems(P),
+          [&] {
+            amp::launch_diag_inv<double>(f->plan->dInvBlocks, (int)P.invBlocks.size(), dp, f->dLx, f->dInv, st);
+          });
+}
+
 // y (permuted order) := A^-1 y
 void csolve_permuted(amp_factor *f, amp::cplx *y) {
   const amp::Plan &P = f->plan->P;
@@ -1192,8 +1258,11 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
     *out = nullptr;
     amp_factor_opts o{AMP_CHOLESKY, AMP_FP64};
     if (opts) o = *opts;
-    if (o.kind != AMP_CHOLESKY && o.kind != AMP_LDLT) return fail(AMP_INVALID, "unknown factor kind");
+    if (o.kind != AMP_CHOLESKY && o.kind != AMP_LDLT && o.kind != AMP_LDLT_BK)
+      return fail(AMP_INVALID, "unknown factor kind");
     if (o.precision != AMP_FP64 && o.precision != AMP_MIXED) return fail(AMP_INVALID, "unknown precision");
+    if (o.kind == AMP_LDLT_BK && o.precision != AMP_FP64)
+      return fail(AMP_INVALID, "Bunch-Kaufman LDL^T: FP64 precision only");
     ck(cudaSetDevice(pl->device), "cudaSetDevice");
     if (!pl->uploaded) {  // the device schedule is uploaded once, by the first factor of the plan
       upload_plan(pl);
@@ -1203,7 +1272,8 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
     }
     auto *f = new amp_factor_s();
     f->plan = pl;
-    f->kind = o.kind;
+    f->kind = o.kind == AMP_LDLT_BK ? AMP_LDLT : o.kind;
+    f->bk = o.kind == AMP_LDLT_BK;
     f->precision = o.precision;
     try {
       ck(cudaStreamCreateWithFlags(&f->stream, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -1219,10 +1289,16 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
         f->dInv = f->mem.alloc<double>((size_t)inv_elems(P));
         f->dMch = f->mem.alloc<double>(chain_elems(P));
         f->dGch = f->mem.alloc<double>(chain_elems(P));
-        if (o.kind == AMP_LDLT) {
+        if (f->kind == AMP_LDLT) {
           f->dW = f->mem.alloc<double>((size_t)P.nnzLStored);
           f->dScal = f->mem.alloc<double>(2);
           f->dCounts = f->mem.alloc<int>(2);
+        }
+        if (f->bk) {  // every front through the dense schedule (built and uploaded once per plan)
+          upload_cx(pl);
+          f->dDoff = f->mem.alloc<double>((size_t)std::max(1, P.n));
+          f->dPiv = f->mem.alloc<int>((size_t)std::max(1, P.n));
+          f->dCxFlags = f->mem.alloc<int>((size_t)std::max(1, pl->cx.nGroupFlags + pl->cx.nGroupTickets));
         }
       } else {
         f->dL32 = f->mem.alloc<float>((size_t)P.nnzLStored);
@@ -1599,6 +1675,18 @@ int amp_factor_download(const amp_factor *f, double *Lx, double *D) {
       for (int64_t i = 0; i < P.nnzLStored; i++) Lx[i] = tmp[i];
     }
     if (D && P.n) ck(cudaMemcpy(D, f->dD, sizeof(double) * P.n, cudaMemcpyDeviceToHost), "copy D");
+    return (int)AMP_OK;
+  });
+}
+
+int amp_factor_download_pivots(const amp_factor *f, double *Doff, int32_t *piv) {
+  return guarded([&] {
+    if (!f) return fail(AMP_INVALID, "null handle");
+    if (!f->bk) return fail(AMP_INVALID, "download_pivots: not a Bunch-Kaufman factor");
+    const amp::Plan &P = f->plan->P;
+    ck(cudaSetDevice(f->plan->device), "cudaSetDevice");
+    if (Doff && P.n) ck(cudaMemcpy(Doff, f->dDoff, sizeof(double) * P.n, cudaMemcpyDeviceToHost), "copy Doff");
+    if (piv && P.n) ck(cudaMemcpy(piv, f->dPiv, sizeof(int32_t) * P.n, cudaMemcpyDeviceToHost), "copy piv");
     return (int)AMP_OK;
   });
 }

@@ -24,6 +24,9 @@ struct DevPlan {
   const int *diagSlot;     // CSR slot of A(i, i), original row i (the LDL^T pivot scale)
   const int *solveSmall;   // supernodes solved whole by one warp (solve tasks of kind 2 index this list)
   long long spin;          // bound of every inter-CTA wait of the solve sweeps, in polls (kSpinLimit by default)
+  // Bunch-Kaufman LDL^T factor (null otherwise): the pivot order inside every 64-column pivot block of every
+  // supernode, lpiv[f + c0 + i] = the block column (0..63) that became pivot i. Set per factor for its solves.
+  const int *lpiv;
 };
 
 // LDL^T variant of the panel and update kernels (ldlt.mjs:450-562); all null for Cholesky.
@@ -35,6 +38,11 @@ struct LdltArgs {
   T *W;                // L21 D (rows of the solved panel times the pivots): the A operand of the FP64 update
   DT *D;               // the pivots, permuted order
   __nv_bfloat16 *Whi, *Wlo;  // mixed precision: BF16 split of L21 D (the A operand of the tensor-core update)
+  // Bunch-Kaufman pivoting inside each 64-column pivot block (null: static perturbation as the reference):
+  // piv[f + c0 + i] = the block column (0..63) that became pivot i; Doff[j] = D(j + 1, j) when (j, j + 1) is a 2 x 2
+  // pivot, else 0 (D[j] holds the diagonal of both 1 x 1 and 2 x 2 pivots)
+  int *piv;
+  DT *Doff;
 };
 
 // Default bound of an inter-CTA wait of the solve sweeps, in polls (about a second with their back-off).

@@ -388,6 +388,184 @@ __device__ bool potrf_block(const T *src, int lds, T *Lp, int m, int w, int f, i
   return potrf_core<T, T>(src, lds, Lp, m, w, f, c0, s, status, ld, -1.0) == 0;
 }
 
+// (value, index) of the largest value over the warp, the smallest index on ties (every lane gets the result)
+__device__ __forceinline__ void warp_argmax(double &v, int &i) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+    if (ov > v || (ov == v && oi < i)) {
+      v = ov;
+      i = oi;
+    }
+  }
+}
+
+// Bunch-Kaufman LDL^T of a pivot block, the pivot search restricted to the block's w columns (so the supernode
+// partition and every row structure stay the reference's): at column k, with colmax = max_{i>k} |B(i, k)| (row r),
+// a 1 x 1 pivot k when |B(k, k)| >= alpha colmax or |B(k, k)| rowmax >= alpha colmax^2 (rowmax = max_{j != r}
+// |B(r, j)|), a 1 x 1 pivot r when |B(r, r)| >= alpha rowmax, else the 2 x 2 pivot (k, r); alpha = (1 + sqrt 17) / 8
+// (Bunch and Kaufman, Math. Comp. 31, 1977). Each interchange is applied to the block's whole rows, the L columns
+// already computed included, so that P B P^T = L D L^T with L unit lower triangular (L(k + 1, k) = 0 inside a 2 x 2
+// pivot, whose off-diagonal is D(k + 1, k)). A column with no entry at or above tau keeps the reference's static
+// perturbation (|d| < tau -> -+tau, a non-finite one fails; ldlt.mjs:513-522). FP64 arithmetic for every T.
+// S: 64 x 65 doubles of shared workspace (a full symmetric copy, S[j][i] = B(i, j)); src: the updated block (entry
+// (i, j), i >= j, at src[j lds + i]). Writes L to Lp (ld m), D, Doff and piv, adds the inertia (a 2 x 2 pivot with a
+// negative determinant has one negative eigenvalue, with a positive one two when its diagonal is negative) and the
+// perturbed count. Returns false (status set) on a non-finite pivot; nothing is written then. Called by every thread.
+template <class T>
+__device__ bool bk_block(const T *src, int lds, double (*S)[kPanel + 1], T *Lp, int m, int w, int f, int c0, int s,
+                         unsigned long long *status, const LdltArgs<T> &ld) {
+  __shared__ int sPerm[kPanel];
+  __shared__ double sD[kPanel], sE[kPanel], sC0[kPanel], sC1[kPanel];
+  __shared__ int sStep, sKp, sFail, sNeg, sPert;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nthr = blockDim.x;
+  const double tau = ld.scal[1];
+  const double alpha = 0.64038820320220756;  // (1 + sqrt(17)) / 8
+  for (int e = tid; e < kPanel * kPanel; e += nthr) {
+    const int i = e & (kPanel - 1), j = e >> 6;
+    double v = i == j ? 1.0 : 0.0;
+    if (i < w && j < w) v = (double)(i >= j ? src[j * lds + i] : src[i * lds + j]);
+    S[j][i] = v;
+  }
+  if (tid < kPanel) {
+    sPerm[tid] = tid;
+    sD[tid] = 1.0;
+    sE[tid] = 0.0;
+  }
+  if (tid == 0) {
+    sFail = -1;
+    sNeg = 0;
+    sPert = 0;
+  }
+  __syncthreads();
+  for (int k = 0; k < w;) {
+    if (warp == 0) {  // the pivot choice
+      double cm = -1.0;
+      int im = -1;
+      for (int i = k + 1 + lane; i < w; i += 32) {
+        const double a = fabs(S[k][i]);
+        if (a > cm) {
+          cm = a;
+          im = i;
+        }
+      }
+      warp_argmax(cm, im);
+      const double colmax = cm > 0.0 ? cm : 0.0, absakk = fabs(S[k][k]);
+      int step = 1, kp = k;
+      if (colmax > 0.0 && !(absakk >= alpha * colmax)) {  // (a NaN diagonal takes the 1 x 1 path and fails below)
+        double rm = 0.0;
+        for (int j = k + lane; j < w; j += 32)
+          if (j != im) rm = fmax(rm, fabs(S[j][im]));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) rm = fmax(rm, __shfl_xor_sync(0xffffffffu, rm, o));
+        if (absakk * rm >= alpha * colmax * colmax) {
+          kp = k;
+        } else if (fabs(S[im][im]) >= alpha * rm) {
+          kp = im;
+        } else {
+          step = 2;
+          kp = im;
+        }
+      }
+      if (lane == 0) {
+        sStep = step;
+        sKp = kp;
+      }
+    }
+    __syncthreads();
+    const int step = sStep, kp = sKp, kk = k + step - 1, k1 = k + step;
+    if (kp != kk) {  // interchange kk and kp: whole rows (L columns included), then the trailing columns
+      if (tid < w) {
+        const double t = S[tid][kk];
+        S[tid][kk] = S[tid][kp];
+        S[tid][kp] = t;
+      }
+      __syncthreads();
+      if (tid >= k && tid < w) {
+        const double t = S[kk][tid];
+        S[kk][tid] = S[kp][tid];
+        S[kp][tid] = t;
+      }
+      if (tid == 0) {
+        const int t = sPerm[kk];
+        sPerm[kk] = sPerm[kp];
+        sPerm[kp] = t;
+      }
+      __syncthreads();
+    }
+    const int nt = w - k1;
+    if (step == 1) {
+      double d = S[k][k];
+      const bool small = !(fabs(d) >= tau);
+      if (small && isfinite(d)) d = d < 0.0 ? -tau : tau;
+      if (tid < w) sC0[tid] = S[k][tid];  // column k, unscaled
+      if (tid == 0) {
+        sD[k] = d;
+        if (!isfinite(d) && sFail < 0) sFail = k;
+        sNeg += d < 0.0 ? 1 : 0;
+        sPert += small ? 1 : 0;
+      }
+      __syncthreads();
+      if (sFail >= 0) break;  // block-uniform
+      const double inv = 1.0 / d;
+      for (int e = tid; e < nt * nt; e += nthr) {
+        const int i = k1 + e % nt, j = k1 + e / nt;
+        S[j][i] -= sC0[i] * (sC0[j] * inv);
+      }
+      if (tid >= k1 && tid < w) S[k][tid] = sC0[tid] * inv;  // L(i, k)
+    } else {
+      // D_k = e [[a, 1], [1, c]], D_k^-1 = (t / e) [[c, -1], [-1, a]] with a = d11 / e, c = d22 / e, t = 1 / (a c - 1)
+      const double d11 = S[k][k], e21 = S[k][k + 1], d22 = S[k + 1][k + 1];
+      const double a = d11 / e21, c = d22 / e21, te = (1.0 / (a * c - 1.0)) / e21;
+      if (tid < w) {
+        sC0[tid] = S[k][tid];
+        sC1[tid] = S[k + 1][tid];
+      }
+      if (tid == 0) {
+        sD[k] = d11;
+        sD[k + 1] = d22;
+        sE[k] = e21;
+        if (!(isfinite(te) && isfinite(a) && isfinite(c)) && sFail < 0) sFail = k;
+        sNeg += a * c - 1.0 < 0.0 ? 1 : (d11 < 0.0 ? 2 : 0);
+      }
+      __syncthreads();
+      if (sFail >= 0) break;  // block-uniform
+      for (int e = tid; e < nt * nt; e += nthr) {
+        const int i = k1 + e % nt, j = k1 + e / nt;
+        const double l1 = te * (c * sC0[i] - sC1[i]), l2 = te * (a * sC1[i] - sC0[i]);
+        S[j][i] -= l1 * sC0[j] + l2 * sC1[j];
+      }
+      if (tid >= k1 && tid < w) {
+        S[k][tid] = te * (c * sC0[tid] - sC1[tid]);  // L(i, k)
+        S[k + 1][tid] = te * (a * sC1[tid] - sC0[tid]);  // L(i, k + 1)
+      }
+      if (tid == 0) S[k][k + 1] = 0.0;  // L(k + 1, k)
+    }
+    __syncthreads();
+    k += step;
+  }
+  __syncthreads();
+  if (sFail >= 0) {
+    if (tid == 0) atomicMin(status, status_word(f + c0 + sFail, 2, s));
+    return false;
+  }
+  for (int e = tid; e < w * w; e += nthr) {
+    const int i = e % w, j = e / w;
+    if (i >= j) Lp[(int64_t)j * m + i] = (T)(i == j ? 1.0 : S[j][i]);
+  }
+  if (tid < w) {
+    ld.D[f + c0 + tid] = sD[tid];
+    ld.Doff[f + c0 + tid] = sE[tid];
+    ld.piv[f + c0 + tid] = sPerm[tid];
+  }
+  if (tid == 0) {
+    atomicAdd(ld.counts, sNeg);
+    atomicAdd(ld.counts + 1, sPert);
+  }
+  return true;
+}
+
 // TRSM of up to 64 rows [r0, r1) of a front (L: its column-major block, ld m) against its factored pivot block
 // [c0, c0 + w): x_k = (a_k - sum_{c<k} x_c M(k, c)) / M(k, k). Four threads per row, thread (row, q) holds columns
 // 16 q .. 16 q + 15 in registers. Phase p: the threads of quarter p solve their 16 columns (the earlier quarters'
@@ -400,11 +578,17 @@ __device__ bool potrf_block(const T *src, int lds, T *Lp, int m, int w, int f, i
 // before it waited for the pivot block (the strip's own rows are final by then).
 // On return Ws[c][r] holds this strip's update operand (x, or x D for LDL^T) and M[c][r] the solved rows x
 // (c < w, r < r1 - r0; zero elsewhere): a diagonal strip's X_c for its own column block.
-template <class T>
+template <class T, bool BK>
 __device__ void trsm_strip(T *L, int m, int f, int c0, int w, int r0, int r1, int64_t lxp, int64_t sp,
                            __nv_bfloat16 *Shi, __nv_bfloat16 *Slo, const LdltArgs<T> &ld, T (*M)[kPanel + 1],
                            T (*Ws)[kPanel + 1], T *invd, T *dv, T (&x)[16]) {
   const bool ldlt = ld.scal != nullptr;
+  // Bunch-Kaufman pivots (real factors): the strip's columns are taken in the block's pivot order, solved against the
+  // unit L11 (W = x L11^-T, the update's operand), then L21 = W D^-1 with the block's 1 x 1 and 2 x 2 pivots:
+  // column c of L21 is dA[c] W_c + dB[c] W_dP[c] (dP[c] = the other column of its 2 x 2 pivot, dB = 0 for a 1 x 1)
+  constexpr bool bk = BK && !is_cplx<T>::value;
+  __shared__ double dA[kPanel], dB[kPanel];
+  __shared__ int dP[kPanel], sPiv[kPanel];
   const int tid = threadIdx.x, r = tid & (kPanel - 1), q = tid >> 6;
   {  // the pivot block: thread (r, q) loads row r of columns 16 q .. 16 q + 15 (times their pivots for LDL^T), and
      // thread r < 64 the pivot of column r, in one round trip
@@ -414,7 +598,7 @@ __device__ void trsm_strip(T *L, int m, int f, int c0, int w, int r0, int r1, in
       const int c = 16 * q + u;
       v[u] = (r < w && c < r) ? ldcg_v(L + (int64_t)(c0 + c) * m + c0 + r) : T(0);
     }
-    if (ldlt) {
+    if (ldlt && !bk) {
 #pragma unroll
       for (int u = 0; u < 16; u++) {
         const int c = 16 * q + u;
@@ -422,8 +606,36 @@ __device__ void trsm_strip(T *L, int m, int f, int c0, int w, int r0, int r1, in
       }
     }
     if (tid < kPanel) {
-      const T d = tid < w ? (ldlt ? (T)ldcg_v(ld.D + f + c0 + tid) : ldcg_v(L + (int64_t)(c0 + tid) * m + c0 + tid))
-                          : T(1);
+      if constexpr (bk) {
+        {
+          const int c = tid;
+          double a = 1.0, b = 0.0;
+          int pc = c;
+          if (c < w) {
+            const double d = ldcg_v(ld.D + f + c0 + c);
+            const double en = ldcg_v(ld.Doff + f + c0 + c), ep = c > 0 ? ldcg_v(ld.Doff + f + c0 + c - 1) : 0.0;
+            if (en != 0.0 || ep != 0.0) {  // 2 x 2 pivot (c, c + 1) or (c - 1, c): the inverse as in bk_block
+              const bool first = en != 0.0;
+              const double e = first ? en : ep;
+              const double d11 = first ? d : ldcg_v(ld.D + f + c0 + c - 1);
+              const double d22 = first ? ldcg_v(ld.D + f + c0 + c + 1) : d;
+              const double aa = d11 / e, cc = d22 / e, te = (1.0 / (aa * cc - 1.0)) / e;
+              a = te * (first ? cc : aa);
+              b = -te;
+              pc = first ? c + 1 : c - 1;
+            } else {
+              a = 1.0 / d;
+            }
+          }
+          dA[c] = a;
+          dB[c] = b;
+          dP[c] = pc;
+          sPiv[c] = c < w ? __ldcg(ld.piv + f + c0 + c) : c;
+        }
+      }
+      const T d = bk ? T(1)
+                     : tid < w ? (ldlt ? (T)ldcg_v(ld.D + f + c0 + tid) : ldcg_v(L + (int64_t)(c0 + tid) * m + c0 + tid))
+                               : T(1);
       dv[tid] = d;
       invd[tid] = T(1) / d;
     }
@@ -433,6 +645,14 @@ __device__ void trsm_strip(T *L, int m, int f, int c0, int w, int r0, int r1, in
   const int row = r0 + r;
   const bool active = row < r1;
   __syncthreads();
+  if constexpr (bk) {  // the strip's columns in the block's pivot order: x_new(c) = x(piv(c))
+#pragma unroll
+    for (int u = 0; u < 16; u++) Ws[16 * q + u][r] = x[u];
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < 16; u++) x[u] = Ws[sPiv[16 * q + u]][r];
+    __syncthreads();
+  }
   for (int p = 0; p < 4; p++) {
     if (q == p) {  // solve this quarter
 #pragma unroll
@@ -461,9 +681,15 @@ __device__ void trsm_strip(T *L, int m, int f, int c0, int w, int r0, int r1, in
 #pragma unroll
   for (int u = 0; u < 16; u++) {
     const int cc = 16 * q + u;
-    const T xv = x[u];
-    const T wv = ldlt ? xv * dv[cc] : xv;
-    Ws[cc][r] = active && cc < w ? wv : T(0);
+    T xv = x[u];
+    T wv = ldlt ? xv * dv[cc] : xv;
+    if constexpr (bk) {
+      {  // x[u] is W (already in Ws, zero outside the strip and the block); L21 = W D^-1
+        wv = x[u];
+        xv = (T)(dA[cc] * (double)x[u] + dB[cc] * (double)Ws[dP[cc]][r]);
+      }
+    }
+    if (!bk) Ws[cc][r] = active && cc < w ? wv : T(0);
     M[cc][r] = active && cc < w ? xv : T(0);  // the pivot block in M is no longer read
     if (!active || cc >= w) continue;
     L[(int64_t)(c0 + cc) * m + row] = xv;
@@ -532,7 +758,7 @@ constexpr int kGroupSmem = 3 * kPanel * (kPanel + 1) * (int)sizeof(double);
 // two CTAs per SM for the real factors (registers capped at 128); the complex one is held to one by its shared memory
 template <class T>
 constexpr int group_min_blocks() { return is_cplx<T>::value ? 1 : 2; }
-template <class T>
+template <class T, bool BK>
 __global__ void __launch_bounds__(256, group_min_blocks<T>()) k_group_panel(const GroupItem *__restrict__ items,
                                                      const StripTask *__restrict__ strips, int nstrips, int *ticket,
                                                      int *flags, DevPlan P, T *__restrict__ Lx,
@@ -578,7 +804,7 @@ __global__ void __launch_bounds__(256, group_min_blocks<T>()) k_group_panel(cons
       }
     }
     if (!panel_wait(Pf + b, 1, status, P.spin)) return;
-    trsm_strip<T>(L, m, f, c0, w, r0, r1, P.snLxp[s], P.snSp[s], Shi, Slo, ld, M, Ws, invd, dv, x);
+    trsm_strip<T, BK>(L, m, f, c0, w, r0, r1, P.snLxp[s], P.snSp[s], Shi, Slo, ld, M, Ws, invd, dv, x);
     if (jd >= 0) panel_release(Df + jd, b + 1);
     // Update with block b (C -= W_r X_c^T, K = w): a diagonal strip first its own pivot block (X_c = its solved rows,
     // left in M by the TRSM; into Ds), then the blocks between block b and its own; a strip below every remaining
@@ -630,7 +856,11 @@ __global__ void __launch_bounds__(256, group_min_blocks<T>()) k_group_panel(cons
   if (jd >= 0) {  // this strip's own pivot block, fully updated: factor it and publish it (also after a failure)
     const int c0 = g0 + jd * kPanel, w = min(kPanel, g1 - c0);
     __syncthreads();  // Ds complete (also when the strip had no earlier pivot block)
-    potrf_block<T>(&Ds[0][0], kPanel + 1, L + (int64_t)c0 * m + c0, m, w, f, c0, s, status, ld);
+    if constexpr (BK && !is_cplx<T>::value)  // FP64 workspace in M (and Ws for FP32 fronts), both free here
+      bk_block<T>(&Ds[0][0], kPanel + 1, reinterpret_cast<double(*)[kPanel + 1]>(gp_raw), L + (int64_t)c0 * m + c0, m,
+                  w, f, c0, s, status, ld);
+    else
+      potrf_block<T>(&Ds[0][0], kPanel + 1, L + (int64_t)c0 * m + c0, m, w, f, c0, s, status, ld);
     panel_release(Pf + jd, 1);
   }
 }
@@ -894,11 +1124,14 @@ cudaError_t init_solve_multi_attributes();
 cudaError_t init_front_small_attributes();
 cudaError_t init_kernel_attributes() {
   // function attributes belong to the current device's context: the caller runs this once per device
-  cudaError_t e = cudaFuncSetAttribute(k_group_panel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGroupSmem);
+  cudaError_t e =
+      cudaFuncSetAttribute(k_group_panel<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGroupSmem);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_group_panel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGroupSmem / 2);
+    e = cudaFuncSetAttribute(k_group_panel<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGroupSmem);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_group_panel<cplx>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGroupSmem * 2);
+    e = cudaFuncSetAttribute(k_group_panel<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGroupSmem / 2);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_group_panel<cplx, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGroupSmem * 2);
   if (e == cudaSuccess) e = init_mixed_attributes();
   if (e == cudaSuccess) e = init_solve_attributes();
   if (e == cudaSuccess) e = init_solve_multi_attributes();
@@ -925,9 +1158,16 @@ template <class T>
 void launch_group_panel(const GroupItem *items, const StripTask *strips, int nstrips, int *ticket, int *flags,
                         const DevPlan &P, T *Lx, unsigned long long *status, __nv_bfloat16 *Shi, __nv_bfloat16 *Slo,
                         const LdltArgs<T> &ld, cudaStream_t st) {
-  if (nstrips > 0)
-    k_group_panel<T><<<(unsigned)nstrips, 256, 3 * kPanel * (kPanel + 1) * sizeof(T), st>>>(
-        items, strips, nstrips, ticket, flags, P, Lx, status, Shi, Slo, ld);
+  if (nstrips <= 0) return;
+  const size_t smem = 3 * kPanel * (kPanel + 1) * sizeof(T);
+  if constexpr (std::is_same<T, double>::value)  // Bunch-Kaufman pivot blocks (FP64 LDL^T with ld.piv set)
+    if (ld.piv) {
+      k_group_panel<T, true><<<(unsigned)nstrips, 256, smem, st>>>(items, strips, nstrips, ticket, flags, P, Lx, status,
+                                                                  Shi, Slo, ld);
+      return;
+    }
+  k_group_panel<T, false><<<(unsigned)nstrips, 256, smem, st>>>(items, strips, nstrips, ticket, flags, P, Lx, status, Shi,
+                                                               Slo, ld);
 }
 template void launch_group_panel<double>(const GroupItem *, const StripTask *, int, int *, int *, const DevPlan &,
                                          double *, unsigned long long *, __nv_bfloat16 *, __nv_bfloat16 *,

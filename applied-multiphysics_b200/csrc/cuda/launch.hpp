@@ -41,8 +41,11 @@ void launch_update(const TileTask *tasks, int64_t ntasks, const DevPlan &P, doub
                    const unsigned long long *status, cudaStream_t st);
 void launch_permute_in(const double *b, double *y, const int *perm, int n, int q, cudaStream_t st);
 void launch_permute_out(const double *y, double *x, const int *perm, int n, int q, cudaStream_t st);
+// inverses of the diagonal blocks (with each block's pivot order folded in when P.lpiv is set)
 template <class TL>
 void launch_diag_inv(const int *blocks, int nblocks, const DevPlan &P, const TL *Lx, TL *Inv, cudaStream_t st);
+// D solve of a Bunch-Kaufman factor (1 x 1 and 2 x 2 pivots), q interleaved vectors, between the sweeps
+void launch_dsolve_bk(int n, int q, const double *D, const double *Doff, double *y, cudaStream_t st);
 template <class TL>
 void launch_fwd_blocks(const int4 *tasks, int ntasks, int *ticket, const DevPlan &P, const TL *Lx, const TL *Inv,
                        const TL *Mch, double *y, double *T, int *flags, unsigned long long *hand, int epoch, int *done,

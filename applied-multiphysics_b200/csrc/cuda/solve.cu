@@ -35,7 +35,11 @@ constexpr int kSB = 64;  // solve block rows
 
 // ---- inverses of the diagonal blocks -----------------------------------------------------------------------------
 // One CTA per 64-column block b of the pivot columns (all supernodes): X = L_kk^-1, w x w column-major, lower part.
-// Thread j computes column j; L is read through the read-only cache.
+// Thread j computes column j; L is read through the read-only cache. For a Bunch-Kaufman factor the stored block is
+// X P_b (P_b the block's pivot order, a full w x w matrix): the forward sweep's r, taken in the original order of the
+// block's rows, becomes y_b = X P_b r, and the backward sweep's x_b = (X P_b)^T r lands in that original order, so
+// L's earlier columns keep the rows of later blocks in their original order (the interchanges are not applied to
+// the left of a block) and the sweeps need no other change.
 template <class TL>
 __global__ void __launch_bounds__(kSB) k_diag_inv(const int *__restrict__ blocks, DevPlan P, const TL *__restrict__ Lx,
                                                   TL *__restrict__ Inv) {
@@ -63,6 +67,16 @@ __global__ void __launch_bounds__(kSB) k_diag_inv(const int *__restrict__ blocks
   }
   __syncthreads();
   TL *X = Inv + P.invOff[b];
+  if (P.lpiv) {  // Bunch-Kaufman factor: X P_b, column piv(k) of it = column k of X (P_b r = r(piv(.)))
+    __shared__ int kOf[kSB];
+    if (j < w) kOf[__ldg(P.lpiv + P.snF[s] + c0 + j)] = j;
+    __syncthreads();
+    for (int e = threadIdx.x; e < w * w; e += kSB) {
+      const int i = e % w, k = kOf[e / w];
+      X[e] = (TL)(i >= k ? Xs[i][k] : 0.0);
+    }
+    return;
+  }
   for (int e = threadIdx.x; e < w * w; e += kSB) {
     const int i = e % w, jj = e / w;
     X[e] = (TL)(i >= jj ? Xs[i][jj] : 0.0);
@@ -199,8 +213,9 @@ __global__ void __launch_bounds__(256, 3) k_fwd_blocks(const int4 *__restrict__ 
     if (q0 == q1) __syncthreads();
     {  // y = X v[0:nc): thread (row, part) sums columns part, part + 4, ... <= row
       double a2 = 0.0;
+      const int cend = P.lpiv ? nc - 1 : row;  // X P_b is full for a Bunch-Kaufman factor
       if (row < nc)
-        for (int c = part; c <= row; c += 4) a2 += Xs[row][c] * vs[c];
+        for (int c = part; c <= cend; c += 4) a2 += Xs[row][c] * vs[c];
       red[part][row] = a2;
     }
     __syncthreads();
@@ -356,8 +371,9 @@ __global__ void __launch_bounds__(256, 3) k_fwd_blocks(const int4 *__restrict__ 
     // w_b = X_b (v_b - the sums so far), X_b lower triangular: thread (row, part) sums columns part, part + 4, ... <= row
     {
       double a2 = 0.0;
+      const int cend = P.lpiv ? rows - 1 : row;  // X P_b is full for a Bunch-Kaufman factor
       if (rowok)
-        for (int c = part; c <= row; c += 4) a2 += Xs[row][c] * rk[c];
+        for (int c = part; c <= cend; c += 4) a2 += Xs[row][c] * rk[c];
       red[part][row] = a2;
     }
     __syncthreads();
@@ -566,7 +582,7 @@ __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ 
       const int i = tid & (kSB - 1), part = tid >> 6;
       double a2 = 0.0;
       if (i < w)
-        for (int j = i + part; j < w; j += 4) a2 += Xs[j][i] * rk[j];
+        for (int j = (P.lpiv ? 0 : i) + part; j < w; j += 4) a2 += Xs[j][i] * rk[j];  // X P_b full (Bunch-Kaufman)
       red[part][i] = a2;
     }
     __syncthreads();
@@ -610,6 +626,29 @@ __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ 
     __syncthreads();
     if (mine >= ntasks || !run(mine)) return;
   }
+}
+
+// D solve of a Bunch-Kaufman factor between the sweeps (y /= D, ldlt.mjs:629, with its 2 x 2 pivots): q interleaved
+// vectors (y[j q + k]); the first row of a 2 x 2 pivot (Doff[j] != 0) solves both rows with the inverse of bk_block.
+__global__ void k_dsolve_bk(int n, int q, const double *__restrict__ D, const double *__restrict__ Doff,
+                            double *__restrict__ y) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)n * q) return;
+  const int j = (int)(idx / q);
+  const double e = Doff[j];
+  if (j > 0 && Doff[j - 1] != 0.0) return;  // the second row of a 2 x 2 pivot
+  if (e == 0.0) {
+    y[idx] = y[idx] / D[j];
+    return;
+  }
+  const double a = D[j] / e, c = D[j + 1] / e, te = (1.0 / (a * c - 1.0)) / e;
+  const double y0 = y[idx], y1 = y[idx + q];
+  y[idx] = te * (c * y0 - y1);
+  y[idx + q] = te * (a * y1 - y0);
+}
+void launch_dsolve_bk(int n, int q, const double *D, const double *Doff, double *y, cudaStream_t st) {
+  const int64_t tot = (int64_t)n * q;
+  if (tot > 0) k_dsolve_bk<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(n, q, D, Doff, y);
 }
 
 cudaError_t init_solve_attributes() {

@@ -4,12 +4,15 @@
 // column (y_k = v_k / L(k, k), v_i -= L(i, k) y_k), write y and the pass-up vector and count the supernode done.
 // Backward: gather the rows below from the ancestors' final values, then x_k = (r_k - sum_{i > k} L(i, k) x_i) /
 // L(k, k) from the last column down (r = y, divided by D for LDL^T, whose stored L(k, k) is 1), and release the
-// supernode's block flag. Waits are bounded (status set on time-out).
+// supernode's block flag. Waits are bounded (status set on time-out). A Bunch-Kaufman factor (P.lpiv set) takes the
+// pivot rows in its pivot order after the gather and writes x back to their original rows (its D solve runs between
+// the sweeps).
 #pragma once
 #include <cuda_runtime.h>
 
 #include <cstdint>
 
+#include "../host/plan.hpp"
 #include "devplan.cuh"
 #include "sync.cuh"
 
@@ -56,6 +59,7 @@ __device__ bool small_fwd_warp(int s, const DevPlan &P, const TL *__restrict__ L
     __syncwarp();
   }
   double v = vs[lane];
+  if (P.lpiv) v = __shfl_sync(0xffffffffu, v, lane < nc ? P.lpiv[f + lane] : lane);  // Bunch-Kaufman pivot order
   const TL *Lp = Lx + P.snLxp[s];
   double lk = lane < m ? (double)Lp[lane] : 0.0;  // column 0
   for (int k = 0; k < nc; k++) {
@@ -98,7 +102,7 @@ __device__ bool small_bwd_warp(int s, const DevPlan &P, const TL *__restrict__ L
     for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
     if (lane == k) x = (x - p) / lk;
   }
-  if (lane < nc) y[f + lane] = x;
+  if (lane < nc) y[f + (P.lpiv ? P.lpiv[f + lane] : lane)] = x;  // back to the original order (Bunch-Kaufman)
   __syncwarp();  // orders the warp's stores before the release
   if (lane == 0) st_release(flags + P.blkOff[s], epoch);
   return true;
@@ -129,6 +133,18 @@ __device__ bool small_fwd_warp_multi(int s, const DevPlan &P, const TL *__restri
       const int r = map[a];
       if (v0) Vs[64 * r + k0] += __ldcg(tc + (int64_t)a * q + k0);
       if (v1) Vs[64 * r + k1] += __ldcg(tc + (int64_t)a * q + k1);
+    }
+  }
+  if (P.lpiv) {  // Bunch-Kaufman pivot order of the pivot rows (each lane permutes its own vectors)
+    double t0[kTinyFront], t1[kTinyFront];
+    for (int r = 0; r < nc; r++) {
+      const int src = P.lpiv[f + r];
+      t0[r] = v0 ? Vs[64 * src + k0] : 0.0;
+      t1[r] = v1 ? Vs[64 * src + k1] : 0.0;
+    }
+    for (int r = 0; r < nc; r++) {
+      if (v0) Vs[64 * r + k0] = t0[r];
+      if (v1) Vs[64 * r + k1] = t1[r];
     }
   }
   // column k of L is held one row per lane (loaded one column ahead) and broadcast by shuffles
@@ -199,8 +215,9 @@ __device__ bool small_bwd_warp_multi(int s, const DevPlan &P, const TL *__restri
     if (v1) Vs[64 * k + k1] = (Vs[64 * k + k1] - s1) / lkk;
   }
   for (int r = 0; r < nc; r++) {
-    if (v0) y[(int64_t)(f + r) * q + k0] = Vs[64 * r + k0];
-    if (v1) y[(int64_t)(f + r) * q + k1] = Vs[64 * r + k1];
+    const int64_t gr = f + (P.lpiv ? P.lpiv[f + r] : r);  // back to the original order (Bunch-Kaufman)
+    if (v0) y[gr * q + k0] = Vs[64 * r + k0];
+    if (v1) y[gr * q + k1] = Vs[64 * r + k1];
   }
   __syncwarp();
   if (lane < ns) st_release(flags + (int64_t)lane * nflags + P.blkOff[s], epoch);  // one flag per vector slice

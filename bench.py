@@ -338,7 +338,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
+    ap.add_argument("--precision", default="both", choices=["fp64", "fp64-bk", "mixed", "both"],
+                    help="both: fp64 and mixed, and for an LDL^T workload also fp64-bk (FP64 LDL^T with Bunch-Kaufman "
+                         "pivots inside each pivot block)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="elastic3d", choices=sorted(SYSTEMS))
     ap.add_argument("--size", type=int, default=0, help="hexes per side, or problems of the batch (0 = benchmark size)")
@@ -384,7 +386,8 @@ def main():
     flops_factor = sym.flops
     work = flops_factor + solve_flops(sym.colCount, w)  # the same algorithmic work for both precisions
 
-    precisions = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    precisions = (["fp64", "fp64-bk", "mixed"] if args.ldlt else ["fp64", "mixed"]) if args.precision == "both" \
+        else [args.precision]
     results = {}
     dev = torch.device("cuda", local)
     vals_d = torch.from_numpy(w.values).to(dev)
@@ -393,9 +396,11 @@ def main():
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
     tuning = {}
     for prec in precisions:
-        kind, precision = amp.LDLT if args.ldlt else amp.CHOLESKY, amp.FP64 if prec == "fp64" else amp.MIXED
+        kind, precision = amp.LDLT if args.ldlt else amp.CHOLESKY, amp.MIXED if prec == "mixed" else amp.FP64
+        if prec == "fp64-bk":
+            kind = amp.LDLT_BK
         psym = sym
-        if not args.no_autotune:  # the schedule per precision, chosen by timing candidates (per pattern, not timed)
+        if not args.no_autotune and prec != "fp64-bk":  # (the Bunch-Kaufman factor has one schedule: every front dense)  # the schedule per precision, chosen by timing candidates (per pattern, not timed)
             if isinstance(w, _Batch):
                 psym = amp.analyze(w.pat, perm=w.perm, device=local)
             else:
@@ -511,7 +516,7 @@ def main():
         "metric": args.metric, "value": total_work / (R["ms"] * 1e-3) / 1e12, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": R["ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if head == "fp64" else "f32+bf16x3 (f64 refinement)", "data": "synthetic",
+        "dtype": "f32+bf16x3 (f64 refinement)" if head == "mixed" else "f64", "data": "synthetic",
         "config": {"workload": args.desc, "n": n, "nnz": w.pat.nnz, "nnzL": sym.nnzL, "rhs": int(nq),
                    "flops_factor": flops_factor, "flops_step": work,
                    "maxFront": sym.maxFront, "nsuper": sym.nsuper, "levels": sym.nlevels, "precision": head,

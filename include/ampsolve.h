@@ -43,7 +43,9 @@ typedef enum {
 } amp_status;
 
 typedef enum { AMP_ORDER_AMD = 0, AMP_ORDER_ND = 1, AMP_ORDER_ND3 = 2, AMP_ORDER_GIVEN = 3 } amp_ordering;
-typedef enum { AMP_CHOLESKY = 0, AMP_LDLT = 1, AMP_LDLT_COMPLEX = 2 } amp_factor_kind;
+/* AMP_LDLT_BK: the real LDL^T with Bunch-Kaufman 1 x 1 / 2 x 2 pivots inside each 64-column pivot block (FP64); the
+   reference has static perturbation only (ldlt.mjs:513-522), which AMP_LDLT reproduces. */
+typedef enum { AMP_CHOLESKY = 0, AMP_LDLT = 1, AMP_LDLT_COMPLEX = 2, AMP_LDLT_BK = 3 } amp_factor_kind;
 typedef enum { AMP_FP64 = 0, AMP_MIXED = 1 } amp_precision;
 
 typedef struct amp_plan_s amp_plan;     /* symbolic analysis + device schedule of one pattern (reference: sym) */
@@ -193,6 +195,13 @@ AMP_API int amp_solve_gmres(amp_factor *f, const double *b, double *x, int on_de
                     amp_gmres_stats *stats);
 /* num.Lx (the m x nc column-major blocks at Lxp) and D (LDL^T) copied to host; either pointer may be null. */
 AMP_API int amp_factor_download(const amp_factor *f, double *Lx, double *D);
+/* The pivots of an AMP_LDLT_BK factor (n entries each, permuted order; either pointer may be null): Doff[j] = D(j+1, j)
+ * when (j, j + 1) is a 2 x 2 pivot, else 0 (amp_factor_download's D holds every pivot's diagonal); piv[f + c0 + i] =
+ * the column of the 64-column pivot block at c0 of the supernode starting at f that became its i-th pivot. The block's
+ * L columns are in that order and its rows in earlier columns of the supernode stay in the original order, so
+ * P_b (A's Schur complement block) P_b^T = L_bb D_b L_bb^T block by block. No counterpart in the reference (its LDL^T
+ * has static perturbation only, ldlt.mjs:513-522). */
+AMP_API int amp_factor_download_pivots(const amp_factor *f, double *Doff, int32_t *piv);
 AMP_API void amp_factor_destroy(amp_factor *f);
 /* Bound of this factor's device waits, in polls (0 = the defaults: about a second for the solve sweeps' inter-CTA
  * waits, half a second for the tensor-core update's pipeline waits). A wait that runs out ends its kernel early and
