@@ -47,7 +47,7 @@ class AmpError(Exception):
 class _AnalyzeOpts(C.Structure):
     _fields_ = [("ordering", C.c_int), ("relax", C.c_int), ("perm", C.c_void_p), ("x", C.c_void_p),
                 ("y", C.c_void_p), ("z", C.c_void_p), ("leaf", C.c_int), ("device", C.c_int),
-                ("group_blocks", C.c_int), ("small_front", C.c_int)]
+                ("group_blocks", C.c_int), ("small_front", C.c_int), ("defer_updates", C.c_int)]
 
 
 class _PlanInfo(C.Structure):
@@ -89,7 +89,8 @@ class _RefineStats(C.Structure):
 
 class _TuneResult(C.Structure):
     _fields_ = [("group_blocks", C.c_int32), ("small_front", C.c_int32), ("cached", C.c_int32),
-                ("candidates", C.c_int32), ("ms_best", C.c_double), ("ms_default", C.c_double)]
+                ("candidates", C.c_int32), ("ms_best", C.c_double), ("ms_default", C.c_double),
+                ("defer_updates", C.c_int32)]
 
 
 class _EigenOpts(C.Structure):
@@ -283,6 +284,7 @@ def analyze(pat, opts: dict | None = None, **kw) -> SymbolicAnalysis:
     ao.device = int(o.get("device", 0))
     ao.group_blocks = int(o.get("groupBlocks", 0) or 0)
     ao.small_front = int(o.get("smallFront", 0) or 0)
+    ao.defer_updates = int(o.get("deferUpdates", 0) or 0)
     keep = []
     perm = o.get("perm")
     if perm is not None:
@@ -323,7 +325,8 @@ def autotune(sym: SymbolicAnalysis, values, kind: int = CHOLESKY, precision: int
     r = _TuneResult()
     _check(lib().amp_plan_autotune(sym.handle, v.ctypes.data if v.size else None, v.size, 0, kind, precision,
                                    C.byref(r)))
-    return {"groupBlocks": r.group_blocks, "smallFront": r.small_front, "cached": bool(r.cached),
+    return {"groupBlocks": r.group_blocks, "smallFront": r.small_front, "deferUpdates": r.defer_updates,
+            "cached": bool(r.cached),
             "candidates": r.candidates, "msBest": r.ms_best, "msDefault": r.ms_default}
 
 

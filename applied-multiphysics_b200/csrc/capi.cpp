@@ -1092,6 +1092,7 @@ int amp_analyze(int32_t n, const int32_t *rowptr, const int32_t *colidx, const a
       amp::Tuning tune;
       if (o.group_blocks > 0) tune.groupBlocks = o.group_blocks;
       if (o.small_front > 0) tune.smallCut = o.small_front;
+      if (o.defer_updates > 0) tune.deferB = o.defer_updates;
       amp::build_plan(pl->S, pl->P, tune);
       pl->key = amp::pattern_key(A);
       pl->rowptr.assign(rowptr, rowptr + n + 1);
@@ -1187,20 +1188,35 @@ int amp_plan_autotune(amp_plan *pl, const double *values, int64_t nvalues, int v
         amp::build_plan(pl->S, pl->P, it->second);
         r.group_blocks = it->second.groupBlocks;
         r.small_front = it->second.smallCut;
+        r.defer_updates = it->second.deferB;
         r.cached = 1;
         *res = r;
         return (int)AMP_OK;
       }
     }
-    const int groups[3] = {4, 2, 8}, smalls[2] = {128, 64};  // the default first
+    const int groups[3] = {4, 2, 8}, smalls[2] = {128, 64}, defers[2] = {2, 4};  // the default first
     amp_factor_opts fo{kind, precision};
     double best = 0.0;
     amp::Tuning bestT;
+    std::vector<amp::Tuning> cands;
     for (int g : groups)
       for (int sc : smalls) {
         amp::Tuning t;
         t.groupBlocks = g;
         t.smallCut = sc;
+        cands.push_back(t);
+      }
+    // the group and whole-front candidates, then the deferrals of the update beyond the next group with the best
+    for (size_t ci = 0; ci < cands.size() + 2; ci++) {
+      amp::Tuning t;
+      if (ci < cands.size()) {
+        t = cands[ci];
+      } else {
+        t = bestT;
+        t.deferB = defers[ci - cands.size()];
+      }
+      {
+        const int g = t.groupBlocks, sc = t.smallCut;
         amp::build_plan(pl->S, pl->P, t);
         amp_factor *f = nullptr;
         int rc = amp_factor_create(pl, &fo, &f);
@@ -1218,12 +1234,13 @@ int amp_plan_autotune(amp_plan *pl, const double *values, int64_t nvalues, int v
         pl->cxUploaded = false;
         if (rc != AMP_OK) return rc;
         r.candidates++;
-        if (g == 4 && sc == 128) r.ms_default = ms;
+        if (g == 4 && sc == 128 && t.deferB == 1) r.ms_default = ms;
         if (r.candidates == 1 || ms < best) {
           best = ms;
           bestT = t;
         }
       }
+    }
     amp::build_plan(pl->S, pl->P, bestT);
     {
       std::lock_guard<std::mutex> lock(mu);
@@ -1231,6 +1248,7 @@ int amp_plan_autotune(amp_plan *pl, const double *values, int64_t nvalues, int v
     }
     r.group_blocks = bestT.groupBlocks;
     r.small_front = bestT.smallCut;
+    r.defer_updates = bestT.deferB;
     r.ms_best = best;
     *res = r;
     return (int)AMP_OK;

@@ -78,8 +78,10 @@ class ArenaPlanner {
 
 void build_plan(const Symbolic &S, Plan &P, const Tuning &tune) {
   P = Plan();
-  if (tune.groupBlocks < 1 || tune.groupBlocks > 16 || tune.smallCut < kTinyFront || tune.smallCut > kSmallFront)
-    throw std::invalid_argument("schedule parameters out of range (group blocks 1..16, small fronts 32..128)");
+  if (tune.groupBlocks < 1 || tune.groupBlocks > 16 || tune.smallCut < kTinyFront || tune.smallCut > kSmallFront ||
+      tune.deferB < 1 || tune.deferB > 8)
+    throw std::invalid_argument(
+        "schedule parameters out of range (group blocks 1..16, small fronts 32..128, deferred updates 1..8)");
   P.tune = tune;
   const int GW = tune.groupBlocks * kPanel;  // group width
   const int n = S.n, ns = S.nsuper;
@@ -201,6 +203,7 @@ void build_plan(const Symbolic &S, Plan &P, const Tuning &tune) {
   P.tinyMid.clear();
   P.smallPtr.assign(1, 0);
   auto isSmall = [&](int s) { return P.snM[s] <= tune.smallCut; };
+  std::vector<int> appliedB(ns, 0);  // per front: pivot columns whose update every column beyond the next group has
   for (int L = 0; L < P.nlevels; L++) {
     // small fronts: the whole front in one kernel; the rest go through the steps below
     int maxM = 0;
@@ -248,15 +251,17 @@ void build_plan(const Symbolic &S, Plan &P, const Tuning &tune) {
       P.asmLvlBytes[L] += b;
     }
     P.asmLvlPtr[L + 1] = (int64_t)P.asmTasks.size();
+    const int defer = std::max(1, tune.deferB);
     for (int k = 0; k < maxSteps; k++) {
+      const bool doB = (k + 1) % defer == 0;  // part B at this step (every deferB steps)
       StepRange sr;
       sr.panelFlops = sr.updateFlopsA = sr.updateFlopsB = 0;
       sr.item0 = (int64_t)P.groupItems.size();
       sr.strip0 = (int64_t)P.strips.size();
       sr.ticket = P.nGroupTickets++;
       // Group k of every front of the level (pivot columns [g0, g1), up to kGroup pivot blocks) in one group-panel
-      // launch; then the columns right of the group receive its update (K = g1 - g0): part A the next group's
-      // columns, part B the rest.
+      // launch; then the columns right of the group receive the updates of the groups since the last part B
+      // (K = [appliedB, g1), the group alone when deferB = 1): part A the next group's columns, part B the rest.
       struct Region {
         int s, lo, hi, kc0, kw;
       };
@@ -274,7 +279,7 @@ void build_plan(const Symbolic &S, Plan &P, const Tuning &tune) {
           const double w = std::min(kPanel, g1 - c0), c1 = c0 + w;
           sr.panelFlops += w * w * w / 3.0 + (m - c1) * w * w + 2.0 * w * trap(m, c1, g1);
         }
-        if (g1 < nc) regions.push_back({s, g1, nc, g0, g1 - g0});
+        if (g1 < nc) regions.push_back({s, g1, nc, appliedB[s], g1 - appliedB[s]});
       }
       const int64_t i0 = sr.item0, i1 = (int64_t)P.groupItems.size();
       for (int64_t it = i0; it < i1; it++) {  // the diagonal strips of every item first (they take the first tickets)
@@ -303,7 +308,11 @@ void build_plan(const Symbolic &S, Plan &P, const Tuning &tune) {
       for (const Region &g : regions) emit(g, g.lo, std::min(g.lo + GW, g.hi), sr.updateFlopsA);
       sr.tileMid = (int64_t)P.tileTasks.size();
       sr.mixMid = (int64_t)P.mixTiles.size();
-      for (const Region &g : regions) emit(g, g.lo + GW, g.hi, sr.updateFlopsB);
+      if (doB)
+        for (const Region &g : regions) {
+          emit(g, g.lo + GW, g.hi, sr.updateFlopsB);
+          appliedB[g.s] = g.lo;  // every column right of the next group now has the groups before g.lo
+        }
       sr.tile1 = (int64_t)P.tileTasks.size();
       sr.mix1 = (int64_t)P.mixTiles.size();
       P.steps.push_back(sr);

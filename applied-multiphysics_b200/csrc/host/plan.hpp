@@ -86,6 +86,10 @@ struct DenseSched {
 struct Tuning {
   int groupBlocks = kGroup;
   int smallCut = kSmallFront;
+  // The update of the columns beyond the next group (part B) is applied every deferB group steps, with K = the
+  // groups since the last one (the next group's columns still receive every group's update at once, part A): larger
+  // K per pass over the trailing matrix, fewer passes. 1 = every step.
+  int deferB = 1;
 };
 
 struct Plan {

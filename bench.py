@@ -525,6 +525,7 @@ def main():
                    if world > 1 else "1 gpu",
                    "symbolic_ms": symbolic_ms,
                    "schedule": {p: {"group_blocks": t["groupBlocks"], "small_front": t["smallFront"],
+                                    "defer_updates": t["deferUpdates"],
                                     "factor_ms_tuned": t["msBest"], "factor_ms_default": t["msDefault"]}
                                 for p, t in tuning.items()} or "default (group 4 x 64 columns, whole fronts <= 128)"},
         "relres": R["relres"], "ir_steps": R["ir_steps"], "factor_ms": R["factor_ms"],

@@ -62,6 +62,8 @@ typedef struct {
   int device;            /* CUDA device ordinal */
   int group_blocks;      /* schedule: 64-column pivot blocks per group panel (1..16; 0 = the default, 4) */
   int small_front;       /* schedule: largest front factored whole by one CTA (32..128; 0 = the default, 128) */
+  int defer_updates;     /* schedule: the update beyond the next group every this many group steps (K = the groups
+                            since the last; 1..8, 0 = the default, 1) */
 } amp_analyze_opts;
 
 /* Scalars of a symbolic analysis (SymbolicAnalysis fields, types.d.mts:13-20). */
@@ -149,7 +151,8 @@ AMP_API int amp_plan_array(const amp_plan *plan, int field, void *dst, int64_t l
 /* Autotuner of the device schedule (no reference counterpart: the reference's fixed crossovers, e.g. WASM_MIN_FRONT
  * and QCAP in la/wasm/*.mjs, are constants). Times the numeric factorization of `values` (kind, precision as in
  * amp_factor_opts) on this plan's device for each candidate schedule -- pivot blocks per group panel {2, 4, 8} x
- * largest whole-front CTA front {64, 128} -- and keeps the fastest; ties go to the earlier candidate. The choice is
+ * largest whole-front CTA front {64, 128}, then with the fastest of those the update beyond the next group deferred
+ * over {2, 4} group steps -- and keeps the fastest; ties go to the earlier candidate. The choice is
  * cached per (pattern fingerprint, kind, precision) for the process, so another plan of the same pattern takes it
  * without timing (cached = 1). Call before the plan's first amp_factor_create (AMP_INVALID otherwise). */
 typedef struct {
@@ -157,6 +160,7 @@ typedef struct {
   int32_t cached;                     /* 1 when taken from the cache, without timing */
   int32_t candidates;                 /* schedules timed */
   double ms_best, ms_default;         /* factorization time of the choice and of the default schedule */
+  int32_t defer_updates;              /* the chosen schedule's deferral of the update beyond the next group */
 } amp_tune_result;
 AMP_API int amp_plan_autotune(amp_plan *plan, const double *values, int64_t nvalues, int values_on_device, int kind,
                               int precision, amp_tune_result *result);

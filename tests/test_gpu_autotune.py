@@ -1,5 +1,5 @@
-"""The schedule autotuner (amp_plan_autotune) and the schedule parameters it searches: every candidate schedule must
-give the same factor to round-off (parity with the oracle at the FP64 bar), the tuner must return one of its
+"""The schedule autotuner (amp_plan_autotune) and the schedule parameters it searches (group width, whole-front
+cut-off, deferral of the update beyond the next group): every candidate schedule must give the same factor to round-off (parity with the oracle at the FP64 bar), the tuner must return one of its
 candidates, keep it, and hand it to a second plan of the same pattern from its cache without timing again."""
 import numpy as np
 import pytest
@@ -15,11 +15,12 @@ def rel(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
-@pytest.mark.parametrize("gb,sf", [(1, 32), (2, 64), (8, 128), (16, 96)])
+@pytest.mark.parametrize("gb,sf,dfr", [(1, 32, 1), (2, 64, 1), (8, 128, 1), (16, 96, 1), (1, 64, 3), (2, 128, 2),
+                                       (2, 64, 8), (4, 128, 4)])
 @pytest.mark.parametrize("precision", [A.FP64, A.MIXED], ids=["fp64", "mixed"])
-def test_every_schedule_matches_the_oracle(gb, sf, precision):
+def test_every_schedule_matches_the_oracle(gb, sf, dfr, precision):
     w = W.elastic3d(14)
-    sym = A.analyze(w.pat, ordering="nd3", x=w.x, y=w.y, z=w.z, groupBlocks=gb, smallFront=sf)
+    sym = A.analyze(w.pat, ordering="nd3", x=w.x, y=w.y, z=w.z, groupBlocks=gb, smallFront=sf, deferUpdates=dfr)
     so = O.analyze(w.pat, perm=sym.perm)
     ok, Lx, *_ = O.factor(so, w.values)
     b = w.rhs[0]
@@ -35,8 +36,8 @@ def test_every_schedule_matches_the_oracle(gb, sf, precision):
 
 def test_ldlt_schedule_parameters():
     w = W.maxwell3d(8, 2, 12.0, 40.0, 5, 1)
-    for gb, sf in ((1, 32), (8, 64)):
-        sym = A.analyze(w.pat, ordering="nd3", x=w.x, y=w.y, z=w.z, groupBlocks=gb, smallFront=sf)
+    for gb, sf, dfr in ((1, 32, 1), (8, 64, 1), (1, 32, 4)):
+        sym = A.analyze(w.pat, ordering="nd3", x=w.x, y=w.y, z=w.z, groupBlocks=gb, smallFront=sf, deferUpdates=dfr)
         f = A.SupernodalLDLT(sym)
         r = f.factor(w.values)
         so = O.analyze(w.pat, perm=sym.perm)
@@ -49,8 +50,8 @@ def test_autotune_picks_caches_and_keeps_a_candidate():
     w = W.elastic3d(16)
     sym = A.analyze(w.pat, ordering="nd3", x=w.x, y=w.y, z=w.z)
     r = A.autotune(sym, w.values, A.CHOLESKY, A.MIXED)
-    assert not r["cached"] and r["candidates"] == 6
-    assert r["groupBlocks"] in (2, 4, 8) and r["smallFront"] in (64, 128)
+    assert not r["cached"] and r["candidates"] == 8
+    assert r["groupBlocks"] in (2, 4, 8) and r["smallFront"] in (64, 128) and r["deferUpdates"] in (1, 2, 4)
     assert 0 < r["msBest"] <= r["msDefault"]
     num = A.NumericFactor(sym, A.CHOLESKY, A.MIXED)  # the tuned schedule factors correctly
     assert num.factor(w.values)
@@ -60,4 +61,5 @@ def test_autotune_picks_caches_and_keeps_a_candidate():
         A.autotune(sym, w.values, A.CHOLESKY, A.MIXED)
     sym2 = A.analyze(w.pat, ordering="nd3", x=w.x, y=w.y, z=w.z)
     r2 = A.autotune(sym2, w.values, A.CHOLESKY, A.MIXED)
-    assert r2["cached"] and (r2["groupBlocks"], r2["smallFront"]) == (r["groupBlocks"], r["smallFront"])
+    assert r2["cached"] and (r2["groupBlocks"], r2["smallFront"], r2["deferUpdates"]) == \
+        (r["groupBlocks"], r["smallFront"], r["deferUpdates"])

@@ -214,8 +214,8 @@ def test_schedule_parameters_leave_the_symbolic_analysis_unchanged(gb, sf):
     assert np.array_equal(base.tinyFronts, tuned.tinyFronts)
 
 
-@pytest.mark.parametrize("gb,sf", [(17, 128), (4, 129), (4, 20)])
-def test_schedule_parameters_out_of_range_are_rejected(gb, sf):
+@pytest.mark.parametrize("gb,sf,dfr", [(17, 128, 0), (4, 129, 0), (4, 20, 0), (4, 128, 9)])
+def test_schedule_parameters_out_of_range_are_rejected(gb, sf, dfr):
     w = wl.poisson2d(8)
     with pytest.raises(amp.AmpError, match="schedule parameters out of range"):
-        amp.analyze(w.pat, groupBlocks=gb, smallFront=sf)
+        amp.analyze(w.pat, groupBlocks=gb, smallFront=sf, deferUpdates=dfr)
