@@ -33,6 +33,7 @@ int launch_dots(const double *V, int nv, int64_t n, const double *w, double *par
 void launch_gs_update(double *w, const double *V, const double *h, int nv, int64_t n, cudaStream_t st);
 void launch_combine_add(double *x, const double *Z, const double *y, int nv, int64_t n, cudaStream_t st);
 void launch_scale_to(double *v, const double *w, double a, int64_t n, cudaStream_t st);
+void launch_scale_by_norm(double *v, const double *w, const double *norm2, int64_t n, cudaStream_t st);
 void launch_sub_from(double *r, const double *b, const double *y, int64_t n, cudaStream_t st);
 int dot_partials();
 }  // namespace amp
@@ -154,6 +155,7 @@ struct amp_plan_s {
   DevMem mem;
   amp::DevPlan dp{};
   amp::AsmTask *dAsm = nullptr;
+  amp::ChildRange *dAsmCh = nullptr;
   amp::GroupItem *dGroupItems = nullptr;
   amp::StripTask *dStrips = nullptr;
   amp::TileTask *dTile = nullptr, *dUTile = nullptr;
@@ -175,6 +177,7 @@ struct amp_plan_s {
   amp::DenseSched cx;
   bool cxUploaded = false;
   amp::AsmTask *dCxAsm = nullptr;
+  amp::ChildRange *dCxAsmCh = nullptr;
   amp::GroupItem *dCxItems = nullptr;
   amp::StripTask *dCxStrips = nullptr;
   amp::TileTask *dCxTiles = nullptr, *dCxU = nullptr;
@@ -313,6 +316,7 @@ void upload_plan(amp_plan *pl) {
   d.diagSlot = m.upload(P.diagSlot);
   d.solveSmall = m.upload(P.solveSmall);
   pl->dAsm = m.upload(P.asmTasks);
+  pl->dAsmCh = m.upload(P.asmCh);
   pl->dGroupItems = m.upload(P.groupItems);
   pl->dStrips = m.upload(P.strips);
   pl->dTile = m.upload(P.tileTasks);
@@ -459,7 +463,7 @@ void enqueue_factor(amp_factor *f) {
       enqueue_small_fronts<float>(f, L, f->dL32, f->dU32, ld32);
       if (P.asmLvlPtr[L + 1] > P.asmLvlPtr[L])
         timed(f, K_ASSEMBLE, 0.0, P.asmLvlBytes[L] / 2, [&] {
-          amp::launch_assemble<float>(f->plan->dAsm + P.asmLvlPtr[L], P.asmLvlPtr[L + 1] - P.asmLvlPtr[L], dp,
+          amp::launch_assemble<float>(f->plan->dAsm + P.asmLvlPtr[L], f->plan->dAsmCh, P.asmLvlPtr[L + 1] - P.asmLvlPtr[L], dp,
                                       f->dValues, f->dL32, f->dU32, f->dStatus, st);
         });
       LookAhead la{f};
@@ -510,7 +514,7 @@ void enqueue_factor(amp_factor *f) {
     enqueue_small_fronts<double>(f, L, f->dLx, f->dU, ld);
     if (P.asmLvlPtr[L + 1] > P.asmLvlPtr[L])
       timed(f, K_ASSEMBLE, 0.0, P.asmLvlBytes[L], [&] {
-        amp::launch_assemble<double>(f->plan->dAsm + P.asmLvlPtr[L], P.asmLvlPtr[L + 1] - P.asmLvlPtr[L], dp,
+        amp::launch_assemble<double>(f->plan->dAsm + P.asmLvlPtr[L], f->plan->dAsmCh, P.asmLvlPtr[L + 1] - P.asmLvlPtr[L], dp,
                                      f->dValues, f->dLx, f->dU, f->dStatus, st);
       });
     LookAhead la{f};
@@ -897,6 +901,7 @@ void upload_cx(amp_plan *pl) {
   amp::build_dense_all(pl->P, pl->cx);
   DevMem &m = pl->mem;
   pl->dCxAsm = m.upload(pl->cx.asmTasks);
+  pl->dCxAsmCh = m.upload(pl->cx.asmCh);
   pl->dCxItems = m.upload(pl->cx.groupItems);
   pl->dCxStrips = m.upload(pl->cx.strips);
   pl->dCxTiles = m.upload(pl->cx.tileTasks);
@@ -922,7 +927,7 @@ void enqueue_cfactor(amp_factor *f) {
   for (int L = 0; L < P.nlevels; L++) {
     if (D.asmLvlPtr[L + 1] > D.asmLvlPtr[L])
       timed(f, K_ASSEMBLE, 0.0, 0.0, [&] {
-        amp::launch_assemble<amp::cplx>(f->plan->dCxAsm + D.asmLvlPtr[L], D.asmLvlPtr[L + 1] - D.asmLvlPtr[L], dp,
+        amp::launch_assemble<amp::cplx>(f->plan->dCxAsm + D.asmLvlPtr[L], f->plan->dCxAsmCh, D.asmLvlPtr[L + 1] - D.asmLvlPtr[L], dp,
                                         f->dValC, f->dLc, f->dUc, f->dStatus, st);
       });
     for (int k = D.lvlStepPtr[L]; k < D.lvlStepPtr[L + 1]; k++) {
@@ -967,7 +972,7 @@ void enqueue_bkfactor(amp_factor *f) {
   for (int L = 0; L < P.nlevels; L++) {
     if (D.asmLvlPtr[L + 1] > D.asmLvlPtr[L])
       timed(f, K_ASSEMBLE, 0.0, 0.0, [&] {
-        amp::launch_assemble<double>(f->plan->dCxAsm + D.asmLvlPtr[L], D.asmLvlPtr[L + 1] - D.asmLvlPtr[L], dp,
+        amp::launch_assemble<double>(f->plan->dCxAsm + D.asmLvlPtr[L], f->plan->dCxAsmCh, D.asmLvlPtr[L + 1] - D.asmLvlPtr[L], dp,
                                      f->dValues, f->dLx, f->dU, f->dStatus, st);
       });
     for (int k = D.lvlStepPtr[L]; k < D.lvlStepPtr[L + 1]; k++) {
@@ -1194,7 +1199,7 @@ int amp_plan_autotune(amp_plan *pl, const double *values, int64_t nvalues, int v
         return (int)AMP_OK;
       }
     }
-    const int groups[3] = {4, 2, 8}, smalls[2] = {128, 64}, defers[2] = {2, 4};  // the default first
+    const int groups[4] = {4, 2, 8, 1}, smalls[2] = {128, 64}, defers[3] = {2, 4, 8};  // the default first
     amp_factor_opts fo{kind, precision};
     double best = 0.0;
     amp::Tuning bestT;
@@ -1207,7 +1212,7 @@ int amp_plan_autotune(amp_plan *pl, const double *values, int64_t nvalues, int v
         cands.push_back(t);
       }
     // the group and whole-front candidates, then the deferrals of the update beyond the next group with the best
-    for (size_t ci = 0; ci < cands.size() + 2; ci++) {
+    for (size_t ci = 0; ci < cands.size() + 3; ci++) {
       amp::Tuning t;
       if (ci < cands.size()) {
         t = cands[ci];
@@ -1577,7 +1582,7 @@ int amp_solve_gmres(amp_factor *f, const double *b, double *x, int on_device, co
       f->gX = f->gmem.alloc<double>((size_t)n);
       f->gB = f->gmem.alloc<double>((size_t)n);
       f->gPart = f->gmem.alloc<double>((size_t)(m + 1) * amp::dot_partials());
-      f->gH = f->gmem.alloc<double>((size_t)m + 1);
+      f->gH = f->gmem.alloc<double>(3 * ((size_t)m + 1));  // both Gram-Schmidt passes and the norm
       f->gmresCap = m;
     }
     double *V = f->gV, *Z = f->gZ, *r = f->gR, *w = f->gW, *xb = f->gX, *bb = f->gB, *part = f->gPart, *dh = f->gH;
@@ -1621,21 +1626,26 @@ int amp_solve_gmres(amp_factor *f, const double *b, double *x, int on_device, co
         timed(f, K_RESIDUAL, 2.0 * P.patNnz, 12.0 * P.patNnz + 16.0 * n, [&] {
           amp::launch_matvec((int)n, f->plan->dRowptr, f->plan->dColidx, f->dValues, Z + (int64_t)k * n, w, 1, st);
         });
-        // classical Gram-Schmidt twice (as stable as modified Gram-Schmidt, two reductions per iteration)
-        for (int j = 0; j <= k; j++) H[(size_t)j * m + k] = 0.0;
+        // classical Gram-Schmidt twice (as stable as modified Gram-Schmidt, two reductions per iteration); the
+        // coefficients of each pass stay on the device for its update, the next vector is scaled there too, and the
+        // host reads all of them with one synchronisation per iteration
+        double *dh1 = dh, *dh2 = dh + (m + 1), *dnn = dh + 2 * (m + 1);
         for (int pass = 0; pass < 2; pass++) {
-          dots(V, k + 1, w);
-          ck(cudaMemcpyAsync(dh, h.data(), sizeof(double) * (k + 1), cudaMemcpyHostToDevice, st), "h");
+          double *dp = pass ? dh2 : dh1;
+          timed(f, K_KRYLOV, 2.0 * n * (k + 1), 8.0 * n * (k + 2),
+                [&] { return amp::launch_dots(V, k + 1, n, w, part, dp, st); });
           timed(f, K_KRYLOV, 2.0 * n * (k + 1), 8.0 * n * (k + 3),
-                [&] { amp::launch_gs_update(w, V, dh, k + 1, n, st); });
-          for (int j = 0; j <= k; j++) H[(size_t)j * m + k] += h[j];
+                [&] { amp::launch_gs_update(w, V, dp, k + 1, n, st); });
         }
-        dots(w, 1, w);
-        const double hn = std::sqrt(h[0]);
+        timed(f, K_KRYLOV, 2.0 * n, 8.0 * n, [&] { return amp::launch_dots(w, 1, n, w, part, dnn, st); });
+        timed(f, K_KRYLOV, (double)n, 16.0 * n,
+              [&] { amp::launch_scale_by_norm(V + (int64_t)(k + 1) * n, w, dnn, n, st); });
+        std::vector<double> hb(3 * ((size_t)m + 1));
+        ck(cudaMemcpyAsync(hb.data(), dh, sizeof(double) * 3 * (m + 1), cudaMemcpyDeviceToHost, st), "dots");
+        ck(cudaStreamSynchronize(st), "dots");
+        for (int j = 0; j <= k; j++) H[(size_t)j * m + k] = (0.0 + hb[j]) + hb[(m + 1) + j];
+        const double hn = std::sqrt(hb[2 * (m + 1)]);
         H[(size_t)(k + 1) * m + k] = hn;
-        if (hn > 0)
-          timed(f, K_KRYLOV, (double)n, 16.0 * n,
-                [&] { amp::launch_scale_to(V + (int64_t)(k + 1) * n, w, 1.0 / hn, n, st); });
         for (int j = 0; j < k; j++) {  // apply the previous Givens rotations
           const double a = H[(size_t)j * m + k], c = H[(size_t)(j + 1) * m + k];
           H[(size_t)j * m + k] = cs[j] * a + sn[j] * c;

@@ -131,30 +131,14 @@ __device__ __forceinline__ bool failed(const unsigned long long *st) {
 // ---------------------------------------------------------------------------------------------------------------
 // Assembly + extend-add
 // ---------------------------------------------------------------------------------------------------------------
-constexpr int kAsmChildren = 64;  // children whose column ranges an assembly CTA locates up front
+constexpr int kAsmChildren = 64;  // children whose column ranges an assembly CTA stages in shared memory up front
 constexpr int kAsmInFlight = 4;   // extend-add entries per lane in flight
 
-// the columns [b0, b1) of child c's update matrix that map into front columns [j0, j1) (its map is increasing)
-__device__ __forceinline__ int2 child_cols(const DevPlan &P, int c, int j0, int j1) {
-  const int muc = P.snM[c] - P.snNc[c];
-  const int *map = P.eaMap + P.eaPtr[c];
-  int lo = 0, hi = max(muc, 0);
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (map[mid] < j0) lo = mid + 1; else hi = mid;
-  }
-  const int b0 = lo;
-  hi = max(muc, 0);
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (map[mid] < j1) lo = mid + 1; else hi = mid;
-  }
-  return make_int2(b0, lo);
-}
-
+// ranges[t.ch0 + q]: the columns of child q's update matrix that map into the task's front columns (computed with
+// the schedule, so a CTA starts without searching the children's maps)
 template <class T>
-__global__ void __launch_bounds__(256) k_assemble(const AsmTask *__restrict__ tasks, DevPlan P,
-                                                  const value_of<T> *__restrict__ values, T *__restrict__ Lx,
+__global__ void __launch_bounds__(256) k_assemble(const AsmTask *__restrict__ tasks, const ChildRange *__restrict__ ranges,
+                                                  DevPlan P, const value_of<T> *__restrict__ values, T *__restrict__ Lx,
                                                   T *__restrict__ U, const unsigned long long *status) {
   if (failed(status)) return;
   const AsmTask t = tasks[blockIdx.x];
@@ -164,11 +148,12 @@ __global__ void __launch_bounds__(256) k_assemble(const AsmTask *__restrict__ ta
   T *Lp = Lx + P.snLxp[s];
   T *Up = (m > nc) ? U + P.snUoff[s] : nullptr;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  // 0. the child columns mapping into [j0, jend), one child per thread (the first kAsmChildren children; the map of
-  // a child is increasing, so they form one range per child): located while the columns are zeroed
-  __shared__ int2 chRange[kAsmChildren];
+  // 0. the child columns mapping into [j0, jend) (one range per child, the first kAsmChildren children staged in
+  // shared memory while the columns are zeroed)
+  __shared__ ChildRange chRange[kAsmChildren];
   const int q0 = P.chPtr[s], nch = P.chPtr[s + 1] - q0;
-  if ((int)threadIdx.x < min(nch, kAsmChildren)) chRange[threadIdx.x] = child_cols(P, P.chList[q0 + threadIdx.x], j0, jend);
+  const ChildRange *rg = ranges + t.ch0;
+  if ((int)threadIdx.x < min(nch, kAsmChildren)) chRange[threadIdx.x] = rg[threadIdx.x];
   // 1. zero the lower part of the owned columns
   for (int j = j0 + warp; j < jend; j += nwarps)
     for (int i = j + lane; i < m; i += 32) *front_addr(Lp, Up, m, nc, i, j) = T(0);
@@ -201,8 +186,8 @@ __global__ void __launch_bounds__(256) k_assemble(const AsmTask *__restrict__ ta
     if (muc <= 0) continue;  // block-uniform
     const int *map = P.eaMap + P.eaPtr[c];
     const T *Uc = U + P.snUoff[c];
-    const int2 br = q < kAsmChildren ? chRange[q] : child_cols(P, c, j0, jend);
-    for (int b = br.x + warp; b < br.y; b += nwarps) {
+    const ChildRange br = q < kAsmChildren ? chRange[q] : rg[q];
+    for (int b = br.b0 + warp; b < br.b1; b += nwarps) {
       const int jj = map[b];
       const T *col = Uc + (int64_t)b * muc;
       // kAsmInFlight entries per lane in flight: gather the child's values and target rows, then read-modify-write
@@ -1144,16 +1129,16 @@ cudaError_t init_kernel_attributes() {
 }
 
 template <class T>
-void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, const value_of<T> *values, T *Lx, T *U,
-                     const unsigned long long *status, cudaStream_t st) {
-  if (ntasks > 0) k_assemble<T><<<(unsigned)ntasks, 256, 0, st>>>(tasks, P, values, Lx, U, status);
+void launch_assemble(const AsmTask *tasks, const ChildRange *ranges, int64_t ntasks, const DevPlan &P,
+                     const value_of<T> *values, T *Lx, T *U, const unsigned long long *status, cudaStream_t st) {
+  if (ntasks > 0) k_assemble<T><<<(unsigned)ntasks, 256, 0, st>>>(tasks, ranges, P, values, Lx, U, status);
 }
-template void launch_assemble<double>(const AsmTask *, int64_t, const DevPlan &, const double *, double *, double *,
-                                      const unsigned long long *, cudaStream_t);
-template void launch_assemble<float>(const AsmTask *, int64_t, const DevPlan &, const double *, float *, float *,
-                                     const unsigned long long *, cudaStream_t);
-template void launch_assemble<cplx>(const AsmTask *, int64_t, const DevPlan &, const cplx *, cplx *, cplx *,
-                                    const unsigned long long *, cudaStream_t);
+template void launch_assemble<double>(const AsmTask *, const ChildRange *, int64_t, const DevPlan &, const double *,
+                                      double *, double *, const unsigned long long *, cudaStream_t);
+template void launch_assemble<float>(const AsmTask *, const ChildRange *, int64_t, const DevPlan &, const double *,
+                                     float *, float *, const unsigned long long *, cudaStream_t);
+template void launch_assemble<cplx>(const AsmTask *, const ChildRange *, int64_t, const DevPlan &, const cplx *,
+                                    cplx *, cplx *, const unsigned long long *, cudaStream_t);
 template <class T>
 void launch_group_panel(const GroupItem *items, const StripTask *strips, int nstrips, int *ticket, int *flags,
                         const DevPlan &P, T *Lx, unsigned long long *status, __nv_bfloat16 *Shi, __nv_bfloat16 *Slo,
@@ -1178,6 +1163,7 @@ template void launch_group_panel<float>(const GroupItem *, const StripTask *, in
 template void launch_group_panel<cplx>(const GroupItem *, const StripTask *, int, int *, int *, const DevPlan &,
                                        cplx *, unsigned long long *, __nv_bfloat16 *, __nv_bfloat16 *,
                                        const LdltArgs<cplx> &, cudaStream_t);
+
 void launch_update_c(const TileTask *tasks, int64_t ntasks, cplx *Lx, cplx *U, const cplx *W,
                      const unsigned long long *status, cudaStream_t st) {
   if (ntasks > 0) k_update_c<<<(unsigned)ntasks, 256, 0, st>>>(tasks, Lx, U, W, status);

@@ -65,6 +65,14 @@ __global__ void k_scale_to(double *__restrict__ v, const double *__restrict__ w,
   if (i < n) v[i] = a * w[i];
 }
 
+// v = w / sqrt(norm2[0]) (the next Arnoldi vector; left unchanged when the norm is zero, where GMRES stops)
+__global__ void k_scale_by_norm(double *__restrict__ v, const double *__restrict__ w, const double *__restrict__ norm2,
+                                int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const double q = *norm2;
+  if (i < n && q > 0.0) v[i] = (1.0 / sqrt(q)) * w[i];
+}
+
 // r = b - y
 __global__ void k_sub_from(double *__restrict__ r, const double *__restrict__ b, const double *__restrict__ y,
                            int64_t n) {
@@ -88,6 +96,9 @@ void launch_combine_add(double *x, const double *Z, const double *y, int nv, int
 }
 void launch_scale_to(double *v, const double *w, double a, int64_t n, cudaStream_t st) {
   if (n > 0) k_scale_to<<<blocks_for(n), 256, 0, st>>>(v, w, a, n);
+}
+void launch_scale_by_norm(double *v, const double *w, const double *norm2, int64_t n, cudaStream_t st) {
+  if (n > 0) k_scale_by_norm<<<blocks_for(n), 256, 0, st>>>(v, w, norm2, n);
 }
 void launch_sub_from(double *r, const double *b, const double *y, int64_t n, cudaStream_t st) {
   if (n > 0) k_sub_from<<<blocks_for(n), 256, 0, st>>>(r, b, y, n);

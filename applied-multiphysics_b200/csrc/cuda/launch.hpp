@@ -13,9 +13,10 @@ namespace amp {
 
 cudaError_t init_kernel_attributes();  // once per device (with that device current), before its first launch
 
+// ranges: the schedule's per-task child column ranges (AsmTask::ch0 indexes them)
 template <class T>
-void launch_assemble(const AsmTask *tasks, int64_t ntasks, const DevPlan &P, const value_of<T> *values, T *Lx, T *U,
-                     const unsigned long long *status, cudaStream_t st);
+void launch_assemble(const AsmTask *tasks, const ChildRange *ranges, int64_t ntasks, const DevPlan &P,
+                     const value_of<T> *values, T *Lx, T *U, const unsigned long long *status, cudaStream_t st);
 // one group of pivot blocks per item: nstrips strip tasks, ticket and flags zeroed before the factorization
 template <class T>
 void launch_group_panel(const GroupItem *items, const StripTask *strips, int nstrips, int *ticket, int *flags,

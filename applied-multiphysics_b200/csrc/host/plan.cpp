@@ -76,6 +76,20 @@ class ArenaPlanner {
 
 }  // namespace
 
+// An assembly task of front columns [j0, j0 + kAsmCols) of supernode s, with the columns [b0, b1) of each child's
+// update matrix that map into them (a child's map is increasing, so they form one range), in the child order.
+static void add_asm_task(const Plan &P, int s, int j0, std::vector<AsmTask> &tasks, std::vector<ChildRange> &ranges) {
+  const int jend = std::min(j0 + kAsmCols, P.snM[s]);
+  tasks.push_back({s, j0, (int)ranges.size()});
+  for (int q = P.chPtr[s]; q < P.chPtr[s + 1]; q++) {
+    const int c = P.chList[q], muc = std::max(0, P.snM[c] - P.snNc[c]);
+    const int *map = P.eaMap.data() + P.eaPtr[c];
+    const int b0 = (int)(std::lower_bound(map, map + muc, j0) - map);
+    const int b1 = (int)(std::lower_bound(map, map + muc, jend) - map);
+    ranges.push_back({b0, b1});
+  }
+}
+
 void build_plan(const Symbolic &S, Plan &P, const Tuning &tune) {
   P = Plan();
   if (tune.groupBlocks < 1 || tune.groupBlocks > 16 || tune.smallCut < kTinyFront || tune.smallCut > kSmallFront ||
@@ -240,7 +254,7 @@ void build_plan(const Symbolic &S, Plan &P, const Tuning &tune) {
     for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
       int s = P.lvlSn[q];
       if (isSmall(s)) continue;
-      for (int j0 = 0; j0 < P.snM[s]; j0 += kAsmCols) P.asmTasks.push_back({s, j0});
+      for (int j0 = 0; j0 < P.snM[s]; j0 += kAsmCols) add_asm_task(P, s, j0, P.asmTasks, P.asmCh);
       maxSteps = std::max(maxSteps, (P.snNc[s] + GW - 1) / (GW));
       // bytes: value + lowerI + lowerSrc per A entry (16); read U + read/write the parent entry per child entry (24)
       double b = 16.0 * (S.lowerP[P.snF[s] + P.snNc[s]] - S.lowerP[P.snF[s]]);
@@ -437,7 +451,7 @@ void build_dense_all(const Plan &P, DenseSched &D) {
     int maxSteps = 0;
     for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
       const int s = P.lvlSn[q];
-      for (int j0 = 0; j0 < P.snM[s]; j0 += kAsmCols) D.asmTasks.push_back({s, j0});
+      for (int j0 = 0; j0 < P.snM[s]; j0 += kAsmCols) add_asm_task(P, s, j0, D.asmTasks, D.asmCh);
       maxSteps = std::max(maxSteps, (P.snNc[s] + GW - 1) / (GW));
     }
     D.asmLvlPtr[L + 1] = (int64_t)D.asmTasks.size();

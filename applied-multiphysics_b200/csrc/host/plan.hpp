@@ -48,8 +48,12 @@ struct MixTask {  // mixed-precision update tile (128 x 256, 8-aligned start) of
   int ilo, jlo, jend;        // rows >= ilo, columns in [jlo, jend) are updated
   int s;                     // supernode (selects the front's TMA descriptors of the split columns)
 };
-struct AsmTask {  // zero + assemble + extend-add front columns [j0, j0 + 32) of supernode s
-  int s, j0;
+struct AsmTask {  // zero + assemble + extend-add front columns [j0, j0 + kAsmCols) of supernode s; the update-matrix
+                  // columns [b0, b1) of each child that map into them (static) are asmCh[ch0 + q], q in child order
+  int s, j0, ch0;
+};
+struct ChildRange {
+  int b0, b1;
 };
 
 // One group step of a level: the group-panel launch over its items (the level's fronts with a group at this index),
@@ -70,6 +74,7 @@ struct StepRange {
 // schedule's fields of Plan.
 struct DenseSched {
   std::vector<AsmTask> asmTasks;
+  std::vector<ChildRange> asmCh;
   std::vector<int64_t> asmLvlPtr;
   std::vector<GroupItem> groupItems;
   std::vector<StripTask> strips;
@@ -111,6 +116,7 @@ struct Plan {
   std::vector<int> lvlPtr, lvlSn;
   // task lists
   std::vector<AsmTask> asmTasks;
+  std::vector<ChildRange> asmCh;  // per assembly task and child: the child's columns that map into the task's
   std::vector<int64_t> asmLvlPtr;  // per level
   std::vector<double> asmLvlBytes;  // algorithmic bytes of each level's assembly (A entries + extend-add)
   std::vector<GroupItem> groupItems;

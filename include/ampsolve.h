@@ -150,9 +150,9 @@ AMP_API int amp_plan_get_info(const amp_plan *plan, amp_plan_info *info);
 AMP_API int amp_plan_array(const amp_plan *plan, int field, void *dst, int64_t len, int64_t *out_len);
 /* Autotuner of the device schedule (no reference counterpart: the reference's fixed crossovers, e.g. WASM_MIN_FRONT
  * and QCAP in la/wasm/*.mjs, are constants). Times the numeric factorization of `values` (kind, precision as in
- * amp_factor_opts) on this plan's device for each candidate schedule -- pivot blocks per group panel {2, 4, 8} x
+ * amp_factor_opts) on this plan's device for each candidate schedule -- pivot blocks per group panel {1, 2, 4, 8} x
  * largest whole-front CTA front {64, 128}, then with the fastest of those the update beyond the next group deferred
- * over {2, 4} group steps -- and keeps the fastest; ties go to the earlier candidate. The choice is
+ * over {2, 4, 8} group steps -- and keeps the fastest; ties go to the earlier candidate. The choice is
  * cached per (pattern fingerprint, kind, precision) for the process, so another plan of the same pattern takes it
  * without timing (cached = 1). Call before the plan's first amp_factor_create (AMP_INVALID otherwise). */
 typedef struct {
