@@ -238,7 +238,7 @@ struct amp_factor_s {
   // solve workspace (grown on demand)
   DevMem smem;
   int qcap = 0;
-  double *dY = nullptr, *dV = nullptr, *dT = nullptr, *dB = nullptr, *dX = nullptr, *dR = nullptr, *dDX = nullptr,
+  double *dY = nullptr, *dT = nullptr, *dB = nullptr, *dX = nullptr, *dR = nullptr, *dDX = nullptr,
          *dNorms = nullptr;
   int *dFlags = nullptr, *dTickets = nullptr;  // solve block ready flags (epoch-stamped) and per-launch tickets
   unsigned long long *dHand = nullptr;          // chain hand-off of consecutive diagonal blocks (epoch-tagged words)
@@ -339,7 +339,6 @@ void ensure_solve_ws(amp_factor *f, int q) {
   const amp::Plan &P = f->plan->P;
   size_t n = (size_t)P.n;
   f->dY = f->smem.alloc<double>(n * q);
-  f->dV = f->smem.alloc<double>((size_t)(P.nsuper ? P.Sp[P.nsuper] : 0) * q);
   f->dT = f->smem.alloc<double>((size_t)P.solveBufDoubles * q);
   f->dB = f->smem.alloc<double>(n * q);
   f->dX = f->smem.alloc<double>(n * q);
@@ -676,10 +675,10 @@ void device_solve_multi_permuted(amp_factor *f, int q) {
   const double *Dp = f->kind == AMP_LDLT && !f->bk ? f->dD : nullptr;  // Bunch-Kaufman: D solve between the sweeps
   timed(f, K_FORWARD, flops, lbytes, [&] {
     if (f->dL32)
-      amp::launch_fwd_multi<float>(fwdTasks, nf, wide, f->dTickets, dp, f->dL32, f->dInv32, f->dY, f->dV, f->dT, f->dFlags,
+      amp::launch_fwd_multi<float>(fwdTasks, nf, wide, f->dTickets, dp, f->dL32, f->dInv32, f->dY, f->dT, f->dFlags,
                                    nfl, efwd, f->dDone, q, f->dSolveStatus, st);
     else
-      amp::launch_fwd_multi<double>(fwdTasks, nf, wide, f->dTickets, dp, f->dLx, f->dInv, f->dY, f->dV, f->dT, f->dFlags,
+      amp::launch_fwd_multi<double>(fwdTasks, nf, wide, f->dTickets, dp, f->dLx, f->dInv, f->dY, f->dT, f->dFlags,
                                     nfl, efwd, f->dDone, q, f->dSolveStatus, st);
   });
   if (f->bk)

@@ -70,7 +70,7 @@ int multi_slices(int q);
 // wide: the list holds .w = -1 tasks (the kernels with the all-vector path)
 template <class TL>
 void launch_fwd_multi(const int4 *tasks, int ntasks, bool wide, int *ticket, const DevPlan &P, const TL *Lx,
-                      const TL *Inv, double *y, double *V, double *T, int *flags, int nflags, int epoch, int *done,
+                      const TL *Inv, double *y, double *T, int *flags, int nflags, int epoch, int *done,
                       int q, unsigned long long *status, cudaStream_t st);
 template <class TL>
 void launch_bwd_multi(const int4 *tasks, int ntasks, bool wide, int *ticket, const DevPlan &P, const TL *Lx,

@@ -139,6 +139,66 @@ __device__ __forceinline__ void ticket_loop(int *ticket, int ntasks, Run &&run) 
   }
 }
 
+// This task's rows [r0, r0 + rows) of the front vector v_s = [y(f .. f + nc); 0] + the children's pass-up vectors,
+// vectors [vb, vb + qs) of q, into Rs (row r at Rs[r LDR], QW >= qs columns; zero outside): the pivot rows from y,
+// then each child's entries that map into these rows, in the reference's child order. Up to kGatherCh children at a
+// time, one per thread: the thread locates the child's entries for these rows (the map is increasing, so they form
+// one range) and waits for the child's pass-up vectors of slices [sl0, sl0 + nsl), so the searches and the waits of
+// all children overlap and every task of the supernode gathers its own rows in parallel. false: a wait gave up.
+constexpr int kGatherCh = 64;
+template <int QW, int LDR>
+__device__ bool gather_front_rows(const DevPlan &P, int s, int r0, int rows, const double *__restrict__ y,
+                                  const double *__restrict__ T, int *done, int sl0, int nsl, int q, int vb, int qs,
+                                  unsigned long long *status, double *Rs) {
+  __shared__ int2 chA[kGatherCh];
+  __shared__ int64_t chMap[kGatherCh], chT[kGatherCh];
+  const int tid = threadIdx.x, f = P.snF[s], nc = P.snNc[s];
+  for (int e = tid; e < kMB * QW; e += blockDim.x) {
+    const int row = e / QW, k = e % QW;
+    Rs[row * LDR + k] = (row < rows && k < qs && r0 + row < nc) ? y[(int64_t)(f + r0 + row) * q + vb + k] : 0.0;
+  }
+  const int q0 = P.chPtr[s], q1 = P.chPtr[s + 1];
+  for (int qb = q0; qb < q1; qb += kGatherCh) {
+    const int nq = min(kGatherCh, q1 - qb);
+    if (qb > q0) __syncthreads();  // the previous chunk's ranges are consumed
+    int ok = 1;
+    if (tid < nq) {
+      const int c = P.chList[qb + tid];
+      const int muc = P.snM[c] - P.snNc[c];
+      const int *map = P.eaMap + P.eaPtr[c];
+      int lo = 0, hi = muc;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (map[mid] < r0) lo = mid + 1; else hi = mid;
+      }
+      const int a0 = lo;
+      hi = muc;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (map[mid] < r0 + rows) lo = mid + 1; else hi = mid;
+      }
+      chA[tid] = make_int2(a0, lo);
+      chMap[tid] = P.eaPtr[c];
+      chT[tid] = P.snTOff[c];
+      const int need = (muc + kMB - 1) / kMB;
+      for (int sl = sl0; sl < sl0 + nsl && ok; sl++) ok = wait_count(done + (int64_t)sl * P.nsuper + c, need, status, s, P.spin);
+    }
+    if (!__syncthreads_and(ok)) return false;  // block-uniform
+    for (int qq = 0; qq < nq; qq++) {
+      const int *map = P.eaMap + chMap[qq];
+      const double *tc = T + chT[qq] * q + vb;
+      const int a0 = chA[qq].x, na = chA[qq].y - a0;
+      for (int e = tid; e < na * QW; e += blockDim.x) {
+        const int a = a0 + e / QW, k = e % QW;
+        if (k < qs) Rs[(map[a] - r0) * LDR + k] += __ldcg(tc + (int64_t)a * q + k);
+      }
+      __syncthreads();
+    }
+  }
+  if (q0 == q1) __syncthreads();
+  return true;
+}
+
 // ---- tasks of supernodes with few pivot blocks: all q vectors at once on the CUDA cores ----------------------------
 // A task of a supernode with at most two pivot blocks (list entry .w = -1) moves all q <= 64 vectors together: out
 // (64 rows x 64 vectors) = sum of A (64 x 32 L chunk) times B (32 x 64 vector chunk), both in shared memory, each
@@ -165,11 +225,11 @@ __device__ __forceinline__ void mm_tile_w(const double *__restrict__ A, const do
   }
 }
 
-// forward: as the sliced task (diagonal y[block] = X (V[block] - L[block, 0:blk 64] y), below T[block] = V[block] -
+// forward: as the sliced task (diagonal y[block] = X (v[block] - L[block, 0:blk 64] y), below T[block] = v[block] -
 // L[block, 0:nc] y), every vector
 template <class TL>
 __device__ __forceinline__ bool fwd_wide_task(const int4 t, const DevPlan &P, const TL *__restrict__ Lx, const TL *__restrict__ Inv,
-                              double *__restrict__ y, double *__restrict__ V, double *__restrict__ T, int *flags,
+                              double *__restrict__ y, double *__restrict__ T, int *flags,
                               int nflags, int epoch, int *done, int q, int ns, unsigned long long *status,
                               double *msm, int &waitOk) {
   double *As = msm, *Bs = msm + kWKC * kWLd, *Rs = msm + 2 * kWKC * kWLd;
@@ -181,37 +241,8 @@ __device__ __forceinline__ bool fwd_wide_task(const int4 t, const DevPlan &P, co
   const int rows = below ? min(kMB, mu - blk * kMB) : min(kMB, nc - blk * kMB);
   const int ncols = below ? nc : blk * kMB;
   int *myflags = flags + P.blkOff[s];  // the slice-0 set: this supernode releases every slice at once
-  const int64_t vbase = (int64_t)P.Sp[s];
-  if (!below && blk == 0) {
-    for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
-      const int c = P.chList[qq];
-      const int need = (P.snM[c] - P.snNc[c] + kMB - 1) / kMB;
-      if (tid == 0) {  // every vector slice of the child done
-        waitOk = 1;
-        for (int sl = 0; sl < ns && waitOk; sl++)
-          waitOk = wait_count(done + (int64_t)sl * P.nsuper + c, need, status, s, P.spin);
-      }
-      __syncthreads();
-      if (!waitOk) return false;
-    }
-    // v_s = [y(f .. f + nc); 0] + the children's pass-up vectors in the reference's child order
-    for (int64_t e = tid; e < (int64_t)m * q; e += kMultiThreads) {
-      const int r = (int)(e / q), k = (int)(e - (int64_t)r * q);
-      V[(vbase + r) * q + k] = r < nc ? y[(int64_t)(f + r) * q + k] : 0.0;
-    }
-    __syncthreads();
-    for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
-      const int c = P.chList[qq];
-      const int muc = P.snM[c] - P.snNc[c];
-      const int *map = P.eaMap + P.eaPtr[c];
-      const double *tc = T + P.snTOff[c] * q;
-      for (int64_t e = tid; e < (int64_t)muc * q; e += kMultiThreads) {
-        const int a = (int)(e / q), k = (int)(e - (int64_t)a * q);
-        V[(vbase + map[a]) * q + k] += __ldcg(tc + e);
-      }
-      __syncthreads();
-    }
-  }
+  // this task's rows of v_s, every vector, into Rs (every slice of each child done)
+  if (!gather_front_rows<kMQ, kWLd>(P, s, r0, rows, y, T, done, 0, ns, q, 0, q, status, Rs)) return false;
   double acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; i++)
@@ -249,7 +280,7 @@ __device__ __forceinline__ bool fwd_wide_task(const int4 t, const DevPlan &P, co
     mm_tile_w(As, Bs, cw, ty, tx, acc);
     __syncthreads();
   }
-  // R = V[block] - acc (V final once the supernode's first diagonal block is: waited above, or gathered here)
+  // R = v[block] - acc (the task's rows of v in Rs)
   if (below) {
     double *to = T + (P.snTOff[s] + (int64_t)blk * kMB) * q;
 #pragma unroll
@@ -259,7 +290,7 @@ __device__ __forceinline__ bool fwd_wide_task(const int4 t, const DevPlan &P, co
 #pragma unroll
       for (int j = 0; j < 4; j++) {
         const int k = 4 * tx + j;
-        if (k < q) to[(int64_t)row * q + k] = __ldcg(V + (vbase + r0 + row) * q + k) - acc[i][j];
+        if (k < q) to[(int64_t)row * q + k] = Rs[row * kWLd + k] - acc[i][j];
       }
     }
     __syncthreads();
@@ -272,7 +303,7 @@ __device__ __forceinline__ bool fwd_wide_task(const int4 t, const DevPlan &P, co
 #pragma unroll
     for (int j = 0; j < 4; j++) {
       const int k = 4 * tx + j;
-      Rs[row * kWLd + k] = (row < rows && k < q) ? __ldcg(V + (vbase + r0 + row) * q + k) - acc[i][j] : 0.0;
+      Rs[row * kWLd + k] = (row < rows && k < q) ? Rs[row * kWLd + k] - acc[i][j] : 0.0;
       acc[i][j] = 0.0;
     }
   }
@@ -435,13 +466,14 @@ __device__ __forceinline__ bool bwd_wide_task(const int4 t, const DevPlan &P, co
 }
 
 // ---- forward ------------------------------------------------------------------------------------------------------
-// task (s, blk, below) of slice sl: as k_fwd_blocks. Diagonal: y[block] = X (V[block] - L[block, 0:blk 64] y[0:blk 64]);
-// below: T[block] = V[block] - L[block, 0:nc] y[0:nc].
+// task (s, blk, below) of slice sl: as k_fwd_blocks. Diagonal: y[block] = X (v[block] - L[block, 0:blk 64] y[0:blk 64]);
+// below: T[block] = v[block] - L[block, 0:nc] y[0:nc], where v[block] is the task's rows of the front vector, gathered
+// by the task itself (gather_front_rows).
 template <class TL, bool WIDE>
 __global__ void __launch_bounds__(kMultiThreads, kMultiCtas) k_fwd_multi(const int4 *__restrict__ tasks, int ntasks, int ns,
                                                                 int *__restrict__ ticket, DevPlan P,
                                                                 const TL *__restrict__ Lx, const TL *__restrict__ Inv,
-                                                                double *__restrict__ y, double *__restrict__ V,
+                                                                double *__restrict__ y,
                                                                 double *__restrict__ T, int *__restrict__ flags,
                                                                 int nflags, int epoch, int *__restrict__ done, int q,
                                                                 unsigned long long *status) {
@@ -465,7 +497,6 @@ __global__ void __launch_bounds__(kMultiThreads, kMultiCtas) k_fwd_multi(const i
     const int ncols = below ? nc : blk * kMB;
     int *myflags = flags + (int64_t)sl * nflags + P.blkOff[s];
     int *mydone = done + (int64_t)sl * P.nsuper;
-    const int64_t vbase = (int64_t)P.Sp[s];
     if (!below) {  // the inverse of the diagonal block, [k][m], arrives while the task sums
       const TL *X = Inv + P.invOff[P.blkOff[s] + blk];
       for (int e = tid; e < kMB * kMB; e += kMultiThreads) {
@@ -475,32 +506,8 @@ __global__ void __launch_bounds__(kMultiThreads, kMultiCtas) k_fwd_multi(const i
       }
       asm volatile("cp.async.commit_group;\n" ::: "memory");
     }
-    if (!below && blk == 0) {
-      for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
-        const int c = P.chList[qq];
-        const int need = (P.snM[c] - P.snNc[c] + kMB - 1) / kMB;
-        if (tid == 0) waitOk = wait_count(mydone + c, need, status, s, P.spin);
-        __syncthreads();
-        if (!waitOk) return bail();
-      }
-      // v_s = [y(f .. f + nc); 0] + the children's pass-up vectors in the reference's child order (this slice)
-      for (int e = tid; e < m * kQS; e += kMultiThreads) {
-        const int r = e >> 4, k = e & (kQS - 1);
-        if (k < qs) V[(vbase + r) * q + vb + k] = r < nc ? y[(int64_t)(f + r) * q + vb + k] : 0.0;
-      }
-      __syncthreads();
-      for (int qq = P.chPtr[s]; qq < P.chPtr[s + 1]; qq++) {
-        const int c = P.chList[qq];
-        const int muc = P.snM[c] - P.snNc[c];
-        const int *map = P.eaMap + P.eaPtr[c];
-        const double *tc = T + P.snTOff[c] * q;
-        for (int e = tid; e < muc * kQS; e += kMultiThreads) {
-          const int a = e >> 4, k = e & (kQS - 1);
-          if (k < qs) V[(vbase + map[a]) * q + vb + k] += __ldcg(tc + (int64_t)a * q + vb + k);
-        }
-        __syncthreads();
-      }
-    }
+    // this task's rows of v_s (this slice) into Rs, gathered by every task of the supernode in parallel
+    if (!gather_front_rows<kQS, kLdB>(P, s, r0, rows, y, T, done, sl, 1, q, vb, qs, status, Rs)) return bail();
     double c[2][4];
 #pragma unroll
     for (int nb = 0; nb < 2; nb++)
@@ -540,7 +547,7 @@ __global__ void __launch_bounds__(kMultiThreads, kMultiCtas) k_fwd_multi(const i
       __syncthreads();
     }
     halves_sum(c, As, warp, lane);
-    // R = V[block] - acc (V final once the supernode's first diagonal block is: waited above, or gathered here)
+    // R = v[block] - acc (the task's rows of v in Rs)
     if (below) {
       if (warp < 4) {
         double *to = T + (P.snTOff[s] + (int64_t)blk * kMB) * q + vb;
@@ -549,7 +556,7 @@ __global__ void __launch_bounds__(kMultiThreads, kMultiCtas) k_fwd_multi(const i
 #pragma unroll
           for (int v = 0; v < 4; v++) {
             const int row = acc_row(warp, lane, v), n = acc_vec(lane, nb, v);
-            if (row < rows && n < qs) to[(int64_t)row * q + n] = __ldcg(V + (vbase + r0 + row) * q + vb + n) - c[nb][v];
+            if (row < rows && n < qs) to[(int64_t)row * q + n] = Rs[row * kLdB + n] - c[nb][v];
           }
       }
       __syncthreads();
@@ -562,7 +569,7 @@ __global__ void __launch_bounds__(kMultiThreads, kMultiCtas) k_fwd_multi(const i
 #pragma unroll
         for (int v = 0; v < 4; v++) {
           const int row = acc_row(warp, lane, v), n = acc_vec(lane, nb, v);
-          Rs[row * kLdB + n] = (row < rows && n < qs) ? __ldcg(V + (vbase + r0 + row) * q + vb + n) - c[nb][v] : 0.0;
+          Rs[row * kLdB + n] = (row < rows && n < qs) ? Rs[row * kLdB + n] - c[nb][v] : 0.0;
         }
     }
 #pragma unroll
@@ -603,7 +610,7 @@ __global__ void __launch_bounds__(kMultiThreads, kMultiCtas) k_fwd_multi(const i
       return waitOk != 0;
     }
     if constexpr (WIDE) {
-      if (t.w < 0) return fwd_wide_task<TL>(t, P, Lx, Inv, y, V, T, flags, nflags, epoch, done, q, ns, status, msm, waitOk);
+      if (t.w < 0) return fwd_wide_task<TL>(t, P, Lx, Inv, y, T, flags, nflags, epoch, done, q, ns, status, msm, waitOk);
     }
     return run_slice(t, t.w);
   };
@@ -933,12 +940,12 @@ static int multi_grid(int64_t ntasks) {
 
 template <class TL>
 void launch_fwd_multi(const int4 *tasks, int ntasks, bool wide, int *ticket, const DevPlan &P, const TL *Lx,
-                      const TL *Inv, double *y, double *V, double *T, int *flags, int nflags, int epoch, int *done,
+                      const TL *Inv, double *y, double *T, int *flags, int nflags, int epoch, int *done,
                       int q, unsigned long long *status, cudaStream_t st) {
   const int ns = multi_slices(q);
   if (ntasks <= 0) return;
   auto k = wide ? k_fwd_multi<TL, true> : k_fwd_multi<TL, false>;
-  k<<<multi_grid(ntasks), kMultiThreads, multi_smem<TL>(), st>>>(tasks, ntasks, ns, ticket, P, Lx, Inv, y, V, T,
+  k<<<multi_grid(ntasks), kMultiThreads, multi_smem<TL>(), st>>>(tasks, ntasks, ns, ticket, P, Lx, Inv, y, T,
                                                                   flags, nflags, epoch, done, q, status);
 }
 template <class TL>
@@ -969,10 +976,10 @@ void launch_residual_multi(int n, const int *rowptr, const int *colidx, const do
   k_residual_multi<<<grid, 256, 0, st>>>(n, rowptr, colidx, val, x, b, r, norms, q, rowGroup);
 }
 template void launch_fwd_multi<double>(const int4 *, int, bool, int *, const DevPlan &, const double *,
-                                       const double *, double *, double *, double *, int *, int, int, int *, int,
+                                       const double *, double *, double *, int *, int, int, int *, int,
                                        unsigned long long *, cudaStream_t);
 template void launch_fwd_multi<float>(const int4 *, int, bool, int *, const DevPlan &, const float *, const float *,
-                                      double *, double *, double *, int *, int, int, int *, int, unsigned long long *,
+                                      double *, double *, int *, int, int, int *, int, unsigned long long *,
                                       cudaStream_t);
 template void launch_bwd_multi<double>(const int4 *, int, bool, int *, const DevPlan &, const double *,
                                        const double *, const double *, double *, int *, int, int, int,
