@@ -307,16 +307,27 @@ def run_reference(args, rank):
 
 # DRAM bytes per launch of the roofline kernel (dram__bytes_read.sum + dram__bytes_write.sum from one ncu capture;
 # profiles/ names the command). Keyed by (workload, size, precision, kernel class).
+# DRAM bytes per launch of the dominant kernel: the largest tcgen05 update launch of an elastic3d-32 mixed factor moves
+# 169.3 MB for 26.2 GFLOP (ncu dram__bytes_read.sum + dram__bytes_write.sum), scaled by the flops of an average cfg2
+# update launch (764.6 GFLOP over 183 launches)
 TRAFFIC = {
-    ("elastic3d", 40, "mixed", "update_syrk"): 50.229e9 / 2485,
+    ("elastic3d", 40, "mixed", "update_syrk"): 169.3e6 / 26.2e9 * 764.6e9 / 183,
 }
+
+
+def schedule_kw(args) -> dict:
+    """analyze options of --schedule G,S,D (pivot blocks per group, largest whole front, deferral of part B)"""
+    if not args.schedule:
+        return {}
+    g, sf, d = (int(v) for v in args.schedule.split(","))
+    return {"groupBlocks": g, "smallFront": sf, "deferUpdates": d}
 
 
 def one_factor(args, w, amp, local):
     if isinstance(w, _Batch):
-        sym = amp.analyze(w.pat, perm=w.perm, device=local)
+        sym = amp.analyze(w.pat, perm=w.perm, device=local, **schedule_kw(args))
     else:
-        sym = amp.analyze(w.pat, ordering="nd3", x=w.x, y=w.y, z=w.z, device=local)
+        sym = amp.analyze(w.pat, ordering="nd3", x=w.x, y=w.y, z=w.z, device=local, **schedule_kw(args))
     prec = amp.FP64 if args.precision == "fp64" else amp.MIXED
     num = amp.NumericFactor(sym, amp.LDLT if args.ldlt else amp.CHOLESKY, prec)
     num.profile(True)  # direct launches, each bracketed by events, in stream order
@@ -346,6 +357,9 @@ def main():
     ap.add_argument("--size", type=int, default=0, help="hexes per side, or problems of the batch (0 = benchmark size)")
     ap.add_argument("--ref-budget", type=float, default=240.0, help="wall seconds of the reference arm's steps")
     ap.add_argument("--no-autotune", action="store_true", help="the default schedule instead of the autotuned one")
+    ap.add_argument("--schedule", default="",
+                    help="G,S,D: a given schedule for every precision instead of the autotuned one (pivot blocks per "
+                         "group panel, largest whole front, part-B deferral), e.g. 2,128,4")
     ap.add_argument("--one-factor", action="store_true",
                     help="profiling case: one factorization of the workload (first precision of --precision) with "
                          "direct launches in stream order; prints the per-class launch index of the longest group "
@@ -400,7 +414,14 @@ def main():
         if prec == "fp64-bk":
             kind = amp.LDLT_BK
         psym = sym
-        if not args.no_autotune and prec != "fp64-bk":  # (the Bunch-Kaufman factor has one schedule: every front dense)  # the schedule per precision, chosen by timing candidates (per pattern, not timed)
+        # the schedule per precision, chosen by timing candidates (per pattern, not timed); the Bunch-Kaufman factor
+        # has one schedule (every front dense)
+        if args.schedule and prec != "fp64-bk":
+            if isinstance(w, _Batch):
+                psym = amp.analyze(w.pat, perm=w.perm, device=local, **schedule_kw(args))
+            else:
+                psym = amp.analyze(w.pat, ordering="nd3", x=w.x, y=w.y, z=w.z, device=local, **schedule_kw(args))
+        elif not args.no_autotune and prec != "fp64-bk":
             if isinstance(w, _Batch):
                 psym = amp.analyze(w.pat, perm=w.perm, device=local)
             else:
@@ -527,7 +548,8 @@ def main():
                    "schedule": {p: {"group_blocks": t["groupBlocks"], "small_front": t["smallFront"],
                                     "defer_updates": t["deferUpdates"],
                                     "factor_ms_tuned": t["msBest"], "factor_ms_default": t["msDefault"]}
-                                for p, t in tuning.items()} or "default (group 4 x 64 columns, whole fronts <= 128)"},
+                                for p, t in tuning.items()} or (f"given (--schedule {args.schedule})" if args.schedule
+                                                                else "default (group 4 x 64 columns, whole fronts <= 128)")},
         "relres": R["relres"], "ir_steps": R["ir_steps"], "factor_ms": R["factor_ms"],
         "e2e": {"value": total_work / (R["e2e_ms"] * 1e-3) / 1e12, "unit": UNIT,
                 "h2d_bytes_per_step": int(8 * w.pat.nnz + 8 * n * nq), "d2h_bytes_per_step": int(8 * n * nq),
