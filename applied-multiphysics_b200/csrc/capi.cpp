@@ -673,12 +673,15 @@ void device_solve_multi_permuted(amp_factor *f, int q) {
   int4 *fwdTasks = f->plan->dFwdSl[ns - 1], *bwdTasks = f->plan->dBwdSl[ns - 1];
   const bool wide = f->plan->wideSl[ns - 1];
   const double *Dp = f->kind == AMP_LDLT && !f->bk ? f->dD : nullptr;  // Bunch-Kaufman: D solve between the sweeps
+  const bool chain = f->kind != AMP_LDLT;  // Cholesky: chain matrices of consecutive diagonal blocks
   timed(f, K_FORWARD, flops, lbytes, [&] {
     if (f->dL32)
-      amp::launch_fwd_multi<float>(fwdTasks, nf, wide, f->dTickets, dp, f->dL32, f->dInv32, f->dY, f->dT, f->dFlags,
+      amp::launch_fwd_multi<float>(fwdTasks, nf, wide, f->dTickets, dp, f->dL32, f->dInv32, chain ? f->dMch32 : nullptr,
+                                   f->dY, f->dT, f->dFlags,
                                    nfl, efwd, f->dDone, q, f->dSolveStatus, st);
     else
-      amp::launch_fwd_multi<double>(fwdTasks, nf, wide, f->dTickets, dp, f->dLx, f->dInv, f->dY, f->dT, f->dFlags,
+      amp::launch_fwd_multi<double>(fwdTasks, nf, wide, f->dTickets, dp, f->dLx, f->dInv, chain ? f->dMch : nullptr,
+                                    f->dY, f->dT, f->dFlags,
                                     nfl, efwd, f->dDone, q, f->dSolveStatus, st);
   });
   if (f->bk)
@@ -686,10 +689,12 @@ void device_solve_multi_permuted(amp_factor *f, int q) {
           [&] { amp::launch_dsolve_bk(P.n, q, f->dD, f->dDoff, f->dY, st); });
   timed(f, K_BACKWARD, flops, lbytes, [&] {
     if (f->dL32)
-      amp::launch_bwd_multi<float>(bwdTasks, nb, wide, f->dTickets + 1, dp, f->dL32, f->dInv32, Dp, f->dY, f->dFlags, nfl,
+      amp::launch_bwd_multi<float>(bwdTasks, nb, wide, f->dTickets + 1, dp, f->dL32, f->dInv32,
+                                   chain ? f->dGch32 : nullptr, Dp, f->dY, f->dFlags, nfl,
                                    ebwd, q, f->dSolveStatus, st);
     else
-      amp::launch_bwd_multi<double>(bwdTasks, nb, wide, f->dTickets + 1, dp, f->dLx, f->dInv, Dp, f->dY, f->dFlags, nfl,
+      amp::launch_bwd_multi<double>(bwdTasks, nb, wide, f->dTickets + 1, dp, f->dLx, f->dInv, chain ? f->dGch : nullptr,
+                                    Dp, f->dY, f->dFlags, nfl,
                                     ebwd, q, f->dSolveStatus, st);
   });
 }

@@ -68,14 +68,15 @@ void launch_chain_mats(const int2 *tasks, int ntasks, const DevPlan &P, const TL
 int multi_max_vectors();
 int multi_slices(int q);
 // wide: the list holds .w = -1 tasks (the kernels with the all-vector path)
+// Mch / Gch: the chain matrices of a Cholesky factor (launch_chain_mats), or null (LDL^T: substitution order)
 template <class TL>
 void launch_fwd_multi(const int4 *tasks, int ntasks, bool wide, int *ticket, const DevPlan &P, const TL *Lx,
-                      const TL *Inv, double *y, double *T, int *flags, int nflags, int epoch, int *done,
+                      const TL *Inv, const TL *Mch, double *y, double *T, int *flags, int nflags, int epoch, int *done,
                       int q, unsigned long long *status, cudaStream_t st);
 template <class TL>
 void launch_bwd_multi(const int4 *tasks, int ntasks, bool wide, int *ticket, const DevPlan &P, const TL *Lx,
-                      const TL *Inv, const double *Dpiv, double *y, int *flags, int nflags, int epoch, int q,
-                      unsigned long long *status, cudaStream_t st);
+                      const TL *Inv, const TL *Gch, const double *Dpiv, double *y, int *flags, int nflags, int epoch,
+                      int q, unsigned long long *status, cudaStream_t st);
 void launch_to_interleaved(const double *B, double *Yil, int n, int q, cudaStream_t st);
 void launch_from_interleaved(const double *Xil, double *X, int n, int q, cudaStream_t st);
 void launch_rows_permute(const double *src, double *dst, const int *perm, int n, int q, bool scatter, cudaStream_t st);

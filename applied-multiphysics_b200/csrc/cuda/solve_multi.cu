@@ -468,12 +468,15 @@ __device__ __forceinline__ bool bwd_wide_task(const int4 t, const DevPlan &P, co
 // ---- forward ------------------------------------------------------------------------------------------------------
 // task (s, blk, below) of slice sl: as k_fwd_blocks. Diagonal: y[block] = X (v[block] - L[block, 0:blk 64] y[0:blk 64]);
 // below: T[block] = v[block] - L[block, 0:nc] y[0:nc], where v[block] is the task's rows of the front vector, gathered
-// by the task itself (gather_front_rows).
+// by the task itself (gather_front_rows). With the chain matrices of a Cholesky factor (Mch, see k_chain_mats), a
+// diagonal task b >= 1 forms W = X (v[block] - L[block, 0:(b-1) 64] y) before its last wait and then, after block
+// b - 1's flag, y[block] = W - M_b y[block b - 1]: one 64 x 64 product per chain step instead of the block's last
+// chunk, the reduction and the inverse product.
 template <class TL, bool WIDE>
 __global__ void __launch_bounds__(kMultiThreads, kMultiCtas) k_fwd_multi(const int4 *__restrict__ tasks, int ntasks, int ns,
                                                                 int *__restrict__ ticket, DevPlan P,
                                                                 const TL *__restrict__ Lx, const TL *__restrict__ Inv,
-                                                                double *__restrict__ y,
+                                                                const TL *__restrict__ Mch, double *__restrict__ y,
                                                                 double *__restrict__ T, int *__restrict__ flags,
                                                                 int nflags, int epoch, int *__restrict__ done, int q,
                                                                 unsigned long long *status) {
@@ -494,7 +497,8 @@ __global__ void __launch_bounds__(kMultiThreads, kMultiCtas) k_fwd_multi(const i
     const TL *Lp = Lx + P.snLxp[s];
     const int r0 = below ? nc + blk * kMB : blk * kMB;
     const int rows = below ? min(kMB, mu - blk * kMB) : min(kMB, nc - blk * kMB);
-    const int ncols = below ? nc : blk * kMB;
+    const bool chain = Mch != nullptr && !below && blk > 0;  // block b - 1 enters through M_b after the last wait
+    const int ncols = below ? nc : (chain ? blk - 1 : blk) * kMB;
     int *myflags = flags + (int64_t)sl * nflags + P.blkOff[s];
     int *mydone = done + (int64_t)sl * P.nsuper;
     if (!below) {  // the inverse of the diagonal block, [k][m], arrives while the task sums
@@ -585,6 +589,57 @@ __global__ void __launch_bounds__(kMultiThreads, kMultiCtas) k_fwd_multi(const i
       if (k0 < rows) mma_k16<true>(Xs, kLdX, Rs, k0, mw, lane, c);
     }
     halves_sum(c, As, warp, lane);
+    if (chain) {
+      // W stays in Rs (its R was consumed by the product); M_b arrives in Xs while the task waits for block b - 1
+      if (warp < 4) {
+#pragma unroll
+        for (int nb = 0; nb < 2; nb++)
+#pragma unroll
+          for (int v = 0; v < 4; v++) {
+            const int row = acc_row(warp, lane, v), n = acc_vec(lane, nb, v);
+            Rs[row * kLdB + n] = c[nb][v];
+          }
+      }
+#pragma unroll
+      for (int nb = 0; nb < 2; nb++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) c[nb][v] = 0.0;
+      __syncthreads();  // every warp is done with X in Xs
+      {  // M_b (rows x 64, column-major), [k][m] like X
+        const TL *M = Mch + (int64_t)(P.blkOff[s] - s + blk - 1) * kMB * kMB;
+        for (int e = tid; e < kMB * kMB; e += kMultiThreads) {
+          const int i = e & (kMB - 1), k = e >> 6;
+          const bool ok = i < rows;
+          cp_async_el(Xs + k * kLdX + i, ok ? M + (int64_t)k * kMB + i : M, (int)sizeof(TL), ok);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+      }
+      if (tid == 0) waitOk = wait_flag(myflags + blk - 1, epoch, status, s, P.spin);
+      __syncthreads();
+      if (!waitOk) return bail();
+      const int cp = (blk - 1) * kMB;  // block b - 1: 64 columns (not the last block)
+      for (int e = tid; e < kMB * kQS; e += kMultiThreads) {
+        const int k = e >> 4, n = e & (kQS - 1);
+        Bs[k * kLdB + n] = n < qs ? __ldcg(y + (int64_t)(f + cp + k) * q + vb + n) : 0.0;
+      }
+      cp_async_all();
+      __syncthreads();
+#pragma unroll
+      for (int h = 0; h < 2; h++) mma_k16<true>(Xs, kLdX, Bs, 32 * h + 16 * kh, mw, lane, c);
+      halves_sum(c, As, warp, lane);
+      if (warp < 4) {
+#pragma unroll
+        for (int nb = 0; nb < 2; nb++)
+#pragma unroll
+          for (int v = 0; v < 4; v++) {
+            const int row = acc_row(warp, lane, v), n = acc_vec(lane, nb, v);
+            if (row < rows && n < qs) y[(int64_t)(f + r0 + row) * q + vb + n] = Rs[row * kLdB + n] - c[nb][v];
+          }
+      }
+      __syncthreads();
+      if (tid == 0) st_release(myflags + blk, epoch);
+      return true;
+    }
     if (warp < 4) {
 #pragma unroll
       for (int nb = 0; nb < 2; nb++)
@@ -619,11 +674,13 @@ __global__ void __launch_bounds__(kMultiThreads, kMultiCtas) k_fwd_multi(const i
 
 // ---- backward -----------------------------------------------------------------------------------------------------
 // task (s, blk) of slice sl: x[block] = X^T (y[block] (/ D for LDL^T) - L[rows below the block, block columns]^T
-// x[those rows]).
+// x[those rows]). With the chain matrices of a Cholesky factor (Gch), block b + 1 is left out of the sum and enters
+// after its flag as x[block] = W - G_b^T x[block b + 1], W = X^T (y[block] - the other rows' terms).
 template <class TL, bool WIDE>
 __global__ void __launch_bounds__(kMultiThreads, kMultiCtas) k_bwd_multi(const int4 *__restrict__ tasks, int ntasks, int ns,
                                                                 int *__restrict__ ticket, DevPlan P,
                                                                 const TL *__restrict__ Lx, const TL *__restrict__ Inv,
+                                                                const TL *__restrict__ Gch,
                                                                 const double *__restrict__ Dpiv,
                                                                 double *__restrict__ y, int *__restrict__ flags,
                                                                 int nflags, int epoch, int q,
@@ -663,8 +720,9 @@ __global__ void __launch_bounds__(kMultiThreads, kMultiCtas) k_bwd_multi(const i
       for (int v = 0; v < 4; v++) c[nb2][v] = 0.0;
     // chunks: the rows below the supernode [nc, m) in kKC steps from the last down, then pivot blocks nb - 1 .. blk + 1
     // (two chunks each)
+    const bool chain = Gch != nullptr && blk + 1 < nb;  // block b + 1 enters through G_b after its flag
     const int nanc = (m - nc + kKC - 1) / kKC;
-    const int npiv = (nb - 1 - blk) * (kMB / kKC);
+    const int npiv = (nb - 1 - blk - (chain ? 1 : 0)) * (kMB / kKC);
     const int nch = nanc + npiv;
     auto chunk = [&](int ch, int &rb, int &rw) {
       if (ch < nanc) {
@@ -763,6 +821,60 @@ __global__ void __launch_bounds__(kMultiThreads, kMultiCtas) k_bwd_multi(const i
       if (k0 < w) mma_k16<false>(Xs, kLdX, Rs, k0, mw, lane, c);
     }
     halves_sum(c, As, warp, lane);
+    if (chain) {
+      // W stays in Rs; G_b^T arrives in Xs while the task waits for block b + 1
+      const int rn = (blk + 1) * kMB, wn = min(kMB, nc - rn);
+      if (warp < 4) {
+#pragma unroll
+        for (int nb2 = 0; nb2 < 2; nb2++)
+#pragma unroll
+          for (int v = 0; v < 4; v++) {
+            const int cc = acc_row(warp, lane, v), n = acc_vec(lane, nb2, v);
+            Rs[cc * kLdB + n] = c[nb2][v];
+          }
+      }
+#pragma unroll
+      for (int nb2 = 0; nb2 < 2; nb2++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) c[nb2][v] = 0.0;
+      __syncthreads();  // every warp is done with X^T in Xs
+      {  // G_b^T ([m][k]): Xs[i][r] = G(r, i) = G[i 64 + r], G (wn x w, column-major)
+        const TL *G = Gch + (int64_t)(P.blkOff[s] - s + blk) * kMB * kMB;
+        for (int e = tid; e < kMB * kMB; e += kMultiThreads) {
+          const int r = e & (kMB - 1), i = e >> 6;
+          const bool ok = i < w && r < wn;
+          cp_async_el(Xs + i * kLdX + r, ok ? G + (int64_t)i * kMB + r : G, (int)sizeof(TL), ok);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+      }
+      if (tid == 0) waitOk = wait_flag(myflags + blk + 1, epoch, status, s, P.spin);
+      __syncthreads();
+      if (!waitOk) return bail();
+      for (int e = tid; e < kMB * kQS; e += kMultiThreads) {
+        const int r = e >> 4, n = e & (kQS - 1);
+        Bs[r * kLdB + n] = (r < wn && n < qs) ? __ldcg(y + (int64_t)(f + rn + r) * q + vb + n) : 0.0;
+      }
+      cp_async_all();
+      __syncthreads();
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int k0 = 32 * h + 16 * kh;
+        if (k0 < wn) mma_k16<false>(Xs, kLdX, Bs, k0, mw, lane, c);
+      }
+      halves_sum(c, As, warp, lane);
+      if (warp < 4) {
+#pragma unroll
+        for (int nb2 = 0; nb2 < 2; nb2++)
+#pragma unroll
+          for (int v = 0; v < 4; v++) {
+            const int cc = acc_row(warp, lane, v), n = acc_vec(lane, nb2, v);
+            if (cc < w && n < qs) y[(int64_t)(f + c0 + cc) * q + vb + n] = Rs[cc * kLdB + n] - c[nb2][v];
+          }
+      }
+      __syncthreads();
+      if (tid == 0) st_release(myflags + blk, epoch);
+      return true;
+    }
     if (warp < 4) {
 #pragma unroll
       for (int nb2 = 0; nb2 < 2; nb2++)
@@ -940,22 +1052,22 @@ static int multi_grid(int64_t ntasks) {
 
 template <class TL>
 void launch_fwd_multi(const int4 *tasks, int ntasks, bool wide, int *ticket, const DevPlan &P, const TL *Lx,
-                      const TL *Inv, double *y, double *T, int *flags, int nflags, int epoch, int *done,
+                      const TL *Inv, const TL *Mch, double *y, double *T, int *flags, int nflags, int epoch, int *done,
                       int q, unsigned long long *status, cudaStream_t st) {
   const int ns = multi_slices(q);
   if (ntasks <= 0) return;
   auto k = wide ? k_fwd_multi<TL, true> : k_fwd_multi<TL, false>;
-  k<<<multi_grid(ntasks), kMultiThreads, multi_smem<TL>(), st>>>(tasks, ntasks, ns, ticket, P, Lx, Inv, y, T,
+  k<<<multi_grid(ntasks), kMultiThreads, multi_smem<TL>(), st>>>(tasks, ntasks, ns, ticket, P, Lx, Inv, Mch, y, T,
                                                                   flags, nflags, epoch, done, q, status);
 }
 template <class TL>
 void launch_bwd_multi(const int4 *tasks, int ntasks, bool wide, int *ticket, const DevPlan &P, const TL *Lx,
-                      const TL *Inv, const double *Dpiv, double *y, int *flags, int nflags, int epoch, int q,
-                      unsigned long long *status, cudaStream_t st) {
+                      const TL *Inv, const TL *Gch, const double *Dpiv, double *y, int *flags, int nflags, int epoch,
+                      int q, unsigned long long *status, cudaStream_t st) {
   const int ns = multi_slices(q);
   if (ntasks <= 0) return;
   auto k = wide ? k_bwd_multi<TL, true> : k_bwd_multi<TL, false>;
-  k<<<multi_grid(ntasks), kMultiThreads, multi_smem<TL>(), st>>>(tasks, ntasks, ns, ticket, P, Lx, Inv, Dpiv, y,
+  k<<<multi_grid(ntasks), kMultiThreads, multi_smem<TL>(), st>>>(tasks, ntasks, ns, ticket, P, Lx, Inv, Gch, Dpiv, y,
                                                                   flags, nflags, epoch, q, status);
 }
 void launch_to_interleaved(const double *B, double *Yil, int n, int q, cudaStream_t st) {
@@ -976,16 +1088,16 @@ void launch_residual_multi(int n, const int *rowptr, const int *colidx, const do
   k_residual_multi<<<grid, 256, 0, st>>>(n, rowptr, colidx, val, x, b, r, norms, q, rowGroup);
 }
 template void launch_fwd_multi<double>(const int4 *, int, bool, int *, const DevPlan &, const double *,
-                                       const double *, double *, double *, int *, int, int, int *, int,
+                                       const double *, const double *, double *, double *, int *, int, int, int *, int,
                                        unsigned long long *, cudaStream_t);
 template void launch_fwd_multi<float>(const int4 *, int, bool, int *, const DevPlan &, const float *, const float *,
-                                      double *, double *, int *, int, int, int *, int, unsigned long long *,
-                                      cudaStream_t);
+                                      const float *, double *, double *, int *, int, int, int *, int,
+                                      unsigned long long *, cudaStream_t);
 template void launch_bwd_multi<double>(const int4 *, int, bool, int *, const DevPlan &, const double *,
-                                       const double *, const double *, double *, int *, int, int, int,
+                                       const double *, const double *, const double *, double *, int *, int, int, int,
                                        unsigned long long *, cudaStream_t);
 template void launch_bwd_multi<float>(const int4 *, int, bool, int *, const DevPlan &, const float *, const float *,
-                                      const double *, double *, int *, int, int, int, unsigned long long *,
-                                      cudaStream_t);
+                                      const float *, const double *, double *, int *, int, int, int,
+                                      unsigned long long *, cudaStream_t);
 
 }  // namespace amp
