@@ -478,12 +478,12 @@ void enqueue_factor(amp_factor *f) {
         if (sr.mixMid > sr.mix0)
           timed(f, K_UPDATE, sr.updateFlopsA, 0.0, [&] {
             amp::launch_update_mx(f->plan->dMixTile + sr.mix0, sr.mixMid - sr.mix0, f->dMaps, f->dL32, f->dU32,
-                                  f->dStatus, amp::num_sms(), st, false, f->waitSpins);
+                                  f->dStatus, amp::num_sms(), st, sr.mixWidthA, f->waitSpins);
           });
         if (sr.mix1 > sr.mixMid)
           la.part_b(K_UPDATE, sr.updateFlopsB, [&] {
             amp::launch_update_mx(f->plan->dMixTile + sr.mixMid, sr.mix1 - sr.mixMid, f->dMaps, f->dL32, f->dU32,
-                                  f->dStatus, amp::num_sms(), f->side, false, f->waitSpins);
+                                  f->dStatus, amp::num_sms(), f->side, 256, f->waitSpins);
           });
       }
       la.join();
@@ -491,7 +491,7 @@ void enqueue_factor(amp_factor *f) {
       if (u1 > u0)
         timed(f, K_UPDATE, P.uLvlFlops[L], 0.0, [&] {
           amp::launch_update_mx(f->plan->dMixU + u0, u1 - u0, f->dMaps, f->dL32, f->dU32, f->dStatus,
-                                amp::num_sms(), st, false, f->waitSpins);
+                                amp::num_sms(), st, 256, f->waitSpins);
         });
     }
     if (P.nflags)

@@ -32,11 +32,10 @@ template <class T>
 int launch_fronts_small(const int *tiny, int ntiny, int ntinyMid, const int *small, int nsmall, int maxM,
                         const DevPlan &P, const double *values, T *Lx, T *U, unsigned long long *status,
                         const LdltArgs<T> &la, cudaStream_t st);
-// narrow: 128 x 64 tiles (tasks whose columns are one 64-column pivot block), else 128 x 256
+// width: the tiles' columns, 256, or 128 / 64 (tasks whose columns are one 128- / 64-column group)
 // spin: bound of each role's wait in polls (0 = the default, about 0.5 s)
 void launch_update_mx(const MixTask *tasks, int64_t ntasks, const CUtensorMap *maps, float *L32, float *U32,
-                      unsigned long long *status, int num_sms, cudaStream_t st, bool narrow = false,
-                      long long spin = 0);
+                      unsigned long long *status, int num_sms, cudaStream_t st, int width = 256, long long spin = 0);
 int num_sms();
 void launch_update(const TileTask *tasks, int64_t ntasks, const DevPlan &P, double *Lx, double *U, const double *W,
                    const unsigned long long *status, cudaStream_t st);

@@ -1,5 +1,5 @@
 // Mixed-precision trailing / update-block tiles on the 5th-generation tensor cores (tcgen05, sm_100a), 128 x 256, or
-// 128 x 64 for the look-ahead's next pivot block (one 64-column block wide).
+// 128 x 128 / 128 x 64 for the look-ahead's next group when it is two pivot blocks (one block) wide.
 //
 // C[i0:i0+128, j0:j0+256] -= A B^T in FP32, where A and B are rows of the factored pivot columns of a front (for
 // LDL^T, A holds those rows times the pivots, L21 D) and the product runs as BF16x3: every FP32 value x is carried
@@ -72,7 +72,7 @@ __device__ __forceinline__ bool mx_wait(uint64_t *bar, uint32_t parity, MxShared
   return false;
 }
 
-// N: tile columns, 256 (the general tiles) or 64 (the next pivot block of the look-ahead, which is 64 columns wide)
+// N: tile columns, 256 (the general tiles), or 128 / 64 (the next group of the look-ahead when it is that wide)
 template <int N>
 __global__ void __launch_bounds__(kThreads, 1) k_update_mx(const MixTask *__restrict__ tasks, int ntasks,
                                                            const CUtensorMap *__restrict__ maps,
@@ -234,17 +234,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_update_mx(const MixTask *__rest
 cudaError_t init_mixed_attributes() {
   cudaError_t e = cudaFuncSetAttribute(k_update_mx<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, mixed_smem<256>());
   if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_update_mx<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, mixed_smem<128>());
+  if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_update_mx<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, mixed_smem<64>());
   return e;
 }
 
 void launch_update_mx(const MixTask *tasks, int64_t ntasks, const CUtensorMap *maps, float *L32, float *U32,
-                      unsigned long long *status, int num_sms, cudaStream_t st, bool narrow, long long spin) {
+                      unsigned long long *status, int num_sms, cudaStream_t st, int width, long long spin) {
   if (ntasks <= 0) return;
   const int grid = (int)(ntasks < num_sms ? ntasks : num_sms);
   if (spin <= 0) spin = kMxSpin;
-  if (narrow)
+  if (width == 64)
     k_update_mx<64><<<grid, kThreads, mixed_smem<64>(), st>>>(tasks, (int)ntasks, maps, L32, U32, status, spin);
+  else if (width == 128)
+    k_update_mx<128><<<grid, kThreads, mixed_smem<128>(), st>>>(tasks, (int)ntasks, maps, L32, U32, status, spin);
   else
     k_update_mx<256><<<grid, kThreads, mixed_smem<256>(), st>>>(tasks, (int)ntasks, maps, L32, U32, status, spin);
 }

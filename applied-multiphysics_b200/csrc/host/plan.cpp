@@ -200,9 +200,9 @@ void build_plan(const Symbolic &S, Plan &P, const Tuning &tune) {
   for (int s = 0; s < ns; s++) P.snSp[s + 1] = P.snSp[s] + (int64_t)((P.snM[s] + 7) & ~7) * P.snNc[s];
   P.splitElems = P.snSp[ns];
   // mixed-precision tiles (128 x 256, starts aligned down to 8, masked by ilo / jlo / jend) of a region
-  auto emitMix = [&](std::vector<MixTask> &out, int s, int rlo, int clo, int chi, int kc0, int kw) {
+  auto emitMix = [&](std::vector<MixTask> &out, int s, int rlo, int clo, int chi, int kc0, int kw, int width = 256) {
     const int m = P.snM[s], nc = P.snNc[s];
-    for (int j0 = clo & ~7; j0 < chi; j0 += 256)
+    for (int j0 = clo & ~7; j0 < chi; j0 += width)
       for (int i0 = std::max(rlo, j0) & ~7; i0 < m; i0 += 128)
         out.push_back({(long long)P.snLxp[s], (long long)P.snUoff[s], (long long)P.snSp[s], m, nc, (m + 7) & ~7, kc0,
                        kw, i0, j0, rlo, clo, chi, s});
@@ -308,23 +308,26 @@ void build_plan(const Symbolic &S, Plan &P, const Tuning &tune) {
       }
       sr.item1 = i1;
       sr.strip1 = (int64_t)P.strips.size();
-      auto emit = [&](const Region &g, int lo, int hi, double &flops) {
+      // part A (the next group's columns, which start on a group boundary) runs tiles as wide as the group when
+      // it is 64 or 128 columns: no masked part of a 128 x 256 tile
+      sr.mixWidthA = GW <= 128 ? GW : 256;
+      auto emit = [&](const Region &g, int lo, int hi, double &flops, int width) {
         if (lo >= hi) return;
         const int m = P.snM[g.s], nc = P.snNc[g.s];
         flops += 2.0 * g.kw * trap(m, lo, hi);
-        emitMix(P.mixTiles, g.s, lo, lo, hi, g.kc0, g.kw);
+        emitMix(P.mixTiles, g.s, lo, lo, hi, g.kc0, g.kw, width);
         for (int j0 = lo; j0 < hi; j0 += kTile)
           for (int i0 = lo + ((j0 - lo) / kTileM) * kTileM; i0 < m; i0 += kTileM)
             P.tileTasks.push_back({(long long)P.snLxp[g.s], (long long)P.snUoff[g.s], m, nc, g.kc0, g.kw, i0, j0, hi, 0});
       };
       sr.tile0 = (int64_t)P.tileTasks.size();
       sr.mix0 = (int64_t)P.mixTiles.size();
-      for (const Region &g : regions) emit(g, g.lo, std::min(g.lo + GW, g.hi), sr.updateFlopsA);
+      for (const Region &g : regions) emit(g, g.lo, std::min(g.lo + GW, g.hi), sr.updateFlopsA, sr.mixWidthA);
       sr.tileMid = (int64_t)P.tileTasks.size();
       sr.mixMid = (int64_t)P.mixTiles.size();
       if (doB)
         for (const Region &g : regions) {
-          emit(g, g.lo + GW, g.hi, sr.updateFlopsB);
+          emit(g, g.lo + GW, g.hi, sr.updateFlopsB, 256);
           appliedB[g.s] = g.lo;  // every column right of the next group now has the groups before g.lo
         }
       sr.tile1 = (int64_t)P.tileTasks.size();

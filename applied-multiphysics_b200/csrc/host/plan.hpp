@@ -64,6 +64,7 @@ struct StepRange {
   int ticket;                            // the launch's ticket counter (index into the group tickets)
   int64_t tile0, tileMid, tile1;  // FP64 update tiles: part A [tile0, tileMid), part B [tileMid, tile1)
   int64_t mix0, mixMid, mix1;     // the same for the mixed-precision tiles
+  int mixWidthA;                  // columns of part A's mixed tiles: the group width when it is 64 or 128, else 256
   double panelFlops, updateFlopsA, updateFlopsB;  // algorithmic flops of the step's launches
 };
 // The update block of every front receives its whole Schur update once, after the group steps of its level:

@@ -312,6 +312,9 @@ def run_reference(args, rank):
 # update launch (764.6 GFLOP over 183 launches)
 TRAFFIC = {
     ("elastic3d", 40, "mixed", "update_syrk"): 169.3e6 / 26.2e9 * 764.6e9 / 183,
+    # the group panel: its longest elastic3d-32 launch moves 22.9 MB for 0.602 GFLOP, scaled by the flops of an average
+    # cfg2 group-panel launch (26.8 GFLOP over 157 launches)
+    ("elastic3d", 40, "mixed", "group_panel"): 22.9e6 / 0.602e9 * 26.8e9 / 157,
 }
 
 
