@@ -436,13 +436,7 @@ void enqueue_chain_mats(amp_factor *f, const T *Lx, const T *Inv, T *Mch, T *Gch
   });
 }
 
-void enqueue_bkfactor(amp_factor *f);
-
 void enqueue_factor(amp_factor *f) {
-  if (f->bk) {
-    enqueue_bkfactor(f);
-    return;
-  }
   const amp::Plan &P = f->plan->P;
   amp::DevPlan dp = f->plan->dp;
   if (f->waitSpins > 0) dp.spin = f->waitSpins;
@@ -503,8 +497,13 @@ void enqueue_factor(amp_factor *f) {
     return;
   }
   const bool ldlt = f->kind == AMP_LDLT;
-  const amp::LdltArgs<double> ld = ldlt ? amp::LdltArgs<double>{f->dScal, f->dCounts, f->dW, f->dD, nullptr, nullptr}
-                                        : amp::LdltArgs<double>{};
+  amp::LdltArgs<double> ld = ldlt ? amp::LdltArgs<double>{f->dScal, f->dCounts, f->dW, f->dD, nullptr, nullptr}
+                                  : amp::LdltArgs<double>{};
+  if (f->bk) {  // Bunch-Kaufman pivots inside each pivot block: the small-front and group-panel kernels' BK variants
+    ld.piv = f->dPiv;
+    ld.Doff = f->dDoff;
+    dp.lpiv = f->dPiv;  // the inverse blocks with each block's pivot order folded in
+  }
   if (ldlt) {
     ck(cudaMemsetAsync(f->dCounts, 0, 2 * sizeof(int), st), "memset counts");
     amp::launch_ldlt_tau(f->dValues, dp, f->dScal, st);
@@ -955,57 +954,6 @@ void enqueue_cfactor(amp_factor *f) {
   }
 }
 
-// The FP64 LDL^T with Bunch-Kaufman pivots inside each pivot block: every front through the dense schedule (the
-// complex factor's: assembly, group steps with the Bunch-Kaufman pivot blocks, FP64 update tiles with A = L21 D), then
-// the inverses of the diagonal blocks with each block's pivot order folded in.
-void enqueue_bkfactor(amp_factor *f) {
-  const amp::Plan &P = f->plan->P;
-  const amp::DenseSched &D = f->plan->cx;
-  amp::DevPlan dp = f->plan->dp;
-  if (f->waitSpins > 0) dp.spin = f->waitSpins;
-  cudaStream_t st = f->stream;
-  ck(cudaMemsetAsync(f->dStatus, 0xff, sizeof(unsigned long long), st), "memset status");
-  ck(cudaMemsetAsync(f->dCounts, 0, 2 * sizeof(int), st), "memset counts");
-  if (D.nGroupFlags + D.nGroupTickets > 0)
-    ck(cudaMemsetAsync(f->dCxFlags, 0, sizeof(int) * (D.nGroupFlags + D.nGroupTickets), st), "memset flags");
-  int *tickets = f->dCxFlags + D.nGroupFlags;
-  amp::launch_ldlt_tau(f->dValues, dp, f->dScal, st);
-  amp::LdltArgs<double> ld{f->dScal, f->dCounts, f->dW, f->dD, nullptr, nullptr};
-  ld.piv = f->dPiv;
-  ld.Doff = f->dDoff;
-  for (int L = 0; L < P.nlevels; L++) {
-    if (D.asmLvlPtr[L + 1] > D.asmLvlPtr[L])
-      timed(f, K_ASSEMBLE, 0.0, 0.0, [&] {
-        amp::launch_assemble<double>(f->plan->dCxAsm + D.asmLvlPtr[L], f->plan->dCxAsmCh, D.asmLvlPtr[L + 1] - D.asmLvlPtr[L], dp,
-                                     f->dValues, f->dLx, f->dU, f->dStatus, st);
-      });
-    for (int k = D.lvlStepPtr[L]; k < D.lvlStepPtr[L + 1]; k++) {
-      const amp::StepRange &sr = D.steps[k];
-      timed(f, K_PANEL, sr.panelFlops, 0.0, [&] {
-        amp::launch_group_panel<double>(f->plan->dCxItems, f->plan->dCxStrips + sr.strip0,
-                                        (int)(sr.strip1 - sr.strip0), tickets + sr.ticket, f->dCxFlags, dp, f->dLx,
-                                        f->dStatus, nullptr, nullptr, ld, st);
-      });
-      if (sr.tile1 > sr.tile0)
-        timed(f, K_UPDATE, sr.updateFlopsA + sr.updateFlopsB, 0.0, [&] {
-          amp::launch_update(f->plan->dCxTiles + sr.tile0, sr.tile1 - sr.tile0, dp, f->dLx, f->dU, f->dW, f->dStatus,
-                             st);
-        });
-    }
-    if (D.uLvlPtr[L + 1] > D.uLvlPtr[L])
-      timed(f, K_UPDATE, 0.0, 0.0, [&] {
-        amp::launch_update(f->plan->dCxU + D.uLvlPtr[L], D.uLvlPtr[L + 1] - D.uLvlPtr[L], dp, f->dLx, f->dU, f->dW,
-                           f->dStatus, st);
-      });
-  }
-  dp.lpiv = f->dPiv;  // the inverse blocks with the pivot order folded in
-  if (P.nflags)
-    timed(f, K_DIAGINV, 0.0, 16.0 * (double)inv_elems(P),
-          [&] {
-            amp::launch_diag_inv<double>(f->plan->dInvBlocks, (int)P.invBlocks.size(), dp, f->dLx, f->dInv, st);
-          });
-}
-
 // y (permuted order) := A^-1 y
 void csolve_permuted(amp_factor *f, amp::cplx *y) {
   const amp::Plan &P = f->plan->P;
@@ -1321,11 +1269,9 @@ int amp_factor_create(amp_plan *pl, const amp_factor_opts *opts, amp_factor **ou
           f->dScal = f->mem.alloc<double>(2);
           f->dCounts = f->mem.alloc<int>(2);
         }
-        if (f->bk) {  // every front through the dense schedule (built and uploaded once per plan)
-          upload_cx(pl);
+        if (f->bk) {
           f->dDoff = f->mem.alloc<double>((size_t)std::max(1, P.n));
           f->dPiv = f->mem.alloc<int>((size_t)std::max(1, P.n));
-          f->dCxFlags = f->mem.alloc<int>((size_t)std::max(1, pl->cx.nGroupFlags + pl->cx.nGroupTickets));
         }
       } else {
         f->dL32 = f->mem.alloc<float>((size_t)P.nnzLStored);

@@ -417,14 +417,13 @@ def main():
         if prec == "fp64-bk":
             kind = amp.LDLT_BK
         psym = sym
-        # the schedule per precision, chosen by timing candidates (per pattern, not timed); the Bunch-Kaufman factor
-        # has one schedule (every front dense)
-        if args.schedule and prec != "fp64-bk":
+        # the schedule per precision, chosen by timing candidates (per pattern, not timed)
+        if args.schedule:
             if isinstance(w, _Batch):
                 psym = amp.analyze(w.pat, perm=w.perm, device=local, **schedule_kw(args))
             else:
                 psym = amp.analyze(w.pat, ordering="nd3", x=w.x, y=w.y, z=w.z, device=local, **schedule_kw(args))
-        elif not args.no_autotune and prec != "fp64-bk":
+        elif not args.no_autotune:
             if isinstance(w, _Batch):
                 psym = amp.analyze(w.pat, perm=w.perm, device=local)
             else:
