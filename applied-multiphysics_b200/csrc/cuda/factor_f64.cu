@@ -233,9 +233,12 @@ __device__ __forceinline__ cplx fast_recip(cplx d) { return cplx(1.0) / d; }
 // scaled: Cholesky L = a / sqrt(d) with sqrt(d) on the diagonal, LDL^T L = a / d with a unit diagonal (D to ld.D).
 // Returns false (status set for the first failing column f + c0 + k) when a pivot failed; the block is then not
 // written back.
-template <class T, class TC>
+// LB (the Bunch-Kaufman fast path): also returns 2, writing nothing, when a multiplier |L(i, k)| of the block exceeds
+// lbound or a pivot was perturbed.
+template <class T, class TC, bool LB = false>
 __device__ int potrf_core(const T *src, int lds, T *Lp, int m, int w, int f, int c0, int s,
-                          unsigned long long *status, const LdltArgs<T> &ld, double promoteBelow) {
+                          unsigned long long *status, const LdltArgs<T> &ld, double promoteBelow,
+                          double lbound = -1.0) {
   __shared__ TC col[2][4][kPanel];  // per 4-column block (double-buffered): the block's unscaled columns, by row
   __shared__ TC pd[kPanel], piv[2][4];
   __shared__ unsigned char pflag[kPanel];
@@ -323,6 +326,20 @@ __device__ int potrf_core(const T *src, int lds, T *Lp, int m, int w, int f, int
   }
   if (myFail >= 0) atomicMin(&fail, myFail);
   if (promoteBelow > 0.0 && tid < w && !(pivot_mag(pd[tid]) >= promoteBelow)) promote = 1;
+  if constexpr (LB && !is_cplx<TC>::value) {
+    {  // every multiplier within the bound and no pivot perturbed, else redo with pivoting
+      if (tid < w && (pflag[tid] & 2)) promote = 1;
+      if (owner) {
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+          for (int c = 0; c < 4; c++) {
+            const int i = 4 * ti + r, j = 4 * tj + c;
+            if (i > j && i < w && !(fabs((double)a[r][c]) <= lbound * fabs((double)pd[j]))) promote = 1;
+          }
+      }
+    }
+  }
   __syncthreads();
   if (promote) return 2;  // the caller redoes the block in higher precision (nothing written)
   if (fail < kPanel) {
@@ -841,10 +858,20 @@ __global__ void __launch_bounds__(256, group_min_blocks<T>()) k_group_panel(cons
   if (jd >= 0) {  // this strip's own pivot block, fully updated: factor it and publish it (also after a failure)
     const int c0 = g0 + jd * kPanel, w = min(kPanel, g1 - c0);
     __syncthreads();  // Ds complete (also when the strip had no earlier pivot block)
-    if constexpr (BK && !is_cplx<T>::value)  // FP64 workspace in M (and Ws for FP32 fronts), both free here
-      bk_block<T>(&Ds[0][0], kPanel + 1, reinterpret_cast<double(*)[kPanel + 1]>(gp_raw), L + (int64_t)c0 * m + c0, m,
-                  w, f, c0, s, status, ld);
-    else
+    if constexpr (BK && !is_cplx<T>::value) {
+      // Bunch-Kaufman keeps every pivot of the block in place exactly when each multiplier is at most 1 / alpha in
+      // magnitude and no pivot needs the perturbation: try the unpivoted LDL^T first (it writes nothing unless it
+      // passes that test), else redo the block with pivots from the untouched entries
+      const int r = potrf_core<T, T, true>(&Ds[0][0], kPanel + 1, L + (int64_t)c0 * m + c0, m, w, f, c0, s, status, ld,
+                                           -1.0, 1.0 / 0.64038820320220756);
+      if (r == 2) {  // FP64 workspace in M (and Ws for FP32 fronts), both free here
+        bk_block<T>(&Ds[0][0], kPanel + 1, reinterpret_cast<double(*)[kPanel + 1]>(gp_raw),
+                    L + (int64_t)c0 * m + c0, m, w, f, c0, s, status, ld);
+      } else if (r == 0 && threadIdx.x < w) {  // the identity pivot order, 1 x 1 pivots
+        ld.piv[f + c0 + threadIdx.x] = threadIdx.x;
+        ld.Doff[f + c0 + threadIdx.x] = 0.0;
+      }
+    } else
       potrf_block<T>(&Ds[0][0], kPanel + 1, L + (int64_t)c0 * m + c0, m, w, f, c0, s, status, ld);
     panel_release(Pf + jd, 1);
   }
