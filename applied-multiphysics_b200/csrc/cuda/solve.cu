@@ -35,15 +35,24 @@ constexpr int kSB = 64;  // solve block rows
 
 // ---- inverses of the diagonal blocks -----------------------------------------------------------------------------
 // One CTA per 64-column block b of the pivot columns (all supernodes): X = L_kk^-1, w x w column-major, lower part.
-// Thread j computes column j; L is read through the read-only cache. For a Bunch-Kaufman factor the stored block is
+// The block's lower triangle is staged in shared memory (coalesced column loads), then thread j computes column j.
+// Shared layouts keep a thread's column walk free of bank conflicts: Ls[t][i] = L(i, t) with 65 entries per column
+// (thread j reads Ls[j + k][i]), Xs[t][j] = X(t, j) with 64 (thread j reads Xs[j + k][j]: an odd stride of 65
+// doubles). For a Bunch-Kaufman factor the stored block is
 // X P_b (P_b the block's pivot order, a full w x w matrix): the forward sweep's r, taken in the original order of the
 // block's rows, becomes y_b = X P_b r, and the backward sweep's x_b = (X P_b)^T r lands in that original order, so
 // L's earlier columns keep the rows of later blocks in their original order (the interchanges are not applied to
 // the left of a block) and the sweeps need no other change.
 template <class TL>
+constexpr int diag_inv_smem() {
+  return kSB * kSB * (int)sizeof(double) + kSB * (kSB + 1) * (int)sizeof(TL);
+}
+template <class TL>
 __global__ void __launch_bounds__(kSB) k_diag_inv(const int *__restrict__ blocks, DevPlan P, const TL *__restrict__ Lx,
                                                   TL *__restrict__ Inv) {
-  __shared__ double Xs[kSB][kSB + 1];
+  extern __shared__ double inv_dyn[];
+  double(*Xs)[kSB] = reinterpret_cast<double(*)[kSB]>(inv_dyn);
+  TL(*Ls)[kSB + 1] = reinterpret_cast<TL(*)[kSB + 1]>(inv_dyn + kSB * kSB);
   __shared__ double dinv[kSB];
   const int b = blocks[blockIdx.x];
   int lo = 0, hi = P.nsuper;  // supernode s with blkOff[s] <= b < blkOff[s + 1]
@@ -55,13 +64,17 @@ __global__ void __launch_bounds__(kSB) k_diag_inv(const int *__restrict__ blocks
   const int m = P.snM[s], w = min(kSB, P.snNc[s] - c0);
   const TL *Lb = Lx + P.snLxp[s] + (int64_t)c0 * m + c0;  // L_kk(i, t) = Lb[t m + i]
   const int j = threadIdx.x;
-  if (j < w) dinv[j] = 1.0 / (double)__ldg(Lb + (int64_t)j * m + j);
+#pragma unroll 8
+  for (int t = 0; t < w; t++)
+    if (j >= t && j < w) Ls[t][j] = __ldg(Lb + (int64_t)t * m + j);
+  __syncthreads();
+  if (j < w) dinv[j] = 1.0 / (double)Ls[j][j];
   __syncthreads();
   if (j < w) {
     Xs[j][j] = dinv[j];
     for (int i = j + 1; i < w; i++) {
       double acc = 0.0;
-      for (int t = j; t < i; t++) acc += (double)__ldg(Lb + (int64_t)t * m + i) * Xs[t][j];
+      for (int t = j; t < i; t++) acc += (double)Ls[t][i] * Xs[t][j];
       Xs[i][j] = -acc * dinv[i];
     }
   }
@@ -117,12 +130,16 @@ __global__ void __launch_bounds__(256) k_chain_mats(const int2 *__restrict__ tas
     }
     __syncthreads();
     TL *M = Mch + (int64_t)(slotBase + b - 1) * kSB * kSB;
-    for (int u = 0; u < 16; u++) {
-      const int c = cg * 16 + u;
-      double a = 0.0;
-      for (int j = 0; j <= i && j < w; j++) a += Xs[i][j] * Lt[j][c];
-      M[c * kSB + i] = (TL)a;
+    double a[16];  // M(i, cg 16 + u); each X(i, j) read once for the 16 columns (Lt[j][.] broadcast in the warp)
+#pragma unroll
+    for (int u = 0; u < 16; u++) a[u] = 0.0;
+    for (int j = 0; j <= i && j < w; j++) {
+      const double x = Xs[i][j];
+#pragma unroll
+      for (int u = 0; u < 16; u++) a[u] += x * Lt[j][cg * 16 + u];
     }
+#pragma unroll
+    for (int u = 0; u < 16; u++) M[(cg * 16 + u) * kSB + i] = (TL)a[u];
     __syncthreads();
   }
   if (b + 1 < nb) {  // G(r, c) = sum_{j >= c} L(c0 + 64 + r, c0 + j) X(j, c)
@@ -133,12 +150,17 @@ __global__ void __launch_bounds__(256) k_chain_mats(const int2 *__restrict__ tas
     }
     __syncthreads();
     TL *G = Gch + (int64_t)(slotBase + b) * kSB * kSB;
-    for (int u = 0; u < 16; u++) {
-      const int c = cg * 16 + u;
-      double a = 0.0;
-      for (int j = c; j < w; j++) a += Lt[i][j] * Xs[j][c];
-      G[c * kSB + i] = (TL)a;
+    double a[16];  // G(i, cg 16 + u) = sum over j >= c of L(i, j) X(j, c); each L(i, j) read once
+#pragma unroll
+    for (int u = 0; u < 16; u++) a[u] = 0.0;
+    for (int j = cg * 16; j < w; j++) {
+      const double l = Lt[i][j];
+#pragma unroll
+      for (int u = 0; u < 16; u++)
+        if (j >= cg * 16 + u) a[u] += l * Xs[j][cg * 16 + u];
     }
+#pragma unroll
+    for (int u = 0; u < 16; u++) G[(cg * 16 + u) * kSB + i] = (TL)a[u];
   }
 }
 
@@ -658,6 +680,10 @@ cudaError_t init_solve_attributes() {
     e = cudaFuncSetAttribute(k_chain_mats<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kChainSmem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_chain_mats<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kChainSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_diag_inv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, diag_inv_smem<double>());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_diag_inv<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, diag_inv_smem<float>());
   return e;
 }
 
@@ -667,7 +693,7 @@ static int solve_grid(int ntasks) { return ntasks < 3 * num_sms() ? ntasks : 3 *
 
 template <class TL>
 void launch_diag_inv(const int *blocks, int nblocks, const DevPlan &P, const TL *Lx, TL *Inv, cudaStream_t st) {
-  if (nblocks > 0) k_diag_inv<TL><<<nblocks, kSB, 0, st>>>(blocks, P, Lx, Inv);
+  if (nblocks > 0) k_diag_inv<TL><<<nblocks, kSB, diag_inv_smem<TL>(), st>>>(blocks, P, Lx, Inv);
 }
 template <class TL>
 void launch_chain_mats(const int2 *tasks, int ntasks, const DevPlan &P, const TL *Lx, const TL *Inv, TL *Mch, TL *Gch,
