@@ -35,25 +35,29 @@ constexpr int kSB = 64;  // solve block rows
 
 // ---- inverses of the diagonal blocks -----------------------------------------------------------------------------
 // One CTA per 64-column block b of the pivot columns (all supernodes): X = L_kk^-1, w x w column-major, lower part.
-// The block's lower triangle is staged in shared memory (coalesced column loads), then thread j computes column j.
-// Shared layouts keep a thread's column walk free of bank conflicts: Ls[t][i] = L(i, t) with 65 entries per column
-// (thread j reads Ls[j + k][i]), Xs[t][j] = X(t, j) with 64 (thread j reads Xs[j + k][j]: an odd stride of 65
-// doubles). For a Bunch-Kaufman factor the stored block is
+// The block's lower triangle is staged in shared memory (coalesced column loads); then a group of 4 lanes computes
+// column j by forward substitution, X(j, j) = 1 / L(j, j), X(i, j) = -(sum_{t=j}^{i-1} L(i, t) X(t, j)) / L(i, i),
+// lane p summing the terms t = j + p, j + p + 4, ... (two shuffles complete the sum) and keeping the entries X(t, j)
+// of its own terms, so that the group needs no barrier between rows. Shared layouts: Ls[t][i] = L(i, t), 65 entries
+// per column; Xs[j][t] = X(t, j), one 64-entry row per column (a group's lanes read consecutive entries).
+// For a Bunch-Kaufman factor the stored block is
 // X P_b (P_b the block's pivot order, a full w x w matrix): the forward sweep's r, taken in the original order of the
 // block's rows, becomes y_b = X P_b r, and the backward sweep's x_b = (X P_b)^T r lands in that original order, so
 // L's earlier columns keep the rows of later blocks in their original order (the interchanges are not applied to
 // the left of a block) and the sweeps need no other change.
+constexpr int kInvThreads = 4 * kSB;
 template <class TL>
 constexpr int diag_inv_smem() {
   return kSB * kSB * (int)sizeof(double) + kSB * (kSB + 1) * (int)sizeof(TL);
 }
 template <class TL>
-__global__ void __launch_bounds__(kSB) k_diag_inv(const int *__restrict__ blocks, DevPlan P, const TL *__restrict__ Lx,
-                                                  TL *__restrict__ Inv) {
+__global__ void __launch_bounds__(kInvThreads) k_diag_inv(const int *__restrict__ blocks, DevPlan P,
+                                                          const TL *__restrict__ Lx, TL *__restrict__ Inv) {
   extern __shared__ double inv_dyn[];
   double(*Xs)[kSB] = reinterpret_cast<double(*)[kSB]>(inv_dyn);
   TL(*Ls)[kSB + 1] = reinterpret_cast<TL(*)[kSB + 1]>(inv_dyn + kSB * kSB);
   __shared__ double dinv[kSB];
+  __shared__ int kOf[kSB];
   const int b = blocks[blockIdx.x];
   int lo = 0, hi = P.nsuper;  // supernode s with blkOff[s] <= b < blkOff[s + 1]
   while (hi - lo > 1) {
@@ -63,36 +67,40 @@ __global__ void __launch_bounds__(kSB) k_diag_inv(const int *__restrict__ blocks
   const int s = lo, c0 = (b - P.blkOff[s]) * kSB;
   const int m = P.snM[s], w = min(kSB, P.snNc[s] - c0);
   const TL *Lb = Lx + P.snLxp[s] + (int64_t)c0 * m + c0;  // L_kk(i, t) = Lb[t m + i]
-  const int j = threadIdx.x;
-#pragma unroll 8
-  for (int t = 0; t < w; t++)
-    if (j >= t && j < w) Ls[t][j] = __ldg(Lb + (int64_t)t * m + j);
+  const int tid = threadIdx.x;
+  for (int e = tid; e < kSB * kSB; e += kInvThreads) {
+    const int t = e >> 6, i = e & (kSB - 1);
+    if (t < w && i >= t && i < w) Ls[t][i] = __ldg(Lb + (int64_t)t * m + i);
+  }
   __syncthreads();
-  if (j < w) dinv[j] = 1.0 / (double)Ls[j][j];
+  if (tid < w) dinv[tid] = 1.0 / (double)Ls[tid][tid];
   __syncthreads();
-  if (j < w) {
-    Xs[j][j] = dinv[j];
+  const int j = tid >> 2, p = tid & 3;
+  if (j < w) {  // the 4 lanes of a group share j, so they take the same branches and trip counts
+    const unsigned gmask = 0xfu << (threadIdx.x & 28);
+    if (p == 0) Xs[j][j] = dinv[j];
     for (int i = j + 1; i < w; i++) {
       double acc = 0.0;
-      for (int t = j; t < i; t++) acc += (double)Ls[t][i] * Xs[t][j];
-      Xs[i][j] = -acc * dinv[i];
+      for (int t = j + p; t < i; t += 4) acc += (double)Ls[t][i] * Xs[j][t];
+      acc += __shfl_xor_sync(gmask, acc, 1);
+      acc += __shfl_xor_sync(gmask, acc, 2);
+      if (((i - j) & 3) == p) Xs[j][i] = -acc * dinv[i];  // read later by this lane only
     }
   }
   __syncthreads();
   TL *X = Inv + P.invOff[b];
   if (P.lpiv) {  // Bunch-Kaufman factor: X P_b, column piv(k) of it = column k of X (P_b r = r(piv(.)))
-    __shared__ int kOf[kSB];
-    if (j < w) kOf[__ldg(P.lpiv + P.snF[s] + c0 + j)] = j;
+    if (tid < w) kOf[__ldg(P.lpiv + P.snF[s] + c0 + tid)] = tid;
     __syncthreads();
-    for (int e = threadIdx.x; e < w * w; e += kSB) {
+    for (int e = tid; e < w * w; e += kInvThreads) {
       const int i = e % w, k = kOf[e / w];
-      X[e] = (TL)(i >= k ? Xs[i][k] : 0.0);
+      X[e] = (TL)(i >= k ? Xs[k][i] : 0.0);
     }
     return;
   }
-  for (int e = threadIdx.x; e < w * w; e += kSB) {
+  for (int e = tid; e < w * w; e += kInvThreads) {
     const int i = e % w, jj = e / w;
-    X[e] = (TL)(i >= jj ? Xs[i][jj] : 0.0);
+    X[e] = (TL)(i >= jj ? Xs[jj][i] : 0.0);
   }
 }
 
@@ -693,7 +701,7 @@ static int solve_grid(int ntasks) { return ntasks < 3 * num_sms() ? ntasks : 3 *
 
 template <class TL>
 void launch_diag_inv(const int *blocks, int nblocks, const DevPlan &P, const TL *Lx, TL *Inv, cudaStream_t st) {
-  if (nblocks > 0) k_diag_inv<TL><<<nblocks, kSB, diag_inv_smem<TL>(), st>>>(blocks, P, Lx, Inv);
+  if (nblocks > 0) k_diag_inv<TL><<<nblocks, kInvThreads, diag_inv_smem<TL>(), st>>>(blocks, P, Lx, Inv);
 }
 template <class TL>
 void launch_chain_mats(const int2 *tasks, int ntasks, const DevPlan &P, const TL *Lx, const TL *Inv, TL *Mch, TL *Gch,
