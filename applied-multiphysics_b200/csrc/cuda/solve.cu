@@ -1,12 +1,12 @@
 // Supernodal triangular solves on sm_100a (sparse.mjs solveNumeric :1261-1305, supernodalSolve :1200-1258).
 //
 // Multifrontal vector form, each sweep one launch over 64-row block tasks:
-//   forward (tasks listed level by level, leaves first)
+//   forward (tasks listed children before parents, the longest estimated path to the sweep's end first)
 //     diagonal task (s, k)  block 0 first gathers v_s = [y(f .. f+nc); 0] + the children's pass-up vectors (extend-add
 //                           in the reference's child order); then r_k = v_k - L[k, 0:k] y(0:k) (row-block dot products)
 //                           and y_k = L_kk^-1 r_k as a 64 x 64 product with the precomputed inverse block
 //     below task (s, j)     the pass-up vector u_j = v_j - L[j, 0:nc] y (read by the parent's gather)
-//   backward (tasks listed level by level, root first; blocks of a supernode from the last down)
+//   backward (tasks listed parents before children, the same way; blocks of a supernode from the last down)
 //     x_k = L_kk^-T (y_k - L[rows below k, k]^T x(rows)), the rows below the supernode gathered from the ancestors'
 //     final values
 // Every L element is read once per sweep. Persistent CTAs (3 per SM) take the next task with an atomic ticket (so a
@@ -175,8 +175,8 @@ __global__ void __launch_bounds__(256) k_chain_mats(const int2 *__restrict__ tas
 // ---- forward block tasks -----------------------------------------------------------------------------------------
 constexpr int kChPre = 64;  // children located and waited for at once by a forward block task
 // task: .x supernode, .y block, .z kind (0 diagonal, 1 below, 2 small supernodes, 3 whole supernode: one-vector list)
-// One launch for the whole sweep: tasks are listed level by level (leaves first), so every wait is on a task with an
-// earlier ticket. Every task first waits for the supernode's children and gathers its own rows of the front vector
+// One launch for the whole sweep: a supernode's tasks are listed after its children's, so every wait is on a task
+// with an earlier ticket. Every task first waits for the supernode's children and gathers its own rows of the front vector
 // v_s = [y(f .. f + nc); 0] + the children's pass-up vectors (in the reference's child order). A below task forms its
 // part of the pass-up vector u_j = v_j - L[j, 0:nc] y and counts itself in done[s]; diagonal task b forms
 // w_b = X_b (v_b - L[b, 0:(b-1) 64] y) while the earlier blocks finish, then waits for block b - 1 alone:
@@ -512,7 +512,7 @@ __global__ void __launch_bounds__(256, 3) k_bwd_blocks(const int4 *__restrict__ 
 #pragma unroll
     for (int u = 0; u < 8; u++) acc[u] = 0.0;
     // Rows of the supernode below its pivot columns (ancestors' rows, ascending), from the last down in chunks of 32
-    // (lane = row; warps over the columns). One launch covers the whole sweep (levels top-down), and the parent's
+    // (lane = row; warps over the columns). One launch covers the whole sweep (parents listed first), and the parent's
     // pivot blocks become final from its last block down, each block's flag set only after the next one's (rows
     // above the parent's pivot columns are final before its last block is). So a chunk waits only for the parent's
     // block that holds its first row, and the chunks of rows in the parent's later blocks are summed while the

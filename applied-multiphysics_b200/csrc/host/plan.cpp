@@ -90,6 +90,189 @@ static void add_asm_task(const Plan &P, int s, int j0, std::vector<AsmTask> &tas
   }
 }
 
+// The one-vector forward task list in critical-path order: a topological order of its tasks (a supernode's tasks
+// after every task that completes a child's pass-up vector, its diagonal blocks in order, its blocks below after its
+// last diagonal block) that lists, among the tasks whose predecessors are already listed, the one with the longest
+// estimated path to the end of the sweep first (ties: the level order). The persistent CTAs take tasks in list
+// order, so the chains under the large separators start as soon as their inputs allow instead of level by level.
+// kinds(s): 0 one-warp supernode (in a group task), 1 whole-supernode task, 2 block tasks.
+static void order_forward_by_path(const Plan &P, const std::vector<int> &kinds, std::vector<int> &tasks) {
+  constexpr int B = 64;
+  constexpr double cDiag = 2.7, cBelow = 3.0, cWhole = 7.0, cSmall = 5.0;  // estimated task times (microseconds)
+  const int ns = (int)P.snNc.size(), nt = (int)(tasks.size() / 4);
+  auto span = [&](int s) {  // from s's children complete to s's pass-up vector complete
+    if (kinds[s] == 0) return cSmall;
+    if (kinds[s] == 1) return cWhole;
+    return ((P.snNc[s] + B - 1) / B) * cDiag + (P.snM[s] > P.snNc[s] ? cBelow : 0.0);
+  };
+  std::vector<double> tail(ns, 0.0);  // from s's pass-up vector complete to the end of the sweep
+  for (int L = P.nlevels - 1; L >= 0; L--)
+    for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
+      const int s = P.lvlSn[q], par = P.snParent[s];
+      tail[s] = par < 0 ? 0.0 : span(par) + tail[par];
+    }
+  // nodes: tasks [0, nt), "s complete" [nt, nt + ns), "s ready" (children complete) [nt + ns, nt + 2 ns)
+  const int nn = nt + 2 * ns;
+  std::vector<std::vector<int>> succ(nn);
+  std::vector<int> indeg(nn, 0);
+  std::vector<double> prio(nt, 0.0);
+  auto edge = [&](int a, int b) {
+    succ[a].push_back(b);
+    indeg[b]++;
+  };
+  std::vector<int> diagAt(P.nflags, -1), lastDiag(ns, -1);
+  for (int t = 0; t < nt; t++) {
+    const int x = tasks[4 * t], y = tasks[4 * t + 1], k = tasks[4 * t + 2];
+    if (k == 0) {
+      diagAt[P.blkOff[x] + y] = t;
+      if (y == P.blkOff[x + 1] - P.blkOff[x] - 1) lastDiag[x] = t;
+    }
+  }
+  for (int t = 0; t < nt; t++) {
+    const int x = tasks[4 * t], y = tasks[4 * t + 1], k = tasks[4 * t + 2];
+    if (k == 2) {  // one-warp supernodes P.solveSmall[x .. x + y)
+      for (int i = x; i < x + y; i++) {
+        const int s = P.solveSmall[i];
+        edge(nt + ns + s, t);
+        edge(t, nt + s);
+        prio[t] = std::max(prio[t], cSmall + tail[s]);
+      }
+    } else if (k == 3) {
+      edge(nt + ns + x, t);
+      edge(t, nt + x);
+      prio[t] = cWhole + tail[x];
+    } else if (k == 0) {
+      const int nb = P.blkOff[x + 1] - P.blkOff[x];
+      edge(y == 0 ? nt + ns + x : diagAt[P.blkOff[x] + y - 1], t);
+      prio[t] = (nb - y) * cDiag + (P.snM[x] > P.snNc[x] ? cBelow : 0.0) + tail[x];
+    } else {
+      edge(lastDiag[x], t);
+      edge(t, nt + x);
+      prio[t] = cBelow + tail[x];
+    }
+  }
+  for (int s = 0; s < ns; s++)
+    if (P.snParent[s] >= 0) edge(nt + s, nt + ns + P.snParent[s]);
+  // Kahn's algorithm: virtual nodes pass through at once, tasks leave the heap by priority
+  std::vector<std::pair<double, int>> heap;  // (priority, -index)
+  auto cmp = [](const std::pair<double, int> &a, const std::pair<double, int> &b) { return a < b; };
+  std::vector<int> stack;
+  auto release = [&](int v) {
+    if (v < nt) {
+      heap.push_back({prio[v], -v});
+      std::push_heap(heap.begin(), heap.end(), cmp);
+    } else {
+      stack.push_back(v);
+    }
+  };
+  auto drain = [&]() {
+    while (!stack.empty()) {
+      const int v = stack.back();
+      stack.pop_back();
+      for (int w : succ[v])
+        if (--indeg[w] == 0) release(w);
+    }
+  };
+  for (int v = 0; v < nn; v++)
+    if (indeg[v] == 0) release(v);
+  drain();
+  std::vector<int> out;
+  out.reserve(tasks.size());
+  while (!heap.empty()) {
+    std::pop_heap(heap.begin(), heap.end(), cmp);
+    const int t = -heap.back().second;
+    heap.pop_back();
+    out.insert(out.end(), tasks.begin() + 4 * (size_t)t, tasks.begin() + 4 * (size_t)t + 4);
+    for (int w : succ[t])
+      if (--indeg[w] == 0) release(w);
+    drain();
+  }
+  if (out.size() != tasks.size()) throw std::logic_error("forward task order: the dependency graph has a cycle");
+  tasks.swap(out);
+}
+
+// The backward task list in critical-path order, as the forward one: a topological order (a supernode's tasks after
+// all of its parent's, its diagonal blocks from the last down) listing first, among the tasks whose predecessors are
+// listed, the one with the longest estimated path to the end of the sweep (its remaining blocks, then the longest
+// chain of descendants below it). small(s): a one-warp supernode (in a group task).
+static void order_backward_by_path(const Plan &P, const std::vector<char> &small, std::vector<int> &tasks) {
+  constexpr double cDiag = 2.7, cSmall = 5.0;  // estimated task times (microseconds)
+  const int ns = (int)P.snNc.size(), nt = (int)(tasks.size() / 4);
+  auto span = [&](int s) { return small[s] ? cSmall : (P.blkOff[s + 1] - P.blkOff[s]) * cDiag; };
+  std::vector<double> tail(ns, 0.0);  // from s's solution complete to the end of the sweep (its descendants)
+  for (int L = 0; L < P.nlevels; L++)
+    for (int q = P.lvlPtr[L]; q < P.lvlPtr[L + 1]; q++) {
+      const int s = P.lvlSn[q], par = P.snParent[s];
+      if (par >= 0) tail[par] = std::max(tail[par], span(s) + tail[s]);
+    }
+  // nodes: tasks [0, nt), "s solved" [nt, nt + ns)
+  const int nn = nt + ns;
+  std::vector<std::vector<int>> succ(nn);
+  std::vector<int> indeg(nn, 0);
+  std::vector<double> prio(nt, 0.0);
+  auto edge = [&](int a, int b) {
+    succ[a].push_back(b);
+    indeg[b]++;
+  };
+  std::vector<int> blkAt(P.nflags, -1);
+  for (int t = 0; t < nt; t++)
+    if (tasks[4 * t + 2] == 0) blkAt[P.blkOff[tasks[4 * t]] + tasks[4 * t + 1]] = t;
+  for (int t = 0; t < nt; t++) {
+    const int x = tasks[4 * t], y = tasks[4 * t + 1], k = tasks[4 * t + 2];
+    if (k == 2) {  // one-warp supernodes P.solveSmall[x .. x + y)
+      for (int i = x; i < x + y; i++) {
+        const int s = P.solveSmall[i];
+        if (P.snParent[s] >= 0) edge(nt + P.snParent[s], t);
+        edge(t, nt + s);
+        prio[t] = std::max(prio[t], cSmall + tail[s]);
+      }
+    } else {
+      const int nb = P.blkOff[x + 1] - P.blkOff[x];
+      if (y == nb - 1) {
+        if (P.snParent[x] >= 0) edge(nt + P.snParent[x], t);
+      } else {
+        edge(blkAt[P.blkOff[x] + y + 1], t);
+      }
+      if (y == 0) edge(t, nt + x);
+      prio[t] = (y + 1) * cDiag + tail[x];
+    }
+  }
+  std::vector<std::pair<double, int>> heap;  // (priority, -index)
+  std::vector<int> stack;
+  auto release = [&](int v) {
+    if (v < nt) {
+      heap.push_back({prio[v], -v});
+      std::push_heap(heap.begin(), heap.end());
+    } else {
+      stack.push_back(v);
+    }
+  };
+  auto drain = [&]() {
+    while (!stack.empty()) {
+      const int v = stack.back();
+      stack.pop_back();
+      for (int w : succ[v])
+        if (--indeg[w] == 0) release(w);
+    }
+  };
+  for (int v = 0; v < nn; v++)
+    if (indeg[v] == 0) release(v);
+  drain();
+  std::vector<int> out;
+  out.reserve(tasks.size());
+  while (!heap.empty()) {
+    std::pop_heap(heap.begin(), heap.end());
+    const int t = -heap.back().second;
+    heap.pop_back();
+    out.insert(out.end(), tasks.begin() + 4 * (size_t)t, tasks.begin() + 4 * (size_t)t + 4);
+    for (int w : succ[t])
+      if (--indeg[w] == 0) release(w);
+    drain();
+  }
+  if (out.size() != tasks.size()) throw std::logic_error("backward task order: the dependency graph has a cycle");
+  tasks.swap(out);
+}
+
 void build_plan(const Symbolic &S, Plan &P, const Tuning &tune) {
   P = Plan();
   if (tune.groupBlocks < 1 || tune.groupBlocks > 16 || tune.smallCut < kTinyFront || tune.smallCut > kSmallFront ||
@@ -436,11 +619,21 @@ void build_plan(const Symbolic &S, Plan &P, const Tuning &tune) {
       }
     P.bwdLvlPtr[L + 1] = (int)(P.bwdTasks.size() / 4);
   }
-  // the whole backward sweep in one launch: levels top-down
+  {
+    std::vector<int> kinds(ns);
+    for (int s = 0; s < ns; s++) kinds[s] = solveSmall(s) ? 0 : whole(s) ? 1 : 2;
+    order_forward_by_path(P, kinds, P.fwdTasks1);
+  }
+  // the whole backward sweep in one launch: levels top-down, then in critical-path order
   P.bwdAll.clear();
   for (int L = P.nlevels - 1; L >= 0; L--)
     P.bwdAll.insert(P.bwdAll.end(), P.bwdTasks.begin() + 4 * (size_t)P.bwdLvlPtr[L],
                     P.bwdTasks.begin() + 4 * (size_t)P.bwdLvlPtr[L + 1]);
+  {
+    std::vector<char> small(ns);
+    for (int s = 0; s < ns; s++) small[s] = solveSmall(s);
+    order_backward_by_path(P, small, P.bwdAll);
+  }
 }
 
 void build_dense_all(const Plan &P, DenseSched &D) {

@@ -82,7 +82,7 @@ typedef struct {
      block y of supernode x, kind 1 the 64-row chunk y of supernode x's rows below, kind 2 the supernodes
      SOLVE_SMALL[x .. x + y) (one warp each), kind 3 the whole supernode x;
    - AMP_F_FWD_TASKS_MULTI: the multi-vector forward sweep's tasks (kinds 0-2);
-   - AMP_F_BWD_TASKS: the backward sweep's tasks, levels top-down (kinds 0 and 2);
+   - AMP_F_BWD_TASKS: the backward sweep's tasks in launch order (kinds 0 and 2), a supernode's after its parent's;
    - AMP_F_SOLVE_SMALL: supernodes solved whole by one warp (m <= 32), grouped by level;
    - AMP_F_TINY_FRONTS, AMP_F_TINY_PTR (int64), AMP_F_TINY_MID (int64): fronts factored whole by one warp (m <= 32):
      level L's are TINY_FRONTS[TINY_PTR[L] .. TINY_PTR[L + 1]), sorted by m, those from TINY_MID[L] on with m > 16. */
