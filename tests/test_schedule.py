@@ -51,14 +51,29 @@ def _cases():
         ("chain-300", lambda: wl.chain(300), "amd"),
         ("arrow-150", lambda: _arrow(150), "amd"),
         ("one", lambda: _diagonal(1), "amd"),
+        # a forest of uneven trees: 12 problems of the batched heat set, block-diagonal, per-matrix AMD orders
+        ("heat2d-batch-12", _batch12, "perm"),
     ]
+
+
+class _Batch:
+    def __init__(self, ws):
+        import batch
+
+        self.pat, offs, _ = batch.block_diagonal([w.pat for w in ws])
+        self.perm = np.concatenate([amp.amdOrder(w.pat) + offs[i] for i, w in enumerate(ws)]).astype(np.int32)
+        self.x = self.y = self.z = None
+
+
+def _batch12():
+    return _Batch(wl.heat2d_batch(12))
 
 
 @pytest.fixture(scope="module", params=_cases(), ids=lambda c: c[0])
 def plan(request):
     _, make, ordering = request.param
     w = make()
-    kw = {"ordering": ordering}
+    kw = {"perm": w.perm} if ordering == "perm" else {"ordering": ordering}
     if ordering in ("nd", "nd3") and w.x is not None:
         kw.update(x=w.x, y=w.y, z=w.z)
     sym = amp.analyze(w.pat, **kw)
@@ -139,10 +154,12 @@ def _backward_violations(tasks, small, nc, par):
     ns = len(nc)
     first, last, _ = _walk(tasks, small)
     bad = [("parent after child", s) for s in range(ns) if par[s] >= 0 and not last[int(par[s])] < first[s]]
-    T = tasks.reshape(-1, 4)
-    for s in range(ns):
-        blks = [int(y) for (x, y, k, _) in T if k == 0 and x == s]
-        if blks != sorted(blks, reverse=True):
+    blks = {}
+    for (x, y, k, _) in tasks.reshape(-1, 4):
+        if k == 0:
+            blks.setdefault(int(x), []).append(int(y))
+    for s in sorted(blks):
+        if blks[s] != sorted(blks[s], reverse=True):
             bad.append(("blocks out of order", s))
     return bad
 
