@@ -27,8 +27,28 @@ import ampsolve as amp
 
 def shiftInvertEigen(pat, K, M, sigma: float, nWant: int, tol: float = 1e-10, blockSize: int = 1,
                      maxBasis: int | None = None, maxRestarts: int = 60, seed: int = 20261106, factor: str = "auto",
-                     kPsd: bool = False, sym=None) -> dict:
-    """Eigenpairs of K x = lambda M x nearest sigma (EigenInput / EigenResult of eigen.ts:14-106)."""
+                     kPsd: bool = False, sym=None, attempts: int = 3) -> dict:
+    """Eigenpairs of K x = lambda M x nearest sigma (EigenInput / EigenResult of eigen.ts:14-106).
+
+    The explicit relative residuals of the refined pairs are checked against max(1e3 tol, 1e-9): a run whose Krylov
+    iteration reported convergence with a pair above that bound (seen intermittently on an indefinite Maxwell pencil,
+    cause not found) is repeated, factorization included, with the next seed, up to `attempts` runs; the result with
+    the smallest worst residual is returned, and stats["attempts"] counts the runs."""
+    best = None
+    for a in range(max(1, attempts)):
+        r = _shift_invert_once(pat, K, M, sigma, nWant, tol, blockSize, maxBasis, maxRestarts, seed + a, factor, kPsd,
+                               sym)
+        worst = float(np.max(r["residual"])) if len(r["residual"]) else 0.0
+        if best is None or worst < best[0]:
+            best = (worst, r)
+        if r["stats"]["converged"] and worst <= max(1e3 * tol, 1e-9):
+            break
+    r = best[1]
+    r["stats"]["attempts"] = a + 1
+    return r
+
+
+def _shift_invert_once(pat, K, M, sigma, nWant, tol, blockSize, maxBasis, maxRestarts, seed, factor, kPsd, sym):
     K = np.ascontiguousarray(K, np.float64)
     M = np.ascontiguousarray(M, np.float64)
     n = int(pat.n)
